@@ -1,0 +1,193 @@
+/*
+ * qm_batch.h — C ABI of the B200 noise-map painter hot path.
+ *
+ * This library replaces what sits behind the painter's exact-evaluation trait
+ * `paint::exact::Batch` (paint/src/exact.rs:163-183) and its CUDA implementor
+ * `paint_gpu::GpuBatch` (paint-gpu/src/batch.rs:247-373). Plain C types only:
+ * host pointers and sizes in, caller-owned host buffers out, a status code back and
+ * `qm_last_error` for the message. Every entry point validates its arguments before
+ * touching the device and names the offending argument in the error text, as
+ * `Gpu::evaluate_pairs` does (paint-gpu/src/device.rs:450-473).
+ *
+ * Frame: positions are lattice steps of `qm_scene_desc.step_m` metres, x east, y north.
+ * Obstacle vertices, sources and receivers all sit on that lattice, so every
+ * segment–edge cross product is an exact integer and crossing lists are reproducible
+ * bit for bit (the reference stores obstacle vertices as exact integers of its own
+ * int16 lattice too: popup/src/obstacles/mod.rs:5-8).
+ */
+#ifndef QM_BATCH_H
+#define QM_BATCH_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define QM_ABI_VERSION 1
+
+#define QM_BANDS 8      /* octave bands 63 Hz .. 8 kHz (physics/src/bands.rs:4) */
+#define QM_PERIODS 3    /* day, evening, night (physics/src/bands.rs:14) */
+#define QM_SECTORS 16   /* favourable-probability sectors (physics/src/weather.rs:16) */
+#define QM_LAYERS 6     /* source layers of a point's bands (paint/src/exact.rs:19) */
+#define QM_THIRDS 28    /* third-octave bands 25 Hz .. 12.5 kHz (physics/src/loudness.rs:12) */
+#define QM_NPD_DISTANCES 10 /* (physics/src/doc29/npd.rs:20) */
+#define QM_PAIR_SUMS 9  /* mixed, calm, downwind per period (paint-gpu/src/device.rs:92) */
+#define QM_POINT_BANDS (QM_LAYERS * QM_PERIODS * QM_BANDS)
+
+typedef enum {
+    QM_OK = 0,
+    QM_ERR_ARGUMENT = 1,    /* an argument is invalid; the message names it */
+    QM_ERR_CUDA = 2,        /* a CUDA call failed; the message starts with "cuda: " */
+    QM_ERR_CAPACITY = 3,    /* a device buffer or per-path capacity was exceeded */
+    QM_ERR_TIMEOUT = 4,     /* a bounded device wait gave up */
+    QM_ERR_UNSUPPORTED = 5  /* no sm_100 device, or a feature this build leaves out */
+} qm_status;
+
+/* Per-pair failure bits, with the reference's meanings (paint-gpu/kernels/common.cuh:27-31). */
+#define QM_FAILED_NOT_READ 1u
+#define QM_FAILED_NO_TERRAIN 2u
+#define QM_FAILED_CAPACITY 4u
+#define QM_FAILED_LINE_CUTOFF 8u
+#define QM_FAILED_TIMEOUT 16u
+
+/* One obstacle outline: a closed ring (its last vertex repeats its first) or an open
+ * wall polyline. Ring vertices are `vertices[first_vertex .. first_vertex + vertex_count)`.
+ * Mirrors the qmobs2 outline record the crossing walk reads
+ * (popup/src/obstacles/crossings.rs:136-149). */
+typedef struct {
+    uint32_t first_vertex;
+    uint32_t vertex_count;
+    uint64_t footprint_id;  /* two walls of one building share it; 0 is reserved */
+    float height_m;         /* above the local ground */
+    uint32_t building;      /* 1 building ring (bounds roofs), 0 barrier/wall */
+} qm_outline;
+
+/* One point source (a 1 m road/rail piece, or any point emitter). Mirrors the
+ * candidate + attribute the pair oracle reads (popup/src/evaluate.rs:47-57, 193-214). */
+typedef struct {
+    int32_t x, y;                 /* lattice steps */
+    float height_m;               /* above its ground */
+    float ground_factor;          /* Gs of (2.5.14); negative: the terrain's under it */
+    float exclusion_radius_m;     /* minimum horizontal distance of the divergence */
+    float platform_half_width_m;  /* terrain clamp near the source (0 for points) */
+    uint64_t footprint_id;        /* the source's own building, 0 none */
+    uint32_t layer;               /* 0 .. QM_LAYERS-1 */
+    uint32_t pad_;
+    float energy[QM_PERIODS][QM_BANDS]; /* A-weighted linear sound power per band */
+} qm_source;
+
+/* A scene: obstacles, terrain, sources and weather, uploaded once and shared by calls. */
+typedef struct {
+    double step_m;                 /* metres per lattice step */
+    int32_t cell_steps;            /* obstacle grid cell side in steps (>= 16) */
+    int32_t extent_steps[2];       /* scene covers [0, extent) steps on each axis */
+    uint32_t n_vertices;
+    const int32_t *vertices;       /* [n_vertices][2] */
+    uint32_t n_outlines;
+    const qm_outline *outlines;
+    /* Terrain: dem_nx == 0 is flat ground at flat_altitude_m with flat_ground_factor.
+     * Otherwise nodes (i, j) at (dem_origin + i*dem_spacing, dem_origin + j*dem_spacing)
+     * steps, row-major [j][i]; altitude and ground factor linear along lattice lines
+     * (physics/src/profile.rs:1-6, popup/src/scene.rs:236-296). */
+    int32_t dem_nx, dem_ny;
+    int32_t dem_origin[2];
+    int32_t dem_spacing;
+    const float *dem_altitude_m;
+    const float *dem_ground_factor;
+    float flat_altitude_m;
+    float flat_ground_factor;
+    uint32_t n_sources;
+    const qm_source *sources;
+    /* Weather of the place (physics/src/weather.rs:46-70): p per period and sector,
+     * sector s centred on bearing 22.5 s degrees clockwise from north; air absorption. */
+    float favourable[QM_PERIODS][QM_SECTORS];
+    float alpha_db_per_km[QM_BANDS];
+} qm_scene_desc;
+
+/* A regular receiver grid for the fused painter: nx*ny receivers at origin + (i, j)*spacing
+ * steps, `height_m` above the ground, in cell order j*nx + i. */
+typedef struct {
+    int32_t origin[2];
+    int32_t spacing;
+    int32_t nx, ny;
+    float height_m;
+    /* Sources [source_begin, source_end) are painted; an empty range means all. */
+    uint32_t source_begin, source_end;
+    /* Histogram of per-cell day dBA levels: bin k holds levels rounding to
+     * level_min_db + k*bin_db (popup/src/distribution.rs:69-72). */
+    float level_min_db;
+    float bin_db;
+    uint32_t n_bins;
+} qm_grid_desc;
+
+typedef struct {
+    uint64_t paths;          /* receiver x source paths evaluated */
+    uint64_t failed_paths;   /* paths re-run by the high-capacity pass */
+    uint64_t crossings;      /* obstacle crossings found */
+    double kernel_ms;        /* device time of the painting kernels */
+} qm_paint_stats;
+
+typedef struct qm_ctx qm_ctx;
+typedef struct qm_scene qm_scene;
+
+/* Library ABI version; a binding checks it before the first call. */
+int qm_abi_version(void);
+
+/* Opens device `device_ordinal` (an sm_100 GPU). Replaces `Gpu::new`
+ * (paint-gpu/src/device.rs:270): kernels are linked in as sm_100a cubins, no NVRTC. */
+qm_status qm_open(int device_ordinal, qm_ctx **out);
+void qm_close(qm_ctx *ctx);
+/* The last error of this context's calls on the calling thread ("" if none). */
+const char *qm_last_error(const qm_ctx *ctx);
+
+/* Uploads a scene: obstacles with their grid cell lists, terrain, sources, weather.
+ * Replaces `DeviceSquare::upload` (paint-gpu/src/square_upload.rs:18). */
+qm_status qm_scene_upload(qm_ctx *ctx, const qm_scene_desc *desc, qm_scene **out);
+void qm_scene_free(qm_scene *scene);
+
+/* Batch::evaluate and Batch::pair_spectra (paint/src/exact.rs:164-170; GPU
+ * `Gpu::evaluate_pairs`, paint-gpu/src/device.rs:440). Receivers at `receiver_xy`
+ * (metres, snapped to the scene lattice), `receiver_height_m` above their ground,
+ * standing in building `own_footprint` (0 none) and adding into point
+ * `point_of_receiver`. Each pair names a source and a receiver; `band_weight` (nullable:
+ * all 1) weighs its spectrum into the point's bands.
+ * Outputs: pair_sums[n_pairs][9] = mixed[3], calm[3], downwind[3] (PairEnergy,
+ * exact.rs:128-132); pair_bands (nullable) [n_pairs][3][8] each pair's unweighted bands
+ * (pair_spectra); point_bands[n_points][6][3][8] += weighted bands by source layer
+ * (add_bands, exact.rs:208-215); pair_status[n_pairs] failure bits. */
+qm_status qm_evaluate_pairs(qm_scene *scene,
+                            const double *receiver_xy, const float *receiver_height_m,
+                            const uint64_t *own_footprint, const uint32_t *point_of_receiver,
+                            size_t n_receivers,
+                            const uint32_t *source_of_pair, const uint32_t *receiver_of_pair,
+                            const float *band_weight, size_t n_pairs,
+                            float *pair_sums, float *pair_bands, uint32_t *pair_status,
+                            float *point_bands, size_t n_points);
+
+/* The fused grid painter: every receiver of `grid` against the source range, with
+ * per-cell compensated energetic sums. Outputs (each nullable): cell_bands[nx*ny][8] day
+ * band levels (dB), cell_dba[nx*ny] day dBA, cell_lden[nx*ny] Lden (dBA), histogram[n_bins]
+ * counts of cell_dba. This is `evaluate_all` over a regular grid (paint/src/exact.rs:218-254)
+ * with `add_bands` folded into the kernel. */
+qm_status qm_paint_grid(qm_scene *scene, const qm_grid_desc *grid,
+                        float *cell_bands, float *cell_dba, float *cell_lden,
+                        uint32_t *histogram, qm_paint_stats *stats);
+
+/* ISO 532-1 stationary Zwicker loudness of n spectra of 28 third-octave levels (dB;
+ * -inf silent): sone[n]. The per-pixel core of `Batch::loudness`
+ * (physics/src/loudness.rs:148; GPU `loud_zwicker`, paint-gpu/kernels/loudness.cuh:85). */
+qm_status qm_zwicker(qm_ctx *ctx, const float *thirds_db, size_t n, float *sone);
+
+/* Level histogram of n levels (dB): counts[n_bins] of round((L - level_min)/bin), clamped
+ * into the grid (popup/src/distribution.rs:69-72). Counts are exact. */
+qm_status qm_level_histogram(qm_ctx *ctx, const float *levels_db, size_t n,
+                             float level_min_db, float bin_db, uint32_t n_bins,
+                             uint32_t *counts);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* QM_BATCH_H */

@@ -1,0 +1,242 @@
+"""ctypes wrapper of the FP64 CPU oracle (oracle/libqm_oracle.so) — TEST INFRASTRUCTURE ONLY.
+
+The oracle restates the reference's CPU physics (quietmap's Rust `physics`, `popup` and `paint`
+crates) in C++ double precision; each C function cites the reference file:line it follows.
+Only tests/, the smoke check and the benchmark's CPU-baseline leg import this module; the
+product path (quietmap_b200) never does.
+"""
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+from quietmap_b200 import abi
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libqm_oracle.so")
+
+_D = C.POINTER(C.c_double)
+_I64 = C.POINTER(C.c_int64)
+_U64 = C.POINTER(C.c_uint64)
+_U32 = C.POINTER(C.c_uint32)
+_I32 = C.POINTER(C.c_int32)
+
+
+def build():
+    """Compiles the oracle with its Makefile (g++ only)."""
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            build()
+        L = C.CDLL(LIB_PATH)
+        L.qmo_alpha_bands.argtypes = [C.c_double, C.c_double, _D]
+        L.qmo_state_boundaries.argtypes = [_D, _D, _D, C.c_size_t, C.c_double, C.c_double, C.c_double,
+                                           C.c_double, C.c_double, _D, C.c_size_t, _D, C.c_size_t, _D, _D]
+        L.qmo_ray_terms.argtypes = [
+            C.c_double, _D, _D, _D, C.c_size_t, _D, _D, _I32, _I32, _U64, C.c_size_t,
+            C.c_double, C.c_int, C.c_double, C.c_double, C.c_int, C.c_double, C.c_double, C.c_uint64,
+            _D, _D, _D, _D, _D, _D, _D, _D, C.c_size_t, C.POINTER(C.c_size_t), _D, C.c_size_t,
+            C.POINTER(C.c_size_t)]
+        L.qmo_crests_of.argtypes = [_D, C.c_size_t, C.c_double, _D, C.c_size_t]
+        L.qmo_crests_of.restype = C.c_size_t
+        L.qmo_scene_new.argtypes = [C.POINTER(abi.SceneDesc)]
+        L.qmo_scene_new.restype = C.c_void_p
+        L.qmo_scene_free.argtypes = [C.c_void_p]
+        L.qmo_crossings.argtypes = [C.c_void_p, _I64, _I64, _D, _U64, _U32, _I32, _I32, C.c_size_t]
+        L.qmo_crossings.restype = C.c_size_t
+        L.qmo_enclosing_buildings.argtypes = [C.c_void_p, _I64, C.c_size_t, _U64, C.c_int]
+        L.qmo_profile.argtypes = [C.c_void_p, _I64, _I64, _D, _D, _D, C.c_size_t, _D]
+        L.qmo_profile.restype = C.c_size_t
+        L.qmo_evaluate_pairs.argtypes = [C.c_void_p, _I64, _D, _U64, _U32, C.c_size_t, _U32, _U32, _D,
+                                         C.c_size_t, _D, _D, _D, C.c_size_t, C.c_int]
+        L.qmo_paint_grid.argtypes = [C.c_void_p, C.POINTER(abi.GridDesc), C.c_uint32, C.c_uint32, _D, _D,
+                                     C.c_int, _U64]
+        L.qmo_zwicker.argtypes = [_D]
+        L.qmo_zwicker.restype = C.c_double
+        L.qmo_zwicker_many.argtypes = [_D, C.c_size_t, _D, C.c_int]
+        L.qmo_level_histogram.argtypes = [_D, C.c_size_t, C.c_double, C.c_double, C.c_uint32, _U32]
+        L.qmo_level_bin.argtypes = [C.c_double, C.c_double, C.c_double, C.c_uint32]
+        L.qmo_level_bin.restype = C.c_uint32
+        _lib = L
+    return _lib
+
+
+def threads():
+    return max(os.cpu_count() or 1, 1)
+
+
+def _d(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def alpha_bands(temperature_c, rh):
+    out = np.zeros(8)
+    lib().qmo_alpha_bands(temperature_c, rh, abi.ptr(out, C.c_double))
+    return out
+
+
+def state_boundaries(d, z, g, source, receiver, source_gf, terrain, tops):
+    """A_boundary of both states of a vertical path: ([2][8] attenuation, [2][8] no-ground)."""
+    d, z, g = _d(d), _d(z), _d(g)
+    terrain = _d(np.asarray(terrain, dtype=np.float64).reshape(-1, 2))
+    tops = _d(np.asarray(tops, dtype=np.float64).reshape(-1, 2))
+    att = np.zeros(16)
+    wog = np.zeros(16)
+    lib().qmo_state_boundaries(abi.ptr(d, C.c_double), abi.ptr(z, C.c_double), abi.ptr(g, C.c_double), len(d),
+                               source[0], source[1], receiver[0], receiver[1], source_gf,
+                               abi.ptr(terrain, C.c_double), len(terrain), abi.ptr(tops, C.c_double), len(tops),
+                               abi.ptr(att, C.c_double), abi.ptr(wog, C.c_double))
+    return att.reshape(2, 8), wog.reshape(2, 8)
+
+
+def ray_terms(horizontal_m, t, ground_m, ground_factor, crossings, ends, p, alpha):
+    """One ray's transfer; crossings rows (t, height, building, bounds_roof, footprint)."""
+    t, zg, gf = _d(t), _d(ground_m), _d(ground_factor)
+    ct = _d([c[0] for c in crossings])
+    ch = _d([c[1] for c in crossings])
+    cb = np.ascontiguousarray([int(c[2]) for c in crossings], dtype=np.int32)
+    cr = np.ascontiguousarray([int(c[3]) for c in crossings], dtype=np.int32)
+    cf = np.ascontiguousarray([c[4] for c in crossings], dtype=np.uint64)
+    p, alpha = _d(p), _d(alpha)
+    slant = np.zeros(1)
+    periods = np.zeros(24)
+    states = np.zeros(16)
+    cap = 4096
+    pd, pz, pg = np.zeros(cap), np.zeros(cap), np.zeros(cap)
+    tops = np.zeros(2 * cap)
+    n_path = C.c_size_t()
+    n_tops = C.c_size_t()
+    sg = ends.get("source_ground_m")
+    sgf = ends.get("source_ground_factor")
+    lib().qmo_ray_terms(horizontal_m, abi.ptr(t, C.c_double), abi.ptr(zg, C.c_double), abi.ptr(gf, C.c_double),
+                        len(t), abi.ptr(ct, C.c_double), abi.ptr(ch, C.c_double), abi.ptr(cb, C.c_int32),
+                        abi.ptr(cr, C.c_int32), abi.ptr(cf, C.c_uint64), len(ct), ends["source_height_m"],
+                        int(sg is not None), float(sg or 0.0), ends["receiver_altitude_m"],
+                        int(sgf is not None), float(sgf or 0.0), ends.get("platform_half_width_m", 0.0),
+                        ends.get("own_footprint", 0), abi.ptr(p, C.c_double), abi.ptr(alpha, C.c_double),
+                        abi.ptr(slant, C.c_double), abi.ptr(periods, C.c_double), abi.ptr(states, C.c_double),
+                        abi.ptr(pd, C.c_double), abi.ptr(pz, C.c_double), abi.ptr(pg, C.c_double), cap,
+                        C.byref(n_path), abi.ptr(tops, C.c_double), cap, C.byref(n_tops))
+    n, m = n_path.value, n_tops.value
+    return dict(slant_m=slant[0], periods=periods.reshape(3, 8), states=states.reshape(2, 8),
+                path_d=pd[:n].copy(), path_z=pz[:n].copy(), path_g=pg[:n].copy(),
+                tops=tops[:2 * m].reshape(m, 2).copy())
+
+
+def crests_of(points, length):
+    xz = _d(np.asarray(points, dtype=np.float64).reshape(-1, 2))
+    out = np.zeros(2 * max(len(xz), 1))
+    n = lib().qmo_crests_of(abi.ptr(xz, C.c_double), len(xz), length, abi.ptr(out, C.c_double), len(xz))
+    return out[:2 * n].reshape(n, 2)
+
+
+class OracleScene:
+    """The oracle's copy of a scene (its own cell lists), built from the ABI descriptor."""
+
+    def __init__(self, scene):
+        self.packed = abi.PackedScene(scene)
+        self.scene = scene
+        self.handle = lib().qmo_scene_new(C.byref(self.packed.desc))
+
+    def __del__(self):
+        if getattr(self, "handle", None):
+            lib().qmo_scene_free(self.handle)
+            self.handle = None
+
+    def crossings(self, frm, to, cap=4096):
+        frm = np.ascontiguousarray(frm, dtype=np.int64)
+        to = np.ascontiguousarray(to, dtype=np.int64)
+        t = np.zeros(cap)
+        fp = np.zeros(cap, np.uint64)
+        edge = np.zeros(cap, np.uint32)
+        br = np.zeros(cap, np.int32)
+        bd = np.zeros(cap, np.int32)
+        n = lib().qmo_crossings(self.handle, abi.ptr(frm, C.c_int64), abi.ptr(to, C.c_int64),
+                                abi.ptr(t, C.c_double), abi.ptr(fp, C.c_uint64), abi.ptr(edge, C.c_uint32),
+                                abi.ptr(br, C.c_int32), abi.ptr(bd, C.c_int32), cap)
+        n = min(n, cap)
+        return dict(t=t[:n].copy(), footprint=fp[:n].copy(), edge=edge[:n].copy(),
+                    bounds_roof=br[:n].astype(bool), building=bd[:n].astype(bool))
+
+    def enclosing(self, xy):
+        xy = np.ascontiguousarray(np.asarray(xy).reshape(-1, 2), dtype=np.int64)
+        out = np.zeros(len(xy), np.uint64)
+        lib().qmo_enclosing_buildings(self.handle, abi.ptr(xy, C.c_int64), len(xy), abi.ptr(out, C.c_uint64),
+                                      threads())
+        return out
+
+    def profile(self, frm, to, cap=65536):
+        frm = np.ascontiguousarray(frm, dtype=np.int64)
+        to = np.ascontiguousarray(to, dtype=np.int64)
+        t, z, g = np.zeros(cap), np.zeros(cap), np.zeros(cap)
+        h = np.zeros(1)
+        n = lib().qmo_profile(self.handle, abi.ptr(frm, C.c_int64), abi.ptr(to, C.c_int64), abi.ptr(t, C.c_double),
+                              abi.ptr(z, C.c_double), abi.ptr(g, C.c_double), cap, abi.ptr(h, C.c_double))
+        return h[0], t[:n].copy(), z[:n].copy(), g[:n].copy()
+
+    def evaluate_pairs(self, receiver_xy, receiver_altitude, own_footprint, point_of_receiver, source_of_pair,
+                       receiver_of_pair, band_weight, n_points, nthreads=None):
+        rxy = np.ascontiguousarray(np.asarray(receiver_xy).reshape(-1, 2), dtype=np.int64)
+        ralt = _d(receiver_altitude)
+        own = np.ascontiguousarray(own_footprint, dtype=np.uint64)
+        por = np.ascontiguousarray(point_of_receiver, dtype=np.uint32)
+        sop = np.ascontiguousarray(source_of_pair, dtype=np.uint32)
+        rop = np.ascontiguousarray(receiver_of_pair, dtype=np.uint32)
+        bw = None if band_weight is None else _d(band_weight)
+        n = len(sop)
+        sums = np.zeros((n, 9))
+        bands = np.zeros((n, 3, 8))
+        points = np.zeros((n_points, 6, 3, 8))
+        lib().qmo_evaluate_pairs(self.handle, abi.ptr(rxy, C.c_int64), abi.ptr(ralt, C.c_double),
+                                 abi.ptr(own, C.c_uint64), abi.ptr(por, C.c_uint32), len(rxy),
+                                 abi.ptr(sop, C.c_uint32), abi.ptr(rop, C.c_uint32),
+                                 abi.ptr(bw, C.c_double) if bw is not None else None, n,
+                                 abi.ptr(sums, C.c_double), abi.ptr(bands, C.c_double), abi.ptr(points, C.c_double),
+                                 n_points, nthreads or threads())
+        return sums, bands, points
+
+    def paint_grid(self, grid, cell_begin=0, cell_end=0, nthreads=None):
+        """Per cell (of [cell_begin, cell_end), all when empty) the day band energies [n][8],
+        the Lden-weighted A energy [n] and the number of edge tests."""
+        g = abi.grid_desc(grid)
+        n = (cell_end - cell_begin) if cell_end > cell_begin else grid.cells
+        energy = np.zeros((n, 8))
+        lden = np.zeros(n)
+        tested = C.c_uint64()
+        lib().qmo_paint_grid(self.handle, C.byref(g), cell_begin, cell_end, abi.ptr(energy, C.c_double),
+                             abi.ptr(lden, C.c_double), nthreads or threads(), C.byref(tested))
+        return energy, lden, tested.value
+
+
+def zwicker(levels28):
+    levels = _d(levels28)
+    return lib().qmo_zwicker(abi.ptr(levels, C.c_double))
+
+
+def zwicker_many(levels, nthreads=None):
+    levels = _d(np.asarray(levels).reshape(-1, 28))
+    out = np.zeros(len(levels))
+    lib().qmo_zwicker_many(abi.ptr(levels, C.c_double), len(levels), abi.ptr(out, C.c_double),
+                           nthreads or threads())
+    return out
+
+
+def level_histogram(levels, level_min, bin_db, n_bins):
+    levels = _d(levels)
+    counts = np.zeros(n_bins, np.uint32)
+    lib().qmo_level_histogram(abi.ptr(levels, C.c_double), len(levels), level_min, bin_db, n_bins,
+                              abi.ptr(counts, C.c_uint32))
+    return counts
+
+
+def level_bin(level, level_min, bin_db, n_bins):
+    return lib().qmo_level_bin(level, level_min, bin_db, n_bins)

@@ -1,0 +1,178 @@
+"""ctypes mirror of include/qm_batch.h: the structs and constants of the C ABI.
+
+The Rust painter binds the same structs through its FFI; this module is the
+Python binding used by the host mirror of `paint::exact::Batch`, the tests and the benchmark.
+"""
+
+import ctypes as C
+
+import numpy as np
+
+ABI_VERSION = 1
+BANDS = 8
+PERIODS = 3
+SECTORS = 16
+LAYERS = 6
+THIRDS = 28
+PAIR_SUMS = 9
+POINT_BANDS = LAYERS * PERIODS * BANDS
+
+QM_OK = 0
+QM_ERR_ARGUMENT = 1
+QM_ERR_CUDA = 2
+QM_ERR_CAPACITY = 3
+QM_ERR_TIMEOUT = 4
+QM_ERR_UNSUPPORTED = 5
+
+FAILED_NOT_READ = 1
+FAILED_NO_TERRAIN = 2
+FAILED_CAPACITY = 4
+FAILED_LINE_CUTOFF = 8
+FAILED_TIMEOUT = 16
+
+
+class Outline(C.Structure):
+    _fields_ = [
+        ("first_vertex", C.c_uint32),
+        ("vertex_count", C.c_uint32),
+        ("footprint_id", C.c_uint64),
+        ("height_m", C.c_float),
+        ("building", C.c_uint32),
+    ]
+
+
+class Source(C.Structure):
+    _fields_ = [
+        ("x", C.c_int32),
+        ("y", C.c_int32),
+        ("height_m", C.c_float),
+        ("ground_factor", C.c_float),
+        ("exclusion_radius_m", C.c_float),
+        ("platform_half_width_m", C.c_float),
+        ("footprint_id", C.c_uint64),
+        ("layer", C.c_uint32),
+        ("pad_", C.c_uint32),
+        ("energy", (C.c_float * BANDS) * PERIODS),
+    ]
+
+
+class SceneDesc(C.Structure):
+    _fields_ = [
+        ("step_m", C.c_double),
+        ("cell_steps", C.c_int32),
+        ("extent_steps", C.c_int32 * 2),
+        ("n_vertices", C.c_uint32),
+        ("vertices", C.POINTER(C.c_int32)),
+        ("n_outlines", C.c_uint32),
+        ("outlines", C.POINTER(Outline)),
+        ("dem_nx", C.c_int32),
+        ("dem_ny", C.c_int32),
+        ("dem_origin", C.c_int32 * 2),
+        ("dem_spacing", C.c_int32),
+        ("dem_altitude_m", C.POINTER(C.c_float)),
+        ("dem_ground_factor", C.POINTER(C.c_float)),
+        ("flat_altitude_m", C.c_float),
+        ("flat_ground_factor", C.c_float),
+        ("n_sources", C.c_uint32),
+        ("sources", C.POINTER(Source)),
+        ("favourable", (C.c_float * SECTORS) * PERIODS),
+        ("alpha_db_per_km", C.c_float * BANDS),
+    ]
+
+
+class GridDesc(C.Structure):
+    _fields_ = [
+        ("origin", C.c_int32 * 2),
+        ("spacing", C.c_int32),
+        ("nx", C.c_int32),
+        ("ny", C.c_int32),
+        ("height_m", C.c_float),
+        ("source_begin", C.c_uint32),
+        ("source_end", C.c_uint32),
+        ("level_min_db", C.c_float),
+        ("bin_db", C.c_float),
+        ("n_bins", C.c_uint32),
+    ]
+
+
+class PaintStats(C.Structure):
+    _fields_ = [
+        ("paths", C.c_uint64),
+        ("failed_paths", C.c_uint64),
+        ("crossings", C.c_uint64),
+        ("kernel_ms", C.c_double),
+    ]
+
+
+# numpy structured dtypes with the same layout (one upload of many records at once).
+OUTLINE_DTYPE = np.dtype(
+    [("first_vertex", "<u4"), ("vertex_count", "<u4"), ("footprint_id", "<u8"),
+     ("height_m", "<f4"), ("building", "<u4")], align=True)
+SOURCE_DTYPE = np.dtype(
+    [("x", "<i4"), ("y", "<i4"), ("height_m", "<f4"), ("ground_factor", "<f4"),
+     ("exclusion_radius_m", "<f4"), ("platform_half_width_m", "<f4"), ("footprint_id", "<u8"),
+     ("layer", "<u4"), ("pad_", "<u4"), ("energy", "<f4", (PERIODS, BANDS))], align=True)
+
+assert OUTLINE_DTYPE.itemsize == C.sizeof(Outline)
+assert SOURCE_DTYPE.itemsize == C.sizeof(Source)
+
+
+def ptr(array, ctype):
+    """A ctypes pointer into a contiguous numpy array (None for None)."""
+    if array is None:
+        return None
+    if not array.flags["C_CONTIGUOUS"]:
+        raise ValueError("array must be C-contiguous")
+    return array.ctypes.data_as(C.POINTER(ctype))
+
+
+class PackedScene:
+    """A scene descriptor with the numpy arrays it points into kept alive."""
+
+    def __init__(self, scene):
+        self.scene = scene
+        self.vertices = np.ascontiguousarray(scene.vertices, dtype=np.int32).reshape(-1, 2)
+        self.outlines = np.ascontiguousarray(scene.outlines, dtype=OUTLINE_DTYPE)
+        self.sources = np.ascontiguousarray(scene.sources, dtype=SOURCE_DTYPE)
+        d = SceneDesc()
+        d.step_m = scene.step_m
+        d.cell_steps = scene.cell_steps
+        d.extent_steps[0], d.extent_steps[1] = scene.extent_steps
+        d.n_vertices = len(self.vertices)
+        d.vertices = ptr(self.vertices, C.c_int32)
+        d.n_outlines = len(self.outlines)
+        d.outlines = self.outlines.ctypes.data_as(C.POINTER(Outline))
+        if scene.dem_altitude is not None:
+            self.dem_z = np.ascontiguousarray(scene.dem_altitude, dtype=np.float32)
+            self.dem_g = np.ascontiguousarray(scene.dem_ground_factor, dtype=np.float32)
+            d.dem_ny, d.dem_nx = self.dem_z.shape
+            d.dem_origin[0], d.dem_origin[1] = scene.dem_origin
+            d.dem_spacing = scene.dem_spacing
+            d.dem_altitude_m = ptr(self.dem_z, C.c_float)
+            d.dem_ground_factor = ptr(self.dem_g, C.c_float)
+        else:
+            d.dem_nx = d.dem_ny = 0
+        d.flat_altitude_m = scene.flat_altitude_m
+        d.flat_ground_factor = scene.flat_ground_factor
+        d.n_sources = len(self.sources)
+        d.sources = self.sources.ctypes.data_as(C.POINTER(Source))
+        fav = np.asarray(scene.favourable, dtype=np.float32).reshape(PERIODS, SECTORS)
+        for p in range(PERIODS):
+            for s in range(SECTORS):
+                d.favourable[p][s] = float(fav[p, s])
+        for b in range(BANDS):
+            d.alpha_db_per_km[b] = float(scene.alpha_db_per_km[b])
+        self.desc = d
+
+
+def grid_desc(grid):
+    g = GridDesc()
+    g.origin[0], g.origin[1] = grid.origin
+    g.spacing = grid.spacing
+    g.nx, g.ny = grid.nx, grid.ny
+    g.height_m = grid.height_m
+    g.source_begin, g.source_end = grid.source_begin, grid.source_end
+    g.level_min_db = grid.level_min_db
+    g.bin_db = grid.bin_db
+    g.n_bins = grid.n_bins
+    return g

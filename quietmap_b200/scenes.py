@@ -1,0 +1,295 @@
+"""Seeded synthetic scenes of the painter workloads (there are no real tiles on this box).
+
+Every scene comes from one `numpy.random.default_rng(seed)` stream. Positions are lattice steps
+(x east, y north) of `step_m` metres; obstacle vertices, receivers and source points are lattice
+points, so crossing tests are exact integer arithmetic (the reference stores obstacle vertices
+as exact integers of its lattice too: popup/src/obstacles/mod.rs:5-8).
+
+Workloads:
+- `road_square` — 1 km x 1 km, flat ground G = 0.5, homogeneous air, 400 straight roads split
+  into 1 m point sources at 0.05 m, 300 rotated rectangular buildings; 128 x 128 receivers at
+  7.8125 m, 4 m high.
+- `terrain_square` — the 16 km^2 terrain square: 2048 x 2048 receivers at 1.953125 m, fBm DEM
+  (Hurst 0.8, 5 m posts, +-40 m), Voronoi ground factor (200 cells, G in {0, 0.5, 1}), 20,000 road
+  and rail segments at 1 m points, 30,000 polygon buildings of 4-12 vertices (log-normal heights,
+  median 9 m, sigma 0.6), favourable probability 0.5 in every sector. `scale` shrinks the side and
+  every count with the area, keeping the densities.
+"""
+
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import abi
+from .physics import alpha_bands
+
+# A-weighted octave shapes (dB relative to the base level), 63 Hz .. 8 kHz: a road's rolling
+# noise and a railway's, each an unweighted shape plus the A-weighting of the bands
+# (physics/src/bands.rs:11).
+A_WEIGHTING_DB = np.array([-26.2, -16.1, -8.6, -3.2, 0.0, 1.2, 1.0, -1.1])
+ROAD_SHAPE_DB = np.array([-7.0, -6.0, -5.0, -4.0, -3.0, -5.0, -8.0, -12.0]) + A_WEIGHTING_DB
+RAIL_SHAPE_DB = np.array([-9.0, -7.0, -5.0, -3.0, -2.0, -3.0, -6.0, -11.0]) + A_WEIGHTING_DB
+# Evening and night emissions relative to the day (dB).
+PERIOD_OFFSETS_DB = np.array([0.0, -3.0, -8.0])
+
+
+@dataclass
+class Scene:
+    step_m: float
+    cell_steps: int
+    extent_steps: tuple
+    vertices: np.ndarray            # [n][2] int32
+    outlines: np.ndarray            # OUTLINE_DTYPE
+    sources: np.ndarray             # SOURCE_DTYPE
+    favourable: np.ndarray          # [3][16]
+    alpha_db_per_km: np.ndarray     # [8]
+    flat_altitude_m: float = 0.0
+    flat_ground_factor: float = 0.5
+    dem_altitude: np.ndarray = None  # [ny][nx] float32
+    dem_ground_factor: np.ndarray = None
+    dem_origin: tuple = (0, 0)
+    dem_spacing: int = 0
+    name: str = ""
+    info: dict = field(default_factory=dict)
+
+
+@dataclass
+class Grid:
+    origin: tuple
+    spacing: int
+    nx: int
+    ny: int
+    height_m: float = 4.0
+    source_begin: int = 0
+    source_end: int = 0
+    level_min_db: float = -30.0
+    bin_db: float = 0.1
+    n_bins: int = 1800
+
+    @property
+    def cells(self):
+        return self.nx * self.ny
+
+    def receiver_xy(self):
+        """[cells][2] lattice steps in cell order j*nx + i."""
+        j, i = np.divmod(np.arange(self.cells, dtype=np.int64), self.nx)
+        return np.stack([self.origin[0] + i * self.spacing, self.origin[1] + j * self.spacing], axis=1)
+
+
+def _outlines(records):
+    out = np.zeros(len(records), dtype=abi.OUTLINE_DTYPE)
+    for k, (first, count, fp, height, building) in enumerate(records):
+        out[k] = (first, count, fp, height, building)
+    return out
+
+
+def _rectangle(rng, centre, sides, angle):
+    c, s = np.cos(angle), np.sin(angle)
+    hx, hy = sides[0] / 2, sides[1] / 2
+    corners = np.array([[-hx, -hy], [hx, -hy], [hx, hy], [-hx, hy]])
+    rot = np.array([[c, -s], [s, c]])
+    return corners @ rot.T + centre
+
+
+def _convex_polygon(rng, centre, radius, n):
+    angles = np.sort(rng.uniform(0, 2 * np.pi, n))
+    # Spread the angles so no two vertices nearly coincide.
+    angles = np.sort((angles + np.linspace(0, 2 * np.pi, n, endpoint=False)) / 2 % (2 * np.pi))
+    r = radius * rng.uniform(0.75, 1.0, n)
+    return centre + np.stack([r * np.cos(angles), r * np.sin(angles)], axis=1)
+
+
+def _signed_area2(p):
+    x, y = p[:, 0], p[:, 1]
+    return float(np.sum(x * np.roll(y, -1) - np.roll(x, -1) * y))
+
+
+def _place_buildings(rng, n, side_m, make, min_gap_m, margin_m):
+    """Rejection-sampled non-overlapping footprints: bounding circles kept `min_gap_m` apart."""
+    cell = 48.0
+    grid = {}
+    placed = []
+    attempts = 0
+    while len(placed) < n and attempts < 200 * n:
+        attempts += 1
+        polygon, radius = make(rng)
+        centre = rng.uniform(margin_m + radius, side_m - margin_m - radius, 2)
+        key = (int(centre[0] // cell), int(centre[1] // cell))
+        ok = True
+        for dx in (-1, 0, 1):
+            for dy in (-1, 0, 1):
+                for (oc, orad) in grid.get((key[0] + dx, key[1] + dy), ()):
+                    if np.hypot(*(oc - centre)) < radius + orad + min_gap_m:
+                        ok = False
+                        break
+                if not ok:
+                    break
+            if not ok:
+                break
+        if not ok:
+            continue
+        grid.setdefault(key, []).append((centre, radius))
+        placed.append(polygon + centre)
+    return placed
+
+
+def _rings_to_arrays(polygons, heights, step_m, first_id=1):
+    verts, records = [], []
+    for k, (poly, height) in enumerate(zip(polygons, heights)):
+        pts = np.round(poly / step_m).astype(np.int64)
+        # Counter-clockwise, distinct consecutive vertices, closed by repeating the first.
+        keep = [pts[0]]
+        for p in pts[1:]:
+            if not np.array_equal(p, keep[-1]):
+                keep.append(p)
+        if np.array_equal(keep[-1], keep[0]) and len(keep) > 1:
+            keep.pop()
+        pts = np.array(keep)
+        if len(pts) < 3:
+            continue
+        if _signed_area2(pts.astype(np.float64)) < 0:
+            pts = pts[::-1]
+        ring = np.vstack([pts, pts[:1]])
+        records.append((sum(len(v) for v in verts), len(ring), first_id + k, float(height), 1))
+        verts.append(ring)
+    vertices = np.vstack(verts).astype(np.int32) if verts else np.zeros((0, 2), np.int32)
+    return vertices, _outlines(records)
+
+
+def _segments_to_points(rng, n_segments, side_m, step_m, kind_of, base_of, margin_m=1.0):
+    """Straight segments with ends uniform in the square, length clipped to [20, 200] m, split
+    into 1 m point sources at their piece centres (snapped to the lattice)."""
+    xs, ys, hs, energy, layers = [], [], [], [], []
+    for k in range(n_segments):
+        a = rng.uniform(margin_m, side_m - margin_m, 2)
+        b = rng.uniform(margin_m, side_m - margin_m, 2)
+        d = b - a
+        length = float(np.hypot(*d))
+        if length < 1e-9:
+            d, length = np.array([1.0, 0.0]), 1.0
+        target = min(max(length, 20.0), 200.0)
+        b = np.clip(a + d * (target / length), margin_m, side_m - margin_m)
+        d = b - a
+        length = float(np.hypot(*d))
+        count = max(int(round(length)), 1)
+        kind = kind_of(k)
+        base = base_of(kind)
+        shape = ROAD_SHAPE_DB if kind == 0 else RAIL_SHAPE_DB
+        levels = base + shape + rng.normal(0.0, 2.0, 8)  # per metre, A-weighted
+        f = (np.arange(count) + 0.5) / count
+        pts = a + f[:, None] * d
+        xs.append(np.round(pts[:, 0] / step_m))
+        ys.append(np.round(pts[:, 1] / step_m))
+        piece_m = length / count
+        e_day = 10.0 ** (levels / 10.0) * piece_m
+        energy.append(np.repeat(e_day[None, :], count, axis=0))
+        hs.append(np.full(count, 0.05 if kind == 0 else 0.5))
+        layers.append(np.full(count, kind))
+    x = np.concatenate(xs).astype(np.int32)
+    y = np.concatenate(ys).astype(np.int32)
+    e = np.concatenate(energy)
+    src = np.zeros(len(x), dtype=abi.SOURCE_DTYPE)
+    src["x"], src["y"] = x, y
+    src["height_m"] = np.concatenate(hs)
+    src["ground_factor"] = -1.0
+    src["layer"] = np.concatenate(layers)
+    for p in range(abi.PERIODS):
+        src["energy"][:, p, :] = e * 10.0 ** (PERIOD_OFFSETS_DB[p] / 10.0)
+    return src
+
+
+def road_square(seed=1, n_roads=400, n_buildings=300, side_m=1000.0, receivers=128,
+                cell_steps=256):
+    """The plain CNOSSOS road painter: flat G = 0.5, homogeneous conditions, 15 C / 70 %."""
+    rng = np.random.default_rng(seed)
+    step_m = 1.0 / 32.0
+    extent = int(round(side_m / step_m))
+
+    def rect(rng):
+        sides = rng.uniform(8.0, 40.0, 2)
+        poly = _rectangle(rng, np.zeros(2), sides, rng.uniform(0, np.pi))
+        return poly, float(np.hypot(*sides) / 2)
+
+    polys = _place_buildings(rng, n_buildings, side_m, rect, 1.0, 1.0)
+    heights = rng.uniform(3.0, 30.0, len(polys))
+    vertices, outlines = _rings_to_arrays(polys, heights, step_m)
+    sources = _segments_to_points(rng, n_roads, side_m, step_m, lambda k: 0,
+                                  lambda kind: rng.uniform(70.0, 100.0))
+    scene = Scene(step_m=step_m, cell_steps=cell_steps, extent_steps=(extent, extent),
+                  vertices=vertices, outlines=outlines, sources=sources,
+                  favourable=np.zeros((3, 16)), alpha_db_per_km=alpha_bands(15.0, 70.0),
+                  flat_altitude_m=0.0, flat_ground_factor=0.5, name="road_square",
+                  info=dict(seed=seed, side_m=side_m, roads=n_roads, buildings=len(polys)))
+    spacing = extent // receivers
+    grid = Grid(origin=(spacing // 2, spacing // 2), spacing=spacing, nx=receivers, ny=receivers)
+    return scene, grid
+
+
+def fbm_dem(rng, n, hurst, relief_m):
+    """Fractional Brownian surface by spectral synthesis: amplitude ~ k^-(H+1), scaled to
+    +-relief_m."""
+    size = 1 << int(np.ceil(np.log2(n)))
+    kx = np.fft.fftfreq(size)[:, None]
+    ky = np.fft.fftfreq(size)[None, :]
+    k = np.sqrt(kx * kx + ky * ky)
+    k[0, 0] = 1.0
+    amplitude = k ** (-(hurst + 1.0))
+    amplitude[0, 0] = 0.0
+    phase = rng.uniform(0, 2 * np.pi, (size, size))
+    field_ = np.real(np.fft.ifft2(amplitude * np.exp(1j * phase)))[:n, :n]
+    field_ -= field_.mean()
+    field_ *= relief_m / np.max(np.abs(field_))
+    return field_.astype(np.float32)
+
+
+def voronoi_ground(rng, n, cells, spacing_m):
+    sites = rng.uniform(0, (n - 1) * spacing_m, (cells, 2))
+    values = rng.choice(np.array([0.0, 0.5, 1.0]), cells)
+    ys, xs = np.mgrid[0:n, 0:n].astype(np.float64) * spacing_m
+    out = np.empty((n, n), np.float32)
+    # Nearest site, row by row (n x cells each).
+    for j in range(n):
+        d = (xs[j][:, None] - sites[None, :, 0]) ** 2 + (ys[j][:, None] - sites[None, :, 1]) ** 2
+        out[j] = values[np.argmin(d, axis=1)]
+    return out
+
+
+def terrain_square(seed=2, scale=1.0, n_segments=20000, n_buildings=30000, side_m=4000.0,
+                   receivers=2048, cell_steps=1024, rail_share=0.2):
+    """The exact painter on terrain. `scale` (0 < scale <= 1) multiplies the square's side and
+    the receiver count per axis, and the segment, building and ground-cell counts by scale^2."""
+    rng = np.random.default_rng(seed)
+    step_m = 1.0 / 64.0
+    side = side_m * scale
+    area = scale * scale
+    n_segments = max(int(round(n_segments * area)), 1)
+    n_buildings = max(int(round(n_buildings * area)), 1)
+    receivers = max(int(round(receivers * scale)), 2)
+    extent = int(round(side / step_m))
+    dem_spacing_m = 5.0
+    nodes = int(round(side / dem_spacing_m)) + 1
+    dem = fbm_dem(rng, nodes, 0.8, 40.0)
+    gf = voronoi_ground(rng, nodes, max(int(round(200 * area)), 2), dem_spacing_m)
+
+    def poly(rng):
+        n = int(rng.integers(4, 13))
+        radius = float(rng.uniform(4.0, 11.0))
+        return _convex_polygon(rng, np.zeros(2), radius, n), radius
+
+    polys = _place_buildings(rng, n_buildings, side, poly, 1.0, 1.0)
+    heights = rng.lognormal(np.log(9.0), 0.6, len(polys))
+    vertices, outlines = _rings_to_arrays(polys, heights, step_m)
+    rail_cut = int(round(n_segments * (1.0 - rail_share)))
+    sources = _segments_to_points(
+        rng, n_segments, side, step_m, lambda k: 0 if k < rail_cut else 1,
+        lambda kind: rng.uniform(70.0, 100.0) if kind == 0 else rng.uniform(80.0, 105.0))
+    scene = Scene(step_m=step_m, cell_steps=cell_steps, extent_steps=(extent, extent),
+                  vertices=vertices, outlines=outlines, sources=sources,
+                  favourable=np.full((3, 16), 0.5), alpha_db_per_km=alpha_bands(15.0, 70.0),
+                  dem_altitude=dem, dem_ground_factor=gf, dem_origin=(0, 0),
+                  dem_spacing=int(round(dem_spacing_m / step_m)), name="terrain_square",
+                  info=dict(seed=seed, scale=scale, side_m=side, segments=n_segments,
+                            buildings=len(polys)))
+    spacing = int(round(side / receivers / step_m))
+    grid = Grid(origin=(spacing // 2, spacing // 2), spacing=spacing, nx=receivers, ny=receivers)
+    return scene, grid
