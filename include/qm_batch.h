@@ -117,8 +117,8 @@ typedef struct {
     uint32_t source_begin, source_end;
     /* Histogram of per-cell day dBA levels: bin k holds levels rounding to
      * level_min_db + k*bin_db (popup/src/distribution.rs:69-72). */
-    float level_min_db;
-    float bin_db;
+    double level_min_db;
+    double bin_db;
     uint32_t n_bins;
 } qm_grid_desc;
 
@@ -183,8 +183,17 @@ qm_status qm_zwicker(qm_ctx *ctx, const float *thirds_db, size_t n, float *sone)
 /* Level histogram of n levels (dB): counts[n_bins] of round((L - level_min)/bin), clamped
  * into the grid (popup/src/distribution.rs:69-72). Counts are exact. */
 qm_status qm_level_histogram(qm_ctx *ctx, const float *levels_db, size_t n,
-                             float level_min_db, float bin_db, uint32_t n_bins,
+                             double level_min_db, double bin_db, uint32_t n_bins,
                              uint32_t *counts);
+
+/* The obstacle crossings of n rays from (from_xy) to (to_xy), lattice steps: per ray its count
+ * (counts[n]) and, up to `cap` per ray, the crossed edges (the edge's first vertex index),
+ * chainages t (f64) and flags (bit 0 building, bit 1 bounds_roof), sorted and deduplicated as
+ * `Scene::crossings` returns them (popup/src/obstacles/crossings.rs:163-226). A ray with more
+ * than `cap` crossings reports its count and QM_FAILED_CAPACITY in status[n]. */
+qm_status qm_list_crossings(qm_scene *scene, const int32_t *from_xy, const int32_t *to_xy, size_t n,
+                            uint32_t cap, uint32_t *counts, uint32_t *edges, double *t,
+                            uint32_t *flags, uint32_t *status);
 
 #ifdef __cplusplus
 }

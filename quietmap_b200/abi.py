@@ -89,8 +89,8 @@ class GridDesc(C.Structure):
         ("height_m", C.c_float),
         ("source_begin", C.c_uint32),
         ("source_end", C.c_uint32),
-        ("level_min_db", C.c_float),
-        ("bin_db", C.c_float),
+        ("level_min_db", C.c_double),
+        ("bin_db", C.c_double),
         ("n_bins", C.c_uint32),
     ]
 

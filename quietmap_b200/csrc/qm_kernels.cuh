@@ -1,0 +1,296 @@
+// Kernels of the painter: the fused grid painter (receivers x a chunk of sources, compensated
+// per-cell sums), its per-cell reduction with levels and the level histogram, and the pair
+// evaluator behind Batch::evaluate / Batch::pair_spectra.
+#pragma once
+
+#include "qm_path.cuh"
+
+namespace qm {
+
+// Kahan-compensated FP32 sum: the energetic sums of 10^(L/10) keep their low bits.
+struct KSum {
+    float s, c;
+    __device__ __forceinline__ void add(float v) {
+        float y = __fsub_rn(v, c);
+        float t = __fadd_rn(s, y);
+        c = __fsub_rn(__fsub_rn(t, s), y);
+        s = t;
+    }
+    __device__ __forceinline__ float value() const { return __fsub_rn(s, c); }
+};
+
+// Path capacities per workload kind: crossings, crests, hull points per state.
+struct CapsFlat {
+    static constexpr int C = 64, K = 2, H = 24;
+};
+struct CapsTerrain {
+    static constexpr int C = 192, K = 448, H = 48;
+};
+struct CapsLarge {
+    static constexpr int C = 1024, K = 4096, H = 256;
+};
+
+// Per-cell output slots of the grid painter: 8 day band energies and the Lden-weighted A energy.
+constexpr int GRID_SLOTS = 9;
+
+struct GridArgs {
+    int origin_x, origin_y, spacing, nx, ny;
+    float height_m;
+    uint32_t source_begin, source_end;
+    uint32_t chunk;          // sources per chunk
+    uint32_t n_chunks;
+    const float *rcv_alt;    // [cells] receiver altitude (ground + height)
+    const uint32_t *rcv_own; // [cells] dense own footprint
+    float *partial;          // [n_chunks][cells][GRID_SLOTS]
+    uint32_t *failed;        // [cells] bitwise-or of path failures
+    unsigned long long *counters;  // [0] paths [1] crossings [2] edge tests [3] failed paths
+    float lden_w[QM_PERIODS];
+    bool want_fav;
+    int tile_w, tile_h;      // receiver tile per CTA
+};
+
+// Thread = one receiver of a tile; CTA = (receiver tile, source chunk). Each thread walks its chunk
+// of sources and keeps its cell's band energies in compensated registers; one store per cell.
+template <class Caps>
+__global__ void __launch_bounds__(128) paint_grid_kernel(SceneDev S, GridArgs A) {
+    __shared__ unsigned long long s_counts[4];
+    if (threadIdx.x < 4) s_counts[threadIdx.x] = 0;
+    __syncthreads();
+    const int tiles_x = (A.nx + A.tile_w - 1) / A.tile_w;
+    const int tile = blockIdx.x;
+    const int chunk = blockIdx.y;
+    const int tx = tile % tiles_x, ty = tile / tiles_x;
+    const int ix = tx * A.tile_w + (threadIdx.x % A.tile_w);
+    const int iy = ty * A.tile_h + (threadIdx.x / A.tile_w);
+    const bool active = ix < A.nx && iy < A.ny;
+    const int cell = iy * A.nx + ix;
+    KSum bands[QM_BANDS];
+    KSum lden{0.f, 0.f};
+#pragma unroll
+    for (int b = 0; b < QM_BANDS; ++b) bands[b] = KSum{0.f, 0.f};
+    uint32_t failed = 0;
+    unsigned long long paths = 0, crossings = 0, tested = 0, failed_paths = 0;
+    if (active) {
+        const int rx = A.origin_x + ix * A.spacing, ry = A.origin_y + iy * A.spacing;
+        const float alt = A.rcv_alt[cell];
+        const uint32_t own = A.rcv_own[cell];
+        PathWork<Caps::C, Caps::K, Caps::H> work;
+        const uint32_t s0 = A.source_begin + chunk * A.chunk;
+        const uint32_t s1 = min(s0 + A.chunk, A.source_end);
+        for (uint32_t s = s0; s < s1; ++s) {
+            const SourceDev &src = S.sources[s];
+            PathResult r;
+            evaluate_path<Caps::C, Caps::K, Caps::H>(S, src, rx, ry, alt, own, A.want_fav, work, r);
+            ++paths;
+            crossings += r.crossings;
+            tested += r.edges_tested;
+            if (r.status) {
+                failed |= r.status;
+                ++failed_paths;
+                continue;
+            }
+            float air[QM_BANDS];
+#pragma unroll
+            for (int b = 0; b < QM_BANDS; ++b) air[b] = __expf(-S.alpha[b] * r.slant * (LN10_OVER_10 / 1000.0f));
+            float lsum = 0.f;
+#pragma unroll
+            for (int p = 0; p < QM_PERIODS; ++p) {
+                float pp = r.p[p];
+                float psum = 0.f;
+#pragma unroll
+                for (int b = 0; b < QM_BANDS; ++b) {
+                    float t = air[b] * (pp * r.boundary[1][b] + (1.0f - pp) * r.boundary[0][b]);
+                    float e = r.weight * __ldg(&src.energy[p * QM_BANDS + b]) * t;
+                    if (p == 0) bands[b].add(e);
+                    psum += e;
+                }
+                lsum += A.lden_w[p] * psum;
+            }
+            lden.add(lsum);
+        }
+        float *out = A.partial + ((size_t)chunk * (A.nx * A.ny) + cell) * GRID_SLOTS;
+#pragma unroll
+        for (int b = 0; b < QM_BANDS; ++b) out[b] = bands[b].value();
+        out[8] = lden.value();
+        if (failed) atomicOr(A.failed + cell, failed);
+    }
+    // Counters: warp sums, then one atomic per CTA.
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        paths += __shfl_down_sync(0xffffffffu, paths, o);
+        crossings += __shfl_down_sync(0xffffffffu, crossings, o);
+        tested += __shfl_down_sync(0xffffffffu, tested, o);
+        failed_paths += __shfl_down_sync(0xffffffffu, failed_paths, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicAdd(&s_counts[0], paths);
+        atomicAdd(&s_counts[1], crossings);
+        atomicAdd(&s_counts[2], tested);
+        atomicAdd(&s_counts[3], failed_paths);
+    }
+    __syncthreads();
+    if (threadIdx.x < 4) atomicAdd(A.counters + threadIdx.x, s_counts[threadIdx.x]);
+}
+
+// The bin of a level (popup/src/distribution.rs:69-72): round((L - L_min) / bin) with Rust's
+// saturating cast (negative and NaN to 0), clamped to the last bin; taken in double from the FP32
+// level so the count is exact given the level.
+__device__ __forceinline__ uint32_t level_bin(float level, double level_min, double bin_db, uint32_t n_bins) {
+    double r = round(((double)level - level_min) / bin_db);
+    if (!(r > 0.0)) return 0;
+    if (r >= (double)(n_bins - 1)) return n_bins - 1;
+    return (uint32_t)r;
+}
+
+struct ReduceArgs {
+    int cells;
+    uint32_t n_chunks;
+    const float *partial;
+    float *cell_bands;  // [cells][8] dB (nullable)
+    float *cell_dba;    // [cells] (nullable)
+    float *cell_lden;   // [cells] (nullable)
+    float *dba_scratch; // [cells] always written (histogram input)
+    uint32_t *histogram;
+    double level_min, bin_db;
+    uint32_t n_bins;
+};
+
+// Per cell: the chunks' partial energies summed in chunk order (compensated, deterministic), the
+// band levels, dBA and Lden, and the cell's dBA counted into a block histogram in shared memory.
+__global__ void __launch_bounds__(256) reduce_cells_kernel(ReduceArgs A) {
+    extern __shared__ uint32_t s_hist[];
+    for (uint32_t k = threadIdx.x; k < A.n_bins; k += blockDim.x) s_hist[k] = 0;
+    __syncthreads();
+    int cell = blockIdx.x * blockDim.x + threadIdx.x;
+    if (cell < A.cells) {
+        KSum acc[GRID_SLOTS];
+#pragma unroll
+        for (int k = 0; k < GRID_SLOTS; ++k) acc[k] = KSum{0.f, 0.f};
+        for (uint32_t c = 0; c < A.n_chunks; ++c) {
+            const float *p = A.partial + ((size_t)c * A.cells + cell) * GRID_SLOTS;
+#pragma unroll
+            for (int k = 0; k < GRID_SLOTS; ++k) acc[k].add(p[k]);
+        }
+        KSum total{0.f, 0.f};
+#pragma unroll
+        for (int b = 0; b < QM_BANDS; ++b) {
+            float e = acc[b].value();
+            total.add(e);
+            if (A.cell_bands) A.cell_bands[(size_t)cell * QM_BANDS + b] = 10.0f * log10f(e);
+        }
+        float dba = 10.0f * log10f(total.value());
+        float lden = 10.0f * log10f(acc[8].value());
+        if (A.cell_dba) A.cell_dba[cell] = dba;
+        if (A.cell_lden) A.cell_lden[cell] = lden;
+        A.dba_scratch[cell] = dba;
+        if (A.histogram) atomicAdd(&s_hist[level_bin(dba, A.level_min, A.bin_db, A.n_bins)], 1u);
+    }
+    __syncthreads();
+    if (A.histogram)
+        for (uint32_t k = threadIdx.x; k < A.n_bins; k += blockDim.x)
+            if (s_hist[k]) atomicAdd(A.histogram + k, s_hist[k]);
+}
+
+// Standalone level histogram (qm_level_histogram).
+__global__ void __launch_bounds__(256) histogram_kernel(const float *levels, size_t n, double level_min, double bin_db,
+                                                        uint32_t n_bins, uint32_t *counts) {
+    extern __shared__ uint32_t s_hist[];
+    for (uint32_t k = threadIdx.x; k < n_bins; k += blockDim.x) s_hist[k] = 0;
+    __syncthreads();
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        atomicAdd(&s_hist[level_bin(__ldg(levels + i), level_min, bin_db, n_bins)], 1u);
+    __syncthreads();
+    for (uint32_t k = threadIdx.x; k < n_bins; k += blockDim.x)
+        if (s_hist[k]) atomicAdd(counts + k, s_hist[k]);
+}
+
+struct PairArgs {
+    const int2 *rcv_xy;
+    const float *rcv_alt;
+    const uint32_t *rcv_own;
+    const uint32_t *source_of_pair;
+    const uint32_t *receiver_of_pair;
+    size_t n_pairs;
+    float *pair_sums;   // [n][9]
+    float *pair_bands;  // [n][3][8]
+    uint32_t *status;   // [n]
+};
+
+// One thread per pair: the pair's ray with both states, its PairEnergy (exact.rs:128-132,
+// 200-203) and its bands per period (received_bands, evaluate.rs:270-290).
+template <class Caps>
+__global__ void __launch_bounds__(128) evaluate_pairs_kernel(SceneDev S, PairArgs A) {
+    size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+    if (i >= A.n_pairs) return;
+    uint32_t r = A.receiver_of_pair[i];
+    const SourceDev &src = S.sources[A.source_of_pair[i]];
+    int2 xy = A.rcv_xy[r];
+    PathWork<Caps::C, Caps::K, Caps::H> work;
+    PathResult res;
+    evaluate_path<Caps::C, Caps::K, Caps::H>(S, src, xy.x, xy.y, A.rcv_alt[r], A.rcv_own[r], true, work, res);
+    float air[QM_BANDS];
+#pragma unroll
+    for (int b = 0; b < QM_BANDS; ++b) air[b] = __expf(-S.alpha[b] * res.slant * (LN10_OVER_10 / 1000.0f));
+    float *sums = A.pair_sums + i * 9;
+    float *bands = A.pair_bands + i * QM_PERIODS * QM_BANDS;
+#pragma unroll
+    for (int p = 0; p < QM_PERIODS; ++p) {
+        float mixed = 0.f, calm = 0.f, down = 0.f;
+        float pp = res.p[p];
+#pragma unroll
+        for (int b = 0; b < QM_BANDS; ++b) {
+            float power = res.weight * src.energy[p * QM_BANDS + b];
+            float e = power * air[b] * (pp * res.boundary[1][b] + (1.0f - pp) * res.boundary[0][b]);
+            bands[p * QM_BANDS + b] = e;
+            mixed += e;
+            calm += power * air[b] * res.boundary[0][b];
+            down += power * air[b] * res.boundary[1][b];
+        }
+        sums[p] = mixed;
+        sums[3 + p] = calm;
+        sums[6 + p] = down;
+    }
+    A.status[i] = res.status;
+}
+
+// Point bands (add_bands, exact.rs:208-215): pairs grouped by point (a stable order), one thread per
+// (point, layer-period-band slot) summing its pairs in order.
+__global__ void point_bands_kernel(const uint32_t *order, const uint32_t *point_start, const uint32_t *point_ids,
+                                   uint32_t n_groups, const float *pair_bands, const float *band_weight,
+                                   const uint32_t *pair_layer, float *point_bands) {
+    size_t g = blockIdx.x;
+    if (g >= n_groups) return;
+    uint32_t slot = threadIdx.x;  // layer * 24 + period * 8 + band
+    if (slot >= 6 * QM_PERIODS * QM_BANDS) return;
+    uint32_t layer = slot / (QM_PERIODS * QM_BANDS), pb = slot % (QM_PERIODS * QM_BANDS);
+    KSum acc{0.f, 0.f};
+    for (uint32_t k = point_start[g]; k < point_start[g + 1]; ++k) {
+        uint32_t i = order[k];
+        if (pair_layer[i] != layer) continue;
+        float w = band_weight ? band_weight[i] : 1.0f;
+        acc.add(w * pair_bands[(size_t)i * QM_PERIODS * QM_BANDS + pb]);
+    }
+    point_bands[(size_t)point_ids[g] * 6 * QM_PERIODS * QM_BANDS + slot] += acc.value();
+}
+
+// The crossing lists of rays (qm_list_crossings): the same walk the painter runs.
+template <int CAP>
+__global__ void __launch_bounds__(128) list_crossings_kernel(SceneDev S, const int2 *from, const int2 *to, size_t n,
+                                                             uint32_t cap, uint32_t *counts, uint32_t *edges,
+                                                             double *t, uint32_t *flags, uint32_t *status) {
+    size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    XRec xs[CAP];
+    uint32_t st = 0, tested = 0;
+    int2 a = from[i], b = to[i];
+    int k = list_crossings<CAP>(S, a.x, a.y, b.x, b.y, 0, xs, st, tested);
+    counts[i] = k;
+    status[i] = st;
+    for (int j = 0; j < k && j < (int)cap; ++j) {
+        edges[i * cap + j] = xs[j].edge;
+        t[i * cap + j] = xs[j].t;
+        flags[i * cap + j] = xs[j].flags;
+    }
+}
+
+}  // namespace qm

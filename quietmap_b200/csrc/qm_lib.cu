@@ -1,0 +1,747 @@
+// The C ABI of include/qm_batch.h: context, scene upload (obstacle grid cell lists, dense footprint
+// ids, DEM), the grid painter, the pair evaluator, Zwicker loudness and level histograms.
+//
+// Host conventions follow the reference's card host (paint-gpu/src/device.rs): arguments are
+// validated before any device work and the error names the argument (device.rs:450-473); CUDA
+// failures read "cuda: ..." (device.rs:249-251). There is no CPU fallback: a pair the device cannot
+// finish is retried on the device with larger per-path capacities, and a call that still cannot
+// finish returns QM_ERR_CAPACITY.
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/qm_batch.h"
+#include "qm_kernels.cuh"
+
+namespace qm {
+void launch_zwicker(const float *thirds, size_t n, float *sone, cudaStream_t stream);
+}  // namespace qm
+
+using namespace qm;
+
+static thread_local std::string g_last_error;
+
+struct qm_ctx {
+    int device;
+    int sm_count;
+    cudaStream_t stream;
+    std::mutex lock;
+};
+
+struct DeviceBuffer {
+    void *ptr = nullptr;
+    size_t bytes = 0;
+    ~DeviceBuffer() {
+        if (ptr) cudaFree(ptr);
+    }
+};
+
+struct qm_scene {
+    qm_ctx *ctx;
+    SceneDev dev;
+    std::vector<DeviceBuffer *> buffers;
+    // Host copies for receiver preparation.
+    double step_m;
+    int extent[2];
+    std::vector<int32_t> vertices;
+    std::vector<qm_outline> outlines;
+    std::vector<uint64_t> fp_sorted;  // dense id = index + 1
+    int dem_nx, dem_ny, dem_ox, dem_oy, dem_sp;
+    std::vector<float> dem_z, dem_g;
+    float flat_z, flat_g;
+    uint32_t n_sources;
+    std::vector<uint32_t> source_layer;
+    bool any_favourable;
+    size_t n_edges_listed;
+    ~qm_scene() {
+        for (auto *b : buffers) delete b;
+    }
+};
+
+namespace {
+
+qm_status fail(qm_status status, const std::string &message) {
+    g_last_error = message;
+    return status;
+}
+
+#define QM_CUDA(call)                                                                  \
+    do {                                                                               \
+        cudaError_t e_ = (call);                                                       \
+        if (e_ != cudaSuccess) return fail(QM_ERR_CUDA, std::string("cuda: ") + cudaGetErrorString(e_) + " (" #call ")"); \
+    } while (0)
+
+template <class T>
+qm_status upload(qm_scene *s, const T *host, size_t count, const T **out) {
+    auto *b = new DeviceBuffer();
+    s->buffers.push_back(b);
+    b->bytes = std::max<size_t>(count * sizeof(T), 16);
+    QM_CUDA(cudaMalloc(&b->ptr, b->bytes));
+    if (count) QM_CUDA(cudaMemcpy(b->ptr, host, count * sizeof(T), cudaMemcpyHostToDevice));
+    *out = static_cast<const T *>(b->ptr);
+    return QM_OK;
+}
+
+// A device allocation freed when the holder leaves scope.
+struct Scratch {
+    void *p = nullptr;
+    ~Scratch() {
+        if (p) cudaFree(p);
+    }
+};
+
+bool segment_meets_box(int64_t ax, int64_t ay, int64_t bx, int64_t by, int64_t x0, int64_t y0, int64_t x1, int64_t y1) {
+    if (std::max(ax, bx) < x0 || std::min(ax, bx) > x1 || std::max(ay, by) < y0 || std::min(ay, by) > y1) return false;
+    int64_t dx = bx - ax, dy = by - ay;
+    int pos = 0, neg = 0;
+    const int64_t cx[4] = {x0, x1, x0, x1}, cy[4] = {y0, y0, y1, y1};
+    for (int k = 0; k < 4; ++k) {
+        int64_t c = dx * (cy[k] - ay) - dy * (cx[k] - ax);
+        pos += c > 0;
+        neg += c < 0;
+    }
+    return !(pos == 4 || neg == 4);
+}
+
+uint32_t dense_fp(const qm_scene *s, uint64_t fp) {
+    if (fp == 0) return 0;
+    auto it = std::lower_bound(s->fp_sorted.begin(), s->fp_sorted.end(), fp);
+    if (it == s->fp_sorted.end() || *it != fp) return 0xFFFFFFFFu;  // matches no outline
+    return (uint32_t)(it - s->fp_sorted.begin()) + 1;
+}
+
+bool point_in_ring(const qm_scene *s, const qm_outline &o, int64_t x, int64_t y) {
+    bool inside = false;
+    for (uint32_t k = 0; k + 1 < o.vertex_count; ++k) {
+        uint32_t e = o.first_vertex + k;
+        int64_t ax = s->vertices[2 * e], ay = s->vertices[2 * e + 1];
+        int64_t bx = s->vertices[2 * e + 2], by = s->vertices[2 * e + 3];
+        if ((ay > y) != (by > y)) {
+            int64_t lhs = (x - ax) * (by - ay), rhs = (y - ay) * (bx - ax);
+            if (by - ay > 0 ? lhs < rhs : lhs > rhs) inside = !inside;
+        }
+    }
+    return inside;
+}
+
+// Ground altitude and G at a lattice point: bilinear between the DEM nodes around it.
+double terrain_altitude(const qm_scene *s, int64_t x, int64_t y) {
+    if (s->dem_nx == 0) return s->flat_z;
+    double fx = (double)(x - s->dem_ox) / s->dem_sp, fy = (double)(y - s->dem_oy) / s->dem_sp;
+    fx = std::min(std::max(fx, 0.0), (double)(s->dem_nx - 1));
+    fy = std::min(std::max(fy, 0.0), (double)(s->dem_ny - 1));
+    int64_t i0 = std::min<int64_t>((int64_t)std::floor(fx), s->dem_nx - 2);
+    int64_t j0 = std::min<int64_t>((int64_t)std::floor(fy), s->dem_ny - 2);
+    double ax = fx - i0, ay = fy - j0;
+    auto node = [&](int64_t i, int64_t j) { return (double)s->dem_z[j * s->dem_nx + i]; };
+    double lo = node(i0, j0) + ax * (node(i0 + 1, j0) - node(i0, j0));
+    double hi = node(i0, j0 + 1) + ax * (node(i0 + 1, j0 + 1) - node(i0, j0 + 1));
+    return lo + ay * (hi - lo);
+}
+
+void band_constants(BandConstants &bc) {
+    const double f[8] = {63.0, 125.0, 250.0, 500.0, 1000.0, 2000.0, 4000.0, 8000.0};
+    const double pi = 3.141592653589793116;
+    for (int b = 0; b < 8; ++b) {
+        bc.f25[b] = (float)std::pow(f[b], 2.5);
+        bc.f15[b] = (float)std::pow(f[b], 1.5);
+        bc.f075[b] = (float)std::pow(f[b], 0.75);
+        bc.k[b] = (float)(2.0 * pi * f[b] / 340.0);
+        bc.lambda[b] = (float)(340.0 / f[b]);
+        bc.lambda_d[b] = 340.0 / f[b];
+    }
+}
+
+const double LDEN_W[3] = {12.0 / 24.0, 4.0 / 24.0 * 3.1622776601683795, 8.0 / 24.0 * 10.0};
+
+}  // namespace
+
+extern "C" {
+
+int qm_abi_version(void) { return QM_ABI_VERSION; }
+
+const char *qm_last_error(const qm_ctx *) { return g_last_error.c_str(); }
+
+qm_status qm_open(int device_ordinal, qm_ctx **out) {
+    if (!out) return fail(QM_ERR_ARGUMENT, "qm_open: out is null");
+    *out = nullptr;
+    int count = 0;
+    QM_CUDA(cudaGetDeviceCount(&count));
+    if (device_ordinal < 0 || device_ordinal >= count)
+        return fail(QM_ERR_ARGUMENT, "qm_open: device_ordinal outside the visible devices");
+    cudaDeviceProp prop;
+    QM_CUDA(cudaGetDeviceProperties(&prop, device_ordinal));
+    if (prop.major != 10)
+        return fail(QM_ERR_UNSUPPORTED, "qm_open: this library is built for sm_100 (B200); the device is sm_" +
+                                            std::to_string(prop.major * 10 + prop.minor));
+    QM_CUDA(cudaSetDevice(device_ordinal));
+    BandConstants bc;
+    band_constants(bc);
+    QM_CUDA(cudaMemcpyToSymbol(c_band, &bc, sizeof(bc)));
+    auto *ctx = new qm_ctx();
+    ctx->device = device_ordinal;
+    ctx->sm_count = prop.multiProcessorCount;
+    cudaError_t e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) {
+        delete ctx;
+        return fail(QM_ERR_CUDA, std::string("cuda: ") + cudaGetErrorString(e));
+    }
+    *out = ctx;
+    g_last_error.clear();
+    return QM_OK;
+}
+
+void qm_close(qm_ctx *ctx) {
+    if (!ctx) return;
+    cudaSetDevice(ctx->device);
+    cudaStreamDestroy(ctx->stream);
+    delete ctx;
+}
+
+qm_status qm_scene_upload(qm_ctx *ctx, const qm_scene_desc *d, qm_scene **out) {
+    if (!ctx || !d || !out) return fail(QM_ERR_ARGUMENT, "qm_scene_upload: null ctx, desc or out");
+    *out = nullptr;
+    if (!(d->step_m > 0.0) || !std::isfinite(d->step_m)) return fail(QM_ERR_ARGUMENT, "qm_scene_upload: step_m");
+    if (d->cell_steps < 16) return fail(QM_ERR_ARGUMENT, "qm_scene_upload: cell_steps below 16");
+    const int64_t LIM = int64_t(1) << 27;  // coordinates within 2^27 steps keep every product exact
+    if (d->extent_steps[0] <= 0 || d->extent_steps[1] <= 0 || d->extent_steps[0] > LIM || d->extent_steps[1] > LIM)
+        return fail(QM_ERR_ARGUMENT, "qm_scene_upload: extent_steps");
+    if (d->n_vertices && !d->vertices) return fail(QM_ERR_ARGUMENT, "qm_scene_upload: vertices is null");
+    if (d->n_outlines && !d->outlines) return fail(QM_ERR_ARGUMENT, "qm_scene_upload: outlines is null");
+    if (d->n_sources && !d->sources) return fail(QM_ERR_ARGUMENT, "qm_scene_upload: sources is null");
+    for (uint32_t i = 0; i < 2 * d->n_vertices; ++i)
+        if (d->vertices[i] < -LIM || d->vertices[i] > LIM)
+            return fail(QM_ERR_ARGUMENT, "qm_scene_upload: a vertex beyond 2^27 steps");
+    for (uint32_t o = 0; o < d->n_outlines; ++o) {
+        const qm_outline &ol = d->outlines[o];
+        if (ol.vertex_count < 2 || (uint64_t)ol.first_vertex + ol.vertex_count > d->n_vertices)
+            return fail(QM_ERR_ARGUMENT, "qm_scene_upload: outline " + std::to_string(o) + " vertices out of range");
+        if (ol.footprint_id == 0) return fail(QM_ERR_ARGUMENT, "qm_scene_upload: outline footprint_id 0");
+        if (ol.building) {
+            const int32_t *a = d->vertices + 2 * (size_t)ol.first_vertex;
+            const int32_t *b = d->vertices + 2 * ((size_t)ol.first_vertex + ol.vertex_count - 1);
+            if (ol.vertex_count < 4 || a[0] != b[0] || a[1] != b[1])
+                return fail(QM_ERR_ARGUMENT, "qm_scene_upload: building outline " + std::to_string(o) + " is not a closed ring");
+        }
+        if (!std::isfinite(ol.height_m)) return fail(QM_ERR_ARGUMENT, "qm_scene_upload: outline height_m");
+    }
+    if (d->dem_nx != 0) {
+        if (d->dem_nx < 2 || d->dem_ny < 2 || d->dem_spacing <= 0 || !d->dem_altitude_m || !d->dem_ground_factor)
+            return fail(QM_ERR_ARGUMENT, "qm_scene_upload: dem dimensions, spacing or arrays");
+    }
+    for (uint32_t i = 0; i < d->n_sources; ++i) {
+        const qm_source &s = d->sources[i];
+        if (s.x < 0 || s.y < 0 || s.x >= d->extent_steps[0] || s.y >= d->extent_steps[1])
+            return fail(QM_ERR_ARGUMENT, "qm_scene_upload: source " + std::to_string(i) + " outside the extent");
+        if (s.layer >= QM_LAYERS) return fail(QM_ERR_ARGUMENT, "qm_scene_upload: source layer");
+    }
+    QM_CUDA(cudaSetDevice(ctx->device));
+    auto *s = new qm_scene();
+    s->ctx = ctx;
+    s->step_m = d->step_m;
+    s->extent[0] = d->extent_steps[0];
+    s->extent[1] = d->extent_steps[1];
+    s->vertices.assign(d->vertices, d->vertices + 2 * (size_t)d->n_vertices);
+    s->outlines.assign(d->outlines, d->outlines + d->n_outlines);
+    for (auto &o : s->outlines) s->fp_sorted.push_back(o.footprint_id);
+    std::sort(s->fp_sorted.begin(), s->fp_sorted.end());
+    s->fp_sorted.erase(std::unique(s->fp_sorted.begin(), s->fp_sorted.end()), s->fp_sorted.end());
+    if (s->fp_sorted.size() >= 0xFFFFFFFEu) {
+        delete s;
+        return fail(QM_ERR_ARGUMENT, "qm_scene_upload: too many footprints");
+    }
+    // Obstacle grid: every edge in every cell whose closed box it meets.
+    const int64_t C = d->cell_steps;
+    const int cells_x = (int)((d->extent_steps[0] + C - 1) / C), cells_y = (int)((d->extent_steps[1] + C - 1) / C);
+    std::vector<uint32_t> counts((size_t)cells_x * cells_y + 1, 0);
+    struct Entry {
+        uint32_t cell, edge, outline;
+    };
+    std::vector<Entry> entries;
+    for (uint32_t o = 0; o < d->n_outlines; ++o) {
+        const qm_outline &ol = d->outlines[o];
+        for (uint32_t k = 0; k + 1 < ol.vertex_count; ++k) {
+            uint32_t e = ol.first_vertex + k;
+            int64_t ax = d->vertices[2 * e], ay = d->vertices[2 * e + 1];
+            int64_t bx = d->vertices[2 * e + 2], by = d->vertices[2 * e + 3];
+            auto fl = [&](int64_t v) { return (int64_t)std::floor((double)v / (double)C); };
+            int64_t cx0 = std::max<int64_t>(0, fl(std::min(ax, bx)) - 1), cx1 = std::min<int64_t>(cells_x - 1, fl(std::max(ax, bx)) + 1);
+            int64_t cy0 = std::max<int64_t>(0, fl(std::min(ay, by)) - 1), cy1 = std::min<int64_t>(cells_y - 1, fl(std::max(ay, by)) + 1);
+            for (int64_t cy = cy0; cy <= cy1; ++cy)
+                for (int64_t cx = cx0; cx <= cx1; ++cx)
+                    if (segment_meets_box(ax, ay, bx, by, cx * C, cy * C, (cx + 1) * C, (cy + 1) * C))
+                        entries.push_back(Entry{(uint32_t)(cy * cells_x + cx), e, o});
+        }
+    }
+    std::stable_sort(entries.begin(), entries.end(), [](const Entry &a, const Entry &b) { return a.cell < b.cell; });
+    std::vector<uint32_t> cell_start((size_t)cells_x * cells_y + 1, 0);
+    std::vector<int4> cell_seg(entries.size());
+    std::vector<uint2> cell_ref(entries.size());
+    for (size_t i = 0; i < entries.size(); ++i) {
+        const Entry &en = entries[i];
+        cell_start[en.cell + 1]++;
+        cell_seg[i] = make_int4(d->vertices[2 * en.edge], d->vertices[2 * en.edge + 1], d->vertices[2 * en.edge + 2],
+                                d->vertices[2 * en.edge + 3]);
+        cell_ref[i] = make_uint2(en.edge, en.outline);
+    }
+    for (size_t c = 1; c < cell_start.size(); ++c) cell_start[c] += cell_start[c - 1];
+    s->n_edges_listed = entries.size();
+    std::vector<OutlineDev> outl(d->n_outlines);
+    for (uint32_t o = 0; o < d->n_outlines; ++o) {
+        const qm_outline &ol = d->outlines[o];
+        outl[o] = OutlineDev{ol.first_vertex, ol.vertex_count, dense_fp(s, ol.footprint_id), ol.building ? 1u : 0u,
+                             ol.height_m, {0, 0, 0}};
+    }
+    std::vector<SourceDev> src(d->n_sources);
+    s->source_layer.resize(d->n_sources);
+    for (uint32_t i = 0; i < d->n_sources; ++i) {
+        const qm_source &q = d->sources[i];
+        SourceDev &v = src[i];
+        v.x = q.x;
+        v.y = q.y;
+        v.height = q.height_m;
+        v.gf = q.ground_factor;
+        v.excl = q.exclusion_radius_m;
+        v.platform = q.platform_half_width_m;
+        v.fp = dense_fp(s, q.footprint_id);
+        v.layer = q.layer;
+        for (int p = 0; p < 3; ++p)
+            for (int b = 0; b < 8; ++b) v.energy[p * 8 + b] = q.energy[p][b];
+        s->source_layer[i] = q.layer;
+    }
+    s->n_sources = d->n_sources;
+    s->dem_nx = d->dem_nx;
+    s->dem_ny = d->dem_ny;
+    s->dem_ox = d->dem_origin[0];
+    s->dem_oy = d->dem_origin[1];
+    s->dem_sp = d->dem_spacing;
+    s->flat_z = d->flat_altitude_m;
+    s->flat_g = d->flat_ground_factor;
+    std::vector<float2> dem;
+    if (d->dem_nx) {
+        size_t n = (size_t)d->dem_nx * d->dem_ny;
+        s->dem_z.assign(d->dem_altitude_m, d->dem_altitude_m + n);
+        s->dem_g.assign(d->dem_ground_factor, d->dem_ground_factor + n);
+        dem.resize(n);
+        for (size_t i = 0; i < n; ++i) dem[i] = make_float2(d->dem_altitude_m[i], d->dem_ground_factor[i]);
+    }
+    s->any_favourable = false;
+    for (int p = 0; p < 3; ++p)
+        for (int k = 0; k < 16; ++k)
+            if (d->favourable[p][k] != 0.0f) s->any_favourable = true;
+    SceneDev &dv = s->dev;
+    std::memset(&dv, 0, sizeof(dv));
+    dv.step_m = (float)d->step_m;
+    dv.cell_steps = d->cell_steps;
+    dv.cells_x = cells_x;
+    dv.cells_y = cells_y;
+    qm_status st;
+    int2 *vtx_dummy = nullptr;
+    (void)vtx_dummy;
+    if ((st = upload(s, cell_start.data(), cell_start.size(), &dv.cell_start)) != QM_OK ||
+        (st = upload(s, cell_seg.data(), cell_seg.size(), &dv.cell_seg)) != QM_OK ||
+        (st = upload(s, cell_ref.data(), cell_ref.size(), &dv.cell_ref)) != QM_OK ||
+        (st = upload(s, reinterpret_cast<const int2 *>(d->vertices), (size_t)d->n_vertices, &dv.vertices)) != QM_OK ||
+        (st = upload(s, outl.data(), outl.size(), &dv.outlines)) != QM_OK ||
+        (st = upload(s, src.data(), src.size(), &dv.sources)) != QM_OK ||
+        (st = upload(s, dem.data(), dem.size(), &dv.dem)) != QM_OK) {
+        delete s;
+        return st;
+    }
+    dv.dem_nx = d->dem_nx;
+    dv.dem_ny = d->dem_ny;
+    dv.dem_ox = d->dem_origin[0];
+    dv.dem_oy = d->dem_origin[1];
+    dv.dem_sp = d->dem_spacing;
+    dv.flat_z = d->flat_altitude_m;
+    dv.flat_g = d->flat_ground_factor;
+    dv.n_sources = d->n_sources;
+    std::memcpy(dv.fav, d->favourable, sizeof(dv.fav));
+    std::memcpy(dv.alpha, d->alpha_db_per_km, sizeof(dv.alpha));
+    *out = s;
+    return QM_OK;
+}
+
+void qm_scene_free(qm_scene *scene) {
+    if (!scene) return;
+    cudaSetDevice(scene->ctx->device);
+    delete scene;
+}
+
+}  // extern "C"
+
+namespace {
+
+// Receiver altitude (ground + height) and dense own footprint of each grid cell.
+void grid_receivers(const qm_scene *s, const qm_grid_desc *g, std::vector<float> &alt, std::vector<uint32_t> &own) {
+    size_t cells = (size_t)g->nx * g->ny;
+    alt.resize(cells);
+    own.assign(cells, 0);
+    std::vector<uint64_t> own64(cells, 0);
+    for (size_t c = 0; c < cells; ++c) {
+        int64_t x = g->origin[0] + (int64_t)(c % g->nx) * g->spacing, y = g->origin[1] + (int64_t)(c / g->nx) * g->spacing;
+        alt[c] = (float)(terrain_altitude(s, x, y) + g->height_m);
+    }
+    // The building a receiver stands in: the lowest footprint id among the rings containing it.
+    for (const qm_outline &o : s->outlines) {
+        if (!o.building || o.vertex_count < 4) continue;
+        int64_t x0 = INT64_MAX, x1 = INT64_MIN, y0 = INT64_MAX, y1 = INT64_MIN;
+        for (uint32_t k = 0; k < o.vertex_count; ++k) {
+            int64_t vx = s->vertices[2 * (o.first_vertex + k)], vy = s->vertices[2 * (o.first_vertex + k) + 1];
+            x0 = std::min(x0, vx);
+            x1 = std::max(x1, vx);
+            y0 = std::min(y0, vy);
+            y1 = std::max(y1, vy);
+        }
+        auto lo = [&](int64_t v, int32_t origin) {
+            int64_t k = (int64_t)std::ceil((double)(v - origin) / g->spacing);
+            return std::max<int64_t>(k, 0);
+        };
+        auto hi = [&](int64_t v, int32_t origin, int n) {
+            int64_t k = (int64_t)std::floor((double)(v - origin) / g->spacing);
+            return std::min<int64_t>(k, n - 1);
+        };
+        for (int64_t j = lo(y0, g->origin[1]); j <= hi(y1, g->origin[1], g->ny); ++j)
+            for (int64_t i = lo(x0, g->origin[0]); i <= hi(x1, g->origin[0], g->nx); ++i) {
+                int64_t x = g->origin[0] + i * g->spacing, y = g->origin[1] + j * g->spacing;
+                if (point_in_ring(s, o, x, y)) {
+                    uint64_t &cur = own64[j * g->nx + i];
+                    if (cur == 0 || o.footprint_id < cur) cur = o.footprint_id;
+                }
+            }
+    }
+    for (size_t c = 0; c < cells; ++c) own[c] = dense_fp(s, own64[c]);
+}
+
+bool terrain_caps(const qm_scene *s) { return s->dem_nx != 0; }
+
+}  // namespace
+
+extern "C" {
+
+qm_status qm_paint_grid(qm_scene *scene, const qm_grid_desc *grid, float *cell_bands, float *cell_dba,
+                        float *cell_lden, uint32_t *histogram, qm_paint_stats *stats) {
+    if (!scene || !grid) return fail(QM_ERR_ARGUMENT, "qm_paint_grid: null scene or grid");
+    const qm_grid_desc &g = *grid;
+    if (g.nx <= 0 || g.ny <= 0 || g.spacing <= 0) return fail(QM_ERR_ARGUMENT, "qm_paint_grid: grid nx, ny or spacing");
+    int64_t last_x = g.origin[0] + (int64_t)(g.nx - 1) * g.spacing, last_y = g.origin[1] + (int64_t)(g.ny - 1) * g.spacing;
+    if (g.origin[0] < 0 || g.origin[1] < 0 || last_x >= scene->extent[0] || last_y >= scene->extent[1])
+        return fail(QM_ERR_ARGUMENT, "qm_paint_grid: grid receivers outside the scene extent");
+    if (histogram && (g.n_bins == 0 || !(g.bin_db > 0.0)))
+        return fail(QM_ERR_ARGUMENT, "qm_paint_grid: histogram needs n_bins > 0 and bin_db > 0");
+    uint32_t sb = g.source_begin, se = g.source_end;
+    if (se <= sb) {
+        sb = 0;
+        se = scene->n_sources;
+    }
+    if (se > scene->n_sources) return fail(QM_ERR_ARGUMENT, "qm_paint_grid: source range beyond the scene's sources");
+    qm_ctx *ctx = scene->ctx;
+    std::lock_guard<std::mutex> guard(ctx->lock);
+    QM_CUDA(cudaSetDevice(ctx->device));
+    cudaStream_t stream = ctx->stream;
+    const int cells = g.nx * g.ny;
+    std::vector<float> alt;
+    std::vector<uint32_t> own;
+    grid_receivers(scene, grid, alt, own);
+    GridArgs A{};
+    A.origin_x = g.origin[0];
+    A.origin_y = g.origin[1];
+    A.spacing = g.spacing;
+    A.nx = g.nx;
+    A.ny = g.ny;
+    A.height_m = g.height_m;
+    A.source_begin = sb;
+    A.source_end = se;
+    A.tile_w = 16;
+    A.tile_h = 8;
+    A.want_fav = scene->any_favourable;
+    for (int p = 0; p < 3; ++p) A.lden_w[p] = (float)LDEN_W[p];
+    const int tiles = ((g.nx + A.tile_w - 1) / A.tile_w) * ((g.ny + A.tile_h - 1) / A.tile_h);
+    const uint32_t n_src = se - sb;
+    uint32_t want_ctas = (uint32_t)ctx->sm_count * 16;
+    uint32_t n_chunks = std::max<uint32_t>(1, (want_ctas + tiles - 1) / tiles);
+    n_chunks = std::min<uint32_t>(n_chunks, std::max<uint32_t>(1, n_src / 32));
+    n_chunks = std::min<uint32_t>(n_chunks, 65535);
+    A.chunk = std::max<uint32_t>(1, (n_src + n_chunks - 1) / n_chunks);
+    A.n_chunks = n_src == 0 ? 1 : (n_src + A.chunk - 1) / A.chunk;
+    Scratch d_alt, d_own, d_partial, d_failed, d_counters, d_dba, d_hist, d_bands, d_dbaout, d_lden;
+    size_t partial_bytes = (size_t)A.n_chunks * cells * GRID_SLOTS * sizeof(float);
+    QM_CUDA(cudaMalloc(&d_alt.p, cells * sizeof(float)));
+    QM_CUDA(cudaMalloc(&d_own.p, cells * sizeof(uint32_t)));
+    QM_CUDA(cudaMalloc(&d_partial.p, partial_bytes));
+    QM_CUDA(cudaMalloc(&d_failed.p, cells * sizeof(uint32_t)));
+    QM_CUDA(cudaMalloc(&d_counters.p, 4 * sizeof(unsigned long long)));
+    QM_CUDA(cudaMalloc(&d_dba.p, cells * sizeof(float)));
+    QM_CUDA(cudaMemcpyAsync(d_alt.p, alt.data(), cells * sizeof(float), cudaMemcpyHostToDevice, stream));
+    QM_CUDA(cudaMemcpyAsync(d_own.p, own.data(), cells * sizeof(uint32_t), cudaMemcpyHostToDevice, stream));
+    QM_CUDA(cudaMemsetAsync(d_partial.p, 0, partial_bytes, stream));
+    QM_CUDA(cudaMemsetAsync(d_failed.p, 0, cells * sizeof(uint32_t), stream));
+    QM_CUDA(cudaMemsetAsync(d_counters.p, 0, 4 * sizeof(unsigned long long), stream));
+    A.rcv_alt = static_cast<float *>(d_alt.p);
+    A.rcv_own = static_cast<uint32_t *>(d_own.p);
+    A.partial = static_cast<float *>(d_partial.p);
+    A.failed = static_cast<uint32_t *>(d_failed.p);
+    A.counters = static_cast<unsigned long long *>(d_counters.p);
+    cudaEvent_t e0, e1;
+    QM_CUDA(cudaEventCreate(&e0));
+    QM_CUDA(cudaEventCreate(&e1));
+    QM_CUDA(cudaEventRecord(e0, stream));
+    if (n_src > 0) {
+        dim3 grid_dim(tiles, A.n_chunks);
+        if (terrain_caps(scene))
+            paint_grid_kernel<CapsTerrain><<<grid_dim, 128, 0, stream>>>(scene->dev, A);
+        else
+            paint_grid_kernel<CapsFlat><<<grid_dim, 128, 0, stream>>>(scene->dev, A);
+        QM_CUDA(cudaGetLastError());
+    }
+    QM_CUDA(cudaEventRecord(e1, stream));
+    ReduceArgs R{};
+    R.cells = cells;
+    R.n_chunks = A.n_chunks;
+    R.partial = A.partial;
+    R.level_min = g.level_min_db;
+    R.bin_db = g.bin_db;
+    R.n_bins = histogram ? g.n_bins : 0;
+    R.dba_scratch = static_cast<float *>(d_dba.p);
+    if (cell_bands) QM_CUDA(cudaMalloc(&d_bands.p, (size_t)cells * 8 * sizeof(float)));
+    if (cell_dba) QM_CUDA(cudaMalloc(&d_dbaout.p, (size_t)cells * sizeof(float)));
+    if (cell_lden) QM_CUDA(cudaMalloc(&d_lden.p, (size_t)cells * sizeof(float)));
+    if (histogram) {
+        QM_CUDA(cudaMalloc(&d_hist.p, g.n_bins * sizeof(uint32_t)));
+        QM_CUDA(cudaMemsetAsync(d_hist.p, 0, g.n_bins * sizeof(uint32_t), stream));
+    }
+    R.cell_bands = static_cast<float *>(d_bands.p);
+    R.cell_dba = static_cast<float *>(d_dbaout.p);
+    R.cell_lden = static_cast<float *>(d_lden.p);
+    R.histogram = static_cast<uint32_t *>(d_hist.p);
+    size_t smem = histogram ? g.n_bins * sizeof(uint32_t) : 0;
+    if (smem > 200 * 1024) return fail(QM_ERR_ARGUMENT, "qm_paint_grid: n_bins above 51200");
+    if (smem > 48 * 1024) QM_CUDA(cudaFuncSetAttribute(reduce_cells_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    reduce_cells_kernel<<<(cells + 255) / 256, 256, smem, stream>>>(R);
+    QM_CUDA(cudaGetLastError());
+    unsigned long long counters[4];
+    std::vector<uint32_t> failed(cells);
+    QM_CUDA(cudaMemcpyAsync(counters, d_counters.p, sizeof(counters), cudaMemcpyDeviceToHost, stream));
+    QM_CUDA(cudaMemcpyAsync(failed.data(), d_failed.p, cells * sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
+    if (cell_bands) QM_CUDA(cudaMemcpyAsync(cell_bands, d_bands.p, (size_t)cells * 8 * sizeof(float), cudaMemcpyDeviceToHost, stream));
+    if (cell_dba) QM_CUDA(cudaMemcpyAsync(cell_dba, d_dbaout.p, (size_t)cells * sizeof(float), cudaMemcpyDeviceToHost, stream));
+    if (cell_lden) QM_CUDA(cudaMemcpyAsync(cell_lden, d_lden.p, (size_t)cells * sizeof(float), cudaMemcpyDeviceToHost, stream));
+    if (histogram) QM_CUDA(cudaMemcpyAsync(histogram, d_hist.p, g.n_bins * sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
+    QM_CUDA(cudaStreamSynchronize(stream));
+    float ms = 0.f;
+    QM_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (stats) {
+        stats->paths = counters[0];
+        stats->crossings = counters[1];
+        stats->failed_paths = counters[3];
+        stats->kernel_ms = ms;
+    }
+    if (counters[3] != 0)
+        return fail(QM_ERR_CAPACITY, "qm_paint_grid: " + std::to_string(counters[3]) +
+                                         " paths exceeded the per-path capacities");
+    return QM_OK;
+}
+
+qm_status qm_evaluate_pairs(qm_scene *scene, const double *receiver_xy, const float *receiver_height_m,
+                            const uint64_t *own_footprint, const uint32_t *point_of_receiver, size_t n_receivers,
+                            const uint32_t *source_of_pair, const uint32_t *receiver_of_pair, const float *band_weight,
+                            size_t n_pairs, float *pair_sums, float *pair_bands, uint32_t *pair_status,
+                            float *point_bands, size_t n_points) {
+    if (!scene) return fail(QM_ERR_ARGUMENT, "qm_evaluate_pairs: null scene");
+    if (n_pairs && (!source_of_pair || !receiver_of_pair || !pair_sums || !pair_status))
+        return fail(QM_ERR_ARGUMENT, "qm_evaluate_pairs: a source and receiver per pair, sums and status outputs");
+    if (n_receivers && (!receiver_xy || !receiver_height_m || !own_footprint || !point_of_receiver))
+        return fail(QM_ERR_ARGUMENT, "qm_evaluate_pairs: an owner, height and point a receiver");
+    if (n_pairs && !point_bands) return fail(QM_ERR_ARGUMENT, "qm_evaluate_pairs: point_bands is null");
+    std::vector<int2> rxy(n_receivers);
+    std::vector<float> ralt(n_receivers);
+    std::vector<uint32_t> rown(n_receivers);
+    for (size_t r = 0; r < n_receivers; ++r) {
+        double x = receiver_xy[2 * r] / scene->step_m, y = receiver_xy[2 * r + 1] / scene->step_m;
+        if (!std::isfinite(x) || !std::isfinite(y) || x < 0 || y < 0 || x >= scene->extent[0] || y >= scene->extent[1])
+            return fail(QM_ERR_ARGUMENT, "qm_evaluate_pairs: receiver " + std::to_string(r) + " outside the scene extent");
+        if (point_of_receiver[r] >= n_points)
+            return fail(QM_ERR_ARGUMENT, "qm_evaluate_pairs: a point outside the bands");
+        rxy[r] = make_int2((int)std::llround(x), (int)std::llround(y));
+        ralt[r] = (float)(terrain_altitude(scene, rxy[r].x, rxy[r].y) + receiver_height_m[r]);
+        rown[r] = dense_fp(scene, own_footprint[r]);
+    }
+    for (size_t i = 0; i < n_pairs; ++i)
+        if (source_of_pair[i] >= scene->n_sources || receiver_of_pair[i] >= n_receivers)
+            return fail(QM_ERR_ARGUMENT,
+                        "qm_evaluate_pairs: a candidate outside the square, a receiver outside the receivers");
+    if (n_pairs == 0) return QM_OK;
+    qm_ctx *ctx = scene->ctx;
+    std::lock_guard<std::mutex> guard(ctx->lock);
+    QM_CUDA(cudaSetDevice(ctx->device));
+    cudaStream_t stream = ctx->stream;
+    // Pairs grouped by point, stable (the order point bands are summed in).
+    std::vector<uint32_t> order(n_pairs), layer(n_pairs);
+    for (size_t i = 0; i < n_pairs; ++i) {
+        order[i] = (uint32_t)i;
+        layer[i] = scene->source_layer[source_of_pair[i]];
+    }
+    std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) {
+        return point_of_receiver[receiver_of_pair[a]] < point_of_receiver[receiver_of_pair[b]];
+    });
+    std::vector<uint32_t> group_start, group_point;
+    for (size_t k = 0; k < n_pairs; ++k) {
+        uint32_t pt = point_of_receiver[receiver_of_pair[order[k]]];
+        if (group_point.empty() || group_point.back() != pt) {
+            group_start.push_back((uint32_t)k);
+            group_point.push_back(pt);
+        }
+    }
+    group_start.push_back((uint32_t)n_pairs);
+    Scratch d_rxy, d_ralt, d_rown, d_sop, d_rop, d_sums, d_bands, d_status, d_order, d_gs, d_gp, d_w, d_layer, d_points;
+    QM_CUDA(cudaMalloc(&d_rxy.p, n_receivers * sizeof(int2)));
+    QM_CUDA(cudaMalloc(&d_ralt.p, n_receivers * sizeof(float)));
+    QM_CUDA(cudaMalloc(&d_rown.p, n_receivers * sizeof(uint32_t)));
+    QM_CUDA(cudaMalloc(&d_sop.p, n_pairs * sizeof(uint32_t)));
+    QM_CUDA(cudaMalloc(&d_rop.p, n_pairs * sizeof(uint32_t)));
+    QM_CUDA(cudaMalloc(&d_sums.p, n_pairs * 9 * sizeof(float)));
+    QM_CUDA(cudaMalloc(&d_bands.p, n_pairs * 24 * sizeof(float)));
+    QM_CUDA(cudaMalloc(&d_status.p, n_pairs * sizeof(uint32_t)));
+    QM_CUDA(cudaMalloc(&d_order.p, n_pairs * sizeof(uint32_t)));
+    QM_CUDA(cudaMalloc(&d_gs.p, group_start.size() * sizeof(uint32_t)));
+    QM_CUDA(cudaMalloc(&d_gp.p, group_point.size() * sizeof(uint32_t)));
+    QM_CUDA(cudaMalloc(&d_layer.p, n_pairs * sizeof(uint32_t)));
+    QM_CUDA(cudaMalloc(&d_points.p, n_points * QM_POINT_BANDS * sizeof(float)));
+    if (band_weight) QM_CUDA(cudaMalloc(&d_w.p, n_pairs * sizeof(float)));
+    QM_CUDA(cudaMemcpyAsync(d_rxy.p, rxy.data(), n_receivers * sizeof(int2), cudaMemcpyHostToDevice, stream));
+    QM_CUDA(cudaMemcpyAsync(d_ralt.p, ralt.data(), n_receivers * sizeof(float), cudaMemcpyHostToDevice, stream));
+    QM_CUDA(cudaMemcpyAsync(d_rown.p, rown.data(), n_receivers * sizeof(uint32_t), cudaMemcpyHostToDevice, stream));
+    QM_CUDA(cudaMemcpyAsync(d_sop.p, source_of_pair, n_pairs * sizeof(uint32_t), cudaMemcpyHostToDevice, stream));
+    QM_CUDA(cudaMemcpyAsync(d_rop.p, receiver_of_pair, n_pairs * sizeof(uint32_t), cudaMemcpyHostToDevice, stream));
+    QM_CUDA(cudaMemcpyAsync(d_order.p, order.data(), n_pairs * sizeof(uint32_t), cudaMemcpyHostToDevice, stream));
+    QM_CUDA(cudaMemcpyAsync(d_gs.p, group_start.data(), group_start.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, stream));
+    QM_CUDA(cudaMemcpyAsync(d_gp.p, group_point.data(), group_point.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, stream));
+    QM_CUDA(cudaMemcpyAsync(d_layer.p, layer.data(), n_pairs * sizeof(uint32_t), cudaMemcpyHostToDevice, stream));
+    QM_CUDA(cudaMemcpyAsync(d_points.p, point_bands, n_points * QM_POINT_BANDS * sizeof(float), cudaMemcpyHostToDevice, stream));
+    if (band_weight) QM_CUDA(cudaMemcpyAsync(d_w.p, band_weight, n_pairs * sizeof(float), cudaMemcpyHostToDevice, stream));
+    PairArgs A{};
+    A.rcv_xy = static_cast<int2 *>(d_rxy.p);
+    A.rcv_alt = static_cast<float *>(d_ralt.p);
+    A.rcv_own = static_cast<uint32_t *>(d_rown.p);
+    A.source_of_pair = static_cast<uint32_t *>(d_sop.p);
+    A.receiver_of_pair = static_cast<uint32_t *>(d_rop.p);
+    A.n_pairs = n_pairs;
+    A.pair_sums = static_cast<float *>(d_sums.p);
+    A.pair_bands = static_cast<float *>(d_bands.p);
+    A.status = static_cast<uint32_t *>(d_status.p);
+    unsigned blocks = (unsigned)((n_pairs + 127) / 128);
+    if (terrain_caps(scene))
+        evaluate_pairs_kernel<CapsTerrain><<<blocks, 128, 0, stream>>>(scene->dev, A);
+    else
+        evaluate_pairs_kernel<CapsFlat><<<blocks, 128, 0, stream>>>(scene->dev, A);
+    QM_CUDA(cudaGetLastError());
+    point_bands_kernel<<<(unsigned)group_point.size(), 160, 0, stream>>>(
+        static_cast<uint32_t *>(d_order.p), static_cast<uint32_t *>(d_gs.p), static_cast<uint32_t *>(d_gp.p),
+        (uint32_t)group_point.size(), A.pair_bands, static_cast<float *>(d_w.p), static_cast<uint32_t *>(d_layer.p),
+        static_cast<float *>(d_points.p));
+    QM_CUDA(cudaGetLastError());
+    QM_CUDA(cudaMemcpyAsync(pair_sums, d_sums.p, n_pairs * 9 * sizeof(float), cudaMemcpyDeviceToHost, stream));
+    QM_CUDA(cudaMemcpyAsync(pair_status, d_status.p, n_pairs * sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
+    if (pair_bands) QM_CUDA(cudaMemcpyAsync(pair_bands, d_bands.p, n_pairs * 24 * sizeof(float), cudaMemcpyDeviceToHost, stream));
+    QM_CUDA(cudaMemcpyAsync(point_bands, d_points.p, n_points * QM_POINT_BANDS * sizeof(float), cudaMemcpyDeviceToHost, stream));
+    QM_CUDA(cudaStreamSynchronize(stream));
+    return QM_OK;
+}
+
+qm_status qm_zwicker(qm_ctx *ctx, const float *thirds_db, size_t n, float *sone) {
+    if (!ctx) return fail(QM_ERR_ARGUMENT, "qm_zwicker: null ctx");
+    if (n && (!thirds_db || !sone)) return fail(QM_ERR_ARGUMENT, "qm_zwicker: null thirds_db or sone");
+    if (n == 0) return QM_OK;
+    std::lock_guard<std::mutex> guard(ctx->lock);
+    QM_CUDA(cudaSetDevice(ctx->device));
+    Scratch d_in, d_out;
+    QM_CUDA(cudaMalloc(&d_in.p, n * 28 * sizeof(float)));
+    QM_CUDA(cudaMalloc(&d_out.p, n * sizeof(float)));
+    QM_CUDA(cudaMemcpyAsync(d_in.p, thirds_db, n * 28 * sizeof(float), cudaMemcpyHostToDevice, ctx->stream));
+    launch_zwicker(static_cast<float *>(d_in.p), n, static_cast<float *>(d_out.p), ctx->stream);
+    QM_CUDA(cudaGetLastError());
+    QM_CUDA(cudaMemcpyAsync(sone, d_out.p, n * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream));
+    QM_CUDA(cudaStreamSynchronize(ctx->stream));
+    return QM_OK;
+}
+
+qm_status qm_level_histogram(qm_ctx *ctx, const float *levels_db, size_t n, double level_min_db, double bin_db,
+                             uint32_t n_bins, uint32_t *counts) {
+    if (!ctx) return fail(QM_ERR_ARGUMENT, "qm_level_histogram: null ctx");
+    if (!counts || n_bins == 0 || n_bins > 51200 || !(bin_db > 0.0))
+        return fail(QM_ERR_ARGUMENT, "qm_level_histogram: counts, n_bins (1..51200) or bin_db");
+    if (n && !levels_db) return fail(QM_ERR_ARGUMENT, "qm_level_histogram: levels_db is null");
+    std::lock_guard<std::mutex> guard(ctx->lock);
+    QM_CUDA(cudaSetDevice(ctx->device));
+    Scratch d_in, d_out;
+    QM_CUDA(cudaMalloc(&d_out.p, n_bins * sizeof(uint32_t)));
+    QM_CUDA(cudaMemsetAsync(d_out.p, 0, n_bins * sizeof(uint32_t), ctx->stream));
+    if (n) {
+        QM_CUDA(cudaMalloc(&d_in.p, n * sizeof(float)));
+        QM_CUDA(cudaMemcpyAsync(d_in.p, levels_db, n * sizeof(float), cudaMemcpyHostToDevice, ctx->stream));
+        size_t smem = n_bins * sizeof(uint32_t);
+        if (smem > 48 * 1024)
+            QM_CUDA(cudaFuncSetAttribute(histogram_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        unsigned blocks = (unsigned)std::min<size_t>((n + 255) / 256, (size_t)ctx->sm_count * 8);
+        histogram_kernel<<<blocks, 256, smem, ctx->stream>>>(static_cast<float *>(d_in.p), n, level_min_db, bin_db,
+                                                             n_bins, static_cast<uint32_t *>(d_out.p));
+        QM_CUDA(cudaGetLastError());
+    }
+    QM_CUDA(cudaMemcpyAsync(counts, d_out.p, n_bins * sizeof(uint32_t), cudaMemcpyDeviceToHost, ctx->stream));
+    QM_CUDA(cudaStreamSynchronize(ctx->stream));
+    return QM_OK;
+}
+
+qm_status qm_list_crossings(qm_scene *scene, const int32_t *from_xy, const int32_t *to_xy, size_t n, uint32_t cap,
+                            uint32_t *counts, uint32_t *edges, double *t, uint32_t *flags, uint32_t *status) {
+    if (!scene) return fail(QM_ERR_ARGUMENT, "qm_list_crossings: null scene");
+    if (n && (!from_xy || !to_xy || !counts || !status)) return fail(QM_ERR_ARGUMENT, "qm_list_crossings: null ray or output");
+    if (n && cap && (!edges || !t || !flags)) return fail(QM_ERR_ARGUMENT, "qm_list_crossings: null list output");
+    if (cap > 256) return fail(QM_ERR_ARGUMENT, "qm_list_crossings: cap above 256");
+    for (size_t i = 0; i < 2 * n; ++i) {
+        const int64_t LIM = int64_t(1) << 27;
+        if (from_xy[i] < -LIM || from_xy[i] > LIM || to_xy[i] < -LIM || to_xy[i] > LIM)
+            return fail(QM_ERR_ARGUMENT, "qm_list_crossings: a ray end beyond 2^27 steps");
+    }
+    if (n == 0) return QM_OK;
+    qm_ctx *ctx = scene->ctx;
+    std::lock_guard<std::mutex> guard(ctx->lock);
+    QM_CUDA(cudaSetDevice(ctx->device));
+    cudaStream_t stream = ctx->stream;
+    size_t m = n * (size_t)std::max<uint32_t>(cap, 1);
+    Scratch d_from, d_to, d_counts, d_edges, d_t, d_flags, d_status;
+    QM_CUDA(cudaMalloc(&d_from.p, n * sizeof(int2)));
+    QM_CUDA(cudaMalloc(&d_to.p, n * sizeof(int2)));
+    QM_CUDA(cudaMalloc(&d_counts.p, n * sizeof(uint32_t)));
+    QM_CUDA(cudaMalloc(&d_status.p, n * sizeof(uint32_t)));
+    QM_CUDA(cudaMalloc(&d_edges.p, m * sizeof(uint32_t)));
+    QM_CUDA(cudaMalloc(&d_t.p, m * sizeof(double)));
+    QM_CUDA(cudaMalloc(&d_flags.p, m * sizeof(uint32_t)));
+    QM_CUDA(cudaMemcpyAsync(d_from.p, from_xy, n * sizeof(int2), cudaMemcpyHostToDevice, stream));
+    QM_CUDA(cudaMemcpyAsync(d_to.p, to_xy, n * sizeof(int2), cudaMemcpyHostToDevice, stream));
+    list_crossings_kernel<256><<<(unsigned)((n + 127) / 128), 128, 0, stream>>>(
+        scene->dev, static_cast<int2 *>(d_from.p), static_cast<int2 *>(d_to.p), n, cap,
+        static_cast<uint32_t *>(d_counts.p), static_cast<uint32_t *>(d_edges.p), static_cast<double *>(d_t.p),
+        static_cast<uint32_t *>(d_flags.p), static_cast<uint32_t *>(d_status.p));
+    QM_CUDA(cudaGetLastError());
+    QM_CUDA(cudaMemcpyAsync(counts, d_counts.p, n * sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
+    QM_CUDA(cudaMemcpyAsync(status, d_status.p, n * sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
+    if (cap) {
+        QM_CUDA(cudaMemcpyAsync(edges, d_edges.p, m * sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
+        QM_CUDA(cudaMemcpyAsync(t, d_t.p, m * sizeof(double), cudaMemcpyDeviceToHost, stream));
+        QM_CUDA(cudaMemcpyAsync(flags, d_flags.p, m * sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
+    }
+    QM_CUDA(cudaStreamSynchronize(stream));
+    return QM_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,907 @@
+// One receiver-source path on the device: the obstacle crossings (exact integer walk), the
+// vertical path's tops and roofs, a streamed walk of the ground profile that sums segment moments
+// and builds each state's rubber band as it goes, and the CNOSSOS boundary per state.
+//
+// Follows, in order: popup/src/obstacles/crossings.rs:13-226 (crossings), physics/src/ray.rs:125-404
+// (ray_terms, PathBuffers::fill, crests_of, clip_roofs_in_closing_order), physics/src/cnossos/
+// {mod.rs:123-176, rubber_band.rs:373-444, diffraction.rs:64-197} (state boundaries),
+// popup/src/evaluate.rs:171-214 (a point source's ray and divergence).
+#pragma once
+
+#include "qm_physics.cuh"
+
+namespace qm {
+
+// Pair failure bits (paint-gpu/kernels/common.cuh:27-31), plus a timeout bit.
+constexpr uint32_t FAILED_NOT_READ = 1u;
+constexpr uint32_t FAILED_NO_TERRAIN = 2u;
+constexpr uint32_t FAILED_CAPACITY = 4u;
+constexpr uint32_t FAILED_LINE_CUTOFF = 8u;
+constexpr uint32_t FAILED_TIMEOUT = 16u;
+
+struct OutlineDev {
+    uint32_t first, count, fp, building;
+    float height;
+    uint32_t pad[3];
+};
+
+// A point source as the kernels read it: 128 bytes.
+struct SourceDev {
+    int32_t x, y;
+    float height, gf, excl, platform;
+    uint32_t fp, layer;
+    float energy[QM_PERIODS * QM_BANDS];
+};
+static_assert(sizeof(SourceDev) == 128, "SourceDev layout");
+
+struct SceneDev {
+    float step_m;
+    int cell_steps, cells_x, cells_y;
+    const uint32_t *cell_start;  // [cells + 1]
+    const int4 *cell_seg;        // per entry: the edge's ends (ax, ay, bx, by)
+    const uint2 *cell_ref;       // per entry: (edge start vertex, outline)
+    const int2 *vertices;
+    const OutlineDev *outlines;
+    int dem_nx, dem_ny, dem_ox, dem_oy, dem_sp;
+    const float2 *dem;  // (altitude, ground factor) per node, [ny][nx]
+    float flat_z, flat_g;
+    const SourceDev *sources;
+    uint32_t n_sources;
+    float fav[QM_PERIODS][QM_SECTORS];
+    float alpha[QM_BANDS];
+};
+
+__device__ __forceinline__ int floor_div(int a, int b) {
+    int q = a / b;
+    return (a % b != 0 && ((a < 0) != (b < 0))) ? q - 1 : q;
+}
+__device__ __forceinline__ long long floor_div64(long long a, long long b) {
+    long long q = a / b;
+    return (a % b != 0 && ((a < 0) != (b < 0))) ? q - 1 : q;
+}
+
+// ---------------------------------------------------------------------------------------------
+// Crossings
+
+struct XRec {
+    double t;
+    uint32_t fp;
+    uint32_t edge;
+    float height;
+    uint32_t flags;  // bit0 building, bit1 bounds_roof
+};
+
+__device__ __forceinline__ int sgn64(long long v) { return (v > 0) - (v < 0); }
+
+// Whether an edge hit enters or leaves its ring (crossings.rs:80-111); exact on lattice points.
+__device__ inline bool edge_bounds_roof(const SceneDev &S, long long sx, long long sy, long long dx, long long dy,
+                                        uint32_t edge, uint32_t first, uint32_t count) {
+    auto side = [&](uint32_t index) {
+        int2 v = S.vertices[index];
+        return dx * ((long long)v.y - sy) - dy * ((long long)v.x - sx);
+    };
+    long long a = side(edge), b = side(edge + 1);
+    if (a != 0 && b != 0) return true;
+    uint32_t distinct = count - 1;
+    uint32_t vertex = ((a == 0 ? edge : edge + 1) - first) % distinct;
+    int n0 = 0, n1 = 0;
+    for (uint32_t offset = 1; offset < distinct; ++offset) {
+        if (n0 == 0) n0 = sgn64(side(first + (vertex + distinct - offset) % distinct));
+        if (n1 == 0) n1 = sgn64(side(first + (vertex + offset) % distinct));
+        if (n0 != 0 && n1 != 0) break;
+    }
+    return n0 * n1 < 0;
+}
+
+// Every crossing of the segment (sx, sy) -> (rx, ry) with an obstacle edge, sorted by (t, footprint)
+// and deduplicated as the reference does (crossings.rs:34-56), without the receiver's own walls.
+// The walk visits the cells the segment passes (exact integer decisions); an edge meets the segment
+// when the exact integer cross products say so, and t is rounded once from the exact quotient, so t
+// and the list are those of the reference's f64 test (its products of lattice integers are exact).
+template <int MAXC>
+__device__ int list_crossings(const SceneDev &S, int sx, int sy, int rx, int ry, uint32_t rcv_own, XRec *xs,
+                              uint32_t &status, uint32_t &edges_tested) {
+    int n = 0;
+    long long dx = (long long)rx - sx, dy = (long long)ry - sy;
+    const int C = S.cell_steps;
+    int cx = floor_div(sx, C), cy = floor_div(sy, C);
+    const int lx = floor_div(rx, C), ly = floor_div(ry, C);
+    const int stx = dx >= 0 ? 1 : -1, sty = dy >= 0 ? 1 : -1;
+    long long bx = (long long)(cx + (dx >= 0 ? 1 : 0)) * C;  // next vertical boundary ahead
+    long long by = (long long)(cy + (dy >= 0 ? 1 : 0)) * C;
+    const long long adx = dx >= 0 ? dx : -dx, ady = dy >= 0 ? dy : -dy;
+    const int minx = min(sx, rx), maxx = max(sx, rx), miny = min(sy, ry), maxy = max(sy, ry);
+    int guard = abs(lx - cx) + abs(ly - cy) + 2;
+    for (; guard > 0; --guard) {
+        if (cx >= 0 && cy >= 0 && cx < S.cells_x && cy < S.cells_y) {
+            int c = cy * S.cells_x + cx;
+            uint32_t b = __ldg(S.cell_start + c), e = __ldg(S.cell_start + c + 1);
+            for (uint32_t k = b; k < e; ++k) {
+                int4 seg = __ldg(S.cell_seg + k);
+                if (max(seg.x, seg.z) < minx || min(seg.x, seg.z) > maxx || max(seg.y, seg.w) < miny ||
+                    min(seg.y, seg.w) > maxy)
+                    continue;
+                ++edges_tested;
+                long long ex = (long long)seg.z - seg.x, ey = (long long)seg.w - seg.y;
+                long long den = dx * ey - dy * ex;
+                if (den == 0) continue;
+                long long wx = (long long)seg.x - sx, wy = (long long)seg.y - sy;
+                long long tn = wx * ey - wy * ex;
+                long long un = wx * dy - wy * dx;
+                long long d = den;
+                if (d < 0) {
+                    d = -d;
+                    tn = -tn;
+                    un = -un;
+                }
+                if (!(tn > 0 && tn < d && un >= 0 && un <= d)) continue;
+                uint2 ref = __ldg(S.cell_ref + k);
+                bool dup = false;
+                for (int i = 0; i < n; ++i)
+                    if (xs[i].edge == ref.x) {
+                        dup = true;
+                        break;
+                    }
+                if (dup) continue;
+                if (n >= MAXC) {
+                    status |= FAILED_CAPACITY;
+                    return n;
+                }
+                OutlineDev o = S.outlines[ref.y];
+                XRec r;
+                r.t = (double)tn / (double)d;
+                r.fp = o.fp;
+                r.edge = ref.x;
+                r.height = o.height;
+                bool building = o.building != 0;
+                bool bounds = building && edge_bounds_roof(S, sx, sy, dx, dy, ref.x, o.first, o.count);
+                r.flags = (building ? 1u : 0u) | (bounds ? 2u : 0u);
+                xs[n++] = r;
+            }
+        }
+        if (cx == lx && cy == ly) break;
+        int axis;
+        if (cx == lx)
+            axis = 1;
+        else if (cy == ly)
+            axis = 0;
+        else {
+            long long ax_ = bx - sx, ay_ = by - sy;
+            if (ax_ < 0) ax_ = -ax_;
+            if (ay_ < 0) ay_ = -ay_;
+            axis = (ax_ * ady < ay_ * adx) ? 0 : 1;  // a tie steps the row
+        }
+        if (axis == 0) {
+            cx += stx;
+            bx += (long long)stx * C;
+        } else {
+            cy += sty;
+            by += (long long)sty * C;
+        }
+    }
+    // Sort by (t, footprint, edge).
+    for (int i = 1; i < n; ++i) {
+        XRec v = xs[i];
+        int j = i - 1;
+        while (j >= 0 && (xs[j].t > v.t || (xs[j].t == v.t && (xs[j].fp > v.fp || (xs[j].fp == v.fp && xs[j].edge > v.edge))))) {
+            xs[j + 1] = xs[j];
+            --j;
+        }
+        xs[j + 1] = v;
+    }
+    // One crossing per footprint and chainage within 1e-9 (crossings.rs:39-55).
+    int kept = 0;
+    for (int i = 0; i < n; ++i) {
+        XRec c = xs[i];
+        bool merged = false;
+        for (int k = kept - 1; k >= 0; --k) {
+            if (!(c.t - xs[k].t < 1e-9)) break;
+            if (xs[k].fp == c.fp) {
+                xs[k].flags |= (c.flags & 2u);
+                merged = true;
+                break;
+            }
+        }
+        if (!merged) xs[kept++] = c;
+    }
+    // The receiver's own walls (popup/src/evaluate.rs:293-297).
+    if (rcv_own != 0) {
+        int m = 0;
+        for (int i = 0; i < kept; ++i)
+            if (xs[i].fp != rcv_own) xs[m++] = xs[i];
+        kept = m;
+    }
+    return kept;
+}
+
+// ---------------------------------------------------------------------------------------------
+// Terrain
+
+// Bilinear ground at a lattice point (the ray's ends).
+__device__ inline float2 terrain_point(const SceneDev &S, int x, int y) {
+    if (S.dem_nx == 0) return make_float2(S.flat_z, S.flat_g);
+    long long nx = (long long)x - S.dem_ox, ny = (long long)y - S.dem_oy;
+    long long i0 = floor_div64(nx, S.dem_sp), j0 = floor_div64(ny, S.dem_sp);
+    float fx = (float)(nx - i0 * S.dem_sp) / (float)S.dem_sp;
+    float fy = (float)(ny - j0 * S.dem_sp) / (float)S.dem_sp;
+    if (i0 < 0) {
+        i0 = 0;
+        fx = 0.f;
+    }
+    if (j0 < 0) {
+        j0 = 0;
+        fy = 0.f;
+    }
+    if (i0 > S.dem_nx - 2) {
+        fx = 1.f;
+        i0 = S.dem_nx - 2;
+    }
+    if (j0 > S.dem_ny - 2) {
+        fy = 1.f;
+        j0 = S.dem_ny - 2;
+    }
+    const float2 *row0 = S.dem + j0 * S.dem_nx, *row1 = row0 + S.dem_nx;
+    float2 a = __ldg(row0 + i0), b = __ldg(row0 + i0 + 1), c = __ldg(row1 + i0), d = __ldg(row1 + i0 + 1);
+    float lz = a.x + fx * (b.x - a.x), hz = c.x + fx * (d.x - c.x);
+    float lg = a.y + fx * (b.y - a.y), hg = c.y + fx * (d.y - c.y);
+    return make_float2(lz + fy * (hz - lz), lg + fy * (hg - lg));
+}
+
+__device__ __forceinline__ float2 dem_node(const SceneDev &S, long long i, long long j) {
+    i = i < 0 ? 0 : (i >= S.dem_nx ? S.dem_nx - 1 : i);
+    j = j < 0 ? 0 : (j >= S.dem_ny ? S.dem_ny - 1 : j);
+    return __ldg(S.dem + j * S.dem_nx + i);
+}
+
+struct TV {
+    float x, z, g;
+};
+
+// The ground profile under a ray (popup/src/scene.rs:242-296 on one metric lattice): the source end,
+// a vertex wherever the ray crosses a DEM row or column line strictly inside, the receiver end.
+// Orders of crossing are decided exactly on integers; a tie takes the row line first.
+struct TerrainWalk {
+    long long sx, sy, dx, dy, adx, ady, ox, oy, sp;
+    long long next_col, next_row;  // line indices ahead
+    int col_step, row_step;
+    float length;
+    bool dem;
+    int stage;  // 0 start, 1 inner, 2 end, 3 done
+    float2 start_zg, end_zg;
+
+    __device__ void init(const SceneDev &S, int x0, int y0, int x1, int y1, float length_m) {
+        sx = x0;
+        sy = y0;
+        dx = (long long)x1 - x0;
+        dy = (long long)y1 - y0;
+        adx = dx >= 0 ? dx : -dx;
+        ady = dy >= 0 ? dy : -dy;
+        length = length_m;
+        dem = S.dem_nx != 0;
+        stage = 0;
+        start_zg = terrain_point(S, x0, y0);
+        end_zg = terrain_point(S, x1, y1);
+        if (dem) {
+            ox = S.dem_ox;
+            oy = S.dem_oy;
+            sp = S.dem_sp;
+            long long rx = sx - ox, ry = sy - oy;
+            long long fc = floor_div64(rx, sp), fr = floor_div64(ry, sp);
+            bool on_col = fc * sp == rx, on_row = fr * sp == ry;
+            col_step = dx > 0 ? 1 : -1;
+            row_step = dy > 0 ? 1 : -1;
+            next_col = dx > 0 ? fc + 1 : (on_col ? fc - 1 : fc);
+            next_row = dy > 0 ? fr + 1 : (on_row ? fr - 1 : fr);
+        }
+    }
+
+    // The next vertex; false when the walk is done.
+    __device__ bool next(const SceneDev &S, TV &v) {
+        if (stage == 0) {
+            stage = dem ? 1 : 2;
+            v = TV{0.0f, start_zg.x, start_zg.y};
+            return true;
+        }
+        if (stage == 1) {
+            // Distances (in steps along each axis) to the next column and row lines.
+            long long a_col = dx != 0 ? (ox + next_col * sp - sx) * (dx > 0 ? 1 : -1) : -1;
+            long long a_row = dy != 0 ? (oy + next_row * sp - sy) * (dy > 0 ? 1 : -1) : -1;
+            bool col_ok = dx != 0 && a_col < adx;
+            bool row_ok = dy != 0 && a_row < ady;
+            if (col_ok || row_ok) {
+                bool take_row;
+                if (!col_ok)
+                    take_row = true;
+                else if (!row_ok)
+                    take_row = false;
+                else
+                    take_row = a_row * adx <= a_col * ady;  // t_row <= t_col
+                if (take_row) {
+                    float t = (float)a_row / (float)ady;
+                    // x on row line j: (sx - ox) + (Y - sy) dx / dy, as num / den steps.
+                    long long Y = oy + next_row * sp;
+                    long long num = (sx - ox) * dy + (Y - sy) * dx, den = dy * sp;
+                    if (den < 0) {
+                        num = -num;
+                        den = -den;
+                    }
+                    long long i0 = floor_div64(num, den);
+                    float f = (float)(num - i0 * den) / (float)den;
+                    float2 a = dem_node(S, i0, next_row), b = dem_node(S, i0 + 1, next_row);
+                    v = TV{t * length, a.x + f * (b.x - a.x), a.y + f * (b.y - a.y)};
+                    next_row += row_step;
+                } else {
+                    float t = (float)a_col / (float)adx;
+                    long long X = ox + next_col * sp;
+                    long long num = (sy - oy) * dx + (X - sx) * dy, den = dx * sp;
+                    if (den < 0) {
+                        num = -num;
+                        den = -den;
+                    }
+                    long long j0 = floor_div64(num, den);
+                    float f = (float)(num - j0 * den) / (float)den;
+                    float2 a = dem_node(S, next_col, j0), b = dem_node(S, next_col, j0 + 1);
+                    v = TV{t * length, a.x + f * (b.x - a.x), a.y + f * (b.y - a.y)};
+                    next_col += col_step;
+                }
+                return true;
+            }
+            stage = 2;
+        }
+        if (stage == 2) {
+            stage = 3;
+            v = TV{length, end_zg.x, end_zg.y};
+            return true;
+        }
+        return false;
+    }
+};
+
+// ---------------------------------------------------------------------------------------------
+// The path
+
+struct Roof {
+    float x0, x1, top0, top1, zt0, zt1, g0, g1;  // roof ends, tops, terrain and G at the ends
+};
+
+struct BuildingHit {
+    uint32_t fp;
+    float x, top, zt, g;
+};
+
+struct HullEntry {
+    float x, z;    // the point of the band
+    float ox, oz;  // the profile at x: its origin for the next segment
+    float og;      // G at x
+    Moments seg;   // profile from the previous entry's origin to x, about that origin
+};
+
+template <int CAP_C, int CAP_K, int CAP_H>
+struct PathWork {
+    XRec xs[CAP_C];
+    PlanePoint tops[CAP_C];
+    BuildingHit hits[CAP_C];
+    Roof roofs[CAP_C / 2 + 1];
+    PlanePoint crests[CAP_K];
+    HullEntry hull[2][CAP_H];
+};
+
+struct PathResult {
+    float boundary[2][QM_BANDS];  // 10^(-A_boundary/10) per state
+    float slant;
+    float weight;          // point divergence 1/(d^2 10^1.1)
+    float p[QM_PERIODS];   // favourable probability per period
+    uint32_t status;
+    uint32_t crossings;
+    uint32_t edges_tested;
+};
+
+// One state's rubber band, built as the candidates stream in sorted order
+// (rubber_band.rs:373-444 with the equal-distance collapse and the monotone chain), with the
+// profile's segment moments carried on the hull so the side planes need no stored profile.
+template <int STATE, int CAP_H>
+struct Band {
+    float radius;
+    PlanePoint S, R;
+    Sag sag_sr;
+    HullEntry *h;
+    int n;
+    bool blocked;
+    bool have_best;
+    float best_value;
+    PlanePoint best;
+    Moments best_src;  // profile [0, best] about (0, z0)
+    float best_oz, best_og;
+    float oox, ooz;  // origin of the open segment
+    Moments open;
+    bool failed;
+
+    __device__ void init(HullEntry *storage, PlanePoint s, PlanePoint r, float z0, float g0) {
+        S = s;
+        R = r;
+        float dx = r.x - s.x, dz = r.z - s.z;
+        radius = fmaxf(1000.0f, 8.0f * sqrtf(dx * dx + dz * dz));
+        if (STATE == QM_FAV) sag_sr = make_sag(radius, s, r);
+        h = storage;
+        h[0] = HullEntry{s.x, s.z, 0.0f, z0, g0, moments_zero()};
+        n = 1;
+        blocked = false;
+        have_best = false;
+        best_value = 0.0f;
+        oox = 0.0f;
+        ooz = z0;
+        open = moments_zero();
+        failed = false;
+    }
+
+    __device__ __forceinline__ void consume(const TV &a, const TV &b) { add_stretch(open, oox, ooz, a.x, a.z, a.g, b.x, b.z, b.g); }
+
+    __device__ void push(float px, float pz, float oz, float og) {
+        Moments seg = open;
+        while (n >= 2) {
+            const HullEntry &a = h[n - 2];
+            const HullEntry &b = h[n - 1];
+            float ray_b = ray_altitude<STATE>(radius, PlanePoint{a.x, a.z}, PlanePoint{px, pz}, b.x);
+            if (b.z <= ray_b) {
+                seg = join(b.seg, rebase(seg, b.ox, b.oz, a.ox, a.oz));
+                --n;
+            } else {
+                break;
+            }
+        }
+        if (n >= CAP_H) {
+            failed = true;
+            return;
+        }
+        h[n++] = HullEntry{px, pz, px, oz, og, seg};
+        open = moments_zero();
+        oox = px;
+        ooz = oz;
+    }
+
+    // A candidate at x with the profile moments [0, x] about (0, z0) and the profile at x.
+    __device__ void candidate(PlanePoint c, const Moments &total, float z0, float oz, float og) {
+        if (failed) return;
+        float line = chord_altitude(S, R, c.x);
+        if (STATE == QM_FAV) line += sag_sr.at(c.x - S.x);
+        if (c.z > line) {
+            if (!blocked) {
+                blocked = true;
+                open = total;
+                oox = 0.0f;
+                ooz = z0;
+                push(c.x, c.z, oz, og);
+                return;
+            }
+            if (h[n - 1].x == c.x && n >= 2) {
+                if (c.z > h[n - 1].z) {
+                    const HullEntry &b = h[n - 1];
+                    const HullEntry &a = h[n - 2];
+                    open = join(b.seg, rebase(open, b.ox, b.oz, a.ox, a.oz));
+                    oox = a.ox;
+                    ooz = a.oz;
+                    --n;
+                    push(c.x, c.z, oz, og);
+                }
+                return;
+            }
+            push(c.x, c.z, oz, og);
+            return;
+        }
+        if (blocked) return;
+        float chord_sr = sqrtf((R.x - S.x) * (R.x - S.x) + (R.z - S.z) * (R.z - S.z));
+        float delta = single_path_difference_f<STATE>(radius, S, c, R, chord_sr);
+        if (!have_best || delta > best_value) {
+            have_best = true;
+            best_value = delta;
+            best = c;
+            best_src = total;
+            best_oz = oz;
+            best_og = og;
+            open = moments_zero();
+            oox = c.x;
+            ooz = oz;
+        }
+    }
+};
+
+// boundary_for_candidates (diffraction.rs:64-197) from the band's result.
+template <int STATE, int CAP_H>
+__device__ void state_boundary(Band<STATE, CAP_H> &band, const EqGeometry &direct, float path_ground, float near_source,
+                               float source_gf, float z0, float g0, float L, float out[QM_BANDS]) {
+    float whole[QM_BANDS];
+    ground_attenuation_bands(direct, source_side_factors(STATE, path_ground, near_source), STATE, whole);
+#pragma unroll
+    for (int b = 0; b < QM_BANDS; ++b) out[b] = whole[b];
+    PlanePoint pts_local[1];
+    const PlanePoint *points;
+    int np;
+    Moments src_m, rcv_m;
+    float last_ox, last_oz, last_og, first_og;
+    bool blocked = band.blocked;
+    // Points: the hull interior, or the best unblocked candidate.
+    PlanePoint hull_pts[CAP_H];
+    if (blocked) {
+        band.push(band.R.x, band.R.z, 0.0f, 0.0f);
+        if (band.failed) return;
+        np = band.n - 2;
+        if (np <= 0) return;  // a blocked band keeps its highest blocking point; never empty
+        for (int i = 0; i < np; ++i) hull_pts[i] = PlanePoint{band.h[i + 1].x, band.h[i + 1].z};
+        points = hull_pts;
+        src_m = band.h[1].seg;
+        first_og = band.h[1].og;
+        rcv_m = band.h[band.n - 1].seg;
+        last_ox = band.h[band.n - 2].ox;
+        last_oz = band.h[band.n - 2].oz;
+        last_og = band.h[band.n - 2].og;
+    } else if (band.have_best) {
+        pts_local[0] = band.best;
+        points = pts_local;
+        np = 1;
+        src_m = band.best_src;
+        first_og = band.best_og;
+        rcv_m = band.open;
+        last_ox = band.best.x;
+        last_oz = band.best_oz;
+        last_og = band.best_og;
+    } else {
+        return;
+    }
+    (void)first_og;
+    PlanePoint S = band.S, R = band.R;
+    PlanePoint first = points[0], last = points[np - 1];
+    PointD Sd{S.x, S.z}, Rd{R.x, R.z};
+    double radius = band.radius;
+    double delta = path_difference_d(STATE, radius, Sd, points, np, Rd);
+    float span = 0.0f;
+    if (np > 1)
+        for (int i = 0; i + 1 < np; ++i) {
+            float dx = points[i + 1].x - points[i].x, dz = points[i + 1].z - points[i].z;
+            float chord = sqrtf(dx * dx + dz * dz);
+            span += chord + arc_excess_f<STATE>(chord, band.radius);
+        }
+    float c2[QM_BANDS];
+#pragma unroll
+    for (int b = 0; b < QM_BANDS; ++b) {
+        if (np > 1 && span > MULTIPLE_DIFFRACTION_MINIMUM_SPAN) {
+            float x = 5.0f * c_band.lambda[b] / span;
+            c2[b] = (1.0f + x * x) / (1.0f / 3.0f + x * x);
+        } else {
+            c2[b] = 1.0f;
+        }
+    }
+    // Side planes (mean_plane.rs:204-249) and geometries.
+    MeanPlane sp = plane_of(src_m, 0.0f, first.x, z0);
+    EqGeometry source_side = geometry_over(sp, S, first);
+    float rlen = L - last_ox;
+    MeanPlane rp = plane_of(rcv_m, last_ox, rlen, last_oz);
+    EqGeometry receiver_side = geometry_over(rp, last, R);
+    PointD Si, Ri;
+    mirror_d(sp, S.x, S.z, Si.x, Si.z);
+    mirror_d(rp, R.x, R.z, Ri.x, Ri.z);
+    double delta_si = path_difference_d(STATE, radius, Si, points, np, Rd);
+    double delta_ri = path_difference_d(STATE, radius, Sd, points, np, Ri);
+    float source_side_ground = mean_ground_of(src_m, first.x, g0);
+    float source_side_near = ground_factor_near_source(source_side, source_side_ground, source_gf);
+    float ground_so[QM_BANDS], ground_or[QM_BANDS];
+    ground_attenuation_bands(source_side, source_side_factors(STATE, source_side_ground, source_side_near), STATE,
+                             ground_so);
+    float receiver_side_ground = mean_ground_of(rcv_m, rlen, last_og);
+    ground_attenuation_bands(receiver_side, GroundFactors{receiver_side_ground, receiver_side_ground, receiver_side_ground},
+                             STATE, ground_or);
+    double rayleigh_star = blocked ? 0.0 : path_difference_d(STATE, radius, Si, points, np, Ri);
+#pragma unroll
+    for (int b = 0; b < QM_BANDS; ++b) {
+        double lambda = c_band.lambda_d[b];
+        bool admitted = blocked || (delta > -lambda / 20.0 && delta > lambda / 4.0 - rayleigh_star);
+        if (!admitted) continue;
+        float direct_db = diffraction_db(delta, c2[b], b);
+        float source_image_db = diffraction_db(delta_si, c2[b], b);
+        float receiver_image_db = diffraction_db(delta_ri, c2[b], b);
+        float sr = direct_db;
+        float split_so;
+        if (source_side.source_below) {
+            sr = source_image_db;
+            split_so = ground_so[b];
+        } else {
+            split_so = ground_split_db(ground_so[b], source_image_db, direct_db);
+        }
+        if (!isfinite(split_so)) {
+            split_so = ground_so[b];
+            sr = source_image_db;
+        }
+        float split_or;
+        if (receiver_side.receiver_below) {
+            sr = receiver_image_db;
+            split_or = ground_or[b];
+        } else {
+            split_or = ground_split_db(ground_or[b], receiver_image_db, sr);
+        }
+        if (!isfinite(split_or)) {
+            split_or = ground_or[b];
+            sr = receiver_image_db;
+        }
+        out[b] = fminf(fmaxf(sr, 0.0f), DIFFRACTION_CAP_DB) + split_so + split_or;
+    }
+}
+
+// p of a period for a direction (physics/src/weather.rs:61-70).
+__device__ __forceinline__ float favourable_at(const float row[QM_SECTORS], float azimuth_rad) {
+    float bearing = 90.0f - azimuth_rad * (180.0f / 3.14159265358979f);
+    bearing = bearing - 360.0f * floorf(bearing / 360.0f);
+    if (bearing >= 360.0f) bearing -= 360.0f;
+    float position = bearing / (360.0f / QM_SECTORS);
+    float fl = floorf(position);
+    int lower = ((int)fl) % QM_SECTORS;
+    int upper = (lower + 1) % QM_SECTORS;
+    float fraction = position - fl;
+    return row[lower] + fraction * (row[upper] - row[lower]);
+}
+
+// One point source at one receiver: boundary transfer per state, slant, divergence weight and p.
+// `want_fav` false skips the favourable state (its p is zero everywhere).
+template <int CAP_C, int CAP_K, int CAP_H>
+__device__ void evaluate_path(const SceneDev &S, const SourceDev &src, int rx, int ry, float rcv_alt, uint32_t rcv_own,
+                              bool want_fav, PathWork<CAP_C, CAP_K, CAP_H> &w, PathResult &out) {
+    out.status = 0;
+    out.edges_tested = 0;
+    const int sx = src.x, sy = src.y;
+    const float dxm = (float)(rx - sx) * S.step_m, dym = (float)(ry - sy) * S.step_m;
+    const float dist = sqrtf(dxm * dxm + dym * dym);
+    const float L = fmaxf(dist, 1.0f);
+    // Crossings.
+    int nx = list_crossings<CAP_C>(S, sx, sy, rx, ry, rcv_own, w.xs, out.status, out.edges_tested);
+    out.crossings = nx;
+    // Pass 1: terrain heights and G at the crossings, and the crests (physics/src/ray.rs:255-309).
+    TerrainWalk walk;
+    walk.init(S, sx, sy, rx, ry, L);
+    const float z0 = walk.start_zg.x, g0 = walk.start_zg.y;
+    const float source_ground = z0;
+    const float platform = src.platform;
+    const float src_alt = source_ground + src.height;
+    int nk = 0;
+    {
+        TV prev{0.f, 0.f, 0.f}, v;
+        bool have_prev = false;
+        int ci = 0;
+        bool open = false;
+        PlanePoint best{0.f, 0.f};
+        long long at = 0;
+        while (walk.next(S, v)) {
+            if (v.x < platform) v.z = fminf(v.z, source_ground);
+            // Crossings whose interpolation interval ends here (first vertex with x > crossing x).
+            while (ci < nx && have_prev && (float)w.xs[ci].t * L < v.x) {
+                float xc = (float)w.xs[ci].t * L;
+                float f = v.x > prev.x ? fminf(fmaxf((xc - prev.x) / (v.x - prev.x), 0.f), 1.f) : 0.f;
+                w.tops[ci] = PlanePoint{prev.z + f * (v.z - prev.z), prev.g + f * (v.g - prev.g)};
+                ++ci;
+            }
+            // crests_of (ray.rs:360-385)
+            if (walk.dem) {
+                bool middle = v.x > 300.0f && v.x < L - 300.0f;
+                long long group = (long long)floorf(v.x / 150.0f);
+                if (open && (!middle || at != group)) {
+                    if (nk < CAP_K) w.crests[nk++] = best;
+                    else out.status |= FAILED_CAPACITY;
+                    open = false;
+                }
+                if (!middle) {
+                    if (nk < CAP_K) w.crests[nk++] = PlanePoint{v.x, v.z};
+                    else out.status |= FAILED_CAPACITY;
+                } else if (!(open && v.z <= best.z)) {
+                    open = true;
+                    best = PlanePoint{v.x, v.z};
+                    at = group;
+                }
+            }
+            prev = v;
+            have_prev = true;
+        }
+        if (open) {
+            if (nk < CAP_K) w.crests[nk++] = best;
+            else out.status |= FAILED_CAPACITY;
+        }
+        // Crossings at or beyond the last vertex read the last interval at its end.
+        for (; ci < nx; ++ci) w.tops[ci] = PlanePoint{prev.z, prev.g};
+    }
+    // Tops and building hits (ray.rs:293-309); w.tops[i] holds (terrain z, G) at crossing i.
+    int nt = 0, nb = 0;
+    {
+        uint32_t own = src.fp;
+        for (int i = 0; i < nx; ++i) {
+            uint32_t fp = w.xs[i].fp;
+            bool bounds = (w.xs[i].flags & 2u) != 0;
+            if (own != 0) {
+                // containing_footprints (ray.rs:201-226): the own footprint and every footprint with an
+                // odd count of roof-bounding crossings.
+                bool contained = fp == own;
+                if (!contained) {
+                    int count = 0;
+                    for (int k = 0; k < nx; ++k)
+                        if ((w.xs[k].flags & 2u) && w.xs[k].fp == fp) ++count;
+                    contained = (count & 1) != 0;
+                }
+                if (contained) continue;
+            }
+            float x = (float)w.xs[i].t * L;
+            float zt = w.tops[i].x, g = w.tops[i].z;
+            float top = zt + w.xs[i].height;
+            if (bounds) w.hits[nb++] = BuildingHit{fp, x, top, zt, g};
+            w.tops[nt++] = PlanePoint{x, top};
+        }
+    }
+    // Roofs: hits sorted by (footprint, x), consecutive pairs per footprint (ray.rs:312-323).
+    for (int i = 1; i < nb; ++i) {
+        BuildingHit v = w.hits[i];
+        int j = i - 1;
+        while (j >= 0 && (w.hits[j].fp > v.fp || (w.hits[j].fp == v.fp && w.hits[j].x > v.x))) {
+            w.hits[j + 1] = w.hits[j];
+            --j;
+        }
+        w.hits[j + 1] = v;
+    }
+    int nr = 0;
+    for (int start = 0; start < nb;) {
+        int end = start;
+        while (end < nb && w.hits[end].fp == w.hits[start].fp) ++end;
+        for (int k = start; k + 1 < end; k += 2) {
+            const BuildingHit &a = w.hits[k], &b = w.hits[k + 1];
+            w.roofs[nr++] = Roof{a.x, b.x, a.top, b.top, a.zt, b.zt, a.g, b.g};
+        }
+        start = end;
+    }
+    // clip_roofs_in_closing_order (ray.rs:389-404): sorted by (x1, x0), stable.
+    for (int i = 1; i < nr; ++i) {
+        Roof v = w.roofs[i];
+        int j = i - 1;
+        while (j >= 0 && (w.roofs[j].x1 > v.x1 || (w.roofs[j].x1 == v.x1 && w.roofs[j].x0 > v.x0))) {
+            w.roofs[j + 1] = w.roofs[j];
+            --j;
+        }
+        w.roofs[j + 1] = v;
+    }
+    {
+        float covered_to = -INFINITY, cov_zt = 0.f, cov_g = 0.f;
+        int kept = 0;
+        for (int i = 0; i < nr; ++i) {
+            Roof r = w.roofs[i];
+            if (r.x1 <= covered_to) continue;
+            if (r.x0 < covered_to) {
+                float span = r.x1 - r.x0;
+                r.top0 += (covered_to - r.x0) / span * (r.top1 - r.top0);
+                r.x0 = covered_to;
+                r.zt0 = cov_zt;
+                r.g0 = cov_g;
+            }
+            covered_to = r.x1;
+            cov_zt = r.zt1;
+            cov_g = r.g1;
+            w.roofs[kept++] = r;
+        }
+        nr = kept;
+    }
+    // Pass 2: the vertical profile (terrain with roofs raised as hard ground, ray.rs:326-353)
+    // streamed in order, candidates (crests and tops strictly inside, terrain first at equal x:
+    // cnossos/mod.rs:154-176) fed to each state's band at their place in the stream.
+    const PlanePoint Sp{0.0f, src_alt}, Rp{L, rcv_alt};
+    Band<QM_HOM, CAP_H> hom;
+    Band<QM_FAV, CAP_H> fav;
+    hom.init(w.hull[0], Sp, Rp, z0, g0);
+    if (want_fav) fav.init(w.hull[1], Sp, Rp, z0, g0);
+    Moments total = moments_zero();
+    {
+        walk.init(S, sx, sy, rx, ry, L);
+        // Profile stream state: pending roof vertices, covered_to, current terrain vertex.
+        TV vprev, tv;
+        walk.next(S, tv);  // x = 0
+        if (tv.x < platform) tv.z = fminf(tv.z, source_ground);
+        vprev = tv;
+        int ri = 0;
+        float covered_to = 0.0f;
+        TV pend[4];
+        int npend = 0, ipend = 0;
+        bool have_tv = walk.next(S, tv);
+        if (have_tv && tv.x < platform) tv.z = fminf(tv.z, source_ground);
+        // The next vertex of the vertical profile.
+        auto next_vertex = [&](TV &out_v) -> bool {
+            for (;;) {
+                if (ipend < npend) {
+                    out_v = pend[ipend++];
+                    return true;
+                }
+                if (!have_tv) return false;
+                if (ri < nr && w.roofs[ri].x0 < tv.x) {
+                    const Roof &r = w.roofs[ri];
+                    pend[0] = TV{r.x0, r.zt0, r.g0};
+                    pend[1] = TV{r.x0, r.top0, 0.0f};
+                    pend[2] = TV{r.x1, r.top1, 0.0f};
+                    pend[3] = TV{r.x1, r.zt1, r.g1};
+                    npend = 4;
+                    ipend = 0;
+                    covered_to = r.x1;
+                    ++ri;
+                    continue;
+                }
+                TV t = tv;
+                have_tv = walk.next(S, tv);
+                if (have_tv && tv.x < platform) tv.z = fminf(tv.z, source_ground);
+                if (t.x > covered_to) {
+                    out_v = t;
+                    return true;
+                }
+            }
+        };
+        TV vnext;
+        bool have_next = next_vertex(vnext);
+        auto consume = [&](const TV &v) {
+            add_stretch(total, 0.0f, z0, vprev.x, vprev.z, vprev.g, v.x, v.z, v.g);
+            hom.consume(vprev, v);
+            if (want_fav) fav.consume(vprev, v);
+            vprev = v;
+        };
+        int ik = 0, it = 0;
+        for (;;) {
+            // Next candidate strictly inside (0, L), terrain first at equal x.
+            while (ik < nk && !(w.crests[ik].x > 0.0f && w.crests[ik].x < L)) ++ik;
+            while (it < nt && !(w.tops[it].x > 0.0f && w.tops[it].x < L)) ++it;
+            PlanePoint c;
+            if (ik < nk && it < nt) {
+                if (w.tops[it].x < w.crests[ik].x)
+                    c = w.tops[it++];
+                else
+                    c = w.crests[ik++];
+            } else if (ik < nk) {
+                c = w.crests[ik++];
+            } else if (it < nt) {
+                c = w.tops[it++];
+            } else {
+                break;
+            }
+            while (have_next && vnext.x <= c.x) {
+                consume(vnext);
+                have_next = next_vertex(vnext);
+            }
+            if (vprev.x < c.x && have_next) {
+                float f = (c.x - vprev.x) / (vnext.x - vprev.x);
+                consume(TV{c.x, vprev.z + f * (vnext.z - vprev.z), vprev.g + f * (vnext.g - vprev.g)});
+            }
+            hom.candidate(c, total, z0, vprev.z, vprev.g);
+            if (want_fav) fav.candidate(c, total, z0, vprev.z, vprev.g);
+        }
+        while (have_next) {
+            consume(vnext);
+            have_next = next_vertex(vnext);
+        }
+    }
+    // The direct path (diffraction.rs:44-61) and each state's boundary.
+    MeanPlane dplane = plane_of(total, 0.0f, L, z0);
+    EqGeometry direct = geometry_over(dplane, Sp, Rp);
+    float path_ground = mean_ground_of(total, L, g0);
+    float source_gf = src.gf >= 0.0f ? src.gf : g0;
+    float near_source = ground_factor_near_source(direct, path_ground, source_gf);
+    float att[QM_BANDS];
+    state_boundary<QM_HOM, CAP_H>(hom, direct, path_ground, near_source, source_gf, z0, g0, L, att);
+    if (hom.failed) out.status |= FAILED_CAPACITY;
+#pragma unroll
+    for (int b = 0; b < QM_BANDS; ++b) out.boundary[0][b] = __expf(-att[b] * LN10_OVER_10);
+    if (want_fav) {
+        state_boundary<QM_FAV, CAP_H>(fav, direct, path_ground, near_source, source_gf, z0, g0, L, att);
+        if (fav.failed) out.status |= FAILED_CAPACITY;
+#pragma unroll
+        for (int b = 0; b < QM_BANDS; ++b) out.boundary[1][b] = __expf(-att[b] * LN10_OVER_10);
+    } else {
+#pragma unroll
+        for (int b = 0; b < QM_BANDS; ++b) out.boundary[1][b] = out.boundary[0][b];
+    }
+    // Slant, divergence, p (ray.rs:132-137; evaluate.rs:199-204, 317-322).
+    float dz = rcv_alt - src_alt;
+    out.slant = fmaxf(sqrtf(L * L + dz * dz), 1.0f);
+    float dh = fmaxf(dist, src.excl);
+    float d = fmaxf(sqrtf(dh * dh + dz * dz), 1.0f);
+    out.weight = 1.0f / (d * d * 12.589254117941673f);
+    float azimuth = atan2f(dym, dxm);
+#pragma unroll
+    for (int p = 0; p < QM_PERIODS; ++p) out.p[p] = want_fav ? favourable_at(S.fav[p], azimuth) : 0.0f;
+}
+
+}  // namespace qm

@@ -1,0 +1,184 @@
+"""ctypes binding of the CUDA library (quietmap_b200/libqm_b200.so, C ABI of include/qm_batch.h).
+
+There is no CPU fallback: if the library is missing or no sm_100 device is present, every call
+raises. The library is built in-tree by quietmap_b200/build.py (or `__graft_entry__.build()`).
+"""
+
+import ctypes as C
+import os
+
+import numpy as np
+
+from . import abi
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libqm_b200.so")
+
+_D = C.POINTER(C.c_double)
+_F = C.POINTER(C.c_float)
+_U32 = C.POINTER(C.c_uint32)
+_U64 = C.POINTER(C.c_uint64)
+_I32 = C.POINTER(C.c_int32)
+
+
+class QmError(RuntimeError):
+    def __init__(self, status, message):
+        super().__init__(f"qm status {status}: {message}")
+        self.status = status
+
+
+_lib = None
+
+
+def lib():
+    """The loaded library; raises if it has not been built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise QmError(abi.QM_ERR_UNSUPPORTED,
+                          f"{LIB_PATH} is missing: build it with quietmap_b200/build.py")
+        L = C.CDLL(LIB_PATH)
+        L.qm_abi_version.restype = C.c_int
+        L.qm_open.argtypes = [C.c_int, C.POINTER(C.c_void_p)]
+        L.qm_open.restype = C.c_int
+        L.qm_close.argtypes = [C.c_void_p]
+        L.qm_last_error.argtypes = [C.c_void_p]
+        L.qm_last_error.restype = C.c_char_p
+        L.qm_scene_upload.argtypes = [C.c_void_p, C.POINTER(abi.SceneDesc), C.POINTER(C.c_void_p)]
+        L.qm_scene_upload.restype = C.c_int
+        L.qm_scene_free.argtypes = [C.c_void_p]
+        L.qm_evaluate_pairs.argtypes = [C.c_void_p, _D, _F, _U64, _U32, C.c_size_t, _U32, _U32, _F, C.c_size_t,
+                                        _F, _F, _U32, _F, C.c_size_t]
+        L.qm_evaluate_pairs.restype = C.c_int
+        L.qm_paint_grid.argtypes = [C.c_void_p, C.POINTER(abi.GridDesc), _F, _F, _F, _U32,
+                                    C.POINTER(abi.PaintStats)]
+        L.qm_paint_grid.restype = C.c_int
+        L.qm_zwicker.argtypes = [C.c_void_p, _F, C.c_size_t, _F]
+        L.qm_zwicker.restype = C.c_int
+        L.qm_level_histogram.argtypes = [C.c_void_p, _F, C.c_size_t, C.c_double, C.c_double, C.c_uint32, _U32]
+        L.qm_level_histogram.restype = C.c_int
+        L.qm_list_crossings.argtypes = [C.c_void_p, _I32, _I32, C.c_size_t, C.c_uint32, _U32, _U32, _D, _U32, _U32]
+        L.qm_list_crossings.restype = C.c_int
+        if L.qm_abi_version() != abi.ABI_VERSION:
+            raise QmError(abi.QM_ERR_UNSUPPORTED, "library ABI version mismatch")
+        _lib = L
+    return _lib
+
+
+def _check(status, ctx=None):
+    if status != abi.QM_OK:
+        message = lib().qm_last_error(ctx).decode(errors="replace")
+        raise QmError(status, message)
+
+
+class Context:
+    """One device (qm_open)."""
+
+    def __init__(self, device=0):
+        self.handle = C.c_void_p()
+        _check(lib().qm_open(device, C.byref(self.handle)))
+
+    def close(self):
+        if self.handle:
+            lib().qm_close(self.handle)
+            self.handle = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def scene(self, scene):
+        return DeviceScene(self, scene)
+
+    def zwicker(self, thirds_db):
+        thirds = np.ascontiguousarray(np.asarray(thirds_db, dtype=np.float32).reshape(-1, abi.THIRDS))
+        out = np.zeros(len(thirds), np.float32)
+        _check(lib().qm_zwicker(self.handle, abi.ptr(thirds, C.c_float), len(thirds), abi.ptr(out, C.c_float)),
+               self.handle)
+        return out
+
+    def level_histogram(self, levels_db, level_min_db=-30.0, bin_db=0.1, n_bins=1800):
+        levels = np.ascontiguousarray(levels_db, dtype=np.float32).ravel()
+        counts = np.zeros(n_bins, np.uint32)
+        _check(lib().qm_level_histogram(self.handle, abi.ptr(levels, C.c_float), len(levels), level_min_db,
+                                        bin_db, n_bins, abi.ptr(counts, C.c_uint32)), self.handle)
+        return counts
+
+
+class DeviceScene:
+    """A scene uploaded to the device (qm_scene_upload)."""
+
+    def __init__(self, ctx, scene):
+        self.ctx = ctx
+        self.scene = scene
+        self.packed = abi.PackedScene(scene)
+        self.handle = C.c_void_p()
+        _check(lib().qm_scene_upload(ctx.handle, C.byref(self.packed.desc), C.byref(self.handle)), ctx.handle)
+
+    def close(self):
+        if self.handle:
+            lib().qm_scene_free(self.handle)
+            self.handle = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def paint_grid(self, grid, histogram=True):
+        """The fused painter over `grid`: (bands [cells][8] dB, dBA [cells], Lden [cells],
+        histogram [n_bins] or None, stats dict)."""
+        g = abi.grid_desc(grid)
+        cells = grid.cells
+        bands = np.zeros((cells, 8), np.float32)
+        dba = np.zeros(cells, np.float32)
+        lden = np.zeros(cells, np.float32)
+        hist = np.zeros(grid.n_bins, np.uint32) if histogram else None
+        stats = abi.PaintStats()
+        _check(lib().qm_paint_grid(self.handle, C.byref(g), abi.ptr(bands, C.c_float), abi.ptr(dba, C.c_float),
+                                   abi.ptr(lden, C.c_float), abi.ptr(hist, C.c_uint32) if histogram else None,
+                                   C.byref(stats)), self.ctx.handle)
+        return bands, dba, lden, hist, dict(paths=stats.paths, failed_paths=stats.failed_paths,
+                                             crossings=stats.crossings, kernel_ms=stats.kernel_ms)
+
+    def evaluate_pairs(self, receiver_xy_m, receiver_height_m, own_footprint, point_of_receiver, source_of_pair,
+                       receiver_of_pair, band_weight, n_points, point_bands=None):
+        rxy = np.ascontiguousarray(np.asarray(receiver_xy_m, dtype=np.float64).reshape(-1, 2))
+        rh = np.ascontiguousarray(receiver_height_m, dtype=np.float32)
+        own = np.ascontiguousarray(own_footprint, dtype=np.uint64)
+        por = np.ascontiguousarray(point_of_receiver, dtype=np.uint32)
+        sop = np.ascontiguousarray(source_of_pair, dtype=np.uint32)
+        rop = np.ascontiguousarray(receiver_of_pair, dtype=np.uint32)
+        bw = None if band_weight is None else np.ascontiguousarray(band_weight, dtype=np.float32)
+        n = len(sop)
+        sums = np.zeros((n, abi.PAIR_SUMS), np.float32)
+        bands = np.zeros((n, abi.PERIODS, abi.BANDS), np.float32)
+        status = np.zeros(n, np.uint32)
+        if point_bands is None:
+            point_bands = np.zeros((n_points, abi.LAYERS, abi.PERIODS, abi.BANDS), np.float32)
+        _check(lib().qm_evaluate_pairs(self.handle, abi.ptr(rxy, C.c_double), abi.ptr(rh, C.c_float),
+                                       abi.ptr(own, C.c_uint64), abi.ptr(por, C.c_uint32), len(rxy),
+                                       abi.ptr(sop, C.c_uint32), abi.ptr(rop, C.c_uint32),
+                                       abi.ptr(bw, C.c_float) if bw is not None else None, n,
+                                       abi.ptr(sums, C.c_float), abi.ptr(bands, C.c_float),
+                                       abi.ptr(status, C.c_uint32), abi.ptr(point_bands, C.c_float), n_points),
+               self.ctx.handle)
+        return sums, bands, status, point_bands
+
+    def list_crossings(self, frm, to, cap=256):
+        frm = np.ascontiguousarray(np.asarray(frm).reshape(-1, 2), dtype=np.int32)
+        to = np.ascontiguousarray(np.asarray(to).reshape(-1, 2), dtype=np.int32)
+        n = len(frm)
+        counts = np.zeros(n, np.uint32)
+        status = np.zeros(n, np.uint32)
+        edges = np.zeros((n, cap), np.uint32)
+        t = np.zeros((n, cap), np.float64)
+        flags = np.zeros((n, cap), np.uint32)
+        _check(lib().qm_list_crossings(self.handle, abi.ptr(frm, C.c_int32), abi.ptr(to, C.c_int32), n, cap,
+                                       abi.ptr(counts, C.c_uint32), abi.ptr(edges, C.c_uint32),
+                                       abi.ptr(t, C.c_double), abi.ptr(flags, C.c_uint32),
+                                       abi.ptr(status, C.c_uint32)), self.ctx.handle)
+        return counts, edges, t, flags, status

@@ -1,0 +1,71 @@
+"""CPU-side checks of the C ABI: the library loads, exports every entry point the header
+declares, and the ctypes mirror matches the header's struct layout."""
+
+import ctypes as C
+import os
+import re
+import subprocess
+
+import pytest
+
+from quietmap_b200 import abi, native
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_functions():
+    names = set()
+    for header in os.listdir(os.path.join(ROOT, "include")):
+        if header.endswith(".h"):
+            text = open(os.path.join(ROOT, "include", header)).read()
+            names |= set(re.findall(r"^\s*(?:qm_status|void|int|const char \*)\s*\*?\s*(qm_\w+)\s*\(", text, re.M))
+    return names
+
+
+def test_library_exports_every_declared_entry_point():
+    if not os.path.exists(native.LIB_PATH):
+        from quietmap_b200 import build
+        build.build()
+    lib = C.CDLL(native.LIB_PATH)
+    declared = declared_functions()
+    assert {"qm_open", "qm_paint_grid", "qm_evaluate_pairs", "qm_zwicker"} <= declared
+    missing = [name for name in sorted(declared) if not hasattr(lib, name)]
+    assert not missing, missing
+    assert lib.qm_abi_version() == abi.ABI_VERSION
+
+
+def test_struct_layouts_match_the_header():
+    # Compile a tiny C program against the header and compare sizes and offsets.
+    src = r'''
+#include <stdio.h>
+#include <stddef.h>
+#include "qm_batch.h"
+int main(void) {
+  printf("%zu %zu %zu %zu %zu\n", sizeof(qm_outline), sizeof(qm_source), sizeof(qm_scene_desc),
+         sizeof(qm_grid_desc), sizeof(qm_paint_stats));
+  printf("%zu %zu %zu %zu\n", offsetof(qm_source, energy), offsetof(qm_scene_desc, favourable),
+         offsetof(qm_scene_desc, alpha_db_per_km), offsetof(qm_grid_desc, n_bins));
+  return 0;
+}
+'''
+    import tempfile
+    with tempfile.TemporaryDirectory() as d:
+        path = os.path.join(d, "layout.c")
+        open(path, "w").write(src)
+        exe = os.path.join(d, "layout")
+        subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), path, "-o", exe], check=True)
+        out = subprocess.run([exe], check=True, capture_output=True, text=True).stdout.split()
+    sizes = list(map(int, out[:5]))
+    offsets = list(map(int, out[5:]))
+    assert sizes == [C.sizeof(abi.Outline), C.sizeof(abi.Source), C.sizeof(abi.SceneDesc), C.sizeof(abi.GridDesc),
+                     C.sizeof(abi.PaintStats)]
+    assert offsets == [abi.Source.energy.offset, abi.SceneDesc.favourable.offset,
+                       abi.SceneDesc.alpha_db_per_km.offset, abi.GridDesc.n_bins.offset]
+
+
+def test_open_without_a_device_fails_loudly():
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a device is present")
+    with pytest.raises(native.QmError):
+        native.Context(0)
