@@ -39,6 +39,8 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="terrain", choices=["terrain", "road"])
     ap.add_argument("--receivers", type=int, default=0, help="receivers per step (0: workload default)")
+    ap.add_argument("--sources", type=int, default=0,
+                    help="paint only the first N sources (a small case for profiling; 0: all)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     return ap.parse_args()
 
@@ -53,11 +55,13 @@ def dist_env():
 def workload(name, rank, receivers):
     from quietmap_b200 import scenes
     if name == "road":
-        scene, grid = scenes.road_square()
-        desc = dict(workload="road square 1 km, 128x128 receivers x 77k point sources (flat, G=0.5, homogeneous)",
-                    global_batch=grid.cells)
-        return scene, [grid], desc
-    scene, full = scenes.terrain_square()
+        scene, full = scenes.road_square()
+        if not receivers:
+            desc = dict(workload="road square 1 km, 128x128 receivers x 77k point sources (flat, G=0.5, "
+                                 "homogeneous)", global_batch=full.cells)
+            return scene, [full], desc
+    else:
+        scene, full = scenes.terrain_square()
     per_step = receivers or 256
     tile_w, tile_h = 16, 8
     n_tiles = max(per_step // (tile_w * tile_h), 1)
@@ -76,9 +80,12 @@ def workload(name, rank, receivers):
         grids.append([scenes.Grid(origin=(full.origin[0] + tx * tile_w * full.spacing,
                                           full.origin[1] + ty * tile_h * full.spacing),
                                   spacing=full.spacing, nx=tile_w, ny=tile_h) for tx, ty in tiles])
-    desc = dict(workload=f"terrain square 16 km^2 (2048^2 grid at 1.953 m), {n_tiles} seeded 16x8 receiver "
-                         f"tiles per step x {len(scene.sources)} point sources, 30,000 buildings, fBm DEM",
-                global_batch=n_tiles * tile_w * tile_h)
+    if name == "road":
+        what = "road square 1 km (128^2 grid at 7.8125 m, flat G=0.5, homogeneous), 300 buildings"
+    else:
+        what = "terrain square 16 km^2 (2048^2 grid at 1.953 m), 30,000 buildings, fBm DEM"
+    desc = dict(workload=f"{what}: {n_tiles} seeded 16x8 receiver tiles per step x {len(scene.sources)} "
+                         f"point sources", global_batch=n_tiles * tile_w * tile_h)
     return scene, grids, desc
 
 
@@ -174,6 +181,12 @@ def main():
     dev = ctx.scene(scene)
     n_src = len(scene.sources)
 
+    if args.sources:
+        for block in grids:
+            for g in (block if isinstance(block, list) else [block]):
+                g.source_begin, g.source_end = 0, min(args.sources, n_src)
+        desc["workload"] += f" (first {min(args.sources, n_src)} sources only)"
+
     def step(i):
         block = grids[i % len(grids)]
         tiles = block if isinstance(block, list) else [block]
@@ -183,10 +196,15 @@ def main():
             paths += st["paths"]
             kms += st["kernel_ms"]
             crossings += st["crossings"]
+            for k in ("edge_tests", "vertices", "candidates"):
+                work[k] += st[k]
         return paths, kms, crossings, len(tiles)
+
+    work = dict(edge_tests=0, vertices=0, candidates=0)
 
     for i in range(args.warmup):
         step(i)
+    work.update(edge_tests=0, vertices=0, candidates=0)
     if world > 1:
         torch.distributed.barrier()
     torch.cuda.synchronize()
@@ -232,7 +250,8 @@ def main():
                     "d2h_bytes_per_step": calls * (cells_per_call * 40 + 1800 * 4) // args.steps if args.steps else 0},
             "gpu_launches": calls * 2,
             "clocks": clocks.summary(),
-            "crossings_per_path": total_cross / max(total_paths, 1),
+            "per_path": dict(crossings=total_cross / max(total_paths, 1),
+                             **{k: v / max(total_paths, 1) for k, v in work.items()}),
         }
         if not args.no_cpu_baseline and world == 1:
             line["cpu_baseline"] = cpu_baseline(scene, grids)

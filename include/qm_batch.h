@@ -126,7 +126,10 @@ typedef struct {
     uint64_t paths;          /* receiver x source paths evaluated */
     uint64_t failed_paths;   /* paths re-run by the high-capacity pass */
     uint64_t crossings;      /* obstacle crossings found */
-    double kernel_ms;        /* device time of the painting kernels */
+    uint64_t edge_tests;     /* exact segment-edge tests of the crossing walk */
+    uint64_t vertices;       /* vertical-profile vertices streamed (terrain and roofs) */
+    uint64_t candidates;     /* diffraction candidates fed to the rubber bands */
+    double kernel_ms;        /* device time of the painting kernels (paint, re-run, reduce) */
 } qm_paint_stats;
 
 typedef struct qm_ctx qm_ctx;

@@ -100,6 +100,9 @@ class PaintStats(C.Structure):
         ("paths", C.c_uint64),
         ("failed_paths", C.c_uint64),
         ("crossings", C.c_uint64),
+        ("edge_tests", C.c_uint64),
+        ("vertices", C.c_uint64),
+        ("candidates", C.c_uint64),
         ("kernel_ms", C.c_double),
     ]
 

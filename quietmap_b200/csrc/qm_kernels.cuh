@@ -24,7 +24,7 @@ struct CapsFlat {
     static constexpr int C = 64, K = 2, H = 24;
 };
 struct CapsTerrain {
-    static constexpr int C = 192, K = 448, H = 48;
+    static constexpr int C = 256, K = 512, H = 64;
 };
 struct CapsLarge {
     static constexpr int C = 1024, K = 4096, H = 256;
@@ -43,18 +43,48 @@ struct GridArgs {
     const uint32_t *rcv_own; // [cells] dense own footprint
     float *partial;          // [n_chunks][cells][GRID_SLOTS]
     uint32_t *failed;        // [cells] bitwise-or of path failures
-    unsigned long long *counters;  // [0] paths [1] crossings [2] edge tests [3] failed paths
+    unsigned long long *counters;  // paths, crossings, edge tests, failed paths, vertices, candidates
+    uint2 *retry;            // failed (cell, source) paths, re-run with large capacities
+    uint32_t retry_cap;
+    unsigned int *retry_count;
     float lden_w[QM_PERIODS];
     bool want_fav;
     int tile_w, tile_h;      // receiver tile per CTA
 };
 
+// The 9 energies one path adds to its cell: day bands (transfer of period 0) and the Lden-weighted
+// A energy over the periods (popup/src/evaluate.rs:135-142; physics/src/bands.rs:59-66).
+__device__ __forceinline__ void path_energies(const SceneDev &S, const PathResult &r, const SourceDev &src,
+                                              const float lden_w[QM_PERIODS], float day[QM_BANDS], float &lden) {
+    float air[QM_BANDS];
+#pragma unroll
+    for (int b = 0; b < QM_BANDS; ++b) air[b] = __expf(-S.air_per_m[b] * r.slant);
+    float lsum = 0.f;
+#pragma unroll
+    for (int p = 0; p < QM_PERIODS; ++p) {
+        float pp = r.p[p];
+        float psum = 0.f;
+#pragma unroll
+        for (int b = 0; b < QM_BANDS; ++b) {
+            float t = air[b] * (pp * r.boundary[1][b] + (1.0f - pp) * r.boundary[0][b]);
+            float e = r.weight * __ldg(&src.energy[p * QM_BANDS + b]) * t;
+            if (p == 0) day[b] = e;
+            psum += e;
+        }
+        lsum += lden_w[p] * psum;
+    }
+    lden = lsum;
+}
+
 // Thread = one receiver of a tile; CTA = (receiver tile, source chunk). Each thread walks its chunk
 // of sources and keeps its cell's band energies in compensated registers; one store per cell.
 template <class Caps>
-__global__ void __launch_bounds__(128) paint_grid_kernel(SceneDev S, GridArgs A) {
-    __shared__ unsigned long long s_counts[4];
-    if (threadIdx.x < 4) s_counts[threadIdx.x] = 0;
+#ifndef QM_PAINT_MIN_BLOCKS
+#define QM_PAINT_MIN_BLOCKS 4  // CTAs of 128 resident per SM: caps registers at 128 a thread
+#endif
+__global__ void __launch_bounds__(128, QM_PAINT_MIN_BLOCKS) paint_grid_kernel(SceneDev S, GridArgs A) {
+    __shared__ unsigned long long s_counts[6];
+    if (threadIdx.x < 6) s_counts[threadIdx.x] = 0;
     __syncthreads();
     const int tiles_x = (A.nx + A.tile_w - 1) / A.tile_w;
     const int tile = blockIdx.x;
@@ -69,7 +99,7 @@ __global__ void __launch_bounds__(128) paint_grid_kernel(SceneDev S, GridArgs A)
 #pragma unroll
     for (int b = 0; b < QM_BANDS; ++b) bands[b] = KSum{0.f, 0.f};
     uint32_t failed = 0;
-    unsigned long long paths = 0, crossings = 0, tested = 0, failed_paths = 0;
+    unsigned long long paths = 0, crossings = 0, tested = 0, failed_paths = 0, vertices = 0, candidates = 0;
     if (active) {
         const int rx = A.origin_x + ix * A.spacing, ry = A.origin_y + iy * A.spacing;
         const float alt = A.rcv_alt[cell];
@@ -84,29 +114,20 @@ __global__ void __launch_bounds__(128) paint_grid_kernel(SceneDev S, GridArgs A)
             ++paths;
             crossings += r.crossings;
             tested += r.edges_tested;
+            vertices += r.vertices;
+            candidates += r.candidates;
             if (r.status) {
                 failed |= r.status;
                 ++failed_paths;
+                unsigned int slot = atomicAdd(A.retry_count, 1u);
+                if (slot < A.retry_cap) A.retry[slot] = make_uint2((uint32_t)cell, s);
                 continue;
             }
-            float air[QM_BANDS];
+            float day[QM_BANDS], le;
+            path_energies(S, r, src, A.lden_w, day, le);
 #pragma unroll
-            for (int b = 0; b < QM_BANDS; ++b) air[b] = __expf(-S.alpha[b] * r.slant * (LN10_OVER_10 / 1000.0f));
-            float lsum = 0.f;
-#pragma unroll
-            for (int p = 0; p < QM_PERIODS; ++p) {
-                float pp = r.p[p];
-                float psum = 0.f;
-#pragma unroll
-                for (int b = 0; b < QM_BANDS; ++b) {
-                    float t = air[b] * (pp * r.boundary[1][b] + (1.0f - pp) * r.boundary[0][b]);
-                    float e = r.weight * __ldg(&src.energy[p * QM_BANDS + b]) * t;
-                    if (p == 0) bands[b].add(e);
-                    psum += e;
-                }
-                lsum += A.lden_w[p] * psum;
-            }
-            lden.add(lsum);
+            for (int b = 0; b < QM_BANDS; ++b) bands[b].add(day[b]);
+            lden.add(le);
         }
         float *out = A.partial + ((size_t)chunk * (A.nx * A.ny) + cell) * GRID_SLOTS;
 #pragma unroll
@@ -121,15 +142,62 @@ __global__ void __launch_bounds__(128) paint_grid_kernel(SceneDev S, GridArgs A)
         crossings += __shfl_down_sync(0xffffffffu, crossings, o);
         tested += __shfl_down_sync(0xffffffffu, tested, o);
         failed_paths += __shfl_down_sync(0xffffffffu, failed_paths, o);
+        vertices += __shfl_down_sync(0xffffffffu, vertices, o);
+        candidates += __shfl_down_sync(0xffffffffu, candidates, o);
     }
     if ((threadIdx.x & 31) == 0) {
         atomicAdd(&s_counts[0], paths);
         atomicAdd(&s_counts[1], crossings);
         atomicAdd(&s_counts[2], tested);
         atomicAdd(&s_counts[3], failed_paths);
+        atomicAdd(&s_counts[4], vertices);
+        atomicAdd(&s_counts[5], candidates);
     }
     __syncthreads();
-    if (threadIdx.x < 4) atomicAdd(A.counters + threadIdx.x, s_counts[threadIdx.x]);
+    if (threadIdx.x < 6) atomicAdd(A.counters + threadIdx.x, s_counts[threadIdx.x]);
+}
+
+// Failed paths again, with large per-path capacities held in global scratch (one work area per
+// thread, grid-stride over the sorted list): each path's 9 energies into `out`.
+__global__ void __launch_bounds__(64) retry_paths_kernel(SceneDev S, GridArgs A, const uint2 *pairs, uint32_t n,
+                                                         PathWork<CapsLarge::C, CapsLarge::K, CapsLarge::H> *works,
+                                                         float *out, uint32_t *status) {
+    uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t stride = gridDim.x * blockDim.x;
+    PathWork<CapsLarge::C, CapsLarge::K, CapsLarge::H> &work = works[tid];
+    for (uint32_t i = tid; i < n; i += stride) {
+        uint2 pr = pairs[i];
+        int cell = (int)pr.x;
+        int ix = cell % A.nx, iy = cell / A.nx;
+        const SourceDev &src = S.sources[pr.y];
+        PathResult r;
+        evaluate_path<CapsLarge::C, CapsLarge::K, CapsLarge::H>(S, src, A.origin_x + ix * A.spacing,
+                                                                A.origin_y + iy * A.spacing, A.rcv_alt[cell],
+                                                                A.rcv_own[cell], A.want_fav, work, r);
+        status[i] = r.status;
+        float day[QM_BANDS], le = 0.f;
+        if (r.status == 0) path_energies(S, r, src, A.lden_w, day, le);
+#pragma unroll
+        for (int b = 0; b < QM_BANDS; ++b) out[(size_t)i * GRID_SLOTS + b] = r.status ? 0.f : day[b];
+        out[(size_t)i * GRID_SLOTS + 8] = le;
+    }
+}
+
+// The re-run paths of each failing cell, summed in (cell, source) order into the partial slice
+// `slice` (deterministic).
+__global__ void fold_retry_kernel(const uint32_t *cell_ids, const uint32_t *cell_start, uint32_t n_cells,
+                                  const float *results, float *partial, uint32_t slice, int cells) {
+    uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n_cells) return;
+    KSum acc[GRID_SLOTS];
+#pragma unroll
+    for (int j = 0; j < GRID_SLOTS; ++j) acc[j] = KSum{0.f, 0.f};
+    for (uint32_t i = cell_start[k]; i < cell_start[k + 1]; ++i)
+#pragma unroll
+        for (int j = 0; j < GRID_SLOTS; ++j) acc[j].add(results[(size_t)i * GRID_SLOTS + j]);
+    float *dst = partial + ((size_t)slice * cells + cell_ids[k]) * GRID_SLOTS;
+#pragma unroll
+    for (int j = 0; j < GRID_SLOTS; ++j) dst[j] = acc[j].value();
 }
 
 // The bin of a level (popup/src/distribution.rs:69-72): round((L - L_min) / bin) with Rust's
@@ -216,23 +284,12 @@ struct PairArgs {
     uint32_t *status;   // [n]
 };
 
-// One thread per pair: the pair's ray with both states, its PairEnergy (exact.rs:128-132,
-// 200-203) and its bands per period (received_bands, evaluate.rs:270-290).
-template <class Caps>
-__global__ void __launch_bounds__(128) evaluate_pairs_kernel(SceneDev S, PairArgs A) {
-    size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
-    if (i >= A.n_pairs) return;
-    uint32_t r = A.receiver_of_pair[i];
-    const SourceDev &src = S.sources[A.source_of_pair[i]];
-    int2 xy = A.rcv_xy[r];
-    PathWork<Caps::C, Caps::K, Caps::H> work;
-    PathResult res;
-    evaluate_path<Caps::C, Caps::K, Caps::H>(S, src, xy.x, xy.y, A.rcv_alt[r], A.rcv_own[r], true, work, res);
+// A pair's PairEnergy sums and its bands per period from its path.
+__device__ __forceinline__ void pair_outputs(const SceneDev &S, const SourceDev &src, const PathResult &res, float *sums,
+                                             float *bands) {
     float air[QM_BANDS];
 #pragma unroll
-    for (int b = 0; b < QM_BANDS; ++b) air[b] = __expf(-S.alpha[b] * res.slant * (LN10_OVER_10 / 1000.0f));
-    float *sums = A.pair_sums + i * 9;
-    float *bands = A.pair_bands + i * QM_PERIODS * QM_BANDS;
+    for (int b = 0; b < QM_BANDS; ++b) air[b] = __expf(-S.air_per_m[b] * res.slant);
 #pragma unroll
     for (int p = 0; p < QM_PERIODS; ++p) {
         float mixed = 0.f, calm = 0.f, down = 0.f;
@@ -250,7 +307,41 @@ __global__ void __launch_bounds__(128) evaluate_pairs_kernel(SceneDev S, PairArg
         sums[3 + p] = calm;
         sums[6 + p] = down;
     }
+}
+
+// One thread per pair: the pair's ray with both states, its PairEnergy (exact.rs:128-132,
+// 200-203) and its bands per period (received_bands, evaluate.rs:270-290).
+template <class Caps>
+__global__ void __launch_bounds__(128) evaluate_pairs_kernel(SceneDev S, PairArgs A) {
+    size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+    if (i >= A.n_pairs) return;
+    uint32_t r = A.receiver_of_pair[i];
+    const SourceDev &src = S.sources[A.source_of_pair[i]];
+    int2 xy = A.rcv_xy[r];
+    PathWork<Caps::C, Caps::K, Caps::H> work;
+    PathResult res;
+    evaluate_path<Caps::C, Caps::K, Caps::H>(S, src, xy.x, xy.y, A.rcv_alt[r], A.rcv_own[r], true, work, res);
+    pair_outputs(S, src, res, A.pair_sums + i * 9, A.pair_bands + i * QM_PERIODS * QM_BANDS);
     A.status[i] = res.status;
+}
+
+// Failed pairs again with large per-path capacities held in global scratch (grid-stride).
+__global__ void __launch_bounds__(64) retry_pairs_kernel(SceneDev S, PairArgs A, const uint32_t *indices, uint32_t n,
+                                                         PathWork<CapsLarge::C, CapsLarge::K, CapsLarge::H> *works) {
+    uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t stride = gridDim.x * blockDim.x;
+    PathWork<CapsLarge::C, CapsLarge::K, CapsLarge::H> &work = works[tid];
+    for (uint32_t k = tid; k < n; k += stride) {
+        size_t i = indices[k];
+        uint32_t r = A.receiver_of_pair[i];
+        const SourceDev &src = S.sources[A.source_of_pair[i]];
+        int2 xy = A.rcv_xy[r];
+        PathResult res;
+        evaluate_path<CapsLarge::C, CapsLarge::K, CapsLarge::H>(S, src, xy.x, xy.y, A.rcv_alt[r], A.rcv_own[r], true,
+                                                                work, res);
+        pair_outputs(S, src, res, A.pair_sums + i * 9, A.pair_bands + i * QM_PERIODS * QM_BANDS);
+        A.status[i] = res.status;
+    }
 }
 
 // Point bands (add_bands, exact.rs:208-215): pairs grouped by point (a stable order), one thread per

@@ -97,6 +97,19 @@ struct Scratch {
     }
 };
 
+// A pair of timing events destroyed when the holder leaves scope.
+struct Events {
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    cudaError_t create() {
+        cudaError_t e = cudaEventCreate(&e0);
+        return e != cudaSuccess ? e : cudaEventCreate(&e1);
+    }
+    ~Events() {
+        if (e0) cudaEventDestroy(e0);
+        if (e1) cudaEventDestroy(e1);
+    }
+};
+
 bool segment_meets_box(int64_t ax, int64_t ay, int64_t bx, int64_t by, int64_t x0, int64_t y0, int64_t x1, int64_t y1) {
     if (std::max(ax, bx) < x0 || std::min(ax, bx) > x1 || std::max(ay, by) < y0 || std::min(ay, by) > y1) return false;
     int64_t dx = bx - ax, dy = by - ay;
@@ -343,8 +356,6 @@ qm_status qm_scene_upload(qm_ctx *ctx, const qm_scene_desc *d, qm_scene **out) {
     dv.cells_x = cells_x;
     dv.cells_y = cells_y;
     qm_status st;
-    int2 *vtx_dummy = nullptr;
-    (void)vtx_dummy;
     if ((st = upload(s, cell_start.data(), cell_start.size(), &dv.cell_start)) != QM_OK ||
         (st = upload(s, cell_seg.data(), cell_seg.size(), &dv.cell_seg)) != QM_OK ||
         (st = upload(s, cell_ref.data(), cell_ref.size(), &dv.cell_ref)) != QM_OK ||
@@ -365,6 +376,7 @@ qm_status qm_scene_upload(qm_ctx *ctx, const qm_scene_desc *d, qm_scene **out) {
     dv.n_sources = d->n_sources;
     std::memcpy(dv.fav, d->favourable, sizeof(dv.fav));
     std::memcpy(dv.alpha, d->alpha_db_per_km, sizeof(dv.alpha));
+    for (int b = 0; b < 8; ++b) dv.air_per_m[b] = (float)((double)d->alpha_db_per_km[b] * (2.302585092994046 / 10.0 / 1000.0));
     *out = s;
     return QM_OK;
 }
@@ -430,12 +442,13 @@ qm_status qm_paint_grid(qm_scene *scene, const qm_grid_desc *grid, float *cell_b
                         float *cell_lden, uint32_t *histogram, qm_paint_stats *stats) {
     if (!scene || !grid) return fail(QM_ERR_ARGUMENT, "qm_paint_grid: null scene or grid");
     const qm_grid_desc &g = *grid;
-    if (g.nx <= 0 || g.ny <= 0 || g.spacing <= 0) return fail(QM_ERR_ARGUMENT, "qm_paint_grid: grid nx, ny or spacing");
+    if (g.nx <= 0 || g.ny <= 0 || g.spacing <= 0 || (int64_t)g.nx * g.ny > (int64_t(1) << 30))
+        return fail(QM_ERR_ARGUMENT, "qm_paint_grid: grid nx, ny or spacing");
     int64_t last_x = g.origin[0] + (int64_t)(g.nx - 1) * g.spacing, last_y = g.origin[1] + (int64_t)(g.ny - 1) * g.spacing;
     if (g.origin[0] < 0 || g.origin[1] < 0 || last_x >= scene->extent[0] || last_y >= scene->extent[1])
         return fail(QM_ERR_ARGUMENT, "qm_paint_grid: grid receivers outside the scene extent");
-    if (histogram && (g.n_bins == 0 || !(g.bin_db > 0.0)))
-        return fail(QM_ERR_ARGUMENT, "qm_paint_grid: histogram needs n_bins > 0 and bin_db > 0");
+    if (histogram && (g.n_bins == 0 || g.n_bins > 51200 || !(g.bin_db > 0.0)))
+        return fail(QM_ERR_ARGUMENT, "qm_paint_grid: histogram needs 0 < n_bins <= 51200 and bin_db > 0");
     uint32_t sb = g.source_begin, se = g.source_end;
     if (se <= sb) {
         sb = 0;
@@ -471,28 +484,35 @@ qm_status qm_paint_grid(qm_scene *scene, const qm_grid_desc *grid, float *cell_b
     n_chunks = std::min<uint32_t>(n_chunks, 65535);
     A.chunk = std::max<uint32_t>(1, (n_src + n_chunks - 1) / n_chunks);
     A.n_chunks = n_src == 0 ? 1 : (n_src + A.chunk - 1) / A.chunk;
-    Scratch d_alt, d_own, d_partial, d_failed, d_counters, d_dba, d_hist, d_bands, d_dbaout, d_lden;
-    size_t partial_bytes = (size_t)A.n_chunks * cells * GRID_SLOTS * sizeof(float);
+    const uint32_t slices = A.n_chunks + 1;  // the last slice holds the re-run paths
+    // The retry list holds up to 1 path in 128 (and at least 1 M): over-capacity paths are rare.
+    A.retry_cap = (uint32_t)std::min<int64_t>(std::max<int64_t>((int64_t)cells * n_src / 128, 1 << 20), 1 << 25);
+    Scratch d_alt, d_own, d_partial, d_failed, d_counters, d_dba, d_hist, d_bands, d_dbaout, d_lden, d_retry, d_rcount;
+    size_t partial_bytes = (size_t)slices * cells * GRID_SLOTS * sizeof(float);
     QM_CUDA(cudaMalloc(&d_alt.p, cells * sizeof(float)));
     QM_CUDA(cudaMalloc(&d_own.p, cells * sizeof(uint32_t)));
     QM_CUDA(cudaMalloc(&d_partial.p, partial_bytes));
     QM_CUDA(cudaMalloc(&d_failed.p, cells * sizeof(uint32_t)));
-    QM_CUDA(cudaMalloc(&d_counters.p, 4 * sizeof(unsigned long long)));
+    QM_CUDA(cudaMalloc(&d_counters.p, 6 * sizeof(unsigned long long)));
     QM_CUDA(cudaMalloc(&d_dba.p, cells * sizeof(float)));
+    QM_CUDA(cudaMalloc(&d_retry.p, (size_t)A.retry_cap * sizeof(uint2)));
+    QM_CUDA(cudaMalloc(&d_rcount.p, sizeof(unsigned int)));
     QM_CUDA(cudaMemcpyAsync(d_alt.p, alt.data(), cells * sizeof(float), cudaMemcpyHostToDevice, stream));
     QM_CUDA(cudaMemcpyAsync(d_own.p, own.data(), cells * sizeof(uint32_t), cudaMemcpyHostToDevice, stream));
     QM_CUDA(cudaMemsetAsync(d_partial.p, 0, partial_bytes, stream));
     QM_CUDA(cudaMemsetAsync(d_failed.p, 0, cells * sizeof(uint32_t), stream));
-    QM_CUDA(cudaMemsetAsync(d_counters.p, 0, 4 * sizeof(unsigned long long), stream));
+    QM_CUDA(cudaMemsetAsync(d_counters.p, 0, 6 * sizeof(unsigned long long), stream));
+    QM_CUDA(cudaMemsetAsync(d_rcount.p, 0, sizeof(unsigned int), stream));
     A.rcv_alt = static_cast<float *>(d_alt.p);
     A.rcv_own = static_cast<uint32_t *>(d_own.p);
     A.partial = static_cast<float *>(d_partial.p);
     A.failed = static_cast<uint32_t *>(d_failed.p);
     A.counters = static_cast<unsigned long long *>(d_counters.p);
-    cudaEvent_t e0, e1;
-    QM_CUDA(cudaEventCreate(&e0));
-    QM_CUDA(cudaEventCreate(&e1));
-    QM_CUDA(cudaEventRecord(e0, stream));
+    A.retry = static_cast<uint2 *>(d_retry.p);
+    A.retry_count = static_cast<unsigned int *>(d_rcount.p);
+    Events ev;
+    QM_CUDA(ev.create());
+    QM_CUDA(cudaEventRecord(ev.e0, stream));
     if (n_src > 0) {
         dim3 grid_dim(tiles, A.n_chunks);
         if (terrain_caps(scene))
@@ -501,10 +521,57 @@ qm_status qm_paint_grid(qm_scene *scene, const qm_grid_desc *grid, float *cell_b
             paint_grid_kernel<CapsFlat><<<grid_dim, 128, 0, stream>>>(scene->dev, A);
         QM_CUDA(cudaGetLastError());
     }
-    QM_CUDA(cudaEventRecord(e1, stream));
+    unsigned int n_retry = 0;
+    QM_CUDA(cudaMemcpyAsync(&n_retry, d_rcount.p, sizeof(n_retry), cudaMemcpyDeviceToHost, stream));
+    QM_CUDA(cudaStreamSynchronize(stream));
+    if (n_retry > A.retry_cap)
+        return fail(QM_ERR_CAPACITY, "qm_paint_grid: " + std::to_string(n_retry) +
+                                         " paths exceeded the per-path capacities, more than the retry list holds");
+    Scratch d_sorted, d_cids, d_cstart, d_works, d_results, d_rstatus;
+    if (n_retry > 0) {
+        // Re-run the failed paths in (cell, source) order with large capacities.
+        std::vector<uint2> list(n_retry);
+        QM_CUDA(cudaMemcpy(list.data(), d_retry.p, n_retry * sizeof(uint2), cudaMemcpyDeviceToHost));
+        std::sort(list.begin(), list.end(), [](uint2 a, uint2 b) { return a.x != b.x ? a.x < b.x : a.y < b.y; });
+        std::vector<uint32_t> cids, cstart;
+        for (uint32_t i = 0; i < n_retry; ++i)
+            if (cids.empty() || cids.back() != list[i].x) {
+                cids.push_back(list[i].x);
+                cstart.push_back(i);
+            }
+        cstart.push_back(n_retry);
+        const uint32_t threads = std::min<uint32_t>(((n_retry + 63) / 64) * 64, 8192);
+        using Large = PathWork<CapsLarge::C, CapsLarge::K, CapsLarge::H>;
+        QM_CUDA(cudaMalloc(&d_sorted.p, n_retry * sizeof(uint2)));
+        QM_CUDA(cudaMalloc(&d_cids.p, cids.size() * sizeof(uint32_t)));
+        QM_CUDA(cudaMalloc(&d_cstart.p, cstart.size() * sizeof(uint32_t)));
+        QM_CUDA(cudaMalloc(&d_works.p, (size_t)threads * sizeof(Large)));
+        QM_CUDA(cudaMalloc(&d_results.p, (size_t)n_retry * GRID_SLOTS * sizeof(float)));
+        QM_CUDA(cudaMalloc(&d_rstatus.p, (size_t)n_retry * sizeof(uint32_t)));
+        QM_CUDA(cudaMemcpyAsync(d_sorted.p, list.data(), n_retry * sizeof(uint2), cudaMemcpyHostToDevice, stream));
+        QM_CUDA(cudaMemcpyAsync(d_cids.p, cids.data(), cids.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, stream));
+        QM_CUDA(cudaMemcpyAsync(d_cstart.p, cstart.data(), cstart.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, stream));
+        retry_paths_kernel<<<threads / 64, 64, 0, stream>>>(scene->dev, A, static_cast<uint2 *>(d_sorted.p), n_retry,
+                                                            static_cast<Large *>(d_works.p),
+                                                            static_cast<float *>(d_results.p),
+                                                            static_cast<uint32_t *>(d_rstatus.p));
+        QM_CUDA(cudaGetLastError());
+        fold_retry_kernel<<<(unsigned)((cids.size() + 127) / 128), 128, 0, stream>>>(
+            static_cast<uint32_t *>(d_cids.p), static_cast<uint32_t *>(d_cstart.p), (uint32_t)cids.size(),
+            static_cast<float *>(d_results.p), A.partial, A.n_chunks, cells);
+        QM_CUDA(cudaGetLastError());
+        std::vector<uint32_t> rstatus(n_retry);
+        QM_CUDA(cudaMemcpyAsync(rstatus.data(), d_rstatus.p, n_retry * sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
+        QM_CUDA(cudaStreamSynchronize(stream));
+        size_t still = 0;
+        for (uint32_t v : rstatus) still += v != 0;
+        if (still)
+            return fail(QM_ERR_CAPACITY, "qm_paint_grid: " + std::to_string(still) +
+                                             " paths exceed even the large per-path capacities");
+    }
     ReduceArgs R{};
     R.cells = cells;
-    R.n_chunks = A.n_chunks;
+    R.n_chunks = slices;
     R.partial = A.partial;
     R.level_min = g.level_min_db;
     R.bin_db = g.bin_db;
@@ -522,32 +589,28 @@ qm_status qm_paint_grid(qm_scene *scene, const qm_grid_desc *grid, float *cell_b
     R.cell_lden = static_cast<float *>(d_lden.p);
     R.histogram = static_cast<uint32_t *>(d_hist.p);
     size_t smem = histogram ? g.n_bins * sizeof(uint32_t) : 0;
-    if (smem > 200 * 1024) return fail(QM_ERR_ARGUMENT, "qm_paint_grid: n_bins above 51200");
     if (smem > 48 * 1024) QM_CUDA(cudaFuncSetAttribute(reduce_cells_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     reduce_cells_kernel<<<(cells + 255) / 256, 256, smem, stream>>>(R);
     QM_CUDA(cudaGetLastError());
-    unsigned long long counters[4];
-    std::vector<uint32_t> failed(cells);
+    QM_CUDA(cudaEventRecord(ev.e1, stream));
+    unsigned long long counters[6];
     QM_CUDA(cudaMemcpyAsync(counters, d_counters.p, sizeof(counters), cudaMemcpyDeviceToHost, stream));
-    QM_CUDA(cudaMemcpyAsync(failed.data(), d_failed.p, cells * sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
     if (cell_bands) QM_CUDA(cudaMemcpyAsync(cell_bands, d_bands.p, (size_t)cells * 8 * sizeof(float), cudaMemcpyDeviceToHost, stream));
     if (cell_dba) QM_CUDA(cudaMemcpyAsync(cell_dba, d_dbaout.p, (size_t)cells * sizeof(float), cudaMemcpyDeviceToHost, stream));
     if (cell_lden) QM_CUDA(cudaMemcpyAsync(cell_lden, d_lden.p, (size_t)cells * sizeof(float), cudaMemcpyDeviceToHost, stream));
     if (histogram) QM_CUDA(cudaMemcpyAsync(histogram, d_hist.p, g.n_bins * sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
     QM_CUDA(cudaStreamSynchronize(stream));
     float ms = 0.f;
-    QM_CUDA(cudaEventElapsedTime(&ms, e0, e1));
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
+    QM_CUDA(cudaEventElapsedTime(&ms, ev.e0, ev.e1));
     if (stats) {
         stats->paths = counters[0];
         stats->crossings = counters[1];
         stats->failed_paths = counters[3];
+        stats->edge_tests = counters[2];
+        stats->vertices = counters[4];
+        stats->candidates = counters[5];
         stats->kernel_ms = ms;
     }
-    if (counters[3] != 0)
-        return fail(QM_ERR_CAPACITY, "qm_paint_grid: " + std::to_string(counters[3]) +
-                                         " paths exceeded the per-path capacities");
     return QM_OK;
 }
 
@@ -644,6 +707,24 @@ qm_status qm_evaluate_pairs(qm_scene *scene, const double *receiver_xy, const fl
     else
         evaluate_pairs_kernel<CapsFlat><<<blocks, 128, 0, stream>>>(scene->dev, A);
     QM_CUDA(cudaGetLastError());
+    // Pairs over the per-path capacities again with large ones (global scratch work areas).
+    std::vector<uint32_t> status_host(n_pairs);
+    QM_CUDA(cudaMemcpyAsync(status_host.data(), d_status.p, n_pairs * sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
+    QM_CUDA(cudaStreamSynchronize(stream));
+    std::vector<uint32_t> again;
+    for (size_t i = 0; i < n_pairs; ++i)
+        if (status_host[i] & QM_FAILED_CAPACITY) again.push_back((uint32_t)i);
+    Scratch d_again, d_works;
+    if (!again.empty()) {
+        using Large = PathWork<CapsLarge::C, CapsLarge::K, CapsLarge::H>;
+        const uint32_t threads = std::min<uint32_t>(((uint32_t)again.size() + 63) / 64 * 64, 8192);
+        QM_CUDA(cudaMalloc(&d_again.p, again.size() * sizeof(uint32_t)));
+        QM_CUDA(cudaMalloc(&d_works.p, (size_t)threads * sizeof(Large)));
+        QM_CUDA(cudaMemcpyAsync(d_again.p, again.data(), again.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, stream));
+        retry_pairs_kernel<<<threads / 64, 64, 0, stream>>>(scene->dev, A, static_cast<uint32_t *>(d_again.p),
+                                                            (uint32_t)again.size(), static_cast<Large *>(d_works.p));
+        QM_CUDA(cudaGetLastError());
+    }
     point_bands_kernel<<<(unsigned)group_point.size(), 160, 0, stream>>>(
         static_cast<uint32_t *>(d_order.p), static_cast<uint32_t *>(d_gs.p), static_cast<uint32_t *>(d_gp.p),
         (uint32_t)group_point.size(), A.pair_bands, static_cast<float *>(d_w.p), static_cast<uint32_t *>(d_layer.p),

@@ -49,6 +49,7 @@ struct SceneDev {
     uint32_t n_sources;
     float fav[QM_PERIODS][QM_SECTORS];
     float alpha[QM_BANDS];
+    float air_per_m[QM_BANDS];  // alpha * ln(10) / 10 / 1000: the air's exponent per metre of slant
 };
 
 __device__ __forceinline__ int floor_div(int a, int b) {
@@ -74,7 +75,7 @@ struct XRec {
 __device__ __forceinline__ int sgn64(long long v) { return (v > 0) - (v < 0); }
 
 // Whether an edge hit enters or leaves its ring (crossings.rs:80-111); exact on lattice points.
-__device__ inline bool edge_bounds_roof(const SceneDev &S, long long sx, long long sy, long long dx, long long dy,
+__device__ __noinline__ bool edge_bounds_roof(const SceneDev &S, long long sx, long long sy, long long dx, long long dy,
                                         uint32_t edge, uint32_t first, uint32_t count) {
     auto side = [&](uint32_t index) {
         int2 v = S.vertices[index];
@@ -257,23 +258,32 @@ struct TV {
     float x, z, g;
 };
 
+// floor(n / d) for d > 0 from a float estimate corrected exactly (no 64-bit division).
+__device__ __forceinline__ long long floor_div_pos(long long n, long long d) {
+    long long q = (long long)floorf((float)n / (float)d);
+    while (q * d > n) --q;
+    while ((q + 1) * d <= n) ++q;
+    return q;
+}
+
 // The ground profile under a ray (popup/src/scene.rs:242-296 on one metric lattice): the source end,
 // a vertex wherever the ray crosses a DEM row or column line strictly inside, the receiver end.
-// Orders of crossing are decided exactly on integers; a tie takes the row line first.
+// Orders of crossing are decided exactly on integers (a tie takes the row line first); each line
+// vertex's node pair and fraction follow incrementally from exact rationals, without divisions.
 struct TerrainWalk {
-    long long sx, sy, dx, dy, adx, ady, ox, oy, sp;
-    long long next_col, next_row;  // line indices ahead
+    long long adx, ady, sp;
+    long long a_col, a_row;          // steps along x (y) from the source to the next column (row) line
+    long long next_col, next_row;    // line indices ahead
+    long long col_i, col_rem, col_den, col_inc;  // column vertex: node row j0 and remainder (in den units)
+    long long row_i, row_rem, row_den, row_inc;  // row vertex: node column i0 and remainder
     int col_step, row_step;
-    float length;
+    float length, inv_adx, inv_ady;
     bool dem;
     int stage;  // 0 start, 1 inner, 2 end, 3 done
     float2 start_zg, end_zg;
 
     __device__ void init(const SceneDev &S, int x0, int y0, int x1, int y1, float length_m) {
-        sx = x0;
-        sy = y0;
-        dx = (long long)x1 - x0;
-        dy = (long long)y1 - y0;
+        long long dx = (long long)x1 - x0, dy = (long long)y1 - y0;
         adx = dx >= 0 ? dx : -dx;
         ady = dy >= 0 ? dy : -dy;
         length = length_m;
@@ -281,17 +291,33 @@ struct TerrainWalk {
         stage = 0;
         start_zg = terrain_point(S, x0, y0);
         end_zg = terrain_point(S, x1, y1);
-        if (dem) {
-            ox = S.dem_ox;
-            oy = S.dem_oy;
-            sp = S.dem_sp;
-            long long rx = sx - ox, ry = sy - oy;
-            long long fc = floor_div64(rx, sp), fr = floor_div64(ry, sp);
-            bool on_col = fc * sp == rx, on_row = fr * sp == ry;
-            col_step = dx > 0 ? 1 : -1;
-            row_step = dy > 0 ? 1 : -1;
-            next_col = dx > 0 ? fc + 1 : (on_col ? fc - 1 : fc);
-            next_row = dy > 0 ? fr + 1 : (on_row ? fr - 1 : fr);
+        if (!dem) return;
+        sp = S.dem_sp;
+        long long rx = (long long)x0 - S.dem_ox, ry = (long long)y0 - S.dem_oy;
+        long long fc = floor_div64(rx, sp), fr = floor_div64(ry, sp);
+        bool on_col = fc * sp == rx, on_row = fr * sp == ry;
+        col_step = dx > 0 ? 1 : -1;
+        row_step = dy > 0 ? 1 : -1;
+        next_col = dx > 0 ? fc + 1 : (on_col ? fc - 1 : fc);
+        next_row = dy > 0 ? fr + 1 : (on_row ? fr - 1 : fr);
+        a_col = dx != 0 ? (next_col * sp - rx) * col_step : -1;
+        a_row = dy != 0 ? (next_row * sp - ry) * row_step : -1;
+        inv_adx = adx ? 1.0f / (float)adx : 0.0f;
+        inv_ady = ady ? 1.0f / (float)ady : 0.0f;
+        if (dy != 0) {
+            // x of the row line's vertex relative to the DEM origin, in units of sp: num / den.
+            long long num = (rx * dy + (next_row * sp - ry) * dx) * row_step;
+            row_den = ady * sp;
+            row_inc = sp * dx;  // per row step (both signs folded in)
+            row_i = floor_div64(num, row_den);
+            row_rem = num - row_i * row_den;
+        }
+        if (dx != 0) {
+            long long num = (ry * dx + (next_col * sp - rx) * dy) * col_step;
+            col_den = adx * sp;
+            col_inc = sp * dy;
+            col_i = floor_div64(num, col_den);
+            col_rem = num - col_i * col_den;
         }
     }
 
@@ -303,46 +329,32 @@ struct TerrainWalk {
             return true;
         }
         if (stage == 1) {
-            // Distances (in steps along each axis) to the next column and row lines.
-            long long a_col = dx != 0 ? (ox + next_col * sp - sx) * (dx > 0 ? 1 : -1) : -1;
-            long long a_row = dy != 0 ? (oy + next_row * sp - sy) * (dy > 0 ? 1 : -1) : -1;
-            bool col_ok = dx != 0 && a_col < adx;
-            bool row_ok = dy != 0 && a_row < ady;
+            bool col_ok = adx != 0 && a_col < adx;
+            bool row_ok = ady != 0 && a_row < ady;
             if (col_ok || row_ok) {
-                bool take_row;
-                if (!col_ok)
-                    take_row = true;
-                else if (!row_ok)
-                    take_row = false;
-                else
-                    take_row = a_row * adx <= a_col * ady;  // t_row <= t_col
+                bool take_row = !col_ok || (row_ok && a_row * adx <= a_col * ady);
                 if (take_row) {
-                    float t = (float)a_row / (float)ady;
-                    // x on row line j: (sx - ox) + (Y - sy) dx / dy, as num / den steps.
-                    long long Y = oy + next_row * sp;
-                    long long num = (sx - ox) * dy + (Y - sy) * dx, den = dy * sp;
-                    if (den < 0) {
-                        num = -num;
-                        den = -den;
-                    }
-                    long long i0 = floor_div64(num, den);
-                    float f = (float)(num - i0 * den) / (float)den;
-                    float2 a = dem_node(S, i0, next_row), b = dem_node(S, i0 + 1, next_row);
+                    float t = (float)a_row * inv_ady;
+                    float f = (float)row_rem / (float)row_den;
+                    float2 a = dem_node(S, row_i, next_row), b = dem_node(S, row_i + 1, next_row);
                     v = TV{t * length, a.x + f * (b.x - a.x), a.y + f * (b.y - a.y)};
                     next_row += row_step;
+                    a_row += sp;
+                    long long r = row_rem + row_inc;
+                    long long q = floor_div_pos(r, row_den);
+                    row_i += q;
+                    row_rem = r - q * row_den;
                 } else {
-                    float t = (float)a_col / (float)adx;
-                    long long X = ox + next_col * sp;
-                    long long num = (sy - oy) * dx + (X - sx) * dy, den = dx * sp;
-                    if (den < 0) {
-                        num = -num;
-                        den = -den;
-                    }
-                    long long j0 = floor_div64(num, den);
-                    float f = (float)(num - j0 * den) / (float)den;
-                    float2 a = dem_node(S, next_col, j0), b = dem_node(S, next_col, j0 + 1);
+                    float t = (float)a_col * inv_adx;
+                    float f = (float)col_rem / (float)col_den;
+                    float2 a = dem_node(S, next_col, col_i), b = dem_node(S, next_col, col_i + 1);
                     v = TV{t * length, a.x + f * (b.x - a.x), a.y + f * (b.y - a.y)};
                     next_col += col_step;
+                    a_col += sp;
+                    long long r = col_rem + col_inc;
+                    long long q = floor_div_pos(r, col_den);
+                    col_i += q;
+                    col_rem = r - q * col_den;
                 }
                 return true;
             }
@@ -362,6 +374,7 @@ struct TerrainWalk {
 
 struct Roof {
     float x0, x1, top0, top1, zt0, zt1, g0, g1;  // roof ends, tops, terrain and G at the ends
+    uint32_t fp;
 };
 
 struct BuildingHit {
@@ -394,6 +407,8 @@ struct PathResult {
     uint32_t status;
     uint32_t crossings;
     uint32_t edges_tested;
+    uint32_t vertices;    // profile vertices streamed (terrain and roofs)
+    uint32_t candidates;  // diffraction candidates fed to the bands
 };
 
 // One state's rubber band, built as the candidates stream in sorted order
@@ -507,7 +522,7 @@ struct Band {
 
 // boundary_for_candidates (diffraction.rs:64-197) from the band's result.
 template <int STATE, int CAP_H>
-__device__ void state_boundary(Band<STATE, CAP_H> &band, const EqGeometry &direct, float path_ground, float near_source,
+__device__ __noinline__ void state_boundary(Band<STATE, CAP_H> &band, const EqGeometry &direct, float path_ground, float near_source,
                                float source_gf, float z0, float g0, float L, float out[QM_BANDS]) {
     float whole[QM_BANDS];
     ground_attenuation_bands(direct, source_side_factors(STATE, path_ground, near_source), STATE, whole);
@@ -730,31 +745,29 @@ __device__ void evaluate_path(const SceneDev &S, const SourceDev &src, int rx, i
             w.tops[nt++] = PlanePoint{x, top};
         }
     }
-    // Roofs: hits sorted by (footprint, x), consecutive pairs per footprint (ray.rs:312-323).
-    for (int i = 1; i < nb; ++i) {
-        BuildingHit v = w.hits[i];
-        int j = i - 1;
-        while (j >= 0 && (w.hits[j].fp > v.fp || (w.hits[j].fp == v.fp && w.hits[j].x > v.x))) {
-            w.hits[j + 1] = w.hits[j];
-            --j;
-        }
-        w.hits[j + 1] = v;
-    }
+    // Roofs: each footprint's hits in order of x, paired consecutively (ray.rs:312-323). The hits
+    // already come in order of x, so a forward scan finds each one's partner; `hits[k].fp` is
+    // cleared once paired.
     int nr = 0;
-    for (int start = 0; start < nb;) {
-        int end = start;
-        while (end < nb && w.hits[end].fp == w.hits[start].fp) ++end;
-        for (int k = start; k + 1 < end; k += 2) {
-            const BuildingHit &a = w.hits[k], &b = w.hits[k + 1];
-            w.roofs[nr++] = Roof{a.x, b.x, a.top, b.top, a.zt, b.zt, a.g, b.g};
-        }
-        start = end;
+    for (int k = 0; k < nb; ++k) {
+        uint32_t fp = w.hits[k].fp;
+        if (fp == 0u) continue;
+        for (int j = k + 1; j < nb; ++j)
+            if (w.hits[j].fp == fp) {
+                const BuildingHit &a = w.hits[k], &b = w.hits[j];
+                w.roofs[nr++] = Roof{a.x, b.x, a.top, b.top, a.zt, b.zt, a.g, b.g, fp};
+                w.hits[j].fp = 0u;
+                break;
+            }
+        w.hits[k].fp = 0u;
     }
-    // clip_roofs_in_closing_order (ray.rs:389-404): sorted by (x1, x0), stable.
+    // clip_roofs_in_closing_order (ray.rs:389-404): sorted by (x1, x0), stable over roofs grouped by
+    // footprint, so equal keys keep footprint order.
     for (int i = 1; i < nr; ++i) {
         Roof v = w.roofs[i];
         int j = i - 1;
-        while (j >= 0 && (w.roofs[j].x1 > v.x1 || (w.roofs[j].x1 == v.x1 && w.roofs[j].x0 > v.x0))) {
+        while (j >= 0 && (w.roofs[j].x1 > v.x1 ||
+                          (w.roofs[j].x1 == v.x1 && (w.roofs[j].x0 > v.x0 || (w.roofs[j].x0 == v.x0 && w.roofs[j].fp > v.fp))))) {
             w.roofs[j + 1] = w.roofs[j];
             --j;
         }
@@ -833,7 +846,9 @@ __device__ void evaluate_path(const SceneDev &S, const SourceDev &src, int rx, i
         };
         TV vnext;
         bool have_next = next_vertex(vnext);
+        uint32_t n_vertices = 0, n_candidates = 0;
         auto consume = [&](const TV &v) {
+            ++n_vertices;
             add_stretch(total, 0.0f, z0, vprev.x, vprev.z, vprev.g, v.x, v.z, v.g);
             hom.consume(vprev, v);
             if (want_fav) fav.consume(vprev, v);
@@ -865,6 +880,7 @@ __device__ void evaluate_path(const SceneDev &S, const SourceDev &src, int rx, i
                 float f = (c.x - vprev.x) / (vnext.x - vprev.x);
                 consume(TV{c.x, vprev.z + f * (vnext.z - vprev.z), vprev.g + f * (vnext.g - vprev.g)});
             }
+            ++n_candidates;
             hom.candidate(c, total, z0, vprev.z, vprev.g);
             if (want_fav) fav.candidate(c, total, z0, vprev.z, vprev.g);
         }
@@ -872,6 +888,8 @@ __device__ void evaluate_path(const SceneDev &S, const SourceDev &src, int rx, i
             consume(vnext);
             have_next = next_vertex(vnext);
         }
+        out.vertices = n_vertices;
+        out.candidates = n_candidates;
     }
     // The direct path (diffraction.rs:44-61) and each state's boundary.
     MeanPlane dplane = plane_of(total, 0.0f, L, z0);

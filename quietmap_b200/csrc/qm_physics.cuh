@@ -168,8 +168,10 @@ __device__ __forceinline__ float favourable_floor_db(const EqGeometry &g, float 
 }
 
 // ground.rs:105-139
-__device__ __forceinline__ void ground_attenuation_bands(const EqGeometry &g, GroundFactors f, int state,
-                                                         float out[QM_BANDS]) {
+// Out of line: called three times per state; inlining each copy would crowd the instruction
+// cache the crossing walk needs.
+__device__ __noinline__ void ground_attenuation_bands(const EqGeometry &g, GroundFactors f, int state,
+                                                      float out[QM_BANDS]) {
     float dp = fmaxf(g.dp, 1e-6f);
     float zs = g.zs, zr = g.zr;
     float imp = fmaxf(f.impedance, 0.0f);
@@ -292,7 +294,7 @@ __device__ __forceinline__ double triangle_excess_d(PointD s, PointD o, PointD r
 
 // StateRay::path_difference (rubber_band.rs:257-301) in FP64: the diffraction path difference
 // cancels catastrophically near grazing, so delta alone is taken in double.
-__device__ inline double path_difference_d(int state, double radius, PointD from, const PlanePoint *points, int n,
+__device__ __noinline__ double path_difference_d(int state, double radius, PointD from, const PlanePoint *points, int n,
                                            PointD to) {
     if (n == 0) return 0.0;
     double chords = 0.0, arcs = 0.0;

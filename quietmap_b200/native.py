@@ -142,7 +142,9 @@ class DeviceScene:
                                    abi.ptr(lden, C.c_float), abi.ptr(hist, C.c_uint32) if histogram else None,
                                    C.byref(stats)), self.ctx.handle)
         return bands, dba, lden, hist, dict(paths=stats.paths, failed_paths=stats.failed_paths,
-                                             crossings=stats.crossings, kernel_ms=stats.kernel_ms)
+                                             crossings=stats.crossings, edge_tests=stats.edge_tests,
+                                             vertices=stats.vertices, candidates=stats.candidates,
+                                             kernel_ms=stats.kernel_ms)
 
     def evaluate_pairs(self, receiver_xy_m, receiver_height_m, own_footprint, point_of_receiver, source_of_pair,
                        receiver_of_pair, band_weight, n_points, point_bands=None):

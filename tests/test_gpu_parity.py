@@ -196,3 +196,34 @@ def test_level_histogram_counts_are_exact(ctx):
     counts = ctx.level_histogram(levels)
     ref = oracle.level_histogram(levels.astype(np.float64), -30.0, 0.1, 1800)
     np.testing.assert_array_equal(counts, ref)
+
+
+def _point_sources(stock, points_m, level_db=90.0, height_m=0.05):
+    from quietmap_b200 import abi
+    src = np.zeros(len(points_m), dtype=abi.SOURCE_DTYPE)
+    for k, p in enumerate(points_m):
+        x, y = stock.steps(p)
+        src[k]["x"], src[k]["y"] = x, y
+        src[k]["height_m"] = height_m
+        src[k]["ground_factor"] = -1.0
+        src[k]["energy"][:] = 10.0 ** (level_db / 10.0)
+    return src
+
+
+def test_over_capacity_paths_are_rerun_on_the_device(ctx):
+    """45 buildings in a row: rays along it cross 90 walls, beyond the flat kernel's per-path
+    capacity; those paths are re-run with large capacities and still match the oracle."""
+    stock = Stock(side_m=2400.0, offset_m=200.0)
+    for i in range(45):
+        stock.building(i + 1, 3.0 + (i % 7), [square(100.0 + 30.0 * i, 0.0, 5.0)])
+    sources = _point_sources(stock, [(40.0, 0.0), (40.0, 1.5), (45.0, -2.0), (60.0, 30.0)])
+    scene = stock.scene(sources=sources)
+    origin = stock.steps((1500.0, -12.0))
+    grid = scenes.Grid(origin=tuple(int(v) for v in origin), spacing=int(round(2.0 / stock.step_m)), nx=8, ny=12)
+    dev = ctx.scene(scene)
+    bands, dba, lden, hist, stats = dev.paint_grid(grid)
+    assert stats["failed_paths"] > 0, stats
+    ora = oracle.OracleScene(scene)
+    e, l, _ = ora.paint_grid(grid)
+    ref = _levels_db(e.sum(axis=1))
+    np.testing.assert_allclose(dba, ref, atol=TOL_DB)
