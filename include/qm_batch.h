@@ -198,6 +198,26 @@ qm_status qm_list_crossings(qm_scene *scene, const int32_t *from_xy, const int32
                             uint32_t cap, uint32_t *counts, uint32_t *edges, double *t,
                             uint32_t *flags, uint32_t *status);
 
+/* The grid painter for callers that cannot allocate device memory while they paint (an engine
+ * that owns every device allocation and cannot let a cudaMalloc synchronise its device, or a thread
+ * that may not allocate after set-up). It has no counterpart in the reference: it is
+ * `qm_paint_grid` with every intermediate buffer carved out of one static device array of
+ * QM_STATIC_SCRATCH_BYTES (64 MiB) that each GPU loading this library holds until exit, so its
+ * success path calls no cudaMalloc, cudaFree or other allocating routine. Limits: at most
+ * QM_STATIC_MAX_CELLS (65,536) cells and QM_STATIC_MAX_BINS (4,096) histogram bins, and the grid's
+ * partial sums must fit the array (rejected with QM_ERR_CAPACITY otherwise); paths over the
+ * per-path capacities are not re-run (QM_ERR_CAPACITY: use qm_paint_grid). cell_bands, cell_dba
+ * and cell_lden are required host outputs; stats->kernel_ms is -1 (not timed). The first call on a
+ * device looks up the array's device address with that device current, so make the first call
+ * before any stream capture. Every call reuses the one array: calls that overlap on the GPU (from
+ * two contexts on one device) race. */
+#define QM_STATIC_SCRATCH_BYTES (64u << 20)
+#define QM_STATIC_MAX_CELLS 65536
+#define QM_STATIC_MAX_BINS 4096
+qm_status qm_paint_grid_static(qm_scene *scene, const qm_grid_desc *grid,
+                               float *cell_bands, float *cell_dba, float *cell_lden,
+                               uint32_t *histogram, qm_paint_stats *stats);
+
 #ifdef __cplusplus
 }
 #endif

@@ -20,6 +20,8 @@
 #include "../../include/qm_batch.h"
 #include "qm_kernels.cuh"
 
+#include <climits>
+
 namespace qm {
 void launch_zwicker(const float *thirds, size_t n, float *sone, cudaStream_t stream);
 }  // namespace qm
@@ -822,6 +824,239 @@ qm_status qm_list_crossings(qm_scene *scene, const int32_t *from_xy, const int32
         QM_CUDA(cudaMemcpyAsync(flags, d_flags.p, m * sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
     }
     QM_CUDA(cudaStreamSynchronize(stream));
+    return QM_OK;
+}
+
+}  // extern "C"
+
+// =============================================================================================
+// The grid painter for callers that cannot allocate device memory.
+//
+// Some callers of this library cannot call cudaMalloc while they paint: an engine that hands the
+// GPU to this library between its own stream-ordered work and owns every device allocation (a
+// cudaMalloc there would synchronise the device and stall its other streams), or a host thread that
+// is not allowed to allocate once its set-up is over. For them `qm_paint_grid_static` paints a grid
+// with every intermediate buffer carved out of one file-scope device array of QM_STATIC_SCRATCH_BYTES,
+// which each GPU that loads this library holds until the process exits. Its success path calls no
+// cudaMalloc, cudaFree or other allocating routine, on the device or the host; the scene must have
+// been uploaded before (qm_scene_upload allocates).
+
+static __device__ __align__(256) unsigned char g_static_scratch[QM_STATIC_SCRATCH_BYTES];
+
+namespace {
+
+// The device address of g_static_scratch per device, taken once with that device current. In host
+// code the array's name is only a host-side stand-in, never a device address.
+std::mutex g_static_lock;
+void *g_static_ptr[64] = {nullptr};
+
+qm_status static_scratch(int device, unsigned char **out) {
+    if (device < 0 || device >= 64) return fail(QM_ERR_UNSUPPORTED, "qm_paint_grid_static: device ordinal above 63");
+    std::lock_guard<std::mutex> guard(g_static_lock);
+    if (!g_static_ptr[device]) {
+        void *ptr = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&ptr, g_static_scratch);
+        if (e != cudaSuccess || !ptr)
+            return fail(QM_ERR_CUDA, std::string("cuda: cudaGetSymbolAddress of the static scratch: ") +
+                                         cudaGetErrorString(e));
+        g_static_ptr[device] = ptr;
+    }
+    *out = static_cast<unsigned char *>(g_static_ptr[device]);
+    return QM_OK;
+}
+
+// Receiver altitude (ground + height) of every grid cell, and UINT_MAX as "no building yet".
+__global__ void static_receivers_kernel(SceneDev S, int ox, int oy, int spacing, int nx, int ny, float height,
+                                        float *alt, uint32_t *own) {
+    int cell = blockIdx.x * blockDim.x + threadIdx.x;
+    if (cell >= nx * ny) return;
+    float2 zg = terrain_point(S, ox + (cell % nx) * spacing, oy + (cell / nx) * spacing);
+    alt[cell] = zg.x + height;
+    own[cell] = 0xFFFFFFFFu;
+}
+
+// The building each grid receiver stands in: every closed ring tests the receivers in its box
+// (exact even-odd rule on lattice integers) and keeps the lowest dense footprint id, which is the
+// lowest footprint id (dense ids keep their order).
+__global__ void static_own_kernel(SceneDev S, uint32_t n_outlines, int ox, int oy, int spacing, int nx, int ny,
+                                  uint32_t *own) {
+    uint32_t o = blockIdx.x * blockDim.x + threadIdx.x;
+    if (o >= n_outlines) return;
+    OutlineDev ol = S.outlines[o];
+    if (!ol.building || ol.count < 4) return;
+    long long x0 = LLONG_MAX, x1 = LLONG_MIN, y0 = LLONG_MAX, y1 = LLONG_MIN;
+    for (uint32_t k = 0; k < ol.count; ++k) {
+        int2 v = S.vertices[ol.first + k];
+        x0 = min(x0, (long long)v.x);
+        x1 = max(x1, (long long)v.x);
+        y0 = min(y0, (long long)v.y);
+        y1 = max(y1, (long long)v.y);
+    }
+    long long i_lo = max(0LL, -floor_div64(-(x0 - ox), spacing)), i_hi = min((long long)nx - 1, floor_div64(x1 - ox, spacing));
+    long long j_lo = max(0LL, -floor_div64(-(y0 - oy), spacing)), j_hi = min((long long)ny - 1, floor_div64(y1 - oy, spacing));
+    for (long long j = j_lo; j <= j_hi; ++j)
+        for (long long i = i_lo; i <= i_hi; ++i) {
+            long long x = ox + i * spacing, y = oy + j * spacing;
+            bool inside = false;
+            for (uint32_t k = 0; k + 1 < ol.count; ++k) {
+                int2 a = S.vertices[ol.first + k], b = S.vertices[ol.first + k + 1];
+                if (((long long)a.y > y) != ((long long)b.y > y)) {
+                    long long lhs = (x - a.x) * ((long long)b.y - a.y), rhs = (y - a.y) * ((long long)b.x - a.x);
+                    if (b.y - a.y > 0 ? lhs < rhs : lhs > rhs) inside = !inside;
+                }
+            }
+            if (inside) atomicMin(own + j * nx + i, ol.fp);
+        }
+}
+
+__global__ void static_own_finish_kernel(uint32_t *own, int cells) {
+    int cell = blockIdx.x * blockDim.x + threadIdx.x;
+    if (cell < cells && own[cell] == 0xFFFFFFFFu) own[cell] = 0;
+}
+
+size_t align256(size_t v) { return (v + 255) & ~size_t(255); }
+
+}  // namespace
+
+extern "C" {
+
+qm_status qm_paint_grid_static(qm_scene *scene, const qm_grid_desc *grid, float *cell_bands, float *cell_dba,
+                               float *cell_lden, uint32_t *histogram, qm_paint_stats *stats) {
+    if (!scene || !grid) return fail(QM_ERR_ARGUMENT, "qm_paint_grid_static: null scene or grid");
+    const qm_grid_desc &g = *grid;
+    if (g.nx <= 0 || g.ny <= 0 || g.spacing <= 0)
+        return fail(QM_ERR_ARGUMENT, "qm_paint_grid_static: grid nx, ny or spacing");
+    if ((int64_t)g.nx * g.ny > QM_STATIC_MAX_CELLS)
+        return fail(QM_ERR_CAPACITY, "qm_paint_grid_static: more than 65536 cells do not fit the static scratch");
+    int64_t last_x = g.origin[0] + (int64_t)(g.nx - 1) * g.spacing, last_y = g.origin[1] + (int64_t)(g.ny - 1) * g.spacing;
+    if (g.origin[0] < 0 || g.origin[1] < 0 || last_x >= scene->extent[0] || last_y >= scene->extent[1])
+        return fail(QM_ERR_ARGUMENT, "qm_paint_grid_static: grid receivers outside the scene extent");
+    if (histogram && (g.n_bins == 0 || g.n_bins > QM_STATIC_MAX_BINS || !(g.bin_db > 0.0)))
+        return fail(QM_ERR_ARGUMENT, "qm_paint_grid_static: histogram needs 0 < n_bins <= 4096 and bin_db > 0");
+    if (!cell_bands || !cell_dba || !cell_lden)
+        return fail(QM_ERR_ARGUMENT, "qm_paint_grid_static: cell_bands, cell_dba and cell_lden are required");
+    uint32_t sb = g.source_begin, se = g.source_end;
+    if (se <= sb) {
+        sb = 0;
+        se = scene->n_sources;
+    }
+    if (se > scene->n_sources) return fail(QM_ERR_ARGUMENT, "qm_paint_grid_static: source range beyond the scene's sources");
+    qm_ctx *ctx = scene->ctx;
+    std::lock_guard<std::mutex> guard(ctx->lock);
+    QM_CUDA(cudaSetDevice(ctx->device));
+    unsigned char *base = nullptr;
+    qm_status st = static_scratch(ctx->device, &base);
+    if (st != QM_OK) return st;
+    cudaStream_t stream = ctx->stream;
+    const int cells = g.nx * g.ny;
+    const uint32_t n_src = se - sb;
+    // Fixed part of the scratch, then as many partial slices as fit (at most one per 16 CTAs a SM).
+    size_t off = 0;
+    auto carve = [&](size_t bytes) {
+        size_t at = off;
+        off = align256(off + bytes);
+        return base + at;
+    };
+    float *d_alt = reinterpret_cast<float *>(carve((size_t)cells * 4));
+    uint32_t *d_own = reinterpret_cast<uint32_t *>(carve((size_t)cells * 4));
+    uint32_t *d_failed = reinterpret_cast<uint32_t *>(carve((size_t)cells * 4));
+    float *d_dba = reinterpret_cast<float *>(carve((size_t)cells * 4));
+    float *d_bands = reinterpret_cast<float *>(carve((size_t)cells * 32));
+    float *d_dbaout = reinterpret_cast<float *>(carve((size_t)cells * 4));
+    float *d_lden = reinterpret_cast<float *>(carve((size_t)cells * 4));
+    uint32_t *d_hist = reinterpret_cast<uint32_t *>(carve((size_t)QM_STATIC_MAX_BINS * 4));
+    unsigned long long *d_counters = reinterpret_cast<unsigned long long *>(carve(6 * 8));
+    unsigned int *d_rcount = reinterpret_cast<unsigned int *>(carve(4));
+    uint2 *d_retry = reinterpret_cast<uint2 *>(carve(256 * sizeof(uint2)));
+    const size_t slice_bytes = (size_t)cells * GRID_SLOTS * sizeof(float);
+    if (off + 2 * slice_bytes > (size_t)QM_STATIC_SCRATCH_BYTES)
+        return fail(QM_ERR_CAPACITY, "qm_paint_grid_static: the grid does not fit the static scratch");
+    GridArgs A{};
+    A.origin_x = g.origin[0];
+    A.origin_y = g.origin[1];
+    A.spacing = g.spacing;
+    A.nx = g.nx;
+    A.ny = g.ny;
+    A.height_m = g.height_m;
+    A.source_begin = sb;
+    A.source_end = se;
+    A.tile_w = 16;
+    A.tile_h = 8;
+    A.want_fav = scene->any_favourable;
+    for (int p = 0; p < 3; ++p) A.lden_w[p] = (float)LDEN_W[p];
+    const int tiles = ((g.nx + A.tile_w - 1) / A.tile_w) * ((g.ny + A.tile_h - 1) / A.tile_h);
+    const uint32_t fit_chunks = (uint32_t)((QM_STATIC_SCRATCH_BYTES - off) / slice_bytes) - 1;
+    uint32_t n_chunks = std::max<uint32_t>(1, ((uint32_t)ctx->sm_count * 16 + tiles - 1) / tiles);
+    n_chunks = std::min<uint32_t>(n_chunks, std::max<uint32_t>(1, n_src / 32));
+    n_chunks = std::min<uint32_t>(n_chunks, fit_chunks);
+    A.chunk = std::max<uint32_t>(1, (n_src + n_chunks - 1) / n_chunks);
+    A.n_chunks = n_src == 0 ? 1 : (n_src + A.chunk - 1) / A.chunk;
+    const uint32_t slices = A.n_chunks + 1;
+    float *d_partial = reinterpret_cast<float *>(carve((size_t)slices * slice_bytes));
+    // The array keeps the last call's contents: clear what must start at zero.
+    QM_CUDA(cudaMemsetAsync(d_partial, 0, (size_t)slices * slice_bytes, stream));
+    QM_CUDA(cudaMemsetAsync(d_failed, 0, (size_t)cells * 4, stream));
+    QM_CUDA(cudaMemsetAsync(d_counters, 0, 6 * 8, stream));
+    QM_CUDA(cudaMemsetAsync(d_rcount, 0, 4, stream));
+    QM_CUDA(cudaMemsetAsync(d_hist, 0, (size_t)QM_STATIC_MAX_BINS * 4, stream));
+    static_receivers_kernel<<<(cells + 127) / 128, 128, 0, stream>>>(scene->dev, g.origin[0], g.origin[1], g.spacing,
+                                                                      g.nx, g.ny, g.height_m, d_alt, d_own);
+    const uint32_t n_outlines = (uint32_t)scene->outlines.size();
+    if (n_outlines)
+        static_own_kernel<<<(n_outlines + 127) / 128, 128, 0, stream>>>(scene->dev, n_outlines, g.origin[0],
+                                                                        g.origin[1], g.spacing, g.nx, g.ny, d_own);
+    static_own_finish_kernel<<<(cells + 127) / 128, 128, 0, stream>>>(d_own, cells);
+    QM_CUDA(cudaGetLastError());
+    A.rcv_alt = d_alt;
+    A.rcv_own = d_own;
+    A.partial = d_partial;
+    A.failed = d_failed;
+    A.counters = d_counters;
+    A.retry = d_retry;
+    A.retry_cap = 256;
+    A.retry_count = d_rcount;
+    if (n_src > 0) {
+        dim3 grid_dim(tiles, A.n_chunks);
+        if (terrain_caps(scene))
+            paint_grid_kernel<CapsTerrain><<<grid_dim, 128, 0, stream>>>(scene->dev, A);
+        else
+            paint_grid_kernel<CapsFlat><<<grid_dim, 128, 0, stream>>>(scene->dev, A);
+        QM_CUDA(cudaGetLastError());
+    }
+    ReduceArgs R{};
+    R.cells = cells;
+    R.n_chunks = slices;
+    R.partial = d_partial;
+    R.level_min = g.level_min_db;
+    R.bin_db = g.bin_db;
+    R.n_bins = histogram ? g.n_bins : 0;
+    R.dba_scratch = d_dba;
+    R.cell_bands = d_bands;
+    R.cell_dba = d_dbaout;
+    R.cell_lden = d_lden;
+    R.histogram = histogram ? d_hist : nullptr;
+    size_t smem = histogram ? g.n_bins * sizeof(uint32_t) : 0;
+    reduce_cells_kernel<<<(cells + 255) / 256, 256, smem, stream>>>(R);
+    QM_CUDA(cudaGetLastError());
+    unsigned long long counters[6];
+    QM_CUDA(cudaMemcpyAsync(counters, d_counters, sizeof(counters), cudaMemcpyDeviceToHost, stream));
+    QM_CUDA(cudaMemcpyAsync(cell_bands, d_bands, (size_t)cells * 32, cudaMemcpyDeviceToHost, stream));
+    QM_CUDA(cudaMemcpyAsync(cell_dba, d_dbaout, (size_t)cells * 4, cudaMemcpyDeviceToHost, stream));
+    QM_CUDA(cudaMemcpyAsync(cell_lden, d_lden, (size_t)cells * 4, cudaMemcpyDeviceToHost, stream));
+    if (histogram) QM_CUDA(cudaMemcpyAsync(histogram, d_hist, (size_t)g.n_bins * 4, cudaMemcpyDeviceToHost, stream));
+    QM_CUDA(cudaStreamSynchronize(stream));
+    if (stats) {
+        stats->paths = counters[0];
+        stats->crossings = counters[1];
+        stats->failed_paths = counters[3];
+        stats->edge_tests = counters[2];
+        stats->vertices = counters[4];
+        stats->candidates = counters[5];
+        stats->kernel_ms = -1.0;  // not timed: timing events are left out of this entry point
+    }
+    if (counters[3] != 0)
+        return fail(QM_ERR_CAPACITY, "qm_paint_grid_static: paths exceeded the per-path capacities; their re-run "
+                                     "needs device allocations, use qm_paint_grid");
     return QM_OK;
 }
 
