@@ -1659,6 +1659,43 @@ void qmo_paint_grid(void *scene, const qm_grid_desc *grid, uint32_t cell_begin, 
     }
 }
 
+// Work counts of one pair (for sizing device buffers): crossings, profile vertices, candidates,
+// blocking candidates and hull points per state. out[7].
+void qmo_path_counts(void *scene, const int64_t from[2], const int64_t to[2], double *out) {
+    const Scene &s = *static_cast<Scene *>(scene);
+    Worker w;
+    fill_profile(s, from, to, w.profile);
+    scene_crossings(s, from, to, w.crossings);
+    RayEnds ends{0.05, false, 0.0, 0.0, false, 0.0, 0.0, 0};
+    double z, g;
+    terrain_at_point(s, to[0], to[1], z, g);
+    ends.receiver_altitude_m = z + 4.0;
+    fill_path(w.ray.pb, w.profile, w.crossings, ends);
+    const PathBuffers &pb = w.ray.pb;
+    VPath path;
+    path.profile = VProfile{pb.d.data(), pb.z.data(), pb.g.data(), pb.d.size()};
+    double length = pb.d.back();
+    path.source = PP{0.0, w.profile.ground_m[0] + 0.05};
+    path.receiver = PP{length, ends.receiver_altitude_m};
+    path.source_ground_factor = w.profile.ground_factor[0];
+    path.terrain = pb.crests.data();
+    path.n_terrain = pb.crests.size();
+    path.tops = pb.tops.data();
+    path.n_tops = pb.tops.size();
+    PathScratch ps;
+    collect_candidates(path, ps.candidates);
+    out[0] = (double)w.crossings.size();
+    out[1] = (double)pb.d.size();
+    out[2] = (double)ps.candidates.size();
+    for (int st = 0; st < 2; ++st) {
+        StateRay ray = StateRay::between(st, path.source, path.receiver);
+        bool blocked;
+        diffraction_path(ray, path.source, path.receiver, ps.candidates, ps.blocking, ps.hull, ps.points, blocked);
+        out[3 + 2 * st] = (double)ps.blocking.size();
+        out[4 + 2 * st] = blocked ? (double)ps.points.size() : 0.0;
+    }
+}
+
 double qmo_zwicker(const double *levels28) { return zwicker_loudness_sone(levels28); }
 
 void qmo_zwicker_many(const double *levels, size_t n, double *sone, int threads) {

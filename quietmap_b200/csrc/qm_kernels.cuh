@@ -21,7 +21,7 @@ struct KSum {
 
 // Path capacities per workload kind: crossings, crests, hull points per state.
 struct CapsFlat {
-    static constexpr int C = 64, K = 2, H = 24;
+    static constexpr int C = 96, K = 2, H = 24;
 };
 struct CapsTerrain {
     static constexpr int C = 256, K = 512, H = 64;
@@ -380,7 +380,7 @@ __global__ void __launch_bounds__(128) list_crossings_kernel(SceneDev S, const i
     for (int j = 0; j < k && j < (int)cap; ++j) {
         edges[i * cap + j] = xs[j].edge;
         t[i * cap + j] = xs[j].t;
-        flags[i * cap + j] = xs[j].flags;
+        flags[i * cap + j] = ((xs[j].info & X_BUILDING) ? 1u : 0u) | ((xs[j].info & X_BOUNDS) ? 2u : 0u);
     }
 }
 

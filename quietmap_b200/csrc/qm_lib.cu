@@ -19,6 +19,7 @@
 
 #include "../../include/qm_batch.h"
 #include "qm_kernels.cuh"
+#include "qm_warp.cuh"
 
 #include <climits>
 
@@ -436,6 +437,11 @@ void grid_receivers(const qm_scene *s, const qm_grid_desc *g, std::vector<float>
 
 bool terrain_caps(const qm_scene *s) { return s->dem_nx != 0; }
 
+#ifndef QM_WARP_PATHS_FOR_TERRAIN
+#define QM_WARP_PATHS_FOR_TERRAIN 0
+#endif
+bool use_warp_paths(const qm_scene *s) { return QM_WARP_PATHS_FOR_TERRAIN && s->dem_nx != 0; }
+
 }  // namespace
 
 extern "C" {
@@ -478,7 +484,10 @@ qm_status qm_paint_grid(qm_scene *scene, const qm_grid_desc *grid, float *cell_b
     A.tile_h = 8;
     A.want_fav = scene->any_favourable;
     for (int p = 0; p < 3; ++p) A.lden_w[p] = (float)LDEN_W[p];
-    const int tiles = ((g.nx + A.tile_w - 1) / A.tile_w) * ((g.ny + A.tile_h - 1) / A.tile_h);
+    // Terrain scenes (long rays over a DEM) run one warp per path; flat scenes one thread per path.
+    const bool warp_paths = use_warp_paths(scene);
+    const int tiles = warp_paths ? (cells + 3) / 4
+                                 : ((g.nx + A.tile_w - 1) / A.tile_w) * ((g.ny + A.tile_h - 1) / A.tile_h);
     const uint32_t n_src = se - sb;
     uint32_t want_ctas = (uint32_t)ctx->sm_count * 16;
     uint32_t n_chunks = std::max<uint32_t>(1, (want_ctas + tiles - 1) / tiles);
@@ -517,10 +526,15 @@ qm_status qm_paint_grid(qm_scene *scene, const qm_grid_desc *grid, float *cell_b
     QM_CUDA(cudaEventRecord(ev.e0, stream));
     if (n_src > 0) {
         dim3 grid_dim(tiles, A.n_chunks);
-        if (terrain_caps(scene))
+        if (warp_paths) {
+            const int smem = 4 * (int)sizeof(WarpShared);
+            QM_CUDA(cudaFuncSetAttribute(paint_grid_warp_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+            paint_grid_warp_kernel<<<grid_dim, 128, smem, stream>>>(scene->dev, A);
+        } else if (terrain_caps(scene)) {
             paint_grid_kernel<CapsTerrain><<<grid_dim, 128, 0, stream>>>(scene->dev, A);
-        else
+        } else {
             paint_grid_kernel<CapsFlat><<<grid_dim, 128, 0, stream>>>(scene->dev, A);
+        }
         QM_CUDA(cudaGetLastError());
     }
     unsigned int n_retry = 0;

@@ -64,13 +64,16 @@ __device__ __forceinline__ long long floor_div64(long long a, long long b) {
 // ---------------------------------------------------------------------------------------------
 // Crossings
 
+// One crossing: chainage, crossed edge (its first vertex) and the outline index with flags
+// (bit 30 building, bit 31 bounds_roof); footprint and height are read from the outline.
 struct XRec {
     double t;
-    uint32_t fp;
     uint32_t edge;
-    float height;
-    uint32_t flags;  // bit0 building, bit1 bounds_roof
+    uint32_t info;
 };
+constexpr uint32_t X_OUTLINE = 0x3fffffffu, X_BUILDING = 0x40000000u, X_BOUNDS = 0x80000000u;
+
+__device__ __forceinline__ uint32_t xrec_fp(const SceneDev &S, const XRec &r) { return S.outlines[r.info & X_OUTLINE].fp; }
 
 __device__ __forceinline__ int sgn64(long long v) { return (v > 0) - (v < 0); }
 
@@ -136,28 +139,15 @@ __device__ int list_crossings(const SceneDev &S, int sx, int sy, int rx, int ry,
                     un = -un;
                 }
                 if (!(tn > 0 && tn < d && un >= 0 && un <= d)) continue;
-                uint2 ref = __ldg(S.cell_ref + k);
-                bool dup = false;
-                for (int i = 0; i < n; ++i)
-                    if (xs[i].edge == ref.x) {
-                        dup = true;
-                        break;
-                    }
-                if (dup) continue;
                 if (n >= MAXC) {
                     status |= FAILED_CAPACITY;
                     return n;
                 }
+                uint2 ref = __ldg(S.cell_ref + k);
                 OutlineDev o = S.outlines[ref.y];
-                XRec r;
-                r.t = (double)tn / (double)d;
-                r.fp = o.fp;
-                r.edge = ref.x;
-                r.height = o.height;
                 bool building = o.building != 0;
                 bool bounds = building && edge_bounds_roof(S, sx, sy, dx, dy, ref.x, o.first, o.count);
-                r.flags = (building ? 1u : 0u) | (bounds ? 2u : 0u);
-                xs[n++] = r;
+                xs[n++] = XRec{(double)tn / (double)d, ref.x, ref.y | (building ? X_BUILDING : 0u) | (bounds ? X_BOUNDS : 0u)};
             }
         }
         if (cx == lx && cy == ly) break;
@@ -180,27 +170,40 @@ __device__ int list_crossings(const SceneDev &S, int sx, int sy, int rx, int ry,
             by += (long long)sty * C;
         }
     }
-    // Sort by (t, footprint, edge).
+    // Sort by (t, footprint, edge): the walk's cells come in order, so the list is nearly sorted; an
+    // edge listed in several cells appears once per visited cell, its copies side by side after.
     for (int i = 1; i < n; ++i) {
         XRec v = xs[i];
         int j = i - 1;
-        while (j >= 0 && (xs[j].t > v.t || (xs[j].t == v.t && (xs[j].fp > v.fp || (xs[j].fp == v.fp && xs[j].edge > v.edge))))) {
-            xs[j + 1] = xs[j];
+        while (j >= 0) {
+            const XRec &u = xs[j];
+            bool after = u.t > v.t;
+            if (!after && u.t == v.t) {
+                uint32_t fu = xrec_fp(S, u), fv = xrec_fp(S, v);
+                after = fu > fv || (fu == fv && u.edge > v.edge);
+            }
+            if (!after) break;
+            xs[j + 1] = u;
             --j;
         }
         xs[j + 1] = v;
     }
-    // One crossing per footprint and chainage within 1e-9 (crossings.rs:39-55).
+    // One crossing per footprint and chainage within 1e-9 (crossings.rs:39-55); copies of one edge
+    // (equal t and edge) are the common case of it.
     int kept = 0;
     for (int i = 0; i < n; ++i) {
         XRec c = xs[i];
+        if (kept > 0 && xs[kept - 1].edge == c.edge && xs[kept - 1].t == c.t) continue;
         bool merged = false;
-        for (int k = kept - 1; k >= 0; --k) {
-            if (!(c.t - xs[k].t < 1e-9)) break;
-            if (xs[k].fp == c.fp) {
-                xs[k].flags |= (c.flags & 2u);
-                merged = true;
-                break;
+        if (kept > 0 && c.t - xs[kept - 1].t < 1e-9) {
+            uint32_t fc = xrec_fp(S, c);
+            for (int k = kept - 1; k >= 0; --k) {
+                if (!(c.t - xs[k].t < 1e-9)) break;
+                if (xrec_fp(S, xs[k]) == fc) {
+                    xs[k].info |= (c.info & X_BOUNDS);
+                    merged = true;
+                    break;
+                }
             }
         }
         if (!merged) xs[kept++] = c;
@@ -209,7 +212,7 @@ __device__ int list_crossings(const SceneDev &S, int sx, int sy, int rx, int ry,
     if (rcv_own != 0) {
         int m = 0;
         for (int i = 0; i < kept; ++i)
-            if (xs[i].fp != rcv_own) xs[m++] = xs[i];
+            if (xrec_fp(S, xs[i]) != rcv_own) xs[m++] = xs[i];
         kept = m;
     }
     return kept;
@@ -418,6 +421,7 @@ template <int STATE, int CAP_H>
 struct Band {
     float radius;
     PlanePoint S, R;
+    float slope_sr;  // (R.z - S.z) / (R.x - S.x): the line of sight, taken once
     Sag sag_sr;
     HullEntry *h;
     int n;
@@ -436,6 +440,7 @@ struct Band {
         R = r;
         float dx = r.x - s.x, dz = r.z - s.z;
         radius = fmaxf(1000.0f, 8.0f * sqrtf(dx * dx + dz * dz));
+        slope_sr = dz / dx;
         if (STATE == QM_FAV) sag_sr = make_sag(radius, s, r);
         h = storage;
         h[0] = HullEntry{s.x, s.z, 0.0f, z0, g0, moments_zero()};
@@ -449,15 +454,24 @@ struct Band {
         failed = false;
     }
 
-    __device__ __forceinline__ void consume(const TV &a, const TV &b) { add_stretch(open, oox, ooz, a.x, a.z, a.g, b.x, b.z, b.g); }
+    // Adds the profile segment since the last event (moments about (sx0, sz0)) to the open segment.
+    __device__ __forceinline__ void fold(const Moments &seg, float sx0, float sz0) {
+        open = join(open, rebase(seg, sx0, sz0, oox, ooz));
+    }
 
     __device__ void push(float px, float pz, float oz, float og) {
         Moments seg = open;
         while (n >= 2) {
             const HullEntry &a = h[n - 2];
             const HullEntry &b = h[n - 1];
-            float ray_b = ray_altitude<STATE>(radius, PlanePoint{a.x, a.z}, PlanePoint{px, pz}, b.x);
-            if (b.z <= ray_b) {
+            bool under;
+            if (STATE == QM_HOM) {
+                // b on or under the chord a -> p, without the division (p.x > a.x).
+                under = (b.z - a.z) * (px - a.x) <= (pz - a.z) * (b.x - a.x);
+            } else {
+                under = b.z <= ray_altitude<STATE>(radius, PlanePoint{a.x, a.z}, PlanePoint{px, pz}, b.x);
+            }
+            if (under) {
                 seg = join(b.seg, rebase(seg, b.ox, b.oz, a.ox, a.oz));
                 --n;
             } else {
@@ -477,7 +491,7 @@ struct Band {
     // A candidate at x with the profile moments [0, x] about (0, z0) and the profile at x.
     __device__ void candidate(PlanePoint c, const Moments &total, float z0, float oz, float og) {
         if (failed) return;
-        float line = chord_altitude(S, R, c.x);
+        float line = S.z + slope_sr * (c.x - S.x);
         if (STATE == QM_FAV) line += sag_sr.at(c.x - S.x);
         if (c.z > line) {
             if (!blocked) {
@@ -724,8 +738,9 @@ __device__ void evaluate_path(const SceneDev &S, const SourceDev &src, int rx, i
     {
         uint32_t own = src.fp;
         for (int i = 0; i < nx; ++i) {
-            uint32_t fp = w.xs[i].fp;
-            bool bounds = (w.xs[i].flags & 2u) != 0;
+            const OutlineDev &o = S.outlines[w.xs[i].info & X_OUTLINE];
+            uint32_t fp = o.fp;
+            bool bounds = (w.xs[i].info & X_BOUNDS) != 0;
             if (own != 0) {
                 // containing_footprints (ray.rs:201-226): the own footprint and every footprint with an
                 // odd count of roof-bounding crossings.
@@ -733,14 +748,14 @@ __device__ void evaluate_path(const SceneDev &S, const SourceDev &src, int rx, i
                 if (!contained) {
                     int count = 0;
                     for (int k = 0; k < nx; ++k)
-                        if ((w.xs[k].flags & 2u) && w.xs[k].fp == fp) ++count;
+                        if ((w.xs[k].info & X_BOUNDS) && xrec_fp(S, w.xs[k]) == fp) ++count;
                     contained = (count & 1) != 0;
                 }
                 if (contained) continue;
             }
             float x = (float)w.xs[i].t * L;
             float zt = w.tops[i].x, g = w.tops[i].z;
-            float top = zt + w.xs[i].height;
+            float top = zt + o.height;
             if (bounds) w.hits[nb++] = BuildingHit{fp, x, top, zt, g};
             w.tops[nt++] = PlanePoint{x, top};
         }
@@ -847,12 +862,22 @@ __device__ void evaluate_path(const SceneDev &S, const SourceDev &src, int rx, i
         TV vnext;
         bool have_next = next_vertex(vnext);
         uint32_t n_vertices = 0, n_candidates = 0;
+        // The profile since the last candidate, about that candidate's place (seg_x, seg_z); folded
+        // into the total and into each band's open segment at the next candidate.
+        Moments seg = moments_zero();
+        float seg_x = 0.0f, seg_z = z0;
         auto consume = [&](const TV &v) {
             ++n_vertices;
-            add_stretch(total, 0.0f, z0, vprev.x, vprev.z, vprev.g, v.x, v.z, v.g);
-            hom.consume(vprev, v);
-            if (want_fav) fav.consume(vprev, v);
+            add_stretch(seg, seg_x, seg_z, vprev.x, vprev.z, vprev.g, v.x, v.z, v.g);
             vprev = v;
+        };
+        auto fold = [&]() {
+            total = join(total, rebase(seg, seg_x, seg_z, 0.0f, z0));
+            hom.fold(seg, seg_x, seg_z);
+            if (want_fav) fav.fold(seg, seg_x, seg_z);
+            seg = moments_zero();
+            seg_x = vprev.x;
+            seg_z = vprev.z;
         };
         int ik = 0, it = 0;
         for (;;) {
@@ -881,6 +906,7 @@ __device__ void evaluate_path(const SceneDev &S, const SourceDev &src, int rx, i
                 consume(TV{c.x, vprev.z + f * (vnext.z - vprev.z), vprev.g + f * (vnext.g - vprev.g)});
             }
             ++n_candidates;
+            fold();
             hom.candidate(c, total, z0, vprev.z, vprev.g);
             if (want_fav) fav.candidate(c, total, z0, vprev.z, vprev.g);
         }
@@ -888,6 +914,7 @@ __device__ void evaluate_path(const SceneDev &S, const SourceDev &src, int rx, i
             consume(vnext);
             have_next = next_vertex(vnext);
         }
+        fold();
         out.vertices = n_vertices;
         out.candidates = n_candidates;
     }

@@ -203,6 +203,26 @@ __device__ __noinline__ void ground_attenuation_bands(const EqGeometry &g, Groun
     }
 }
 
+// One band of ground_attenuation_bands (ground.rs:105-139), for a lane that owns that band.
+__device__ __noinline__ float ground_attenuation_band(const EqGeometry &g, GroundFactors f, int state, int b) {
+    float dp = fmaxf(g.dp, 1e-6f);
+    float zs = g.zs, zr = g.zr;
+    float imp = fmaxf(f.impedance, 0.0f);
+    float gw13 = imp > 0.0f ? __expf(1.3f * __logf(imp)) : 0.0f;
+    if (state == QM_HOM) {
+        if (f.path < HARD_GROUND_BELOW) return -3.0f;
+        return fmaxf(analytic_ground_db(b, dp, zs, zr, gw13), -3.0f * (1.0f - f.floor));
+    }
+    float floor = favourable_floor_db(g, f.floor);
+    if (f.path < HARD_GROUND_BELOW) return floor;
+    float height_sum = fmaxf(zs + zr, MINIMUM_HEIGHT_SUM);
+    float curvature = FAVOURABLE_CURVATURE_A0 * dp * dp * 0.5f;
+    float terrain = FAVOURABLE_TERRAIN_COEFF * dp / height_sum;
+    float rs = zs / height_sum, rr = zr / height_sum;
+    return fmaxf(analytic_ground_db(b, dp, zs + curvature * rs * rs + terrain, zr + curvature * rr * rr + terrain, gw13),
+                 floor);
+}
+
 // diffraction.rs:200-213
 __device__ __forceinline__ GroundFactors source_side_factors(int state, float path_ground, float near_source) {
     return GroundFactors{path_ground, state == QM_HOM ? near_source : path_ground, near_source};
