@@ -66,6 +66,19 @@ def lib():
         L.qmo_level_histogram.argtypes = [_D, C.c_size_t, C.c_double, C.c_double, C.c_uint32, _U32]
         L.qmo_level_bin.argtypes = [C.c_double, C.c_double, C.c_double, C.c_uint32]
         L.qmo_level_bin.restype = C.c_uint32
+        for name in ("qmo_lateral_attenuation_db", "qmo_speed_correction_db"):
+            getattr(L, name).argtypes = [C.c_double, C.c_double]
+            getattr(L, name).restype = C.c_double
+        L.qmo_finite_segment_energy_fraction.argtypes = [C.c_double, C.c_double, C.c_double]
+        L.qmo_finite_segment_energy_fraction.restype = C.c_double
+        L.qmo_installation_energy_gain.argtypes = [C.c_uint32, C.c_double, C.c_double]
+        L.qmo_installation_energy_gain.restype = C.c_double
+        L.qmo_npd_level.argtypes = [_D, C.c_double, C.c_double]
+        L.qmo_npd_level.restype = C.c_double
+        L.qmo_tail_absorption.argtypes = [_D]
+        L.qmo_tail_absorption.restype = C.c_double
+        L.qmo_flight_grid.argtypes = [C.c_void_p, C.c_uint32, C.c_void_p, C.c_size_t, C.POINTER(abi.FlightGridDesc),
+                                      C.c_uint32, C.c_uint32, _D, _D, _D, C.c_int]
         _lib = L
     return _lib
 
@@ -240,3 +253,45 @@ def level_histogram(levels, level_min, bin_db, n_bins):
 
 def level_bin(level, level_min, bin_db, n_bins):
     return lib().qmo_level_bin(level, level_min, bin_db, n_bins)
+
+
+# ---------------------------------------------------------------------------------------------
+# Doc 29 (physics/src/doc29/{npd,corrections,segment}.rs)
+
+def lateral_attenuation_db(height_m, lateral_m):
+    return lib().qmo_lateral_attenuation_db(height_m, lateral_m)
+
+
+def speed_correction_db(v_ref_kt, speed_kt):
+    return lib().qmo_speed_correction_db(v_ref_kt, speed_kt)
+
+
+def finite_segment_energy_fraction(along_m, length_m, scaled_m):
+    return lib().qmo_finite_segment_energy_fraction(along_m, length_m, scaled_m)
+
+
+def installation_energy_gain(installation, height_m, slant_m):
+    return lib().qmo_installation_energy_gain(installation, height_m, slant_m)
+
+
+def npd_level(curve10, slant_m, tail_alpha):
+    c = _d(curve10)
+    return lib().qmo_npd_level(abi.ptr(c, C.c_double), slant_m, tail_alpha)
+
+
+def tail_absorption(sel10):
+    c = _d(sel10)
+    return lib().qmo_tail_absorption(abi.ptr(c, C.c_double))
+
+
+def flight_grid(flights, cell_begin=0, cell_end=0, grid=None, nthreads=None):
+    """Per cell of [cell_begin, cell_end): (LAE [n], thirds [n][28], sone [n])."""
+    g = abi.flight_grid_desc(grid or flights.grid)
+    n = (cell_end - cell_begin) if cell_end > cell_begin else g.nx * g.ny
+    types = np.ascontiguousarray(flights.types, dtype=abi.AIRCRAFT_TYPE_DTYPE)
+    segs = np.ascontiguousarray(flights.segments, dtype=abi.FLIGHT_SEGMENT_DTYPE)
+    lae, thirds, sone = np.zeros(n), np.zeros((n, 28)), np.zeros(n)
+    lib().qmo_flight_grid(types.ctypes.data, len(types), segs.ctypes.data, len(segs), C.byref(g), cell_begin,
+                          cell_end, abi.ptr(lae, C.c_double), abi.ptr(thirds, C.c_double), abi.ptr(sone, C.c_double),
+                          nthreads or threads())
+    return lae, thirds, sone

@@ -116,6 +116,40 @@ SOURCE_DTYPE = np.dtype(
      ("exclusion_radius_m", "<f4"), ("platform_half_width_m", "<f4"), ("footprint_id", "<u8"),
      ("layer", "<u4"), ("pad_", "<u4"), ("energy", "<f4", (PERIODS, BANDS))], align=True)
 
+AIRCRAFT_TYPE_DTYPE = np.dtype(
+    [("sel_db", "<f4", (2, 10, 10)), ("lamax_db", "<f4", (2, 10, 10)), ("v_ref_kt", "<f4"), ("installation", "<u4"),
+     ("spectrum_db", "<f4", (THIRDS,)), ("pad_", "<u4", (2,))], align=True)
+FLIGHT_SEGMENT_DTYPE = np.dtype(
+    [("start", "<f4", (3,)), ("end", "<f4", (3,)), ("power", "<f4"), ("speed_mps", "<f4"), ("type", "<u4"),
+     ("departure", "<u4"), ("flight", "<u4"), ("pad_", "<u4")], align=True)
+
+
+class FlightGridDesc(C.Structure):
+    _fields_ = [
+        ("origin_m", C.c_double * 2),
+        ("spacing_m", C.c_double),
+        ("nx", C.c_int32),
+        ("ny", C.c_int32),
+        ("receiver_height_m", C.c_float),
+        ("pad_", C.c_float),
+        ("reach_m", C.c_double),
+        ("duration_s", C.c_double),
+    ]
+
+
+def flight_grid_desc(grid):
+    g = FlightGridDesc()
+    g.origin_m[0], g.origin_m[1] = grid["origin_m"]
+    g.spacing_m = grid["spacing_m"]
+    g.nx, g.ny = grid["nx"], grid["ny"]
+    g.receiver_height_m = grid["receiver_height_m"]
+    g.reach_m = grid["reach_m"]
+    g.duration_s = grid["duration_s"]
+    return g
+
+
+assert AIRCRAFT_TYPE_DTYPE.itemsize == 4 * (200 + 200 + 2 + 28 + 2)
+assert FLIGHT_SEGMENT_DTYPE.itemsize == 48
 assert OUTLINE_DTYPE.itemsize == C.sizeof(Outline)
 assert SOURCE_DTYPE.itemsize == C.sizeof(Source)
 

@@ -18,6 +18,7 @@
 #include <vector>
 
 #include "../../include/qm_batch.h"
+#include "qm_aircraft.cuh"
 #include "qm_kernels.cuh"
 #include "qm_warp.cuh"
 
@@ -1075,3 +1076,148 @@ qm_status qm_paint_grid_static(qm_scene *scene, const qm_grid_desc *grid, float 
 }
 
 }  // extern "C"
+
+// =============================================================================================
+// Doc 29 aircraft on a receiver grid (qm_aircraft.h).
+
+namespace {
+
+const double NPD_FT[10] = {200.0, 400.0, 630.0, 1000.0, 2000.0, 4000.0, 6300.0, 10000.0, 16000.0, 25000.0};
+const double A_THIRDS[28] = {-44.7, -39.4, -34.6, -30.2, -26.2, -22.5, -19.1, -16.1, -13.4, -10.9, -8.6, -6.6, -4.8, -3.2,
+                             -1.9,  -0.8,  0.0,   0.6,   1.0,   1.2,   1.3,   1.2,   1.0,   0.5,   -0.1, -1.1, -2.5, -4.3};
+
+// The tail's absorption of a SEL curve (npd.rs:169-186), in double on the host.
+double tail_alpha_of(const float *sel) {
+    double sx = 0, sy = 0, sxx = 0, sxy = 0;
+    for (int i = 0; i < 3; ++i) {
+        int k = 7 + i;
+        double d = NPD_FT[k] * 0.3048;
+        double y = sel[k] + 20.0 * std::log10(d / (25000.0 * 0.3048));
+        sx += d;
+        sy += y;
+        sxx += d * d;
+        sxy += d * y;
+    }
+    return std::max(-(3.0 * sxy - sx * sy) / (3.0 * sxx - sx * sx), 0.0);
+}
+
+}  // namespace
+
+extern "C" qm_status qm_flight_grid(qm_ctx *ctx, const qm_aircraft_type *types, uint32_t n_types,
+                                    const qm_flight_segment *segments, size_t n_segments,
+                                    const qm_flight_grid_desc *grid, float *lae_db, float *thirds_db, float *sone) {
+    if (!ctx || !grid) return fail(QM_ERR_ARGUMENT, "qm_flight_grid: null ctx or grid");
+    if (n_types == 0 || n_types > 48 || !types) return fail(QM_ERR_ARGUMENT, "qm_flight_grid: 1 to 48 aircraft types");
+    if (n_segments && !segments) return fail(QM_ERR_ARGUMENT, "qm_flight_grid: segments is null");
+    if (n_segments >= (1ull << 31)) return fail(QM_ERR_ARGUMENT, "qm_flight_grid: too many segments");
+    const qm_flight_grid_desc &g = *grid;
+    if (g.nx <= 0 || g.ny <= 0 || !(g.spacing_m > 0.0) || (int64_t)g.nx * g.ny > (int64_t(1) << 28) || !(g.duration_s > 0.0))
+        return fail(QM_ERR_ARGUMENT, "qm_flight_grid: grid nx, ny, spacing_m or duration_s");
+    uint32_t n_flights = 0, last_flight = 0;
+    for (size_t i = 0; i < n_segments; ++i) {
+        const qm_flight_segment &q = segments[i];
+        if (q.type >= n_types) return fail(QM_ERR_ARGUMENT, "qm_flight_grid: segment " + std::to_string(i) + " type");
+        if (!(q.power >= 0.0f && q.power <= 9.0f))
+            return fail(QM_ERR_ARGUMENT, "qm_flight_grid: segment " + std::to_string(i) + " power outside [0, 9]");
+        for (int k = 0; k < 3; ++k)
+            if (!std::isfinite(q.start[k]) || !std::isfinite(q.end[k]))
+                return fail(QM_ERR_ARGUMENT, "qm_flight_grid: segment " + std::to_string(i) + " ends");
+        if (i > 0 && q.flight < last_flight)
+            return fail(QM_ERR_ARGUMENT, "qm_flight_grid: segments not grouped by flight");
+        last_flight = q.flight;
+        n_flights = std::max(n_flights, q.flight + 1);
+    }
+    std::vector<AcRow> rows((size_t)n_types * 20);
+    std::vector<AcType> tv(n_types);
+    for (uint32_t t = 0; t < n_types; ++t) {
+        const qm_aircraft_type &a = types[t];
+        if (!(a.v_ref_kt > 0.0f) || a.installation > 2)
+            return fail(QM_ERR_ARGUMENT, "qm_flight_grid: type " + std::to_string(t) + " v_ref_kt or installation");
+        for (int op = 0; op < 2; ++op)
+            for (int r = 0; r < 10; ++r) {
+                AcRow &R = rows[(size_t)t * 20 + op * 10 + r];
+                bool placeholder = true;
+                for (int k = 0; k < 10; ++k) {
+                    R.sel[k] = a.sel_db[op][r][k];
+                    double sml = (double)a.sel_db[op][r][k] - (double)a.lamax_db[op][r][k];
+                    R.sml[k] = (float)sml;
+                    if (std::fabs(sml - 12.0) >= 1e-9) placeholder = false;
+                }
+                R.tail_alpha = (float)tail_alpha_of(a.sel_db[op][r]);
+                R.d0 = (float)(2.0 / 3.141592653589793 * a.v_ref_kt * 1852.0 / 3600.0);
+                R.dipole = placeholder ? 1u : 0u;
+                R.pad = 0;
+            }
+        tv[t].v_ref_kt = a.v_ref_kt;
+        tv[t].installation = a.installation;
+        double weighted = 0.0;
+        for (int b = 0; b < 28; ++b) weighted += std::pow(10.0, (a.spectrum_db[b] + A_THIRDS[b]) / 10.0);
+        for (int b = 0; b < 28; ++b) tv[t].share[b] = (float)(std::pow(10.0, a.spectrum_db[b] / 10.0) / weighted);
+    }
+    std::vector<float4> boxes(std::max<uint32_t>(n_flights, 1), make_float4(1e30f, 1e30f, -1e30f, -1e30f));
+    for (size_t i = 0; i < n_segments; ++i) {
+        const qm_flight_segment &q = segments[i];
+        float4 &b = boxes[q.flight];
+        b.x = std::min({b.x, q.start[0], q.end[0]});
+        b.y = std::min({b.y, q.start[1], q.end[1]});
+        b.z = std::max({b.z, q.start[0], q.end[0]});
+        b.w = std::max({b.w, q.start[1], q.end[1]});
+    }
+    std::lock_guard<std::mutex> guard(ctx->lock);
+    QM_CUDA(cudaSetDevice(ctx->device));
+    cudaStream_t stream = ctx->stream;
+    const size_t cells = (size_t)g.nx * g.ny;
+    Scratch d_segs, d_boxes, d_rows, d_types, d_lae, d_thirds, d_sone, d_error;
+    QM_CUDA(cudaMalloc(&d_segs.p, std::max<size_t>(n_segments, 1) * sizeof(qm_flight_segment)));
+    QM_CUDA(cudaMalloc(&d_boxes.p, boxes.size() * sizeof(float4)));
+    QM_CUDA(cudaMalloc(&d_rows.p, rows.size() * sizeof(AcRow)));
+    QM_CUDA(cudaMalloc(&d_types.p, tv.size() * sizeof(AcType)));
+    QM_CUDA(cudaMalloc(&d_lae.p, cells * sizeof(float)));
+    QM_CUDA(cudaMalloc(&d_thirds.p, cells * 28 * sizeof(float)));
+    QM_CUDA(cudaMalloc(&d_error.p, sizeof(unsigned)));
+    if (sone) QM_CUDA(cudaMalloc(&d_sone.p, cells * sizeof(float)));
+    if (n_segments)
+        QM_CUDA(cudaMemcpyAsync(d_segs.p, segments, n_segments * sizeof(qm_flight_segment), cudaMemcpyHostToDevice, stream));
+    QM_CUDA(cudaMemcpyAsync(d_boxes.p, boxes.data(), boxes.size() * sizeof(float4), cudaMemcpyHostToDevice, stream));
+    QM_CUDA(cudaMemcpyAsync(d_rows.p, rows.data(), rows.size() * sizeof(AcRow), cudaMemcpyHostToDevice, stream));
+    QM_CUDA(cudaMemcpyAsync(d_types.p, tv.data(), tv.size() * sizeof(AcType), cudaMemcpyHostToDevice, stream));
+    QM_CUDA(cudaMemsetAsync(d_error.p, 0, sizeof(unsigned), stream));
+    FlightGridArgs A{};
+    A.segs = static_cast<qm_flight_segment *>(d_segs.p);
+    A.n_segs = (uint32_t)n_segments;
+    A.boxes = static_cast<float4 *>(d_boxes.p);
+    A.rows = static_cast<AcRow *>(d_rows.p);
+    A.types = static_cast<AcType *>(d_types.p);
+    A.n_types = n_types;
+    A.ox = g.origin_m[0];
+    A.oy = g.origin_m[1];
+    A.spacing = g.spacing_m;
+    A.nx = g.nx;
+    A.ny = g.ny;
+    A.height = g.receiver_height_m;
+    A.reach2 = g.reach_m > 0.0 ? g.reach_m * g.reach_m : 0.0;
+    A.inv_duration = (float)(1.0 / g.duration_s);
+    A.lae = static_cast<float *>(d_lae.p);
+    A.thirds = static_cast<float *>(d_thirds.p);
+    A.error = static_cast<unsigned *>(d_error.p);
+    const size_t smem = 2 * AC_TILE * sizeof(qm_flight_segment) + 16 + (size_t)n_types * 20 * sizeof(AcRow) +
+                        n_types * sizeof(AcType) + (size_t)n_types * 2 * AC_THREADS * sizeof(float);
+    if (smem > 227 * 1024)
+        return fail(QM_ERR_UNSUPPORTED, "qm_flight_grid: " + std::to_string(n_types) + " types exceed shared memory");
+    QM_CUDA(cudaFuncSetAttribute(flight_grid_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    const unsigned blocks = (unsigned)(((g.nx + 15) / 16) * ((g.ny + 15) / 16));
+    flight_grid_kernel<<<blocks, AC_THREADS, smem, stream>>>(A);
+    QM_CUDA(cudaGetLastError());
+    if (sone) {
+        launch_zwicker(A.thirds, cells, static_cast<float *>(d_sone.p), stream);
+        QM_CUDA(cudaGetLastError());
+    }
+    unsigned error = 0;
+    QM_CUDA(cudaMemcpyAsync(&error, d_error.p, sizeof(unsigned), cudaMemcpyDeviceToHost, stream));
+    if (lae_db) QM_CUDA(cudaMemcpyAsync(lae_db, d_lae.p, cells * sizeof(float), cudaMemcpyDeviceToHost, stream));
+    if (thirds_db) QM_CUDA(cudaMemcpyAsync(thirds_db, d_thirds.p, cells * 28 * sizeof(float), cudaMemcpyDeviceToHost, stream));
+    if (sone) QM_CUDA(cudaMemcpyAsync(sone, d_sone.p, cells * sizeof(float), cudaMemcpyDeviceToHost, stream));
+    QM_CUDA(cudaStreamSynchronize(stream));
+    if (error) return fail(QM_ERR_TIMEOUT, "qm_flight_grid: a segment tile's copy did not arrive in time");
+    return QM_OK;
+}

@@ -59,6 +59,9 @@ def lib():
         L.qm_level_histogram.restype = C.c_int
         L.qm_list_crossings.argtypes = [C.c_void_p, _I32, _I32, C.c_size_t, C.c_uint32, _U32, _U32, _D, _U32, _U32]
         L.qm_list_crossings.restype = C.c_int
+        L.qm_flight_grid.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_size_t,
+                                     C.POINTER(abi.FlightGridDesc), _F, _F, _F]
+        L.qm_flight_grid.restype = C.c_int
         if L.qm_abi_version() != abi.ABI_VERSION:
             raise QmError(abi.QM_ERR_UNSUPPORTED, "library ABI version mismatch")
         _lib = L
@@ -98,6 +101,20 @@ class Context:
         _check(lib().qm_zwicker(self.handle, abi.ptr(thirds, C.c_float), len(thirds), abi.ptr(out, C.c_float)),
                self.handle)
         return out
+
+    def flight_grid(self, flights, grid=None, sone=True):
+        """Doc 29 flights over a receiver grid: (LAE [cells], thirds [cells][28], sone [cells])."""
+        g = abi.flight_grid_desc(grid or flights.grid)
+        cells = g.nx * g.ny
+        types = np.ascontiguousarray(flights.types, dtype=abi.AIRCRAFT_TYPE_DTYPE)
+        segs = np.ascontiguousarray(flights.segments, dtype=abi.FLIGHT_SEGMENT_DTYPE)
+        lae = np.zeros(cells, np.float32)
+        thirds = np.zeros((cells, abi.THIRDS), np.float32)
+        out_sone = np.zeros(cells, np.float32) if sone else None
+        _check(lib().qm_flight_grid(self.handle, types.ctypes.data, len(types), segs.ctypes.data, len(segs),
+                                    C.byref(g), abi.ptr(lae, C.c_float), abi.ptr(thirds, C.c_float),
+                                    abi.ptr(out_sone, C.c_float) if sone else None), self.handle)
+        return lae, thirds, out_sone
 
     def level_histogram(self, levels_db, level_min_db=-30.0, bin_db=0.1, n_bins=1800):
         levels = np.ascontiguousarray(levels_db, dtype=np.float32).ravel()

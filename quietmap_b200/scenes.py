@@ -293,3 +293,80 @@ def terrain_square(seed=2, scale=1.0, n_segments=20000, n_buildings=30000, side_
     spacing = int(round(side / receivers / step_m))
     grid = Grid(origin=(spacing // 2, spacing // 2), spacing=spacing, nx=receivers, ny=receivers)
     return scene, grid
+
+
+# ---------------------------------------------------------------------------------------------
+# Aircraft: Doc 29 flights over a receiver grid.
+
+NPD_DISTANCES_FT = np.array([200.0, 400.0, 630.0, 1000.0, 2000.0, 4000.0, 6300.0, 10000.0, 16000.0, 25000.0])
+
+
+@dataclass
+class FlightScene:
+    types: np.ndarray       # AIRCRAFT_TYPE_DTYPE
+    segments: np.ndarray    # FLIGHT_SEGMENT_DTYPE
+    grid: dict              # origin_m, spacing_m, nx, ny, receiver_height_m, reach_m, duration_s
+    epnl_db: np.ndarray = None  # [types][2][10][10] EPNL-like curves (the NPD's third metric)
+    la_db: np.ndarray = None    # [types][2][10][10] LA curves (the fourth)
+    info: dict = field(default_factory=dict)
+
+
+def flights_square(seed=3, n_flights=2000, segments_per_flight=50, n_types=10, receivers=1024, spacing_m=100.0,
+                   segment_m=1000.0, reach_m=25000.0):
+    """Doc 29 aircraft: `n_flights` 3D polyline tracks of `segments_per_flight` segments (departures
+    climbing from 0 to up to 3000 m, approaches descending, 70-250 m/s), `n_types` types with seeded
+    NPD tables (10 powers x 10 distances x 4 metrics, monotone: ~ -20 lg d - 0.005 dB/m) and 28-band
+    spectra, over `receivers`^2 cells at `spacing_m`."""
+    from . import abi
+    rng = np.random.default_rng(seed)
+    side = receivers * spacing_m
+    d_m = NPD_DISTANCES_FT * 0.3048
+    types = np.zeros(n_types, dtype=abi.AIRCRAFT_TYPE_DTYPE)
+    epnl = np.zeros((n_types, 2, 10, 10), np.float32)
+    la = np.zeros((n_types, 2, 10, 10), np.float32)
+    bands = np.arange(28)
+    for t in range(n_types):
+        base = rng.uniform(85.0, 100.0)
+        for op in range(2):
+            for r in range(10):
+                level0 = base + (1.4 * r if op == 1 else 0.8 * r) - (4.0 if op == 0 else 0.0)
+                sel = level0 - 20.0 * np.log10(d_m / d_m[0]) - 0.005 * (d_m - d_m[0]) + rng.normal(0, 0.15, 10)
+                sel = np.minimum.accumulate(sel)  # monotone decreasing in distance
+                duration = 6.0 + 3.0 * np.log10(d_m / d_m[0]) + rng.uniform(-0.5, 0.5)
+                types[t]["sel_db"][op, r] = sel
+                types[t]["lamax_db"][op, r] = sel - duration
+                epnl[t, op, r] = sel + 2.0
+                la[t, op, r] = sel - duration - 2.0
+        types[t]["v_ref_kt"] = rng.uniform(140.0, 180.0)
+        types[t]["installation"] = rng.integers(0, 3)
+        peak = rng.uniform(12.0, 18.0)
+        types[t]["spectrum_db"] = -0.35 * (bands - peak) ** 2 / 4.0 + rng.normal(0, 1.0, 28)
+    segs = np.zeros(n_flights * segments_per_flight, dtype=abi.FLIGHT_SEGMENT_DTYPE)
+    k = 0
+    for f in range(n_flights):
+        departure = int(rng.integers(0, 2))
+        ty = int(rng.integers(0, n_types))
+        p = rng.uniform(0.1 * side, 0.9 * side, 2)
+        heading = rng.uniform(0, 2 * np.pi)
+        top = rng.uniform(1500.0, 3000.0)
+        v0, v1 = (rng.uniform(70.0, 100.0), rng.uniform(180.0, 250.0))
+        z = 0.0 if departure else top
+        for s in range(segments_per_flight):
+            heading += rng.normal(0.0, 0.05)
+            q = p + segment_m * np.array([np.cos(heading), np.sin(heading)])
+            frac = (s + 1) / segments_per_flight
+            z1 = top * min(frac * 2.0, 1.0) if departure else top * max(1.0 - frac * 2.0, 0.0)
+            segs[k]["start"] = (p[0], p[1], z)
+            segs[k]["end"] = (q[0], q[1], z1)
+            power = (9.0 - 6.0 * frac) if departure else (2.0 + 1.0 * (1.0 - frac))
+            segs[k]["power"] = np.clip(power + rng.normal(0, 0.2), 0.0, 9.0)
+            segs[k]["speed_mps"] = v0 + (v1 - v0) * (frac if departure else 1.0 - frac)
+            segs[k]["type"] = ty
+            segs[k]["departure"] = departure
+            segs[k]["flight"] = f
+            p, z = q, z1
+            k += 1
+    grid = dict(origin_m=(spacing_m / 2, spacing_m / 2), spacing_m=spacing_m, nx=receivers, ny=receivers,
+                receiver_height_m=4.0, reach_m=reach_m, duration_s=86400.0)
+    return FlightScene(types=types, segments=segs, grid=grid, epnl_db=epnl, la_db=la,
+                       info=dict(seed=seed, flights=n_flights, types=n_types))
