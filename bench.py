@@ -1,11 +1,23 @@
 """Benchmark of the exact painter: receiver-source paths per second on one B200.
 
-Workload (default `terrain`): the 16 km^2 terrain square at full size (fBm DEM at 5 m posts, Voronoi
-ground factor, 20,000 road and rail segments as ~4.0 M one-metre point sources, 30,000 polygon
-buildings, favourable probability 0.5), painted for a seeded sample of receiver tiles of the
-2048 x 2048 grid against every source. A step paints one sample block of receivers.
+Workload (default `terrain`): the 16 km^2 terrain square at full size (2048 x 2048 receivers at
+1.953 m, fBm DEM at 5 m posts with +-40 m relief, Voronoi ground factor over 200 cells, 20,000 road
+and rail segments split into ~4.0 M one-metre point sources, 30,000 polygon buildings, favourable
+probability 0.5 per sector). Painting the whole square is ~10^13 paths, so a step paints one
+seeded 16 x 8 receiver tile of the grid against one eighth of the source list (~0.5 M sources,
+~64 M paths); eight consecutive steps paint a tile against every source. Workload `road` paints
+the whole 1 km road square (128 x 128 receivers x 77,354 point sources) per step. Workload
+`flights` paints the Doc 29 aircraft grid (1024^2 cells x 10^5 flight segments) with loudness.
 
-  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload terrain|road]
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload ...]
+
+`value` is paths per second of device time (CUDA events around the painting kernels, inputs
+resident); `e2e` is the same metric through the C ABI call with host buffers (receiver set-up,
+host-device copies and the read-back of the cell levels and histogram inside the timed region).
+L2 is flushed between steps (a 256 MB write). `roofline` rates the main painting kernel: the
+kernel is compute-bound, so its work is counted in FP32 operations from the per-path work counters
+the kernel returns (an operation model, below) against the nominal FP32 peak; `roofline_hbm`
+gives its algorithmic bytes against the measured HBM bandwidth with the DRAM traffic ncu saw.
 
 `--impl reference` times the reference's CPU path on the host cores instead: the reference is Rust
 and cannot be built on this image, so its FP64 restatement (oracle/) stands in for it, on all
@@ -17,6 +29,7 @@ tiles with no exchange) and rank 0 prints the JSON line with the max time over r
 import argparse
 import json
 import os
+import re
 import subprocess
 import sys
 import threading
@@ -28,7 +41,20 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "receiver–source paths/s at ≤0.1 dB vs FP64 oracle; surrogate vs exact, 1 B200"
-FP32_NOMINAL_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12
+SM_COUNT, FP32_LANES, MUFU_LANES = 148, 128, 16
+NOMINAL_SM_MHZ = 1965.0
+
+# Operation model of one path (FP32 operations; SFU operations apart), from the exact path code:
+#   a segment-edge test 12, a profile vertex (terrain lattice step or roof vertex: position,
+#   height, segment moments, ground share) 20, a crossing (chainage, height, roof pairing) 10, a
+#   diffraction candidate (hull test and push) 12, and per path the ground attenuation of two
+#   states x 8 bands x 40, air absorption 8, geometry 30 and the three period sums 3 x 8 x 4.
+#   Diffraction's own arithmetic (path differences in FP64, ~500 operations per diffracted
+#   state) is not counted, so the model is a lower bound of the work.
+OPS = dict(edge_test=12, vertex=20, crossing=10, candidate=12, path=2 * 8 * 40 + 8 + 30 + 3 * 8 * 4)
+# SFU operations per path: 5 per band and state (exp, sqrt, log10 of the ground term), 8 exp of
+# air absorption, 3 x 8 exp of the period energies.
+SFU_PER_PATH = 2 * 8 * 5 + 8 + 3 * 8
 
 
 def parse():
@@ -37,8 +63,8 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="terrain", choices=["terrain", "road"])
-    ap.add_argument("--receivers", type=int, default=0, help="receivers per step (0: workload default)")
+    ap.add_argument("--workload", default="terrain", choices=["terrain", "road", "flights"])
+    ap.add_argument("--slices", type=int, default=8, help="terrain: source-list slices (a step paints one)")
     ap.add_argument("--sources", type=int, default=0,
                     help="paint only the first N sources (a small case for profiling; 0: all)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -52,41 +78,39 @@ def dist_env():
     return rank, world, local
 
 
-def workload(name, rank, receivers):
+def workload(name, rank, slices, sources):
+    """The scene and a list of steps (each a list of grids painted in that step)."""
     from quietmap_b200 import scenes
     if name == "road":
         scene, full = scenes.road_square()
-        if not receivers:
-            desc = dict(workload="road square 1 km, 128x128 receivers x 77k point sources (flat, G=0.5, "
-                                 "homogeneous)", global_batch=full.cells)
-            return scene, [full], desc
-    else:
-        scene, full = scenes.terrain_square()
-    per_step = receivers or 256
+        n_src = min(sources, len(scene.sources)) if sources else len(scene.sources)
+        full.source_begin, full.source_end = 0, n_src
+        desc = dict(workload=f"road square 1 km: 128x128 receivers at 7.8125 m x {n_src} point sources from 400 "
+                             "road segments, 300 buildings, flat G=0.5, homogeneous, one whole grid per step")
+        return scene, [[full]], desc
+    scene, full = scenes.terrain_square()
+    n_all = len(scene.sources)
+    n_src = min(sources, n_all) if sources else n_all
+    slices = max(1, slices)
+    per = (n_src + slices - 1) // slices
     tile_w, tile_h = 16, 8
-    n_tiles = max(per_step // (tile_w * tile_h), 1)
     rng = np.random.default_rng(1000 + rank)
-    blocks = []
-    for _ in range(64):
-        tiles = []
-        for _ in range(n_tiles):
-            tx = int(rng.integers(0, full.nx // tile_w))
-            ty = int(rng.integers(0, full.ny // tile_h))
-            tiles.append((tx, ty))
-        blocks.append(tiles)
-    grids = []
-    for tiles in blocks:
-        # One grid per tile; a step paints all tiles of its block.
-        grids.append([scenes.Grid(origin=(full.origin[0] + tx * tile_w * full.spacing,
-                                          full.origin[1] + ty * tile_h * full.spacing),
-                                  spacing=full.spacing, nx=tile_w, ny=tile_h) for tx, ty in tiles])
-    if name == "road":
-        what = "road square 1 km (128^2 grid at 7.8125 m, flat G=0.5, homogeneous), 300 buildings"
-    else:
-        what = "terrain square 16 km^2 (2048^2 grid at 1.953 m), 30,000 buildings, fBm DEM"
-    desc = dict(workload=f"{what}: {n_tiles} seeded 16x8 receiver tiles per step x {len(scene.sources)} "
-                         f"point sources", global_batch=n_tiles * tile_w * tile_h)
-    return scene, grids, desc
+    steps = []
+    for t in range(8):
+        tx = int(rng.integers(0, full.nx // tile_w))
+        ty = int(rng.integers(0, full.ny // tile_h))
+        for s in range(slices):
+            b, e = s * per, min((s + 1) * per, n_src)
+            if b >= e:
+                continue
+            steps.append([scenes.Grid(origin=(full.origin[0] + tx * tile_w * full.spacing,
+                                              full.origin[1] + ty * tile_h * full.spacing),
+                                      spacing=full.spacing, nx=tile_w, ny=tile_h, source_begin=b, source_end=e)])
+    desc = dict(workload=f"terrain square 16 km^2 (2048^2 grid at 1.953 m, fBm DEM, 30,000 buildings, "
+                         f"{n_all} point sources from 20,000 road/rail segments, p=0.5): a step is one seeded "
+                         f"16x8 receiver tile x one 1/{slices} slice ({per} sources) of the source list",
+                scene_sources=n_all)
+    return scene, steps, desc
 
 
 class ClockSampler:
@@ -130,35 +154,78 @@ class ClockSampler:
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         reasons = sorted({names[k] for s in self.samples for k in range(4) if s[3 + k].lower() == "active"})
         return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": reasons}
+                "reasons": reasons, "samples": len(self.samples)}
 
 
-def cpu_baseline(scene, grid_list, seconds=12.0):
-    """The FP64 oracle on all host threads: paths/s on a bounded sample (one receiver of the first
-    tile against a prefix of the sources, grown until it takes about `seconds`)."""
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return json.load(f)
+    except (OSError, ValueError):
+        return {}
+
+
+def profile_figure(name, key):
+    """A figure (`key = value`) from a committed ncu summary under profiles/, or None."""
+    try:
+        with open(os.path.join(ROOT, "profiles", name)) as f:
+            for line in f:
+                m = re.match(rf"\s*[-*]?\s*`?{re.escape(key)}`?\s*=\s*([0-9.eE+-]+)", line)
+                if m:
+                    return float(m.group(1))
+    except OSError:
+        pass
+    return None
+
+
+def cpu_sample(scene, g0, seconds):
+    """Grows a sample (receivers of the first tile x a prefix of the sources) until the oracle
+    takes about `seconds` on all host threads; returns (receivers, sources)."""
     from oracle import oracle
     from quietmap_b200 import scenes
     ora = oracle.OracleScene(scene)
-    g0 = grid_list[0][0] if isinstance(grid_list[0], list) else grid_list[0]
     threads = oracle.threads()
-    n = 2000
+    k = max(1, min(threads, 16))
+    n = 500
     while True:
-        grid = scenes.Grid(origin=g0.origin, spacing=g0.spacing, nx=1, ny=1, source_begin=0,
+        grid = scenes.Grid(origin=g0.origin, spacing=g0.spacing, nx=k, ny=1, source_begin=0,
                            source_end=min(n, len(scene.sources)))
         t0 = time.perf_counter()
         ora.paint_grid(grid, nthreads=threads)
         dt = time.perf_counter() - t0
-        if dt > seconds / 4 or n >= len(scene.sources):
+        if dt > seconds / 3 or n >= len(scene.sources):
             break
-        n = min(int(n * max(2.0, seconds / 4 / max(dt, 1e-3))), len(scene.sources))
-    # Spread the sample over threads: several receivers of the tile, the same source prefix.
-    k = max(1, min(threads, 8))
+        n = min(int(n * max(2.0, seconds / 3 / max(dt, 1e-3))), len(scene.sources))
+    n = min(len(scene.sources), max(1, int(n * seconds / max(dt, 1e-3))))
+    return ora, k, n, threads
+
+
+def cpu_run(ora, g0, k, n, threads):
+    from quietmap_b200 import scenes
     grid = scenes.Grid(origin=g0.origin, spacing=g0.spacing, nx=k, ny=1, source_begin=0, source_end=n)
     t0 = time.perf_counter()
     ora.paint_grid(grid, nthreads=threads)
-    dt = time.perf_counter() - t0
+    return time.perf_counter() - t0
+
+
+def cpu_baseline(scene, steps, seconds=12.0):
+    """The FP64 oracle on all host threads: paths/s on a bounded sample of the workload."""
+    g0 = steps[0][0]
+    ora, k, n, threads = cpu_sample(scene, g0, seconds)
+    dt = cpu_run(ora, g0, k, n, threads)
     return dict(value=k * n / dt, unit="paths/s", cores=threads, kind="port",
-                sample=f"{k} receivers x first {n} point sources ({k * n} paths, {dt:.1f} s)")
+                sample=f"{k} receivers of the first tile x the first {n} point sources ({k * n} paths, "
+                       f"{dt:.1f} s)")
+
+
+def algorithmic_bytes(scene, grid, n_src):
+    """Bytes one painting launch must move at least: its source slice (128 B a record), the
+    outlines and vertices, the DEM (altitude and ground factor, 4 B each), and the partial sums it
+    writes (9 floats per cell and source chunk are bounded by the cell outputs: 36 B a cell)."""
+    b = n_src * 128 + scene.outlines.nbytes + scene.vertices.nbytes
+    if scene.dem_altitude is not None:
+        b += scene.dem_altitude.size * 8
+    return b + grid.nx * grid.ny * 36
 
 
 def main():
@@ -174,92 +241,159 @@ def main():
         tdist.init_process_group(backend, timeout=timedelta(seconds=600))
     if args.impl == "reference":
         return reference_arm(args, rank, world)
+    if args.workload == "flights":
+        return flights(args, rank, world, local)
     import torch
     from quietmap_b200 import native
-    scene, grids, desc = workload(args.workload, rank, args.receivers)
+    scene, steps, desc = workload(args.workload, rank, args.slices, args.sources)
     ctx = native.Context(local if world > 1 else 0)
     dev = ctx.scene(scene)
-    n_src = len(scene.sources)
+    torch.cuda.set_device(local if world > 1 else 0)
+    flush = torch.empty(64 << 20, dtype=torch.float32, device="cuda")  # 256 MB > 126 MB L2
 
-    if args.sources:
-        for block in grids:
-            for g in (block if isinstance(block, list) else [block]):
-                g.source_begin, g.source_end = 0, min(args.sources, n_src)
-        desc["workload"] += f" (first {min(args.sources, n_src)} sources only)"
+    work = dict(paths=0, edge_tests=0, vertices=0, candidates=0, crossings=0, failed_paths=0)
+    timing = dict(kernel_ms=0.0, paint_ms=0.0, wall_s=0.0, launches=0, paint_launches=0, alg_bytes=0)
 
     def step(i):
-        block = grids[i % len(grids)]
-        tiles = block if isinstance(block, list) else [block]
-        paths, kms, crossings = 0, 0.0, 0
-        for g in tiles:
+        for g in steps[i % len(steps)]:
+            flush.zero_()
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
             _, _, _, _, st = dev.paint_grid(g)
-            paths += st["paths"]
-            kms += st["kernel_ms"]
-            crossings += st["crossings"]
-            for k in ("edge_tests", "vertices", "candidates"):
+            timing["wall_s"] += time.perf_counter() - t0
+            timing["kernel_ms"] += st["kernel_ms"]
+            timing["paint_ms"] += st["paint_ms"]
+            timing["launches"] += 2 + (2 if st["failed_paths"] else 0)
+            timing["paint_launches"] += 1
+            timing["alg_bytes"] += algorithmic_bytes(scene, g, g.source_end - g.source_begin)
+            for k in work:
                 work[k] += st[k]
-        return paths, kms, crossings, len(tiles)
-
-    work = dict(edge_tests=0, vertices=0, candidates=0)
 
     for i in range(args.warmup):
         step(i)
-    work.update(edge_tests=0, vertices=0, candidates=0)
+    for d in (work, timing):
+        for k in d:
+            d[k] = 0
     if world > 1:
         torch.distributed.barrier()
     torch.cuda.synchronize()
-    total_paths, total_ms, total_cross, calls = 0, 0.0, 0, 0
     with ClockSampler(local) as clocks:
-        t0 = time.perf_counter()
         for i in range(args.steps):
-            p, k, c, n = step(args.warmup + i)
-            total_paths += p
-            total_ms += k
-            total_cross += c
-            calls += n
+            step(args.warmup + i)
         torch.cuda.synchronize()
-        wall = time.perf_counter() - t0
     if world > 1:
-        t = torch.tensor([total_ms, wall], dtype=torch.float64, device="cuda")
+        t = torch.tensor([timing["kernel_ms"], timing["wall_s"], timing["paint_ms"]], dtype=torch.float64,
+                         device="cuda")
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        total_ms, wall = float(t[0]), float(t[1])
-        tp = torch.tensor([total_paths], dtype=torch.float64, device="cuda")
+        timing["kernel_ms"], timing["wall_s"], timing["paint_ms"] = float(t[0]), float(t[1]), float(t[2])
+        tp = torch.tensor([work["paths"]], dtype=torch.float64, device="cuda")
         torch.distributed.all_reduce(tp)
         total_paths = int(tp[0])
+    else:
+        total_paths = work["paths"]
     if rank == 0:
-        value = total_paths / (total_ms / 1e3)
-        e2e = total_paths / wall
-        cells_per_call = grids[0][0].cells if isinstance(grids[0], list) else grids[0].cells
+        clk = clocks.summary()
+        peaks = measured_peaks()
+        cells_per_call = steps[0][0].cells
+        calls = sum(len(steps[(args.warmup + i) % len(steps)]) for i in range(args.steps))
+        paths = max(work["paths"], 1)
+        ops = (OPS["edge_test"] * work["edge_tests"] + OPS["vertex"] * work["vertices"]
+               + OPS["crossing"] * work["crossings"] + OPS["candidate"] * work["candidates"]
+               + OPS["path"] * work["paths"])
+        paint_s = timing["paint_ms"] / 1e3
+        fp32_peak = SM_COUNT * FP32_LANES * 2 * NOMINAL_SM_MHZ * 1e6 / 1e12
+        achieved = ops / paint_s / 1e12 if paint_s > 0 else None
+        sfu_peak = SM_COUNT * MUFU_LANES * NOMINAL_SM_MHZ * 1e6
+        caps = "terrain" if args.workload == "terrain" else "road"
+        traffic_per_path = profile_figure(f"paint_grid_kernel_{caps}.md", "dram_bytes_per_path")
+        hbm_peak = peaks.get("hbm_gbs")
+        alg_gbs = timing["alg_bytes"] / paint_s / 1e9 if paint_s > 0 else None
         line = {
             "metric": METRIC,
-            "value": value,
+            "value": total_paths / (timing["kernel_ms"] / 1e3),
             "unit": "paths/s",
             "n_gpus": world,
             "steps": args.steps,
             "warmup": args.warmup,
-            "ms_per_step": total_ms / args.steps,
+            "ms_per_step": timing["kernel_ms"] / args.steps,
             "higher_is_better": True,
             "scaling": "weak",
             "vs_baseline": None,
             "dtype": "f32 (f64 for path differences and crossing chainage)",
             "data": "synthetic (seeded generator of the workload's geometry)",
-            "config": dict(desc, sources=n_src, parallelism=f"replicas x{world}",
-                           l2="inputs larger than L2 (sources 511 MB resident)"),
-            "e2e": {"value": e2e, "unit": "paths/s",
-                    "h2d_bytes_per_step": calls * cells_per_call * 8 // args.steps if args.steps else 0,
-                    "d2h_bytes_per_step": calls * (cells_per_call * 40 + 1800 * 4) // args.steps if args.steps else 0},
-            "gpu_launches": calls * 2,
-            "clocks": clocks.summary(),
-            "per_path": dict(crossings=total_cross / max(total_paths, 1),
-                             **{k: v / max(total_paths, 1) for k, v in work.items()}),
+            "config": dict(desc, paths_per_step=work["paths"] // max(args.steps, 1),
+                           parallelism=f"replicas x{world}", l2="flushed between steps (256 MB write)"),
+            "e2e": {"value": total_paths / timing["wall_s"], "unit": "paths/s",
+                    "h2d_bytes_per_step": calls * cells_per_call * 8 // args.steps,
+                    "d2h_bytes_per_step": calls * (cells_per_call * 40 + 1800 * 4) // args.steps},
+            "gpu_launches": timing["launches"],
+            "clocks": clk,
+            "roofline": {
+                "kernel": f"paint_grid_kernel<Caps{caps.capitalize()}>",
+                "bound": "fp32",
+                "achieved": achieved,
+                "peak": fp32_peak,
+                "unit": "TFLOP/s",
+                "frac": achieved / fp32_peak if achieved else None,
+                "peak_source": "nominal FP32 (148 SMs x 128 lanes x 2 x 1965 MHz); the measured peaks file "
+                               "holds no FP32 figure",
+                "ops_per_path": ops / paths,
+                "sfu_frac": (SFU_PER_PATH * work["paths"] / paint_s / sfu_peak) if paint_s > 0 else None,
+                "traffic": traffic_per_path * work["paths"] / max(timing["paint_launches"], 1)
+                if traffic_per_path else None,
+                "launch_ms": timing["paint_ms"] / max(timing["paint_launches"], 1),
+            },
+            "roofline_hbm": {
+                "bound": "hbm",
+                "achieved": alg_gbs,
+                "peak": hbm_peak,
+                "unit": "GB/s",
+                "frac": alg_gbs / hbm_peak if (alg_gbs and hbm_peak) else None,
+                "peak_source": "measured" if hbm_peak else None,
+                "algorithmic_bytes_per_launch": timing["alg_bytes"] / max(timing["paint_launches"], 1),
+                "traffic": traffic_per_path * work["paths"] / max(timing["paint_launches"], 1)
+                if traffic_per_path else None,
+            },
+            "per_path": {k: work[k] / paths for k in ("crossings", "edge_tests", "vertices", "candidates")},
+            "failed_paths_rerun": work["failed_paths"],
         }
         if not args.no_cpu_baseline and world == 1:
-            line["cpu_baseline"] = cpu_baseline(scene, grids)
+            line["cpu_baseline"] = cpu_baseline(scene, steps)
         print(json.dumps(line), flush=True)
     dev.close()
     ctx.close()
     if world > 1:
         torch.distributed.destroy_process_group()
+
+
+def flights(args, rank, world, local):
+    """Doc 29 flights (1024^2 cells at 100 m x 2000 flights x 50 segments) with loudness."""
+    import torch
+    from quietmap_b200 import native, scenes
+    f = scenes.flights_square(seed=3 + rank)
+    ctx = native.Context(local if world > 1 else 0)
+    cells = f.grid["nx"] * f.grid["ny"]
+    for _ in range(args.warmup):
+        ctx.flight_grid(f)
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clocks:
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            ctx.flight_grid(f)
+        wall = time.perf_counter() - t0
+    if rank == 0:
+        pairs = cells * len(f.segments) * args.steps
+        print(json.dumps({
+            "metric": "Doc 29 cells/s (cell x flight-segment pairs with Zwicker loudness), 1 B200",
+            "value": cells * args.steps / wall, "unit": "cells/s", "pairs_per_s": pairs / wall,
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": wall * 1e3 / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded flights and NPD tables)",
+            "config": {"workload": "1024^2 cells at 100 m x 2000 flights x 50 segments, 10 types, reach 25 km, "
+                                   "timed through the C ABI call (host buffers in and out)"},
+            "clocks": clocks.summary(), "gpu_launches": 2 * args.steps,
+        }), flush=True)
+    ctx.close()
 
 
 def reference_arm(args, rank, world):
@@ -269,21 +403,20 @@ def reference_arm(args, rank, world):
             import torch.distributed as tdist
             tdist.destroy_process_group()
         return
-    scene, grids, desc = workload(args.workload, 0, args.receivers)
-    base = None
-    for _ in range(args.warmup):
-        pass
-    samples = []
-    for _ in range(max(args.steps, 1)):
-        base = cpu_baseline(scene, grids, seconds=8.0)
-        samples.append(base["value"])
+    workload_name = "terrain" if args.workload == "flights" else args.workload
+    scene, steps, desc = workload(workload_name, 0, args.slices, args.sources)
+    g0 = steps[0][0]
+    # Warm-up: the sample is sized here (untimed), then each timed step runs it once.
+    ora, k, n, threads = cpu_sample(scene, g0, seconds=8.0)
+    samples = [k * n / cpu_run(ora, g0, k, n, threads) for _ in range(max(args.steps, 1))]
     value = float(np.median(samples))
     line = {
         "metric": METRIC, "value": value, "unit": "paths/s", "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f64", "data": "synthetic (seeded generator of the workload's geometry)",
+        "warmup": args.warmup, "ms_per_step": k * n / value * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generator of the workload's geometry)",
         "config": dict(desc, parallelism="host threads"), "impl": "reference",
-        "cpu_baseline": dict(base, value=value),
+        "cpu_baseline": dict(value=value, unit="paths/s", cores=threads, kind="port",
+                             sample=f"{k} receivers of the first tile x the first {n} point sources per step"),
         "e2e": {"value": value, "unit": "paths/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)

@@ -25,7 +25,7 @@
 extern "C" {
 #endif
 
-#define QM_ABI_VERSION 1
+#define QM_ABI_VERSION 2
 
 #define QM_BANDS 8      /* octave bands 63 Hz .. 8 kHz (physics/src/bands.rs:4) */
 #define QM_PERIODS 3    /* day, evening, night (physics/src/bands.rs:14) */
@@ -130,6 +130,7 @@ typedef struct {
     uint64_t vertices;       /* vertical-profile vertices streamed (terrain and roofs) */
     uint64_t candidates;     /* diffraction candidates fed to the rubber bands */
     double kernel_ms;        /* device time of the painting kernels (paint, re-run, reduce) */
+    double paint_ms;         /* device time of the main painting kernel alone */
 } qm_paint_stats;
 
 typedef struct qm_ctx qm_ctx;

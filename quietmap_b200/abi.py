@@ -8,7 +8,7 @@ import ctypes as C
 
 import numpy as np
 
-ABI_VERSION = 1
+ABI_VERSION = 2
 BANDS = 8
 PERIODS = 3
 SECTORS = 16
@@ -104,6 +104,7 @@ class PaintStats(C.Structure):
         ("vertices", C.c_uint64),
         ("candidates", C.c_uint64),
         ("kernel_ms", C.c_double),
+        ("paint_ms", C.c_double),
     ]
 
 

@@ -103,14 +103,16 @@ struct Scratch {
 
 // A pair of timing events destroyed when the holder leaves scope.
 struct Events {
-    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr, e2 = nullptr;
     cudaError_t create() {
         cudaError_t e = cudaEventCreate(&e0);
-        return e != cudaSuccess ? e : cudaEventCreate(&e1);
+        if (e == cudaSuccess) e = cudaEventCreate(&e1);
+        return e != cudaSuccess ? e : cudaEventCreate(&e2);
     }
     ~Events() {
         if (e0) cudaEventDestroy(e0);
         if (e1) cudaEventDestroy(e1);
+        if (e2) cudaEventDestroy(e2);
     }
 };
 
@@ -538,6 +540,7 @@ qm_status qm_paint_grid(qm_scene *scene, const qm_grid_desc *grid, float *cell_b
         }
         QM_CUDA(cudaGetLastError());
     }
+    QM_CUDA(cudaEventRecord(ev.e2, stream));
     unsigned int n_retry = 0;
     QM_CUDA(cudaMemcpyAsync(&n_retry, d_rcount.p, sizeof(n_retry), cudaMemcpyDeviceToHost, stream));
     QM_CUDA(cudaStreamSynchronize(stream));
@@ -617,8 +620,9 @@ qm_status qm_paint_grid(qm_scene *scene, const qm_grid_desc *grid, float *cell_b
     if (cell_lden) QM_CUDA(cudaMemcpyAsync(cell_lden, d_lden.p, (size_t)cells * sizeof(float), cudaMemcpyDeviceToHost, stream));
     if (histogram) QM_CUDA(cudaMemcpyAsync(histogram, d_hist.p, g.n_bins * sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
     QM_CUDA(cudaStreamSynchronize(stream));
-    float ms = 0.f;
+    float ms = 0.f, paint_ms = 0.f;
     QM_CUDA(cudaEventElapsedTime(&ms, ev.e0, ev.e1));
+    QM_CUDA(cudaEventElapsedTime(&paint_ms, ev.e0, ev.e2));
     if (stats) {
         stats->paths = counters[0];
         stats->crossings = counters[1];
@@ -627,6 +631,7 @@ qm_status qm_paint_grid(qm_scene *scene, const qm_grid_desc *grid, float *cell_b
         stats->vertices = counters[4];
         stats->candidates = counters[5];
         stats->kernel_ms = ms;
+        stats->paint_ms = paint_ms;
     }
     return QM_OK;
 }
@@ -1068,6 +1073,7 @@ qm_status qm_paint_grid_static(qm_scene *scene, const qm_grid_desc *grid, float 
         stats->vertices = counters[4];
         stats->candidates = counters[5];
         stats->kernel_ms = -1.0;  // not timed: timing events are left out of this entry point
+        stats->paint_ms = -1.0;
     }
     if (counters[3] != 0)
         return fail(QM_ERR_CAPACITY, "qm_paint_grid_static: paths exceeded the per-path capacities; their re-run "

@@ -161,7 +161,7 @@ class DeviceScene:
         return bands, dba, lden, hist, dict(paths=stats.paths, failed_paths=stats.failed_paths,
                                              crossings=stats.crossings, edge_tests=stats.edge_tests,
                                              vertices=stats.vertices, candidates=stats.candidates,
-                                             kernel_ms=stats.kernel_ms)
+                                             kernel_ms=stats.kernel_ms, paint_ms=stats.paint_ms)
 
     def evaluate_pairs(self, receiver_xy_m, receiver_height_m, own_footprint, point_of_receiver, source_of_pair,
                        receiver_of_pair, band_weight, n_points, point_bands=None):
