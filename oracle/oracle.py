@@ -77,6 +77,8 @@ def lib():
         L.qmo_npd_level.restype = C.c_double
         L.qmo_tail_absorption.argtypes = [_D]
         L.qmo_tail_absorption.restype = C.c_double
+        L.qmo_surrogate_samples.argtypes = [C.c_void_p, C.POINTER(abi.GridDesc), C.c_uint32, C.c_uint32, _D, _D,
+                                            C.POINTER(C.c_uint8), C.c_int]
         L.qmo_flight_grid.argtypes = [C.c_void_p, C.c_uint32, C.c_void_p, C.c_size_t, C.POINTER(abi.FlightGridDesc),
                                       C.c_uint32, C.c_uint32, _D, _D, _D, C.c_int]
         _lib = L
@@ -228,6 +230,22 @@ class OracleScene:
         lib().qmo_paint_grid(self.handle, C.byref(g), cell_begin, cell_end, abi.ptr(energy, C.c_double),
                              abi.ptr(lden, C.c_double), nthreads or threads(), C.byref(tested))
         return energy, lden, tested.value
+
+    def surrogate_samples(self, grid, cell_begin=0, cell_end=0, nthreads=None):
+        """Surrogate features [rows][32], exact A_boundary labels [rows][8] (dB) and eligibility of
+        every path of cells [cell_begin, cell_end) (all when empty) against the grid's sources."""
+        g = abi.grid_desc(grid)
+        if cell_end <= cell_begin:
+            cell_begin, cell_end = 0, grid.cells
+        n_src = (grid.source_end - grid.source_begin) if grid.source_end > grid.source_begin else len(self.scene.sources)
+        rows = (cell_end - cell_begin) * n_src
+        f = np.zeros((rows, 32))
+        lab = np.zeros((rows, 8))
+        e = np.zeros(rows, np.uint8)
+        lib().qmo_surrogate_samples(self.handle, C.byref(g), cell_begin, cell_end, abi.ptr(f, C.c_double),
+                                    abi.ptr(lab, C.c_double), e.ctypes.data_as(C.POINTER(C.c_uint8)),
+                                    nthreads or threads())
+        return f, lab, e.astype(bool)
 
 
 def zwicker(levels28):

@@ -1712,4 +1712,87 @@ uint32_t qmo_level_bin(double level, double level_min, double bin_db, uint32_t n
     return level_bin(level, level_min, bin_db, n_bins);
 }
 
+// Surrogate training samples (the features of include/qm_surrogate.h and the exact A_boundary of
+// the homogeneous state as the label) for cells [cell_begin, cell_end) of a grid against its
+// source range: row (cell - cell_begin) * n_src + (source - source_begin). The roofs are the
+// vertical path's after clip_roofs_in_closing_order (physics/src/ray.rs:389-404); a path is
+// eligible when every obstacle top is a roof-bounding hit, every hit pairs into a roof and at
+// most 16 hits (8 roofs) are crossed.
+void qmo_surrogate_samples(void *scene, const qm_grid_desc *grid, uint32_t cell_begin, uint32_t cell_end,
+                           double *features, double *labels, uint8_t *eligible, int threads) {
+    const Scene &s = *static_cast<Scene *>(scene);
+    uint32_t sb = grid->source_begin, se = grid->source_end;
+    if (se <= sb) {
+        sb = 0;
+        se = (uint32_t)s.sources.size();
+    }
+    const uint32_t n_src = se - sb;
+    std::vector<Worker> workers(std::max(threads, 1));
+    parallel_for(cell_end - cell_begin, threads, [&](size_t k, int t) {
+        uint32_t cell = cell_begin + (uint32_t)k;
+        int64_t x = grid->origin[0] + (int64_t)(cell % grid->nx) * grid->spacing;
+        int64_t y = grid->origin[1] + (int64_t)(cell / grid->nx) * grid->spacing;
+        Receiver r = make_receiver(s, x, y, grid->height_m, enclosing_building(s, x, y));
+        Worker &w = workers[t];
+        for (uint32_t si = sb; si < se; ++si) {
+            const qm_source &src = s.sources[si];
+            size_t row = k * n_src + (si - sb);
+            int64_t from[2] = {src.x, src.y}, to[2] = {r.x, r.y};
+            fill_profile(s, from, to, w.profile);
+            scene_crossings(s, from, to, w.crossings);
+            if (r.own_footprint != 0) {
+                size_t kept = 0;
+                for (size_t i = 0; i < w.crossings.size(); ++i)
+                    if (w.crossings[i].footprint_id != r.own_footprint) w.crossings[kept++] = w.crossings[i];
+                w.crossings.resize(kept);
+            }
+            RayEnds ends;
+            ends.source_height_m = src.height_m;
+            ends.has_source_ground = false;
+            ends.source_ground_m = 0.0;
+            ends.receiver_altitude_m = r.altitude_m;
+            ends.has_source_ground_factor = src.ground_factor >= 0.0f;
+            ends.source_ground_factor = src.ground_factor;
+            ends.platform_half_width_m = src.platform_half_width_m;
+            ends.own_footprint = src.footprint_id;
+            double p[PERIODS] = {0.0, 0.0, 0.0};
+            Transfer transfer;
+            StateBoundary boundaries[2];
+            ray_terms(w.profile, w.crossings, ends, p, s.alpha, w.ray, transfer, boundaries, false);
+            const PathBuffers &pb = w.ray.pb;
+            for (int b = 0; b < BANDS; ++b) labels[row * BANDS + b] = boundaries[0].attenuation[b];
+            // Eligibility: tops all roof-bounding, hits all paired, at most 16 hits.
+            bool ok = pb.tops.size() == pb.buildings.size() && pb.buildings.size() <= 16;
+            for (size_t a = 0; a < pb.buildings.size() && ok;) {
+                size_t e = a;
+                while (e < pb.buildings.size() && pb.buildings[e].id == pb.buildings[a].id) ++e;
+                if ((e - a) % 2 != 0) ok = false;
+                a = e;
+            }
+            eligible[row] = ok ? 1 : 0;
+            double zs, gs, zr, gr, zm, gm;
+            terrain_at_point(s, src.x, src.y, zs, gs);
+            terrain_at_point(s, r.x, r.y, zr, gr);
+            terrain_at_point(s, (src.x + r.x) / 2, (src.y + r.y) / 2, zm, gm);
+            double L = std::max(w.profile.horizontal_m, 1.0);
+            double *f = features + row * 32;
+            f[0] = L / 1000.0;
+            f[1] = src.height_m / 10.0;
+            f[2] = (r.altitude_m - zr) / 10.0;
+            f[3] = (zr - zs) / 10.0;
+            f[4] = 0.0;
+            f[5] = src.ground_factor >= 0.0f ? (double)src.ground_factor : gs;
+            f[6] = gm;
+            f[7] = gr;
+            for (int q = 0; q < 8; ++q) {
+                bool present = q < (int)pb.roofs.size();
+                const Roof *rf = present ? &pb.roofs[q] : nullptr;
+                f[8 + 3 * q] = present ? rf->x0 / L : 0.0;
+                f[9 + 3 * q] = present ? rf->x1 / L : 0.0;
+                f[10 + 3 * q] = present ? ((rf->top0 + rf->top1) / 2.0 - zs) / 10.0 : 0.0;
+            }
+        }
+    });
+}
+
 }  // extern "C"

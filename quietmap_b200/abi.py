@@ -203,6 +203,23 @@ class PackedScene:
         self.desc = d
 
 
+SURR_FEATURES, SURR_HIDDEN, SURR_OUTPUTS = 32, 256, 8
+SURR_DIMS = (32, 256, 256, 256, 256, 8)
+SURR_WEIGHTS = sum(SURR_DIMS[k + 1] * SURR_DIMS[k] + SURR_DIMS[k + 1] for k in range(5))
+SURR_PARAMS = SURR_WEIGHTS + 32 + 32 + 8 + 8 + 32 + 32 + 8 + 8
+
+
+class TrainConfig(C.Structure):
+    _fields_ = [
+        ("epochs", C.c_uint32),
+        ("batch", C.c_uint32),
+        ("learning_rate", C.c_float),
+        ("seed", C.c_uint32),
+        ("max_samples", C.c_uint32),
+        ("pad_", C.c_uint32),
+    ]
+
+
 def grid_desc(grid):
     g = GridDesc()
     g.origin[0], g.origin[1] = grid.origin

@@ -11,7 +11,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libqm_b200.so")
-SOURCES = ["qm_lib.cu", "qm_zwicker.cu"]
+SOURCES = ["qm_lib.cu", "qm_zwicker.cu", "qm_mlp.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-O2",
          "--expt-relaxed-constexpr", "-rdc=false"]
@@ -25,7 +25,8 @@ def nvcc():
 
 def newest_input():
     paths = [os.path.join(CSRC, f) for f in os.listdir(CSRC)]
-    paths.append(os.path.join(os.path.dirname(HERE), "include", "qm_batch.h"))
+    inc = os.path.join(os.path.dirname(HERE), "include")
+    paths += [os.path.join(inc, f) for f in os.listdir(inc)]
     paths.append(__file__)
     return max(os.path.getmtime(p) for p in paths)
 

@@ -14,12 +14,16 @@
 #include <cstdio>
 #include <cstring>
 #include <mutex>
+#include <random>
 #include <string>
 #include <vector>
 
 #include "../../include/qm_batch.h"
+#include "../../include/qm_surrogate.h"
 #include "qm_aircraft.cuh"
 #include "qm_kernels.cuh"
+#include "qm_mlp.h"
+#include "qm_surrogate.cuh"
 #include "qm_warp.cuh"
 
 #include <climits>
@@ -440,6 +444,53 @@ void grid_receivers(const qm_scene *s, const qm_grid_desc *g, std::vector<float>
 
 bool terrain_caps(const qm_scene *s) { return s->dem_nx != 0; }
 
+// Re-runs a grid call's failed paths in (cell, source) order with large per-path capacities and
+// sums them into the partial slice `slice`.
+qm_status rerun_failed(qm_scene *scene, const GridArgs &A, const uint2 *d_retry, unsigned int n_retry, uint32_t slice,
+                       int cells, cudaStream_t stream) {
+    Scratch d_sorted, d_cids, d_cstart, d_works, d_results, d_rstatus;
+    // Re-run the failed paths in (cell, source) order with large capacities.
+    std::vector<uint2> list(n_retry);
+    QM_CUDA(cudaMemcpy(list.data(), d_retry, n_retry * sizeof(uint2), cudaMemcpyDeviceToHost));
+    std::sort(list.begin(), list.end(), [](uint2 a, uint2 b) { return a.x != b.x ? a.x < b.x : a.y < b.y; });
+    std::vector<uint32_t> cids, cstart;
+    for (uint32_t i = 0; i < n_retry; ++i)
+        if (cids.empty() || cids.back() != list[i].x) {
+            cids.push_back(list[i].x);
+            cstart.push_back(i);
+        }
+    cstart.push_back(n_retry);
+    const uint32_t threads = std::min<uint32_t>(((n_retry + 63) / 64) * 64, 8192);
+    using Large = PathWork<CapsLarge::C, CapsLarge::K, CapsLarge::H>;
+    QM_CUDA(cudaMalloc(&d_sorted.p, n_retry * sizeof(uint2)));
+    QM_CUDA(cudaMalloc(&d_cids.p, cids.size() * sizeof(uint32_t)));
+    QM_CUDA(cudaMalloc(&d_cstart.p, cstart.size() * sizeof(uint32_t)));
+    QM_CUDA(cudaMalloc(&d_works.p, (size_t)threads * sizeof(Large)));
+    QM_CUDA(cudaMalloc(&d_results.p, (size_t)n_retry * GRID_SLOTS * sizeof(float)));
+    QM_CUDA(cudaMalloc(&d_rstatus.p, (size_t)n_retry * sizeof(uint32_t)));
+    QM_CUDA(cudaMemcpyAsync(d_sorted.p, list.data(), n_retry * sizeof(uint2), cudaMemcpyHostToDevice, stream));
+    QM_CUDA(cudaMemcpyAsync(d_cids.p, cids.data(), cids.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, stream));
+    QM_CUDA(cudaMemcpyAsync(d_cstart.p, cstart.data(), cstart.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, stream));
+    retry_paths_kernel<<<threads / 64, 64, 0, stream>>>(scene->dev, A, static_cast<uint2 *>(d_sorted.p), n_retry,
+                                                        static_cast<Large *>(d_works.p),
+                                                        static_cast<float *>(d_results.p),
+                                                        static_cast<uint32_t *>(d_rstatus.p));
+    QM_CUDA(cudaGetLastError());
+    fold_retry_kernel<<<(unsigned)((cids.size() + 127) / 128), 128, 0, stream>>>(
+        static_cast<uint32_t *>(d_cids.p), static_cast<uint32_t *>(d_cstart.p), (uint32_t)cids.size(),
+        static_cast<float *>(d_results.p), A.partial, slice, cells);
+    QM_CUDA(cudaGetLastError());
+    std::vector<uint32_t> rstatus(n_retry);
+    QM_CUDA(cudaMemcpyAsync(rstatus.data(), d_rstatus.p, n_retry * sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
+    QM_CUDA(cudaStreamSynchronize(stream));
+    size_t still = 0;
+    for (uint32_t v : rstatus) still += v != 0;
+    if (still)
+        return fail(QM_ERR_CAPACITY, "qm_paint_grid: " + std::to_string(still) +
+                                         " paths exceed even the large per-path capacities");
+    return QM_OK;
+}
+
 #ifndef QM_WARP_PATHS_FOR_TERRAIN
 #define QM_WARP_PATHS_FOR_TERRAIN 0
 #endif
@@ -547,47 +598,9 @@ qm_status qm_paint_grid(qm_scene *scene, const qm_grid_desc *grid, float *cell_b
     if (n_retry > A.retry_cap)
         return fail(QM_ERR_CAPACITY, "qm_paint_grid: " + std::to_string(n_retry) +
                                          " paths exceeded the per-path capacities, more than the retry list holds");
-    Scratch d_sorted, d_cids, d_cstart, d_works, d_results, d_rstatus;
     if (n_retry > 0) {
-        // Re-run the failed paths in (cell, source) order with large capacities.
-        std::vector<uint2> list(n_retry);
-        QM_CUDA(cudaMemcpy(list.data(), d_retry.p, n_retry * sizeof(uint2), cudaMemcpyDeviceToHost));
-        std::sort(list.begin(), list.end(), [](uint2 a, uint2 b) { return a.x != b.x ? a.x < b.x : a.y < b.y; });
-        std::vector<uint32_t> cids, cstart;
-        for (uint32_t i = 0; i < n_retry; ++i)
-            if (cids.empty() || cids.back() != list[i].x) {
-                cids.push_back(list[i].x);
-                cstart.push_back(i);
-            }
-        cstart.push_back(n_retry);
-        const uint32_t threads = std::min<uint32_t>(((n_retry + 63) / 64) * 64, 8192);
-        using Large = PathWork<CapsLarge::C, CapsLarge::K, CapsLarge::H>;
-        QM_CUDA(cudaMalloc(&d_sorted.p, n_retry * sizeof(uint2)));
-        QM_CUDA(cudaMalloc(&d_cids.p, cids.size() * sizeof(uint32_t)));
-        QM_CUDA(cudaMalloc(&d_cstart.p, cstart.size() * sizeof(uint32_t)));
-        QM_CUDA(cudaMalloc(&d_works.p, (size_t)threads * sizeof(Large)));
-        QM_CUDA(cudaMalloc(&d_results.p, (size_t)n_retry * GRID_SLOTS * sizeof(float)));
-        QM_CUDA(cudaMalloc(&d_rstatus.p, (size_t)n_retry * sizeof(uint32_t)));
-        QM_CUDA(cudaMemcpyAsync(d_sorted.p, list.data(), n_retry * sizeof(uint2), cudaMemcpyHostToDevice, stream));
-        QM_CUDA(cudaMemcpyAsync(d_cids.p, cids.data(), cids.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, stream));
-        QM_CUDA(cudaMemcpyAsync(d_cstart.p, cstart.data(), cstart.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, stream));
-        retry_paths_kernel<<<threads / 64, 64, 0, stream>>>(scene->dev, A, static_cast<uint2 *>(d_sorted.p), n_retry,
-                                                            static_cast<Large *>(d_works.p),
-                                                            static_cast<float *>(d_results.p),
-                                                            static_cast<uint32_t *>(d_rstatus.p));
-        QM_CUDA(cudaGetLastError());
-        fold_retry_kernel<<<(unsigned)((cids.size() + 127) / 128), 128, 0, stream>>>(
-            static_cast<uint32_t *>(d_cids.p), static_cast<uint32_t *>(d_cstart.p), (uint32_t)cids.size(),
-            static_cast<float *>(d_results.p), A.partial, A.n_chunks, cells);
-        QM_CUDA(cudaGetLastError());
-        std::vector<uint32_t> rstatus(n_retry);
-        QM_CUDA(cudaMemcpyAsync(rstatus.data(), d_rstatus.p, n_retry * sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
-        QM_CUDA(cudaStreamSynchronize(stream));
-        size_t still = 0;
-        for (uint32_t v : rstatus) still += v != 0;
-        if (still)
-            return fail(QM_ERR_CAPACITY, "qm_paint_grid: " + std::to_string(still) +
-                                             " paths exceed even the large per-path capacities");
+        qm_status st = rerun_failed(scene, A, static_cast<uint2 *>(d_retry.p), n_retry, A.n_chunks, cells, stream);
+        if (st != QM_OK) return st;
     }
     ReduceArgs R{};
     R.cells = cells;
@@ -1227,3 +1240,649 @@ extern "C" qm_status qm_flight_grid(qm_ctx *ctx, const qm_aircraft_type *types, 
     if (error) return fail(QM_ERR_TIMEOUT, "qm_flight_grid: a segment tile's copy did not arrive in time");
     return QM_OK;
 }
+
+// ---------------------------------------------------------------------------------------------
+// The learned surrogate (include/qm_surrogate.h).
+
+struct qm_surrogate {
+    qm_ctx *ctx = nullptr;
+    qm::MlpDev net;
+    ~qm_surrogate() {
+        cudaFree(net.master);
+        cudaFree(net.w16);
+        cudaFree(net.adam_m);
+        cudaFree(net.adam_v);
+    }
+};
+
+namespace {
+
+static_assert(QM_SURR_WEIGHTS == MLP_WEIGHTS, "surrogate parameter layout");
+static_assert(QM_SURR_FEATURES == MLP_IN && QM_SURR_OUTPUTS == MLP_OUT, "surrogate widths");
+
+void scales_from_params(const float *p, MlpScales &s) {
+    const float *q = p + QM_SURR_WEIGHTS;
+    auto take = [&](float *dst, int n) {
+        std::memcpy(dst, q, n * sizeof(float));
+        q += n;
+    };
+    take(s.in_shift, MLP_IN);
+    take(s.in_scale, MLP_IN);
+    take(s.out_shift, MLP_OUT);
+    take(s.out_scale, MLP_OUT);
+    take(s.feat_lo, MLP_IN);
+    take(s.feat_hi, MLP_IN);
+    take(s.lab_lo, MLP_OUT);
+    take(s.lab_hi, MLP_OUT);
+}
+
+void scales_to_params(const MlpScales &s, float *p) {
+    float *q = p + QM_SURR_WEIGHTS;
+    auto put = [&](const float *src, int n) {
+        std::memcpy(q, src, n * sizeof(float));
+        q += n;
+    };
+    put(s.in_shift, MLP_IN);
+    put(s.in_scale, MLP_IN);
+    put(s.out_shift, MLP_OUT);
+    put(s.out_scale, MLP_OUT);
+    put(s.feat_lo, MLP_IN);
+    put(s.feat_hi, MLP_IN);
+    put(s.lab_lo, MLP_OUT);
+    put(s.lab_hi, MLP_OUT);
+}
+
+// The grid checks qm_paint_grid makes.
+qm_status check_grid(const qm_scene *scene, const qm_grid_desc &g, const char *name) {
+    if (g.nx <= 0 || g.ny <= 0 || g.spacing <= 0 || (int64_t)g.nx * g.ny > (int64_t(1) << 30))
+        return fail(QM_ERR_ARGUMENT, std::string(name) + ": grid nx, ny or spacing");
+    int64_t last_x = g.origin[0] + (int64_t)(g.nx - 1) * g.spacing, last_y = g.origin[1] + (int64_t)(g.ny - 1) * g.spacing;
+    if (g.origin[0] < 0 || g.origin[1] < 0 || last_x >= scene->extent[0] || last_y >= scene->extent[1])
+        return fail(QM_ERR_ARGUMENT, std::string(name) + ": grid receivers outside the scene extent");
+    uint32_t sb = g.source_begin, se = g.source_end;
+    if (se > sb && se > scene->n_sources)
+        return fail(QM_ERR_ARGUMENT, std::string(name) + ": source range beyond the scene's sources");
+    return QM_OK;
+}
+
+// Receivers of a grid on the device and its (tile, source chunk) launch shape.
+struct GridSetup {
+    Scratch alt, own;
+    GridArgs A{};
+    int cells = 0, tiles = 0;
+};
+
+qm_status setup_grid(qm_scene *scene, const qm_grid_desc &g, uint32_t sb, uint32_t se, GridSetup &G,
+                     cudaStream_t stream) {
+    qm_ctx *ctx = scene->ctx;
+    G.cells = g.nx * g.ny;
+    std::vector<float> alt;
+    std::vector<uint32_t> own;
+    grid_receivers(scene, &g, alt, own);
+    GridArgs &A = G.A;
+    A.origin_x = g.origin[0];
+    A.origin_y = g.origin[1];
+    A.spacing = g.spacing;
+    A.nx = g.nx;
+    A.ny = g.ny;
+    A.height_m = g.height_m;
+    A.source_begin = sb;
+    A.source_end = se;
+    A.tile_w = 16;
+    A.tile_h = 8;
+    A.want_fav = false;
+    for (int p = 0; p < 3; ++p) A.lden_w[p] = (float)LDEN_W[p];
+    G.tiles = ((g.nx + A.tile_w - 1) / A.tile_w) * ((g.ny + A.tile_h - 1) / A.tile_h);
+    const uint32_t n_src = se - sb;
+    uint32_t want_ctas = (uint32_t)ctx->sm_count * 16;
+    uint32_t n_chunks = std::max<uint32_t>(1, (want_ctas + G.tiles - 1) / G.tiles);
+    n_chunks = std::min<uint32_t>(n_chunks, std::max<uint32_t>(1, n_src / 32));
+    n_chunks = std::min<uint32_t>(n_chunks, 65535);
+    A.chunk = std::max<uint32_t>(1, (n_src + n_chunks - 1) / n_chunks);
+    A.n_chunks = n_src == 0 ? 1 : (n_src + A.chunk - 1) / A.chunk;
+    QM_CUDA(cudaMalloc(&G.alt.p, G.cells * sizeof(float)));
+    QM_CUDA(cudaMalloc(&G.own.p, G.cells * sizeof(uint32_t)));
+    QM_CUDA(cudaMemcpyAsync(G.alt.p, alt.data(), G.cells * sizeof(float), cudaMemcpyHostToDevice, stream));
+    QM_CUDA(cudaMemcpyAsync(G.own.p, own.data(), G.cells * sizeof(uint32_t), cudaMemcpyHostToDevice, stream));
+    A.rcv_alt = static_cast<float *>(G.alt.p);
+    A.rcv_own = static_cast<uint32_t *>(G.own.p);
+    return QM_OK;
+}
+
+// Launch shape of a source sub-range [b0, b1) of a set-up grid.
+void chunk_range(const qm_ctx *ctx, GridArgs &A, int tiles, uint32_t b0, uint32_t b1) {
+    A.source_begin = b0;
+    A.source_end = b1;
+    const uint32_t n_src = b1 - b0;
+    uint32_t want_ctas = (uint32_t)ctx->sm_count * 16;
+    uint32_t n_chunks = std::max<uint32_t>(1, (want_ctas + tiles - 1) / tiles);
+    n_chunks = std::min<uint32_t>(n_chunks, std::max<uint32_t>(1, n_src / 32));
+    n_chunks = std::min<uint32_t>(n_chunks, 65535);
+    A.chunk = std::max<uint32_t>(1, (n_src + n_chunks - 1) / n_chunks);
+    A.n_chunks = n_src == 0 ? 1 : (n_src + A.chunk - 1) / A.chunk;
+}
+
+__global__ void gather_rows_kernel(const float *src, const uint32_t *index, size_t n, int w, float *dst) {
+    size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+    if (i >= n * w) return;
+    size_t r = i / w;
+    dst[i] = src[(size_t)index[r] * w + (i - r * w)];
+}
+
+__global__ void affine_rows_kernel(float *rows, size_t n, int w, const float *shift, const float *inv_scale) {
+    __shared__ float sh[64], sc[64];
+    if (threadIdx.x < w) {
+        sh[threadIdx.x] = shift[threadIdx.x];
+        sc[threadIdx.x] = inv_scale[threadIdx.x];
+    }
+    __syncthreads();
+    size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+    if (i >= n * w) return;
+    int c = (int)(i % w);
+    rows[i] = (rows[i] - sh[c]) * sc[c];
+}
+
+// Exact training samples of one grid: every path's raw features, label and eligibility on the device.
+qm_status grid_samples(qm_scene *scene, const qm_grid_desc &g, Scratch &feat, Scratch &lab, Scratch &elig,
+                       size_t &rows, cudaStream_t stream) {
+    uint32_t sb = g.source_begin, se = g.source_end;
+    if (se <= sb) {
+        sb = 0;
+        se = scene->n_sources;
+    }
+    GridSetup G;
+    qm_status st = setup_grid(scene, g, sb, se, G, stream);
+    if (st != QM_OK) return st;
+    rows = (size_t)G.cells * (se - sb);
+    if (rows == 0) return QM_OK;
+    QM_CUDA(cudaMalloc(&feat.p, rows * MLP_IN * sizeof(float)));
+    QM_CUDA(cudaMalloc(&lab.p, rows * MLP_OUT * sizeof(float)));
+    QM_CUDA(cudaMalloc(&elig.p, rows));
+    SampleArgs P{};
+    P.g = G.A;
+    P.features = static_cast<float *>(feat.p);
+    P.labels = static_cast<float *>(lab.p);
+    P.eligible = static_cast<uint8_t *>(elig.p);
+    surrogate_samples_kernel<<<dim3(G.tiles, G.A.n_chunks), 128, 0, stream>>>(scene->dev, P);
+    QM_CUDA(cudaGetLastError());
+    QM_CUDA(cudaStreamSynchronize(stream));
+    return QM_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+qm_status qm_surrogate_create(qm_ctx *ctx, const float *params, qm_surrogate **out) {
+    if (!ctx || !params || !out) return fail(QM_ERR_ARGUMENT, "qm_surrogate_create: null ctx, params or out");
+    for (size_t i = 0; i < QM_SURR_PARAMS; ++i)
+        if (!std::isfinite(params[i])) return fail(QM_ERR_ARGUMENT, "qm_surrogate_create: params[" + std::to_string(i) + "] is not finite");
+    std::lock_guard<std::mutex> guard(ctx->lock);
+    QM_CUDA(cudaSetDevice(ctx->device));
+    auto *s = new qm_surrogate;
+    s->ctx = ctx;
+    scales_from_params(params, s->net.scales);
+    cudaError_t e = cudaMalloc(&s->net.master, MLP_WEIGHTS * sizeof(float));
+    if (e == cudaSuccess) e = cudaMalloc(&s->net.w16, MLP_W16 * sizeof(__nv_bfloat16));
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(s->net.master, params, MLP_WEIGHTS * sizeof(float), cudaMemcpyHostToDevice, ctx->stream);
+    if (e == cudaSuccess) e = mlp_cast(s->net, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) {
+        delete s;
+        return fail(QM_ERR_CUDA, std::string("cuda: ") + cudaGetErrorString(e));
+    }
+    *out = s;
+    return QM_OK;
+}
+
+void qm_surrogate_free(qm_surrogate *net) {
+    if (!net) return;
+    std::lock_guard<std::mutex> guard(net->ctx->lock);
+    cudaSetDevice(net->ctx->device);
+    delete net;
+}
+
+qm_status qm_surrogate_params(const qm_surrogate *net, float *params) {
+    if (!net || !params) return fail(QM_ERR_ARGUMENT, "qm_surrogate_params: null net or params");
+    std::lock_guard<std::mutex> guard(net->ctx->lock);
+    QM_CUDA(cudaSetDevice(net->ctx->device));
+    QM_CUDA(cudaMemcpyAsync(params, net->net.master, MLP_WEIGHTS * sizeof(float), cudaMemcpyDeviceToHost, net->ctx->stream));
+    QM_CUDA(cudaStreamSynchronize(net->ctx->stream));
+    scales_to_params(net->net.scales, params);
+    return QM_OK;
+}
+
+qm_status qm_surrogate_samples(qm_scene *scene, const qm_grid_desc *grid, float *features, float *labels,
+                               uint8_t *eligible) {
+    if (!scene || !grid || !features || !labels || !eligible)
+        return fail(QM_ERR_ARGUMENT, "qm_surrogate_samples: null scene, grid or output");
+    if (scene->dem_nx != 0) return fail(QM_ERR_UNSUPPORTED, "qm_surrogate_samples: the surrogate covers flat scenes only");
+    qm_status st = check_grid(scene, *grid, "qm_surrogate_samples");
+    if (st != QM_OK) return st;
+    std::lock_guard<std::mutex> guard(scene->ctx->lock);
+    QM_CUDA(cudaSetDevice(scene->ctx->device));
+    cudaStream_t stream = scene->ctx->stream;
+    Scratch f, l, e;
+    size_t rows = 0;
+    st = grid_samples(scene, *grid, f, l, e, rows, stream);
+    if (st != QM_OK) return st;
+    if (rows == 0) return QM_OK;
+    QM_CUDA(cudaMemcpy(features, f.p, rows * MLP_IN * sizeof(float), cudaMemcpyDeviceToHost));
+    QM_CUDA(cudaMemcpy(labels, l.p, rows * MLP_OUT * sizeof(float), cudaMemcpyDeviceToHost));
+    QM_CUDA(cudaMemcpy(eligible, e.p, rows, cudaMemcpyDeviceToHost));
+    return QM_OK;
+}
+
+qm_status qm_surrogate_forward(qm_surrogate *net, const float *features, size_t n, float *outputs) {
+    if (!net || (n && (!features || !outputs))) return fail(QM_ERR_ARGUMENT, "qm_surrogate_forward: null net, features or outputs");
+    if (n == 0) return QM_OK;
+    std::lock_guard<std::mutex> guard(net->ctx->lock);
+    QM_CUDA(cudaSetDevice(net->ctx->device));
+    cudaStream_t stream = net->ctx->stream;
+    Scratch raw, x, out;
+    QM_CUDA(cudaMalloc(&raw.p, n * MLP_IN * sizeof(float)));
+    QM_CUDA(cudaMalloc(&x.p, n * MLP_IN * sizeof(__nv_bfloat16)));
+    QM_CUDA(cudaMalloc(&out.p, n * MLP_OUT * sizeof(float)));
+    QM_CUDA(cudaMemcpyAsync(raw.p, features, n * MLP_IN * sizeof(float), cudaMemcpyHostToDevice, stream));
+    QM_CUDA(mlp_normalise(net->net.scales, static_cast<float *>(raw.p), n, static_cast<__nv_bfloat16 *>(x.p), stream));
+    QM_CUDA(mlp_forward(net->net, static_cast<__nv_bfloat16 *>(x.p), n, static_cast<float *>(out.p), stream));
+    QM_CUDA(cudaMemcpyAsync(outputs, out.p, n * MLP_OUT * sizeof(float), cudaMemcpyDeviceToHost, stream));
+    QM_CUDA(cudaStreamSynchronize(stream));
+    return QM_OK;
+}
+
+qm_status qm_surrogate_gradients(qm_surrogate *net, const float *features, const float *labels, size_t n,
+                                 float *grads, double *loss) {
+    if (!net || !features || !labels || !grads || !loss)
+        return fail(QM_ERR_ARGUMENT, "qm_surrogate_gradients: null net, features, labels, grads or loss");
+    if (n == 0 || n % 8 != 0 || n > (1u << 24))
+        return fail(QM_ERR_ARGUMENT, "qm_surrogate_gradients: n must be a positive multiple of 8 up to 2^24");
+    std::lock_guard<std::mutex> guard(net->ctx->lock);
+    QM_CUDA(cudaSetDevice(net->ctx->device));
+    cudaStream_t stream = net->ctx->stream;
+    std::vector<float> y(n * MLP_OUT);
+    for (size_t i = 0; i < n; ++i)
+        for (int o = 0; o < MLP_OUT; ++o)
+            y[i * MLP_OUT + o] = (labels[i * MLP_OUT + o] - net->net.scales.out_shift[o]) / net->net.scales.out_scale[o];
+    Scratch raw, x, dy, dg, dl;
+    QM_CUDA(cudaMalloc(&raw.p, n * MLP_IN * sizeof(float)));
+    QM_CUDA(cudaMalloc(&x.p, n * MLP_IN * sizeof(__nv_bfloat16)));
+    QM_CUDA(cudaMalloc(&dy.p, n * MLP_OUT * sizeof(float)));
+    QM_CUDA(cudaMalloc(&dg.p, MLP_WEIGHTS * sizeof(float)));
+    QM_CUDA(cudaMalloc(&dl.p, sizeof(double)));
+    QM_CUDA(cudaMemcpyAsync(raw.p, features, n * MLP_IN * sizeof(float), cudaMemcpyHostToDevice, stream));
+    QM_CUDA(cudaMemcpyAsync(dy.p, y.data(), n * MLP_OUT * sizeof(float), cudaMemcpyHostToDevice, stream));
+    QM_CUDA(mlp_normalise(net->net.scales, static_cast<float *>(raw.p), n, static_cast<__nv_bfloat16 *>(x.p), stream));
+    MlpWork *w = mlp_work_create(n);
+    if (!w) return fail(QM_ERR_CUDA, "cuda: out of memory for the activations");
+    cudaError_t e = mlp_gradients(net->net, w, static_cast<__nv_bfloat16 *>(x.p), static_cast<float *>(dy.p), n,
+                                  static_cast<float *>(dg.p), static_cast<double *>(dl.p), stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+    mlp_work_free(w);
+    if (e != cudaSuccess) return fail(QM_ERR_CUDA, std::string("cuda: ") + cudaGetErrorString(e));
+    QM_CUDA(cudaMemcpy(grads, dg.p, MLP_WEIGHTS * sizeof(float), cudaMemcpyDeviceToHost));
+    QM_CUDA(cudaMemcpy(loss, dl.p, sizeof(double), cudaMemcpyDeviceToHost));
+    return QM_OK;
+}
+
+qm_status qm_surrogate_train(qm_surrogate *net, qm_scene *scene, const qm_grid_desc *grids, size_t n_grids,
+                             const qm_train_config *config, double *loss_history, uint64_t *n_samples) {
+    if (!net || !scene || !grids || !config || n_grids == 0)
+        return fail(QM_ERR_ARGUMENT, "qm_surrogate_train: null net, scene, grids or config");
+    if (scene->ctx != net->ctx) return fail(QM_ERR_ARGUMENT, "qm_surrogate_train: net and scene on different contexts");
+    if (scene->dem_nx != 0) return fail(QM_ERR_UNSUPPORTED, "qm_surrogate_train: the surrogate covers flat scenes only");
+    const qm_train_config &c = *config;
+    if (c.epochs == 0 || c.batch < 256 || c.batch % 128 != 0 || c.batch > (1u << 20) || !(c.learning_rate > 0.0f))
+        return fail(QM_ERR_ARGUMENT, "qm_surrogate_train: epochs >= 1, batch a multiple of 128 in [256, 2^20], learning_rate > 0");
+    for (size_t k = 0; k < n_grids; ++k) {
+        qm_status st = check_grid(scene, grids[k], "qm_surrogate_train");
+        if (st != QM_OK) return st;
+    }
+    std::lock_guard<std::mutex> guard(net->ctx->lock);
+    QM_CUDA(cudaSetDevice(net->ctx->device));
+    cudaStream_t stream = net->ctx->stream;
+    // Samples: every path of each grid, eligible ones gathered in row order.
+    size_t upper = 0;
+    for (size_t k = 0; k < n_grids; ++k) {
+        const qm_grid_desc &g = grids[k];
+        uint32_t n_src = g.source_end > g.source_begin ? g.source_end - g.source_begin : scene->n_sources;
+        upper += (size_t)g.nx * g.ny * n_src;
+    }
+    if (upper == 0) return fail(QM_ERR_ARGUMENT, "qm_surrogate_train: the grids hold no paths");
+    Scratch all_f, all_l;
+    QM_CUDA(cudaMalloc(&all_f.p, upper * MLP_IN * sizeof(float)));
+    QM_CUDA(cudaMalloc(&all_l.p, upper * MLP_OUT * sizeof(float)));
+    size_t total = 0;
+    for (size_t k = 0; k < n_grids; ++k) {
+        Scratch f, l, e, idx;
+        size_t rows = 0;
+        qm_status st = grid_samples(scene, grids[k], f, l, e, rows, stream);
+        if (st != QM_OK) return st;
+        if (rows == 0) continue;
+        std::vector<uint8_t> flags(rows);
+        QM_CUDA(cudaMemcpy(flags.data(), e.p, rows, cudaMemcpyDeviceToHost));
+        std::vector<uint32_t> keep;
+        keep.reserve(rows);
+        for (size_t i = 0; i < rows; ++i)
+            if (flags[i]) keep.push_back((uint32_t)i);
+        if (keep.empty()) continue;
+        QM_CUDA(cudaMalloc(&idx.p, keep.size() * sizeof(uint32_t)));
+        QM_CUDA(cudaMemcpyAsync(idx.p, keep.data(), keep.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, stream));
+        size_t nf = keep.size() * MLP_IN, nl = keep.size() * MLP_OUT;
+        gather_rows_kernel<<<(unsigned)((nf + 255) / 256), 256, 0, stream>>>(
+            static_cast<float *>(f.p), static_cast<uint32_t *>(idx.p), keep.size(), MLP_IN,
+            static_cast<float *>(all_f.p) + total * MLP_IN);
+        gather_rows_kernel<<<(unsigned)((nl + 255) / 256), 256, 0, stream>>>(
+            static_cast<float *>(l.p), static_cast<uint32_t *>(idx.p), keep.size(), MLP_OUT,
+            static_cast<float *>(all_l.p) + total * MLP_OUT);
+        QM_CUDA(cudaGetLastError());
+        QM_CUDA(cudaStreamSynchronize(stream));
+        total += keep.size();
+    }
+    std::mt19937_64 rng(c.seed);
+    if (c.max_samples && total > c.max_samples) {
+        // A seeded subset, kept in row order.
+        std::vector<uint32_t> pick(total);
+        for (size_t i = 0; i < total; ++i) pick[i] = (uint32_t)i;
+        std::shuffle(pick.begin(), pick.end(), rng);
+        pick.resize(c.max_samples);
+        std::sort(pick.begin(), pick.end());
+        Scratch idx, f2, l2;
+        QM_CUDA(cudaMalloc(&idx.p, pick.size() * sizeof(uint32_t)));
+        QM_CUDA(cudaMalloc(&f2.p, pick.size() * MLP_IN * sizeof(float)));
+        QM_CUDA(cudaMalloc(&l2.p, pick.size() * MLP_OUT * sizeof(float)));
+        QM_CUDA(cudaMemcpyAsync(idx.p, pick.data(), pick.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, stream));
+        size_t nf = pick.size() * MLP_IN, nl = pick.size() * MLP_OUT;
+        gather_rows_kernel<<<(unsigned)((nf + 255) / 256), 256, 0, stream>>>(
+            static_cast<float *>(all_f.p), static_cast<uint32_t *>(idx.p), pick.size(), MLP_IN, static_cast<float *>(f2.p));
+        gather_rows_kernel<<<(unsigned)((nl + 255) / 256), 256, 0, stream>>>(
+            static_cast<float *>(all_l.p), static_cast<uint32_t *>(idx.p), pick.size(), MLP_OUT, static_cast<float *>(l2.p));
+        QM_CUDA(cudaGetLastError());
+        QM_CUDA(cudaStreamSynchronize(stream));
+        std::swap(all_f.p, f2.p);
+        std::swap(all_l.p, l2.p);
+        total = pick.size();
+    }
+    if (total < c.batch) return fail(QM_ERR_ARGUMENT, "qm_surrogate_train: fewer eligible samples than one batch");
+    if (n_samples) *n_samples = total;
+    // Normalisation and ranges from the samples.
+    Scratch stats;
+    const size_t stats_bytes = (MLP_IN + MLP_OUT) * (2 * sizeof(double) + 2 * sizeof(float));
+    QM_CUDA(cudaMalloc(&stats.p, stats_bytes));
+    double *d_sum = static_cast<double *>(stats.p), *d_sq = d_sum + MLP_IN + MLP_OUT;
+    float *d_lo = reinterpret_cast<float *>(d_sq + MLP_IN + MLP_OUT), *d_hi = d_lo + MLP_IN + MLP_OUT;
+    {
+        std::vector<double> zeros(2 * (MLP_IN + MLP_OUT), 0.0);
+        std::vector<float> lo(MLP_IN + MLP_OUT, INFINITY), hi(MLP_IN + MLP_OUT, -INFINITY);
+        QM_CUDA(cudaMemcpyAsync(d_sum, zeros.data(), zeros.size() * sizeof(double), cudaMemcpyHostToDevice, stream));
+        QM_CUDA(cudaMemcpyAsync(d_lo, lo.data(), lo.size() * sizeof(float), cudaMemcpyHostToDevice, stream));
+        QM_CUDA(cudaMemcpyAsync(d_hi, hi.data(), hi.size() * sizeof(float), cudaMemcpyHostToDevice, stream));
+    }
+    QM_CUDA(mlp_column_stats(static_cast<float *>(all_f.p), nullptr, total, MLP_IN, d_sum, d_sq, d_lo, d_hi, stream));
+    QM_CUDA(mlp_column_stats(static_cast<float *>(all_l.p), nullptr, total, MLP_OUT, d_sum + MLP_IN, d_sq + MLP_IN,
+                             d_lo + MLP_IN, d_hi + MLP_IN, stream));
+    std::vector<double> sum(MLP_IN + MLP_OUT), sq(MLP_IN + MLP_OUT);
+    std::vector<float> lo(MLP_IN + MLP_OUT), hi(MLP_IN + MLP_OUT);
+    QM_CUDA(cudaMemcpyAsync(sum.data(), d_sum, sum.size() * sizeof(double), cudaMemcpyDeviceToHost, stream));
+    QM_CUDA(cudaMemcpyAsync(sq.data(), d_sq, sq.size() * sizeof(double), cudaMemcpyDeviceToHost, stream));
+    QM_CUDA(cudaMemcpyAsync(lo.data(), d_lo, lo.size() * sizeof(float), cudaMemcpyDeviceToHost, stream));
+    QM_CUDA(cudaMemcpyAsync(hi.data(), d_hi, hi.size() * sizeof(float), cudaMemcpyDeviceToHost, stream));
+    QM_CUDA(cudaStreamSynchronize(stream));
+    MlpScales &S = net->net.scales;
+    for (int k = 0; k < MLP_IN + MLP_OUT; ++k) {
+        double mean = sum[k] / (double)total;
+        double var = std::max(sq[k] / (double)total - mean * mean, 0.0);
+        double sd = std::sqrt(var);
+        if (k < MLP_IN) {
+            S.in_shift[k] = (float)mean;
+            S.in_scale[k] = sd > 1e-6 ? (float)(1.0 / sd) : 1.0f;
+            S.feat_lo[k] = lo[k];
+            S.feat_hi[k] = hi[k];
+        } else {
+            int o = k - MLP_IN;
+            S.out_shift[o] = (float)mean;
+            S.out_scale[o] = sd > 1e-6 ? (float)sd : 1.0f;
+            S.lab_lo[o] = lo[k];
+            S.lab_hi[o] = hi[k];
+        }
+    }
+    // Normalised training set: BF16 features, FP32 labels.
+    Scratch X, shift_scale;
+    QM_CUDA(cudaMalloc(&X.p, total * MLP_IN * sizeof(__nv_bfloat16)));
+    QM_CUDA(mlp_normalise(S, static_cast<float *>(all_f.p), total, static_cast<__nv_bfloat16 *>(X.p), stream));
+    {
+        std::vector<float> ss(2 * MLP_OUT);
+        for (int o = 0; o < MLP_OUT; ++o) {
+            ss[o] = S.out_shift[o];
+            ss[MLP_OUT + o] = 1.0f / S.out_scale[o];
+        }
+        QM_CUDA(cudaMalloc(&shift_scale.p, ss.size() * sizeof(float)));
+        QM_CUDA(cudaMemcpyAsync(shift_scale.p, ss.data(), ss.size() * sizeof(float), cudaMemcpyHostToDevice, stream));
+        size_t nl = total * MLP_OUT;
+        affine_rows_kernel<<<(unsigned)((nl + 255) / 256), 256, 0, stream>>>(
+            static_cast<float *>(all_l.p), total, MLP_OUT, static_cast<float *>(shift_scale.p),
+            static_cast<float *>(shift_scale.p) + MLP_OUT);
+        QM_CUDA(cudaGetLastError());
+    }
+    QM_CUDA(cudaStreamSynchronize(stream));
+    cudaFree(all_f.p);
+    all_f.p = nullptr;
+    // Adam state.
+    if (!net->net.adam_m) QM_CUDA(cudaMalloc(&net->net.adam_m, MLP_WEIGHTS * sizeof(float)));
+    if (!net->net.adam_v) QM_CUDA(cudaMalloc(&net->net.adam_v, MLP_WEIGHTS * sizeof(float)));
+    QM_CUDA(cudaMemsetAsync(net->net.adam_m, 0, MLP_WEIGHTS * sizeof(float), stream));
+    QM_CUDA(cudaMemsetAsync(net->net.adam_v, 0, MLP_WEIGHTS * sizeof(float), stream));
+    // Shuffled order, batches in a fresh order each epoch.
+    std::vector<uint32_t> perm(total);
+    for (size_t i = 0; i < total; ++i) perm[i] = (uint32_t)i;
+    std::shuffle(perm.begin(), perm.end(), rng);
+    Scratch d_perm, bx, by, grads, losses;
+    const size_t B = c.batch, steps = total / B;
+    QM_CUDA(cudaMalloc(&d_perm.p, total * sizeof(uint32_t)));
+    QM_CUDA(cudaMemcpyAsync(d_perm.p, perm.data(), total * sizeof(uint32_t), cudaMemcpyHostToDevice, stream));
+    QM_CUDA(cudaMalloc(&bx.p, B * MLP_IN * sizeof(__nv_bfloat16)));
+    QM_CUDA(cudaMalloc(&by.p, B * MLP_OUT * sizeof(float)));
+    QM_CUDA(cudaMalloc(&grads.p, MLP_WEIGHTS * sizeof(float)));
+    QM_CUDA(cudaMalloc(&losses.p, steps * sizeof(double)));
+    MlpWork *work = mlp_work_create(B);
+    if (!work) return fail(QM_ERR_CUDA, "cuda: out of memory for the activations");
+    std::vector<size_t> order(steps);
+    std::vector<double> step_loss(steps);
+    const double total_steps = (double)steps * c.epochs;
+    int t = 0;
+    cudaError_t e = cudaSuccess;
+    for (uint32_t epoch = 0; epoch < c.epochs && e == cudaSuccess; ++epoch) {
+        for (size_t k = 0; k < steps; ++k) order[k] = k;
+        std::shuffle(order.begin(), order.end(), rng);
+        for (size_t k = 0; k < steps && e == cudaSuccess; ++k) {
+            e = mlp_gather(static_cast<__nv_bfloat16 *>(X.p), static_cast<float *>(all_l.p),
+                           static_cast<uint32_t *>(d_perm.p) + order[k] * B, B, static_cast<__nv_bfloat16 *>(bx.p),
+                           static_cast<float *>(by.p), stream);
+            if (e == cudaSuccess)
+                e = mlp_gradients(net->net, work, static_cast<__nv_bfloat16 *>(bx.p), static_cast<float *>(by.p), B,
+                                  static_cast<float *>(grads.p), static_cast<double *>(losses.p) + k, stream);
+            ++t;
+            double frac = t / total_steps;
+            float lr = c.learning_rate * (float)(0.05 + 0.95 * 0.5 * (1.0 + std::cos(3.141592653589793 * frac)));
+            if (e == cudaSuccess) e = mlp_adam(net->net, static_cast<float *>(grads.p), lr, t, stream);
+        }
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(step_loss.data(), losses.p, steps * sizeof(double), cudaMemcpyDeviceToHost, stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+        if (e == cudaSuccess && loss_history) {
+            double m = 0.0;
+            for (double v : step_loss) m += v;
+            loss_history[epoch] = m / (double)steps;
+        }
+    }
+    mlp_work_free(work);
+    if (e != cudaSuccess) return fail(QM_ERR_CUDA, std::string("cuda: ") + cudaGetErrorString(e));
+    return QM_OK;
+}
+
+qm_status qm_paint_grid_surrogate(qm_scene *scene, const qm_grid_desc *grid, qm_surrogate *net, float *cell_bands,
+                                  float *cell_dba, float *cell_lden, uint32_t *histogram, qm_paint_stats *stats,
+                                  uint64_t *surrogate_paths) {
+    if (!scene || !grid || !net) return fail(QM_ERR_ARGUMENT, "qm_paint_grid_surrogate: null scene, grid or net");
+    if (scene->ctx != net->ctx) return fail(QM_ERR_ARGUMENT, "qm_paint_grid_surrogate: net and scene on different contexts");
+    if (scene->dem_nx != 0 || scene->any_favourable)
+        return fail(QM_ERR_UNSUPPORTED, "qm_paint_grid_surrogate: flat scenes in homogeneous conditions only");
+    const qm_grid_desc &g = *grid;
+    qm_status st = check_grid(scene, g, "qm_paint_grid_surrogate");
+    if (st != QM_OK) return st;
+    if (histogram && (g.n_bins == 0 || g.n_bins > 51200 || !(g.bin_db > 0.0)))
+        return fail(QM_ERR_ARGUMENT, "qm_paint_grid_surrogate: histogram needs 0 < n_bins <= 51200 and bin_db > 0");
+    uint32_t sb = g.source_begin, se = g.source_end;
+    if (se <= sb) {
+        sb = 0;
+        se = scene->n_sources;
+    }
+    qm_ctx *ctx = scene->ctx;
+    std::lock_guard<std::mutex> guard(ctx->lock);
+    QM_CUDA(cudaSetDevice(ctx->device));
+    cudaStream_t stream = ctx->stream;
+    GridSetup G;
+    st = setup_grid(scene, g, sb, se, G, stream);
+    if (st != QM_OK) return st;
+    const int cells = G.cells;
+    const uint32_t n_src = se - sb;
+    // Sources in batches of whole 128-row tiles per cell, at most 2^25 rows a batch.
+    const size_t max_rows = size_t(1) << 25;
+    uint32_t batch = (uint32_t)std::max<size_t>(128, (max_rows / (size_t)cells) / 128 * 128);
+    batch = std::min<uint32_t>(batch, ((n_src + 127) / 128) * 128);
+    uint32_t max_chunks = 1;
+    for (uint32_t b0 = sb; b0 < se; b0 += batch) {
+        GridArgs tmp = G.A;
+        chunk_range(ctx, tmp, G.tiles, b0, std::min(se, b0 + batch));
+        max_chunks = std::max(max_chunks, tmp.n_chunks);
+    }
+    const uint32_t mlp_slices = std::max<uint32_t>(1, batch / 128);
+    const uint32_t slices = max_chunks + 1 + mlp_slices;
+    const size_t rows_cap = (size_t)cells * std::max<uint32_t>(batch, 128);
+    GridArgs A = G.A;
+    A.retry_cap = (uint32_t)std::min<int64_t>(std::max<int64_t>((int64_t)cells * n_src / 128, 1 << 20), 1 << 25);
+    Scratch d_partial, d_failed, d_counters, d_retry, d_rcount, d_x, d_coef, d_elig, d_taken, d_dba, d_hist, d_bands,
+        d_dbaout, d_lden;
+    const size_t partial_bytes = (size_t)slices * cells * GRID_SLOTS * sizeof(float);
+    QM_CUDA(cudaMalloc(&d_partial.p, partial_bytes));
+    QM_CUDA(cudaMalloc(&d_failed.p, cells * sizeof(uint32_t)));
+    QM_CUDA(cudaMalloc(&d_counters.p, 6 * sizeof(unsigned long long)));
+    QM_CUDA(cudaMalloc(&d_retry.p, (size_t)A.retry_cap * sizeof(uint2)));
+    QM_CUDA(cudaMalloc(&d_rcount.p, sizeof(unsigned int)));
+    QM_CUDA(cudaMalloc(&d_x.p, rows_cap * MLP_IN * sizeof(__nv_bfloat16)));
+    QM_CUDA(cudaMalloc(&d_coef.p, rows_cap * 16 * sizeof(float)));
+    QM_CUDA(cudaMalloc(&d_elig.p, rows_cap));
+    QM_CUDA(cudaMalloc(&d_taken.p, sizeof(unsigned long long)));
+    QM_CUDA(cudaMalloc(&d_dba.p, cells * sizeof(float)));
+    QM_CUDA(cudaMemsetAsync(d_partial.p, 0, partial_bytes, stream));
+    QM_CUDA(cudaMemsetAsync(d_failed.p, 0, cells * sizeof(uint32_t), stream));
+    QM_CUDA(cudaMemsetAsync(d_counters.p, 0, 6 * sizeof(unsigned long long), stream));
+    QM_CUDA(cudaMemsetAsync(d_rcount.p, 0, sizeof(unsigned int), stream));
+    QM_CUDA(cudaMemsetAsync(d_taken.p, 0, sizeof(unsigned long long), stream));
+    A.partial = static_cast<float *>(d_partial.p);
+    A.failed = static_cast<uint32_t *>(d_failed.p);
+    A.counters = static_cast<unsigned long long *>(d_counters.p);
+    A.retry = static_cast<uint2 *>(d_retry.p);
+    A.retry_count = static_cast<unsigned int *>(d_rcount.p);
+    const MlpScales &S = net->net.scales;
+    Events ev;
+    QM_CUDA(ev.create());
+    QM_CUDA(cudaEventRecord(ev.e0, stream));
+    for (uint32_t b0 = sb; b0 < se; b0 += batch) {
+        const uint32_t b1 = std::min(se, b0 + batch);
+        const uint32_t rpc = ((b1 - b0 + 127) / 128) * 128;
+        const size_t rows = (size_t)cells * rpc;
+        SurrPaintArgs P{};
+        P.g = A;
+        chunk_range(ctx, P.g, G.tiles, b0, b1);
+        P.x = static_cast<__nv_bfloat16 *>(d_x.p);
+        P.coef = static_cast<float *>(d_coef.p);
+        P.eligible = static_cast<uint8_t *>(d_elig.p);
+        P.rows_per_cell = rpc;
+        for (int k = 0; k < MLP_IN; ++k) {
+            P.in_shift[k] = S.in_shift[k];
+            P.in_scale[k] = S.in_scale[k];
+            P.lo[k] = S.feat_lo[k];
+            P.hi[k] = S.feat_hi[k];
+        }
+        QM_CUDA(cudaMemsetAsync(d_elig.p, 0, rows, stream));
+        surrogate_front_kernel<<<dim3(G.tiles, P.g.n_chunks), 128, 0, stream>>>(scene->dev, P);
+        QM_CUDA(cudaGetLastError());
+        MlpPaintArgs M{};
+        M.x = P.x;
+        M.coef = P.coef;
+        M.eligible = P.eligible;
+        M.rows = rows;
+        M.rows_per_cell = rpc;
+        M.cells = cells;
+        M.partial = A.partial + (size_t)(max_chunks + 1) * cells * GRID_SLOTS;
+        M.source_begin = b0;
+        M.n_sources = b1 - b0;
+        M.retry = A.retry;
+        M.retry_cap = A.retry_cap;
+        M.retry_count = A.retry_count;
+        M.taken = static_cast<unsigned long long *>(d_taken.p);
+        QM_CUDA(mlp_paint(net->net, M, stream));
+    }
+    QM_CUDA(cudaEventRecord(ev.e2, stream));
+    unsigned int n_retry = 0;
+    QM_CUDA(cudaMemcpyAsync(&n_retry, d_rcount.p, sizeof(n_retry), cudaMemcpyDeviceToHost, stream));
+    QM_CUDA(cudaStreamSynchronize(stream));
+    if (n_retry > A.retry_cap)
+        return fail(QM_ERR_CAPACITY, "qm_paint_grid_surrogate: " + std::to_string(n_retry) +
+                                         " paths to re-run, more than the re-run list holds");
+    if (n_retry > 0) {
+        st = rerun_failed(scene, A, static_cast<uint2 *>(d_retry.p), n_retry, max_chunks, cells, stream);
+        if (st != QM_OK) return st;
+    }
+    ReduceArgs R{};
+    R.cells = cells;
+    R.n_chunks = slices;
+    R.partial = A.partial;
+    R.level_min = g.level_min_db;
+    R.bin_db = g.bin_db;
+    R.n_bins = histogram ? g.n_bins : 0;
+    R.dba_scratch = static_cast<float *>(d_dba.p);
+    if (cell_bands) QM_CUDA(cudaMalloc(&d_bands.p, (size_t)cells * 8 * sizeof(float)));
+    if (cell_dba) QM_CUDA(cudaMalloc(&d_dbaout.p, (size_t)cells * sizeof(float)));
+    if (cell_lden) QM_CUDA(cudaMalloc(&d_lden.p, (size_t)cells * sizeof(float)));
+    if (histogram) {
+        QM_CUDA(cudaMalloc(&d_hist.p, g.n_bins * sizeof(uint32_t)));
+        QM_CUDA(cudaMemsetAsync(d_hist.p, 0, g.n_bins * sizeof(uint32_t), stream));
+    }
+    R.cell_bands = static_cast<float *>(d_bands.p);
+    R.cell_dba = static_cast<float *>(d_dbaout.p);
+    R.cell_lden = static_cast<float *>(d_lden.p);
+    R.histogram = static_cast<uint32_t *>(d_hist.p);
+    size_t smem = histogram ? g.n_bins * sizeof(uint32_t) : 0;
+    if (smem > 48 * 1024) QM_CUDA(cudaFuncSetAttribute(reduce_cells_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    reduce_cells_kernel<<<(cells + 255) / 256, 256, smem, stream>>>(R);
+    QM_CUDA(cudaGetLastError());
+    QM_CUDA(cudaEventRecord(ev.e1, stream));
+    unsigned long long counters[6], taken = 0;
+    QM_CUDA(cudaMemcpyAsync(counters, d_counters.p, sizeof(counters), cudaMemcpyDeviceToHost, stream));
+    QM_CUDA(cudaMemcpyAsync(&taken, d_taken.p, sizeof(taken), cudaMemcpyDeviceToHost, stream));
+    if (cell_bands) QM_CUDA(cudaMemcpyAsync(cell_bands, d_bands.p, (size_t)cells * 8 * sizeof(float), cudaMemcpyDeviceToHost, stream));
+    if (cell_dba) QM_CUDA(cudaMemcpyAsync(cell_dba, d_dbaout.p, (size_t)cells * sizeof(float), cudaMemcpyDeviceToHost, stream));
+    if (cell_lden) QM_CUDA(cudaMemcpyAsync(cell_lden, d_lden.p, (size_t)cells * sizeof(float), cudaMemcpyDeviceToHost, stream));
+    if (histogram) QM_CUDA(cudaMemcpyAsync(histogram, d_hist.p, g.n_bins * sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
+    QM_CUDA(cudaStreamSynchronize(stream));
+    float ms = 0.f, front_ms = 0.f;
+    QM_CUDA(cudaEventElapsedTime(&ms, ev.e0, ev.e1));
+    QM_CUDA(cudaEventElapsedTime(&front_ms, ev.e0, ev.e2));
+    if (stats) {
+        stats->paths = counters[0];
+        stats->crossings = counters[1];
+        stats->failed_paths = counters[3];
+        stats->edge_tests = counters[2];
+        stats->vertices = counters[4];
+        stats->candidates = counters[5];
+        stats->kernel_ms = ms;
+        stats->paint_ms = front_ms;
+    }
+    if (surrogate_paths) *surrogate_paths = taken;
+    return QM_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,751 @@
+// The surrogate network's kernels: BF16 tensor-core matrix products with FP32 accumulation
+// (mma.sync m16n8k16), fused five-layer inference with the activations chained through
+// registers, training products for the backward pass, and Adam on FP32 master weights.
+#include "qm_mlp.h"
+
+#include <algorithm>
+#include <cmath>
+
+namespace qm {
+namespace {
+
+__device__ __forceinline__ uint32_t pack_bf16(float lo, float hi) {
+    __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
+    return *reinterpret_cast<uint32_t *>(&v);
+}
+
+// D += A (16x16, row) * B (16x8, col), BF16 in, FP32 accumulate.
+__device__ __forceinline__ void mma_bf16(float (&d)[4], const uint32_t (&a)[4], uint32_t b0, uint32_t b1) {
+    asm volatile(
+        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+        "{%0,%1,%2,%3};"
+        : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+
+__device__ __forceinline__ void ldsm_x4(uint32_t &r0, uint32_t &r1, uint32_t &r2, uint32_t &r3, const void *p) {
+    unsigned a = (unsigned)__cvta_generic_to_shared(p);
+    asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0,%1,%2,%3}, [%4];"
+                 : "=r"(r0), "=r"(r1), "=r"(r2), "=r"(r3)
+                 : "r"(a));
+}
+
+__device__ __forceinline__ void ldsm_x2(uint32_t &r0, uint32_t &r1, const void *p) {
+    unsigned a = (unsigned)__cvta_generic_to_shared(p);
+    asm volatile("ldmatrix.sync.aligned.m8n8.x2.shared.b16 {%0,%1}, [%2];" : "=r"(r0), "=r"(r1) : "r"(a));
+}
+
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
+    unsigned a = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(a), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_wait() {
+    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+// GELU in its erf form, and its derivative.
+__device__ __forceinline__ float gelu(float z) { return 0.5f * z * (1.0f + erff(z * 0.70710678118654752f)); }
+__device__ __forceinline__ float gelu_grad(float z) {
+    return 0.5f * (1.0f + erff(z * 0.70710678118654752f)) + z * 0.39894228040143268f * __expf(-0.5f * z * z);
+}
+
+// ---------------------------------------------------------------------------------------------
+// Fused inference: a CTA of 8 warps takes 128 rows (16 a warp) through all five layers. The
+// weights stream through shared memory in chunks of 64 output rows (cp.async, double buffered);
+// each layer's FP32 results become the next layer's BF16 A fragments in registers (the m16n8
+// accumulator layout is the m16k16 operand layout, two n-tiles per k-tile).
+
+constexpr int FT_ROWS = 128, FT_THREADS = 256;
+constexpr int CH_ROWS = 64, CH_STRIDE = 256 + 8;  // padded rows: conflict-free ldmatrix
+constexpr int CH_ELEMS = CH_ROWS * CH_STRIDE;
+constexpr int CHUNKS = 17;  // 4 per hidden layer, 1 for the output layer
+
+struct FusedArgs {
+    const __nv_bfloat16 *w16;
+    const float *master;
+    float out_shift[MLP_OUT], out_scale[MLP_OUT], lab_lo[MLP_OUT], lab_hi[MLP_OUT];
+    const __nv_bfloat16 *x;
+    size_t rows;
+    float *out;      // forward mode: [rows][8]
+    MlpPaintArgs p;  // paint mode
+};
+
+__device__ __forceinline__ void issue_chunk(const __nv_bfloat16 *w16, int q, __nv_bfloat16 *buf) {
+    const int l = q < 16 ? q / 4 : 4, c = q < 16 ? q % 4 : 0;
+    const int K = l == 0 ? 32 : 256, rows = l == 4 ? 8 : CH_ROWS;
+    const __nv_bfloat16 *src = w16 + mlp_w16_offset(l) + (size_t)c * CH_ROWS * K;
+    const int per_row = K / 8, total = rows * per_row;
+    for (int v = threadIdx.x; v < total; v += FT_THREADS) {
+        int r = v / per_row, k8 = (v - r * per_row) * 8;
+        cp_async16(buf + r * CH_STRIDE + k8, src + (size_t)r * K + k8);
+    }
+}
+
+struct Pipe {
+    __nv_bfloat16 *bufs;
+    const __nv_bfloat16 *w16;
+    int sel;
+    __device__ __forceinline__ const __nv_bfloat16 *begin(int q_next, bool has_next) {
+        if (has_next) issue_chunk(w16, q_next, bufs + (sel ^ 1) * CH_ELEMS);
+        cp_commit();
+        cp_wait<1>();
+        __syncthreads();
+        return bufs + sel * CH_ELEMS;
+    }
+    __device__ __forceinline__ void end() {
+        __syncthreads();
+        sel ^= 1;
+    }
+};
+
+// One chunk of 64 outputs over KT k-tiles of input.
+template <int KT>
+__device__ __forceinline__ void chunk_mma(const __nv_bfloat16 *buf, const uint32_t (&a)[KT][4], float (&acc)[8][4],
+                                          int lane) {
+#pragma unroll
+    for (int nt = 0; nt < 8; ++nt)
+#pragma unroll
+        for (int i = 0; i < 4; ++i) acc[nt][i] = 0.0f;
+    const int j = lane >> 3, i = lane & 7;
+#pragma unroll
+    for (int kt = 0; kt < KT; ++kt) {
+#pragma unroll
+        for (int p = 0; p < 4; ++p) {
+            uint32_t b0, b1, b2, b3;
+            ldsm_x4(b0, b1, b2, b3, buf + (16 * p + i + 8 * (j >> 1)) * CH_STRIDE + 16 * kt + 8 * (j & 1));
+            mma_bf16(acc[2 * p], a[kt], b0, b1);
+            mma_bf16(acc[2 * p + 1], a[kt], b2, b3);
+        }
+    }
+}
+
+// Bias + GELU of a chunk's accumulators into k-tiles 4c..4c+3 of the next layer's A fragments.
+__device__ __forceinline__ void chunk_gelu(const float (&acc)[8][4], const float *bias, int c, int t,
+                                           uint32_t (&next)[16][4]) {
+#pragma unroll
+    for (int nt = 0; nt < 8; ++nt) {
+        int col = 64 * c + 8 * nt + 2 * t;
+        float b0 = __ldg(bias + col), b1 = __ldg(bias + col + 1);
+        uint32_t lo = pack_bf16(gelu(acc[nt][0] + b0), gelu(acc[nt][1] + b1));
+        uint32_t hi = pack_bf16(gelu(acc[nt][2] + b0), gelu(acc[nt][3] + b1));
+        int q = 4 * c + nt / 2;
+        if ((nt & 1) == 0) {
+            next[q][0] = lo;
+            next[q][1] = hi;
+        } else {
+            next[q][2] = lo;
+            next[q][3] = hi;
+        }
+    }
+}
+
+template <int KT>
+__device__ __forceinline__ void hidden_layer(Pipe &pipe, int first_q, const uint32_t (&in)[KT][4], const float *bias,
+                                             uint32_t (&out)[16][4], int lane, bool has_next_tile) {
+    const int t = lane & 3;
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+        int q = first_q + c;
+        const __nv_bfloat16 *buf = pipe.begin((q + 1) % CHUNKS, q + 1 < CHUNKS || has_next_tile);
+        float acc[8][4];
+        chunk_mma<KT>(buf, in, acc, lane);
+        chunk_gelu(acc, bias, c, t, out);
+        pipe.end();
+    }
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(FT_THREADS, 1) mlp_fused_kernel(FusedArgs A) {
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    __shared__ float s_red[8][9];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int g = lane >> 2, t = lane & 3;
+    const size_t n_tiles = (A.rows + FT_ROWS - 1) / FT_ROWS;
+    Pipe pipe{reinterpret_cast<__nv_bfloat16 *>(smem_raw), A.w16, 0};
+    if (blockIdx.x >= n_tiles) return;
+    issue_chunk(A.w16, 0, pipe.bufs);
+    cp_commit();
+    const float *bias[MLP_LAYERS];
+#pragma unroll
+    for (int l = 0; l < MLP_LAYERS; ++l) bias[l] = A.master + mlp_b_offset(l);
+    for (size_t tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {
+        const bool has_next = tile + gridDim.x < n_tiles;
+        const size_t r0 = tile * FT_ROWS + warp * 16 + g, r1 = r0 + 8;
+        // Layer 1 input fragments straight from the feature rows.
+        uint32_t xa[2][4];
+#pragma unroll
+        for (int kt = 0; kt < 2; ++kt) {
+            int col = 16 * kt + 2 * t;
+            const uint32_t *x0 = reinterpret_cast<const uint32_t *>(A.x + r0 * MLP_IN + col);
+            const uint32_t *x1 = reinterpret_cast<const uint32_t *>(A.x + r1 * MLP_IN + col);
+            xa[kt][0] = r0 < A.rows ? __ldg(x0) : 0u;
+            xa[kt][1] = r1 < A.rows ? __ldg(x1) : 0u;
+            xa[kt][2] = r0 < A.rows ? __ldg(x0 + 4) : 0u;
+            xa[kt][3] = r1 < A.rows ? __ldg(x1 + 4) : 0u;
+        }
+        uint32_t ha[16][4], hb[16][4];
+        hidden_layer<2>(pipe, 0, xa, bias[0], ha, lane, has_next);
+        hidden_layer<16>(pipe, 4, ha, bias[1], hb, lane, has_next);
+        hidden_layer<16>(pipe, 8, hb, bias[2], ha, lane, has_next);
+        hidden_layer<16>(pipe, 12, ha, bias[3], hb, lane, has_next);
+        // Output layer: 8 outputs, one n-tile.
+        float y[4] = {0.f, 0.f, 0.f, 0.f};
+        {
+            const __nv_bfloat16 *buf = pipe.begin(0, has_next);
+            const int i = lane & 7, j = (lane >> 3) & 1;
+#pragma unroll
+            for (int kt = 0; kt < 16; ++kt) {
+                uint32_t b0, b1;
+                ldsm_x2(b0, b1, buf + i * CH_STRIDE + 16 * kt + 8 * j);
+                mma_bf16(y, hb[kt], b0, b1);
+            }
+            pipe.end();
+        }
+        const int o = 2 * t;
+        float a00 = (y[0] + __ldg(bias[4] + o)) * A.out_scale[o] + A.out_shift[o];
+        float a01 = (y[1] + __ldg(bias[4] + o + 1)) * A.out_scale[o + 1] + A.out_shift[o + 1];
+        float a10 = (y[2] + __ldg(bias[4] + o)) * A.out_scale[o] + A.out_shift[o];
+        float a11 = (y[3] + __ldg(bias[4] + o + 1)) * A.out_scale[o + 1] + A.out_shift[o + 1];
+        if (MODE == 0) {
+            if (r0 < A.rows) *reinterpret_cast<float2 *>(A.out + r0 * MLP_OUT + o) = make_float2(a00, a01);
+            if (r1 < A.rows) *reinterpret_cast<float2 *>(A.out + r1 * MLP_OUT + o) = make_float2(a10, a11);
+        } else {
+            const MlpPaintArgs &P = A.p;
+            float v[9];
+#pragma unroll
+            for (int k = 0; k < 9; ++k) v[k] = 0.0f;
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const size_t r = h ? r1 : r0;
+                const float x0 = h ? a10 : a00, x1 = h ? a11 : a01;
+                bool use = r < A.rows && P.eligible[r];
+                bool out_of_range = !(x0 >= A.lab_lo[o] - 1.0f && x0 <= A.lab_hi[o] + 1.0f) ||
+                                    !(x1 >= A.lab_lo[o + 1] - 1.0f && x1 <= A.lab_hi[o + 1] + 1.0f);
+                // Any band of the row out of range sends the row to the exact path.
+                unsigned bad = __ballot_sync(0xffffffffu, use && out_of_range);
+                bool row_bad = ((bad >> (lane & ~3)) & 0xfu) != 0;
+                if (use && row_bad) {
+                    if (t == 0) {
+                        uint32_t cell = (uint32_t)(r / P.rows_per_cell), s = (uint32_t)(r % P.rows_per_cell);
+                        unsigned slot = atomicAdd(P.retry_count, 1u);
+                        if (slot < P.retry_cap) P.retry[slot] = make_uint2(cell, P.source_begin + s);
+                    }
+                    use = false;
+                }
+                if (use) {
+                    const float *cf = P.coef + r * 16;
+                    float e0 = exp2f(-x0 * 0.33219280948873623f), e1 = exp2f(-x1 * 0.33219280948873623f);
+                    float d0 = __ldg(cf + o) * e0, d1 = __ldg(cf + o + 1) * e1;
+                    float l = __ldg(cf + 8 + o) * e0 + __ldg(cf + 8 + o + 1) * e1;
+                    v[o] += d0;  // o varies by lane: written into the lane's own two bands
+                    v[o + 1] += d1;
+                    v[8] += l;
+                    if (t == 0) atomicAdd(P.taken, 1ull);
+                }
+            }
+            // v[k] is nonzero only for k in {o, o+1, 8}: sum over the warp per band, then over warps.
+#pragma unroll
+            for (int k = 0; k < 9; ++k) {
+                float s = v[k];
+#pragma unroll
+                for (int m = 16; m > 0; m >>= 1) s += __shfl_xor_sync(0xffffffffu, s, m);
+                v[k] = s;
+            }
+            if (lane == 0)
+#pragma unroll
+                for (int k = 0; k < 9; ++k) s_red[warp][k] = v[k];
+            __syncthreads();
+            if (threadIdx.x < 9) {
+                float s = 0.0f;
+                for (int w = 0; w < 8; ++w) s += s_red[w][threadIdx.x];
+                const size_t row0 = tile * FT_ROWS;
+                const size_t cell = row0 / P.rows_per_cell, slice = (row0 % P.rows_per_cell) / FT_ROWS;
+                float *dst = P.partial + (slice * (size_t)P.cells + cell) * 9 + threadIdx.x;
+                *dst += s;
+            }
+            __syncthreads();
+        }
+    }
+    cp_wait<0>();
+}
+
+// ---------------------------------------------------------------------------------------------
+// Training product: C[M][N] (op) A(m, k) * B(k, n), BF16 operands, FP32 accumulation.
+// A is stored [M][K] (A_MK) or [K][M]; B is stored [N][K] (B_NK) or [K][N]. Tiles of 128 x 128
+// x 32 per CTA of 8 warps (warp tile 64 x 32); split-K over blockIdx.z.
+
+enum { EPI_STORE = 0, EPI_ATOMIC = 1, EPI_BIAS_GELU = 2, EPI_BIAS = 3, EPI_GELU_GRAD = 4 };
+
+struct GemmArgs {
+    const __nv_bfloat16 *a, *b;
+    int M, N, K;
+    int lda, ldb;      // row strides of the stored matrices
+    int k_per_split;   // multiple of 32
+    float *c;          // [M][N] FP32 (EPI_STORE, EPI_ATOMIC, EPI_BIAS: output; EPI_BIAS_GELU: Z)
+    const float *bias; // [N]
+    __nv_bfloat16 *h;  // [M][N] BF16 (EPI_BIAS_GELU: GELU(Z); EPI_GELU_GRAD: dZ of the layer below)
+    const float *z;    // [M][N] (EPI_GELU_GRAD: the layer below's pre-activation)
+};
+
+constexpr int GT_M = 128, GT_N = 128, GT_K = 32, GT_STRIDE = GT_K + 8;
+
+template <bool A_MK, bool B_NK, int EPI>
+__global__ void __launch_bounds__(256) gemm_kernel(GemmArgs G) {
+    __shared__ __align__(16) __nv_bfloat16 As[GT_M * GT_STRIDE];
+    __shared__ __align__(16) __nv_bfloat16 Bs[GT_N * GT_STRIDE];
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int wm = warp >> 2, wn = warp & 3;  // 2 x 4 warps
+    const int m0 = blockIdx.y * GT_M, n0 = blockIdx.x * GT_N;
+    const int k_begin = blockIdx.z * G.k_per_split;
+    const int k_end = min(G.K, k_begin + G.k_per_split);
+    float acc[4][4][4];
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int b = 0; b < 4; ++b)
+#pragma unroll
+            for (int c = 0; c < 4; ++c) acc[a][b][c] = 0.0f;
+    const __nv_bfloat16 zero = __float2bfloat16(0.0f);
+    for (int kb = k_begin; kb < k_end; kb += GT_K) {
+        // Stage the tiles as [row][k] in shared memory.
+        uint4 ra[2], rb[2];
+#pragma unroll
+        for (int i = 0; i < 2; ++i) {
+            int v = tid + 256 * i;
+            if (A_MK) {
+                int r = v >> 2, k = kb + (v & 3) * 8;
+                bool ok = m0 + r < G.M && k < k_end;
+                ra[i] = ok ? *reinterpret_cast<const uint4 *>(G.a + (size_t)(m0 + r) * G.lda + k) : make_uint4(0, 0, 0, 0);
+            } else {
+                int k = kb + (v >> 4), m = m0 + (v & 15) * 8;
+                bool ok = m < G.M && k < k_end;
+                ra[i] = ok ? *reinterpret_cast<const uint4 *>(G.a + (size_t)k * G.lda + m) : make_uint4(0, 0, 0, 0);
+            }
+            if (B_NK) {
+                int r = v >> 2, k = kb + (v & 3) * 8;
+                bool ok = n0 + r < G.N && k < k_end;
+                rb[i] = ok ? *reinterpret_cast<const uint4 *>(G.b + (size_t)(n0 + r) * G.ldb + k) : make_uint4(0, 0, 0, 0);
+            } else {
+                int k = kb + (v >> 4), n = n0 + (v & 15) * 8;
+                bool ok = n < G.N && k < k_end;
+                rb[i] = ok ? *reinterpret_cast<const uint4 *>(G.b + (size_t)k * G.ldb + n) : make_uint4(0, 0, 0, 0);
+            }
+        }
+        __syncthreads();
+#pragma unroll
+        for (int i = 0; i < 2; ++i) {
+            int v = tid + 256 * i;
+            if (A_MK) {
+                *reinterpret_cast<uint4 *>(As + (v >> 2) * GT_STRIDE + (v & 3) * 8) = ra[i];
+            } else {
+                const __nv_bfloat16 *e = reinterpret_cast<const __nv_bfloat16 *>(&ra[i]);
+                int k = v >> 4, m = (v & 15) * 8;
+#pragma unroll
+                for (int q = 0; q < 8; ++q) As[(m + q) * GT_STRIDE + k] = e[q];
+            }
+            if (B_NK) {
+                *reinterpret_cast<uint4 *>(Bs + (v >> 2) * GT_STRIDE + (v & 3) * 8) = rb[i];
+            } else {
+                const __nv_bfloat16 *e = reinterpret_cast<const __nv_bfloat16 *>(&rb[i]);
+                int k = v >> 4, n = (v & 15) * 8;
+#pragma unroll
+                for (int q = 0; q < 8; ++q) Bs[(n + q) * GT_STRIDE + k] = e[q];
+            }
+        }
+        (void)zero;
+        __syncthreads();
+        const int j = lane >> 3, i = lane & 7;
+#pragma unroll
+        for (int kk = 0; kk < GT_K; kk += 16) {
+            uint32_t af[4][4], bf[4][2];
+#pragma unroll
+            for (int mt = 0; mt < 4; ++mt)
+                ldsm_x4(af[mt][0], af[mt][1], af[mt][2], af[mt][3],
+                        As + (wm * 64 + mt * 16 + i + 8 * (j & 1)) * GT_STRIDE + kk + 8 * (j >> 1));
+#pragma unroll
+            for (int p = 0; p < 2; ++p)
+                ldsm_x4(bf[2 * p][0], bf[2 * p][1], bf[2 * p + 1][0], bf[2 * p + 1][1],
+                        Bs + (wn * 32 + 16 * p + i + 8 * (j >> 1)) * GT_STRIDE + kk + 8 * (j & 1));
+#pragma unroll
+            for (int mt = 0; mt < 4; ++mt)
+#pragma unroll
+                for (int nt = 0; nt < 4; ++nt) mma_bf16(acc[mt][nt], af[mt], bf[nt][0], bf[nt][1]);
+        }
+    }
+    const int g = lane >> 2, t = lane & 3;
+#pragma unroll
+    for (int mt = 0; mt < 4; ++mt)
+#pragma unroll
+        for (int nt = 0; nt < 4; ++nt)
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                int m = m0 + wm * 64 + mt * 16 + g + 8 * h;
+                int n = n0 + wn * 32 + nt * 8 + 2 * t;
+                if (m >= G.M || n >= G.N) continue;
+                float v0 = acc[mt][nt][2 * h], v1 = acc[mt][nt][2 * h + 1];
+                size_t idx = (size_t)m * G.N + n;
+                if (EPI == EPI_STORE) {
+                    *reinterpret_cast<float2 *>(G.c + idx) = make_float2(v0, v1);
+                } else if (EPI == EPI_ATOMIC) {
+                    atomicAdd(G.c + idx, v0);
+                    atomicAdd(G.c + idx + 1, v1);
+                } else if (EPI == EPI_BIAS || EPI == EPI_BIAS_GELU) {
+                    v0 += G.bias[n];
+                    v1 += G.bias[n + 1];
+                    *reinterpret_cast<float2 *>(G.c + idx) = make_float2(v0, v1);
+                    if (EPI == EPI_BIAS_GELU)
+                        *reinterpret_cast<uint32_t *>(G.h + idx) = pack_bf16(gelu(v0), gelu(v1));
+                } else {  // EPI_GELU_GRAD
+                    float2 z = *reinterpret_cast<const float2 *>(G.z + idx);
+                    *reinterpret_cast<uint32_t *>(G.h + idx) = pack_bf16(v0 * gelu_grad(z.x), v1 * gelu_grad(z.y));
+                }
+            }
+}
+
+template <bool A_MK, bool B_NK, int EPI>
+cudaError_t gemm(const GemmArgs &g, int splits, cudaStream_t stream) {
+    GemmArgs a = g;
+    int k_tiles = (g.K + GT_K - 1) / GT_K;
+    splits = std::max(1, std::min(splits, k_tiles));
+    a.k_per_split = ((k_tiles + splits - 1) / splits) * GT_K;
+    splits = (g.K + a.k_per_split - 1) / a.k_per_split;
+    dim3 grid((g.N + GT_N - 1) / GT_N, (g.M + GT_M - 1) / GT_M, splits);
+    gemm_kernel<A_MK, B_NK, EPI><<<grid, 256, 0, stream>>>(a);
+    return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------------------------
+// Element-wise kernels.
+
+__global__ void cast_kernel(const float *master, __nv_bfloat16 *w16) {
+    // Matrices only: layer l's [out][in] block of the master vector -> its BF16 block.
+    size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+    if (i >= MLP_W16) return;
+    int l = 0;
+    size_t base16 = 0, base32 = 0;
+    for (; l < MLP_LAYERS; ++l) {
+        size_t n = (size_t)mlp_dim(l + 1) * mlp_dim(l);
+        if (i < base16 + n) break;
+        base16 += n;
+        base32 += n + mlp_dim(l + 1);
+    }
+    w16[i] = __float2bfloat16_rn(master[base32 + (i - base16)]);
+}
+
+__global__ void normalise_kernel(MlpScales s, const float *raw, size_t n, __nv_bfloat16 *out) {
+    size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+    if (i >= n * MLP_IN) return;
+    int f = (int)(i % MLP_IN);
+    out[i] = __float2bfloat16_rn((raw[i] - s.in_shift[f]) * s.in_scale[f]);
+}
+
+// MSE on n rows of 8: dOut = 2 (out - y) / (8 n) as BF16; the loss summed into *loss.
+__global__ void loss_kernel(const float *out, const float *y, size_t n, __nv_bfloat16 *dout, double *loss) {
+    __shared__ float s[256];
+    size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+    float e2 = 0.0f;
+    if (i < n * MLP_OUT) {
+        float d = out[i] - y[i];
+        e2 = d * d;
+        dout[i] = __float2bfloat16_rn(2.0f * d / (float)(n * MLP_OUT));
+    }
+    s[threadIdx.x] = e2;
+    __syncthreads();
+    for (int k = 128; k > 0; k >>= 1) {
+        if (threadIdx.x < k) s[threadIdx.x] += s[threadIdx.x + k];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) atomicAdd(loss, (double)s[0] / (double)(n * MLP_OUT));
+}
+
+// Column sums of a BF16 matrix [n][w] into db (added).
+__global__ void bias_grad_kernel(const __nv_bfloat16 *dz, size_t n, int w, float *db) {
+    int col = blockIdx.x * 32 + (threadIdx.x & 31);
+    int lane_row = threadIdx.x >> 5;  // 8 row lanes
+    float s = 0.0f;
+    if (col < w)
+        for (size_t r = blockIdx.y * 8 + lane_row; r < n; r += 8 * gridDim.y) s += __bfloat162float(dz[r * w + col]);
+    __shared__ float red[8][33];
+    red[lane_row][threadIdx.x & 31] = s;
+    __syncthreads();
+    if (threadIdx.x < 32 && col < w) {
+        float t = 0.0f;
+        for (int k = 0; k < 8; ++k) t += red[k][threadIdx.x];
+        atomicAdd(db + col, t);
+    }
+}
+
+__global__ void adam_kernel(float *p, const float *g, float *m, float *v, size_t n, float lr, float c1, float c2) {
+    size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float b1 = 0.9f, b2 = 0.999f, eps = 1e-8f;
+    float gi = g[i];
+    float mi = b1 * m[i] + (1.0f - b1) * gi;
+    float vi = b2 * v[i] + (1.0f - b2) * gi * gi;
+    m[i] = mi;
+    v[i] = vi;
+    p[i] -= lr * (mi * c1) / (sqrtf(vi * c2) + eps);
+}
+
+__global__ void gather_kernel(const __nv_bfloat16 *x, const float *y, const uint32_t *index, size_t n,
+                              __nv_bfloat16 *bx, float *by) {
+    size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    size_t r = index[i];
+    const uint4 *src = reinterpret_cast<const uint4 *>(x + r * MLP_IN);
+    uint4 *dst = reinterpret_cast<uint4 *>(bx + i * MLP_IN);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) dst[k] = src[k];
+    const float4 *ys = reinterpret_cast<const float4 *>(y + r * MLP_OUT);
+    float4 *yd = reinterpret_cast<float4 *>(by + i * MLP_OUT);
+    yd[0] = ys[0];
+    yd[1] = ys[1];
+}
+
+__device__ __forceinline__ void atomic_min_f(float *a, float v) {
+    int *ai = reinterpret_cast<int *>(a);
+    int old = *ai;
+    while (__int_as_float(old) > v) {
+        int prev = atomicCAS(ai, old, __float_as_int(v));
+        if (prev == old) break;
+        old = prev;
+    }
+}
+__device__ __forceinline__ void atomic_max_f(float *a, float v) {
+    int *ai = reinterpret_cast<int *>(a);
+    int old = *ai;
+    while (__int_as_float(old) < v) {
+        int prev = atomicCAS(ai, old, __float_as_int(v));
+        if (prev == old) break;
+        old = prev;
+    }
+}
+
+// One thread per (row block, column): sums over its rows, then one atomic each.
+__global__ void stats_kernel(const float *rows, const uint8_t *keep, size_t n, int w, double *sum, double *sumsq,
+                             float *lo, float *hi) {
+    int col = threadIdx.x % w;
+    int lanes = blockDim.x / w;
+    int sub = threadIdx.x / w;
+    if (sub >= lanes) return;
+    double s = 0.0, s2 = 0.0;
+    float mn = INFINITY, mx = -INFINITY;
+    for (size_t r = blockIdx.x * (size_t)lanes + sub; r < n; r += (size_t)gridDim.x * lanes) {
+        if (keep && !keep[r]) continue;
+        float v = rows[r * w + col];
+        s += v;
+        s2 += (double)v * v;
+        mn = fminf(mn, v);
+        mx = fmaxf(mx, v);
+    }
+    atomicAdd(sum + col, s);
+    atomicAdd(sumsq + col, s2);
+    atomic_min_f(lo + col, mn);
+    atomic_max_f(hi + col, mx);
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------------------------
+// Host side.
+
+namespace {
+
+cudaError_t set_fused_smem() {
+    const int smem = 2 * CH_ELEMS * (int)sizeof(__nv_bfloat16);
+    cudaError_t e = cudaFuncSetAttribute(mlp_fused_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(mlp_fused_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    return e;
+}
+
+FusedArgs fused_args(const MlpDev &net) {
+    FusedArgs a{};
+    a.w16 = net.w16;
+    a.master = net.master;
+    for (int o = 0; o < MLP_OUT; ++o) {
+        a.out_shift[o] = net.scales.out_shift[o];
+        a.out_scale[o] = net.scales.out_scale[o];
+        a.lab_lo[o] = net.scales.lab_lo[o];
+        a.lab_hi[o] = net.scales.lab_hi[o];
+    }
+    return a;
+}
+
+unsigned fused_grid(size_t rows) {
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    size_t tiles = (rows + FT_ROWS - 1) / FT_ROWS;
+    return (unsigned)std::max<size_t>(1, std::min<size_t>(tiles, (size_t)sms));
+}
+
+}  // namespace
+
+cudaError_t mlp_cast(const MlpDev &net, cudaStream_t stream) {
+    cast_kernel<<<(unsigned)((MLP_W16 + 255) / 256), 256, 0, stream>>>(net.master, net.w16);
+    return cudaGetLastError();
+}
+
+cudaError_t mlp_normalise(const MlpScales &s, const float *raw, size_t n, __nv_bfloat16 *out, cudaStream_t stream) {
+    if (n == 0) return cudaSuccess;
+    size_t total = n * MLP_IN;
+    normalise_kernel<<<(unsigned)((total + 255) / 256), 256, 0, stream>>>(s, raw, n, out);
+    return cudaGetLastError();
+}
+
+cudaError_t mlp_forward(const MlpDev &net, const __nv_bfloat16 *x, size_t n, float *out, cudaStream_t stream) {
+    if (n == 0) return cudaSuccess;
+    cudaError_t e = set_fused_smem();
+    if (e != cudaSuccess) return e;
+    FusedArgs a = fused_args(net);
+    a.x = x;
+    a.rows = n;
+    a.out = out;
+    mlp_fused_kernel<0><<<fused_grid(n), FT_THREADS, 2 * CH_ELEMS * sizeof(__nv_bfloat16), stream>>>(a);
+    return cudaGetLastError();
+}
+
+cudaError_t mlp_paint(const MlpDev &net, const MlpPaintArgs &p, cudaStream_t stream) {
+    if (p.rows == 0) return cudaSuccess;
+    cudaError_t e = set_fused_smem();
+    if (e != cudaSuccess) return e;
+    FusedArgs a = fused_args(net);
+    a.x = p.x;
+    a.rows = p.rows;
+    a.p = p;
+    mlp_fused_kernel<1><<<fused_grid(p.rows), FT_THREADS, 2 * CH_ELEMS * sizeof(__nv_bfloat16), stream>>>(a);
+    return cudaGetLastError();
+}
+
+struct MlpWork {
+    size_t max_rows = 0;
+    float *z[MLP_LAYERS] = {};           // pre-activations (the last: the outputs)
+    __nv_bfloat16 *h[MLP_LAYERS - 1] = {};  // GELU of the hidden pre-activations
+    __nv_bfloat16 *dz[2] = {};
+    __nv_bfloat16 *dout = nullptr;
+};
+
+MlpWork *mlp_work_create(size_t max_rows) {
+    MlpWork *w = new MlpWork;
+    w->max_rows = max_rows;
+    bool ok = true;
+    for (int l = 0; l < MLP_LAYERS; ++l) ok &= cudaMalloc(&w->z[l], max_rows * mlp_dim(l + 1) * sizeof(float)) == cudaSuccess;
+    for (int l = 0; l < MLP_LAYERS - 1; ++l)
+        ok &= cudaMalloc(&w->h[l], max_rows * MLP_HID * sizeof(__nv_bfloat16)) == cudaSuccess;
+    for (int k = 0; k < 2; ++k) ok &= cudaMalloc(&w->dz[k], max_rows * MLP_HID * sizeof(__nv_bfloat16)) == cudaSuccess;
+    ok &= cudaMalloc(&w->dout, max_rows * MLP_OUT * sizeof(__nv_bfloat16)) == cudaSuccess;
+    if (!ok) {
+        mlp_work_free(w);
+        return nullptr;
+    }
+    return w;
+}
+
+void mlp_work_free(MlpWork *w) {
+    if (!w) return;
+    for (auto p : w->z) cudaFree(p);
+    for (auto p : w->h) cudaFree(p);
+    for (auto p : w->dz) cudaFree(p);
+    cudaFree(w->dout);
+    delete w;
+}
+
+cudaError_t mlp_gradients(const MlpDev &net, MlpWork *w, const __nv_bfloat16 *x, const float *y, size_t n,
+                          float *grads, double *loss, cudaStream_t stream) {
+    if (n == 0 || n > w->max_rows || n % 8 != 0) return cudaErrorInvalidValue;
+    cudaError_t e;
+    if ((e = cudaMemsetAsync(grads, 0, MLP_WEIGHTS * sizeof(float), stream)) != cudaSuccess) return e;
+    if ((e = cudaMemsetAsync(loss, 0, sizeof(double), stream)) != cudaSuccess) return e;
+    const int M = (int)n;
+    // Forward, keeping the pre-activations.
+    const __nv_bfloat16 *in = x;
+    for (int l = 0; l < MLP_LAYERS; ++l) {
+        GemmArgs g{};
+        g.a = in;
+        g.lda = mlp_dim(l);
+        g.b = net.w16 + mlp_w16_offset(l);
+        g.ldb = mlp_dim(l);
+        g.M = M;
+        g.N = mlp_dim(l + 1);
+        g.K = mlp_dim(l);
+        g.c = w->z[l];
+        g.bias = net.master + mlp_b_offset(l);
+        if (l < MLP_LAYERS - 1) {
+            g.h = w->h[l];
+            e = gemm<true, true, EPI_BIAS_GELU>(g, 1, stream);
+            in = w->h[l];
+        } else {
+            e = gemm<true, true, EPI_BIAS>(g, 1, stream);
+        }
+        if (e != cudaSuccess) return e;
+    }
+    size_t outs = n * MLP_OUT;
+    loss_kernel<<<(unsigned)((outs + 255) / 256), 256, 0, stream>>>(w->z[MLP_LAYERS - 1], y, n, w->dout, loss);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    // Backward.
+    const __nv_bfloat16 *dz = w->dout;
+    int flip = 0;
+    for (int l = MLP_LAYERS - 1; l >= 0; --l) {
+        const int out_w = mlp_dim(l + 1), in_w = mlp_dim(l);
+        const __nv_bfloat16 *layer_in = l > 0 ? w->h[l - 1] : x;
+        GemmArgs g{};
+        g.a = dz;
+        g.lda = out_w;
+        g.b = layer_in;
+        g.ldb = in_w;
+        g.M = out_w;
+        g.N = in_w;
+        g.K = M;
+        g.c = grads + mlp_w_offset(l);
+        int splits = std::max(1, std::min(128, M / 256));
+        if ((e = gemm<false, false, EPI_ATOMIC>(g, splits, stream)) != cudaSuccess) return e;
+        dim3 bg((out_w + 31) / 32, (unsigned)std::max<size_t>(1, std::min<size_t>(256, n / 64)));
+        bias_grad_kernel<<<bg, 256, 0, stream>>>(dz, n, out_w, grads + mlp_b_offset(l));
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+        if (l > 0) {
+            GemmArgs d{};
+            d.a = dz;
+            d.lda = out_w;
+            d.b = net.w16 + mlp_w16_offset(l);
+            d.ldb = in_w;
+            d.M = M;
+            d.N = in_w;
+            d.K = out_w;
+            d.z = w->z[l - 1];
+            d.h = w->dz[flip];
+            if ((e = gemm<true, false, EPI_GELU_GRAD>(d, 1, stream)) != cudaSuccess) return e;
+            dz = w->dz[flip];
+            flip ^= 1;
+        }
+    }
+    return cudaSuccess;
+}
+
+cudaError_t mlp_adam(MlpDev &net, const float *grads, float lr, int step, cudaStream_t stream) {
+    float c1 = 1.0f / (1.0f - std::pow(0.9f, (float)step)), c2 = 1.0f / (1.0f - std::pow(0.999f, (float)step));
+    adam_kernel<<<(unsigned)((MLP_WEIGHTS + 255) / 256), 256, 0, stream>>>(net.master, grads, net.adam_m, net.adam_v,
+                                                                          MLP_WEIGHTS, lr, c1, c2);
+    cudaError_t e = cudaGetLastError();
+    return e != cudaSuccess ? e : mlp_cast(net, stream);
+}
+
+cudaError_t mlp_gather(const __nv_bfloat16 *x, const float *y, const uint32_t *index, size_t n, __nv_bfloat16 *bx,
+                       float *by, cudaStream_t stream) {
+    if (n == 0) return cudaSuccess;
+    gather_kernel<<<(unsigned)((n + 255) / 256), 256, 0, stream>>>(x, y, index, n, bx, by);
+    return cudaGetLastError();
+}
+
+cudaError_t mlp_column_stats(const float *rows, const uint8_t *keep, size_t n, int w, double *sum, double *sumsq,
+                             float *lo, float *hi, cudaStream_t stream) {
+    if (n == 0) return cudaSuccess;
+    int lanes = 256 / w;
+    unsigned blocks = (unsigned)std::max<size_t>(1, std::min<size_t>(1184, (n + lanes - 1) / lanes));
+    stats_kernel<<<blocks, lanes * w, 0, stream>>>(rows, keep, n, w, sum, sumsq, lo, hi);
+    return cudaGetLastError();
+}
+
+}  // namespace qm

@@ -62,6 +62,24 @@ def lib():
         L.qm_flight_grid.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_size_t,
                                      C.POINTER(abi.FlightGridDesc), _F, _F, _F]
         L.qm_flight_grid.restype = C.c_int
+        P = C.POINTER(C.c_void_p)
+        L.qm_surrogate_create.argtypes = [C.c_void_p, _F, P]
+        L.qm_surrogate_create.restype = C.c_int
+        L.qm_surrogate_free.argtypes = [C.c_void_p]
+        L.qm_surrogate_params.argtypes = [C.c_void_p, _F]
+        L.qm_surrogate_params.restype = C.c_int
+        L.qm_surrogate_samples.argtypes = [C.c_void_p, C.POINTER(abi.GridDesc), _F, _F, C.POINTER(C.c_uint8)]
+        L.qm_surrogate_samples.restype = C.c_int
+        L.qm_surrogate_forward.argtypes = [C.c_void_p, _F, C.c_size_t, _F]
+        L.qm_surrogate_forward.restype = C.c_int
+        L.qm_surrogate_gradients.argtypes = [C.c_void_p, _F, _F, C.c_size_t, _F, _D]
+        L.qm_surrogate_gradients.restype = C.c_int
+        L.qm_surrogate_train.argtypes = [C.c_void_p, C.c_void_p, C.POINTER(abi.GridDesc), C.c_size_t,
+                                         C.POINTER(abi.TrainConfig), _D, _U64]
+        L.qm_surrogate_train.restype = C.c_int
+        L.qm_paint_grid_surrogate.argtypes = [C.c_void_p, C.POINTER(abi.GridDesc), C.c_void_p, _F, _F, _F, _U32,
+                                              C.POINTER(abi.PaintStats), _U64]
+        L.qm_paint_grid_surrogate.restype = C.c_int
         if L.qm_abi_version() != abi.ABI_VERSION:
             raise QmError(abi.QM_ERR_UNSUPPORTED, "library ABI version mismatch")
         _lib = L
@@ -163,6 +181,39 @@ class DeviceScene:
                                              vertices=stats.vertices, candidates=stats.candidates,
                                              kernel_ms=stats.kernel_ms, paint_ms=stats.paint_ms)
 
+    def surrogate_samples(self, grid):
+        """Every path of `grid`: (raw features [rows][32], exact A_boundary labels [rows][8] dB,
+        eligible [rows]) with row = cell * n_sources + source offset."""
+        n_src = (grid.source_end - grid.source_begin) if grid.source_end > grid.source_begin else len(self.scene.sources)
+        rows = grid.cells * n_src
+        g = abi.grid_desc(grid)
+        f = np.zeros((rows, 32), np.float32)
+        lab = np.zeros((rows, 8), np.float32)
+        e = np.zeros(rows, np.uint8)
+        _check(lib().qm_surrogate_samples(self.handle, C.byref(g), abi.ptr(f, C.c_float), abi.ptr(lab, C.c_float),
+                                          e.ctypes.data_as(C.POINTER(C.c_uint8))), self.ctx.handle)
+        return f, lab, e.astype(bool)
+
+    def paint_grid_surrogate(self, grid, net, histogram=True):
+        """The painter with the surrogate: like paint_grid, plus stats["surrogate_paths"]."""
+        g = abi.grid_desc(grid)
+        cells = grid.cells
+        bands = np.zeros((cells, 8), np.float32)
+        dba = np.zeros(cells, np.float32)
+        lden = np.zeros(cells, np.float32)
+        hist = np.zeros(grid.n_bins, np.uint32) if histogram else None
+        stats = abi.PaintStats()
+        taken = C.c_uint64()
+        _check(lib().qm_paint_grid_surrogate(self.handle, C.byref(g), net.handle, abi.ptr(bands, C.c_float),
+                                             abi.ptr(dba, C.c_float), abi.ptr(lden, C.c_float),
+                                             abi.ptr(hist, C.c_uint32) if histogram else None, C.byref(stats),
+                                             C.byref(taken)), self.ctx.handle)
+        return bands, dba, lden, hist, dict(paths=stats.paths, failed_paths=stats.failed_paths,
+                                             crossings=stats.crossings, edge_tests=stats.edge_tests,
+                                             vertices=stats.vertices, candidates=stats.candidates,
+                                             kernel_ms=stats.kernel_ms, paint_ms=stats.paint_ms,
+                                             surrogate_paths=taken.value)
+
     def evaluate_pairs(self, receiver_xy_m, receiver_height_m, own_footprint, point_of_receiver, source_of_pair,
                        receiver_of_pair, band_weight, n_points, point_bands=None):
         rxy = np.ascontiguousarray(np.asarray(receiver_xy_m, dtype=np.float64).reshape(-1, 2))
@@ -201,3 +252,78 @@ class DeviceScene:
                                        abi.ptr(t, C.c_double), abi.ptr(flags, C.c_uint32),
                                        abi.ptr(status, C.c_uint32)), self.ctx.handle)
         return counts, edges, t, flags, status
+
+
+def init_params(seed=0):
+    """A fresh parameter vector: He-normal weights, zero biases, identity normalisation and
+    unbounded ranges (training sets them)."""
+    rng = np.random.default_rng(seed)
+    p = np.zeros(abi.SURR_PARAMS, np.float32)
+    o = 0
+    d = abi.SURR_DIMS
+    for k in range(5):
+        n = d[k + 1] * d[k]
+        p[o:o + n] = rng.normal(0.0, np.sqrt(2.0 / d[k]), n).astype(np.float32)
+        o += n + d[k + 1]
+    q = abi.SURR_WEIGHTS
+    p[q + 32:q + 64] = 1.0            # in_scale
+    p[q + 72:q + 80] = 1.0            # out_scale
+    p[q + 80:q + 112] = -3e38         # feat_lo
+    p[q + 112:q + 144] = 3e38         # feat_hi
+    p[q + 144:q + 152] = -3e38        # lab_lo
+    p[q + 152:q + 160] = 3e38         # lab_hi
+    return p
+
+
+class Surrogate:
+    """The learned A_boundary network on a device (qm_surrogate_*)."""
+
+    def __init__(self, ctx, params=None, seed=0):
+        self.ctx = ctx
+        p = np.ascontiguousarray(init_params(seed) if params is None else params, dtype=np.float32)
+        if p.shape != (abi.SURR_PARAMS,):
+            raise ValueError(f"params must hold {abi.SURR_PARAMS} floats")
+        self.handle = C.c_void_p()
+        _check(lib().qm_surrogate_create(ctx.handle, abi.ptr(p, C.c_float), C.byref(self.handle)), ctx.handle)
+
+    def close(self):
+        if self.handle:
+            lib().qm_surrogate_free(self.handle)
+            self.handle = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def params(self):
+        p = np.zeros(abi.SURR_PARAMS, np.float32)
+        _check(lib().qm_surrogate_params(self.handle, abi.ptr(p, C.c_float)), self.ctx.handle)
+        return p
+
+    def forward(self, features):
+        x = np.ascontiguousarray(features, dtype=np.float32).reshape(-1, 32)
+        out = np.zeros((len(x), 8), np.float32)
+        _check(lib().qm_surrogate_forward(self.handle, abi.ptr(x, C.c_float), len(x), abi.ptr(out, C.c_float)),
+               self.ctx.handle)
+        return out
+
+    def gradients(self, features, labels):
+        x = np.ascontiguousarray(features, dtype=np.float32).reshape(-1, 32)
+        y = np.ascontiguousarray(labels, dtype=np.float32).reshape(-1, 8)
+        g = np.zeros(abi.SURR_WEIGHTS, np.float32)
+        loss = C.c_double()
+        _check(lib().qm_surrogate_gradients(self.handle, abi.ptr(x, C.c_float), abi.ptr(y, C.c_float), len(x),
+                                            abi.ptr(g, C.c_float), C.byref(loss)), self.ctx.handle)
+        return g, loss.value
+
+    def train(self, device_scene, grids, epochs=4, batch=16384, learning_rate=2e-3, seed=1, max_samples=0):
+        """Trains on every eligible path of `grids`; returns (loss per epoch, samples used)."""
+        descs = (abi.GridDesc * len(grids))(*[abi.grid_desc(g) for g in grids])
+        cfg = abi.TrainConfig(epochs, batch, learning_rate, seed, max_samples, 0)
+        hist = np.zeros(epochs, np.float64)
+        n = C.c_uint64()
+        _check(lib().qm_surrogate_train(self.handle, device_scene.handle, descs, len(grids), C.byref(cfg),
+                                        abi.ptr(hist, C.c_double), C.byref(n)), self.ctx.handle)
+        return hist, n.value

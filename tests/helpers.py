@@ -52,3 +52,15 @@ class Stock:
 
 def square(cx, cy, half):
     return [(cx - half, cy - half), (cx + half, cy - half), (cx + half, cy + half), (cx - half, cy + half)]
+
+
+def point_sources(stock, points_m, level_db=90.0, height_m=0.05):
+    """Point sources at `points_m` (metres), every band and period at `level_db`."""
+    src = np.zeros(len(points_m), dtype=abi.SOURCE_DTYPE)
+    for k, p in enumerate(points_m):
+        x, y = stock.steps(p)
+        src[k]["x"], src[k]["y"] = x, y
+        src[k]["height_m"] = height_m
+        src[k]["ground_factor"] = -1.0
+        src[k]["energy"][:] = 10.0 ** (level_db / 10.0)
+    return src
