@@ -63,7 +63,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="terrain", choices=["terrain", "road", "flights"])
+    ap.add_argument("--workload", default="terrain", choices=["terrain", "road", "flights", "surrogate"])
     ap.add_argument("--slices", type=int, default=8, help="terrain: source-list slices (a step paints one)")
     ap.add_argument("--sources", type=int, default=0,
                     help="paint only the first N sources (a small case for profiling; 0: all)")
@@ -243,6 +243,8 @@ def main():
         return reference_arm(args, rank, world)
     if args.workload == "flights":
         return flights(args, rank, world, local)
+    if args.workload == "surrogate":
+        return surrogate(args, rank, world, local)
     import torch
     from quietmap_b200 import native
     scene, steps, desc = workload(args.workload, rank, args.slices, args.sources)
@@ -392,6 +394,77 @@ def flights(args, rank, world, local):
             "config": {"workload": "1024^2 cells at 100 m x 2000 flights x 50 segments, 10 types, reach 25 km, "
                                    "timed through the C ABI call (host buffers in and out)"},
             "clocks": clocks.summary(), "gpu_launches": 2 * args.steps,
+        }), flush=True)
+    ctx.close()
+
+
+def surrogate(args, rank, world, local):
+    """The surrogate painter against the exact painter on the config-1 style 2048^2 square (the
+    1 km road square with 2048 x 2048 receivers at 0.469 m): the network is trained first (50 M
+    exact paths of the same geometry, untimed), then each step paints one seeded 16 x 8 tile
+    against every source with both painters."""
+    import torch
+    from quietmap_b200 import native, scenes
+    scene, full = scenes.road_square(receivers=2048)
+    ctx = native.Context(local if world > 1 else 0)
+    dev = ctx.scene(scene)
+    net = native.Surrogate(ctx, seed=1)
+
+    def coarse(n, off):
+        sp = (scene.extent_steps[0] - 2 * off) // n
+        return scenes.Grid(origin=(off, off), spacing=sp, nx=n, ny=n)
+
+    t0 = time.perf_counter()
+    hist, n_train = net.train(dev, [coarse(24, 37 + 101 * k) for k in range(4)], epochs=3, batch=16384,
+                              learning_rate=2e-3, seed=3, max_samples=50_000_000)
+    train_s = time.perf_counter() - t0
+    # Held-out paths: the network against the exact labels.
+    f, lab, ok = dev.surrogate_samples(scenes.Grid(origin=(555, 777), spacing=7001, nx=4, ny=4, source_end=40000))
+    err = np.abs(net.forward(f[ok]) - lab[ok])
+    rng = np.random.default_rng(2000 + rank)
+    tiles = []
+    for _ in range(max(args.steps + args.warmup, 1)):
+        tx, ty = int(rng.integers(0, full.nx // 16)), int(rng.integers(0, full.ny // 8))
+        tiles.append(scenes.Grid(origin=(full.origin[0] + tx * 16 * full.spacing, full.origin[1] + ty * 8 * full.spacing),
+                                 spacing=full.spacing, nx=16, ny=8))
+    flush = torch.empty(64 << 20, dtype=torch.float32, device="cuda")
+    for i in range(args.warmup):
+        dev.paint_grid_surrogate(tiles[i], net)
+        dev.paint_grid(tiles[i])
+    s_ms = e_ms = 0.0
+    paths = taken = 0
+    cell_err = []
+    with ClockSampler(local) as clocks:
+        for i in range(args.steps):
+            g = tiles[args.warmup + i]
+            flush.zero_()
+            torch.cuda.synchronize()
+            sb, sdba, _, _, sst = dev.paint_grid_surrogate(g, net)
+            flush.zero_()
+            torch.cuda.synchronize()
+            eb, edba, _, _, est = dev.paint_grid(g)
+            s_ms += sst["kernel_ms"]
+            e_ms += est["kernel_ms"]
+            paths += sst["paths"]
+            taken += sst["surrogate_paths"]
+            cell_err.append(np.abs(sdba - edba))
+    cell_err = np.concatenate(cell_err)
+    if rank == 0:
+        value, exact = paths / (s_ms / 1e3), paths / (e_ms / 1e3)
+        print(json.dumps({
+            "metric": METRIC, "value": value, "unit": "paths/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": s_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "bf16 network (fp32 accumulate), f32 path code",
+            "data": "synthetic (seeded road square geometry)",
+            "config": {"workload": "surrogate painter, road square 1 km with 2048^2 receivers (0.469 m): a step is one "
+                                   "seeded 16x8 tile x 77,354 point sources", "l2": "flushed between painters"},
+            "exact_value": exact, "speedup_vs_exact": value / exact, "surrogate_share": taken / max(paths, 1),
+            "path_error_db": {"p50": float(np.percentile(err, 50)), "p99": float(np.percentile(err, 99)),
+                              "samples": int(err.size)},
+            "cell_dba_error_db": {"p50": float(np.median(cell_err)), "p99": float(np.percentile(cell_err, 99)),
+                                  "max": float(cell_err.max())},
+            "training": {"samples": int(n_train), "epochs": 3, "seconds": train_s, "loss": [float(v) for v in hist]},
+            "clocks": clocks.summary(), "gpu_launches": args.steps * 5,
         }), flush=True)
     ctx.close()
 
