@@ -220,6 +220,30 @@ class TrainConfig(C.Structure):
     ]
 
 
+class TileDesc(C.Structure):
+    _fields_ = [
+        ("origin", C.c_int32 * 2),
+        ("spacing", C.c_int32),
+        ("nx", C.c_int32),
+        ("ny", C.c_int32),
+        ("height_m", C.c_float),
+        ("source_begin", C.c_uint32),
+        ("source_end", C.c_uint32),
+        ("cell_offset", C.c_uint64),
+    ]
+
+
+class TileConfig(C.Structure):
+    _fields_ = [("block_w", C.c_uint32), ("block_h", C.c_uint32), ("threads", C.c_uint32), ("chunk", C.c_uint32)]
+
+
+TILE_BUCKETS, TILE_CANDIDATES = 4, 25
+
+
+class TuneTable(C.Structure):
+    _fields_ = [("bucket", TileConfig * TILE_BUCKETS)]
+
+
 def grid_desc(grid):
     g = GridDesc()
     g.origin[0], g.origin[1] = grid.origin

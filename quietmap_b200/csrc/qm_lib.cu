@@ -13,6 +13,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <memory>
 #include <mutex>
 #include <random>
 #include <string>
@@ -20,10 +21,12 @@
 
 #include "../../include/qm_batch.h"
 #include "../../include/qm_surrogate.h"
+#include "../../include/qm_tiles.h"
 #include "qm_aircraft.cuh"
 #include "qm_kernels.cuh"
 #include "qm_mlp.h"
 #include "qm_surrogate.cuh"
+#include "qm_tiles.cuh"
 #include "qm_warp.cuh"
 
 #include <climits>
@@ -442,7 +445,12 @@ void grid_receivers(const qm_scene *s, const qm_grid_desc *g, std::vector<float>
     for (size_t c = 0; c < cells; ++c) own[c] = dense_fp(s, own64[c]);
 }
 
-bool terrain_caps(const qm_scene *s) { return s->dem_nx != 0; }
+// The larger per-path capacities: terrain scenes, and flat scenes whose rays may run longer than
+// 1.5 km (more crossings than the flat capacities hold).
+bool terrain_caps(const qm_scene *s) {
+    double diagonal_m = std::hypot((double)s->extent[0], (double)s->extent[1]) * s->step_m;
+    return s->dem_nx != 0 || diagonal_m > 1500.0;
+}
 
 // Re-runs a grid call's failed paths in (cell, source) order with large per-path capacities and
 // sums them into the partial slice `slice`.
@@ -1882,6 +1890,435 @@ qm_status qm_paint_grid_surrogate(qm_scene *scene, const qm_grid_desc *grid, qm_
         stats->paint_ms = front_ms;
     }
     if (surrogate_paths) *surrogate_paths = taken;
+    return QM_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------------------------
+// Batches of uneven tiles (include/qm_tiles.h).
+
+struct qm_batch_plan {
+    qm_scene *scene = nullptr;
+    uint64_t n_cells = 0;
+    bool use_graph = false;
+    std::vector<TileDev> tiles;
+    struct Launch {
+        int threads = 128;
+        uint32_t n_items = 0, grid = 0;
+        Scratch items, next;
+    };
+    std::vector<Launch> launches;  // one per threads-per-CTA value in use
+    Scratch d_tiles, d_cell_tile, d_rcv_xy, d_alt, d_own, d_partial, d_retry, d_rcount, d_counters, d_retry_acc,
+        d_bands, d_dba, d_lden;
+    uint32_t retry_cap = 0;
+    size_t partial_slots = 0;
+    float lden_w[3];
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    ~qm_batch_plan() {
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+    }
+};
+
+namespace {
+
+const qm_tile_config TILE_BLOCKS[5] = {{16, 8, 128, 0}, {16, 16, 256, 0}, {32, 16, 128, 0}, {32, 32, 256, 0}, {64, 64, 256, 0}};
+const uint32_t TILE_CHUNKS[5] = {128, 256, 512, 1024, 2048};
+
+qm_tile_config tile_candidate(int k) {
+    qm_tile_config c = TILE_BLOCKS[k / 5];
+    c.chunk = TILE_CHUNKS[k % 5];
+    return c;
+}
+
+bool tile_config_ok(const qm_tile_config &c) {
+    return c.block_w >= 8 && c.block_w <= 64 && c.block_w % 8 == 0 && c.block_h >= 8 && c.block_h <= 64 &&
+           c.block_h % 8 == 0 && (c.threads == 128 || c.threads == 256) && c.chunk >= 32 && c.chunk <= 65536;
+}
+
+// The batch's launches (queue resets, persistent CTAs) on the stream, graph or not.
+cudaError_t batch_launch(qm_batch_plan *P, cudaStream_t stream) {
+    cudaError_t e;
+    if ((e = cudaMemsetAsync(P->d_rcount.p, 0, sizeof(unsigned int), stream)) != cudaSuccess) return e;
+    if ((e = cudaMemsetAsync(P->d_counters.p, 0, 6 * sizeof(unsigned long long), stream)) != cudaSuccess) return e;
+    if ((e = cudaMemsetAsync(P->d_retry_acc.p, 0, P->n_cells * GRID_SLOTS * sizeof(float), stream)) != cudaSuccess)
+        return e;
+    const bool terrain = terrain_caps(P->scene);
+    for (auto &L : P->launches) {
+        if ((e = cudaMemsetAsync(L.next.p, 0, sizeof(unsigned int), stream)) != cudaSuccess) return e;
+        BatchArgs B{};
+        B.tiles = static_cast<TileDev *>(P->d_tiles.p);
+        B.items = static_cast<WorkItem *>(L.items.p);
+        B.n_items = L.n_items;
+        B.next = static_cast<unsigned int *>(L.next.p);
+        B.rcv_alt = static_cast<float *>(P->d_alt.p);
+        B.rcv_own = static_cast<uint32_t *>(P->d_own.p);
+        B.partial = static_cast<float *>(P->d_partial.p);
+        B.retry = static_cast<uint2 *>(P->d_retry.p);
+        B.retry_cap = P->retry_cap;
+        B.retry_count = static_cast<unsigned int *>(P->d_rcount.p);
+        B.counters = static_cast<unsigned long long *>(P->d_counters.p);
+        for (int k = 0; k < 3; ++k) B.lden_w[k] = P->lden_w[k];
+        B.want_fav = P->scene->any_favourable;
+        if (L.threads == 256) {
+            if (terrain)
+                batch_paint_kernel<CapsTerrain, 256><<<L.grid, 256, 0, stream>>>(P->scene->dev, B);
+            else
+                batch_paint_kernel<CapsFlat, 256><<<L.grid, 256, 0, stream>>>(P->scene->dev, B);
+        } else {
+            if (terrain)
+                batch_paint_kernel<CapsTerrain, 128><<<L.grid, 128, 0, stream>>>(P->scene->dev, B);
+            else
+                batch_paint_kernel<CapsFlat, 128><<<L.grid, 128, 0, stream>>>(P->scene->dev, B);
+        }
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
+
+}  // namespace
+
+extern "C" {
+
+uint32_t qm_tile_bucket(const qm_tile_desc *tile) {
+    int side = std::max(tile->nx, tile->ny);
+    return side < 64 ? 0u : side < 128 ? 1u : side < 256 ? 2u : 3u;
+}
+
+void qm_tune_default(qm_tune_table *table) {
+    for (int b = 0; b < QM_TILE_BUCKETS; ++b) table->bucket[b] = qm_tile_config{16, 8, 128, 512};
+}
+
+void qm_batch_plan_free(qm_batch_plan *plan) {
+    if (!plan) return;
+    std::lock_guard<std::mutex> guard(plan->scene->ctx->lock);
+    cudaSetDevice(plan->scene->ctx->device);
+    delete plan;
+}
+
+qm_status qm_batch_plan_create(qm_scene *scene, const qm_tile_desc *tiles, size_t n_tiles, uint64_t n_cells,
+                               const qm_tune_table *table, uint32_t flags, qm_batch_plan **out) {
+    if (!scene || !out || (n_tiles && !tiles)) return fail(QM_ERR_ARGUMENT, "qm_batch_plan_create: null scene, tiles or out");
+    if (n_tiles == 0 || n_tiles > (1u << 20)) return fail(QM_ERR_ARGUMENT, "qm_batch_plan_create: 1 to 2^20 tiles");
+    if (n_cells == 0 || n_cells > (1ull << 31)) return fail(QM_ERR_ARGUMENT, "qm_batch_plan_create: n_cells in [1, 2^31]");
+    qm_tune_table tab;
+    if (table)
+        tab = *table;
+    else
+        qm_tune_default(&tab);
+    for (int b = 0; b < QM_TILE_BUCKETS; ++b)
+        if (!tile_config_ok(tab.bucket[b]))
+            return fail(QM_ERR_ARGUMENT, "qm_batch_plan_create: table bucket " + std::to_string(b) +
+                                             ": block sides multiples of 8 in [8, 64], threads 128 or 256, chunk in [32, 65536]");
+    // Tiles: inside the scene, cells within n_cells and disjoint.
+    std::vector<std::pair<uint64_t, uint64_t>> ranges(n_tiles);
+    for (size_t t = 0; t < n_tiles; ++t) {
+        const qm_tile_desc &d = tiles[t];
+        const std::string name = "qm_batch_plan_create: tile " + std::to_string(t);
+        if (d.nx <= 0 || d.ny <= 0 || d.spacing <= 0 || (int64_t)d.nx * d.ny > (int64_t(1) << 26))
+            return fail(QM_ERR_ARGUMENT, name + ": nx, ny or spacing");
+        int64_t last_x = d.origin[0] + (int64_t)(d.nx - 1) * d.spacing, last_y = d.origin[1] + (int64_t)(d.ny - 1) * d.spacing;
+        if (d.origin[0] < 0 || d.origin[1] < 0 || last_x >= scene->extent[0] || last_y >= scene->extent[1])
+            return fail(QM_ERR_ARGUMENT, name + ": receivers outside the scene extent");
+        if (d.source_end > d.source_begin && d.source_end > scene->n_sources)
+            return fail(QM_ERR_ARGUMENT, name + ": source range beyond the scene's sources");
+        uint64_t cells = (uint64_t)d.nx * d.ny;
+        if (d.cell_offset + cells > n_cells) return fail(QM_ERR_ARGUMENT, name + ": cells beyond n_cells");
+        ranges[t] = {d.cell_offset, d.cell_offset + cells};
+    }
+    {
+        std::vector<std::pair<uint64_t, uint64_t>> sorted = ranges;
+        std::sort(sorted.begin(), sorted.end());
+        for (size_t k = 1; k < sorted.size(); ++k)
+            if (sorted[k].first < sorted[k - 1].second) return fail(QM_ERR_ARGUMENT, "qm_batch_plan_create: tiles share output cells");
+    }
+    qm_ctx *ctx = scene->ctx;
+    std::lock_guard<std::mutex> guard(ctx->lock);
+    QM_CUDA(cudaSetDevice(ctx->device));
+    cudaStream_t stream = ctx->stream;
+    auto *P = new qm_batch_plan;
+    std::unique_ptr<qm_batch_plan> hold(P);
+    P->scene = scene;
+    P->n_cells = n_cells;
+    P->use_graph = (flags & QM_BATCH_GRAPH) != 0;
+    for (int p = 0; p < 3; ++p) P->lden_w[p] = (float)LDEN_W[p];
+    std::vector<float> alt(n_cells, 0.0f);
+    std::vector<uint32_t> own(n_cells, 0), cell_tile(n_cells, ~0u);
+    std::vector<int2> xy(n_cells, make_int2(0, 0));
+    struct Pending {
+        WorkItem item;
+        uint64_t work;
+    };
+    std::vector<Pending> pending[2];  // 128 and 256 threads
+    uint64_t total_paths = 0;
+    for (size_t t = 0; t < n_tiles; ++t) {
+        const qm_tile_desc &d = tiles[t];
+        const qm_tile_config &c = tab.bucket[qm_tile_bucket(&d)];
+        uint32_t sb = d.source_begin, se = d.source_end;
+        if (se <= sb) {
+            sb = 0;
+            se = scene->n_sources;
+        }
+        TileDev T{};
+        T.origin_x = d.origin[0];
+        T.origin_y = d.origin[1];
+        T.spacing = d.spacing;
+        T.nx = d.nx;
+        T.ny = d.ny;
+        T.source_begin = sb;
+        T.source_end = se;
+        T.block_w = c.block_w;
+        T.block_h = c.block_h;
+        T.chunk = c.chunk;
+        T.n_chunks = se > sb ? (se - sb + c.chunk - 1) / c.chunk : 0;
+        T.cell_offset = d.cell_offset;
+        T.partial_offset = P->partial_slots;
+        const uint64_t cells = (uint64_t)d.nx * d.ny;
+        P->partial_slots += cells * T.n_chunks;
+        total_paths += cells * (se - sb);
+        P->tiles.push_back(T);
+        qm_grid_desc g{};
+        g.origin[0] = d.origin[0];
+        g.origin[1] = d.origin[1];
+        g.spacing = d.spacing;
+        g.nx = d.nx;
+        g.ny = d.ny;
+        g.height_m = d.height_m;
+        std::vector<float> a;
+        std::vector<uint32_t> o;
+        grid_receivers(scene, &g, a, o);
+        for (uint64_t k = 0; k < cells; ++k) {
+            uint64_t gc = d.cell_offset + k;
+            alt[gc] = a[k];
+            own[gc] = o[k];
+            cell_tile[gc] = (uint32_t)t;
+            xy[gc] = make_int2(d.origin[0] + (int)(k % d.nx) * d.spacing, d.origin[1] + (int)(k / d.nx) * d.spacing);
+        }
+        const uint32_t bx = (d.nx + c.block_w - 1) / c.block_w, by = (d.ny + c.block_h - 1) / c.block_h;
+        for (uint32_t b = 0; b < bx * by; ++b) {
+            uint32_t w = std::min<uint32_t>(c.block_w, d.nx - (b % bx) * c.block_w);
+            uint32_t h = std::min<uint32_t>(c.block_h, d.ny - (b / bx) * c.block_h);
+            for (uint32_t ch = 0; ch < T.n_chunks; ++ch) {
+                uint32_t n = std::min<uint32_t>(c.chunk, se - sb - ch * c.chunk);
+                pending[c.threads == 256 ? 1 : 0].push_back(Pending{WorkItem{(uint32_t)t, b, ch, 0}, (uint64_t)w * h * n});
+            }
+        }
+    }
+    if (P->partial_slots > (size_t(1) << 31))
+        return fail(QM_ERR_CAPACITY, "qm_batch_plan_create: the batch's partial sums exceed 2^31 slots; use larger chunks");
+    // Largest items first: the persistent CTAs then finish together.
+    for (int k = 0; k < 2; ++k) {
+        if (pending[k].empty()) continue;
+        std::stable_sort(pending[k].begin(), pending[k].end(), [](const Pending &a, const Pending &b) { return a.work > b.work; });
+        if (pending[k].size() >= (1ull << 32)) return fail(QM_ERR_CAPACITY, "qm_batch_plan_create: too many work items");
+        P->launches.emplace_back();
+        auto &L = P->launches.back();
+        L.threads = k == 1 ? 256 : 128;
+        L.n_items = (uint32_t)pending[k].size();
+        L.grid = (uint32_t)std::min<uint64_t>(L.n_items, (uint64_t)ctx->sm_count * (512 / L.threads));
+        std::vector<WorkItem> items(L.n_items);
+        for (uint32_t i = 0; i < L.n_items; ++i) items[i] = pending[k][i].item;
+        QM_CUDA(cudaMalloc(&L.items.p, items.size() * sizeof(WorkItem)));
+        QM_CUDA(cudaMalloc(&L.next.p, sizeof(unsigned int)));
+        QM_CUDA(cudaMemcpyAsync(L.items.p, items.data(), items.size() * sizeof(WorkItem), cudaMemcpyHostToDevice, stream));
+        QM_CUDA(cudaStreamSynchronize(stream));
+    }
+    P->retry_cap = (uint32_t)std::min<uint64_t>(std::max<uint64_t>(total_paths / 128, 1 << 20), 1 << 25);
+    QM_CUDA(cudaMalloc(&P->d_tiles.p, P->tiles.size() * sizeof(TileDev)));
+    QM_CUDA(cudaMalloc(&P->d_cell_tile.p, n_cells * sizeof(uint32_t)));
+    QM_CUDA(cudaMalloc(&P->d_rcv_xy.p, n_cells * sizeof(int2)));
+    QM_CUDA(cudaMalloc(&P->d_alt.p, n_cells * sizeof(float)));
+    QM_CUDA(cudaMalloc(&P->d_own.p, n_cells * sizeof(uint32_t)));
+    QM_CUDA(cudaMalloc(&P->d_partial.p, std::max<size_t>(P->partial_slots, 1) * GRID_SLOTS * sizeof(float)));
+    QM_CUDA(cudaMalloc(&P->d_retry.p, (size_t)P->retry_cap * sizeof(uint2)));
+    QM_CUDA(cudaMalloc(&P->d_rcount.p, sizeof(unsigned int)));
+    QM_CUDA(cudaMalloc(&P->d_counters.p, 6 * sizeof(unsigned long long)));
+    QM_CUDA(cudaMalloc(&P->d_retry_acc.p, n_cells * GRID_SLOTS * sizeof(float)));
+    QM_CUDA(cudaMalloc(&P->d_bands.p, n_cells * QM_BANDS * sizeof(float)));
+    QM_CUDA(cudaMalloc(&P->d_dba.p, n_cells * sizeof(float)));
+    QM_CUDA(cudaMalloc(&P->d_lden.p, n_cells * sizeof(float)));
+    QM_CUDA(cudaMemcpyAsync(P->d_tiles.p, P->tiles.data(), P->tiles.size() * sizeof(TileDev), cudaMemcpyHostToDevice, stream));
+    QM_CUDA(cudaMemcpyAsync(P->d_cell_tile.p, cell_tile.data(), n_cells * sizeof(uint32_t), cudaMemcpyHostToDevice, stream));
+    QM_CUDA(cudaMemcpyAsync(P->d_rcv_xy.p, xy.data(), n_cells * sizeof(int2), cudaMemcpyHostToDevice, stream));
+    QM_CUDA(cudaMemcpyAsync(P->d_alt.p, alt.data(), n_cells * sizeof(float), cudaMemcpyHostToDevice, stream));
+    QM_CUDA(cudaMemcpyAsync(P->d_own.p, own.data(), n_cells * sizeof(uint32_t), cudaMemcpyHostToDevice, stream));
+    QM_CUDA(cudaStreamSynchronize(stream));
+    if (P->use_graph) {
+        QM_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+        cudaError_t e = batch_launch(P, stream);
+        cudaGraph_t graph = nullptr;
+        cudaError_t e2 = cudaStreamEndCapture(stream, &graph);
+        if (e != cudaSuccess || e2 != cudaSuccess) {
+            if (graph) cudaGraphDestroy(graph);
+            return fail(QM_ERR_CUDA, std::string("cuda: graph capture: ") + cudaGetErrorString(e != cudaSuccess ? e : e2));
+        }
+        P->graph = graph;
+        QM_CUDA(cudaGraphInstantiate(&P->exec, P->graph, 0));
+    }
+    *out = hold.release();
+    return QM_OK;
+}
+
+qm_status qm_batch_plan_run(qm_batch_plan *P, qm_paint_stats *stats) {
+    if (!P) return fail(QM_ERR_ARGUMENT, "qm_batch_plan_run: null plan");
+    qm_scene *scene = P->scene;
+    qm_ctx *ctx = scene->ctx;
+    std::lock_guard<std::mutex> guard(ctx->lock);
+    QM_CUDA(cudaSetDevice(ctx->device));
+    cudaStream_t stream = ctx->stream;
+    Events ev;
+    QM_CUDA(ev.create());
+    QM_CUDA(cudaEventRecord(ev.e0, stream));
+    if (P->use_graph)
+        QM_CUDA(cudaGraphLaunch(P->exec, stream));
+    else
+        QM_CUDA(batch_launch(P, stream));
+    QM_CUDA(cudaEventRecord(ev.e2, stream));
+    unsigned int n_retry = 0;
+    QM_CUDA(cudaMemcpyAsync(&n_retry, P->d_rcount.p, sizeof(n_retry), cudaMemcpyDeviceToHost, stream));
+    QM_CUDA(cudaStreamSynchronize(stream));
+    if (n_retry > P->retry_cap)
+        return fail(QM_ERR_CAPACITY, "qm_batch_plan_run: " + std::to_string(n_retry) + " over-capacity paths, more than the re-run list holds");
+    if (n_retry > 0) {
+        std::vector<uint2> list(n_retry);
+        QM_CUDA(cudaMemcpy(list.data(), P->d_retry.p, n_retry * sizeof(uint2), cudaMemcpyDeviceToHost));
+        std::sort(list.begin(), list.end(), [](uint2 a, uint2 b) { return a.x != b.x ? a.x < b.x : a.y < b.y; });
+        std::vector<uint32_t> cids, cstart;
+        for (uint32_t i = 0; i < n_retry; ++i)
+            if (cids.empty() || cids.back() != list[i].x) {
+                cids.push_back(list[i].x);
+                cstart.push_back(i);
+            }
+        cstart.push_back(n_retry);
+        const uint32_t threads = std::min<uint32_t>(((n_retry + 63) / 64) * 64, 8192);
+        using Large = PathWork<CapsLarge::C, CapsLarge::K, CapsLarge::H>;
+        Scratch d_sorted, d_cids, d_cstart, d_works, d_results, d_rstatus;
+        QM_CUDA(cudaMalloc(&d_sorted.p, n_retry * sizeof(uint2)));
+        QM_CUDA(cudaMalloc(&d_cids.p, cids.size() * sizeof(uint32_t)));
+        QM_CUDA(cudaMalloc(&d_cstart.p, cstart.size() * sizeof(uint32_t)));
+        QM_CUDA(cudaMalloc(&d_works.p, (size_t)threads * sizeof(Large)));
+        QM_CUDA(cudaMalloc(&d_results.p, (size_t)n_retry * GRID_SLOTS * sizeof(float)));
+        QM_CUDA(cudaMalloc(&d_rstatus.p, (size_t)n_retry * sizeof(uint32_t)));
+        QM_CUDA(cudaMemcpyAsync(d_sorted.p, list.data(), n_retry * sizeof(uint2), cudaMemcpyHostToDevice, stream));
+        QM_CUDA(cudaMemcpyAsync(d_cids.p, cids.data(), cids.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, stream));
+        QM_CUDA(cudaMemcpyAsync(d_cstart.p, cstart.data(), cstart.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, stream));
+        BatchRetryArgs RA{};
+        RA.rcv_xy = static_cast<int2 *>(P->d_rcv_xy.p);
+        RA.rcv_alt = static_cast<float *>(P->d_alt.p);
+        RA.rcv_own = static_cast<uint32_t *>(P->d_own.p);
+        for (int k = 0; k < 3; ++k) RA.lden_w[k] = P->lden_w[k];
+        RA.want_fav = scene->any_favourable;
+        batch_retry_kernel<<<threads / 64, 64, 0, stream>>>(scene->dev, RA, static_cast<uint2 *>(d_sorted.p), n_retry,
+                                                            static_cast<Large *>(d_works.p),
+                                                            static_cast<float *>(d_results.p),
+                                                            static_cast<uint32_t *>(d_rstatus.p));
+        QM_CUDA(cudaGetLastError());
+        fold_retry_kernel<<<(unsigned)((cids.size() + 127) / 128), 128, 0, stream>>>(
+            static_cast<uint32_t *>(d_cids.p), static_cast<uint32_t *>(d_cstart.p), (uint32_t)cids.size(),
+            static_cast<float *>(d_results.p), static_cast<float *>(P->d_retry_acc.p), 0, (int)P->n_cells);
+        QM_CUDA(cudaGetLastError());
+        std::vector<uint32_t> rstatus(n_retry);
+        QM_CUDA(cudaMemcpyAsync(rstatus.data(), d_rstatus.p, n_retry * sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
+        QM_CUDA(cudaStreamSynchronize(stream));
+        size_t still = 0;
+        for (uint32_t v : rstatus) still += v != 0;
+        if (still)
+            return fail(QM_ERR_CAPACITY, "qm_batch_plan_run: " + std::to_string(still) + " paths exceed even the large per-path capacities");
+    }
+    BatchReduceArgs R{};
+    R.tiles = static_cast<TileDev *>(P->d_tiles.p);
+    R.cell_tile = static_cast<uint32_t *>(P->d_cell_tile.p);
+    R.n_cells = P->n_cells;
+    R.partial = static_cast<float *>(P->d_partial.p);
+    R.retry_acc = static_cast<float *>(P->d_retry_acc.p);
+    R.cell_bands = static_cast<float *>(P->d_bands.p);
+    R.cell_dba = static_cast<float *>(P->d_dba.p);
+    R.cell_lden = static_cast<float *>(P->d_lden.p);
+    batch_reduce_kernel<<<(unsigned)((P->n_cells + 255) / 256), 256, 0, stream>>>(R);
+    QM_CUDA(cudaGetLastError());
+    QM_CUDA(cudaEventRecord(ev.e1, stream));
+    unsigned long long counters[6];
+    QM_CUDA(cudaMemcpyAsync(counters, P->d_counters.p, sizeof(counters), cudaMemcpyDeviceToHost, stream));
+    QM_CUDA(cudaStreamSynchronize(stream));
+    float ms = 0.f, paint_ms = 0.f;
+    QM_CUDA(cudaEventElapsedTime(&ms, ev.e0, ev.e1));
+    QM_CUDA(cudaEventElapsedTime(&paint_ms, ev.e0, ev.e2));
+    if (stats) {
+        stats->paths = counters[0];
+        stats->crossings = counters[1];
+        stats->edge_tests = counters[2];
+        stats->failed_paths = counters[3];
+        stats->vertices = counters[4];
+        stats->candidates = counters[5];
+        stats->kernel_ms = ms;
+        stats->paint_ms = paint_ms;
+    }
+    return QM_OK;
+}
+
+qm_status qm_batch_plan_read(qm_batch_plan *P, float *cell_bands, float *cell_dba, float *cell_lden) {
+    if (!P) return fail(QM_ERR_ARGUMENT, "qm_batch_plan_read: null plan");
+    qm_ctx *ctx = P->scene->ctx;
+    std::lock_guard<std::mutex> guard(ctx->lock);
+    QM_CUDA(cudaSetDevice(ctx->device));
+    cudaStream_t stream = ctx->stream;
+    if (cell_bands)
+        QM_CUDA(cudaMemcpyAsync(cell_bands, P->d_bands.p, P->n_cells * QM_BANDS * sizeof(float), cudaMemcpyDeviceToHost, stream));
+    if (cell_dba) QM_CUDA(cudaMemcpyAsync(cell_dba, P->d_dba.p, P->n_cells * sizeof(float), cudaMemcpyDeviceToHost, stream));
+    if (cell_lden) QM_CUDA(cudaMemcpyAsync(cell_lden, P->d_lden.p, P->n_cells * sizeof(float), cudaMemcpyDeviceToHost, stream));
+    QM_CUDA(cudaStreamSynchronize(stream));
+    return QM_OK;
+}
+
+qm_status qm_batch_autotune(qm_scene *scene, const qm_tile_desc *sample, size_t n_sample, qm_tune_table *table,
+                            float *timings) {
+    if (!scene || !table || (n_sample && !sample)) return fail(QM_ERR_ARGUMENT, "qm_batch_autotune: null scene, sample or table");
+    qm_tune_default(table);
+    if (timings)
+        for (int k = 0; k < QM_TILE_BUCKETS * QM_TILE_CANDIDATES; ++k) timings[k] = -1.0f;
+    for (int b = 0; b < QM_TILE_BUCKETS; ++b) {
+        // This bucket's samples, clipped to their first 64 x 64 receivers and 4,096 sources.
+        std::vector<qm_tile_desc> tiles;
+        uint64_t cells = 0;
+        for (size_t k = 0; k < n_sample; ++k) {
+            if ((int)qm_tile_bucket(&sample[k]) != b) continue;
+            qm_tile_desc d = sample[k];
+            d.nx = std::min(d.nx, 64);
+            d.ny = std::min(d.ny, 64);
+            uint32_t sb = d.source_begin, se = d.source_end;
+            if (se <= sb) {
+                sb = 0;
+                se = scene->n_sources;
+            }
+            d.source_begin = sb;
+            d.source_end = std::min(se, sb + 4096u);
+            d.cell_offset = cells;
+            cells += (uint64_t)d.nx * d.ny;
+            tiles.push_back(d);
+        }
+        if (tiles.empty()) continue;
+        float best = INFINITY;
+        for (int k = 0; k < QM_TILE_CANDIDATES; ++k) {
+            qm_tune_table t;
+            for (int q = 0; q < QM_TILE_BUCKETS; ++q) t.bucket[q] = tile_candidate(k);
+            qm_batch_plan *plan = nullptr;
+            qm_status st = qm_batch_plan_create(scene, tiles.data(), tiles.size(), cells, &t, 0, &plan);
+            if (st != QM_OK) return st;
+            qm_paint_stats s1{}, s2{};
+            st = qm_batch_plan_run(plan, &s1);
+            if (st == QM_OK) st = qm_batch_plan_run(plan, &s2);
+            qm_batch_plan_free(plan);
+            if (st != QM_OK) return st;
+            float ms = (float)s2.paint_ms;
+            if (timings) timings[b * QM_TILE_CANDIDATES + k] = ms;
+            if (ms < best) {
+                best = ms;
+                table->bucket[b] = tile_candidate(k);
+            }
+        }
+    }
     return QM_OK;
 }
 

@@ -80,6 +80,19 @@ def lib():
         L.qm_paint_grid_surrogate.argtypes = [C.c_void_p, C.POINTER(abi.GridDesc), C.c_void_p, _F, _F, _F, _U32,
                                               C.POINTER(abi.PaintStats), _U64]
         L.qm_paint_grid_surrogate.restype = C.c_int
+        L.qm_tile_bucket.argtypes = [C.POINTER(abi.TileDesc)]
+        L.qm_tile_bucket.restype = C.c_uint32
+        L.qm_tune_default.argtypes = [C.POINTER(abi.TuneTable)]
+        L.qm_batch_autotune.argtypes = [C.c_void_p, C.POINTER(abi.TileDesc), C.c_size_t, C.POINTER(abi.TuneTable), _F]
+        L.qm_batch_autotune.restype = C.c_int
+        L.qm_batch_plan_create.argtypes = [C.c_void_p, C.POINTER(abi.TileDesc), C.c_size_t, C.c_uint64,
+                                           C.POINTER(abi.TuneTable), C.c_uint32, P]
+        L.qm_batch_plan_create.restype = C.c_int
+        L.qm_batch_plan_free.argtypes = [C.c_void_p]
+        L.qm_batch_plan_run.argtypes = [C.c_void_p, C.POINTER(abi.PaintStats)]
+        L.qm_batch_plan_run.restype = C.c_int
+        L.qm_batch_plan_read.argtypes = [C.c_void_p, _F, _F, _F]
+        L.qm_batch_plan_read.restype = C.c_int
         if L.qm_abi_version() != abi.ABI_VERSION:
             raise QmError(abi.QM_ERR_UNSUPPORTED, "library ABI version mismatch")
         _lib = L
@@ -327,3 +340,75 @@ class Surrogate:
         _check(lib().qm_surrogate_train(self.handle, device_scene.handle, descs, len(grids), C.byref(cfg),
                                         abi.ptr(hist, C.c_double), C.byref(n)), self.ctx.handle)
         return hist, n.value
+
+
+def tile_descs(tiles):
+    """ctypes array of qm_tile_desc from dicts (origin, spacing, nx, ny, height_m, source_begin,
+    source_end, cell_offset)."""
+    arr = (abi.TileDesc * len(tiles))()
+    for k, t in enumerate(tiles):
+        d = arr[k]
+        d.origin[0], d.origin[1] = t["origin"]
+        d.spacing, d.nx, d.ny = t["spacing"], t["nx"], t["ny"]
+        d.height_m = t.get("height_m", 4.0)
+        d.source_begin, d.source_end = t["source_begin"], t["source_end"]
+        d.cell_offset = t["cell_offset"]
+    return arr
+
+
+def tile_bucket(tile):
+    return lib().qm_tile_bucket(C.byref(tile_descs([tile])[0]))
+
+
+def tune_default():
+    t = abi.TuneTable()
+    lib().qm_tune_default(C.byref(t))
+    return t
+
+
+def autotune(device_scene, sample_tiles):
+    """(qm_tune_table, timings [buckets][candidates] ms, -1 where not timed)."""
+    arr = tile_descs(sample_tiles)
+    table = abi.TuneTable()
+    timings = np.zeros((abi.TILE_BUCKETS, abi.TILE_CANDIDATES), np.float32)
+    _check(lib().qm_batch_autotune(device_scene.handle, arr, len(sample_tiles), C.byref(table),
+                                   abi.ptr(timings, C.c_float)), device_scene.ctx.handle)
+    return table, timings
+
+
+class BatchPlan:
+    """A planned batch of tiles (qm_batch_plan_*)."""
+
+    def __init__(self, device_scene, tiles, n_cells=None, table=None, graph=True):
+        self.dev = device_scene
+        arr = tile_descs(tiles)
+        self.n_cells = n_cells if n_cells is not None else max(t["cell_offset"] + t["nx"] * t["ny"] for t in tiles)
+        self.handle = C.c_void_p()
+        _check(lib().qm_batch_plan_create(device_scene.handle, arr, len(tiles), self.n_cells,
+                                          C.byref(table) if table is not None else None, 1 if graph else 0,
+                                          C.byref(self.handle)), device_scene.ctx.handle)
+
+    def close(self):
+        if self.handle:
+            lib().qm_batch_plan_free(self.handle)
+            self.handle = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def run(self):
+        st = abi.PaintStats()
+        _check(lib().qm_batch_plan_run(self.handle, C.byref(st)), self.dev.ctx.handle)
+        return dict(paths=st.paths, failed_paths=st.failed_paths, crossings=st.crossings, edge_tests=st.edge_tests,
+                    vertices=st.vertices, candidates=st.candidates, kernel_ms=st.kernel_ms, paint_ms=st.paint_ms)
+
+    def read(self):
+        bands = np.zeros((self.n_cells, 8), np.float32)
+        dba = np.zeros(self.n_cells, np.float32)
+        lden = np.zeros(self.n_cells, np.float32)
+        _check(lib().qm_batch_plan_read(self.handle, abi.ptr(bands, C.c_float), abi.ptr(dba, C.c_float),
+                                        abi.ptr(lden, C.c_float)), self.dev.ctx.handle)
+        return bands, dba, lden

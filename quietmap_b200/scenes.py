@@ -370,3 +370,35 @@ def flights_square(seed=3, n_flights=2000, segments_per_flight=50, n_types=10, r
                 receiver_height_m=4.0, reach_m=reach_m, duration_s=86400.0)
     return FlightScene(types=types, segments=segs, grid=grid, epnl_db=epnl, la_db=la,
                        info=dict(seed=seed, flights=n_flights, types=n_types))
+
+
+# ---------------------------------------------------------------------------------------------
+# Batches of uneven tiles.
+
+def tiles_world():
+    """The world tile batches are cut from: the config-1 road square (1 km, 400 roads as 1 m point
+    sources, 300 buildings, flat G = 0.5, homogeneous)."""
+    return road_square()[0]
+
+
+def uneven_tiles(scene, n_tiles=4096, seed=5, side=(32, 512), sources=(10, 50000), spacing_steps=60):
+    """`n_tiles` receiver tiles with sides (nx, ny) log-uniform in `side` receivers at
+    `spacing_steps` lattice steps, each with a contiguous range of the scene's sources whose
+    length is log-uniform in `sources`, at seeded positions inside the scene. Cells are numbered
+    tile after tile."""
+    rng = np.random.default_rng(seed)
+    extent = scene.extent_steps[0]
+    n_src = len(scene.sources)
+    out, offset = [], 0
+    for _ in range(n_tiles):
+        nx, ny = (int(round(np.exp(rng.uniform(np.log(side[0]), np.log(side[1]))))) for _ in range(2))
+        nx, ny = min(nx, (extent - 1) // spacing_steps), min(ny, (extent - 1) // spacing_steps)
+        ox = int(rng.integers(0, extent - (nx - 1) * spacing_steps))
+        oy = int(rng.integers(0, extent - (ny - 1) * spacing_steps))
+        k = int(round(np.exp(rng.uniform(np.log(sources[0]), np.log(sources[1])))))
+        k = max(1, min(k, n_src))
+        b = int(rng.integers(0, n_src - k + 1))
+        out.append(dict(origin=(ox, oy), spacing=spacing_steps, nx=nx, ny=ny, height_m=4.0, source_begin=b,
+                        source_end=b + k, cell_offset=offset))
+        offset += nx * ny
+    return out
