@@ -181,7 +181,10 @@ void band_constants(BandConstants &bc) {
         bc.f075[b] = (float)std::pow(f[b], 0.75);
         bc.k[b] = (float)(2.0 * pi * f[b] / 340.0);
         bc.lambda[b] = (float)(340.0 / f[b]);
+        bc.inv_lambda[b] = (float)(f[b] / 340.0);
         bc.lambda_d[b] = 340.0 / f[b];
+        bc.lambda_over_20_d[b] = bc.lambda_d[b] / 20.0;
+        bc.lambda_over_4_d[b] = bc.lambda_d[b] / 4.0;
     }
 }
 

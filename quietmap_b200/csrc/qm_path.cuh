@@ -77,12 +77,16 @@ __device__ __forceinline__ uint32_t xrec_fp(const SceneDev &S, const XRec &r) { 
 
 __device__ __forceinline__ int sgn64(long long v) { return (v > 0) - (v < 0); }
 
+// 32 x 32 -> 64-bit product (one wide multiply): lattice coordinates and their differences fit in
+// 32 bits (scenes are limited to 2^27 steps).
+__device__ __forceinline__ long long mulw(int a, int b) { return (long long)a * (long long)b; }
+
 // Whether an edge hit enters or leaves its ring (crossings.rs:80-111); exact on lattice points.
 __device__ __noinline__ bool edge_bounds_roof(const SceneDev &S, long long sx, long long sy, long long dx, long long dy,
                                         uint32_t edge, uint32_t first, uint32_t count) {
     auto side = [&](uint32_t index) {
         int2 v = S.vertices[index];
-        return dx * ((long long)v.y - sy) - dy * ((long long)v.x - sx);
+        return mulw((int)dx, v.y - (int)sy) - mulw((int)dy, v.x - (int)sx);
     };
     long long a = side(edge), b = side(edge + 1);
     if (a != 0 && b != 0) return true;
@@ -106,7 +110,8 @@ template <int MAXC>
 __device__ int list_crossings(const SceneDev &S, int sx, int sy, int rx, int ry, uint32_t rcv_own, XRec *xs,
                               uint32_t &status, uint32_t &edges_tested) {
     int n = 0;
-    long long dx = (long long)rx - sx, dy = (long long)ry - sy;
+    const int idx = rx - sx, idy = ry - sy;
+    long long dx = idx, dy = idy;
     const int C = S.cell_steps;
     int cx = floor_div(sx, C), cy = floor_div(sy, C);
     const int lx = floor_div(rx, C), ly = floor_div(ry, C);
@@ -126,12 +131,12 @@ __device__ int list_crossings(const SceneDev &S, int sx, int sy, int rx, int ry,
                     min(seg.y, seg.w) > maxy)
                     continue;
                 ++edges_tested;
-                long long ex = (long long)seg.z - seg.x, ey = (long long)seg.w - seg.y;
-                long long den = dx * ey - dy * ex;
+                const int ex = seg.z - seg.x, ey = seg.w - seg.y;
+                long long den = mulw(idx, ey) - mulw(idy, ex);
                 if (den == 0) continue;
-                long long wx = (long long)seg.x - sx, wy = (long long)seg.y - sy;
-                long long tn = wx * ey - wy * ex;
-                long long un = wx * dy - wy * dx;
+                const int wx = seg.x - sx, wy = seg.y - sy;
+                long long tn = mulw(wx, ey) - mulw(wy, ex);
+                long long un = mulw(wx, idy) - mulw(wy, idx);
                 long long d = den;
                 if (d < 0) {
                     d = -d;
@@ -157,10 +162,10 @@ __device__ int list_crossings(const SceneDev &S, int sx, int sy, int rx, int ry,
         else if (cy == ly)
             axis = 0;
         else {
-            long long ax_ = bx - sx, ay_ = by - sy;
+            int ax_ = (int)(bx - sx), ay_ = (int)(by - sy);
             if (ax_ < 0) ax_ = -ax_;
             if (ay_ < 0) ay_ = -ay_;
-            axis = (ax_ * ady < ay_ * adx) ? 0 : 1;  // a tie steps the row
+            axis = (mulw(ax_, (int)ady) < mulw(ay_, (int)adx)) ? 0 : 1;  // a tie steps the row
         }
         if (axis == 0) {
             cx += stx;
@@ -619,14 +624,14 @@ __device__ __noinline__ void state_boundary(Band<STATE, CAP_H> &band, const EqGe
     ground_attenuation_bands(receiver_side, GroundFactors{receiver_side_ground, receiver_side_ground, receiver_side_ground},
                              STATE, ground_or);
     double rayleigh_star = blocked ? 0.0 : path_difference_d(STATE, radius, Si, points, np, Ri);
+    const float delta_f = (float)delta, delta_si_f = (float)delta_si, delta_ri_f = (float)delta_ri;
 #pragma unroll
     for (int b = 0; b < QM_BANDS; ++b) {
-        double lambda = c_band.lambda_d[b];
-        bool admitted = blocked || (delta > -lambda / 20.0 && delta > lambda / 4.0 - rayleigh_star);
+        bool admitted = blocked || (delta > -c_band.lambda_over_20_d[b] && delta > c_band.lambda_over_4_d[b] - rayleigh_star);
         if (!admitted) continue;
-        float direct_db = diffraction_db(delta, c2[b], b);
-        float source_image_db = diffraction_db(delta_si, c2[b], b);
-        float receiver_image_db = diffraction_db(delta_ri, c2[b], b);
+        float direct_db = diffraction_db(delta_f, c2[b], b);
+        float source_image_db = diffraction_db(delta_si_f, c2[b], b);
+        float receiver_image_db = diffraction_db(delta_ri_f, c2[b], b);
         float sr = direct_db;
         float split_so;
         if (source_side.source_below) {

@@ -982,8 +982,7 @@ __device__ inline float lane_state_boundary(int state, int b, const EqGeometry &
         float x = 5.0f * c_band.lambda[b] / span;
         c2 = (1.0f + x * x) / (1.0f / 3.0f + x * x);
     }
-    double lambda = c_band.lambda_d[b];
-    bool admitted = res.blocked || (delta > -lambda / 20.0 && delta > lambda / 4.0 - rayleigh_star);
+    bool admitted = res.blocked || (delta > -c_band.lambda_over_20_d[b] && delta > c_band.lambda_over_4_d[b] - rayleigh_star);
     if (!admitted) return whole;
     float source_side_ground = mean_ground_of(src_m, first.x, g0);
     float source_side_near = ground_factor_near_source(source_side, source_side_ground, source_gf);
@@ -992,9 +991,9 @@ __device__ inline float lane_state_boundary(int state, int b, const EqGeometry &
     float receiver_side_ground = mean_ground_of(rcv_m, rlen, last_gat);
     float ground_or = ground_attenuation_band(
         receiver_side, GroundFactors{receiver_side_ground, receiver_side_ground, receiver_side_ground}, state, b);
-    float direct_db = diffraction_db(delta, c2, b);
-    float source_image_db = diffraction_db(delta_si, c2, b);
-    float receiver_image_db = diffraction_db(delta_ri, c2, b);
+    float direct_db = diffraction_db((float)delta, c2, b);
+    float source_image_db = diffraction_db((float)delta_si, c2, b);
+    float receiver_image_db = diffraction_db((float)delta_ri, c2, b);
     float sr = direct_db;
     float split_so;
     if (source_side.source_below) {

@@ -212,11 +212,11 @@ def _point_sources(stock, points_m, level_db=90.0, height_m=0.05):
 
 
 def test_over_capacity_paths_are_rerun_on_the_device(ctx):
-    """70 buildings in a row: rays along it cross 140 walls, beyond the flat kernel's per-path
+    """140 buildings in a row: rays along it cross 280 walls, beyond the painter's per-path
     capacity; those paths are re-run with large capacities and still match the oracle."""
     stock = Stock(side_m=2600.0, offset_m=200.0)
-    for i in range(70):
-        stock.building(i + 1, 3.0 + (i % 7), [square(100.0 + 24.0 * i, 0.0, 5.0)])
+    for i in range(140):
+        stock.building(i + 1, 3.0 + (i % 7), [square(100.0 + 12.0 * i, 0.0, 5.0)])
     sources = _point_sources(stock, [(40.0, 0.0), (40.0, 1.5), (45.0, -2.0), (60.0, 30.0)])
     scene = stock.scene(sources=sources)
     origin = stock.steps((1900.0, -12.0))
