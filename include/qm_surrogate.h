@@ -50,6 +50,11 @@ typedef struct qm_surrogate qm_surrogate;
 /* A network on the context's device from `params` (QM_SURR_PARAMS floats). */
 qm_status qm_surrogate_create(qm_ctx *ctx, const float *params, qm_surrogate **out);
 void qm_surrogate_free(qm_surrogate *net);
+/* Selects the inference kernel: 0 (the default) accumulates on the fifth-generation tensor cores
+ * in tensor memory (tcgen05, operands staged by TMA bulk copies); 1 uses warp-level mma.sync with
+ * register accumulators. Both compute the same network; the choice exists to compare them. */
+qm_status qm_surrogate_set_kernel(qm_surrogate *net, int kernel);
+
 /* Its current parameters (QM_SURR_PARAMS floats; the FP32 master copy). */
 qm_status qm_surrogate_params(const qm_surrogate *net, float *params);
 

@@ -8,7 +8,6 @@ against the same operands. Only tests/ import this module.
 """
 
 import numpy as np
-from scipy.special import erf
 
 DIMS = (32, 256, 256, 256, 256, 8)
 WEIGHTS = sum(DIMS[k + 1] * DIMS[k] + DIMS[k + 1] for k in range(5))
@@ -36,12 +35,17 @@ def unpack(params):
     return ws, bs, scales
 
 
+GELU_C, GELU_A = np.sqrt(2.0 / np.pi), 0.044715
+
+
 def gelu(z):
-    return 0.5 * z * (1.0 + erf(z / np.sqrt(2.0)))
+    """GELU in its tanh form (Hendrycks and Gimpel, 2016), as the device computes it."""
+    return 0.5 * z * (1.0 + np.tanh(GELU_C * (z + GELU_A * z ** 3)))
 
 
 def gelu_grad(z):
-    return 0.5 * (1.0 + erf(z / np.sqrt(2.0))) + z * np.exp(-0.5 * z * z) / np.sqrt(2.0 * np.pi)
+    t = np.tanh(GELU_C * (z + GELU_A * z ** 3))
+    return 0.5 * (1.0 + t) + 0.5 * z * (1.0 - t * t) * GELU_C * (1.0 + 3.0 * GELU_A * z * z)
 
 
 def _forward(ws, bs, x, round_):

@@ -1261,6 +1261,8 @@ struct qm_surrogate {
     ~qm_surrogate() {
         cudaFree(net.master);
         cudaFree(net.w16);
+        cudaFree(net.wpack);
+        cudaFree(net.error);
         cudaFree(net.adam_m);
         cudaFree(net.adam_v);
     }
@@ -1435,6 +1437,9 @@ qm_status qm_surrogate_create(qm_ctx *ctx, const float *params, qm_surrogate **o
     scales_from_params(params, s->net.scales);
     cudaError_t e = cudaMalloc(&s->net.master, MLP_WEIGHTS * sizeof(float));
     if (e == cudaSuccess) e = cudaMalloc(&s->net.w16, MLP_W16 * sizeof(__nv_bfloat16));
+    if (e == cudaSuccess) e = cudaMalloc(&s->net.wpack, mlp_packed_bytes());
+    if (e == cudaSuccess) e = cudaMalloc(&s->net.error, sizeof(unsigned));
+    if (e == cudaSuccess) e = cudaMemsetAsync(s->net.error, 0, sizeof(unsigned), ctx->stream);
     if (e == cudaSuccess)
         e = cudaMemcpyAsync(s->net.master, params, MLP_WEIGHTS * sizeof(float), cudaMemcpyHostToDevice, ctx->stream);
     if (e == cudaSuccess) e = mlp_cast(s->net, ctx->stream);
@@ -1452,6 +1457,13 @@ void qm_surrogate_free(qm_surrogate *net) {
     std::lock_guard<std::mutex> guard(net->ctx->lock);
     cudaSetDevice(net->ctx->device);
     delete net;
+}
+
+qm_status qm_surrogate_set_kernel(qm_surrogate *net, int kernel) {
+    if (!net || (kernel != 0 && kernel != 1)) return fail(QM_ERR_ARGUMENT, "qm_surrogate_set_kernel: kernel is 0 or 1");
+    std::lock_guard<std::mutex> guard(net->ctx->lock);
+    net->net.kernel = kernel;
+    return QM_OK;
 }
 
 qm_status qm_surrogate_params(const qm_surrogate *net, float *params) {
@@ -1499,7 +1511,10 @@ qm_status qm_surrogate_forward(qm_surrogate *net, const float *features, size_t 
     QM_CUDA(mlp_normalise(net->net.scales, static_cast<float *>(raw.p), n, static_cast<__nv_bfloat16 *>(x.p), stream));
     QM_CUDA(mlp_forward(net->net, static_cast<__nv_bfloat16 *>(x.p), n, static_cast<float *>(out.p), stream));
     QM_CUDA(cudaMemcpyAsync(outputs, out.p, n * MLP_OUT * sizeof(float), cudaMemcpyDeviceToHost, stream));
+    unsigned err = 0;
+    QM_CUDA(cudaMemcpyAsync(&err, net->net.error, sizeof(err), cudaMemcpyDeviceToHost, stream));
     QM_CUDA(cudaStreamSynchronize(stream));
+    if (err) return fail(QM_ERR_TIMEOUT, "qm_surrogate_forward: a bounded wait of the inference kernel gave up");
     return QM_OK;
 }
 
@@ -1872,8 +1887,10 @@ qm_status qm_paint_grid_surrogate(qm_scene *scene, const qm_grid_desc *grid, qm_
     QM_CUDA(cudaGetLastError());
     QM_CUDA(cudaEventRecord(ev.e1, stream));
     unsigned long long counters[6], taken = 0;
+    unsigned net_error = 0;
     QM_CUDA(cudaMemcpyAsync(counters, d_counters.p, sizeof(counters), cudaMemcpyDeviceToHost, stream));
     QM_CUDA(cudaMemcpyAsync(&taken, d_taken.p, sizeof(taken), cudaMemcpyDeviceToHost, stream));
+    QM_CUDA(cudaMemcpyAsync(&net_error, net->net.error, sizeof(net_error), cudaMemcpyDeviceToHost, stream));
     if (cell_bands) QM_CUDA(cudaMemcpyAsync(cell_bands, d_bands.p, (size_t)cells * 8 * sizeof(float), cudaMemcpyDeviceToHost, stream));
     if (cell_dba) QM_CUDA(cudaMemcpyAsync(cell_dba, d_dbaout.p, (size_t)cells * sizeof(float), cudaMemcpyDeviceToHost, stream));
     if (cell_lden) QM_CUDA(cudaMemcpyAsync(cell_lden, d_lden.p, (size_t)cells * sizeof(float), cudaMemcpyDeviceToHost, stream));
@@ -1892,6 +1909,7 @@ qm_status qm_paint_grid_surrogate(qm_scene *scene, const qm_grid_desc *grid, qm_
         stats->kernel_ms = ms;
         stats->paint_ms = front_ms;
     }
+    if (net_error) return fail(QM_ERR_TIMEOUT, "qm_paint_grid_surrogate: a bounded wait of the inference kernel gave up");
     if (surrogate_paths) *surrogate_paths = taken;
     return QM_OK;
 }

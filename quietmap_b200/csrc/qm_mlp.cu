@@ -45,10 +45,21 @@ __device__ __forceinline__ void cp_wait() {
     asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
 }
 
-// GELU in its erf form, and its derivative.
-__device__ __forceinline__ float gelu(float z) { return 0.5f * z * (1.0f + erff(z * 0.70710678118654752f)); }
+// GELU in its tanh form (Hendrycks and Gimpel, 2016): 0.5 z (1 + tanh(sqrt(2/pi) (z + 0.044715 z^3))),
+// with the hardware tanh; and its derivative. Training and inference use the same function.
+__device__ __forceinline__ float tanh_hw(float x) {
+    float y;
+    asm("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+constexpr float GELU_C = 0.7978845608028654f, GELU_A = 0.044715f;
+__device__ __forceinline__ float gelu(float z) {
+    float t = tanh_hw(GELU_C * fmaf(GELU_A * z, z * z, z));
+    return 0.5f * z * (1.0f + t);
+}
 __device__ __forceinline__ float gelu_grad(float z) {
-    return 0.5f * (1.0f + erff(z * 0.70710678118654752f)) + z * 0.39894228040143268f * __expf(-0.5f * z * z);
+    float t = tanh_hw(GELU_C * fmaf(GELU_A * z, z * z, z));
+    return 0.5f * (1.0f + t) + 0.5f * z * (1.0f - t * t) * GELU_C * fmaf(3.0f * GELU_A * z, z, 1.0f);
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -269,6 +280,321 @@ __global__ void __launch_bounds__(FT_THREADS, 1) mlp_fused_kernel(FusedArgs A) {
         }
     }
     cp_wait<0>();
+}
+
+// ---------------------------------------------------------------------------------------------
+// Fused inference on the fifth-generation tensor cores (tcgen05). A CTA of 8 warps takes 128 rows
+// (the MMA's M) through all five layers: one thread issues tcgen05.mma (BF16 operands from shared
+// memory through matrix descriptors, FP32 accumulators in tensor memory, 128 x 256 per layer), the
+// layer's weights arrive by one TMA bulk copy into shared memory while the previous layer's
+// epilogue runs, and the epilogue (tcgen05.ld, bias, GELU, BF16) writes the next layer's A operand
+// back into shared memory. Operands use the canonical K-major layout without swizzle: 8-row x
+// 16-byte core matrices, adjacent along K 128 bytes apart (LBO), 8-row groups K/8 * 128 bytes
+// apart (SBO). Every wait on an mbarrier is bounded by %globaltimer.
+
+constexpr int UM_THREADS = 256;
+constexpr int UM_A_BYTES = 128 * 256 * 2;   // layer input, 128 rows x 256
+constexpr int UM_B_BYTES = 256 * 256 * 2;   // one layer's weights
+constexpr int UM_X_BYTES = 128 * MLP_IN * 2; // feature rows as they arrive (row-major)
+constexpr int UM_BIAS_FLOATS = 4 * 256 + 16;
+constexpr size_t UM_SMEM = UM_A_BYTES + UM_B_BYTES + UM_X_BYTES + UM_BIAS_FLOATS * 4 + 64;
+constexpr int UM_TMEM_COLS = 256;
+static_assert(UM_SMEM <= 227 * 1024, "shared memory");
+
+// Rows and columns of layer l's B operand as packed (the output layer padded to 16 rows).
+__host__ __device__ constexpr int um_n(int l) { return l == MLP_LAYERS - 1 ? 16 : MLP_HID; }
+__host__ __device__ constexpr int um_k(int l) { return mlp_dim(l); }
+__host__ __device__ constexpr size_t um_w_offset(int l) {  // bytes
+    size_t o = 0;
+    for (int k = 0; k < l; ++k) o += (size_t)um_n(k) * um_k(k) * 2;
+    return o;
+}
+constexpr size_t UM_W_BYTES = um_w_offset(MLP_LAYERS);
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+    uint64_t d = (uint64_t)((saddr >> 4) & 0x3FFFu);
+    d |= (uint64_t)((lbo >> 4) & 0x3FFFu) << 16;
+    d |= (uint64_t)((sbo >> 4) & 0x3FFFu) << 32;
+    d |= (uint64_t)1 << 46;  // descriptor version of tcgen05; base offset 0, no swizzle
+    return d;
+}
+// kind::f16 instruction descriptor: FP32 accumulate, BF16 A and B, both K-major, N and M.
+__host__ __device__ constexpr uint32_t umma_idesc(int M, int N) {
+    return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+
+__device__ __forceinline__ void umma_bf16(uint32_t tmem_d, uint64_t a, uint64_t b, uint32_t idesc, uint32_t accumulate) {
+    asm volatile(
+        "{\n.reg .pred p;\nsetp.ne.b32 p, %4, 0;\n"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem_d),
+        "l"(a), "l"(b), "r"(idesc), "r"(accumulate));
+}
+__device__ __forceinline__ void umma_commit(uint64_t *bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+                 : "memory");
+}
+__device__ __forceinline__ void tc_before_sync() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_after_sync() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void async_proxy_fence() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
+    uint32_t r[16];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
+          "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+__device__ __forceinline__ void um_mbar_init(uint64_t *bar, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
+}
+__device__ __forceinline__ void um_bulk(void *dst, const void *src, unsigned bytes, uint64_t *bar) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_u32(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
+}
+__device__ __forceinline__ uint64_t um_ns() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
+    return t;
+}
+// Waits for the barrier's phase for at most about a second; false when it gave up.
+__device__ __forceinline__ bool um_wait(uint64_t *bar, unsigned phase) {
+    const uint32_t b = smem_u32(bar);
+    const uint64_t start = um_ns();
+    for (;;) {
+        unsigned done;
+        asm volatile(
+            "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2; selp.u32 %0, 1, 0, p; }"
+            : "=r"(done)
+            : "r"(b), "r"(phase)
+            : "memory");
+        if (done) return true;
+        if (um_ns() - start > 1000000000ull) return false;
+    }
+}
+
+// Packs the BF16 matrices into the tcgen05 operand layout (output layer padded to 16 rows).
+__global__ void pack_umma_kernel(const __nv_bfloat16 *w16, __nv_bfloat16 *packed) {
+    size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+    if (i >= UM_W_BYTES / 2) return;
+    int l = 0;
+    while (l < MLP_LAYERS - 1 && i >= um_w_offset(l + 1) / 2) ++l;
+    const size_t e = i - um_w_offset(l) / 2;
+    const int K = um_k(l), sbo = K / 8 * 64;  // in elements
+    const int n = (int)(e / K), k = (int)(e % K);
+    const size_t dst = um_w_offset(l) / 2 + (size_t)(n / 8) * sbo + (k / 8) * 64 + (n % 8) * 8 + (k % 8);
+    packed[dst] = n < mlp_dim(l + 1) ? w16[mlp_w16_offset(l) + (size_t)n * K + k] : __float2bfloat16(0.0f);
+}
+
+struct UmmaArgs {
+    const __nv_bfloat16 *wpack;  // [UM_W_BYTES] packed matrices
+    const float *master;
+    float out_shift[MLP_OUT], out_scale[MLP_OUT], lab_lo[MLP_OUT], lab_hi[MLP_OUT];
+    const __nv_bfloat16 *x;
+    size_t rows;
+    float *out;
+    MlpPaintArgs p;
+    unsigned *error;
+};
+
+template <int MODE>
+__global__ void __launch_bounds__(UM_THREADS, 1) mlp_umma_kernel(UmmaArgs A) {
+    extern __shared__ __align__(1024) unsigned char um_smem[];
+    unsigned char *sA = um_smem;
+    unsigned char *sB = sA + UM_A_BYTES;
+    unsigned char *sX = sB + UM_B_BYTES;
+    float *sBias = reinterpret_cast<float *>(sX + UM_X_BYTES);
+    uint64_t *bars = reinterpret_cast<uint64_t *>(sBias + UM_BIAS_FLOATS);  // w, x, mma
+    uint32_t *sTmem = reinterpret_cast<uint32_t *>(bars + 3);
+    __shared__ float s_red[4][9];
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const size_t n_tiles = (A.rows + 127) / 128;
+    if (blockIdx.x >= n_tiles) return;
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(sTmem)),
+                     "r"(UM_TMEM_COLS)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    if (tid == 0) {
+        um_mbar_init(&bars[0], 1);
+        um_mbar_init(&bars[1], 1);
+        um_mbar_init(&bars[2], 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    for (int i = tid; i < UM_BIAS_FLOATS; i += UM_THREADS) {
+        int l = i / 256, c = i % 256;
+        float v = 0.0f;
+        if (l < 4) v = A.master[mlp_b_offset(l) + c];
+        else if (c < MLP_OUT) v = A.master[mlp_b_offset(4) + c];
+        sBias[i] = v;
+    }
+    tc_before_sync();
+    __syncthreads();
+    tc_after_sync();
+    const uint32_t tmem = *sTmem;
+    unsigned pw = 0, px = 0, pm = 0;
+    bool ok = true;
+    auto x_bytes = [&](size_t tile) { return (unsigned)(min((size_t)128, A.rows - tile * 128) * MLP_IN * 2); };
+    if (tid == 0) {
+        um_bulk(sB, A.wpack, (unsigned)(um_n(0) * um_k(0) * 2), &bars[0]);
+        um_bulk(sX, A.x + blockIdx.x * 128 * MLP_IN, x_bytes(blockIdx.x), &bars[1]);
+    }
+    const int lq = warp & 3, ch = warp >> 2;  // TMEM lane quarter and column half of this warp
+    const int row = 32 * lq + lane;            // this thread's row of the tile
+    for (size_t tile = blockIdx.x; tile < n_tiles && ok; tile += gridDim.x) {
+        const bool has_next = tile + gridDim.x < n_tiles;
+        const size_t r_global = tile * 128 + row;
+        const int rows_here = (int)min((size_t)128, A.rows - tile * 128);
+        ok = __syncthreads_and(um_wait(&bars[1], px));
+        px ^= 1;
+        if (!ok) break;
+        // Feature rows (row-major, 64 B) into the A layout (K = 32: SBO 512 B); missing rows zero.
+        if (tid < 128) {
+            const uint4 *src = reinterpret_cast<const uint4 *>(sX + tid * 64);
+            for (int q = 0; q < 4; ++q) {
+                uint4 v = tid < rows_here ? src[q] : make_uint4(0, 0, 0, 0);
+                *reinterpret_cast<uint4 *>(sA + (tid / 8) * 512 + q * 128 + (tid % 8) * 16) = v;
+            }
+        }
+        async_proxy_fence();
+        __syncthreads();
+        if (tid == 0 && has_next) um_bulk(sX, A.x + (tile + gridDim.x) * 128 * MLP_IN, x_bytes(tile + gridDim.x), &bars[1]);
+        for (int l = 0; l < MLP_LAYERS && ok; ++l) {
+            ok = __syncthreads_and(um_wait(&bars[0], pw));
+            pw ^= 1;
+            if (!ok) break;
+            const int K = um_k(l), N = um_n(l);
+            if (tid == 0) {
+                tc_after_sync();
+                const uint32_t a0 = smem_u32(sA), b0 = smem_u32(sB);
+                const uint32_t sbo = (uint32_t)(K / 8 * 128);
+                for (int s = 0; s < K / 16; ++s)
+                    umma_bf16(tmem, umma_desc(a0 + 256 * s, 128, sbo), umma_desc(b0 + 256 * s, 128, sbo),
+                              umma_idesc(128, N), s > 0 ? 1u : 0u);
+                umma_commit(&bars[2]);
+            }
+            ok = __syncthreads_and(um_wait(&bars[2], pm));
+            pm ^= 1;
+            if (!ok) break;
+            tc_after_sync();
+            // The weights are consumed: fetch the next layer's (or the next tile's first).
+            if (tid == 0 && (l + 1 < MLP_LAYERS || has_next)) {
+                const int nl = (l + 1) % MLP_LAYERS;
+                um_bulk(sB, reinterpret_cast<const unsigned char *>(A.wpack) + um_w_offset(nl),
+                        (unsigned)(um_n(nl) * um_k(nl) * 2), &bars[0]);
+            }
+            const uint32_t t_row = tmem + ((uint32_t)(32 * lq) << 16);
+            if (l < MLP_LAYERS - 1) {
+                // Hidden epilogue: this warp's 128 columns of its 32 rows -> GELU -> BF16 A layout (K = 256).
+                const float *bias = sBias + l * 256;
+                for (int c = 0; c < 8; ++c) {
+                    const int col = 128 * ch + 16 * c;
+                    float v[16];
+                    tmem_ld16(t_row + col, v);
+                    uint32_t pk[8];
+#pragma unroll
+                    for (int q = 0; q < 8; ++q) {
+                        __nv_bfloat162 h = __floats2bfloat162_rn(gelu(v[2 * q] + bias[col + 2 * q]),
+                                                                 gelu(v[2 * q + 1] + bias[col + 2 * q + 1]));
+                        pk[q] = *reinterpret_cast<uint32_t *>(&h);
+                    }
+                    unsigned char *dst = sA + (row / 8) * 4096 + (col / 8) * 128 + (row % 8) * 16;
+                    *reinterpret_cast<uint4 *>(dst) = make_uint4(pk[0], pk[1], pk[2], pk[3]);
+                    *reinterpret_cast<uint4 *>(dst + 128) = make_uint4(pk[4], pk[5], pk[6], pk[7]);
+                }
+                async_proxy_fence();
+                tc_before_sync();
+                __syncthreads();
+            } else {
+                // Output epilogue: warps 0..3, one row each thread.
+                float y[MLP_OUT];
+                bool use = false, bad = false;
+                if (ch == 0) {
+                    float v[16];
+                    tmem_ld16(t_row, v);
+#pragma unroll
+                    for (int o = 0; o < MLP_OUT; ++o) {
+                        y[o] = (v[o] + sBias[4 * 256 + o]) * A.out_scale[o] + A.out_shift[o];
+                        bad = bad || !(y[o] >= A.lab_lo[o] - 1.0f && y[o] <= A.lab_hi[o] + 1.0f);
+                    }
+                }
+                if (MODE == 0) {
+                    if (ch == 0 && r_global < A.rows) {
+                        float4 *o4 = reinterpret_cast<float4 *>(A.out + r_global * MLP_OUT);
+                        o4[0] = make_float4(y[0], y[1], y[2], y[3]);
+                        o4[1] = make_float4(y[4], y[5], y[6], y[7]);
+                    }
+                } else {
+                    const MlpPaintArgs &P = A.p;
+                    float e[9];
+#pragma unroll
+                    for (int k = 0; k < 9; ++k) e[k] = 0.0f;
+                    if (ch == 0 && r_global < A.rows) {
+                        use = P.eligible[r_global] != 0;
+                        if (use && bad) {
+                            uint32_t cell = (uint32_t)(r_global / P.rows_per_cell),
+                                     s = (uint32_t)(r_global % P.rows_per_cell);
+                            unsigned slot = atomicAdd(P.retry_count, 1u);
+                            if (slot < P.retry_cap) P.retry[slot] = make_uint2(cell, P.source_begin + s);
+                            use = false;
+                        }
+                        if (use) {
+                            const float4 *cf = reinterpret_cast<const float4 *>(P.coef + r_global * 16);
+                            float c[16];
+#pragma unroll
+                            for (int q = 0; q < 4; ++q) {
+                                float4 f = __ldg(cf + q);
+                                c[4 * q] = f.x;
+                                c[4 * q + 1] = f.y;
+                                c[4 * q + 2] = f.z;
+                                c[4 * q + 3] = f.w;
+                            }
+#pragma unroll
+                            for (int o = 0; o < MLP_OUT; ++o) {
+                                float en = exp2f(-y[o] * 0.33219280948873623f);
+                                e[o] = c[o] * en;
+                                e[8] += c[8 + o] * en;
+                            }
+                        }
+                    }
+                    if (ch == 0) {
+                        unsigned taken = __popc(__ballot_sync(0xffffffffu, use));
+                        if (lane == 0 && taken) atomicAdd(P.taken, (unsigned long long)taken);
+#pragma unroll
+                        for (int k = 0; k < 9; ++k) {
+                            float sum = e[k];
+#pragma unroll
+                            for (int m = 16; m > 0; m >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, m);
+                            if (lane == 0) s_red[lq][k] = sum;
+                        }
+                    }
+                    __syncthreads();
+                    if (tid < 9) {
+                        float sum = s_red[0][tid] + s_red[1][tid] + s_red[2][tid] + s_red[3][tid];
+                        const size_t row0 = tile * 128;
+                        const size_t cell = row0 / P.rows_per_cell, slice = (row0 % P.rows_per_cell) / 128;
+                        P.partial[(slice * (size_t)P.cells + cell) * 9 + tid] += sum;
+                    }
+                }
+                tc_before_sync();
+                __syncthreads();
+            }
+        }
+    }
+    if (!ok && tid == 0) atomicOr(A.error, 1u);
+    tc_after_sync();
+    __syncthreads();
+    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(UM_TMEM_COLS) : "memory");
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -553,6 +879,27 @@ __global__ void stats_kernel(const float *rows, const uint8_t *keep, size_t n, i
 
 namespace {
 
+cudaError_t set_umma_smem() {
+    cudaError_t e = cudaFuncSetAttribute(mlp_umma_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)UM_SMEM);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(mlp_umma_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)UM_SMEM);
+    return e;
+}
+
+UmmaArgs umma_args(const MlpDev &net) {
+    UmmaArgs a{};
+    a.wpack = net.wpack;
+    a.master = net.master;
+    for (int o = 0; o < MLP_OUT; ++o) {
+        a.out_shift[o] = net.scales.out_shift[o];
+        a.out_scale[o] = net.scales.out_scale[o];
+        a.lab_lo[o] = net.scales.lab_lo[o];
+        a.lab_hi[o] = net.scales.lab_hi[o];
+    }
+    a.error = net.error;
+    return a;
+}
+
 cudaError_t set_fused_smem() {
     const int smem = 2 * CH_ELEMS * (int)sizeof(__nv_bfloat16);
     cudaError_t e = cudaFuncSetAttribute(mlp_fused_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
@@ -584,8 +931,13 @@ unsigned fused_grid(size_t rows) {
 
 }  // namespace
 
+size_t mlp_packed_bytes() { return UM_W_BYTES; }
+
 cudaError_t mlp_cast(const MlpDev &net, cudaStream_t stream) {
     cast_kernel<<<(unsigned)((MLP_W16 + 255) / 256), 256, 0, stream>>>(net.master, net.w16);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess || !net.wpack) return e;
+    pack_umma_kernel<<<(unsigned)((UM_W_BYTES / 2 + 255) / 256), 256, 0, stream>>>(net.w16, net.wpack);
     return cudaGetLastError();
 }
 
@@ -598,6 +950,16 @@ cudaError_t mlp_normalise(const MlpScales &s, const float *raw, size_t n, __nv_b
 
 cudaError_t mlp_forward(const MlpDev &net, const __nv_bfloat16 *x, size_t n, float *out, cudaStream_t stream) {
     if (n == 0) return cudaSuccess;
+    if (net.kernel == 0) {
+        cudaError_t e = set_umma_smem();
+        if (e != cudaSuccess) return e;
+        UmmaArgs a = umma_args(net);
+        a.x = x;
+        a.rows = n;
+        a.out = out;
+        mlp_umma_kernel<0><<<fused_grid(n), UM_THREADS, UM_SMEM, stream>>>(a);
+        return cudaGetLastError();
+    }
     cudaError_t e = set_fused_smem();
     if (e != cudaSuccess) return e;
     FusedArgs a = fused_args(net);
@@ -610,6 +972,16 @@ cudaError_t mlp_forward(const MlpDev &net, const __nv_bfloat16 *x, size_t n, flo
 
 cudaError_t mlp_paint(const MlpDev &net, const MlpPaintArgs &p, cudaStream_t stream) {
     if (p.rows == 0) return cudaSuccess;
+    if (net.kernel == 0) {
+        cudaError_t e = set_umma_smem();
+        if (e != cudaSuccess) return e;
+        UmmaArgs a = umma_args(net);
+        a.x = p.x;
+        a.rows = p.rows;
+        a.p = p;
+        mlp_umma_kernel<1><<<fused_grid(p.rows), UM_THREADS, UM_SMEM, stream>>>(a);
+        return cudaGetLastError();
+    }
     cudaError_t e = set_fused_smem();
     if (e != cudaSuccess) return e;
     FusedArgs a = fused_args(net);

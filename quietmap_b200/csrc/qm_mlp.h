@@ -46,11 +46,17 @@ struct MlpScales {
 struct MlpDev {
     float *master = nullptr;          // [MLP_WEIGHTS] FP32 weights and biases
     __nv_bfloat16 *w16 = nullptr;     // [MLP_W16] BF16 matrices
+    __nv_bfloat16 *wpack = nullptr;   // [mlp_packed_bytes()] the matrices in the tcgen05 operand layout
+    unsigned *error = nullptr;        // set by an inference kernel whose bounded wait gave up
+    int kernel = 0;                   // inference: 0 tcgen05 (tensor memory), 1 mma.sync
     float *adam_m = nullptr, *adam_v = nullptr;  // Adam moments (allocated by training)
     MlpScales scales;
 };
 
-// Refreshes the BF16 matrices from the FP32 master weights.
+// Bytes of the packed tcgen05 operand copy of the matrices.
+size_t mlp_packed_bytes();
+
+// Refreshes the BF16 matrices (and their packed copy, when allocated) from the FP32 master weights.
 cudaError_t mlp_cast(const MlpDev &net, cudaStream_t stream);
 
 // Normalised BF16 feature rows from raw FP32 rows: x' = (x - shift) * scale.

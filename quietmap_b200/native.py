@@ -66,6 +66,8 @@ def lib():
         L.qm_surrogate_create.argtypes = [C.c_void_p, _F, P]
         L.qm_surrogate_create.restype = C.c_int
         L.qm_surrogate_free.argtypes = [C.c_void_p]
+        L.qm_surrogate_set_kernel.argtypes = [C.c_void_p, C.c_int]
+        L.qm_surrogate_set_kernel.restype = C.c_int
         L.qm_surrogate_params.argtypes = [C.c_void_p, _F]
         L.qm_surrogate_params.restype = C.c_int
         L.qm_surrogate_samples.argtypes = [C.c_void_p, C.POINTER(abi.GridDesc), _F, _F, C.POINTER(C.c_uint8)]
@@ -309,6 +311,10 @@ class Surrogate:
             self.close()
         except Exception:
             pass
+
+    def set_kernel(self, kernel):
+        """0: the tcgen05 inference kernel (default); 1: the mma.sync one."""
+        _check(lib().qm_surrogate_set_kernel(self.handle, kernel), self.ctx.handle)
 
     def params(self):
         p = np.zeros(abi.SURR_PARAMS, np.float32)

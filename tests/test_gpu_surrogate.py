@@ -75,6 +75,22 @@ def test_forward_matches_the_oracle(ctx, road):
     np.testing.assert_allclose(net.forward(x[:131]), out[:131], rtol=0, atol=1e-6)
 
 
+def test_tensor_memory_and_mma_sync_kernels_agree(ctx, road):
+    """The tcgen05 inference kernel (the default) and the mma.sync one on the same rows, including a
+    ragged last tile."""
+    scene, full = road
+    dev = ctx.scene(scene)
+    f, lab, ok = dev.surrogate_samples(_coarse_grid(full, 2, 3000, source_end=700))
+    x = f[ok][:1000]
+    net = native.Surrogate(ctx, _random_params(13, x))
+    a = net.forward(x)
+    net.set_kernel(1)
+    b = net.forward(x)
+    net.set_kernel(0)
+    d = np.abs(a - b) / 4.0
+    assert np.percentile(d, 99) < 0.005 and d.max() < 0.02, (np.percentile(d, 99), d.max())
+
+
 def test_gradients_match_the_oracle(ctx, road):
     scene, full = road
     dev = ctx.scene(scene)
