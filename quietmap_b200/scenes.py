@@ -199,7 +199,7 @@ def _segments_to_points(rng, n_segments, side_m, step_m, kind_of, base_of, margi
 
 
 def road_square(seed=1, n_roads=400, n_buildings=300, side_m=1000.0, receivers=128,
-                cell_steps=256):
+                cell_steps=1024):
     """The plain CNOSSOS road painter: flat G = 0.5, homogeneous conditions, 15 C / 70 %."""
     rng = np.random.default_rng(seed)
     step_m = 1.0 / 32.0
