@@ -11,18 +11,26 @@
  *
  * with BF16 weights and activations in the matrix products and FP32 accumulation. The network
  * is trained on the GPU by this library's own forward and backward kernels, on labels the exact
- * path code computes. Geometry: flat ground (no DEM) with buildings, homogeneous conditions.
+ * path code computes. A network serves one feature set, fixed by the scene it was trained on.
  *
- * Features of a path from source S to receiver R (horizontal length L metres):
+ * Flat feature set (scenes without a DEM, homogeneous conditions), path from source S to
+ * receiver R (horizontal length L metres):
  *   f0 L / 1000; f1 source height above the ground at S / 10; f2 receiver height above the
  *   ground at R / 10; f3 (ground at R - ground at S) / 10; f4 condition (0 homogeneous);
  *   f5, f6, f7 ground factor at S (the source's own G when it has one), at the middle and at R;
  *   f8 .. f31 up to 8 roofs crossed (the vertical path's roof spans after clipping, in their
  *   closing order), each as (x0 / L, x1 / L, height above the ground / 10); absent roofs are
  *   zeros (a present roof has x1 > x0 > 0, which is its mask).
- * A path is eligible when all its obstacle tops pair into roofs, it crosses at most 8 roofs and
- * its features lie inside the training ranges; other paths, and paths whose predicted levels
- * fall outside the training labels' range, are evaluated by the exact path code.
+ * Terrain feature set (scenes with a DEM; both conditions, one row per state): f0 .. f3 and
+ *   f5 .. f7 as above (f6 the mean ground factor of the samples below), f4 the state (0
+ *   homogeneous, 1 favourable); f8 .. f19 over 12 equal stretches of the path, the largest rise
+ *   of the terrain above the straight source-receiver line among 3 DEM samples each (metres /
+ *   10); f20 .. f31 over the same stretches, the largest rise of the obstacle tops the path
+ *   crosses above that line (-10 where it crosses none).
+ * A flat path is eligible when all its obstacle tops pair into roofs and it crosses at most 8
+ * roofs, a terrain path when its crossing list fits; both need their features inside the
+ * training ranges. Other paths, and paths whose predicted levels fall outside the training
+ * labels' range, are evaluated by the exact path code.
  */
 #ifndef QM_SURROGATE_H
 #define QM_SURROGATE_H
@@ -40,10 +48,10 @@ extern "C" {
 #define QM_SURR_MAX_ROOFS 8
 /* Parameters, in this order (FP32): W1[256][32], b1[256], W2..W4[256][256], b2..b4[256],
  * W5[8][256], b5[8], then the input shift[32] and scale[32] (x' = (x - shift) * scale), the
- * output shift[8] and scale[8] (A = y * scale + shift), and the eligible feature range lo[32],
- * hi[32] and label range lo[8], hi[8]. */
+ * output shift[8] and scale[8] (A = y * scale + shift), the eligible feature range lo[32],
+ * hi[32], the label range lo[8], hi[8], and the feature set (0 flat, 1 terrain). */
 #define QM_SURR_WEIGHTS (256 * 32 + 256 + 3 * (256 * 256 + 256) + 8 * 256 + 8)
-#define QM_SURR_PARAMS (QM_SURR_WEIGHTS + 32 + 32 + 8 + 8 + 32 + 32 + 8 + 8)
+#define QM_SURR_PARAMS (QM_SURR_WEIGHTS + 32 + 32 + 8 + 8 + 32 + 32 + 8 + 8 + 1)
 
 typedef struct qm_surrogate qm_surrogate;
 
@@ -58,10 +66,11 @@ qm_status qm_surrogate_set_kernel(qm_surrogate *net, int kernel);
 /* Its current parameters (QM_SURR_PARAMS floats; the FP32 master copy). */
 qm_status qm_surrogate_params(const qm_surrogate *net, float *params);
 
-/* Training samples from the exact path code: for every path (cell, source) of the grid, row
- * cell * n_sources + (source - source_begin): its raw features (features[rows][32]), its exact
- * A_boundary per band of the homogeneous state (labels[rows][8], dB), and whether its geometry
- * is eligible (eligible[rows], 0/1; the feature range test is not applied). */
+/* Training samples from the exact path code: for every path (cell, source) of the grid, its raw
+ * features (features[rows][32]), its exact A_boundary per band (labels[rows][8], dB) and whether
+ * its geometry is eligible (eligible[rows], 0/1; the feature range test is not applied). Flat
+ * scenes: one row per path, row cell * n_sources + (source - source_begin), the homogeneous
+ * state. Terrain scenes: two rows per path (2 * that + state), homogeneous then favourable. */
 qm_status qm_surrogate_samples(qm_scene *scene, const qm_grid_desc *grid, float *features,
                                float *labels, uint8_t *eligible);
 
@@ -93,8 +102,8 @@ qm_status qm_surrogate_train(qm_surrogate *net, qm_scene *scene, const qm_grid_d
 
 /* The grid painter with the surrogate: `qm_paint_grid`'s outputs, where eligible paths take
  * A_boundary from the network and the others (and out-of-range predictions) run the exact
- * path. stats->paths counts every path; surrogate_paths (nullable) those the network took.
- * Flat scenes (no DEM) in homogeneous conditions only (QM_ERR_UNSUPPORTED otherwise). */
+ * path. stats->paths counts every path; surrogate_paths (nullable) those the network took. The
+ * scene must be of the network's feature set (flat scenes: homogeneous conditions only). */
 qm_status qm_paint_grid_surrogate(qm_scene *scene, const qm_grid_desc *grid, qm_surrogate *net,
                                   float *cell_bands, float *cell_dba, float *cell_lden,
                                   uint32_t *histogram, qm_paint_stats *stats,

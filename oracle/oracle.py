@@ -233,12 +233,13 @@ class OracleScene:
 
     def surrogate_samples(self, grid, cell_begin=0, cell_end=0, nthreads=None):
         """Surrogate features [rows][32], exact A_boundary labels [rows][8] (dB) and eligibility of
-        every path of cells [cell_begin, cell_end) (all when empty) against the grid's sources."""
+        every path of cells [cell_begin, cell_end) (all when empty) against the grid's sources
+        (terrain scenes: two rows a path, homogeneous then favourable)."""
         g = abi.grid_desc(grid)
         if cell_end <= cell_begin:
             cell_begin, cell_end = 0, grid.cells
         n_src = (grid.source_end - grid.source_begin) if grid.source_end > grid.source_begin else len(self.scene.sources)
-        rows = (cell_end - cell_begin) * n_src
+        rows = (cell_end - cell_begin) * n_src * (2 if self.scene.dem_altitude is not None else 1)
         f = np.zeros((rows, 32))
         lab = np.zeros((rows, 8))
         e = np.zeros(rows, np.uint8)

@@ -1438,6 +1438,61 @@ uint32_t level_bin(double level_db, double level_min, double bin_db, uint32_t n_
 
 // =============================================================================================
 // C entry points (ctypes).
+// The terrain feature set of include/qm_surrogate.h for one path, two rows (homogeneous and
+// favourable): 36 DEM samples at lattice points rounded from t = (i + 0.5) / 36 along the path,
+// the largest rise of the ground above the straight source-receiver line in each of 12 stretches,
+// and the largest rise of the obstacle tops crossed (walls standing on the ground at their
+// rounded crossing points) in each stretch.
+void terrain_sample(const Scene &s, const qm_source &src, const Receiver &r, const Worker &w, const PathBuffers &pb,
+                    const StateBoundary boundaries[2], double *f, double *labels, uint8_t *eligible) {
+    const int64_t dx = r.x - src.x, dy = r.y - src.y;
+    const double L = std::max(w.profile.horizontal_m, 1.0);
+    double zs, gs, zr, gr;
+    terrain_at_point(s, src.x, src.y, zs, gs);
+    terrain_at_point(s, r.x, r.y, zr, gr);
+    const double src_alt = zs + src.height_m;
+    const double rise = (r.altitude_m - src_alt) / L;
+    auto ground_at = [&](double t, double &z, double &g) {
+        int64_t px = src.x + (int64_t)std::llrint(t * (double)dx), py = src.y + (int64_t)std::llrint(t * (double)dy);
+        terrain_at_point(s, px, py, z, g);
+    };
+    double gsum = 0.0;
+    for (int j = 0; j < 12; ++j) {
+        double top = -INF;
+        for (int q = 0; q < 3; ++q) {
+            double t = (j * 3 + q + 0.5) / 36.0, z, g;
+            ground_at(t, z, g);
+            top = std::max(top, z - (src_alt + rise * t * L));
+            gsum += g;
+        }
+        f[8 + j] = top / 10.0;
+    }
+    for (int j = 0; j < 12; ++j) f[20 + j] = -10.0;
+    for (const Crossing &c : w.crossings) {
+        if (std::binary_search(pb.containing.begin(), pb.containing.end(), c.footprint_id)) continue;
+        double z, g;
+        ground_at(c.t, z, g);
+        int j = std::min((int)(c.t * 12.0), 11);
+        f[20 + j] = std::max(f[20 + j], (z + c.height_m - (src_alt + rise * c.t * L)) / 10.0);
+    }
+    const bool ok = true;
+    f[0] = L / 1000.0;
+    f[1] = src.height_m / 10.0;
+    f[2] = (r.altitude_m - zr) / 10.0;
+    f[3] = (zr - zs) / 10.0;
+    f[5] = src.ground_factor >= 0.0f ? (double)src.ground_factor : gs;
+    f[6] = gsum / 36.0;
+    f[7] = gr;
+    for (int state = 0; state < 2; ++state) {
+        double *fs = f + state * 32;
+        if (state == 1)
+            for (int k = 0; k < 32; ++k) fs[k] = f[k];
+        fs[4] = (double)state;
+        for (int b = 0; b < BANDS; ++b) labels[state * BANDS + b] = boundaries[state].attenuation[b];
+        eligible[state] = ok ? 1 : 0;
+    }
+}
+
 extern "C" {
 
 int qmo_version(void) { return 1; }
@@ -1727,6 +1782,7 @@ void qmo_surrogate_samples(void *scene, const qm_grid_desc *grid, uint32_t cell_
         se = (uint32_t)s.sources.size();
     }
     const uint32_t n_src = se - sb;
+    const bool terrain = s.dem_nx != 0;
     std::vector<Worker> workers(std::max(threads, 1));
     parallel_for(cell_end - cell_begin, threads, [&](size_t k, int t) {
         uint32_t cell = cell_begin + (uint32_t)k;
@@ -1736,7 +1792,7 @@ void qmo_surrogate_samples(void *scene, const qm_grid_desc *grid, uint32_t cell_
         Worker &w = workers[t];
         for (uint32_t si = sb; si < se; ++si) {
             const qm_source &src = s.sources[si];
-            size_t row = k * n_src + (si - sb);
+            size_t row = (k * n_src + (si - sb)) * (terrain ? 2 : 1);
             int64_t from[2] = {src.x, src.y}, to[2] = {r.x, r.y};
             fill_profile(s, from, to, w.profile);
             scene_crossings(s, from, to, w.crossings);
@@ -1758,8 +1814,13 @@ void qmo_surrogate_samples(void *scene, const qm_grid_desc *grid, uint32_t cell_
             double p[PERIODS] = {0.0, 0.0, 0.0};
             Transfer transfer;
             StateBoundary boundaries[2];
-            ray_terms(w.profile, w.crossings, ends, p, s.alpha, w.ray, transfer, boundaries, false);
+            ray_terms(w.profile, w.crossings, ends, p, s.alpha, w.ray, transfer, boundaries, terrain);
             const PathBuffers &pb = w.ray.pb;
+            if (terrain) {
+                terrain_sample(s, src, r, w, pb, boundaries, features + row * 32, labels + row * BANDS,
+                               eligible + row);
+                continue;
+            }
             for (int b = 0; b < BANDS; ++b) labels[row * BANDS + b] = boundaries[0].attenuation[b];
             // Eligibility: tops all roof-bounding, hits all paired, at most 16 hits.
             bool ok = pb.tops.size() == pb.buildings.size() && pb.buildings.size() <= 16;

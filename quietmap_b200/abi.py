@@ -206,7 +206,7 @@ class PackedScene:
 SURR_FEATURES, SURR_HIDDEN, SURR_OUTPUTS = 32, 256, 8
 SURR_DIMS = (32, 256, 256, 256, 256, 8)
 SURR_WEIGHTS = sum(SURR_DIMS[k + 1] * SURR_DIMS[k] + SURR_DIMS[k + 1] for k in range(5))
-SURR_PARAMS = SURR_WEIGHTS + 32 + 32 + 8 + 8 + 32 + 32 + 8 + 8
+SURR_PARAMS = SURR_WEIGHTS + 32 + 32 + 8 + 8 + 32 + 32 + 8 + 8 + 1
 
 
 class TrainConfig(C.Structure):

@@ -561,8 +561,9 @@ qm_status qm_paint_grid(qm_scene *scene, const qm_grid_desc *grid, float *cell_b
     A.chunk = std::max<uint32_t>(1, (n_src + n_chunks - 1) / n_chunks);
     A.n_chunks = n_src == 0 ? 1 : (n_src + A.chunk - 1) / A.chunk;
     const uint32_t slices = A.n_chunks + 1;  // the last slice holds the re-run paths
-    // The retry list holds up to 1 path in 128 (and at least 1 M): over-capacity paths are rare.
-    A.retry_cap = (uint32_t)std::min<int64_t>(std::max<int64_t>((int64_t)cells * n_src / 128, 1 << 20), 1 << 25);
+    // The re-run list holds up to 1 path in 16 (at least 1 M, at most 2^27): over-capacity paths are
+    // rare, but tiles in dense quarters with kilometre-long rays reach a few per cent.
+    A.retry_cap = (uint32_t)std::min<int64_t>(std::max<int64_t>((int64_t)cells * n_src / 16, 1 << 20), 1 << 27);
     Scratch d_alt, d_own, d_partial, d_failed, d_counters, d_dba, d_hist, d_bands, d_dbaout, d_lden, d_retry, d_rcount;
     size_t partial_bytes = (size_t)slices * cells * GRID_SLOTS * sizeof(float);
     QM_CUDA(cudaMalloc(&d_alt.p, cells * sizeof(float)));
@@ -1287,6 +1288,7 @@ void scales_from_params(const float *p, MlpScales &s) {
     take(s.feat_hi, MLP_IN);
     take(s.lab_lo, MLP_OUT);
     take(s.lab_hi, MLP_OUT);
+    take(&s.feature_set, 1);
 }
 
 void scales_to_params(const MlpScales &s, float *p) {
@@ -1303,6 +1305,7 @@ void scales_to_params(const MlpScales &s, float *p) {
     put(s.feat_hi, MLP_IN);
     put(s.lab_lo, MLP_OUT);
     put(s.lab_hi, MLP_OUT);
+    put(&s.feature_set, 1);
 }
 
 // The grid checks qm_paint_grid makes.
@@ -1343,7 +1346,7 @@ qm_status setup_grid(qm_scene *scene, const qm_grid_desc &g, uint32_t sb, uint32
     A.source_end = se;
     A.tile_w = 16;
     A.tile_h = 8;
-    A.want_fav = false;
+    A.want_fav = scene->any_favourable;
     for (int p = 0; p < 3; ++p) A.lden_w[p] = (float)LDEN_W[p];
     G.tiles = ((g.nx + A.tile_w - 1) / A.tile_w) * ((g.ny + A.tile_h - 1) / A.tile_h);
     const uint32_t n_src = se - sb;
@@ -1406,7 +1409,8 @@ qm_status grid_samples(qm_scene *scene, const qm_grid_desc &g, Scratch &feat, Sc
     GridSetup G;
     qm_status st = setup_grid(scene, g, sb, se, G, stream);
     if (st != QM_OK) return st;
-    rows = (size_t)G.cells * (se - sb);
+    const size_t per_path = scene->dem_nx != 0 ? 2 : 1;
+    rows = (size_t)G.cells * (se - sb) * per_path;
     if (rows == 0) return QM_OK;
     QM_CUDA(cudaMalloc(&feat.p, rows * MLP_IN * sizeof(float)));
     QM_CUDA(cudaMalloc(&lab.p, rows * MLP_OUT * sizeof(float)));
@@ -1416,7 +1420,10 @@ qm_status grid_samples(qm_scene *scene, const qm_grid_desc &g, Scratch &feat, Sc
     P.features = static_cast<float *>(feat.p);
     P.labels = static_cast<float *>(lab.p);
     P.eligible = static_cast<uint8_t *>(elig.p);
-    surrogate_samples_kernel<<<dim3(G.tiles, G.A.n_chunks), 128, 0, stream>>>(scene->dev, P);
+    if (per_path == 2)
+        surrogate_samples_terrain_kernel<<<dim3(G.tiles, G.A.n_chunks), 128, 0, stream>>>(scene->dev, P);
+    else
+        surrogate_samples_kernel<<<dim3(G.tiles, G.A.n_chunks), 128, 0, stream>>>(scene->dev, P);
     QM_CUDA(cudaGetLastError());
     QM_CUDA(cudaStreamSynchronize(stream));
     return QM_OK;
@@ -1480,7 +1487,6 @@ qm_status qm_surrogate_samples(qm_scene *scene, const qm_grid_desc *grid, float 
                                uint8_t *eligible) {
     if (!scene || !grid || !features || !labels || !eligible)
         return fail(QM_ERR_ARGUMENT, "qm_surrogate_samples: null scene, grid or output");
-    if (scene->dem_nx != 0) return fail(QM_ERR_UNSUPPORTED, "qm_surrogate_samples: the surrogate covers flat scenes only");
     qm_status st = check_grid(scene, *grid, "qm_surrogate_samples");
     if (st != QM_OK) return st;
     std::lock_guard<std::mutex> guard(scene->ctx->lock);
@@ -1557,7 +1563,6 @@ qm_status qm_surrogate_train(qm_surrogate *net, qm_scene *scene, const qm_grid_d
     if (!net || !scene || !grids || !config || n_grids == 0)
         return fail(QM_ERR_ARGUMENT, "qm_surrogate_train: null net, scene, grids or config");
     if (scene->ctx != net->ctx) return fail(QM_ERR_ARGUMENT, "qm_surrogate_train: net and scene on different contexts");
-    if (scene->dem_nx != 0) return fail(QM_ERR_UNSUPPORTED, "qm_surrogate_train: the surrogate covers flat scenes only");
     const qm_train_config &c = *config;
     if (c.epochs == 0 || c.batch < 256 || c.batch % 128 != 0 || c.batch > (1u << 20) || !(c.learning_rate > 0.0f))
         return fail(QM_ERR_ARGUMENT, "qm_surrogate_train: epochs >= 1, batch a multiple of 128 in [256, 2^20], learning_rate > 0");
@@ -1573,7 +1578,7 @@ qm_status qm_surrogate_train(qm_surrogate *net, qm_scene *scene, const qm_grid_d
     for (size_t k = 0; k < n_grids; ++k) {
         const qm_grid_desc &g = grids[k];
         uint32_t n_src = g.source_end > g.source_begin ? g.source_end - g.source_begin : scene->n_sources;
-        upper += (size_t)g.nx * g.ny * n_src;
+        upper += (size_t)g.nx * g.ny * n_src * (scene->dem_nx != 0 ? 2 : 1);
     }
     if (upper == 0) return fail(QM_ERR_ARGUMENT, "qm_surrogate_train: the grids hold no paths");
     Scratch all_f, all_l;
@@ -1656,6 +1661,7 @@ qm_status qm_surrogate_train(qm_surrogate *net, qm_scene *scene, const qm_grid_d
     QM_CUDA(cudaMemcpyAsync(hi.data(), d_hi, hi.size() * sizeof(float), cudaMemcpyDeviceToHost, stream));
     QM_CUDA(cudaStreamSynchronize(stream));
     MlpScales &S = net->net.scales;
+    S.feature_set = scene->dem_nx != 0 ? 1.0f : 0.0f;
     for (int k = 0; k < MLP_IN + MLP_OUT; ++k) {
         double mean = sum[k] / (double)total;
         double var = std::max(sq[k] / (double)total - mean * mean, 0.0);
@@ -1752,8 +1758,13 @@ qm_status qm_paint_grid_surrogate(qm_scene *scene, const qm_grid_desc *grid, qm_
                                   uint64_t *surrogate_paths) {
     if (!scene || !grid || !net) return fail(QM_ERR_ARGUMENT, "qm_paint_grid_surrogate: null scene, grid or net");
     if (scene->ctx != net->ctx) return fail(QM_ERR_ARGUMENT, "qm_paint_grid_surrogate: net and scene on different contexts");
-    if (scene->dem_nx != 0 || scene->any_favourable)
+    const bool terrain = scene->dem_nx != 0;
+    if (!terrain && scene->any_favourable)
         return fail(QM_ERR_UNSUPPORTED, "qm_paint_grid_surrogate: flat scenes in homogeneous conditions only");
+    if ((net->net.scales.feature_set != 0.0f) != terrain)
+        return fail(QM_ERR_ARGUMENT, std::string("qm_paint_grid_surrogate: the network was trained for ") +
+                                         (terrain ? "flat" : "terrain") + " scenes");
+    const uint32_t per_path = terrain ? 2 : 1;
     const qm_grid_desc &g = *grid;
     qm_status st = check_grid(scene, g, "qm_paint_grid_surrogate");
     if (st != QM_OK) return st;
@@ -1775,7 +1786,7 @@ qm_status qm_paint_grid_surrogate(qm_scene *scene, const qm_grid_desc *grid, qm_
     const uint32_t n_src = se - sb;
     // Sources in batches of whole 128-row tiles per cell, at most 2^25 rows a batch.
     const size_t max_rows = size_t(1) << 25;
-    uint32_t batch = (uint32_t)std::max<size_t>(128, (max_rows / (size_t)cells) / 128 * 128);
+    uint32_t batch = (uint32_t)std::max<size_t>(128, (max_rows / (size_t)cells / per_path) / 128 * 128);
     batch = std::min<uint32_t>(batch, ((n_src + 127) / 128) * 128);
     uint32_t max_chunks = 1;
     for (uint32_t b0 = sb; b0 < se; b0 += batch) {
@@ -1783,11 +1794,11 @@ qm_status qm_paint_grid_surrogate(qm_scene *scene, const qm_grid_desc *grid, qm_
         chunk_range(ctx, tmp, G.tiles, b0, std::min(se, b0 + batch));
         max_chunks = std::max(max_chunks, tmp.n_chunks);
     }
-    const uint32_t mlp_slices = std::max<uint32_t>(1, batch / 128);
+    const uint32_t mlp_slices = std::max<uint32_t>(1, batch * per_path / 128);
     const uint32_t slices = max_chunks + 1 + mlp_slices;
-    const size_t rows_cap = (size_t)cells * std::max<uint32_t>(batch, 128);
+    const size_t rows_cap = (size_t)cells * std::max<uint32_t>(batch, 128) * per_path;
     GridArgs A = G.A;
-    A.retry_cap = (uint32_t)std::min<int64_t>(std::max<int64_t>((int64_t)cells * n_src / 128, 1 << 20), 1 << 25);
+    A.retry_cap = (uint32_t)std::min<int64_t>(std::max<int64_t>((int64_t)cells * n_src / 16, 1 << 20), 1 << 27);
     Scratch d_partial, d_failed, d_counters, d_retry, d_rcount, d_x, d_coef, d_elig, d_taken, d_dba, d_hist, d_bands,
         d_dbaout, d_lden;
     const size_t partial_bytes = (size_t)slices * cells * GRID_SLOTS * sizeof(float);
@@ -1817,7 +1828,7 @@ qm_status qm_paint_grid_surrogate(qm_scene *scene, const qm_grid_desc *grid, qm_
     QM_CUDA(cudaEventRecord(ev.e0, stream));
     for (uint32_t b0 = sb; b0 < se; b0 += batch) {
         const uint32_t b1 = std::min(se, b0 + batch);
-        const uint32_t rpc = ((b1 - b0 + 127) / 128) * 128;
+        const uint32_t rpc = ((per_path * (b1 - b0) + 127) / 128) * 128;
         const size_t rows = (size_t)cells * rpc;
         SurrPaintArgs P{};
         P.g = A;
@@ -1833,7 +1844,10 @@ qm_status qm_paint_grid_surrogate(qm_scene *scene, const qm_grid_desc *grid, qm_
             P.hi[k] = S.feat_hi[k];
         }
         QM_CUDA(cudaMemsetAsync(d_elig.p, 0, rows, stream));
-        surrogate_front_kernel<<<dim3(G.tiles, P.g.n_chunks), 128, 0, stream>>>(scene->dev, P);
+        if (terrain)
+            surrogate_front_terrain_kernel<<<dim3(G.tiles, P.g.n_chunks), 128, 0, stream>>>(scene->dev, P);
+        else
+            surrogate_front_kernel<<<dim3(G.tiles, P.g.n_chunks), 128, 0, stream>>>(scene->dev, P);
         QM_CUDA(cudaGetLastError());
         MlpPaintArgs M{};
         M.x = P.x;
@@ -1845,6 +1859,7 @@ qm_status qm_paint_grid_surrogate(qm_scene *scene, const qm_grid_desc *grid, qm_
         M.partial = A.partial + (size_t)(max_chunks + 1) * cells * GRID_SLOTS;
         M.source_begin = b0;
         M.n_sources = b1 - b0;
+        M.rows_per_path = per_path;
         M.retry = A.retry;
         M.retry_cap = A.retry_cap;
         M.retry_count = A.retry_count;
@@ -2146,7 +2161,7 @@ qm_status qm_batch_plan_create(qm_scene *scene, const qm_tile_desc *tiles, size_
         QM_CUDA(cudaMemcpyAsync(L.items.p, items.data(), items.size() * sizeof(WorkItem), cudaMemcpyHostToDevice, stream));
         QM_CUDA(cudaStreamSynchronize(stream));
     }
-    P->retry_cap = (uint32_t)std::min<uint64_t>(std::max<uint64_t>(total_paths / 128, 1 << 20), 1 << 25);
+    P->retry_cap = (uint32_t)std::min<uint64_t>(std::max<uint64_t>(total_paths / 16, 1 << 20), 1 << 27);
     QM_CUDA(cudaMalloc(&P->d_tiles.p, P->tiles.size() * sizeof(TileDev)));
     QM_CUDA(cudaMalloc(&P->d_cell_tile.p, n_cells * sizeof(uint32_t)));
     QM_CUDA(cudaMalloc(&P->d_rcv_xy.p, n_cells * sizeof(int2)));

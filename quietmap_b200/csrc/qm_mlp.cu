@@ -539,16 +539,28 @@ __global__ void __launch_bounds__(UM_THREADS, 1) mlp_umma_kernel(UmmaArgs A) {
                     float e[9];
 #pragma unroll
                     for (int k = 0; k < 9; ++k) e[k] = 0.0f;
-                    if (ch == 0 && r_global < A.rows) {
-                        use = P.eligible[r_global] != 0;
-                        if (use && bad) {
-                            uint32_t cell = (uint32_t)(r_global / P.rows_per_cell),
-                                     s = (uint32_t)(r_global % P.rows_per_cell);
-                            unsigned slot = atomicAdd(P.retry_count, 1u);
-                            if (slot < P.retry_cap) P.retry[slot] = make_uint2(cell, P.source_begin + s);
+                    if (ch == 0) {
+                        use = r_global < A.rows && P.eligible[r_global] != 0;
+                        // A path whose row (or, with two rows a path, either row) leaves the label
+                        // range goes to the exact re-run once, and none of its rows is used.
+                        bool drop = use && bad;
+                        if (P.rows_per_path == 2) {
+                            // Every lane takes part in the shuffle (no short-circuit around it).
+                            const bool partner = __shfl_xor_sync(0xffffffffu, drop, 1) != 0;
+                            drop = drop || partner;
+                        }
+                        if (drop) {
+                            if (P.rows_per_path == 1 || (lane & 1) == 0) {
+                                uint32_t cell = (uint32_t)(r_global / P.rows_per_cell),
+                                         s = (uint32_t)((r_global % P.rows_per_cell) / P.rows_per_path);
+                                unsigned slot = atomicAdd(P.retry_count, 1u);
+                                if (slot < P.retry_cap) P.retry[slot] = make_uint2(cell, P.source_begin + s);
+                            }
                             use = false;
                         }
-                        if (use) {
+                    }
+                    if (ch == 0 && use) {
+                        {
                             const float4 *cf = reinterpret_cast<const float4 *>(P.coef + r_global * 16);
                             float c[16];
 #pragma unroll
@@ -568,7 +580,7 @@ __global__ void __launch_bounds__(UM_THREADS, 1) mlp_umma_kernel(UmmaArgs A) {
                         }
                     }
                     if (ch == 0) {
-                        unsigned taken = __popc(__ballot_sync(0xffffffffu, use));
+                        unsigned taken = __popc(__ballot_sync(0xffffffffu, use && (P.rows_per_path == 1 || (lane & 1) == 0)));
                         if (lane == 0 && taken) atomicAdd(P.taken, (unsigned long long)taken);
 #pragma unroll
                         for (int k = 0; k < 9; ++k) {
@@ -972,7 +984,7 @@ cudaError_t mlp_forward(const MlpDev &net, const __nv_bfloat16 *x, size_t n, flo
 
 cudaError_t mlp_paint(const MlpDev &net, const MlpPaintArgs &p, cudaStream_t stream) {
     if (p.rows == 0) return cudaSuccess;
-    if (net.kernel == 0) {
+    if (net.kernel == 0 || p.rows_per_path == 2) {  // the mma.sync kernel takes one row a path only
         cudaError_t e = set_umma_smem();
         if (e != cudaSuccess) return e;
         UmmaArgs a = umma_args(net);

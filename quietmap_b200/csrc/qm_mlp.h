@@ -41,6 +41,7 @@ struct MlpScales {
     float out_shift[MLP_OUT], out_scale[MLP_OUT];
     float feat_lo[MLP_IN], feat_hi[MLP_IN];
     float lab_lo[MLP_OUT], lab_hi[MLP_OUT];
+    float feature_set;  // 0 flat, 1 terrain
 };
 
 struct MlpDev {
@@ -75,6 +76,7 @@ struct MlpPaintArgs {
     const uint8_t *eligible;
     size_t rows;
     uint32_t rows_per_cell;
+    uint32_t rows_per_path;  // 1, or 2 (homogeneous and favourable rows of one path, adjacent)
     int cells;
     float *partial;  // [rows_per_cell / 128][cells][9]
     uint32_t source_begin, n_sources;

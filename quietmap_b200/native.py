@@ -198,9 +198,10 @@ class DeviceScene:
 
     def surrogate_samples(self, grid):
         """Every path of `grid`: (raw features [rows][32], exact A_boundary labels [rows][8] dB,
-        eligible [rows]) with row = cell * n_sources + source offset."""
+        eligible [rows]) with row = cell * n_sources + source offset (terrain scenes: two rows a
+        path, homogeneous then favourable)."""
         n_src = (grid.source_end - grid.source_begin) if grid.source_end > grid.source_begin else len(self.scene.sources)
-        rows = grid.cells * n_src
+        rows = grid.cells * n_src * (2 if self.scene.dem_altitude is not None else 1)
         g = abi.grid_desc(grid)
         f = np.zeros((rows, 32), np.float32)
         lab = np.zeros((rows, 8), np.float32)
@@ -287,6 +288,7 @@ def init_params(seed=0):
     p[q + 112:q + 144] = 3e38         # feat_hi
     p[q + 144:q + 152] = -3e38        # lab_lo
     p[q + 152:q + 160] = 3e38         # lab_hi
+    p[q + 160] = 0.0                  # feature set: flat
     return p
 
 

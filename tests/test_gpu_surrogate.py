@@ -158,3 +158,51 @@ def test_surrogate_painter_matches_the_exact_painter(ctx, road, trained):
     print(f"cells dBA |surrogate - exact| p50 {np.median(d):.4f} p99 {np.percentile(d, 99):.4f} max {d.max():.4f}; "
           f"surrogate paths {sst['surrogate_paths']} of {sst['paths']}")
     assert np.percentile(d, 99) < 0.5
+
+
+@pytest.fixture(scope="module")
+def terrain():
+    return scenes.terrain_square(scale=0.25)
+
+
+def test_terrain_samples_match_the_oracle(ctx, terrain):
+    scene, full = terrain
+    dev = ctx.scene(scene)
+    sp = full.spacing * (full.nx // 3)
+    grid = scenes.Grid(origin=(full.origin[0] + 7, full.origin[1] + 11), spacing=sp, nx=3, ny=3, source_begin=0,
+                       source_end=1200)
+    f, lab, ok = dev.surrogate_samples(grid)
+    rf, rlab, rok = oracle.OracleScene(scene).surrogate_samples(grid)
+    assert len(f) == 2 * 9 * 1200
+    assert np.array_equal(ok, rok), (ok.sum(), rok.sum())
+    assert ok.mean() > 0.3
+    assert np.array_equal(f[:, 4], np.tile([0.0, 1.0], len(f) // 2))
+    df = np.abs(f[ok] - rf[ok])
+    assert df.max() < 2e-3, (df.max(axis=0), np.argwhere(df > 2e-3)[:5])
+    err = np.abs(lab - rlab)[ok]
+    assert np.percentile(err, 99) <= 0.05 and np.median(err) < 0.005, (np.percentile(err, 99), err.max())
+
+
+def test_terrain_surrogate_trains_and_paints(ctx, terrain):
+    scene, full = terrain
+    dev = ctx.scene(scene)
+    net = native.Surrogate(ctx, seed=2)
+    grids = [scenes.Grid(origin=(full.origin[0] + 13 * k, full.origin[1] + 29 * k), spacing=full.spacing * 32,
+                         nx=16, ny=16) for k in range(2)]
+    hist, n = net.train(dev, grids, epochs=3, batch=8192, learning_rate=2e-3, seed=5, max_samples=3_000_000)
+    assert hist[-1] < 0.8 * hist[0], hist
+    tile = scenes.Grid(origin=(full.origin[0] + 100 * full.spacing, full.origin[1] + 60 * full.spacing),
+                       spacing=full.spacing, nx=16, ny=8)
+    _, edba, _, _, est = dev.paint_grid(tile)
+    _, sdba, _, _, sst = dev.paint_grid_surrogate(tile, net)
+    d = np.abs(sdba - edba)
+    print(f"terrain: samples {n}, loss {hist}, surrogate paths {sst['surrogate_paths']} of {sst['paths']}, cell dBA "
+          f"p50 {np.median(d):.3f} p99 {np.percentile(d, 99):.3f} max {d.max():.3f}; exact {est['kernel_ms']:.1f} ms, "
+          f"surrogate {sst['kernel_ms']:.1f} ms")
+    assert sst["paths"] == est["paths"]
+    assert sst["surrogate_paths"] > 0.3 * sst["paths"]
+    assert np.percentile(d, 99) < 1.0
+    # a flat network refuses terrain scenes
+    flat = native.Surrogate(ctx, seed=3)
+    with pytest.raises(native.QmError):
+        dev.paint_grid_surrogate(tile, flat)

@@ -27,7 +27,7 @@ def _small_net(seed=3):
 
 def test_parameter_layout():
     assert abi.SURR_WEIGHTS == mlp.WEIGHTS == 207880
-    assert abi.SURR_PARAMS == abi.SURR_WEIGHTS + 160
+    assert abi.SURR_PARAMS == abi.SURR_WEIGHTS + 161
 
 
 def test_oracle_gradient_matches_finite_differences():
