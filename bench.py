@@ -63,7 +63,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="terrain", choices=["terrain", "road", "flights", "surrogate", "tiles"])
+    ap.add_argument("--workload", default="terrain", choices=["terrain", "road", "flights", "surrogate", "surrogate_terrain", "tiles"])
     ap.add_argument("--tiles", type=int, default=32, help="tiles workload: tiles per batch, drawn from the 4096")
     ap.add_argument("--slices", type=int, default=8, help="terrain: source-list slices (a step paints one)")
     ap.add_argument("--sources", type=int, default=0,
@@ -246,6 +246,8 @@ def main():
         return flights(args, rank, world, local)
     if args.workload == "surrogate":
         return surrogate(args, rank, world, local)
+    if args.workload == "surrogate_terrain":
+        return surrogate_terrain(args, rank, world, local)
     if args.workload == "tiles":
         return tile_batch(args, rank, world, local)
     import torch
@@ -467,6 +469,71 @@ def surrogate(args, rank, world, local):
             "cell_dba_error_db": {"p50": float(np.median(cell_err)), "p99": float(np.percentile(cell_err, 99)),
                                   "max": float(cell_err.max())},
             "training": {"samples": int(n_train), "epochs": 3, "seconds": train_s, "loss": [float(v) for v in hist]},
+            "clocks": clocks.summary(), "gpu_launches": args.steps * 5,
+        }), flush=True)
+    ctx.close()
+
+
+def surrogate_terrain(args, rank, world, local):
+    """The surrogate painter against the exact painter on the terrain square (full size: fBm DEM,
+    30,000 buildings, 3.99 M point sources, favourable p = 0.5): the network is trained first
+    (untimed) on exact paths of 12 coarse receiver grids x 25,000-source slices (80 M rows, two
+    per path), then each step paints one seeded 16 x 8 tile against one 1/8 slice of the sources
+    with both painters."""
+    import torch
+    from quietmap_b200 import native, scenes
+    scene, full = scenes.terrain_square()
+    ctx = native.Context(local if world > 1 else 0)
+    dev = ctx.scene(scene)
+    net = native.Surrogate(ctx, seed=1)
+    ns = len(scene.sources)
+    grids = [scenes.Grid(origin=(full.origin[0] + 131 * k, full.origin[1] + 257 * k), spacing=full.spacing * 128,
+                         nx=16, ny=16, source_begin=(k * 331_001) % (ns - 25_000),
+                         source_end=(k * 331_001) % (ns - 25_000) + 25_000) for k in range(12)]
+    t0 = time.perf_counter()
+    hist, n_train = net.train(dev, grids, epochs=6, batch=16384, learning_rate=2e-3, seed=3, max_samples=80_000_000)
+    train_s = time.perf_counter() - t0
+    f, lab, ok = dev.surrogate_samples(scenes.Grid(origin=(full.origin[0] + 555, full.origin[1] + 777),
+                                                   spacing=full.spacing * 300, nx=4, ny=4, source_begin=0,
+                                                   source_end=20000))
+    err = np.abs(net.forward(f[ok]) - lab[ok])
+    _, steps, _ = workload("terrain", rank, args.slices, 0)
+    flush = torch.empty(64 << 20, dtype=torch.float32, device="cuda")
+    for i in range(args.warmup):
+        dev.paint_grid_surrogate(steps[i][0], net)
+    s_ms = e_ms = 0.0
+    paths = taken = 0
+    cell_err = []
+    with ClockSampler(local) as clocks:
+        for i in range(args.steps):
+            g = steps[args.warmup + i][0]
+            flush.zero_()
+            torch.cuda.synchronize()
+            _, sdba, _, _, sst = dev.paint_grid_surrogate(g, net)
+            flush.zero_()
+            torch.cuda.synchronize()
+            _, edba, _, _, est = dev.paint_grid(g)
+            s_ms += sst["kernel_ms"]
+            e_ms += est["kernel_ms"]
+            paths += sst["paths"]
+            taken += sst["surrogate_paths"]
+            cell_err.append(np.abs(sdba - edba))
+    cell_err = np.concatenate(cell_err)
+    if rank == 0:
+        value, exact = paths / (s_ms / 1e3), paths / (e_ms / 1e3)
+        print(json.dumps({
+            "metric": METRIC, "value": value, "unit": "paths/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": s_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "bf16 network (fp32 accumulate, tcgen05), f32 path code",
+            "data": "synthetic (seeded terrain square)",
+            "config": {"workload": "surrogate painter, terrain square 16 km^2: a step is one seeded 16x8 tile x one "
+                                   f"1/{args.slices} slice of the 3.99 M sources", "l2": "flushed between painters"},
+            "exact_value": exact, "speedup_vs_exact": value / exact, "surrogate_share": taken / max(paths, 1),
+            "path_error_db": {"p50": float(np.percentile(err, 50)), "p99": float(np.percentile(err, 99)),
+                              "samples": int(err.size)},
+            "cell_dba_error_db": {"p50": float(np.median(cell_err)), "p99": float(np.percentile(cell_err, 99)),
+                                  "max": float(cell_err.max())},
+            "training": {"samples": int(n_train), "epochs": 6, "seconds": train_s, "loss": [float(v) for v in hist]},
             "clocks": clocks.summary(), "gpu_launches": args.steps * 5,
         }), flush=True)
     ctx.close()
