@@ -151,7 +151,10 @@ __device__ int list_crossings(const SceneDev &S, int sx, int sy, int rx, int ry,
                 uint2 ref = __ldg(S.cell_ref + k);
                 OutlineDev o = S.outlines[ref.y];
                 bool building = o.building != 0;
-                bool bounds = building && edge_bounds_roof(S, sx, sy, dx, dy, ref.x, o.first, o.count);
+                // The segment's side of the edge's ends is -un and den - un: when the segment passes
+                // through neither end the hit bounds the roof (edge_bounds_roof's first case), so
+                // the ring is walked only for hits through a vertex.
+                bool bounds = building && ((un != 0 && un != d) || edge_bounds_roof(S, sx, sy, dx, dy, ref.x, o.first, o.count));
                 xs[n++] = XRec{(double)tn / (double)d, ref.x, ref.y | (building ? X_BUILDING : 0u) | (bounds ? X_BOUNDS : 0u)};
             }
         }
@@ -427,6 +430,7 @@ struct Band {
     float radius;
     PlanePoint S, R;
     float slope_sr;  // (R.z - S.z) / (R.x - S.x): the line of sight, taken once
+    float chord_sr;  // |SR|
     Sag sag_sr;
     HullEntry *h;
     int n;
@@ -444,7 +448,8 @@ struct Band {
         S = s;
         R = r;
         float dx = r.x - s.x, dz = r.z - s.z;
-        radius = fmaxf(1000.0f, 8.0f * sqrtf(dx * dx + dz * dz));
+        chord_sr = sqrtf(dx * dx + dz * dz);
+        radius = fmaxf(1000.0f, 8.0f * chord_sr);
         slope_sr = dz / dx;
         if (STATE == QM_FAV) sag_sr = make_sag(radius, s, r);
         h = storage;
@@ -523,7 +528,6 @@ struct Band {
             return;
         }
         if (blocked) return;
-        float chord_sr = sqrtf((R.x - S.x) * (R.x - S.x) + (R.z - S.z) * (R.z - S.z));
         float delta = single_path_difference_f<STATE>(radius, S, c, R, chord_sr);
         if (!have_best || delta > best_value) {
             have_best = true;
