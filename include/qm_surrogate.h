@@ -23,9 +23,10 @@
  *   zeros (a present roof has x1 > x0 > 0, which is its mask).
  * Terrain feature set (scenes with a DEM; both conditions, one row per state): f0 .. f3 and
  *   f5 .. f7 as above (f6 the mean ground factor of the samples below), f4 the state (0
- *   homogeneous, 1 favourable); f8 .. f19 over 12 equal stretches of the path, the largest rise
- *   of the terrain above the straight source-receiver line among 3 DEM samples each (metres /
- *   10); f20 .. f31 over the same stretches, the largest rise of the obstacle tops the path
+ *   homogeneous, 1 favourable); f8 .. f19 over 12 stretches of the path (ends at 0, 2, 5, 10,
+ *   20, 35, 50, 65, 80, 90, 95, 98 and 100 % of L), the largest rise of the terrain above the
+ *   straight source-receiver line among 3 DEM samples each (metres / 10); f20 .. f31 over the
+ *   same stretches, the largest rise of the obstacle tops the path
  *   crosses above that line (-10 where it crosses none).
  * A flat path is eligible when all its obstacle tops pair into roofs and it crosses at most 8
  * roofs, a terrain path when its crossing list fits; both need their features inside the

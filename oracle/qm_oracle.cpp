@@ -1439,8 +1439,9 @@ uint32_t level_bin(double level_db, double level_min, double bin_db, uint32_t n_
 // =============================================================================================
 // C entry points (ctypes).
 // The terrain feature set of include/qm_surrogate.h for one path, two rows (homogeneous and
-// favourable): 36 DEM samples at lattice points rounded from t = (i + 0.5) / 36 along the path,
-// the largest rise of the ground above the straight source-receiver line in each of 12 stretches,
+// favourable): 3 DEM samples in each of 12 stretches (ends at 0, 2, 5, 10, 20, 35, 50, 65, 80, 90,
+// 95, 98, 100 % of the path) at lattice points rounded from t along the path, the largest rise
+// of the ground above the straight source-receiver line in each stretch,
 // and the largest rise of the obstacle tops crossed (walls standing on the ground at their
 // rounded crossing points) in each stretch.
 void terrain_sample(const Scene &s, const qm_source &src, const Receiver &r, const Worker &w, const PathBuffers &pb,
@@ -1456,11 +1457,12 @@ void terrain_sample(const Scene &s, const qm_source &src, const Receiver &r, con
         int64_t px = src.x + (int64_t)std::llrint(t * (double)dx), py = src.y + (int64_t)std::llrint(t * (double)dy);
         terrain_at_point(s, px, py, z, g);
     };
+    const float E[13] = {0.0f, 0.02f, 0.05f, 0.1f, 0.2f, 0.35f, 0.5f, 0.65f, 0.8f, 0.9f, 0.95f, 0.98f, 1.0f};
     double gsum = 0.0;
     for (int j = 0; j < 12; ++j) {
         double top = -INF;
         for (int q = 0; q < 3; ++q) {
-            double t = (j * 3 + q + 0.5) / 36.0, z, g;
+            double t = (double)E[j] + (q + 0.5) / 3.0 * (double)(E[j + 1] - E[j]), z, g;
             ground_at(t, z, g);
             top = std::max(top, z - (src_alt + rise * t * L));
             gsum += g;
@@ -1472,7 +1474,8 @@ void terrain_sample(const Scene &s, const qm_source &src, const Receiver &r, con
         if (std::binary_search(pb.containing.begin(), pb.containing.end(), c.footprint_id)) continue;
         double z, g;
         ground_at(c.t, z, g);
-        int j = std::min((int)(c.t * 12.0), 11);
+        int j = 0;
+        while (j < 11 && c.t >= (double)E[j + 1]) ++j;
         f[20 + j] = std::max(f[20 + j], (z + c.height_m - (src_alt + rise * c.t * L)) / 10.0);
     }
     const bool ok = true;

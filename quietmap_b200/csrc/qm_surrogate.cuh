@@ -125,6 +125,13 @@ __device__ __noinline__ bool surrogate_front(const SceneDev &S, const SourceDev 
 }
 
 constexpr int SURR_STRETCHES = 12, SURR_SAMPLES = 36;
+// Stretch ends along the path, finer near the source and the receiver (where obstacles and the
+// ground shape decide diffraction most).
+__device__ __forceinline__ float surr_stretch_end(int j) {
+    constexpr float E[SURR_STRETCHES + 1] = {0.0f, 0.02f, 0.05f, 0.1f, 0.2f, 0.35f, 0.5f,
+                                             0.65f, 0.8f, 0.9f, 0.95f, 0.98f, 1.0f};
+    return E[j];
+}
 
 // The terrain feature set (include/qm_surrogate.h) of one path, f4 left 0 for the caller to set;
 // eligible when its crossing list fits. Positions along the path are rounded to the lattice
@@ -153,9 +160,9 @@ __device__ __noinline__ bool surrogate_front_terrain(const SceneDev &S, const So
 #pragma unroll 1
     for (int j = 0; j < SURR_STRETCHES; ++j) {
         float top = -INFINITY;
+        const float e0 = surr_stretch_end(j), e1 = surr_stretch_end(j + 1);
         for (int q = 0; q < SURR_SAMPLES / SURR_STRETCHES; ++q) {
-            const int i = j * (SURR_SAMPLES / SURR_STRETCHES) + q;
-            const double t = (i + 0.5) / SURR_SAMPLES;
+            const double t = (double)e0 + (q + 0.5) / (SURR_SAMPLES / SURR_STRETCHES) * (double)(e1 - e0);
             const float2 zg = ground_at(t);
             top = fmaxf(top, zg.x - (src_alt + rise * (float)t * L));
             gsum += zg.y;
@@ -182,7 +189,8 @@ __device__ __noinline__ bool surrogate_front_terrain(const SceneDev &S, const So
         }
         const double t = xs[i].t;
         const float top = ground_at(t).x + o.height;
-        const int j = min((int)(t * SURR_STRETCHES), SURR_STRETCHES - 1);
+        int j = 0;
+        while (j < SURR_STRETCHES - 1 && t >= (double)surr_stretch_end(j + 1)) ++j;
         f[20 + j] = fmaxf(f[20 + j], (top - (src_alt + rise * (float)t * L)) * 0.1f);
     }
     const bool eligible = status == 0;
