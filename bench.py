@@ -79,6 +79,19 @@ def dist_env():
     return rank, world, local
 
 
+def combine_ranks(timing, paths, device):
+    """Replicas: every rank's times become the max over ranks (device times and wall time), the
+    path counts their sum. Returns the total paths; `timing` is updated in place."""
+    import torch
+    import torch.distributed as tdist
+    t = torch.tensor([timing["kernel_ms"], timing["wall_s"], timing["paint_ms"]], dtype=torch.float64, device=device)
+    tdist.all_reduce(t, op=tdist.ReduceOp.MAX)
+    timing["kernel_ms"], timing["wall_s"], timing["paint_ms"] = float(t[0]), float(t[1]), float(t[2])
+    tp = torch.tensor([float(paths)], dtype=torch.float64, device=device)
+    tdist.all_reduce(tp)
+    return int(tp[0])
+
+
 def workload(name, rank, slices, sources):
     """The scene and a list of steps (each a list of grids painted in that step)."""
     from quietmap_b200 import scenes
@@ -289,13 +302,7 @@ def main():
             step(args.warmup + i)
         torch.cuda.synchronize()
     if world > 1:
-        t = torch.tensor([timing["kernel_ms"], timing["wall_s"], timing["paint_ms"]], dtype=torch.float64,
-                         device="cuda")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        timing["kernel_ms"], timing["wall_s"], timing["paint_ms"] = float(t[0]), float(t[1]), float(t[2])
-        tp = torch.tensor([work["paths"]], dtype=torch.float64, device="cuda")
-        torch.distributed.all_reduce(tp)
-        total_paths = int(tp[0])
+        total_paths = combine_ranks(timing, work["paths"], "cuda")
     else:
         total_paths = work["paths"]
     if rank == 0:
