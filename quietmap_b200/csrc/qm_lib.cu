@@ -27,7 +27,6 @@
 #include "qm_mlp.h"
 #include "qm_surrogate.cuh"
 #include "qm_tiles.cuh"
-#include "qm_warp.cuh"
 
 #include <climits>
 
@@ -502,10 +501,6 @@ qm_status rerun_failed(qm_scene *scene, const GridArgs &A, const uint2 *d_retry,
     return QM_OK;
 }
 
-#ifndef QM_WARP_PATHS_FOR_TERRAIN
-#define QM_WARP_PATHS_FOR_TERRAIN 0
-#endif
-bool use_warp_paths(const qm_scene *s) { return QM_WARP_PATHS_FOR_TERRAIN && s->dem_nx != 0; }
 
 }  // namespace
 
@@ -549,10 +544,7 @@ qm_status qm_paint_grid(qm_scene *scene, const qm_grid_desc *grid, float *cell_b
     A.tile_h = 8;
     A.want_fav = scene->any_favourable;
     for (int p = 0; p < 3; ++p) A.lden_w[p] = (float)LDEN_W[p];
-    // Terrain scenes (long rays over a DEM) run one warp per path; flat scenes one thread per path.
-    const bool warp_paths = use_warp_paths(scene);
-    const int tiles = warp_paths ? (cells + 3) / 4
-                                 : ((g.nx + A.tile_w - 1) / A.tile_w) * ((g.ny + A.tile_h - 1) / A.tile_h);
+    const int tiles = ((g.nx + A.tile_w - 1) / A.tile_w) * ((g.ny + A.tile_h - 1) / A.tile_h);
     const uint32_t n_src = se - sb;
     uint32_t want_ctas = (uint32_t)ctx->sm_count * 16;
     uint32_t n_chunks = std::max<uint32_t>(1, (want_ctas + tiles - 1) / tiles);
@@ -592,11 +584,7 @@ qm_status qm_paint_grid(qm_scene *scene, const qm_grid_desc *grid, float *cell_b
     QM_CUDA(cudaEventRecord(ev.e0, stream));
     if (n_src > 0) {
         dim3 grid_dim(tiles, A.n_chunks);
-        if (warp_paths) {
-            const int smem = 4 * (int)sizeof(WarpShared);
-            QM_CUDA(cudaFuncSetAttribute(paint_grid_warp_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-            paint_grid_warp_kernel<<<grid_dim, 128, smem, stream>>>(scene->dev, A);
-        } else if (terrain_caps(scene)) {
+        if (terrain_caps(scene)) {
             paint_grid_kernel<CapsTerrain><<<grid_dim, 128, 0, stream>>>(scene->dev, A);
         } else {
             paint_grid_kernel<CapsFlat><<<grid_dim, 128, 0, stream>>>(scene->dev, A);
