@@ -158,12 +158,17 @@ def _check_pairs(ctx, scene, rng):
     ground = np.array([ora.profile(p, p)[2][0] for p in rxy_steps])
     ref_sums, ref_bands, ref_points = ora.evaluate_pairs(rxy_steps, ground + 4.0, own, point, sop, rop, weight,
                                                          n_receivers)
-    err = np.abs(_levels_db(sums.astype(np.float64)) - _levels_db(ref_sums))
-    err = err[np.isfinite(err)]
+    got, ref = _levels_db(sums.astype(np.float64)), _levels_db(ref_sums)
+    # Silent sums (no energy in a state or period) must be silent on both sides.
+    assert np.array_equal(np.isfinite(got), np.isfinite(ref))
+    heard = np.isfinite(ref)
+    err = np.abs(got[heard] - ref[heard])
     assert np.percentile(err, 99) < TOL_DB, np.percentile(err, [50, 99, 100])
     assert np.median(err) < 0.005
-    pe = np.abs(_levels_db(points.astype(np.float64)) - _levels_db(ref_points))
-    pe = pe[np.isfinite(pe)]
+    got_p, ref_p = _levels_db(points.astype(np.float64)), _levels_db(ref_points)
+    assert np.array_equal(np.isfinite(got_p), np.isfinite(ref_p))
+    heard = np.isfinite(ref_p)
+    pe = np.abs(got_p[heard] - ref_p[heard])
     assert np.percentile(pe, 99) < TOL_DB
 
 
