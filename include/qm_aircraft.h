@@ -58,14 +58,22 @@ typedef struct {
     double duration_s;  /* averaging time of the levels (86,400 s: a day's Leq) */
 } qm_flight_grid_desc;
 
+/* Work and device time of one qm_flight_grid call. */
+typedef struct {
+    uint64_t pairs;          /* cells x segments */
+    uint64_t pairs_in_reach; /* of which evaluated (the others were culled with their flight) */
+    double kernel_ms;        /* device time of the flight kernel */
+    double loudness_ms;      /* device time of the Zwicker kernel (0 without sone) */
+} qm_flight_stats;
+
 /* Per cell: the total A-weighted sound exposure level (lae_db), the day-average third-octave
  * levels (thirds_db[cells][28]) of the summed flights and their Zwicker loudness (sone). Each
  * output is nullable. Segments must be grouped by flight (flight ids non-decreasing); 1 to 48
- * aircraft types (their NPD rows are held in shared memory). */
+ * aircraft types (their NPD rows are held in shared memory). stats is nullable. */
 qm_status qm_flight_grid(qm_ctx *ctx, const qm_aircraft_type *types, uint32_t n_types,
                          const qm_flight_segment *segments, size_t n_segments,
                          const qm_flight_grid_desc *grid, float *lae_db, float *thirds_db,
-                         float *sone);
+                         float *sone, qm_flight_stats *stats);
 
 #ifdef __cplusplus
 }

@@ -25,7 +25,7 @@
 extern "C" {
 #endif
 
-#define QM_ABI_VERSION 2
+#define QM_ABI_VERSION 3
 
 #define QM_BANDS 8      /* octave bands 63 Hz .. 8 kHz (physics/src/bands.rs:4) */
 #define QM_PERIODS 3    /* day, evening, night (physics/src/bands.rs:14) */

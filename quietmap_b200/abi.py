@@ -8,7 +8,7 @@ import ctypes as C
 
 import numpy as np
 
-ABI_VERSION = 2
+ABI_VERSION = 3
 BANDS = 8
 PERIODS = 3
 SECTORS = 16
@@ -136,6 +136,11 @@ class FlightGridDesc(C.Structure):
         ("reach_m", C.c_double),
         ("duration_s", C.c_double),
     ]
+
+
+class FlightStats(C.Structure):
+    _fields_ = [("pairs", C.c_uint64), ("pairs_in_reach", C.c_uint64), ("kernel_ms", C.c_double),
+                ("loudness_ms", C.c_double)]
 
 
 def flight_grid_desc(grid):

@@ -1124,7 +1124,8 @@ double tail_alpha_of(const float *sel) {
 
 extern "C" qm_status qm_flight_grid(qm_ctx *ctx, const qm_aircraft_type *types, uint32_t n_types,
                                     const qm_flight_segment *segments, size_t n_segments,
-                                    const qm_flight_grid_desc *grid, float *lae_db, float *thirds_db, float *sone) {
+                                    const qm_flight_grid_desc *grid, float *lae_db, float *thirds_db, float *sone,
+                                    qm_flight_stats *stats) {
     if (!ctx || !grid) return fail(QM_ERR_ARGUMENT, "qm_flight_grid: null ctx or grid");
     if (n_types == 0 || n_types > 48 || !types) return fail(QM_ERR_ARGUMENT, "qm_flight_grid: 1 to 48 aircraft types");
     if (n_segments && !segments) return fail(QM_ERR_ARGUMENT, "qm_flight_grid: segments is null");
@@ -1186,7 +1187,7 @@ extern "C" qm_status qm_flight_grid(qm_ctx *ctx, const qm_aircraft_type *types, 
     QM_CUDA(cudaSetDevice(ctx->device));
     cudaStream_t stream = ctx->stream;
     const size_t cells = (size_t)g.nx * g.ny;
-    Scratch d_segs, d_boxes, d_rows, d_types, d_lae, d_thirds, d_sone, d_error;
+    Scratch d_segs, d_boxes, d_rows, d_types, d_lae, d_thirds, d_sone, d_error, d_pairs;
     QM_CUDA(cudaMalloc(&d_segs.p, std::max<size_t>(n_segments, 1) * sizeof(qm_flight_segment)));
     QM_CUDA(cudaMalloc(&d_boxes.p, boxes.size() * sizeof(float4)));
     QM_CUDA(cudaMalloc(&d_rows.p, rows.size() * sizeof(AcRow)));
@@ -1194,6 +1195,8 @@ extern "C" qm_status qm_flight_grid(qm_ctx *ctx, const qm_aircraft_type *types, 
     QM_CUDA(cudaMalloc(&d_lae.p, cells * sizeof(float)));
     QM_CUDA(cudaMalloc(&d_thirds.p, cells * 28 * sizeof(float)));
     QM_CUDA(cudaMalloc(&d_error.p, sizeof(unsigned)));
+    QM_CUDA(cudaMalloc(&d_pairs.p, sizeof(unsigned long long)));
+    QM_CUDA(cudaMemsetAsync(d_pairs.p, 0, sizeof(unsigned long long), stream));
     if (sone) QM_CUDA(cudaMalloc(&d_sone.p, cells * sizeof(float)));
     if (n_segments)
         QM_CUDA(cudaMemcpyAsync(d_segs.p, segments, n_segments * sizeof(qm_flight_segment), cudaMemcpyHostToDevice, stream));
@@ -1219,18 +1222,27 @@ extern "C" qm_status qm_flight_grid(qm_ctx *ctx, const qm_aircraft_type *types, 
     A.lae = static_cast<float *>(d_lae.p);
     A.thirds = static_cast<float *>(d_thirds.p);
     A.error = static_cast<unsigned *>(d_error.p);
+    A.pairs = static_cast<unsigned long long *>(d_pairs.p);
     const size_t smem = 2 * AC_TILE * sizeof(qm_flight_segment) + 16 + (size_t)n_types * 20 * sizeof(AcRow) +
-                        n_types * sizeof(AcType) + (size_t)n_types * 2 * AC_THREADS * sizeof(float);
+                        n_types * sizeof(AcType) + (size_t)n_types * 2 * AC_THREADS * sizeof(float) +
+                        AC_TILE * sizeof(SegPre);
     if (smem > 227 * 1024)
         return fail(QM_ERR_UNSUPPORTED, "qm_flight_grid: " + std::to_string(n_types) + " types exceed shared memory");
     QM_CUDA(cudaFuncSetAttribute(flight_grid_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     const unsigned blocks = (unsigned)(((g.nx + 15) / 16) * ((g.ny + 15) / 16));
+    Events ev;
+    QM_CUDA(ev.create());
+    QM_CUDA(cudaEventRecord(ev.e0, stream));
     flight_grid_kernel<<<blocks, AC_THREADS, smem, stream>>>(A);
     QM_CUDA(cudaGetLastError());
+    QM_CUDA(cudaEventRecord(ev.e1, stream));
     if (sone) {
         launch_zwicker(A.thirds, cells, static_cast<float *>(d_sone.p), stream);
         QM_CUDA(cudaGetLastError());
     }
+    QM_CUDA(cudaEventRecord(ev.e2, stream));
+    unsigned long long pairs_in_reach = 0;
+    QM_CUDA(cudaMemcpyAsync(&pairs_in_reach, d_pairs.p, sizeof(pairs_in_reach), cudaMemcpyDeviceToHost, stream));
     unsigned error = 0;
     QM_CUDA(cudaMemcpyAsync(&error, d_error.p, sizeof(unsigned), cudaMemcpyDeviceToHost, stream));
     if (lae_db) QM_CUDA(cudaMemcpyAsync(lae_db, d_lae.p, cells * sizeof(float), cudaMemcpyDeviceToHost, stream));
@@ -1238,6 +1250,15 @@ extern "C" qm_status qm_flight_grid(qm_ctx *ctx, const qm_aircraft_type *types, 
     if (sone) QM_CUDA(cudaMemcpyAsync(sone, d_sone.p, cells * sizeof(float), cudaMemcpyDeviceToHost, stream));
     QM_CUDA(cudaStreamSynchronize(stream));
     if (error) return fail(QM_ERR_TIMEOUT, "qm_flight_grid: a segment tile's copy did not arrive in time");
+    if (stats) {
+        float k_ms = 0.f, z_ms = 0.f;
+        QM_CUDA(cudaEventElapsedTime(&k_ms, ev.e0, ev.e1));
+        QM_CUDA(cudaEventElapsedTime(&z_ms, ev.e1, ev.e2));
+        stats->pairs = (uint64_t)cells * n_segments;
+        stats->pairs_in_reach = pairs_in_reach;
+        stats->kernel_ms = k_ms;
+        stats->loudness_ms = sone ? z_ms : 0.0;
+    }
     return QM_OK;
 }
 

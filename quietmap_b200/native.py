@@ -60,7 +60,7 @@ def lib():
         L.qm_list_crossings.argtypes = [C.c_void_p, _I32, _I32, C.c_size_t, C.c_uint32, _U32, _U32, _D, _U32, _U32]
         L.qm_list_crossings.restype = C.c_int
         L.qm_flight_grid.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_size_t,
-                                     C.POINTER(abi.FlightGridDesc), _F, _F, _F]
+                                     C.POINTER(abi.FlightGridDesc), _F, _F, _F, C.POINTER(abi.FlightStats)]
         L.qm_flight_grid.restype = C.c_int
         P = C.POINTER(C.c_void_p)
         L.qm_surrogate_create.argtypes = [C.c_void_p, _F, P]
@@ -135,8 +135,9 @@ class Context:
                self.handle)
         return out
 
-    def flight_grid(self, flights, grid=None, sone=True):
-        """Doc 29 flights over a receiver grid: (LAE [cells], thirds [cells][28], sone [cells])."""
+    def flight_grid(self, flights, grid=None, sone=True, stats=False):
+        """Doc 29 flights over a receiver grid: (LAE [cells], thirds [cells][28], sone [cells]),
+        and a dict of work and device times when `stats`."""
         g = abi.flight_grid_desc(grid or flights.grid)
         cells = g.nx * g.ny
         types = np.ascontiguousarray(flights.types, dtype=abi.AIRCRAFT_TYPE_DTYPE)
@@ -144,9 +145,13 @@ class Context:
         lae = np.zeros(cells, np.float32)
         thirds = np.zeros((cells, abi.THIRDS), np.float32)
         out_sone = np.zeros(cells, np.float32) if sone else None
+        st = abi.FlightStats()
         _check(lib().qm_flight_grid(self.handle, types.ctypes.data, len(types), segs.ctypes.data, len(segs),
                                     C.byref(g), abi.ptr(lae, C.c_float), abi.ptr(thirds, C.c_float),
-                                    abi.ptr(out_sone, C.c_float) if sone else None), self.handle)
+                                    abi.ptr(out_sone, C.c_float) if sone else None, C.byref(st)), self.handle)
+        if stats:
+            return lae, thirds, out_sone, dict(pairs=st.pairs, pairs_in_reach=st.pairs_in_reach,
+                                               kernel_ms=st.kernel_ms, loudness_ms=st.loudness_ms)
         return lae, thirds, out_sone
 
     def level_histogram(self, levels_db, level_min_db=-30.0, bin_db=0.1, n_bins=1800):
