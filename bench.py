@@ -65,6 +65,8 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="terrain", choices=["terrain", "road", "flights", "surrogate", "surrogate_terrain", "tiles"])
     ap.add_argument("--tiles", type=int, default=32, help="tiles workload: tiles per batch, drawn from the 4096")
+    ap.add_argument("--flights", type=int, default=2000, help="flights workload: flights (a small case for profiling)")
+    ap.add_argument("--cells-side", type=int, default=1024, help="flights workload: receivers per side")
     ap.add_argument("--slices", type=int, default=8, help="terrain: source-list slices (a step paints one)")
     ap.add_argument("--sources", type=int, default=0,
                     help="paint only the first N sources (a small case for profiling; 0: all)")
@@ -393,7 +395,7 @@ def flights(args, rank, world, local):
     """Doc 29 flights (1024^2 cells at 100 m x 2000 flights x 50 segments) with loudness."""
     import torch
     from quietmap_b200 import native, scenes
-    f = scenes.flights_square(seed=3 + rank)
+    f = scenes.flights_square(seed=3 + rank, n_flights=args.flights, receivers=args.cells_side)
     ctx = native.Context(local if world > 1 else 0)
     cells = f.grid["nx"] * f.grid["ny"]
     for _ in range(args.warmup):
@@ -421,7 +423,8 @@ def flights(args, rank, world, local):
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": (k_ms + z_ms) / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded flights and NPD tables)",
-            "config": {"workload": "1024^2 cells at 100 m x 2000 flights x 50 segments, 10 types, reach 25 km",
+            "config": {"workload": f"{args.cells_side}^2 cells at 100 m x {args.flights} flights x 50 segments, 10 types, "
+                                   "reach 25 km",
                        "pairs_in_reach_per_step": in_reach // args.steps},
             "e2e": {"value": cells * args.steps / wall, "unit": "cells/s",
                     "h2d_bytes_per_step": len(f.segments) * 48 + len(f.types) * f.types.itemsize,
