@@ -546,6 +546,9 @@ qm_status qm_paint_grid(qm_scene *scene, const qm_grid_desc *grid, float *cell_b
     for (int p = 0; p < 3; ++p) A.lden_w[p] = (float)LDEN_W[p];
     const int tiles = ((g.nx + A.tile_w - 1) / A.tile_w) * ((g.ny + A.tile_h - 1) / A.tile_h);
     const uint32_t n_src = se - sb;
+    // Source chunks: about 16 CTAs per SM, several waves so that uneven chunk times even out. On
+    // a 1 km terrain tile (80 k sources) 9 per SM took 834 ms, 16 took 745, 24 took 747 and 48
+    // took 740; the road tile is flat from 16 up.
     uint32_t want_ctas = (uint32_t)ctx->sm_count * 16;
     uint32_t n_chunks = std::max<uint32_t>(1, (want_ctas + tiles - 1) / tiles);
     n_chunks = std::min<uint32_t>(n_chunks, std::max<uint32_t>(1, n_src / 32));
