@@ -76,15 +76,16 @@ __device__ __forceinline__ void path_energies(const SceneDev &S, const PathResul
     lden = lsum;
 }
 
-// Thread = one receiver of a tile; CTA = (receiver tile, source chunk). Each thread walks its chunk
-// of sources and keeps its cell's band energies in compensated registers; one store per cell.
-template <class Caps>
 #ifndef QM_PAINT_MIN_BLOCKS
 // CTAs of 128 resident per SM: 3 caps registers at 170 a thread. Measured on a terrain tile
 // (16 x 8 receivers x 80,000 sources): 2 CTAs 847 ms, 3 CTAs 741 ms, 4 CTAs 786 ms, 5 CTAs 814 ms,
 // 6 CTAs 880 ms; the road square is within 2 % for 3 and 4.
 #define QM_PAINT_MIN_BLOCKS 3
 #endif
+
+// Thread = one receiver of a tile; CTA = (receiver tile, source chunk). Each thread walks its chunk
+// of sources and keeps its cell's band energies in compensated registers; one store per cell.
+template <class Caps>
 __global__ void __launch_bounds__(128, QM_PAINT_MIN_BLOCKS) paint_grid_kernel(SceneDev S, GridArgs A) {
     __shared__ unsigned long long s_counts[6];
     if (threadIdx.x < 6) s_counts[threadIdx.x] = 0;
