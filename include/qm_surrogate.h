@@ -90,13 +90,15 @@ typedef struct {
     float learning_rate;     /* Adam, cosine decay to 5 % over the run */
     uint32_t seed;           /* shuffling */
     uint32_t max_samples;    /* 0: every eligible path of the grids */
-    uint32_t pad_;
+    float exact_within_m;    /* paths shorter than this (horizontal metres) are left to the exact
+                                path: not trained on, and below the eligible range of f0, so the
+                                painter evaluates them exactly; 0 for none */
 } qm_train_config;
 
 /* Trains the network in place on the device: samples from every path of each grid (exact
- * labels, eligible paths only), the normalisation and eligible ranges set from them, then Adam
- * over shuffled batches. loss_history[epochs] (nullable) gets each epoch's mean loss;
- * n_samples (nullable) the number of samples used. */
+ * labels, eligible paths at least exact_within_m long), the normalisation and eligible ranges
+ * set from them, then Adam over shuffled batches. loss_history[epochs] (nullable) gets each
+ * epoch's mean loss; n_samples (nullable) the number of samples used. */
 qm_status qm_surrogate_train(qm_surrogate *net, qm_scene *scene, const qm_grid_desc *grids,
                              size_t n_grids, const qm_train_config *config, double *loss_history,
                              uint64_t *n_samples);

@@ -221,7 +221,7 @@ class TrainConfig(C.Structure):
         ("learning_rate", C.c_float),
         ("seed", C.c_uint32),
         ("max_samples", C.c_uint32),
-        ("pad_", C.c_uint32),
+        ("exact_within_m", C.c_float),
     ]
 
 

@@ -1390,6 +1390,12 @@ void chunk_range(const qm_ctx *ctx, GridArgs &A, int tiles, uint32_t b0, uint32_
     A.n_chunks = n_src == 0 ? 1 : (n_src + A.chunk - 1) / A.chunk;
 }
 
+// Rows whose first feature (L / 1000) is below `f0_min` lose their eligible flag.
+__global__ void floor_rows_kernel(const float *features, uint8_t *eligible, size_t rows, float f0_min) {
+    size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+    if (i < rows && features[i * MLP_IN] < f0_min) eligible[i] = 0;
+}
+
 __global__ void gather_rows_kernel(const float *src, const uint32_t *index, size_t n, int w, float *dst) {
     size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
     if (i >= n * w) return;
@@ -1578,6 +1584,8 @@ qm_status qm_surrogate_train(qm_surrogate *net, qm_scene *scene, const qm_grid_d
     const qm_train_config &c = *config;
     if (c.epochs == 0 || c.batch < 256 || c.batch % 128 != 0 || c.batch > (1u << 20) || !(c.learning_rate > 0.0f))
         return fail(QM_ERR_ARGUMENT, "qm_surrogate_train: epochs >= 1, batch a multiple of 128 in [256, 2^20], learning_rate > 0");
+    if (!(c.exact_within_m >= 0.0f) || !std::isfinite(c.exact_within_m))
+        return fail(QM_ERR_ARGUMENT, "qm_surrogate_train: exact_within_m must be finite and >= 0");
     for (size_t k = 0; k < n_grids; ++k) {
         qm_status st = check_grid(scene, grids[k], "qm_surrogate_train");
         if (st != QM_OK) return st;
@@ -1603,6 +1611,11 @@ qm_status qm_surrogate_train(qm_surrogate *net, qm_scene *scene, const qm_grid_d
         qm_status st = grid_samples(scene, grids[k], f, l, e, rows, stream);
         if (st != QM_OK) return st;
         if (rows == 0) continue;
+        if (c.exact_within_m > 0.0f) {
+            floor_rows_kernel<<<(unsigned)((rows + 255) / 256), 256, 0, stream>>>(
+                static_cast<const float *>(f.p), static_cast<uint8_t *>(e.p), rows, c.exact_within_m * 1e-3f);
+            QM_CUDA(cudaGetLastError());
+        }
         std::vector<uint8_t> flags(rows);
         QM_CUDA(cudaMemcpy(flags.data(), e.p, rows, cudaMemcpyDeviceToHost));
         std::vector<uint32_t> keep;

@@ -344,10 +344,12 @@ class Surrogate:
                                             abi.ptr(g, C.c_float), C.byref(loss)), self.ctx.handle)
         return g, loss.value
 
-    def train(self, device_scene, grids, epochs=4, batch=16384, learning_rate=2e-3, seed=1, max_samples=0):
-        """Trains on every eligible path of `grids`; returns (loss per epoch, samples used)."""
+    def train(self, device_scene, grids, epochs=4, batch=16384, learning_rate=2e-3, seed=1, max_samples=0,
+              exact_within_m=0.0):
+        """Trains on every eligible path of `grids` at least `exact_within_m` long (shorter paths
+        stay on the exact path when painting); returns (loss per epoch, samples used)."""
         descs = (abi.GridDesc * len(grids))(*[abi.grid_desc(g) for g in grids])
-        cfg = abi.TrainConfig(epochs, batch, learning_rate, seed, max_samples, 0)
+        cfg = abi.TrainConfig(epochs, batch, learning_rate, seed, max_samples, exact_within_m)
         hist = np.zeros(epochs, np.float64)
         n = C.c_uint64()
         _check(lib().qm_surrogate_train(self.handle, device_scene.handle, descs, len(grids), C.byref(cfg),

@@ -40,11 +40,13 @@ def test_struct_layouts_match_the_header():
 #include <stdio.h>
 #include <stddef.h>
 #include "qm_batch.h"
+#include "qm_surrogate.h"
 int main(void) {
   printf("%zu %zu %zu %zu %zu\n", sizeof(qm_outline), sizeof(qm_source), sizeof(qm_scene_desc),
          sizeof(qm_grid_desc), sizeof(qm_paint_stats));
   printf("%zu %zu %zu %zu\n", offsetof(qm_source, energy), offsetof(qm_scene_desc, favourable),
          offsetof(qm_scene_desc, alpha_db_per_km), offsetof(qm_grid_desc, n_bins));
+  printf("%zu %zu\n", sizeof(qm_train_config), offsetof(qm_train_config, exact_within_m));
   return 0;
 }
 '''
@@ -56,7 +58,8 @@ int main(void) {
         subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), path, "-o", exe], check=True)
         out = subprocess.run([exe], check=True, capture_output=True, text=True).stdout.split()
     sizes = list(map(int, out[:5]))
-    offsets = list(map(int, out[5:]))
+    offsets = list(map(int, out[5:9]))
+    assert list(map(int, out[9:])) == [C.sizeof(abi.TrainConfig), abi.TrainConfig.exact_within_m.offset]
     assert sizes == [C.sizeof(abi.Outline), C.sizeof(abi.Source), C.sizeof(abi.SceneDesc), C.sizeof(abi.GridDesc),
                      C.sizeof(abi.PaintStats)]
     assert offsets == [abi.Source.energy.offset, abi.SceneDesc.favourable.offset,

@@ -206,3 +206,34 @@ def test_terrain_surrogate_trains_and_paints(ctx, terrain):
     flat = native.Surrogate(ctx, seed=3)
     with pytest.raises(native.QmError):
         dev.paint_grid_surrogate(tile, flat)
+
+
+def test_paths_inside_the_exact_radius_stay_exact(ctx, terrain):
+    """A network trained with exact_within_m leaves every shorter path to the exact path: its
+    eligible range starts at that length, and on a tile the network takes no path that short."""
+    scene, full = terrain
+    dev = ctx.scene(scene)
+    net = native.Surrogate(ctx, seed=4)
+    radius = 150.0
+    grid = scenes.Grid(origin=(full.origin[0] + 17, full.origin[1] + 23), spacing=full.spacing * 32, nx=16, ny=16,
+                       source_begin=0, source_end=20000)
+    net.train(dev, [grid], epochs=2, batch=8192, learning_rate=2e-3, seed=6, max_samples=1_000_000,
+              exact_within_m=radius)
+    lo0 = net.params()[abi.SURR_WEIGHTS + 32 + 32 + 8 + 8]
+    assert lo0 >= radius * 1e-3, lo0
+    tile = scenes.Grid(origin=(full.origin[0] + 100 * full.spacing, full.origin[1] + 60 * full.spacing),
+                       spacing=full.spacing, nx=16, ny=8)
+    _, edba, _, _, est = dev.paint_grid(tile)
+    _, sdba, _, _, sst = dev.paint_grid_surrogate(tile, net)
+    # Paths shorter than the radius, counted on the host (a small margin for float rounding).
+    rx = (tile.origin[0] + tile.spacing * np.arange(tile.nx))[None, :].repeat(tile.ny, 0).ravel()
+    ry = (tile.origin[1] + tile.spacing * np.arange(tile.ny))[:, None].repeat(tile.nx, 1).ravel()
+    sx = scene.sources["x"].astype(np.float64)
+    sy = scene.sources["y"].astype(np.float64)
+    short = 0
+    for x, y in zip(rx, ry):
+        short += int(np.count_nonzero(np.hypot((x - sx) * scene.step_m, (y - sy) * scene.step_m) < radius - 0.01))
+    assert short > 0
+    assert sst["surrogate_paths"] <= sst["paths"] - short, (sst["surrogate_paths"], sst["paths"], short)
+    d = np.abs(sdba - edba)
+    assert np.percentile(d, 99) < 0.5, np.percentile(d, [50, 99, 100])
