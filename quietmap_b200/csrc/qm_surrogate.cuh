@@ -211,7 +211,8 @@ __global__ void __launch_bounds__(128, QM_PAINT_MIN_BLOCKS) surrogate_samples_te
     const GridArgs &A = P.g;
     const int tiles_x = (A.nx + A.tile_w - 1) / A.tile_w;
     const int tx = blockIdx.x % tiles_x, ty = blockIdx.x / tiles_x;
-    const int ix = tx * A.tile_w + (threadIdx.x % A.tile_w), iy = ty * A.tile_h + (threadIdx.x / A.tile_w);
+    const int2 slot = tile_slot(A.tile_w, A.tile_h);
+    const int ix = tx * A.tile_w + slot.x, iy = ty * A.tile_h + slot.y;
     if (ix >= A.nx || iy >= A.ny) return;
     const int cell = iy * A.nx + ix;
     const int rx = A.origin_x + ix * A.spacing, ry = A.origin_y + iy * A.spacing;
@@ -248,7 +249,8 @@ __global__ void __launch_bounds__(128, QM_PAINT_MIN_BLOCKS) surrogate_samples_ke
     const GridArgs &A = P.g;
     const int tiles_x = (A.nx + A.tile_w - 1) / A.tile_w;
     const int tx = blockIdx.x % tiles_x, ty = blockIdx.x / tiles_x;
-    const int ix = tx * A.tile_w + (threadIdx.x % A.tile_w), iy = ty * A.tile_h + (threadIdx.x / A.tile_w);
+    const int2 slot = tile_slot(A.tile_w, A.tile_h);
+    const int ix = tx * A.tile_w + slot.x, iy = ty * A.tile_h + slot.y;
     if (ix >= A.nx || iy >= A.ny) return;
     const int cell = iy * A.nx + ix;
     const int rx = A.origin_x + ix * A.spacing, ry = A.origin_y + iy * A.spacing;
@@ -294,7 +296,8 @@ __global__ void __launch_bounds__(128, QM_PAINT_MIN_BLOCKS) surrogate_front_kern
     const GridArgs &A = P.g;
     const int tiles_x = (A.nx + A.tile_w - 1) / A.tile_w;
     const int tx = blockIdx.x % tiles_x, ty = blockIdx.x / tiles_x;
-    const int ix = tx * A.tile_w + (threadIdx.x % A.tile_w), iy = ty * A.tile_h + (threadIdx.x / A.tile_w);
+    const int2 slot = tile_slot(A.tile_w, A.tile_h);
+    const int ix = tx * A.tile_w + slot.x, iy = ty * A.tile_h + slot.y;
     const bool active = ix < A.nx && iy < A.ny;
     const int cell = iy * A.nx + ix;
     unsigned long long paths = 0, crossings = 0, tested = 0, failed_paths = 0, vertices = 0, candidates = 0;
@@ -415,7 +418,8 @@ __global__ void __launch_bounds__(128, QM_PAINT_MIN_BLOCKS) surrogate_front_terr
     const GridArgs &A = P.g;
     const int tiles_x = (A.nx + A.tile_w - 1) / A.tile_w;
     const int tx = blockIdx.x % tiles_x, ty = blockIdx.x / tiles_x;
-    const int ix = tx * A.tile_w + (threadIdx.x % A.tile_w), iy = ty * A.tile_h + (threadIdx.x / A.tile_w);
+    const int2 slot = tile_slot(A.tile_w, A.tile_h);
+    const int ix = tx * A.tile_w + slot.x, iy = ty * A.tile_h + slot.y;
     const bool active = ix < A.nx && iy < A.ny;
     const int cell = iy * A.nx + ix;
     unsigned long long paths = 0, crossings = 0, tested = 0, failed_paths = 0, vertices = 0, candidates = 0;
