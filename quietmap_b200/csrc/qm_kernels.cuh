@@ -76,17 +76,23 @@ __device__ __forceinline__ void path_energies(const SceneDev &S, const PathResul
     lden = lsum;
 }
 
-// A thread's receiver inside its CTA's tile_w x tile_h tile. With the 16 x 8 tile of 128 threads
-// each warp takes an 8 x 4 block of receivers rather than two rows of 16: its lanes' rays to a
-// source lie closer together, so their crossing walks and profiles diverge less (a terrain tile,
-// 16 x 8 receivers x 80,000 sources: 699 ms against 742 ms, cell results bit for bit the same;
-// 4 x 8 blocks measured the same as 8 x 4). Other tile shapes are row-major.
-__device__ __forceinline__ int2 tile_slot(int tile_w, int tile_h) {
-    if (tile_w == 16 && tile_h == 8 && blockDim.x == 128) {
-        const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
-        return make_int2((w & 1) * 8 + (l & 7), (w >> 1) * 4 + (l >> 3));
+// Receiver r (0 <= r < block_w * block_h) of a block of receivers: each 32 consecutive r (a warp)
+// cover an 8 x 4 patch when the block's sides are multiples of 8 and 4, else the block is
+// row-major. A warp's rays to a source then lie closer together than along a row of 16 or 32, so
+// their crossing walks and profiles diverge less (a terrain tile, 16 x 8 receivers x 80,000
+// sources: 699 ms against 742 ms with two rows of 16 a warp, cell results bit for bit the same;
+// 4 x 8 patches measured the same as 8 x 4).
+__device__ __forceinline__ int2 block_slot(uint32_t r, uint32_t block_w, uint32_t block_h) {
+    if (block_w % 8 == 0 && block_h % 4 == 0) {
+        const uint32_t g = r >> 5, l = r & 31, groups_x = block_w / 8;
+        return make_int2((int)((g % groups_x) * 8 + (l & 7)), (int)((g / groups_x) * 4 + (l >> 3)));
     }
-    return make_int2((int)threadIdx.x % tile_w, (int)threadIdx.x / tile_w);
+    return make_int2((int)(r % block_w), (int)(r / block_w));
+}
+
+// A thread's receiver inside its CTA's tile (one thread per receiver).
+__device__ __forceinline__ int2 tile_slot(int tile_w, int tile_h) {
+    return block_slot(threadIdx.x, (uint32_t)tile_w, (uint32_t)tile_h);
 }
 
 #ifndef QM_PAINT_MIN_BLOCKS

@@ -59,7 +59,8 @@ __global__ void __launch_bounds__(THREADS, 512 / THREADS) batch_paint_kernel(Sce
         const uint32_t s0 = T.source_begin + w.chunk * T.chunk, s1 = min(s0 + T.chunk, T.source_end);
         const uint32_t cells_t = (uint32_t)T.nx * T.ny;
         for (uint32_t r = threadIdx.x; r < per; r += THREADS) {
-            const uint32_t ix = bx * T.block_w + r % T.block_w, iy = by * T.block_h + r / T.block_w;
+            const int2 slot = block_slot(r, T.block_w, T.block_h);
+            const uint32_t ix = bx * T.block_w + (uint32_t)slot.x, iy = by * T.block_h + (uint32_t)slot.y;
             if (ix >= (uint32_t)T.nx || iy >= (uint32_t)T.ny) continue;
             const uint32_t cell = iy * T.nx + ix;
             const unsigned long long gcell = T.cell_offset + cell;
