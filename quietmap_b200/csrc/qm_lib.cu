@@ -48,6 +48,9 @@ struct qm_ctx {
 struct DeviceBuffer {
     void *ptr = nullptr;
     size_t bytes = 0;
+    DeviceBuffer() = default;
+    DeviceBuffer(const DeviceBuffer &) = delete;
+    DeviceBuffer &operator=(const DeviceBuffer &) = delete;
     ~DeviceBuffer() {
         if (ptr) cudaFree(ptr);
     }
@@ -100,15 +103,33 @@ qm_status upload(qm_scene *s, const T *host, size_t count, const T **out) {
 }
 
 // A device allocation freed when the holder leaves scope.
+// A device buffer freed when its owner leaves scope. Move-only: a copy would free the buffer
+// twice (and leave the other copy pointing at freed memory), e.g. when a vector of structs that
+// hold one grows.
 struct Scratch {
     void *p = nullptr;
+    Scratch() = default;
+    Scratch(const Scratch &) = delete;
+    Scratch &operator=(const Scratch &) = delete;
+    Scratch(Scratch &&o) noexcept : p(o.p) { o.p = nullptr; }
+    Scratch &operator=(Scratch &&o) noexcept {
+        if (this != &o) {
+            if (p) cudaFree(p);
+            p = o.p;
+            o.p = nullptr;
+        }
+        return *this;
+    }
     ~Scratch() {
         if (p) cudaFree(p);
     }
 };
 
-// A pair of timing events destroyed when the holder leaves scope.
+// Timing events destroyed when the holder leaves scope (not copyable, for the same reason).
 struct Events {
+    Events() = default;
+    Events(const Events &) = delete;
+    Events &operator=(const Events &) = delete;
     cudaEvent_t e0 = nullptr, e1 = nullptr, e2 = nullptr;
     cudaError_t create() {
         cudaError_t e = cudaEventCreate(&e0);

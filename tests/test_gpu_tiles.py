@@ -78,3 +78,29 @@ def test_autotune_picks_a_timed_candidate(setup):
         else:
             assert np.all(timings[b] == -1)
             assert (c.block_w, c.chunk) == (16, 512)
+
+
+def test_plans_mixing_thread_counts_keep_their_buffers(setup):
+    """A table whose buckets use 128- and 256-thread CTAs gives a plan with two launches. Building
+    it must not free the first launch's work list (it once did, when the launch list grew), so
+    the plan paints the default plan's levels, frees cleanly, and later plans still capture."""
+    ctx, scene, dev, tiles = setup
+    buckets = {native.tile_bucket(t) for t in tiles}
+    assert {0, 1} <= buckets
+    table = abi.TuneTable()
+    table.bucket[0] = abi.TileConfig(16, 8, 128, 512)
+    for k in range(1, abi.TILE_BUCKETS):
+        table.bucket[k] = abi.TileConfig(32, 32, 256, 128)
+    ref = native.BatchPlan(dev, tiles)
+    ref.run()
+    ref_dba = ref.read()[1]
+    ref.close()
+    for _ in range(2):
+        mixed = native.BatchPlan(dev, tiles, table=table)
+        mixed.run()
+        np.testing.assert_allclose(mixed.read()[1], ref_dba, atol=0.01)
+        mixed.close()
+    again = native.BatchPlan(dev, tiles)
+    again.run()
+    assert np.array_equal(again.read()[1], ref_dba)
+    again.close()
