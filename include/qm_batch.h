@@ -190,6 +190,29 @@ qm_status qm_level_histogram(qm_ctx *ctx, const float *levels_db, size_t n,
                              double level_min_db, double bin_db, uint32_t n_bins,
                              uint32_t *counts);
 
+/* Map cells of n pixels, one byte per layer and one for the total (last), as
+ * `PaintedCells::from_painted` makes them (paint/src/levels.rs:55-68, called by the painter at
+ * paint/src/paint.rs:497):
+ * - Lden cells (lden_cells[n][QM_LAYERS + 1]) from the linear Lden energy of each layer
+ *   (lden_energy[n][QM_LAYERS]): round(2 Lden dB), at most 253, QM_CELL_SILENCE below energy 1
+ *   (`lden_cell`, levels.rs:87-98); the total sums the layers' energies before the logarithm
+ *   (`lden_cells`, levels.rs:100-111);
+ * - loudness cells (nden_cells[n][QM_LAYERS + 1], wanted only with sone[n][QM_LAYERS + 1]):
+ *   round(80 + 20 log2 sone), twice the loudness level in phon, at most 253, QM_CELL_SILENCE
+ *   under 0 phon or for NaN (`cell`, levels.rs:25-33).
+ * Pixels with assessed[p] == 0 (assessed may be null: every pixel assessed) are QM_CELL_NO_LEVEL
+ * in every byte. An assessed pixel with a negative or non-finite Lden energy, or whose layers sum
+ * to a non-finite total, fails the call with QM_ERR_ARGUMENT and a message naming the lowest such
+ * pixel and its first bad layer ("pixel P, layer L: ..." or "pixel P, total: ..."), the outputs
+ * left unwritten. Arithmetic is f64 rounded as the reference rounds it; a byte can differ from
+ * the reference's only where CUDA's and the host's log10/log2 differ in the last bit at a half
+ * step. */
+#define QM_CELL_NO_LEVEL 255
+#define QM_CELL_SILENCE 254
+qm_status qm_quantize_cells(qm_ctx *ctx, const double *lden_energy, const double *sone,
+                            const uint8_t *assessed, size_t n, uint8_t *lden_cells,
+                            uint8_t *nden_cells);
+
 /* The obstacle crossings of n rays from (from_xy) to (to_xy), lattice steps: per ray its count
  * (counts[n]) and, up to `cap` per ray, the crossed edges (the edge's first vertex index),
  * chainages t (f64) and flags (bit 0 building, bit 1 bounds_roof), sorted and deduplicated as

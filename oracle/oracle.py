@@ -66,6 +66,13 @@ def lib():
         L.qmo_level_histogram.argtypes = [_D, C.c_size_t, C.c_double, C.c_double, C.c_uint32, _U32]
         L.qmo_level_bin.argtypes = [C.c_double, C.c_double, C.c_double, C.c_uint32]
         L.qmo_level_bin.restype = C.c_uint32
+        _B = C.POINTER(C.c_uint8)
+        L.qmo_nden_cell.argtypes = [C.c_double]
+        L.qmo_nden_cell.restype = C.c_uint8
+        L.qmo_lden_cell.argtypes = [C.c_double]
+        L.qmo_lden_cell.restype = C.c_int
+        L.qmo_quantize_cells.argtypes = [_D, _D, _B, C.c_size_t, _B, _B]
+        L.qmo_quantize_cells.restype = C.c_int64
         for name in ("qmo_lateral_attenuation_db", "qmo_speed_correction_db"):
             getattr(L, name).argtypes = [C.c_double, C.c_double]
             getattr(L, name).restype = C.c_double
@@ -272,6 +279,38 @@ def level_histogram(levels, level_min, bin_db, n_bins):
 
 def level_bin(level, level_min, bin_db, n_bins):
     return lib().qmo_level_bin(level, level_min, bin_db, n_bins)
+
+
+def nden_cell(sone):
+    """The map cell of a loudness (paint/src/levels.rs:25-33)."""
+    return int(lib().qmo_nden_cell(float(sone)))
+
+
+def lden_cell(energy):
+    """The map cell of a linear Lden energy (paint/src/levels.rs:87-98); ValueError where the
+    reference returns its error."""
+    c = lib().qmo_lden_cell(float(energy))
+    if c < 0:
+        raise ValueError(f"invalid Lden energy {energy}")
+    return c
+
+
+def quantize_cells(lden_energy, sone=None, assessed=None):
+    """Map cells of pixels (paint/src/levels.rs:55-111): (lden_cells [n][7], nden_cells [n][7] or
+    None); ValueError naming the first invalid pixel and layer, as the reference's error does."""
+    e = np.ascontiguousarray(np.asarray(lden_energy, dtype=np.float64).reshape(-1, abi.LAYERS))
+    n = len(e)
+    s = None if sone is None else np.ascontiguousarray(np.asarray(sone, dtype=np.float64).reshape(n, abi.LAYERS + 1))
+    a = None if assessed is None else np.ascontiguousarray(np.asarray(assessed, dtype=np.uint8).reshape(n))
+    lc = np.zeros((n, abi.LAYERS + 1), np.uint8)
+    nc = None if s is None else np.zeros((n, abi.LAYERS + 1), np.uint8)
+    bad = lib().qmo_quantize_cells(abi.ptr(e, C.c_double), abi.ptr(s, C.c_double), abi.ptr(a, C.c_uint8), n,
+                                   abi.ptr(lc, C.c_uint8), abi.ptr(nc, C.c_uint8))
+    if bad >= 0:
+        pixel, layer = divmod(int(bad), 8)
+        where = f"layer {layer}" if layer < abi.LAYERS else "total"
+        raise ValueError(f"pixel {pixel}, {where}: invalid Lden energy")
+    return lc, nc
 
 
 # ---------------------------------------------------------------------------------------------

@@ -1770,6 +1770,56 @@ uint32_t qmo_level_bin(double level, double level_min, double bin_db, uint32_t n
     return level_bin(level, level_min, bin_db, n_bins);
 }
 
+// Map cells. `cell` (paint/src/levels.rs:25-33): 80 + 20 log2(sone), silence (254) when NaN or
+// below 0, else rounded half away from zero and capped at 253.
+uint8_t qmo_nden_cell(double sone) {
+    const double byte = 80.0 + 20.0 * std::log2(sone);
+    if (std::isnan(byte) || byte < 0.0) return 254;
+    return (uint8_t)std::min(std::round(byte), 253.0);
+}
+
+// `lden_cell` (paint/src/levels.rs:87-98): -1 for an energy that is negative or not finite (the
+// reference's error), 254 below 1, else round(2 level_db) capped at 253, level_db = 10 log10
+// (physics/src/bands.rs:45-56).
+int qmo_lden_cell(double energy) {
+    if (!std::isfinite(energy) || energy < 0.0) return -1;
+    if (energy < 1.0) return 254;
+    return (int)std::min(std::round(2.0 * (10.0 * std::log10(energy))), 253.0);
+}
+
+// `PaintedCells::from_painted` (paint/src/levels.rs:55-68) with `lden_cells` (:100-111) and
+// `cells_of` (:36-38) over n pixels: lden_cells[n][7] from lden_energy[n][6], nden_cells[n][7]
+// from sone[n][7] (both skipped when sone is null), 255 for unassessed pixels (assessed null: all
+// assessed). Returns -1, or pixel * 8 + layer of the first invalid energy in pixel order (layer 6:
+// the total, the layers summed in order), after which the outputs are not meaningful.
+int64_t qmo_quantize_cells(const double *lden_energy, const double *sone, const uint8_t *assessed, size_t n,
+                           uint8_t *lden_cells, uint8_t *nden_cells) {
+    constexpr int L = QM_LAYERS, W = QM_LAYERS + 1;
+    for (size_t p = 0; p < n; ++p) {
+        if (assessed && assessed[p] == 0) {
+            for (int l = 0; l < W; ++l) {
+                lden_cells[p * W + l] = 255;
+                if (sone) nden_cells[p * W + l] = 255;
+            }
+            continue;
+        }
+        double total = 0.0;
+        for (int l = 0; l < L; ++l) {
+            const double e = lden_energy[p * L + l];
+            const int c = qmo_lden_cell(e);
+            if (c < 0) return (int64_t)(p * 8 + l);
+            lden_cells[p * W + l] = (uint8_t)c;
+            total += e;
+        }
+        const int c = qmo_lden_cell(total);
+        if (c < 0) return (int64_t)(p * 8 + L);
+        lden_cells[p * W + L] = (uint8_t)c;
+        if (sone)
+            for (int l = 0; l < W; ++l) nden_cells[p * W + l] = qmo_nden_cell(sone[p * W + l]);
+    }
+    return -1;
+}
+
 // Surrogate training samples (the features of include/qm_surrogate.h and the exact A_boundary of
 // the homogeneous state as the label) for cells [cell_begin, cell_end) of a grid against its
 // source range: row (cell - cell_begin) * n_src + (source - source_begin). The roofs are the

@@ -14,6 +14,7 @@ PERIODS = 3
 SECTORS = 16
 LAYERS = 6
 THIRDS = 28
+CELL_NO_LEVEL, CELL_SILENCE = 255, 254
 PAIR_SUMS = 9
 POINT_BANDS = LAYERS * PERIODS * BANDS
 

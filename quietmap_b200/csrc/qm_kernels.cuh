@@ -296,6 +296,59 @@ __global__ void __launch_bounds__(256) histogram_kernel(const float *levels, siz
         if (s_hist[k]) atomicAdd(counts + k, s_hist[k]);
 }
 
+// Map cells (qm_quantize_cells; paint/src/levels.rs). The products and sums are rounded one by
+// one (no fused multiply-add), as the reference's f64 arithmetic is.
+__device__ __forceinline__ uint8_t lden_cell_of(double energy) {  // levels.rs:87-98, energy valid
+    if (energy < 1.0) return QM_CELL_SILENCE;
+    return (uint8_t)fmin(round(__dmul_rn(2.0, __dmul_rn(10.0, log10(energy)))), (double)(QM_CELL_SILENCE - 1));
+}
+
+__device__ __forceinline__ uint8_t nden_cell_of(double sone) {  // levels.rs:25-33
+    const double byte = __dadd_rn(80.0, __dmul_rn(20.0, log2(sone)));
+    if (isnan(byte) || byte < 0.0) return QM_CELL_SILENCE;
+    return (uint8_t)fmin(round(byte), (double)(QM_CELL_SILENCE - 1));
+}
+
+// Thread = pixel (grid-stride). An invalid Lden energy of an assessed pixel lowers *first_bad to
+// pixel * 8 + layer (layer QM_LAYERS: the total); that pixel's bytes are then not meaningful.
+__global__ void __launch_bounds__(256) quantize_cells_kernel(const double *lden_energy, const double *sone,
+                                                             const uint8_t *assessed, size_t n, uint8_t *lden_cells,
+                                                             uint8_t *nden_cells, unsigned long long *first_bad) {
+    constexpr int W = QM_LAYERS + 1;
+    for (size_t p = blockIdx.x * (size_t)blockDim.x + threadIdx.x; p < n; p += (size_t)gridDim.x * blockDim.x) {
+        uint8_t lc[W], nc[W];
+        if (assessed && assessed[p] == 0) {
+#pragma unroll
+            for (int l = 0; l < W; ++l) lc[l] = nc[l] = QM_CELL_NO_LEVEL;
+        } else {
+#pragma unroll
+            for (int l = 0; l < W; ++l) lc[l] = nc[l] = QM_CELL_SILENCE;
+            double total = 0.0;
+            int bad = -1;
+#pragma unroll
+            for (int l = 0; l < QM_LAYERS; ++l) {
+                const double e = lden_energy[p * QM_LAYERS + l];
+                if (bad < 0 && !(isfinite(e) && e >= 0.0)) bad = l;
+                if (bad < 0) lc[l] = lden_cell_of(e);
+                total = __dadd_rn(total, e);  // in layer order, as the reference's sum
+            }
+            if (bad < 0 && !(isfinite(total) && total >= 0.0)) bad = QM_LAYERS;
+            if (bad < 0) lc[QM_LAYERS] = lden_cell_of(total);
+            if (bad >= 0) atomicMin(first_bad, (unsigned long long)p * 8ull + (unsigned long long)bad);
+            if (nden_cells) {
+#pragma unroll
+                for (int l = 0; l < W; ++l) nc[l] = nden_cell_of(sone[p * W + l]);
+            }
+        }
+#pragma unroll
+        for (int l = 0; l < W; ++l) lden_cells[p * W + l] = lc[l];
+        if (nden_cells) {
+#pragma unroll
+            for (int l = 0; l < W; ++l) nden_cells[p * W + l] = nc[l];
+        }
+    }
+}
+
 struct PairArgs {
     const int2 *rcv_xy;
     const float *rcv_alt;

@@ -112,14 +112,6 @@ struct Scratch {
     Scratch(const Scratch &) = delete;
     Scratch &operator=(const Scratch &) = delete;
     Scratch(Scratch &&o) noexcept : p(o.p) { o.p = nullptr; }
-    Scratch &operator=(Scratch &&o) noexcept {
-        if (this != &o) {
-            if (p) cudaFree(p);
-            p = o.p;
-            o.p = nullptr;
-        }
-        return *this;
-    }
     ~Scratch() {
         if (p) cudaFree(p);
     }
@@ -838,6 +830,69 @@ qm_status qm_level_histogram(qm_ctx *ctx, const float *levels_db, size_t n, doub
     }
     QM_CUDA(cudaMemcpyAsync(counts, d_out.p, n_bins * sizeof(uint32_t), cudaMemcpyDeviceToHost, ctx->stream));
     QM_CUDA(cudaStreamSynchronize(ctx->stream));
+    return QM_OK;
+}
+
+qm_status qm_quantize_cells(qm_ctx *ctx, const double *lden_energy, const double *sone, const uint8_t *assessed,
+                            size_t n, uint8_t *lden_cells, uint8_t *nden_cells) {
+    if (!ctx) return fail(QM_ERR_ARGUMENT, "qm_quantize_cells: null ctx");
+    if ((sone == nullptr) != (nden_cells == nullptr))
+        return fail(QM_ERR_ARGUMENT, "qm_quantize_cells: sone and nden_cells are given together or not at all");
+    if (n == 0) return QM_OK;
+    if (!lden_energy || !lden_cells) return fail(QM_ERR_ARGUMENT, "qm_quantize_cells: null lden_energy or lden_cells");
+    if (n > (size_t(1) << 40)) return fail(QM_ERR_ARGUMENT, "qm_quantize_cells: more than 2^40 pixels");
+    constexpr size_t W = QM_LAYERS + 1;
+    std::lock_guard<std::mutex> guard(ctx->lock);
+    QM_CUDA(cudaSetDevice(ctx->device));
+    cudaStream_t stream = ctx->stream;
+    Scratch d_energy, d_sone, d_assessed, d_lc, d_nc, d_bad;
+    QM_CUDA(cudaMalloc(&d_energy.p, n * QM_LAYERS * sizeof(double)));
+    QM_CUDA(cudaMalloc(&d_lc.p, n * W));
+    QM_CUDA(cudaMalloc(&d_bad.p, sizeof(unsigned long long)));
+    QM_CUDA(cudaMemcpyAsync(d_energy.p, lden_energy, n * QM_LAYERS * sizeof(double), cudaMemcpyHostToDevice, stream));
+    if (sone) {
+        QM_CUDA(cudaMalloc(&d_sone.p, n * W * sizeof(double)));
+        QM_CUDA(cudaMalloc(&d_nc.p, n * W));
+        QM_CUDA(cudaMemcpyAsync(d_sone.p, sone, n * W * sizeof(double), cudaMemcpyHostToDevice, stream));
+    }
+    if (assessed) {
+        QM_CUDA(cudaMalloc(&d_assessed.p, n));
+        QM_CUDA(cudaMemcpyAsync(d_assessed.p, assessed, n, cudaMemcpyHostToDevice, stream));
+    }
+    QM_CUDA(cudaMemsetAsync(d_bad.p, 0xff, sizeof(unsigned long long), stream));
+    const unsigned blocks = (unsigned)std::min<size_t>((n + 255) / 256, (size_t)ctx->sm_count * 16);
+    quantize_cells_kernel<<<blocks, 256, 0, stream>>>(
+        static_cast<const double *>(d_energy.p), static_cast<const double *>(d_sone.p),
+        static_cast<const uint8_t *>(d_assessed.p), n, static_cast<uint8_t *>(d_lc.p), static_cast<uint8_t *>(d_nc.p),
+        static_cast<unsigned long long *>(d_bad.p));
+    QM_CUDA(cudaGetLastError());
+    unsigned long long bad = 0;
+    QM_CUDA(cudaMemcpyAsync(&bad, d_bad.p, sizeof(bad), cudaMemcpyDeviceToHost, stream));
+    QM_CUDA(cudaStreamSynchronize(stream));
+    if (bad != ~0ull) {
+        // The reference's message (levels.rs:100-111), with the offending value from the input.
+        const size_t pixel = (size_t)(bad / 8);
+        const int layer = (int)(bad % 8);
+        double value = 0.0;
+        if (layer < QM_LAYERS) {
+            value = lden_energy[pixel * QM_LAYERS + layer];
+        } else {
+            for (int l = 0; l < QM_LAYERS; ++l) value += lden_energy[pixel * QM_LAYERS + l];
+        }
+        char text[64];
+        if (std::isnan(value))
+            std::snprintf(text, sizeof text, "NaN");
+        else if (std::isinf(value))
+            std::snprintf(text, sizeof text, value > 0 ? "inf" : "-inf");
+        else
+            std::snprintf(text, sizeof text, "%.17g", value);
+        const std::string where = layer < QM_LAYERS ? "layer " + std::to_string(layer) : std::string("total");
+        return fail(QM_ERR_ARGUMENT, "qm_quantize_cells: pixel " + std::to_string(pixel) + ", " + where +
+                                         ": invalid Lden energy " + text);
+    }
+    QM_CUDA(cudaMemcpyAsync(lden_cells, d_lc.p, n * W, cudaMemcpyDeviceToHost, stream));
+    if (sone) QM_CUDA(cudaMemcpyAsync(nden_cells, d_nc.p, n * W, cudaMemcpyDeviceToHost, stream));
+    QM_CUDA(cudaStreamSynchronize(stream));
     return QM_OK;
 }
 

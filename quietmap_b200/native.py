@@ -19,6 +19,7 @@ _F = C.POINTER(C.c_float)
 _U32 = C.POINTER(C.c_uint32)
 _U64 = C.POINTER(C.c_uint64)
 _I32 = C.POINTER(C.c_int32)
+_U8 = C.POINTER(C.c_uint8)
 
 
 class QmError(RuntimeError):
@@ -57,6 +58,8 @@ def lib():
         L.qm_zwicker.restype = C.c_int
         L.qm_level_histogram.argtypes = [C.c_void_p, _F, C.c_size_t, C.c_double, C.c_double, C.c_uint32, _U32]
         L.qm_level_histogram.restype = C.c_int
+        L.qm_quantize_cells.argtypes = [C.c_void_p, _D, _D, _U8, C.c_size_t, _U8, _U8]
+        L.qm_quantize_cells.restype = C.c_int
         L.qm_list_crossings.argtypes = [C.c_void_p, _I32, _I32, C.c_size_t, C.c_uint32, _U32, _U32, _D, _U32, _U32]
         L.qm_list_crossings.restype = C.c_int
         L.qm_flight_grid.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_size_t,
@@ -153,6 +156,20 @@ class Context:
             return lae, thirds, out_sone, dict(pairs=st.pairs, pairs_in_reach=st.pairs_in_reach,
                                                kernel_ms=st.kernel_ms, loudness_ms=st.loudness_ms)
         return lae, thirds, out_sone
+
+    def quantize_cells(self, lden_energy, sone=None, assessed=None):
+        """Map cells of pixels (qm_quantize_cells): (lden_cells [n][7], nden_cells [n][7] or None)
+        from linear Lden energies [n][6], loudness [n][7] (sone) and assessed flags [n]."""
+        energy = np.ascontiguousarray(np.asarray(lden_energy, dtype=np.float64).reshape(-1, abi.LAYERS))
+        n = len(energy)
+        s = None if sone is None else np.ascontiguousarray(np.asarray(sone, dtype=np.float64).reshape(n, abi.LAYERS + 1))
+        a = None if assessed is None else np.ascontiguousarray(np.asarray(assessed, dtype=np.uint8).reshape(n))
+        lc = np.zeros((n, abi.LAYERS + 1), np.uint8)
+        nc = None if s is None else np.zeros((n, abi.LAYERS + 1), np.uint8)
+        _check(lib().qm_quantize_cells(self.handle, abi.ptr(energy, C.c_double), abi.ptr(s, C.c_double),
+                                       abi.ptr(a, C.c_uint8), n, abi.ptr(lc, C.c_uint8), abi.ptr(nc, C.c_uint8)),
+               self.handle)
+        return lc, nc
 
     def level_histogram(self, levels_db, level_min_db=-30.0, bin_db=0.1, n_bins=1800):
         levels = np.ascontiguousarray(levels_db, dtype=np.float32).ravel()

@@ -1,0 +1,78 @@
+"""Map cells (the bytes `PaintedCells::from_painted` writes, paint/src/levels.rs): the oracle pinned
+to the reference's known answers (levels.rs:115-137) and to the loudness cell's definition
+(levels.rs:22-33: twice the loudness level in phon, 40 + 10 log2 sone)."""
+
+import math
+
+import numpy as np
+import pytest
+
+from oracle import oracle
+from quietmap_b200 import abi
+
+ROAD, RAILWAY, AIRCRAFT = 0, 1, 5  # tiles/src/sources.rs:59-66
+
+
+def energy(level_db):
+    """physics/src/bands.rs:34-36: exp(L ln10 / 10)."""
+    return math.exp(level_db * (2.302585092994046 / 10.0))
+
+
+def test_lden_cells_match_the_reference_known_answers():
+    assert oracle.lden_cell(0.0) == abi.CELL_SILENCE
+    assert oracle.lden_cell(energy(-0.01)) == abi.CELL_SILENCE
+    assert oracle.lden_cell(1.0) == 0
+    assert oracle.lden_cell(energy(60.26)) == 121
+    assert oracle.lden_cell(energy(150.0)) == 253
+    for bad in (-1.0, math.inf, math.nan):
+        with pytest.raises(ValueError):
+            oracle.lden_cell(bad)
+
+
+def test_layers_are_summed_before_the_logarithm():
+    layers = np.zeros((13, abi.LAYERS))
+    layers[12, ROAD] = energy(60.0)
+    layers[12, AIRCRAFT] = energy(60.0)
+    cells, _ = oracle.quantize_cells(layers)
+    assert cells[12, abi.LAYERS] == 126
+    assert cells[12, RAILWAY] == abi.CELL_SILENCE
+    assert cells[12, ROAD] == 120
+    layers[12, 2] = math.nan
+    with pytest.raises(ValueError, match="pixel 12, layer 2"):
+        oracle.quantize_cells(layers)
+
+
+def test_a_total_that_overflows_is_an_error_and_unassessed_pixels_are_not_checked():
+    layers = np.full((3, abi.LAYERS), 1e308)
+    with pytest.raises(ValueError, match="pixel 0, total"):
+        oracle.quantize_cells(layers)
+    cells, _ = oracle.quantize_cells(layers, assessed=np.zeros(3, np.uint8))
+    assert np.all(cells == abi.CELL_NO_LEVEL)
+
+
+def test_loudness_cells_follow_the_definition():
+    # 1 sone = 40 phon -> 80; a doubling is 20 steps; 1/16 sone = 0 phon -> 0; below: silence.
+    assert [oracle.nden_cell(s) for s in (1.0, 2.0, 0.5, 1.0 / 16.0)] == [80, 100, 60, 0]
+    assert oracle.nden_cell(0.06) == abi.CELL_SILENCE
+    assert oracle.nden_cell(0.0) == abi.CELL_SILENCE
+    assert oracle.nden_cell(math.nan) == abi.CELL_SILENCE
+    assert oracle.nden_cell(-1.0) == abi.CELL_SILENCE
+    assert oracle.nden_cell(math.inf) == 253
+    assert oracle.nden_cell(2.0 ** 8.6) == 252
+
+
+def test_pixels_quantize_per_layer_and_in_total():
+    rng = np.random.default_rng(3)
+    n = 2000
+    layers = 10.0 ** rng.uniform(-3, 15, (n, abi.LAYERS))
+    layers[rng.random((n, abi.LAYERS)) < 0.2] = 0.0
+    sone = 2.0 ** rng.uniform(-6, 9, (n, abi.LAYERS + 1))
+    assessed = (rng.random(n) > 0.1).astype(np.uint8)
+    lc, nc = oracle.quantize_cells(layers, sone, assessed)
+    for p in range(0, n, 97):
+        if not assessed[p]:
+            assert np.all(lc[p] == abi.CELL_NO_LEVEL) and np.all(nc[p] == abi.CELL_NO_LEVEL)
+            continue
+        assert [oracle.lden_cell(e) for e in layers[p]] == list(lc[p, :abi.LAYERS])
+        assert oracle.lden_cell(sum(layers[p])) == lc[p, abi.LAYERS]
+        assert [oracle.nden_cell(s) for s in sone[p]] == list(nc[p])
