@@ -213,6 +213,19 @@ qm_status qm_quantize_cells(qm_ctx *ctx, const double *lden_energy, const double
                             const uint8_t *assessed, size_t n, uint8_t *lden_cells,
                             uint8_t *nden_cells);
 
+/* HM3 / HMD tile streams up to their Brotli stage (`encode_metric_tile`, paint/src/hm3.rs:95-109):
+ * per tile, the 5-byte header ("HM3 \x07" for loudness cells, metric 0; "HMD \x01" for Lden cells,
+ * metric 1; hm3.rs:22-27), the layer byte, then the 512 x 512 cells (row-major from the
+ * north-west) as PNG Paeth residuals, cell - prediction mod 256 (filter 4 with its left, above,
+ * upper-left tie order and zeros outside the tile; `paeth_prediction`, hm3.rs:68-93).
+ * cells[n_tiles][512 * 512], layers[n_tiles] (each at most QM_LAYERS: the total), streams
+ * [n_tiles][QM_HM3_STREAM_BYTES]. The reference then compresses each stream with Google's Brotli
+ * encoder (quality 10 for loudness, 9 for Lden, window 2^19); that stage is the caller's. */
+#define QM_HM3_TILE_PX 512
+#define QM_HM3_STREAM_BYTES (6 + 512 * 512)
+qm_status qm_hm3_predict(qm_ctx *ctx, const uint8_t *cells, const uint8_t *layers, size_t n_tiles,
+                         int metric, uint8_t *streams);
+
 /* The obstacle crossings of n rays from (from_xy) to (to_xy), lattice steps: per ray its count
  * (counts[n]) and, up to `cap` per ray, the crossed edges (the edge's first vertex index),
  * chainages t (f64) and flags (bit 0 building, bit 1 bounds_roof), sorted and deduplicated as

@@ -73,6 +73,10 @@ def lib():
         L.qmo_lden_cell.restype = C.c_int
         L.qmo_quantize_cells.argtypes = [_D, _D, _B, C.c_size_t, _B, _B]
         L.qmo_quantize_cells.restype = C.c_int64
+        L.qmo_hm3_predict.argtypes = [_B, C.c_uint8, C.c_int, _B]
+        L.qmo_hm3_predict.restype = C.c_int
+        L.qmo_hm3_unpredict.argtypes = [_B]
+        L.qmo_hm3_unpredict.restype = None
         for name in ("qmo_lateral_attenuation_db", "qmo_speed_correction_db"):
             getattr(L, name).argtypes = [C.c_double, C.c_double]
             getattr(L, name).restype = C.c_double
@@ -293,6 +297,27 @@ def lden_cell(energy):
     if c < 0:
         raise ValueError(f"invalid Lden energy {energy}")
     return c
+
+
+HM3_TILE_PX = 512
+HM3_STREAM_BYTES = 6 + HM3_TILE_PX * HM3_TILE_PX
+
+
+def hm3_predict(cells, layer, metric):
+    """One tile's HM3 / HMD stream before Brotli (paint/src/hm3.rs:95-109): uint8 [6 + 512^2]."""
+    c = np.ascontiguousarray(np.asarray(cells, dtype=np.uint8).reshape(HM3_TILE_PX * HM3_TILE_PX))
+    out = np.zeros(HM3_STREAM_BYTES, np.uint8)
+    if lib().qmo_hm3_predict(abi.ptr(c, C.c_uint8), int(layer), int(metric), abi.ptr(out, C.c_uint8)) != 0:
+        raise ValueError(f"unknown HM3 layer {layer}")
+    return out
+
+
+def hm3_unpredict(residuals):
+    """The Paeth residuals of a stream (its bytes after the 6-byte head) back to the cells
+    (paint/src/hm3.rs:162-165): uint8 [512][512]."""
+    r = np.array(np.asarray(residuals, dtype=np.uint8).reshape(HM3_TILE_PX * HM3_TILE_PX), copy=True)
+    lib().qmo_hm3_unpredict(abi.ptr(r, C.c_uint8))
+    return r.reshape(HM3_TILE_PX, HM3_TILE_PX)
 
 
 def quantize_cells(lden_energy, sone=None, assessed=None):

@@ -1787,6 +1787,39 @@ int qmo_lden_cell(double energy) {
     return (int)std::min(std::round(2.0 * (10.0 * std::log10(energy))), 253.0);
 }
 
+// HM3 streams. `paeth_prediction` (paint/src/hm3.rs:68-93): PNG filter 4 over a 512-wide tile,
+// zeros outside it, ties to left, then above.
+static uint8_t hm3_paeth(const uint8_t *cells, size_t at) {
+    const size_t P = QM_HM3_TILE_PX;
+    const bool has_left = at % P != 0, has_above = at >= P;
+    const int left = has_left ? cells[at - 1] : 0;
+    const int above = has_above ? cells[at - P] : 0;
+    const int corner = has_left && has_above ? cells[at - P - 1] : 0;
+    const int estimate = left + above - corner;
+    const int dl = std::abs(estimate - left), da = std::abs(estimate - above), dc = std::abs(estimate - corner);
+    if (dl <= da && dl <= dc) return (uint8_t)left;
+    return (uint8_t)(da <= dc ? above : corner);
+}
+
+// `encode_metric_tile` up to its Brotli stage (paint/src/hm3.rs:95-109): header ("HM3 \x07" or
+// "HMD \x01", hm3.rs:22-27), layer byte, residuals. Returns 0, or -1 for a layer above QM_LAYERS.
+int qmo_hm3_predict(const uint8_t *cells, uint8_t layer, int metric, uint8_t *stream) {
+    if (layer > QM_LAYERS) return -1;
+    static const uint8_t header[2][5] = {{'H', 'M', '3', ' ', 0x07}, {'H', 'M', 'D', ' ', 0x01}};
+    std::memcpy(stream, header[metric ? 1 : 0], 5);
+    stream[5] = layer;
+    const size_t n = (size_t)QM_HM3_TILE_PX * QM_HM3_TILE_PX;
+    for (size_t at = 0; at < n; ++at) stream[6 + at] = (uint8_t)(cells[at] - hm3_paeth(cells, at));
+    return 0;
+}
+
+// The residuals' inverse, as `decode_metric_tile` applies it after Brotli (paint/src/hm3.rs:
+// 162-165): in place, in order, each byte plus the prediction from the bytes already restored.
+void qmo_hm3_unpredict(uint8_t *residuals) {
+    const size_t n = (size_t)QM_HM3_TILE_PX * QM_HM3_TILE_PX;
+    for (size_t at = 0; at < n; ++at) residuals[at] = (uint8_t)(residuals[at] + hm3_paeth(residuals, at));
+}
+
 // `PaintedCells::from_painted` (paint/src/levels.rs:55-68) with `lden_cells` (:100-111) and
 // `cells_of` (:36-38) over n pixels: lden_cells[n][7] from lden_energy[n][6], nden_cells[n][7]
 // from sone[n][7] (both skipped when sone is null), 255 for unassessed pixels (assessed null: all

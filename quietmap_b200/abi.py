@@ -15,6 +15,8 @@ SECTORS = 16
 LAYERS = 6
 THIRDS = 28
 CELL_NO_LEVEL, CELL_SILENCE = 255, 254
+HM3_TILE_PX = 512
+HM3_STREAM_BYTES = 6 + HM3_TILE_PX * HM3_TILE_PX
 PAIR_SUMS = 9
 POINT_BANDS = LAYERS * PERIODS * BANDS
 

@@ -349,6 +349,39 @@ __global__ void __launch_bounds__(256) quantize_cells_kernel(const double *lden_
     }
 }
 
+// HM3 / HMD stream bytes before Brotli (qm_hm3_predict; paint/src/hm3.rs:68-109). Thread = one
+// output byte of one tile (grid-stride); the tile's first thread also writes its header.
+__device__ __forceinline__ uint8_t paeth_residual(const uint8_t *tile, uint32_t at) {
+    constexpr uint32_t P = QM_HM3_TILE_PX;
+    const bool has_left = (at % P) != 0, has_above = at >= P;
+    const int left = has_left ? tile[at - 1] : 0;
+    const int above = has_above ? tile[at - P] : 0;
+    const int corner = (has_left && has_above) ? tile[at - P - 1] : 0;
+    const int estimate = left + above - corner;
+    const int dl = abs(estimate - left), da = abs(estimate - above), dc = abs(estimate - corner);
+    const int predicted = (dl <= da && dl <= dc) ? left : (da <= dc ? above : corner);
+    return (uint8_t)(tile[at] - predicted);
+}
+
+__global__ void __launch_bounds__(256) hm3_predict_kernel(const uint8_t *cells, const uint8_t *layers, size_t n_tiles,
+                                                          uint32_t header_word, uint8_t header_last,
+                                                          uint8_t *streams) {
+    constexpr size_t PIX = (size_t)QM_HM3_TILE_PX * QM_HM3_TILE_PX;
+    const size_t total = n_tiles * PIX;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
+        const size_t tile = i / PIX;
+        const uint32_t at = (uint32_t)(i - tile * PIX);
+        uint8_t *out = streams + tile * (size_t)QM_HM3_STREAM_BYTES;
+        if (at == 0) {
+#pragma unroll
+            for (int k = 0; k < 4; ++k) out[k] = (uint8_t)(header_word >> (8 * k));
+            out[4] = header_last;
+            out[5] = layers[tile];
+        }
+        out[6 + at] = paeth_residual(cells + tile * PIX, at);
+    }
+}
+
 struct PairArgs {
     const int2 *rcv_xy;
     const float *rcv_alt;

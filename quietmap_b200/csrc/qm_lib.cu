@@ -896,6 +896,41 @@ qm_status qm_quantize_cells(qm_ctx *ctx, const double *lden_energy, const double
     return QM_OK;
 }
 
+qm_status qm_hm3_predict(qm_ctx *ctx, const uint8_t *cells, const uint8_t *layers, size_t n_tiles, int metric,
+                         uint8_t *streams) {
+    if (!ctx) return fail(QM_ERR_ARGUMENT, "qm_hm3_predict: null ctx");
+    if (metric != 0 && metric != 1) return fail(QM_ERR_ARGUMENT, "qm_hm3_predict: metric is 0 (loudness) or 1 (Lden)");
+    if (n_tiles == 0) return QM_OK;
+    if (!cells || !layers || !streams) return fail(QM_ERR_ARGUMENT, "qm_hm3_predict: null cells, layers or streams");
+    if (n_tiles > (size_t(1) << 16)) return fail(QM_ERR_ARGUMENT, "qm_hm3_predict: more than 65,536 tiles in one call");
+    for (size_t t = 0; t < n_tiles; ++t)
+        if (layers[t] > QM_LAYERS)
+            return fail(QM_ERR_ARGUMENT, "qm_hm3_predict: tile " + std::to_string(t) + ": unknown layer " +
+                                             std::to_string(layers[t]));
+    constexpr size_t PIX = (size_t)QM_HM3_TILE_PX * QM_HM3_TILE_PX;
+    // "HM3 \x07" (loudness) or "HMD \x01" (Lden): the first four bytes little-endian, then the fifth.
+    const uint8_t header[2][5] = {{'H', 'M', '3', ' ', 0x07}, {'H', 'M', 'D', ' ', 0x01}};
+    const uint8_t *h = header[metric];
+    const uint32_t word = (uint32_t)h[0] | ((uint32_t)h[1] << 8) | ((uint32_t)h[2] << 16) | ((uint32_t)h[3] << 24);
+    std::lock_guard<std::mutex> guard(ctx->lock);
+    QM_CUDA(cudaSetDevice(ctx->device));
+    cudaStream_t stream = ctx->stream;
+    Scratch d_cells, d_layers, d_streams;
+    QM_CUDA(cudaMalloc(&d_cells.p, n_tiles * PIX));
+    QM_CUDA(cudaMalloc(&d_layers.p, n_tiles));
+    QM_CUDA(cudaMalloc(&d_streams.p, n_tiles * (size_t)QM_HM3_STREAM_BYTES));
+    QM_CUDA(cudaMemcpyAsync(d_cells.p, cells, n_tiles * PIX, cudaMemcpyHostToDevice, stream));
+    QM_CUDA(cudaMemcpyAsync(d_layers.p, layers, n_tiles, cudaMemcpyHostToDevice, stream));
+    const unsigned blocks = (unsigned)std::min<size_t>((n_tiles * PIX + 255) / 256, (size_t)ctx->sm_count * 16);
+    hm3_predict_kernel<<<blocks, 256, 0, stream>>>(static_cast<const uint8_t *>(d_cells.p),
+                                                   static_cast<const uint8_t *>(d_layers.p), n_tiles, word, h[4],
+                                                   static_cast<uint8_t *>(d_streams.p));
+    QM_CUDA(cudaGetLastError());
+    QM_CUDA(cudaMemcpyAsync(streams, d_streams.p, n_tiles * (size_t)QM_HM3_STREAM_BYTES, cudaMemcpyDeviceToHost, stream));
+    QM_CUDA(cudaStreamSynchronize(stream));
+    return QM_OK;
+}
+
 qm_status qm_list_crossings(qm_scene *scene, const int32_t *from_xy, const int32_t *to_xy, size_t n, uint32_t cap,
                             uint32_t *counts, uint32_t *edges, double *t, uint32_t *flags, uint32_t *status) {
     if (!scene) return fail(QM_ERR_ARGUMENT, "qm_list_crossings: null scene");

@@ -60,6 +60,8 @@ def lib():
         L.qm_level_histogram.restype = C.c_int
         L.qm_quantize_cells.argtypes = [C.c_void_p, _D, _D, _U8, C.c_size_t, _U8, _U8]
         L.qm_quantize_cells.restype = C.c_int
+        L.qm_hm3_predict.argtypes = [C.c_void_p, _U8, _U8, C.c_size_t, C.c_int, _U8]
+        L.qm_hm3_predict.restype = C.c_int
         L.qm_list_crossings.argtypes = [C.c_void_p, _I32, _I32, C.c_size_t, C.c_uint32, _U32, _U32, _D, _U32, _U32]
         L.qm_list_crossings.restype = C.c_int
         L.qm_flight_grid.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_size_t,
@@ -170,6 +172,16 @@ class Context:
                                        abi.ptr(a, C.c_uint8), n, abi.ptr(lc, C.c_uint8), abi.ptr(nc, C.c_uint8)),
                self.handle)
         return lc, nc
+
+    def hm3_predict(self, cells, layers, metric):
+        """HM3 / HMD tile streams before Brotli (qm_hm3_predict): cells [n][512][512] uint8,
+        layers [n], metric 0 (loudness) or 1 (Lden) -> streams [n][6 + 512 * 512]."""
+        c = np.ascontiguousarray(np.asarray(cells, dtype=np.uint8).reshape(-1, abi.HM3_TILE_PX * abi.HM3_TILE_PX))
+        lay = np.ascontiguousarray(np.asarray(layers, dtype=np.uint8).reshape(len(c)))
+        out = np.zeros((len(c), abi.HM3_STREAM_BYTES), np.uint8)
+        _check(lib().qm_hm3_predict(self.handle, abi.ptr(c, C.c_uint8), abi.ptr(lay, C.c_uint8), len(c), int(metric),
+                                    abi.ptr(out, C.c_uint8)), self.handle)
+        return out
 
     def level_histogram(self, levels_db, level_min_db=-30.0, bin_db=0.1, n_bins=1800):
         levels = np.ascontiguousarray(levels_db, dtype=np.float32).ravel()

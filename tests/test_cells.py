@@ -76,3 +76,51 @@ def test_pixels_quantize_per_layer_and_in_total():
         assert [oracle.lden_cell(e) for e in layers[p]] == list(lc[p, :abi.LAYERS])
         assert oracle.lden_cell(sum(layers[p])) == lc[p, abi.LAYERS]
         assert [oracle.nden_cell(s) for s in sone[p]] == list(nc[p])
+
+
+# HM3 / HMD streams before Brotli (paint/src/hm3.rs:68-109).
+
+def _neighbourhood(left, above, corner, cell=100):
+    """A tile whose pixel (1, 1) has the given left, above and upper-left neighbours."""
+    t = np.zeros((512, 512), np.uint8)
+    t[0, 0], t[0, 1], t[1, 0], t[1, 1] = corner, above, left, cell
+    return t
+
+
+@pytest.mark.parametrize("left,above,corner,predicted", [
+    (10, 10, 10, 10),   # all equal: left
+    (5, 15, 10, 10),    # the corner is nearest the estimate
+    (20, 10, 0, 20),    # left nearest
+    (10, 20, 0, 20),    # above nearest
+    (10, 10, 0, 10),    # left and above tie: left
+    (0, 30, 10, 30),    # above and corner tie: above
+])
+def test_paeth_prediction_follows_the_png_tie_order(left, above, corner, predicted):
+    stream = oracle.hm3_predict(_neighbourhood(left, above, corner), 2, 1)
+    assert stream[6 + 512 + 1] == (100 - predicted) % 256
+
+
+def test_streams_start_with_their_header_and_edges_use_zeros():
+    rng = np.random.default_rng(4)
+    tile = rng.integers(0, 256, (512, 512), dtype=np.uint8)
+    nden = oracle.hm3_predict(tile, 6, 0)
+    lden = oracle.hm3_predict(tile, 0, 1)
+    assert bytes(nden[:6]) == b"HM3 \x07\x06" and bytes(lden[:6]) == b"HMD \x01\x00"
+    assert np.array_equal(nden[6:], lden[6:])
+    r = nden[6:].reshape(512, 512)
+    assert r[0, 0] == tile[0, 0]
+    np.testing.assert_array_equal(r[0, 1:], tile[0, 1:] - tile[0, :-1])          # first row: left
+    col = tile[:, 0].astype(np.int16)
+    np.testing.assert_array_equal(r[1:, 0], (col[1:] - col[:-1]).astype(np.uint8))  # first column: above
+    with pytest.raises(ValueError):
+        oracle.hm3_predict(tile, 7, 0)
+
+
+def test_residuals_invert_to_the_cells():
+    rng = np.random.default_rng(5)
+    smooth = np.clip(120 + 40 * np.sin(np.arange(512)[:, None] / 37.0) * np.cos(np.arange(512) / 23.0), 0, 253)
+    tiles = [rng.integers(0, 256, (512, 512), dtype=np.uint8), smooth.astype(np.uint8),
+             np.full((512, 512), abi.CELL_SILENCE, np.uint8)]
+    tiles[1][100:140, 300:380] = abi.CELL_NO_LEVEL
+    for t in tiles:
+        np.testing.assert_array_equal(oracle.hm3_unpredict(oracle.hm3_predict(t, 1, 0)[6:]), t)

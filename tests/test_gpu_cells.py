@@ -71,3 +71,21 @@ def test_errors_name_the_lowest_bad_pixel_and_layer(ctx):
         ctx.quantize_cells(over)
     cells, _ = ctx.quantize_cells(over, assessed=np.zeros(2, np.uint8))
     assert np.all(cells == abi.CELL_NO_LEVEL)
+
+
+def test_hm3_streams_match_the_oracle(ctx):
+    rng = np.random.default_rng(22)
+    y, x = np.mgrid[0:512, 0:512]
+    smooth = np.clip(110 + 50 * np.sin(y / 41.0) * np.cos(x / 29.0) + rng.normal(0, 2, (512, 512)), 0, 253)
+    tiles = np.stack([rng.integers(0, 256, (512, 512)), smooth, np.full((512, 512), 254), (x + 3 * y) % 256,
+                      rng.integers(0, 2, (512, 512)) * 255]).astype(np.uint8)
+    tiles[1, 200:260, 40:90] = 255
+    layers = np.array([0, 3, 6, 5, 1], np.uint8)
+    for metric in (0, 1):
+        got = ctx.hm3_predict(tiles, layers, metric)
+        for k in range(len(tiles)):
+            np.testing.assert_array_equal(got[k], oracle.hm3_predict(tiles[k], layers[k], metric))
+    with pytest.raises(native.QmError, match="unknown layer 7"):
+        ctx.hm3_predict(tiles[:1], np.array([7], np.uint8), 0)
+    with pytest.raises(native.QmError, match="metric"):
+        ctx.hm3_predict(tiles[:1], layers[:1], 2)
