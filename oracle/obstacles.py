@@ -1,0 +1,148 @@
+"""The reference's `obstacles` tile writer (qmobs2), restated in Python — TEST INFRASTRUCTURE ONLY.
+
+It makes the tiles the library's reader is tested on: `edge_cells` follows the supercover cell
+walk of tiles/src/obstacles/cells.rs:13-47 and `encode` the byte layout of
+tiles/src/obstacles.rs:151-276 (header, occupied-cell bitmap and counts, first runs, footprint
+squares, runs, outline records, vertices). Only tests import this module.
+"""
+
+import math
+import struct
+
+MAGIC = b"qmobs2\n\0"
+CELL_STEPS = 256
+CELLS_PER_SIDE = 128
+CELLS = CELLS_PER_SIDE * CELLS_PER_SIDE
+HALF_TILE_CELLS = CELLS_PER_SIDE // 2
+HEADER_BYTES = 32
+CELL_WORDS = CELLS // 64
+CELL_INDEX_BYTES = CELL_WORDS * (8 + 2)
+RUN_BYTES, OUTLINE_BYTES, VERTEX_BYTES = 8, 12, 4
+EXTERIOR, HOLE, WALL = 0, 1, 2
+OUTDOOR, RESIDENTIAL, COMMERCIAL, INDUSTRIAL, HISTORIC, DEFAULT = range(6)
+
+
+def edge_cells(start, end):
+    """The 256-step cells the edge start -> end passes through, 4-connected in walking order; a
+    tie steps the row, and the walk never leaves the box of its end cells (cells.rs:13-47)."""
+    cell = [start[0] // CELL_STEPS, start[1] // CELL_STEPS]
+    last = [end[0] // CELL_STEPS, end[1] // CELL_STEPS]
+    delta = [float(end[0] - start[0]), float(end[1] - start[1])]
+    step = [1 if d >= 0.0 else -1 for d in delta]
+    t_delta = [abs(CELL_STEPS / d) if d != 0.0 else math.inf for d in delta]
+    t_max = []
+    for axis in (0, 1):
+        if delta[axis] == 0.0:
+            t_max.append(math.inf)
+            continue
+        boundary = (cell[axis] + (1 if delta[axis] >= 0.0 else 0)) * CELL_STEPS
+        t_max.append(abs((boundary - start[axis]) / delta[axis]))
+    visited = []
+    while True:
+        visited.append((cell[0], cell[1]))
+        if cell == last:
+            return visited
+        if cell[0] == last[0]:
+            axis = 1
+        elif cell[1] == last[1] or t_max[0] < t_max[1]:
+            axis = 0
+        else:
+            axis = 1
+        t_max[axis] += t_delta[axis]
+        cell[axis] += step[axis]
+
+
+def _height_code(height_m):
+    """Decimetres rounded half away from zero (obstacles.rs:139-146)."""
+    x = height_m * 10.0
+    f = math.floor(x)
+    code = f + 1 if x - f >= 0.5 else f
+    assert 1 <= code <= 0xFFFF, height_m
+    return int(code)
+
+
+def encode(outlines):
+    """The bytes of a tile holding `outlines` (dicts: footprint_id, kind, envelope, height_m,
+    vertices [(x, y) int16, ...]), stored in the given order, which is sorted by footprint id."""
+    cells = [[] for _ in range(CELLS)]
+    for index, outline in enumerate(outlines):
+        vertices = [tuple(v) for v in outline["vertices"]]
+        if outline["kind"] == WALL:
+            assert len(vertices) >= 2
+        else:
+            assert len(vertices) >= 4 and vertices[0] == vertices[-1]
+        assert index == 0 or outlines[index - 1]["footprint_id"] <= outline["footprint_id"]
+        for edge in range(len(vertices) - 1):
+            for column, row in edge_cells(vertices[edge], vertices[edge + 1]):
+                column, row = column + HALF_TILE_CELLS, row + HALF_TILE_CELLS
+                if not (0 <= column < CELLS_PER_SIDE and 0 <= row < CELLS_PER_SIDE):
+                    continue
+                runs = cells[row * CELLS_PER_SIDE + column]
+                if runs and runs[-1][0] == index and runs[-1][1] + runs[-1][2] == edge:
+                    runs[-1][2] += 1
+                else:
+                    runs.append([index, edge, 1])
+    vertex_count = sum(len(o["vertices"]) for o in outlines)
+    run_count = sum(len(runs) for runs in cells)
+    occupied = sum(1 for runs in cells if runs)
+    squares = []
+    for outline in outlines:
+        high = outline["footprint_id"] >> 32
+        if not squares or squares[-1] != high:
+            squares.append(high)
+    assert len(squares) <= 256
+    out = bytearray(MAGIC)
+    for count in (len(outlines), vertex_count, run_count, occupied, len(squares), 0):
+        out += struct.pack("<I", count)
+    words = []
+    for w in range(CELL_WORDS):
+        bits = 0
+        for bit in range(64):
+            if cells[64 * w + bit]:
+                bits |= 1 << bit
+        words.append(bits)
+    for word in words:
+        out += struct.pack("<Q", word)
+    before = 0
+    for word in words:
+        out += struct.pack("<H", before)
+        before += bin(word).count("1")
+    first_run = 0
+    for runs in cells:
+        if runs:
+            out += struct.pack("<I", first_run)
+            first_run += len(runs)
+    out += struct.pack("<I", first_run)
+    for square in squares:
+        out += struct.pack("<I", square)
+    for runs in cells:
+        for outline, first_edge, edge_count in runs:
+            out += struct.pack("<IHH", outline, first_edge, edge_count)
+    first_vertex = 0
+    for outline in outlines:
+        row = squares.index(outline["footprint_id"] >> 32)
+        out += struct.pack("<IIHBB", first_vertex, outline["footprint_id"] & 0xFFFFFFFF,
+                           _height_code(outline["height_m"]), row, outline["kind"] | outline["envelope"] << 2)
+        first_vertex += len(outline["vertices"])
+    for outline in outlines:
+        for x, y in outline["vertices"]:
+            out += struct.pack("<hh", x, y)
+    return bytes(out)
+
+
+def cell_runs(outlines):
+    """Every cell's runs as `encode` lists them: {cell: [(outline, first edge, edge count)]}."""
+    cells = {}
+    for index, outline in enumerate(outlines):
+        vertices = [tuple(v) for v in outline["vertices"]]
+        for edge in range(len(vertices) - 1):
+            for column, row in edge_cells(vertices[edge], vertices[edge + 1]):
+                column, row = column + HALF_TILE_CELLS, row + HALF_TILE_CELLS
+                if not (0 <= column < CELLS_PER_SIDE and 0 <= row < CELLS_PER_SIDE):
+                    continue
+                runs = cells.setdefault(row * CELLS_PER_SIDE + column, [])
+                if runs and runs[-1][0] == index and runs[-1][1] + runs[-1][2] == edge:
+                    runs[-1][2] += 1
+                else:
+                    runs.append([index, edge, 1])
+    return {cell: [tuple(r) for r in runs] for cell, runs in cells.items()}

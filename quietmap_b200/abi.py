@@ -34,6 +34,11 @@ FAILED_LINE_CUTOFF = 8
 FAILED_TIMEOUT = 16
 
 
+class ObstaclesCounts(C.Structure):
+    _fields_ = [(name, C.c_uint32) for name in
+                ("outlines", "vertices", "runs", "occupied_cells", "footprint_squares", "pad_")]
+
+
 class Outline(C.Structure):
     _fields_ = [
         ("first_vertex", C.c_uint32),

@@ -21,6 +21,7 @@
 
 #include "../../include/qm_batch.h"
 #include "../../include/qm_surrogate.h"
+#include "../../include/qm_obstacles.h"
 #include "../../include/qm_tiles.h"
 #include "qm_aircraft.cuh"
 #include "qm_kernels.cuh"
@@ -2490,6 +2491,174 @@ qm_status qm_batch_autotune(qm_scene *scene, const qm_tile_desc *sample, size_t 
                 table->bucket[b] = tile_candidate(k);
             }
         }
+    }
+    return QM_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------------------------
+// `obstacles` tiles (qmobs2; tiles/src/obstacles.rs:1-24 gives the layout, parse.rs:23-128 the
+// checks, whose order and messages these follow).
+
+namespace {
+
+uint16_t le16(const uint8_t *p) { return (uint16_t)(p[0] | (p[1] << 8)); }
+uint32_t le32(const uint8_t *p) {
+    return (uint32_t)p[0] | ((uint32_t)p[1] << 8) | ((uint32_t)p[2] << 16) | ((uint32_t)p[3] << 24);
+}
+uint64_t le64(const uint8_t *p) { return (uint64_t)le32(p) | ((uint64_t)le32(p + 4) << 32); }
+
+// A checked tile: its sections, every index inside them verified.
+struct ObstaclesView {
+    static constexpr size_t HEADER = 32, CELLS = 128 * 128, WORDS = CELLS / 64;
+    static constexpr size_t RUN = 8, OUTLINE = 12, VERTEX = 4, MAX_SQUARES = 256;
+    const uint8_t *words, *before, *first_runs, *squares, *runs, *outlines, *vertices;
+    size_t occupied, n_squares, n_runs, n_outlines, n_vertices;
+
+    uint64_t word(size_t w) const { return le64(words + 8 * w); }
+    size_t first_run(size_t rank) const { return le32(first_runs + 4 * rank); }
+    const uint8_t *outline(size_t i) const { return outlines + OUTLINE * i; }
+    size_t first_vertex(size_t i) const { return le32(outline(i)); }
+    size_t end_vertex(size_t i) const { return i + 1 < n_outlines ? first_vertex(i + 1) : n_vertices; }
+    uint64_t footprint_id(const uint8_t *rec) const {
+        return ((uint64_t)le32(squares + 4 * (size_t)rec[10]) << 32) | le32(rec + 4);
+    }
+    uint32_t vertex(size_t k) const { return le32(vertices + VERTEX * k); }  // both int16, packed
+};
+
+qm_status obstacles_view(const uint8_t *b, size_t n, ObstaclesView &v) {
+    using V = ObstaclesView;
+    auto bad = [](const char *message) { return fail(QM_ERR_ARGUMENT, message); };
+    if (!b && n) return fail(QM_ERR_ARGUMENT, "obstacles: null bytes");
+    if (n < V::HEADER || std::memcmp(b, "qmobs2\n\0", 8) != 0) return bad("obstacles: bad magic");
+    const uint64_t outlines = le32(b + 8), vertices = le32(b + 12), runs = le32(b + 16), occupied = le32(b + 20),
+                   squares = le32(b + 24);
+    if (le32(b + 28) != 0 || occupied > V::CELLS || squares > V::MAX_SQUARES) return bad("obstacles: bad header");
+    const uint64_t lengths[7] = {8 * V::WORDS,   2 * V::WORDS,          4 * (occupied + 1),   4 * squares,
+                                 V::RUN * runs, V::OUTLINE * outlines, V::VERTEX * vertices};
+    uint64_t at[8];
+    at[0] = V::HEADER;
+    for (int k = 0; k < 7; ++k) at[k + 1] = at[k] + lengths[k];
+    if ((uint64_t)n != at[7]) return bad("obstacles: length does not match the counts");
+    v.words = b + at[0];
+    v.before = b + at[1];
+    v.first_runs = b + at[2];
+    v.squares = b + at[3];
+    v.runs = b + at[4];
+    v.outlines = b + at[5];
+    v.vertices = b + at[6];
+    v.occupied = occupied;
+    v.n_squares = squares;
+    v.n_runs = runs;
+    v.n_outlines = outlines;
+    v.n_vertices = vertices;
+    size_t before = 0;
+    for (size_t w = 0; w < V::WORDS; ++w) {
+        if ((size_t)le16(v.before + 2 * w) != before) return bad("obstacles: occupied cells miscounted");
+        before += (size_t)__builtin_popcountll(v.word(w));
+    }
+    bool ordered = before == v.occupied && v.first_run(0) == 0 && v.first_run(v.occupied) == v.n_runs;
+    for (size_t r = 0; ordered && r < v.occupied; ++r) ordered = v.first_run(r + 1) > v.first_run(r);
+    if (!ordered) return bad("obstacles: cell runs out of order");
+    for (size_t r = 1; r < v.n_squares; ++r)
+        if (le32(v.squares + 4 * r) <= le32(v.squares + 4 * r - 4)) return bad("obstacles: footprint squares out of order");
+    if (v.n_outlines > 0 && v.first_vertex(0) != 0) return bad("obstacles: vertices before the first outline");
+    uint64_t previous_id = 0;
+    for (size_t i = 0; i < v.n_outlines; ++i) {
+        const uint8_t *rec = v.outline(i);
+        const int kind = rec[11] & 3, envelope = rec[11] >> 2;
+        if (kind > 2 || envelope > 5) return bad("obstacles: unknown outline kind or envelope");
+        if (le16(rec + 8) == 0 || (size_t)rec[10] >= v.n_squares) return bad("obstacles: zero height or a missing square");
+        const size_t first = v.first_vertex(i), end = v.end_vertex(i);
+        const uint64_t id = v.footprint_id(rec);
+        if (end < first || end > v.n_vertices || id < previous_id) return bad("obstacles: outline out of range or order");
+        const size_t count = end - first;
+        const bool well_formed = kind == 2 ? count >= 2 : count >= 4 && v.vertex(first) == v.vertex(end - 1);
+        if (!well_formed) return bad("obstacles: open ring or short outline");
+        previous_id = id;
+    }
+    for (size_t r = 0; r < v.n_runs; ++r) {
+        const uint8_t *run = v.runs + V::RUN * r;
+        const size_t outline = le32(run), first_edge = le16(run + 4), edge_count = le16(run + 6);
+        if (outline >= v.n_outlines || edge_count == 0 ||
+            first_edge + edge_count >= v.end_vertex(outline) - v.first_vertex(outline))
+            return bad("obstacles: run out of range");
+    }
+    return QM_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+qm_status qm_obstacles_check(const uint8_t *bytes, size_t n_bytes, qm_obstacles_counts *counts) {
+    ObstaclesView v;
+    qm_status st = obstacles_view(bytes, n_bytes, v);
+    if (st != QM_OK) return st;
+    if (counts) {
+        counts->outlines = (uint32_t)v.n_outlines;
+        counts->vertices = (uint32_t)v.n_vertices;
+        counts->runs = (uint32_t)v.n_runs;
+        counts->occupied_cells = (uint32_t)v.occupied;
+        counts->footprint_squares = (uint32_t)v.n_squares;
+        counts->pad_ = 0;
+    }
+    return QM_OK;
+}
+
+qm_status qm_obstacles_outlines(const uint8_t *bytes, size_t n_bytes, int32_t offset_x, int32_t offset_y,
+                                uint32_t first_vertex_base, qm_outline *outlines, int32_t *vertices_xy,
+                                uint8_t *envelope) {
+    ObstaclesView v;
+    qm_status st = obstacles_view(bytes, n_bytes, v);
+    if (st != QM_OK) return st;
+    if ((v.n_outlines && !outlines) || (v.n_vertices && !vertices_xy))
+        return fail(QM_ERR_ARGUMENT, "qm_obstacles_outlines: null outlines or vertices_xy");
+    if ((uint64_t)first_vertex_base + v.n_vertices > UINT32_MAX)
+        return fail(QM_ERR_ARGUMENT, "qm_obstacles_outlines: vertex indices beyond 2^32");
+    for (size_t k = 0; k < v.n_vertices; ++k) {
+        const uint8_t *p = v.vertices + ObstaclesView::VERTEX * k;
+        const int64_t x = (int64_t)(int16_t)le16(p) + offset_x, y = (int64_t)(int16_t)le16(p + 2) + offset_y;
+        if (x < INT32_MIN || x > INT32_MAX || y < INT32_MIN || y > INT32_MAX)
+            return fail(QM_ERR_ARGUMENT, "qm_obstacles_outlines: a vertex leaves the int32 lattice");
+        vertices_xy[2 * k] = (int32_t)x;
+        vertices_xy[2 * k + 1] = (int32_t)y;
+    }
+    for (size_t i = 0; i < v.n_outlines; ++i) {
+        const uint8_t *rec = v.outline(i);
+        qm_outline &o = outlines[i];
+        o.first_vertex = first_vertex_base + (uint32_t)v.first_vertex(i);
+        o.vertex_count = (uint32_t)(v.end_vertex(i) - v.first_vertex(i));
+        o.footprint_id = v.footprint_id(rec);
+        o.height_m = (float)((double)le16(rec + 8) / 10.0);
+        o.building = (rec[11] & 3) != 2 ? 1u : 0u;
+        if (envelope) envelope[i] = rec[11] >> 2;
+    }
+    return QM_OK;
+}
+
+qm_status qm_obstacles_cell_runs(const uint8_t *bytes, size_t n_bytes, uint32_t column, uint32_t row, uint32_t *runs,
+                                 uint32_t cap, uint32_t *count) {
+    ObstaclesView v;
+    qm_status st = obstacles_view(bytes, n_bytes, v);
+    if (st != QM_OK) return st;
+    if (!count || (cap && !runs)) return fail(QM_ERR_ARGUMENT, "qm_obstacles_cell_runs: null count or runs");
+    if (column >= QM_OBSTACLES_CELLS_PER_SIDE || row >= QM_OBSTACLES_CELLS_PER_SIDE)
+        return fail(QM_ERR_ARGUMENT, "qm_obstacles_cell_runs: cell outside the tile");
+    const size_t cell = (size_t)row * QM_OBSTACLES_CELLS_PER_SIDE + column;
+    const uint64_t word = v.word(cell / 64);
+    const unsigned bit = (unsigned)(cell % 64);
+    *count = 0;
+    if (!((word >> bit) & 1)) return QM_OK;
+    const size_t rank = le16(v.before + 2 * (cell / 64)) + (size_t)__builtin_popcountll(word & ((1ull << bit) - 1));
+    const size_t r0 = v.first_run(rank), r1 = v.first_run(rank + 1);
+    *count = (uint32_t)(r1 - r0);
+    for (size_t r = r0; r < r1 && r - r0 < cap; ++r) {
+        const uint8_t *run = v.runs + ObstaclesView::RUN * r;
+        runs[3 * (r - r0)] = le32(run);
+        runs[3 * (r - r0) + 1] = le16(run + 4);
+        runs[3 * (r - r0) + 2] = le16(run + 6);
     }
     return QM_OK;
 }

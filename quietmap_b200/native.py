@@ -62,6 +62,13 @@ def lib():
         L.qm_quantize_cells.restype = C.c_int
         L.qm_hm3_predict.argtypes = [C.c_void_p, _U8, _U8, C.c_size_t, C.c_int, _U8]
         L.qm_hm3_predict.restype = C.c_int
+        L.qm_obstacles_check.argtypes = [_U8, C.c_size_t, C.POINTER(abi.ObstaclesCounts)]
+        L.qm_obstacles_check.restype = C.c_int
+        L.qm_obstacles_outlines.argtypes = [_U8, C.c_size_t, C.c_int32, C.c_int32, C.c_uint32, C.c_void_p,
+                                            _I32, _U8]
+        L.qm_obstacles_outlines.restype = C.c_int
+        L.qm_obstacles_cell_runs.argtypes = [_U8, C.c_size_t, C.c_uint32, C.c_uint32, _U32, C.c_uint32, _U32]
+        L.qm_obstacles_cell_runs.restype = C.c_int
         L.qm_list_crossings.argtypes = [C.c_void_p, _I32, _I32, C.c_size_t, C.c_uint32, _U32, _U32, _D, _U32, _U32]
         L.qm_list_crossings.restype = C.c_int
         L.qm_flight_grid.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_size_t,
@@ -189,6 +196,44 @@ class Context:
         _check(lib().qm_level_histogram(self.handle, abi.ptr(levels, C.c_float), len(levels), level_min_db,
                                         bin_db, n_bins, abi.ptr(counts, C.c_uint32)), self.handle)
         return counts
+
+
+def _tile_bytes(data):
+    b = np.frombuffer(bytes(data), dtype=np.uint8)
+    return b, abi.ptr(b, C.c_uint8) if len(b) else None
+
+
+def obstacles_check(data):
+    """Checks an `obstacles` tile (qmobs2) and returns its header counts (qm_obstacles_check)."""
+    b, p = _tile_bytes(data)
+    counts = abi.ObstaclesCounts()
+    _check(lib().qm_obstacles_check(p, len(b), C.byref(counts)))
+    return {name: getattr(counts, name) for name in
+            ("outlines", "vertices", "runs", "occupied_cells", "footprint_squares")}
+
+
+def obstacles_outlines(data, offset=(0, 0), first_vertex_base=0):
+    """A tile's outlines for a scene (qm_obstacles_outlines): (outlines [OUTLINE_DTYPE], vertices
+    int32 [n][2] = the tile's int16 vertices + offset, envelope class codes uint8)."""
+    counts = obstacles_check(data)
+    b, p = _tile_bytes(data)
+    outlines = np.zeros(counts["outlines"], abi.OUTLINE_DTYPE)
+    vertices = np.zeros((counts["vertices"], 2), np.int32)
+    envelope = np.zeros(counts["outlines"], np.uint8)
+    _check(lib().qm_obstacles_outlines(p, len(b), int(offset[0]), int(offset[1]), first_vertex_base,
+                                       outlines.ctypes.data if len(outlines) else None,
+                                       abi.ptr(vertices, C.c_int32) if len(vertices) else None,
+                                       abi.ptr(envelope, C.c_uint8) if len(envelope) else None))
+    return outlines, vertices, envelope
+
+
+def obstacles_cell_runs(data, column, row, cap=64):
+    """The runs of one cell of a tile: [(outline, first edge, edge count), ...]."""
+    b, p = _tile_bytes(data)
+    runs = np.zeros((cap, 3), np.uint32)
+    count = C.c_uint32()
+    _check(lib().qm_obstacles_cell_runs(p, len(b), column, row, abi.ptr(runs, C.c_uint32), cap, C.byref(count)))
+    return [tuple(int(v) for v in r) for r in runs[:min(count.value, cap)]]
 
 
 class DeviceScene:
