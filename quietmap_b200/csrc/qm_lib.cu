@@ -12,6 +12,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cerrno>
 #include <cstring>
 #include <memory>
 #include <mutex>
@@ -23,6 +24,7 @@
 #include "../../include/qm_surrogate.h"
 #include "../../include/qm_obstacles.h"
 #include "../../include/qm_tiles.h"
+#include "../../include/qm_weather.h"
 #include "qm_aircraft.cuh"
 #include "qm_kernels.cuh"
 #include "qm_mlp.h"
@@ -2660,6 +2662,113 @@ qm_status qm_obstacles_cell_runs(const uint8_t *bytes, size_t n_bytes, uint32_t 
         runs[3 * (r - r0) + 1] = le16(run + 4);
         runs[3 * (r - r0) + 2] = le16(run + 6);
     }
+    return QM_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------------------------
+// The global weather table (qmwthr2; physics/src/weather.rs).
+
+namespace {
+
+constexpr size_t WEATHER_NODE = QM_WEATHER_NODE_BYTES;
+
+bool weather_percentages_valid(const uint8_t *node) {  // weather.rs:168-170
+    for (int k = 0; k < QM_PERIODS * QM_SECTORS; ++k)
+        if (node[k] > 100) return false;
+    return true;
+}
+
+// The four nodes around a place and their bilinear weights, longitude wrapping (weather.rs:172-187).
+void weather_corners(double lat, double lon, size_t index[4], double weight[4]) {
+    const double nodes = 2.0;
+    const double y = std::min(std::max((90.0 - lat) * nodes, 0.0), (double)(QM_WEATHER_ROWS - 1));
+    double wrapped = std::fmod(lon, 360.0);
+    if (wrapped < 0.0) wrapped += 360.0;
+    const double x = wrapped * nodes;
+    const size_t row = std::min((size_t)std::floor(y), (size_t)QM_WEATHER_ROWS - 2), column = (size_t)std::floor(x);
+    const double fy = y - (double)row, fx = x - (double)column;
+    auto at = [](size_t r, size_t c) { return r * QM_WEATHER_COLUMNS + c % QM_WEATHER_COLUMNS; };
+    index[0] = at(row, column);
+    weight[0] = (1.0 - fy) * (1.0 - fx);
+    index[1] = at(row, column + 1);
+    weight[1] = (1.0 - fy) * fx;
+    index[2] = at(row + 1, column);
+    weight[2] = fy * (1.0 - fx);
+    index[3] = at(row + 1, column + 1);
+    weight[3] = fy * fx;
+}
+
+// A place's weather from its four nodes (weather.rs:189-214): each value the weighted sum in
+// corner order, over 100.
+void weather_place_of(const uint8_t *const node[4], const double weight[4], double *favourable, double *alpha) {
+    for (int k = 0; k < QM_PERIODS * QM_SECTORS; ++k) {
+        double sum = 0.0;
+        for (int c = 0; c < 4; ++c) sum += weight[c] * (double)node[c][k];
+        favourable[k] = sum / 100.0;
+    }
+    for (int b = 0; b < QM_BANDS; ++b) {
+        const size_t at = QM_PERIODS * QM_SECTORS + 2 * b;
+        double sum = 0.0;
+        for (int c = 0; c < 4; ++c) sum += weight[c] * (double)le16(node[c] + at);
+        alpha[b] = sum / 100.0;
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+qm_status qm_weather_place(const uint8_t *table, size_t n_bytes, double lat, double lon, double *favourable,
+                           double *alpha_db_per_km) {
+    if (!favourable || !alpha_db_per_km) return fail(QM_ERR_ARGUMENT, "qm_weather_place: null outputs");
+    if (!table || n_bytes != (size_t)QM_WEATHER_TABLE_BYTES || std::memcmp(table, "qmwthr2\n", 8) != 0)
+        return fail(QM_ERR_ARGUMENT, "weather table: bad magic or length");
+    const uint8_t *nodes = table + 8;
+    for (size_t k = 0; k < (size_t)QM_WEATHER_ROWS * QM_WEATHER_COLUMNS; ++k)
+        if (!weather_percentages_valid(nodes + k * WEATHER_NODE))
+            return fail(QM_ERR_ARGUMENT, "weather table: a percentage above 100");
+    if (!std::isfinite(lat) || !std::isfinite(lon)) return fail(QM_ERR_ARGUMENT, "qm_weather_place: lat and lon finite");
+    size_t index[4];
+    double weight[4];
+    weather_corners(lat, lon, index, weight);
+    const uint8_t *node[4];
+    for (int c = 0; c < 4; ++c) node[c] = nodes + index[c] * WEATHER_NODE;
+    weather_place_of(node, weight, favourable, alpha_db_per_km);
+    return QM_OK;
+}
+
+qm_status qm_weather_read_place(const char *path, double lat, double lon, double *favourable,
+                                double *alpha_db_per_km) {
+    if (!path || !favourable || !alpha_db_per_km) return fail(QM_ERR_ARGUMENT, "qm_weather_read_place: null argument");
+    if (!std::isfinite(lat) || !std::isfinite(lon))
+        return fail(QM_ERR_ARGUMENT, "qm_weather_read_place: lat and lon finite");
+    const std::string name(path);
+    std::FILE *f = std::fopen(path, "rb");
+    if (!f) return fail(QM_ERR_ARGUMENT, name + ": " + std::strerror(errno));
+    std::unique_ptr<std::FILE, int (*)(std::FILE *)> hold(f, std::fclose);
+    if (fseeko(f, 0, SEEK_END) != 0) return fail(QM_ERR_ARGUMENT, name + ": " + std::strerror(errno));
+    const off_t length = ftello(f);
+    uint8_t magic[8];
+    auto read_at = [&](void *dst, size_t bytes, off_t at) {
+        return fseeko(f, at, SEEK_SET) == 0 && std::fread(dst, 1, bytes, f) == bytes;
+    };
+    if (length != (off_t)QM_WEATHER_TABLE_BYTES || !read_at(magic, 8, 0) || std::memcmp(magic, "qmwthr2\n", 8) != 0)
+        return fail(QM_ERR_ARGUMENT, name + ": weather table: bad magic or length");
+    size_t index[4];
+    double weight[4];
+    weather_corners(lat, lon, index, weight);
+    uint8_t bytes[4][WEATHER_NODE];
+    const uint8_t *node[4];
+    for (int c = 0; c < 4; ++c) {
+        if (!read_at(bytes[c], WEATHER_NODE, (off_t)(8 + index[c] * WEATHER_NODE)))
+            return fail(QM_ERR_ARGUMENT, name + ": short read");
+        if (!weather_percentages_valid(bytes[c]))
+            return fail(QM_ERR_ARGUMENT, name + ": weather table: a percentage above 100");
+        node[c] = bytes[c];
+    }
+    weather_place_of(node, weight, favourable, alpha_db_per_km);
     return QM_OK;
 }
 

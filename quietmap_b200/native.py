@@ -69,6 +69,10 @@ def lib():
         L.qm_obstacles_outlines.restype = C.c_int
         L.qm_obstacles_cell_runs.argtypes = [_U8, C.c_size_t, C.c_uint32, C.c_uint32, _U32, C.c_uint32, _U32]
         L.qm_obstacles_cell_runs.restype = C.c_int
+        L.qm_weather_place.argtypes = [_U8, C.c_size_t, C.c_double, C.c_double, _D, _D]
+        L.qm_weather_place.restype = C.c_int
+        L.qm_weather_read_place.argtypes = [C.c_char_p, C.c_double, C.c_double, _D, _D]
+        L.qm_weather_read_place.restype = C.c_int
         L.qm_list_crossings.argtypes = [C.c_void_p, _I32, _I32, C.c_size_t, C.c_uint32, _U32, _U32, _D, _U32, _U32]
         L.qm_list_crossings.restype = C.c_int
         L.qm_flight_grid.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_size_t,
@@ -234,6 +238,25 @@ def obstacles_cell_runs(data, column, row, cap=64):
     count = C.c_uint32()
     _check(lib().qm_obstacles_cell_runs(p, len(b), column, row, abi.ptr(runs, C.c_uint32), cap, C.byref(count)))
     return [tuple(int(v) for v in r) for r in runs[:min(count.value, cap)]]
+
+
+def weather_place(table, lat, lon):
+    """The weather of a place from the whole weather table's bytes (qm_weather_place):
+    (favourable [3][16] in [0, 1], alpha_db_per_km [8])."""
+    b, p = _tile_bytes(table)
+    fav = np.zeros((abi.PERIODS, abi.SECTORS))
+    alpha = np.zeros(abi.BANDS)
+    _check(lib().qm_weather_place(p, len(b), lat, lon, abi.ptr(fav, C.c_double), abi.ptr(alpha, C.c_double)))
+    return fav, alpha
+
+
+def weather_read_place(path, lat, lon):
+    """The same from the table's file, reading four nodes (qm_weather_read_place)."""
+    fav = np.zeros((abi.PERIODS, abi.SECTORS))
+    alpha = np.zeros(abi.BANDS)
+    _check(lib().qm_weather_read_place(os.fsencode(path), lat, lon, abi.ptr(fav, C.c_double),
+                                       abi.ptr(alpha, C.c_double)))
+    return fav, alpha
 
 
 class DeviceScene:
