@@ -67,6 +67,8 @@ def lib():
         L.qmo_level_bin.argtypes = [C.c_double, C.c_double, C.c_double, C.c_uint32]
         L.qmo_level_bin.restype = C.c_uint32
         _B = C.POINTER(C.c_uint8)
+        L.qmo_favourable_at.argtypes = [C.POINTER(C.c_float), C.c_double]
+        L.qmo_favourable_at.restype = C.c_double
         L.qmo_nden_cell.argtypes = [C.c_double]
         L.qmo_nden_cell.restype = C.c_uint8
         L.qmo_lden_cell.argtypes = [C.c_double]
@@ -283,6 +285,13 @@ def level_histogram(levels, level_min, bin_db, n_bins):
 
 def level_bin(level, level_min, bin_db, n_bins):
     return lib().qmo_level_bin(level, level_min, bin_db, n_bins)
+
+
+def favourable_at(row, azimuth_rad):
+    """p of a period's 16-sector row (float, as a scene stores it) along an azimuth
+    (physics/src/weather.rs:61-70)."""
+    r = np.ascontiguousarray(np.asarray(row, dtype=np.float32).reshape(16))
+    return lib().qmo_favourable_at(abi.ptr(r, C.c_float), float(azimuth_rad))
 
 
 def nden_cell(sone):

@@ -1766,6 +1766,10 @@ void qmo_level_histogram(const double *levels, size_t n, double level_min, doubl
     for (size_t i = 0; i < n; ++i) counts[level_bin(levels[i], level_min, bin_db, n_bins)]++;
 }
 
+// p of one period's row for sound travelling along azimuth_rad (atan2(north, east)): the scene's
+// favourable row (float) interpolated between sector centres (physics/src/weather.rs:61-70).
+double qmo_favourable_at(const float *row, double azimuth_rad) { return favourable_at(row, azimuth_rad); }
+
 uint32_t qmo_level_bin(double level, double level_min, double bin_db, uint32_t n_bins) {
     return level_bin(level, level_min, bin_db, n_bins);
 }

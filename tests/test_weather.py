@@ -65,3 +65,15 @@ def test_percentages_above_100_are_refused():
     table = encode(percent, alpha)
     with pytest.raises(native.QmError, match="a percentage above 100"):
         native.weather_place(table, 0.0, 0.0)
+
+
+def test_sectors_interpolate_and_wrap_through_north():
+    """physics/src/weather.rs:219-233, on the float row a scene stores (hence 1e-7)."""
+    from oracle import oracle
+    import math
+    row = np.zeros(16, np.float32)
+    row[0], row[15], row[4] = 0.8, 0.4, 0.6
+    north = math.pi / 2
+    assert abs(oracle.favourable_at(row, north) - 0.8) < 1e-7
+    assert abs(oracle.favourable_at(row, 0.0) - 0.6) < 1e-7, "east is sector 4"
+    assert abs(oracle.favourable_at(row, north + math.radians(11.25)) - 0.6) < 1e-7
