@@ -52,6 +52,18 @@ qm_status qm_obstacles_outlines(const uint8_t *bytes, size_t n_bytes, int32_t of
                                 int32_t offset_y, uint32_t first_vertex_base, qm_outline *outlines,
                                 int32_t *vertices_xy, uint8_t *envelope);
 
+/* The outlines of several tiles as one scene's: tile k (bytes[k], n_bytes[k]) with its centre at
+ * offsets_xy[k] in the scene's steps. An outline crossing several tiles is stored whole in each,
+ * with bit-identical global vertices under the same footprint id (tiles/src/obstacles.rs:5-6), so
+ * it is kept once: the first occurrence, tiles in the given order, each tile's outlines in stored
+ * order, of every (footprint id, kind, vertices) it meets. With null outlines and vertices_xy the
+ * call only counts: *n_outlines and *n_vertices get the merged counts. Otherwise they hold the
+ * arrays' capacities on entry (QM_ERR_CAPACITY when short) and the counts written on return;
+ * envelope (nullable) gets the envelope class codes. Every tile is checked first. */
+qm_status qm_obstacles_merge(const uint8_t *const *bytes, const size_t *n_bytes, const int32_t *offsets_xy,
+                             size_t n_tiles, qm_outline *outlines, uint32_t *n_outlines,
+                             int32_t *vertices_xy, uint32_t *n_vertices, uint8_t *envelope);
+
 /* The runs of cell (column, row) of a checked tile (`cell_runs`, parse.rs:190-207): up to cap
  * runs as runs[k][3] = (outline, first edge, edge count); count gets the cell's number of runs
  * (which may exceed cap). */

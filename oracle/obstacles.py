@@ -3,7 +3,8 @@
 It makes the tiles the library's reader is tested on: `edge_cells` follows the supercover cell
 walk of tiles/src/obstacles/cells.rs:13-47 and `encode` the byte layout of
 tiles/src/obstacles.rs:151-276 (header, occupied-cell bitmap and counts, first runs, footprint
-squares, runs, outline records, vertices). Only tests import this module.
+squares, runs, outline records, vertices); `tiles_crossed` names the tiles that store an outline
+(cells.rs:49-75). Only tests import this module.
 """
 
 import math
@@ -146,3 +147,26 @@ def cell_runs(outlines):
                 else:
                     runs.append([index, edge, 1])
     return {cell: [tuple(r) for r in runs] for cell, runs in cells.items()}
+
+
+TILES_PER_AXIS = 1 << 12
+STEPS_PER_TILE = CELLS_PER_SIDE * CELL_STEPS  # 32,768
+
+
+def tile_centre(tile):
+    """A z12 tile's centre in global steps (tiles/src/geo.rs:133-138)."""
+    return (tile[0] * STEPS_PER_TILE + STEPS_PER_TILE // 2, tile[1] * STEPS_PER_TILE + STEPS_PER_TILE // 2)
+
+
+def tiles_crossed(vertices):
+    """The tiles (x, y) whose cells an outline's edges (global steps) pass through, sorted: every
+    tile that stores it (tiles/src/obstacles/cells.rs:49-75; rows beyond the poles have no tiles,
+    columns wrap at the antimeridian)."""
+    tiles = set()
+    for a, b in zip(vertices[:-1], vertices[1:]):
+        for column, row in edge_cells(a, b):
+            y = row // CELLS_PER_SIDE
+            if not 0 <= y < TILES_PER_AXIS:
+                continue
+            tiles.add(((column // CELLS_PER_SIDE) % TILES_PER_AXIS, y))
+    return sorted(tiles)

@@ -18,6 +18,7 @@
 #include <mutex>
 #include <random>
 #include <string>
+#include <unordered_map>
 #include <vector>
 
 #include "../../include/qm_batch.h"
@@ -2636,6 +2637,85 @@ qm_status qm_obstacles_outlines(const uint8_t *bytes, size_t n_bytes, int32_t of
         o.height_m = (float)((double)le16(rec + 8) / 10.0);
         o.building = (rec[11] & 3) != 2 ? 1u : 0u;
         if (envelope) envelope[i] = rec[11] >> 2;
+    }
+    return QM_OK;
+}
+
+qm_status qm_obstacles_merge(const uint8_t *const *bytes, const size_t *n_bytes, const int32_t *offsets_xy,
+                             size_t n_tiles, qm_outline *outlines, uint32_t *n_outlines, int32_t *vertices_xy,
+                             uint32_t *n_vertices, uint8_t *envelope) {
+    if (!n_outlines || !n_vertices) return fail(QM_ERR_ARGUMENT, "qm_obstacles_merge: null n_outlines or n_vertices");
+    if (n_tiles && (!bytes || !n_bytes || !offsets_xy))
+        return fail(QM_ERR_ARGUMENT, "qm_obstacles_merge: null bytes, n_bytes or offsets_xy");
+    const bool counting = !outlines && !vertices_xy;
+    if (!counting && (!outlines || !vertices_xy))
+        return fail(QM_ERR_ARGUMENT, "qm_obstacles_merge: outlines and vertices_xy are given together");
+    struct Kept {
+        uint64_t id;
+        uint32_t first, count;
+        uint16_t height_dm;
+        uint8_t kind, envelope;
+    };
+    std::vector<Kept> kept;
+    std::vector<int32_t> xy;  // the kept outlines' global vertices
+    std::unordered_map<uint64_t, std::vector<uint32_t>> by_key;
+    std::vector<int32_t> g;
+    for (size_t t = 0; t < n_tiles; ++t) {
+        ObstaclesView v;
+        qm_status st = obstacles_view(bytes[t], n_bytes[t], v);
+        if (st != QM_OK) return fail(st, "qm_obstacles_merge: tile " + std::to_string(t) + ": " + g_last_error);
+        for (size_t i = 0; i < v.n_outlines; ++i) {
+            const uint8_t *rec = v.outline(i);
+            const size_t first = v.first_vertex(i), count = v.end_vertex(i) - first;
+            g.resize(2 * count);
+            uint64_t key = v.footprint_id(rec) * 0x9E3779B97F4A7C15ull ^ (uint64_t)(rec[11] & 3) ^ ((uint64_t)count << 40);
+            for (size_t k = 0; k < count; ++k) {
+                const uint8_t *p = v.vertices + ObstaclesView::VERTEX * (first + k);
+                const int64_t x = (int64_t)(int16_t)le16(p) + offsets_xy[2 * t];
+                const int64_t y = (int64_t)(int16_t)le16(p + 2) + offsets_xy[2 * t + 1];
+                if (x < INT32_MIN || x > INT32_MAX || y < INT32_MIN || y > INT32_MAX)
+                    return fail(QM_ERR_ARGUMENT, "qm_obstacles_merge: a vertex leaves the int32 lattice");
+                g[2 * k] = (int32_t)x;
+                g[2 * k + 1] = (int32_t)y;
+                key = (key ^ (uint32_t)x) * 0x100000001B3ull;
+                key = (key ^ (uint32_t)y) * 0x100000001B3ull;
+            }
+            const uint64_t id = v.footprint_id(rec);
+            const uint8_t kind = rec[11] & 3;
+            bool duplicate = false;
+            auto &bucket = by_key[key];
+            for (uint32_t j : bucket) {
+                const Kept &o = kept[j];
+                if (o.id == id && o.kind == kind && o.count == count &&
+                    std::equal(g.begin(), g.end(), xy.begin() + 2 * (size_t)o.first)) {
+                    duplicate = true;
+                    break;
+                }
+            }
+            if (duplicate) continue;
+            if (xy.size() / 2 + count > UINT32_MAX) return fail(QM_ERR_CAPACITY, "qm_obstacles_merge: more than 2^32 vertices");
+            bucket.push_back((uint32_t)kept.size());
+            kept.push_back(Kept{id, (uint32_t)(xy.size() / 2), (uint32_t)count, le16(rec + 8), kind, (uint8_t)(rec[11] >> 2)});
+            xy.insert(xy.end(), g.begin(), g.end());
+        }
+    }
+    const uint32_t cap_outlines = *n_outlines, cap_vertices = *n_vertices;
+    *n_outlines = (uint32_t)kept.size();
+    *n_vertices = (uint32_t)(xy.size() / 2);
+    if (counting) return QM_OK;
+    if (kept.size() > cap_outlines || xy.size() / 2 > cap_vertices)
+        return fail(QM_ERR_CAPACITY, "qm_obstacles_merge: outlines or vertices_xy too short (" +
+                                         std::to_string(kept.size()) + " outlines, " + std::to_string(xy.size() / 2) +
+                                         " vertices)");
+    std::copy(xy.begin(), xy.end(), vertices_xy);
+    for (size_t j = 0; j < kept.size(); ++j) {
+        qm_outline &o = outlines[j];
+        o.first_vertex = kept[j].first;
+        o.vertex_count = kept[j].count;
+        o.footprint_id = kept[j].id;
+        o.height_m = (float)((double)kept[j].height_dm / 10.0);
+        o.building = kept[j].kind != 2 ? 1u : 0u;
+        if (envelope) envelope[j] = kept[j].envelope;
     }
     return QM_OK;
 }

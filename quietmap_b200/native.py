@@ -67,6 +67,9 @@ def lib():
         L.qm_obstacles_outlines.argtypes = [_U8, C.c_size_t, C.c_int32, C.c_int32, C.c_uint32, C.c_void_p,
                                             _I32, _U8]
         L.qm_obstacles_outlines.restype = C.c_int
+        L.qm_obstacles_merge.argtypes = [C.POINTER(C.c_void_p), C.POINTER(C.c_size_t), _I32, C.c_size_t, C.c_void_p,
+                                         _U32, _I32, _U32, _U8]
+        L.qm_obstacles_merge.restype = C.c_int
         L.qm_obstacles_cell_runs.argtypes = [_U8, C.c_size_t, C.c_uint32, C.c_uint32, _U32, C.c_uint32, _U32]
         L.qm_obstacles_cell_runs.restype = C.c_int
         L.qm_weather_place.argtypes = [_U8, C.c_size_t, C.c_double, C.c_double, _D, _D]
@@ -229,6 +232,25 @@ def obstacles_outlines(data, offset=(0, 0), first_vertex_base=0):
                                        abi.ptr(vertices, C.c_int32) if len(vertices) else None,
                                        abi.ptr(envelope, C.c_uint8) if len(envelope) else None))
     return outlines, vertices, envelope
+
+
+def obstacles_merge(tiles, offsets):
+    """Several tiles' outlines as one scene's (qm_obstacles_merge): each outline once, tiles at
+    `offsets` (their centres in scene steps). Returns (outlines, vertices [n][2], envelope)."""
+    arrays = [np.frombuffer(bytes(t), dtype=np.uint8) for t in tiles]
+    ptrs = (C.c_void_p * len(arrays))(*[a.ctypes.data for a in arrays])
+    sizes = (C.c_size_t * len(arrays))(*[len(a) for a in arrays])
+    off = np.ascontiguousarray(np.asarray(offsets, dtype=np.int32).reshape(len(arrays), 2))
+    n_out, n_vert = C.c_uint32(0), C.c_uint32(0)
+    _check(lib().qm_obstacles_merge(ptrs, sizes, abi.ptr(off, C.c_int32), len(arrays), None, C.byref(n_out), None,
+                                    C.byref(n_vert), None))
+    outlines = np.zeros(n_out.value, abi.OUTLINE_DTYPE)
+    vertices = np.zeros((max(n_vert.value, 1), 2), np.int32)
+    envelope = np.zeros(max(n_out.value, 1), np.uint8)
+    _check(lib().qm_obstacles_merge(ptrs, sizes, abi.ptr(off, C.c_int32), len(arrays),
+                                    outlines.ctypes.data if len(outlines) else None, C.byref(n_out),
+                                    abi.ptr(vertices, C.c_int32), C.byref(n_vert), abi.ptr(envelope, C.c_uint8)))
+    return outlines, vertices[:n_vert.value], envelope[:n_out.value]
 
 
 def obstacles_cell_runs(data, column, row, cap=64):

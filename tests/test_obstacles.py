@@ -132,3 +132,48 @@ def test_a_crowded_tile_reads_back_whole():
     for cell in range(0, ob.CELLS, 7):
         got = native.obstacles_cell_runs(data, cell % 128, cell // 128, cap=512)
         assert got == expected.get(cell, []), cell
+
+
+def test_an_outline_is_listed_in_every_tile_whose_cells_it_crosses():
+    """tiles/src/obstacles/tests.rs:103-134."""
+    centre = ob.tile_centre((2212, 1387))
+    east_edge = (centre[0] + 16_383, centre[1])
+    assert ob.tiles_crossed([east_edge, (east_edge[0] + 2, east_edge[1])]) == [(2212, 1387), (2213, 1387)]
+    assert ob.tiles_crossed([(-10, 5_000), (10, 5_000)]) == [(0, 0), (ob.TILES_PER_AXIS - 1, 0)]
+    assert ob.tiles_crossed([(0, -600), (0, -300)]) == []
+
+
+def test_tiles_merge_into_one_scene_keeping_each_outline_once():
+    rng = np.random.default_rng(12)
+    block = [(10, 10), (11, 10), (10, 11), (11, 11)]
+    corner = ob.tile_centre((11, 11))
+    corner = (corner[0] - ob.STEPS_PER_TILE // 2, corner[1] - ob.STEPS_PER_TILE // 2)  # shared by the four
+    world = []
+    for k in range(120):
+        cx, cy = (int(v) for v in corner + rng.integers(-9_000, 9_000, 2))
+        w, h = (int(v) for v in rng.integers(100, 3_000, 2))
+        kind = ob.WALL if k % 9 == 0 else ob.EXTERIOR
+        verts = ([(cx, cy), (cx + w, cy + h)] if kind == ob.WALL else
+                 [(cx, cy), (cx + w, cy), (cx + w, cy + h), (cx, cy + h), (cx, cy)])
+        world.append(dict(footprint_id=(0x0300 << 32) | k, kind=kind, envelope=ob.OUTDOOR if kind == ob.WALL else
+                          ob.COMMERCIAL, height_m=12.5, vertices=verts))
+    files, offsets, stored = [], [], 0
+    origin = ob.tile_centre(block[0])
+    origin = (origin[0] - ob.STEPS_PER_TILE // 2, origin[1] - ob.STEPS_PER_TILE // 2)  # the scene's (0, 0)
+    for tile in block:
+        cx, cy = ob.tile_centre(tile)
+        mine = [dict(o, vertices=[(x - cx, y - cy) for x, y in o["vertices"]])
+                for o in world if tile in ob.tiles_crossed(o["vertices"])]
+        stored += len(mine)
+        files.append(ob.encode(mine))
+        offsets.append((cx - origin[0], cy - origin[1]))
+    assert stored > len(world)  # some outlines are stored in several tiles
+    outlines, vertices, envelope = native.obstacles_merge(files, offsets)
+    got = {int(o["footprint_id"]): [tuple(p) for p in vertices[o["first_vertex"]:o["first_vertex"] + o["vertex_count"]]]
+           for o in outlines}
+    assert len(outlines) == len(world) == len(got)
+    for o in world:
+        assert got[o["footprint_id"]] == [(x - origin[0], y - origin[1]) for x, y in o["vertices"]]
+    assert set(int(e) for e in envelope) == {ob.OUTDOOR, ob.COMMERCIAL}
+    with pytest.raises(native.QmError, match="tile 1: obstacles: bad magic"):
+        native.obstacles_merge([files[0], b"x" * 40], offsets[:2])
