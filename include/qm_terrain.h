@@ -1,0 +1,45 @@
+/*
+ * qm_terrain.h — decoding the reference's `terrain` tiles ("qmterr2").
+ *
+ * A tile (tiles/src/terrain.rs:1-30, 180-214) is the one-arc-second node window of a z12 tile —
+ * rows from north_node southwards, columns from west_node eastwards, latitude = node / 3600
+ * degrees — as a 24-byte header and one zstd frame of five planes: the height residual's low and
+ * high bytes (zigzag-coded, after a planar prediction from the west, north and north-west nodes in
+ * the u16 ring), imperviousness (%), forest cover (%) and canopy height (m). Heights are codes:
+ * metres = -500 + code / 5, 65535 missing. Host only; zstd comes from the system's libzstd.so.1,
+ * loaded on first use (QM_ERR_UNSUPPORTED without it).
+ *
+ * Errors are QM_ERR_ARGUMENT with the reference's messages ("terrain: bad magic", "terrain: a
+ * window no tile has", "terrain: the frame does not decode", "terrain: the frame does not match
+ * the window"); `qm_last_error(NULL)` returns them.
+ */
+#ifndef QM_TERRAIN_H
+#define QM_TERRAIN_H
+
+#include "qm_batch.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define QM_TERRAIN_HEIGHT_MISSING 65535
+#define QM_TERRAIN_MAX_WINDOW_NODES 1024
+
+typedef struct {
+    int32_t north_node;  /* global node index of row 0 (latitude north_node / 3600) */
+    int32_t west_node;   /* global node index of column 0 (longitude west_node / 3600) */
+    uint32_t rows, columns;
+} qm_terrain_window;
+
+/* `Terrain::parse` (tiles/src/terrain.rs:232-272): the window, then, when height_codes is given,
+ * every node row-major: height_codes[rows * columns] and, each nullable, impervious, forest and
+ * canopy (one byte a node). With height_codes null only the header is read. */
+qm_status qm_terrain_decode(const uint8_t *bytes, size_t n_bytes, qm_terrain_window *window,
+                            uint16_t *height_codes, uint8_t *impervious, uint8_t *forest,
+                            uint8_t *canopy);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* QM_TERRAIN_H */

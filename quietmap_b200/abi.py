@@ -34,6 +34,10 @@ FAILED_LINE_CUTOFF = 8
 FAILED_TIMEOUT = 16
 
 
+class TerrainWindow(C.Structure):
+    _fields_ = [("north_node", C.c_int32), ("west_node", C.c_int32), ("rows", C.c_uint32), ("columns", C.c_uint32)]
+
+
 class ObstaclesCounts(C.Structure):
     _fields_ = [(name, C.c_uint32) for name in
                 ("outlines", "vertices", "runs", "occupied_cells", "footprint_squares", "pad_")]

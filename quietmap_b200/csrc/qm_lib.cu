@@ -13,6 +13,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cerrno>
+#include <dlfcn.h>
 #include <cstring>
 #include <memory>
 #include <mutex>
@@ -23,6 +24,7 @@
 
 #include "../../include/qm_batch.h"
 #include "../../include/qm_surrogate.h"
+#include "../../include/qm_terrain.h"
 #include "../../include/qm_obstacles.h"
 #include "../../include/qm_tiles.h"
 #include "../../include/qm_weather.h"
@@ -2849,6 +2851,81 @@ qm_status qm_weather_read_place(const char *path, double lat, double lon, double
         node[c] = bytes[c];
     }
     weather_place_of(node, weight, favourable, alpha_db_per_km);
+    return QM_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------------------------
+// `terrain` tiles (qmterr2; tiles/src/terrain.rs).
+
+namespace {
+
+// The two functions of zstd's public C API the decoder needs, from the system's libzstd.
+struct Zstd {
+    size_t (*decompress)(void *dst, size_t capacity, const void *src, size_t size) = nullptr;
+    unsigned (*is_error)(size_t code) = nullptr;
+    bool loaded() const { return decompress && is_error; }
+};
+
+const Zstd &zstd() {
+    static const Zstd z = [] {
+        Zstd out;
+        void *h = dlopen("libzstd.so.1", RTLD_NOW | RTLD_LOCAL);
+        if (!h) return out;
+        out.decompress = reinterpret_cast<size_t (*)(void *, size_t, const void *, size_t)>(dlsym(h, "ZSTD_decompress"));
+        out.is_error = reinterpret_cast<unsigned (*)(size_t)>(dlsym(h, "ZSTD_isError"));
+        return out;
+    }();
+    return z;
+}
+
+}  // namespace
+
+extern "C" {
+
+qm_status qm_terrain_decode(const uint8_t *bytes, size_t n_bytes, qm_terrain_window *window, uint16_t *height_codes,
+                            uint8_t *impervious, uint8_t *forest, uint8_t *canopy) {
+    constexpr size_t HEADER = 24, PLANES = 5;
+    if (!window) return fail(QM_ERR_ARGUMENT, "qm_terrain_decode: null window");
+    if (!bytes || n_bytes < HEADER || std::memcmp(bytes, "qmterr2\n", 8) != 0)
+        return fail(QM_ERR_ARGUMENT, "terrain: bad magic");
+    qm_terrain_window w;
+    w.north_node = (int32_t)le32(bytes + 8);
+    w.west_node = (int32_t)le32(bytes + 12);
+    w.rows = le32(bytes + 16);
+    w.columns = le32(bytes + 20);
+    if (w.rows < 1 || w.rows > QM_TERRAIN_MAX_WINDOW_NODES || w.columns < 1 || w.columns > QM_TERRAIN_MAX_WINDOW_NODES)
+        return fail(QM_ERR_ARGUMENT, "terrain: a window no tile has");
+    *window = w;
+    if (!height_codes) return QM_OK;
+    const Zstd &z = zstd();
+    if (!z.loaded()) return fail(QM_ERR_UNSUPPORTED, "qm_terrain_decode: libzstd.so.1 is not available");
+    const size_t n = (size_t)w.rows * w.columns, columns = w.columns;
+    std::vector<uint8_t> planes(PLANES * n);
+    const size_t got = z.decompress(planes.data(), planes.size(), bytes + HEADER, n_bytes - HEADER);
+    if (z.is_error(got)) return fail(QM_ERR_ARGUMENT, "terrain: the frame does not decode");
+    if (got != PLANES * n) return fail(QM_ERR_ARGUMENT, "terrain: the frame does not match the window");
+    // The planar prediction undone row by row (terrain.rs:157-180): code = residual + west + north
+    // - north-west in the u16 ring, the residual zigzag-decoded from its two byte planes.
+    const uint8_t *low = planes.data(), *high = low + n;
+    std::vector<uint16_t> north_row(columns, 0);
+    for (size_t r = 0; r < w.rows; ++r) {
+        uint16_t west = 0, north_west = 0;
+        for (size_t c = 0; c < columns; ++c) {
+            const size_t at = r * columns + c;
+            const uint16_t zigzag = (uint16_t)(low[at] | (high[at] << 8));
+            const uint16_t residual = (uint16_t)((uint16_t)(zigzag >> 1) ^ (uint16_t)(-(int)(zigzag & 1)));
+            const uint16_t code = (uint16_t)(residual + (uint16_t)(west + north_row[c] - north_west));
+            north_west = north_row[c];
+            north_row[c] = code;
+            west = code;
+            height_codes[at] = code;
+        }
+    }
+    if (impervious) std::memcpy(impervious, planes.data() + 2 * n, n);
+    if (forest) std::memcpy(forest, planes.data() + 3 * n, n);
+    if (canopy) std::memcpy(canopy, planes.data() + 4 * n, n);
     return QM_OK;
 }
 

@@ -72,6 +72,9 @@ def lib():
         L.qm_obstacles_merge.restype = C.c_int
         L.qm_obstacles_cell_runs.argtypes = [_U8, C.c_size_t, C.c_uint32, C.c_uint32, _U32, C.c_uint32, _U32]
         L.qm_obstacles_cell_runs.restype = C.c_int
+        L.qm_terrain_decode.argtypes = [_U8, C.c_size_t, C.POINTER(abi.TerrainWindow), C.POINTER(C.c_uint16), _U8,
+                                        _U8, _U8]
+        L.qm_terrain_decode.restype = C.c_int
         L.qm_weather_place.argtypes = [_U8, C.c_size_t, C.c_double, C.c_double, _D, _D]
         L.qm_weather_place.restype = C.c_int
         L.qm_weather_read_place.argtypes = [C.c_char_p, C.c_double, C.c_double, _D, _D]
@@ -260,6 +263,21 @@ def obstacles_cell_runs(data, column, row, cap=64):
     count = C.c_uint32()
     _check(lib().qm_obstacles_cell_runs(p, len(b), column, row, abi.ptr(runs, C.c_uint32), cap, C.byref(count)))
     return [tuple(int(v) for v in r) for r in runs[:min(count.value, cap)]]
+
+
+def terrain_decode(data):
+    """A terrain tile's window and nodes (qm_terrain_decode): (window dict, height codes uint16
+    [rows][columns], impervious, forest and canopy uint8 [rows][columns])."""
+    b, p = _tile_bytes(data)
+    w = abi.TerrainWindow()
+    _check(lib().qm_terrain_decode(p, len(b), C.byref(w), None, None, None, None))
+    shape = (w.rows, w.columns)
+    heights = np.zeros(shape, np.uint16)
+    imp, forest, canopy = (np.zeros(shape, np.uint8) for _ in range(3))
+    _check(lib().qm_terrain_decode(p, len(b), C.byref(w), heights.ctypes.data_as(C.POINTER(C.c_uint16)),
+                                   abi.ptr(imp, C.c_uint8), abi.ptr(forest, C.c_uint8), abi.ptr(canopy, C.c_uint8)))
+    window = dict(north_node=w.north_node, west_node=w.west_node, rows=w.rows, columns=w.columns)
+    return window, heights, imp, forest, canopy
 
 
 def weather_place(table, lat, lon):

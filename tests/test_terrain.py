@@ -1,0 +1,70 @@
+"""`terrain` tiles (qmterr2): the library's decoder against tiles the oracle writes, pinned to the
+reference's own decode test (tiles/src/terrain.rs:438-473). Host only."""
+
+import numpy as np
+import pytest
+
+from oracle import terrain as ot
+from quietmap_b200 import native
+
+
+def _xorshift(seed):
+    mask = (1 << 64) - 1
+    while True:
+        seed ^= (seed << 13) & mask
+        seed ^= seed >> 7
+        seed ^= (seed << 17) & mask
+        yield seed
+
+
+def _reference_nodes(rows, columns):
+    """The reference test's nodes: random heights (steep jumps, the missing code and the u16
+    ends wrap the prediction), percents and canopies, from its own generator and seed."""
+    draw = _xorshift(0x9E37_79B9_7F4A_7C15)
+    heights = np.zeros(rows * columns, np.uint16)
+    imp, forest, canopy = (np.zeros(rows * columns, np.uint8) for _ in range(3))
+    for at in range(rows * columns):
+        kind = next(draw) % 7
+        if kind == 0:
+            heights[at] = ot.HEIGHT_MISSING
+        elif kind == 1:
+            heights[at] = 0
+        elif kind == 2:
+            heights[at] = next(draw) % 65_536
+        else:
+            heights[at] = (2_500 + (at % 65_536 % 53) * 3 + next(draw) % 5) & 0xFFFF
+        imp[at] = next(draw) % 101
+        forest[at] = next(draw) % 102
+        canopy[at] = next(draw) % 61
+    shape = (rows, columns)
+    return heights.reshape(shape), imp.reshape(shape), forest.reshape(shape), canopy.reshape(shape)
+
+
+def test_a_tile_decodes_to_the_nodes_it_was_encoded_from():
+    heights, imp, forest, canopy = _reference_nodes(37, 53)
+    data = ot.encode(181_042, 50_625, heights, imp, forest, canopy)
+    window, h, i, f, c = native.terrain_decode(data)
+    assert window == dict(north_node=181_042, west_node=50_625, rows=37, columns=53)
+    np.testing.assert_array_equal(h, heights)
+    np.testing.assert_array_equal(i, imp)
+    np.testing.assert_array_equal(f, forest)
+    np.testing.assert_array_equal(c, canopy)
+
+
+def test_broken_tiles_are_refused():
+    heights, imp, forest, canopy = _reference_nodes(4, 5)
+    data = ot.encode(180_001, 50_000, heights, imp, forest, canopy)
+    native.terrain_decode(data)
+    with pytest.raises(native.QmError, match="does not decode"):
+        native.terrain_decode(data[:-1])
+    with pytest.raises(native.QmError, match="bad magic"):
+        native.terrain_decode(b"qmterr1\n" + data[8:])
+    for rows, columns in ((0, 5), (4, 1025)):
+        bad = bytearray(data)
+        bad[16:20] = rows.to_bytes(4, "little")
+        bad[20:24] = columns.to_bytes(4, "little")
+        with pytest.raises(native.QmError, match="a window no tile has"):
+            native.terrain_decode(bytes(bad))
+    short = data[:24] + ot.compress(ot.planes(heights, imp, forest, canopy)[:-5])
+    with pytest.raises(native.QmError, match="does not match the window"):
+        native.terrain_decode(short)
