@@ -49,6 +49,9 @@ struct qm_ctx {
     int sm_count;
     cudaStream_t stream;
     std::mutex lock;
+    // Scenes and networks made on the context hold it: qm_close releases it once they are freed.
+    int children = 0;
+    bool closed = false;
 };
 
 struct DeviceBuffer {
@@ -79,6 +82,9 @@ struct qm_scene {
     std::vector<uint32_t> source_layer;
     bool any_favourable;
     size_t n_edges_listed;
+    // Batch plans made on the scene hold it: qm_scene_free releases it once they are freed.
+    int plans = 0;
+    bool freed = false;
     ~qm_scene() {
         for (auto *b : buffers) delete b;
     }
@@ -89,6 +95,22 @@ namespace {
 qm_status fail(qm_status status, const std::string &message) {
     g_last_error = message;
     return status;
+}
+
+void ctx_destroy(qm_ctx *ctx) {
+    cudaSetDevice(ctx->device);
+    cudaStreamDestroy(ctx->stream);
+    delete ctx;
+}
+
+// One holder of the context gone: the context goes too once it is closed and holds nothing.
+void ctx_release(qm_ctx *ctx) {
+    bool last;
+    {
+        std::lock_guard<std::mutex> guard(ctx->lock);
+        last = --ctx->children == 0 && ctx->closed;
+    }
+    if (last) ctx_destroy(ctx);
 }
 
 #define QM_CUDA(call)                                                                  \
@@ -247,9 +269,13 @@ qm_status qm_open(int device_ordinal, qm_ctx **out) {
 
 void qm_close(qm_ctx *ctx) {
     if (!ctx) return;
-    cudaSetDevice(ctx->device);
-    cudaStreamDestroy(ctx->stream);
-    delete ctx;
+    bool now;
+    {
+        std::lock_guard<std::mutex> guard(ctx->lock);
+        ctx->closed = true;
+        now = ctx->children == 0;
+    }
+    if (now) ctx_destroy(ctx);
 }
 
 qm_status qm_scene_upload(qm_ctx *ctx, const qm_scene_desc *d, qm_scene **out) {
@@ -411,14 +437,27 @@ qm_status qm_scene_upload(qm_ctx *ctx, const qm_scene_desc *d, qm_scene **out) {
     std::memcpy(dv.fav, d->favourable, sizeof(dv.fav));
     std::memcpy(dv.alpha, d->alpha_db_per_km, sizeof(dv.alpha));
     for (int b = 0; b < 8; ++b) dv.air_per_m[b] = (float)((double)d->alpha_db_per_km[b] * (2.302585092994046 / 10.0 / 1000.0));
+    {
+        std::lock_guard<std::mutex> guard(ctx->lock);
+        ++ctx->children;
+    }
     *out = s;
     return QM_OK;
 }
 
 void qm_scene_free(qm_scene *scene) {
     if (!scene) return;
-    cudaSetDevice(scene->ctx->device);
+    qm_ctx *ctx = scene->ctx;
+    bool now;
+    {
+        std::lock_guard<std::mutex> guard(ctx->lock);
+        scene->freed = true;
+        now = scene->plans == 0;
+    }
+    if (!now) return;  // its last plan's qm_batch_plan_free deletes it
+    cudaSetDevice(ctx->device);
     delete scene;
+    ctx_release(ctx);
 }
 
 }  // extern "C"
@@ -1590,15 +1629,20 @@ qm_status qm_surrogate_create(qm_ctx *ctx, const float *params, qm_surrogate **o
         delete s;
         return fail(QM_ERR_CUDA, std::string("cuda: ") + cudaGetErrorString(e));
     }
+    ++ctx->children;
     *out = s;
     return QM_OK;
 }
 
 void qm_surrogate_free(qm_surrogate *net) {
     if (!net) return;
-    std::lock_guard<std::mutex> guard(net->ctx->lock);
-    cudaSetDevice(net->ctx->device);
-    delete net;
+    qm_ctx *ctx = net->ctx;
+    {
+        std::lock_guard<std::mutex> guard(ctx->lock);
+        cudaSetDevice(ctx->device);
+        delete net;
+    }
+    ctx_release(ctx);
 }
 
 qm_status qm_surrogate_set_kernel(qm_surrogate *net, int kernel) {
@@ -2171,9 +2215,18 @@ void qm_tune_default(qm_tune_table *table) {
 
 void qm_batch_plan_free(qm_batch_plan *plan) {
     if (!plan) return;
-    std::lock_guard<std::mutex> guard(plan->scene->ctx->lock);
-    cudaSetDevice(plan->scene->ctx->device);
-    delete plan;
+    qm_scene *scene = plan->scene;
+    qm_ctx *ctx = scene->ctx;
+    bool scene_done;
+    {
+        std::lock_guard<std::mutex> guard(ctx->lock);
+        cudaSetDevice(ctx->device);
+        delete plan;
+        scene_done = --scene->plans == 0 && scene->freed;
+    }
+    if (!scene_done) return;
+    delete scene;  // freed by its owner while this plan still held it
+    ctx_release(ctx);
 }
 
 qm_status qm_batch_plan_create(qm_scene *scene, const qm_tile_desc *tiles, size_t n_tiles, uint64_t n_cells,
@@ -2335,6 +2388,7 @@ qm_status qm_batch_plan_create(qm_scene *scene, const qm_tile_desc *tiles, size_
         P->graph = graph;
         QM_CUDA(cudaGraphInstantiate(&P->exec, P->graph, 0));
     }
+    ++scene->plans;
     *out = hold.release();
     return QM_OK;
 }
