@@ -142,6 +142,8 @@ int qm_abi_version(void);
 /* Opens device `device_ordinal` (an sm_100 GPU). Replaces `Gpu::new`
  * (paint-gpu/src/device.rs:270): kernels are linked in as sm_100a cubins, no NVRTC. */
 qm_status qm_open(int device_ordinal, qm_ctx **out);
+/* Closes a context. Scenes and surrogate networks made on it stay usable: the context is
+ * released when the last of them is freed. */
 void qm_close(qm_ctx *ctx);
 /* The last error of this context's calls on the calling thread ("" if none). */
 const char *qm_last_error(const qm_ctx *ctx);
@@ -149,6 +151,7 @@ const char *qm_last_error(const qm_ctx *ctx);
 /* Uploads a scene: obstacles with their grid cell lists, terrain, sources, weather.
  * Replaces `DeviceSquare::upload` (paint-gpu/src/square_upload.rs:18). */
 qm_status qm_scene_upload(qm_ctx *ctx, const qm_scene_desc *desc, qm_scene **out);
+/* Frees a scene; batch plans made on it stay usable, and it is released with the last of them. */
 void qm_scene_free(qm_scene *scene);
 
 /* Batch::evaluate and Batch::pair_spectra (paint/src/exact.rs:164-170; GPU
