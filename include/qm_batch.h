@@ -229,6 +229,13 @@ qm_status qm_quantize_cells(qm_ctx *ctx, const double *lden_energy, const double
 qm_status qm_hm3_predict(qm_ctx *ctx, const uint8_t *cells, const uint8_t *layers, size_t n_tiles,
                          int metric, uint8_t *streams);
 
+/* The inverse, on the host (`decode_metric_tile` after its Brotli stage, paint/src/hm3.rs:127-169):
+ * a decompressed stream of QM_HM3_STREAM_BYTES whose header must be the metric's and whose layer
+ * byte must be `layer` ("not this layer's HM3 tile" otherwise; "unknown HM3 layer" for a layer
+ * above QM_LAYERS), back to its 512 x 512 cells (cells[512 * 512]). Needs no device. */
+qm_status qm_hm3_unpredict(const uint8_t *stream, size_t n_bytes, uint32_t layer, int metric,
+                           uint8_t *cells);
+
 /* The obstacle crossings of n rays from (from_xy) to (to_xy), lattice steps: per ray its count
  * (counts[n]) and, up to `cap` per ray, the crossed edges (the edge's first vertex index),
  * chainages t (f64) and flags (bit 0 building, bit 1 bounds_roof), sorted and deduplicated as

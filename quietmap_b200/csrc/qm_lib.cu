@@ -941,6 +941,29 @@ qm_status qm_quantize_cells(qm_ctx *ctx, const double *lden_energy, const double
     return QM_OK;
 }
 
+qm_status qm_hm3_unpredict(const uint8_t *stream, size_t n_bytes, uint32_t layer, int metric, uint8_t *cells) {
+    if (layer > QM_LAYERS) return fail(QM_ERR_ARGUMENT, "unknown HM3 layer");
+    if (metric != 0 && metric != 1) return fail(QM_ERR_ARGUMENT, "qm_hm3_unpredict: metric is 0 (loudness) or 1 (Lden)");
+    if (!cells) return fail(QM_ERR_ARGUMENT, "qm_hm3_unpredict: null cells");
+    const uint8_t header[2][5] = {{'H', 'M', '3', ' ', 0x07}, {'H', 'M', 'D', ' ', 0x01}};
+    if (!stream || n_bytes != (size_t)QM_HM3_STREAM_BYTES || std::memcmp(stream, header[metric], 5) != 0 ||
+        stream[5] != layer)
+        return fail(QM_ERR_ARGUMENT, "not this layer's HM3 tile");
+    // In order, each cell is its residual plus the Paeth prediction from the cells already restored
+    // (hm3.rs:165-167): left, above, upper-left, zeros outside the tile, ties to left then above.
+    constexpr size_t P = QM_HM3_TILE_PX;
+    for (size_t at = 0; at < P * P; ++at) {
+        const bool has_left = at % P != 0, has_above = at >= P;
+        const int left = has_left ? cells[at - 1] : 0, above = has_above ? cells[at - P] : 0;
+        const int corner = has_left && has_above ? cells[at - P - 1] : 0;
+        const int estimate = left + above - corner;
+        const int dl = std::abs(estimate - left), da = std::abs(estimate - above), dc = std::abs(estimate - corner);
+        const int predicted = (dl <= da && dl <= dc) ? left : (da <= dc ? above : corner);
+        cells[at] = (uint8_t)(stream[6 + at] + predicted);
+    }
+    return QM_OK;
+}
+
 qm_status qm_hm3_predict(qm_ctx *ctx, const uint8_t *cells, const uint8_t *layers, size_t n_tiles, int metric,
                          uint8_t *streams) {
     if (!ctx) return fail(QM_ERR_ARGUMENT, "qm_hm3_predict: null ctx");

@@ -62,6 +62,8 @@ def lib():
         L.qm_quantize_cells.restype = C.c_int
         L.qm_hm3_predict.argtypes = [C.c_void_p, _U8, _U8, C.c_size_t, C.c_int, _U8]
         L.qm_hm3_predict.restype = C.c_int
+        L.qm_hm3_unpredict.argtypes = [_U8, C.c_size_t, C.c_uint32, C.c_int, _U8]
+        L.qm_hm3_unpredict.restype = C.c_int
         L.qm_obstacles_check.argtypes = [_U8, C.c_size_t, C.POINTER(abi.ObstaclesCounts)]
         L.qm_obstacles_check.restype = C.c_int
         L.qm_obstacles_outlines.argtypes = [_U8, C.c_size_t, C.c_int32, C.c_int32, C.c_uint32, C.c_void_p,
@@ -211,6 +213,14 @@ class Context:
 def _tile_bytes(data):
     b = np.frombuffer(bytes(data), dtype=np.uint8)
     return b, abi.ptr(b, C.c_uint8) if len(b) else None
+
+
+def hm3_unpredict(stream, layer, metric):
+    """A decompressed HM3 / HMD stream back to its 512 x 512 cells (qm_hm3_unpredict), host only."""
+    b, p = _tile_bytes(stream)
+    cells = np.zeros((abi.HM3_TILE_PX, abi.HM3_TILE_PX), np.uint8)
+    _check(lib().qm_hm3_unpredict(p, len(b), layer, metric, abi.ptr(cells, C.c_uint8)))
+    return cells
 
 
 def obstacles_check(data):

@@ -124,3 +124,21 @@ def test_residuals_invert_to_the_cells():
     tiles[1][100:140, 300:380] = abi.CELL_NO_LEVEL
     for t in tiles:
         np.testing.assert_array_equal(oracle.hm3_unpredict(oracle.hm3_predict(t, 1, 0)[6:]), t)
+
+
+def test_the_library_restores_cells_from_a_stream():
+    from quietmap_b200 import native
+    rng = np.random.default_rng(6)
+    y, x = np.mgrid[0:512, 0:512]
+    tiles = [rng.integers(0, 256, (512, 512), dtype=np.uint8),
+             np.clip(100 + 60 * np.sin(y / 33.0) * np.cos(x / 47.0), 0, 253).astype(np.uint8)]
+    for metric in (0, 1):
+        for t in tiles:
+            stream = oracle.hm3_predict(t, 4, metric)
+            np.testing.assert_array_equal(native.hm3_unpredict(stream, 4, metric), t)
+    stream = oracle.hm3_predict(tiles[0], 4, 0)
+    for layer, metric, data in ((3, 0, stream), (4, 1, stream), (4, 0, stream[:-1])):
+        with pytest.raises(native.QmError, match="not this layer's HM3 tile"):
+            native.hm3_unpredict(data, layer, metric)
+    with pytest.raises(native.QmError, match="unknown HM3 layer"):
+        native.hm3_unpredict(stream, 7, 0)
