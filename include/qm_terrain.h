@@ -38,6 +38,18 @@ qm_status qm_terrain_decode(const uint8_t *bytes, size_t n_bytes, qm_terrain_win
                             uint16_t *height_codes, uint8_t *impervious, uint8_t *forest,
                             uint8_t *canopy);
 
+/* `terrain-fine` tiles ("qmtfin2", tiles/src/terrain_fine.rs:1-11, 70-110): a national model's
+ * detail on the 1/6 arc-second lattice over the `terrain` tile's window (six fine intervals to
+ * each; rows and columns at most 6 * 1023 + 1), in signed 0.2 m codes, stored as a directory of
+ * frame ends and one zstd frame per block of 128 x 128 cells (each block also holds the node row
+ * and column closing its last cells), each the planar residual as in `terrain`. The window,
+ * then, when details is given, every node row-major (`FineTerrain::parse` and `codes`,
+ * terrain_fine.rs:128-172, 266-281): details[rows * columns]. Errors: "terrain-fine: bad magic",
+ * "... a window no tile has", "... the directory is cut", "... a frame outside the tile",
+ * "... a block does not decode". */
+qm_status qm_terrain_fine_decode(const uint8_t *bytes, size_t n_bytes, qm_terrain_window *window,
+                                 int16_t *details);
+
 #ifdef __cplusplus
 }
 #endif

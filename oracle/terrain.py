@@ -70,3 +70,36 @@ def encode(north_node, west_node, heights, impervious, forest, canopy):
     rows, columns = heights.shape
     header = MAGIC + struct.pack("<iiII", north_node, west_node, rows, columns)
     return header + compress(planes(heights, impervious, forest, canopy))
+
+
+FINE_MAGIC = b"qmtfin2\n"
+BLOCK_CELLS = 128
+
+
+def _block_span(block, nodes):
+    """tiles/src/terrain_fine.rs:52-56."""
+    first = block * BLOCK_CELLS
+    return first, min(first + BLOCK_CELLS, nodes - 1)
+
+
+def _blocks_along(nodes):
+    """tiles/src/terrain_fine.rs:47-50."""
+    return max(-(-(nodes - 1) // BLOCK_CELLS), 1)
+
+
+def encode_fine(north_node, west_node, details):
+    """A fine terrain tile (tiles/src/terrain_fine.rs:58-110): header, the directory of each
+    block's frame end, then per block (row-major) one frame of its planar residual's two planes."""
+    rows, columns = details.shape
+    codes = details.astype(np.int16).view(np.uint16)
+    frames, ends = b"", []
+    for br in range(_blocks_along(rows)):
+        r0, r1 = _block_span(br, rows)
+        for bc in range(_blocks_along(columns)):
+            c0, c1 = _block_span(bc, columns)
+            block = codes[r0:r1 + 1, c0:c1 + 1]
+            zero = np.zeros(block.shape, np.uint8)
+            frames += compress(planes(block, zero, zero, zero)[:2 * block.size])
+            ends.append(len(frames))
+    header = FINE_MAGIC + struct.pack("<iiII", north_node, west_node, rows, columns)
+    return header + b"".join(struct.pack("<I", e) for e in ends) + frames

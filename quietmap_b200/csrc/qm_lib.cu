@@ -3006,4 +3006,69 @@ qm_status qm_terrain_decode(const uint8_t *bytes, size_t n_bytes, qm_terrain_win
     return QM_OK;
 }
 
+qm_status qm_terrain_fine_decode(const uint8_t *bytes, size_t n_bytes, qm_terrain_window *window, int16_t *details) {
+    constexpr size_t HEADER = 24;
+    constexpr uint32_t BLOCK = 128, FINE = 6;
+    if (!window) return fail(QM_ERR_ARGUMENT, "qm_terrain_fine_decode: null window");
+    if (!bytes || n_bytes < HEADER || std::memcmp(bytes, "qmtfin2\n", 8) != 0)
+        return fail(QM_ERR_ARGUMENT, "terrain-fine: bad magic");
+    qm_terrain_window w;
+    w.north_node = (int32_t)le32(bytes + 8);
+    w.west_node = (int32_t)le32(bytes + 12);
+    w.rows = le32(bytes + 16);
+    w.columns = le32(bytes + 20);
+    const uint32_t most = (QM_TERRAIN_MAX_WINDOW_NODES - 1) * FINE + 1;
+    if (w.rows < 2 || w.rows > most || w.columns < 2 || w.columns > most)
+        return fail(QM_ERR_ARGUMENT, "terrain-fine: a window no tile has");
+    // Blocks along an axis of `nodes` nodes, and the first and last node block b stores
+    // (terrain_fine.rs:47-56).
+    auto blocks_along = [](uint32_t nodes) { return std::max<uint32_t>((nodes - 1 + BLOCK - 1) / BLOCK, 1); };
+    const uint32_t down = blocks_along(w.rows), across = blocks_along(w.columns);
+    const size_t count = (size_t)down * across, first = HEADER + 4 * count;
+    if (n_bytes < first) return fail(QM_ERR_ARGUMENT, "terrain-fine: the directory is cut");
+    std::vector<std::pair<size_t, size_t>> frames(count);
+    size_t start = first;
+    for (size_t b = 0; b < count; ++b) {
+        const size_t end = first + le32(bytes + HEADER + 4 * b);
+        if (end < start || end > n_bytes) return fail(QM_ERR_ARGUMENT, "terrain-fine: a frame outside the tile");
+        frames[b] = {start, end};
+        start = end;
+    }
+    *window = w;
+    if (!details) return QM_OK;
+    const Zstd &z = zstd();
+    if (!z.loaded()) return fail(QM_ERR_UNSUPPORTED, "qm_terrain_fine_decode: libzstd.so.1 is not available");
+    std::vector<uint8_t> planes;
+    std::vector<uint16_t> north_row;
+    // Blocks in row-major order, so a node two blocks share is the later block's, the block the
+    // reference reads it from (terrain_fine.rs:150-155).
+    for (uint32_t br = 0; br < down; ++br) {
+        const uint32_t r0 = br * BLOCK, r1 = std::min(r0 + BLOCK, w.rows - 1);
+        for (uint32_t bc = 0; bc < across; ++bc) {
+            const uint32_t c0 = bc * BLOCK, c1 = std::min(c0 + BLOCK, w.columns - 1);
+            const size_t rows = r1 - r0 + 1, columns = c1 - c0 + 1, nodes = rows * columns;
+            const auto &f = frames[(size_t)br * across + bc];
+            planes.resize(2 * nodes);
+            const size_t got = z.decompress(planes.data(), planes.size(), bytes + f.first, f.second - f.first);
+            if (z.is_error(got) || got != 2 * nodes) return fail(QM_ERR_ARGUMENT, "terrain-fine: a block does not decode");
+            const uint8_t *low = planes.data(), *high = low + nodes;
+            north_row.assign(columns, 0);
+            for (size_t r = 0; r < rows; ++r) {
+                uint16_t west = 0, north_west = 0;
+                for (size_t c = 0; c < columns; ++c) {
+                    const size_t at = r * columns + c;
+                    const uint16_t zigzag = (uint16_t)(low[at] | (high[at] << 8));
+                    const uint16_t residual = (uint16_t)((uint16_t)(zigzag >> 1) ^ (uint16_t)(-(int)(zigzag & 1)));
+                    const uint16_t code = (uint16_t)(residual + (uint16_t)(west + north_row[c] - north_west));
+                    north_west = north_row[c];
+                    north_row[c] = code;
+                    west = code;
+                    details[(size_t)(r0 + r) * w.columns + c0 + c] = (int16_t)code;
+                }
+            }
+        }
+    }
+    return QM_OK;
+}
+
 }  // extern "C"

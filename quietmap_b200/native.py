@@ -77,6 +77,8 @@ def lib():
         L.qm_terrain_decode.argtypes = [_U8, C.c_size_t, C.POINTER(abi.TerrainWindow), C.POINTER(C.c_uint16), _U8,
                                         _U8, _U8]
         L.qm_terrain_decode.restype = C.c_int
+        L.qm_terrain_fine_decode.argtypes = [_U8, C.c_size_t, C.POINTER(abi.TerrainWindow), C.POINTER(C.c_int16)]
+        L.qm_terrain_fine_decode.restype = C.c_int
         L.qm_weather_place.argtypes = [_U8, C.c_size_t, C.c_double, C.c_double, _D, _D]
         L.qm_weather_place.restype = C.c_int
         L.qm_weather_read_place.argtypes = [C.c_char_p, C.c_double, C.c_double, _D, _D]
@@ -288,6 +290,17 @@ def terrain_decode(data):
                                    abi.ptr(imp, C.c_uint8), abi.ptr(forest, C.c_uint8), abi.ptr(canopy, C.c_uint8)))
     window = dict(north_node=w.north_node, west_node=w.west_node, rows=w.rows, columns=w.columns)
     return window, heights, imp, forest, canopy
+
+
+def terrain_fine_decode(data):
+    """A fine terrain tile's window and details (qm_terrain_fine_decode): (window dict, codes
+    int16 [rows][columns], 0.2 m each)."""
+    b, p = _tile_bytes(data)
+    w = abi.TerrainWindow()
+    _check(lib().qm_terrain_fine_decode(p, len(b), C.byref(w), None))
+    details = np.zeros((w.rows, w.columns), np.int16)
+    _check(lib().qm_terrain_fine_decode(p, len(b), C.byref(w), details.ctypes.data_as(C.POINTER(C.c_int16))))
+    return dict(north_node=w.north_node, west_node=w.west_node, rows=w.rows, columns=w.columns), details
 
 
 def weather_place(table, lat, lon):

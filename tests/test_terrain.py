@@ -68,3 +68,27 @@ def test_broken_tiles_are_refused():
     short = data[:24] + ot.compress(ot.planes(heights, imp, forest, canopy)[:-5])
     with pytest.raises(native.QmError, match="does not match the window"):
         native.terrain_decode(short)
+
+
+def test_a_fine_tile_decodes_to_the_details_it_was_encoded_from():
+    """tiles/src/terrain_fine.rs:286-330: blocks of every shape (2.3 blocks by 1.5), negative and
+    positive details and the i16 ends; a cut tile and a bad frame are errors."""
+    rows, columns = 2 * 128 + 40, 128 + 65
+    at = np.arange(rows * columns)
+    k = at % 97
+    details = np.where(k == 0, -32768, np.where(k == 1, 32767, (k - 48) * 3 + (at // 300) % 7)).astype(np.int16)
+    details = details.reshape(rows, columns)
+    data = ot.encode_fine(1_076_760, 307_800, details)
+    window, got = native.terrain_fine_decode(data)
+    assert window == dict(north_node=1_076_760, west_node=307_800, rows=rows, columns=columns)
+    np.testing.assert_array_equal(got, details)
+    with pytest.raises(native.QmError, match="terrain-fine"):
+        native.terrain_fine_decode(data[:24 + 8])
+    broken = bytearray(data)
+    broken[-1] ^= 0xFF
+    with pytest.raises(native.QmError, match="a block does not decode"):
+        native.terrain_fine_decode(bytes(broken))
+    small = np.array([[0, 5, 10], [15, 20, 25], [30, 35, -40]], np.int16)
+    assert np.array_equal(native.terrain_fine_decode(ot.encode_fine(6, 0, small))[1], small)
+    with pytest.raises(native.QmError, match="a window no tile has"):
+        native.terrain_fine_decode(ot.encode_fine(6, 0, small[:1]))
