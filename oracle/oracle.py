@@ -67,6 +67,12 @@ def lib():
         L.qmo_level_bin.argtypes = [C.c_double, C.c_double, C.c_double, C.c_uint32]
         L.qmo_level_bin.restype = C.c_uint32
         _B = C.POINTER(C.c_uint8)
+        L.qmo_line_geometry.argtypes = [_D, _D, _D]
+        L.qmo_line_geometry.restype = C.c_int
+        L.qmo_line_in_plane_angle_at.argtypes = [_D, _D, C.c_double]
+        L.qmo_line_in_plane_angle_at.restype = C.c_double
+        L.qmo_line_nodes.argtypes = [_D, _D, _D, C.c_size_t, _D, _D, _B, C.c_size_t]
+        L.qmo_line_nodes.restype = C.c_int
         L.qmo_favourable_at.argtypes = [C.POINTER(C.c_float), C.c_double]
         L.qmo_favourable_at.restype = C.c_double
         L.qmo_nden_cell.argtypes = [C.c_double]
@@ -285,6 +291,40 @@ def level_histogram(levels, level_min, bin_db, n_bins):
 
 def level_bin(level, level_min, bin_db, n_bins):
     return lib().qmo_level_bin(level, level_min, bin_db, n_bins)
+
+
+def _xyz(p):
+    return np.ascontiguousarray(np.asarray(p, dtype=np.float64).reshape(3))
+
+
+def line_geometry(start, end):
+    """A straight piece seen from the receiver at the origin (physics/src/line.rs:86-124): dict of
+    length, perpendicular, subtended angle and divergence factor; None under a millimetre."""
+    out = np.zeros(4)
+    if lib().qmo_line_geometry(abi.ptr(_xyz(start), C.c_double), abi.ptr(_xyz(end), C.c_double),
+                               abi.ptr(out, C.c_double)) != 0:
+        return None
+    return dict(length_m=out[0], perpendicular_m=out[1], subtended_rad=out[2], divergence_factor=out[3])
+
+
+def line_in_plane_angle_at(start, end, along_m):
+    return lib().qmo_line_in_plane_angle_at(abi.ptr(_xyz(start), C.c_double), abi.ptr(_xyz(end), C.c_double),
+                                            float(along_m))
+
+
+def line_nodes(start, end, arcs=()):
+    """A piece's quadrature nodes (physics/src/line.rs:180-355) given obstacle edge arcs
+    [(azimuth lo, azimuth hi, nearest range)]: (along_m, weight_rad, obstacles_on_ray) arrays."""
+    a = np.ascontiguousarray(np.asarray(arcs, dtype=np.float64).reshape(-1, 3))
+    cap = 64 * 9 * 5
+    along, weight = np.zeros(cap), np.zeros(cap)
+    on_ray = np.zeros(cap, np.uint8)
+    n = lib().qmo_line_nodes(abi.ptr(_xyz(start), C.c_double), abi.ptr(_xyz(end), C.c_double),
+                             abi.ptr(a, C.c_double) if len(a) else None, len(a), abi.ptr(along, C.c_double),
+                             abi.ptr(weight, C.c_double), abi.ptr(on_ray, C.c_uint8), cap)
+    if n < 0:
+        return None
+    return along[:n], weight[:n], on_ray[:n].astype(bool)
 
 
 def favourable_at(row, azimuth_rad):

@@ -1766,6 +1766,206 @@ void qmo_level_histogram(const double *levels, size_t n, double level_min, doubl
     for (size_t i = 0; i < n; ++i) counts[level_bin(levels[i], level_min, bin_db, n_bins)]++;
 }
 
+// ---------------------------------------------------------------------------------------------
+// Line pieces: the CNOSSOS-EU point sum of a straight piece by quadrature in the in-plane angle
+// (physics/src/line.rs). Positions are receiver-relative metres (x east, y north, z up).
+
+static const double LINE_PI = 3.14159265358979323846;
+static const int LINE_BUCKETS = 5;                                   // line.rs:19
+static const double LINE_ONE_BUCKET_SPAN = 3.0 * LINE_PI / 180.0;    // line.rs:23
+static const double LINE_WIDE_MIN_SPAN = 3.0 * LINE_PI / 180.0;      // line.rs:26
+static const int LINE_MASK_BINS = 128;                               // line.rs:28
+static const double LINE_PART_MAX_SPAN = 0.26;                       // line.rs:30
+static const int LINE_MAX_PARTS = 9;                                 // line.rs:31
+static const double LINE_PERP_FLOOR = 0.5;                           // line.rs:34
+static const double LINE_DIVERGENCE = 12.589254117941673;            // 10^1.1, line.rs:36
+
+static double line_wrap_to_pi(double angle) {  // line.rs:39-48
+    const double tau = 2.0 * LINE_PI;
+    double a = std::fmod(angle, tau);
+    if (a > LINE_PI) return a - tau;
+    if (a <= -LINE_PI) return a + tau;
+    return a;
+}
+
+struct LinePiece {  // line.rs:53-62, 86-124
+    double start[3], unit[3], length, foot, perp, angle0, angle1;
+    bool make(const double s[3], const double e[3]) {
+        const double a[3] = {e[0] - s[0], e[1] - s[1], e[2] - s[2]};
+        length = std::sqrt(a[0] * a[0] + a[1] * a[1] + a[2] * a[2]);
+        if (length < 1e-3) return false;
+        for (int k = 0; k < 3; ++k) {
+            start[k] = s[k];
+            unit[k] = a[k] / length;
+        }
+        foot = -(s[0] * unit[0] + s[1] * unit[1] + s[2] * unit[2]);
+        const double f[3] = {s[0] + foot * unit[0], s[1] + foot * unit[1], s[2] + foot * unit[2]};
+        perp = std::max(std::sqrt(f[0] * f[0] + f[1] * f[1] + f[2] * f[2]), LINE_PERP_FLOOR);
+        angle0 = std::atan((0.0 - foot) / perp);
+        angle1 = std::atan((length - foot) / perp);
+        return true;
+    }
+    double span() const { return angle1 - angle0; }
+    double divergence() const { return std::hypot(unit[0], unit[1]) / (LINE_DIVERGENCE * perp); }
+    double angle_at(double along) const { return std::atan((along - foot) / perp); }
+    double along_at_angle(double angle) const {
+        return std::min(std::max(foot + perp * std::tan(angle), 0.0), length);
+    }
+    void point(double along, double p[3]) const {
+        for (int k = 0; k < 3; ++k) p[k] = start[k] + along * unit[k];
+    }
+    // Where the horizontal ray at `azimuth` meets the ground track, clamped; false when parallel.
+    bool along_at_azimuth(double azimuth, double &along) const {
+        const double dx = std::cos(azimuth), dy = std::sin(azimuth);
+        const double ux = unit[0] * length, uy = unit[1] * length;
+        const double den = dx * uy - dy * ux;
+        if (std::fabs(den) < 1e-12) return false;
+        const double fraction = (dy * start[0] - dx * start[1]) / den;
+        along = std::min(std::max(fraction, 0.0), 1.0) * length;
+        return true;
+    }
+    double azimuth_at(double along) const {
+        double p[3];
+        point(along, p);
+        return std::atan2(p[1], p[0]);
+    }
+    double range_at(double along) const {
+        double p[3];
+        point(along, p);
+        return std::hypot(p[0], p[1]);
+    }
+};
+
+struct LineNode {
+    double along, weight;
+    bool on_ray;
+};
+
+// mark_blocked_bins (line.rs:317-355): the bins of the span one edge's arc blocks where the edge
+// stands at least a metre nearer than the piece seen there.
+static void line_mark(const LinePiece &g, const double arc[3], double radius, double lo, double hi, double width,
+                      bool blocked[LINE_MASK_BINS]) {
+    if (arc[2] > radius) return;
+    for (double shift : {0.0, 2.0 * LINE_PI, -2.0 * LINE_PI}) {
+        const double piece_lo = std::max(arc[0] + shift, lo), piece_hi = std::min(arc[1] + shift, hi);
+        if (piece_hi <= piece_lo) continue;
+        double along;
+        if (!g.along_at_azimuth(0.5 * (piece_lo + piece_hi), along)) continue;
+        if (g.range_at(along) - arc[2] <= 1.0) continue;
+        const size_t first = (size_t)std::max(std::floor((piece_lo - lo) / width), 0.0);
+        const double up = std::ceil((piece_hi - lo) / width);
+        size_t last = up > 0.0 ? (size_t)up : 0;
+        last = last > 0 ? last - 1 : 0;
+        last = std::min(std::max(last, first), (size_t)LINE_MASK_BINS - 1);
+        for (size_t b = first; b <= last; ++b) blocked[b] = true;
+    }
+}
+
+// push_wide_bucket_nodes (line.rs:208-315): geometry-placed nodes of a wide bucket with something
+// in front of it; nothing otherwise.
+static void line_wide_nodes(const LinePiece &g, double angle_lo, double angle_hi, const double *arcs, size_t n_arcs,
+                            std::vector<LineNode> &nodes) {
+    const double along_lo = g.along_at_angle(angle_lo), along_hi = g.along_at_angle(angle_hi);
+    const double azimuth_a = g.azimuth_at(along_lo);
+    const double turn = line_wrap_to_pi(g.azimuth_at(along_hi) - azimuth_a);
+    const double span = std::fabs(turn);
+    if (span < LINE_WIDE_MIN_SPAN) return;
+    const double span_lo = turn < 0.0 ? azimuth_a + turn : azimuth_a;
+    const double span_hi = turn < 0.0 ? azimuth_a : azimuth_a + turn;
+    const double range_lo = g.range_at(along_lo), range_hi = g.range_at(along_hi);
+    double a[3], b[3];
+    g.point(along_lo, a);
+    g.point(along_hi, b);
+    const double chord = std::hypot(a[0] - b[0], a[1] - b[1]);
+    const double centre_range = g.range_at(g.along_at_angle(0.5 * (angle_lo + angle_hi)));
+    const double radius = std::min(std::min(range_lo, range_hi), centre_range) + chord;
+    const double width = span / LINE_MASK_BINS;
+    bool blocked[LINE_MASK_BINS] = {};
+    for (size_t k = 0; k < n_arcs; ++k) line_mark(g, arcs + 3 * k, radius, span_lo, span_hi, width, blocked);
+    bool any = false;
+    for (bool v : blocked) any = any || v;
+    if (!any) return;
+    const double lo_a = std::min(along_lo, along_hi), hi_a = std::max(along_lo, along_hi);
+    auto angle_at_azimuth = [&](double azimuth, double fallback) {
+        double along;
+        if (!g.along_at_azimuth(azimuth, along)) return fallback;
+        return g.angle_at(std::min(std::max(along, lo_a), hi_a));
+    };
+    const double angle_at_span_lo = turn < 0.0 ? angle_hi : angle_lo;
+    const double angle_at_span_hi = turn < 0.0 ? angle_lo : angle_hi;
+    int bin = 0;
+    while (bin < LINE_MASK_BINS) {
+        const bool run_blocked = blocked[bin];
+        int run_end = bin;
+        while (run_end < LINE_MASK_BINS && blocked[run_end] == run_blocked) ++run_end;
+        const double run_lo = span_lo + bin * width;
+        const double run_hi = run_end == LINE_MASK_BINS ? span_hi : span_lo + run_end * width;
+        const int parts = (int)std::min(std::max(std::ceil((run_hi - run_lo) / LINE_PART_MAX_SPAN), 1.0),
+                                        (double)LINE_MAX_PARTS);
+        const double step = (run_hi - run_lo) / parts;
+        for (int part = 0; part < parts; ++part) {
+            const double part_lo = run_lo + part * step;
+            const double part_hi = (part + 1 == parts && run_end == LINE_MASK_BINS) ? span_hi : part_lo + step;
+            const double edge_lo = (bin == 0 && part == 0) ? angle_at_span_lo : angle_at_azimuth(part_lo, angle_at_span_lo);
+            const double edge_hi =
+                (run_end == LINE_MASK_BINS && part + 1 == parts) ? angle_at_span_hi : angle_at_azimuth(part_hi, angle_at_span_hi);
+            double along;
+            if (!g.along_at_azimuth(0.5 * (part_lo + part_hi), along)) along = g.along_at_angle(0.5 * (edge_lo + edge_hi));
+            nodes.push_back(LineNode{along, std::fabs(edge_hi - edge_lo), run_blocked});
+        }
+        bin = run_end;
+    }
+}
+
+// line_quadrature_nodes (line.rs:180-206): one bucket under 3 degrees, else five of equal dphi,
+// each its centre node unless it is wide and something stands in front of it.
+static void line_nodes(const LinePiece &g, const double *arcs, size_t n_arcs, std::vector<LineNode> &nodes) {
+    nodes.clear();
+    const double span = g.span();
+    const int buckets = span < LINE_ONE_BUCKET_SPAN ? 1 : LINE_BUCKETS;
+    const double bucket_angle = span / buckets;
+    for (int bucket = 0; bucket < buckets; ++bucket) {
+        const double angle_lo = g.angle0 + bucket * bucket_angle, angle_hi = angle_lo + bucket_angle;
+        const size_t before = nodes.size();
+        line_wide_nodes(g, angle_lo, angle_hi, arcs, n_arcs, nodes);
+        if (nodes.size() == before)
+            nodes.push_back(LineNode{g.along_at_angle(angle_lo + 0.5 * bucket_angle), angle_hi - angle_lo, true});
+    }
+}
+
+// The geometry of a piece: out = (length, perpendicular, subtended angle, divergence factor);
+// -1 for a piece shorter than a millimetre.
+int qmo_line_geometry(const double *start, const double *end, double *out) {
+    LinePiece g;
+    if (!g.make(start, end)) return -1;
+    out[0] = g.length;
+    out[1] = g.perp;
+    out[2] = g.span();
+    out[3] = g.divergence();
+    return 0;
+}
+
+double qmo_line_in_plane_angle_at(const double *start, const double *end, double along) {
+    LinePiece g;
+    return g.make(start, end) ? g.angle_at(along) : NAN;
+}
+
+// The quadrature nodes of a piece given every obstacle edge's arc (arcs[n][3]: azimuth lo, hi,
+// nearest horizontal range); up to cap written. Returns the count, -1 for a degenerate piece.
+int qmo_line_nodes(const double *start, const double *end, const double *arcs, size_t n_arcs, double *along,
+                   double *weight, uint8_t *on_ray, size_t cap) {
+    LinePiece g;
+    if (!g.make(start, end)) return -1;
+    std::vector<LineNode> nodes;
+    line_nodes(g, arcs, n_arcs, nodes);
+    for (size_t k = 0; k < nodes.size() && k < cap; ++k) {
+        along[k] = nodes[k].along;
+        weight[k] = nodes[k].weight;
+        on_ray[k] = nodes[k].on_ray ? 1 : 0;
+    }
+    return (int)nodes.size();
+}
+
 // p of one period's row for sound travelling along azimuth_rad (atan2(north, east)): the scene's
 // favourable row (float) interpolated between sector centres (physics/src/weather.rs:61-70).
 double qmo_favourable_at(const float *row, double azimuth_rad) { return favourable_at(row, azimuth_rad); }
