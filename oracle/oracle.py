@@ -67,6 +67,13 @@ def lib():
         L.qmo_level_bin.argtypes = [C.c_double, C.c_double, C.c_double, C.c_uint32]
         L.qmo_level_bin.restype = C.c_uint32
         _B = C.POINTER(C.c_uint8)
+        L.qmo_path_difference.argtypes = [C.c_int, C.c_double, _D, _D, _D, _D, C.c_size_t, _D]
+        L.qmo_path_difference.restype = C.c_double
+        L.qmo_diffraction_path.argtypes = [C.c_int, C.c_double, _D, _D, _D, C.c_size_t, _D,
+                                           C.POINTER(C.c_size_t), _D, C.POINTER(C.c_size_t), C.c_size_t]
+        L.qmo_diffraction_path.restype = C.c_int
+        L.qmo_state_ray_altitude.argtypes = [C.c_int, C.c_double, _D, _D, _D, _D, C.c_double]
+        L.qmo_state_ray_altitude.restype = C.c_double
         L.qmo_line_geometry.argtypes = [_D, _D, _D]
         L.qmo_line_geometry.restype = C.c_int
         L.qmo_line_in_plane_angle_at.argtypes = [_D, _D, C.c_double]
@@ -291,6 +298,50 @@ def level_histogram(levels, level_min, bin_db, n_bins):
 
 def level_bin(level, level_min, bin_db, n_bins):
     return lib().qmo_level_bin(level, level_min, bin_db, n_bins)
+
+
+def _pts(points):
+    a = np.ascontiguousarray(np.asarray(points, dtype=np.float64).reshape(-1, 2))
+    return a, abi.ptr(a, C.c_double) if len(a) else None
+
+
+class StateRay:
+    """A meteorological state's ray between source and receiver (physics/src/cnossos/
+    rubber_band.rs:207-317): state 0 homogeneous, 1 favourable; radius_m None takes `between`'s."""
+
+    def __init__(self, state, source, receiver, radius_m=None):
+        self.state, self.radius = state, (radius_m or 0.0)
+        self.source, _ = _pts(source)
+        self.receiver, _ = _pts(receiver)
+
+    def _ends(self):
+        return abi.ptr(self.source, C.c_double), abi.ptr(self.receiver, C.c_double)
+
+    def path_difference(self, start, points, end):
+        p, pp = _pts(points)
+        a, _ = _pts(start)
+        b, _ = _pts(end)
+        return lib().qmo_path_difference(self.state, self.radius, *self._ends(), abi.ptr(a, C.c_double), pp, len(p),
+                                         abi.ptr(b, C.c_double))
+
+    def diffraction_path(self, candidates):
+        """(blocked, band points [(x, z)], blocking candidates [(x, z)]) (rubber_band.rs:373-444)."""
+        c, cp = _pts(candidates)
+        cap = max(len(c), 1)
+        points, blocking = np.zeros((cap, 2)), np.zeros((cap, 2))
+        n_points, n_blocking = C.c_size_t(), C.c_size_t()
+        blocked = lib().qmo_diffraction_path(self.state, self.radius, *self._ends(), cp, len(c),
+                                             abi.ptr(points, C.c_double), C.byref(n_points),
+                                             abi.ptr(blocking, C.c_double), C.byref(n_blocking), cap)
+        return (bool(blocked), [tuple(p) for p in points[:n_points.value]],
+                [tuple(p) for p in blocking[:n_blocking.value]])
+
+    def altitude(self, a, b, x):
+        """The ray from a to b at x: chord altitude plus the arc's sag."""
+        pa, _ = _pts(a)
+        pb, _ = _pts(b)
+        return lib().qmo_state_ray_altitude(self.state, self.radius, *self._ends(), abi.ptr(pa, C.c_double),
+                                            abi.ptr(pb, C.c_double), float(x))
 
 
 def _xyz(p):

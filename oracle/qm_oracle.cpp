@@ -1933,6 +1933,57 @@ static void line_nodes(const LinePiece &g, const double *arcs, size_t n_arcs, st
     }
 }
 
+// ---------------------------------------------------------------------------------------------
+// The state rays and the rubber band on their own (physics/src/cnossos/rubber_band.rs), for the
+// reference's rubber-band tests. Points are (x, z) pairs; state 0 homogeneous, 1 favourable; a
+// radius_m <= 0 takes the state ray between source and receiver (`StateRay::between`).
+
+static StateRay rb_ray(int state, double radius_m, const double *source, const double *receiver) {
+    StateRay ray = StateRay::between(state, PP{source[0], source[1]}, PP{receiver[0], receiver[1]});
+    if (radius_m > 0.0) ray.radius = radius_m;
+    return ray;
+}
+
+double qmo_path_difference(int state, double radius_m, const double *source, const double *receiver,
+                           const double *from, const double *points, size_t n, const double *to) {
+    const StateRay ray = rb_ray(state, radius_m, source, receiver);
+    std::vector<PP> p(n);
+    for (size_t k = 0; k < n; ++k) p[k] = PP{points[2 * k], points[2 * k + 1]};
+    return ray.path_difference(PP{from[0], from[1]}, p.data(), n, PP{to[0], to[1]});
+}
+
+// diffraction_path: returns whether the direct ray is blocked; the band's points (up to cap) and
+// the blocking candidates (up to cap), with their counts.
+int qmo_diffraction_path(int state, double radius_m, const double *source, const double *receiver,
+                         const double *candidates, size_t n, double *points, size_t *n_points, double *blocking,
+                         size_t *n_blocking, size_t cap) {
+    const StateRay ray = rb_ray(state, radius_m, source, receiver);
+    std::vector<PP> c(n), out;
+    for (size_t k = 0; k < n; ++k) c[k] = PP{candidates[2 * k], candidates[2 * k + 1]};
+    std::vector<Blocking> block, hull;
+    bool blocked = false;
+    diffraction_path(ray, PP{source[0], source[1]}, PP{receiver[0], receiver[1]}, c, block, hull, out, blocked);
+    *n_points = out.size();
+    for (size_t k = 0; k < out.size() && k < cap; ++k) {
+        points[2 * k] = out[k].x;
+        points[2 * k + 1] = out[k].z;
+    }
+    *n_blocking = block.size();
+    for (size_t k = 0; k < block.size() && k < cap; ++k) {
+        blocking[2 * k] = block[k].x;
+        blocking[2 * k + 1] = block[k].z;
+    }
+    return blocked ? 1 : 0;
+}
+
+// The state's ray from a to b at x: the chord's altitude plus the arc's sag.
+double qmo_state_ray_altitude(int state, double radius_m, const double *source, const double *receiver,
+                              const double *a, const double *b, double x) {
+    const StateRay ray = rb_ray(state, radius_m, source, receiver);
+    const PP pa{a[0], a[1]}, pb{b[0], b[1]};
+    return chord_altitude(pa, pb, x) + ray.sag(pa, pb).at(x - pa.x);
+}
+
 // The geometry of a piece: out = (length, perpendicular, subtended angle, divergence factor);
 // -1 for a piece shorter than a millimetre.
 int qmo_line_geometry(const double *start, const double *end, double *out) {
