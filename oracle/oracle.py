@@ -67,6 +67,8 @@ def lib():
         L.qmo_level_bin.argtypes = [C.c_double, C.c_double, C.c_double, C.c_uint32]
         L.qmo_level_bin.restype = C.c_uint32
         _B = C.POINTER(C.c_uint8)
+        L.qmo_ground_attenuation_bands.argtypes = [C.c_double] * 9 + [C.c_int, _D]
+        L.qmo_ground_attenuation_bands.restype = None
         L.qmo_path_difference.argtypes = [C.c_int, C.c_double, _D, _D, _D, _D, C.c_size_t, _D]
         L.qmo_path_difference.restype = C.c_double
         L.qmo_diffraction_path.argtypes = [C.c_int, C.c_double, _D, _D, _D, C.c_size_t, _D,
@@ -298,6 +300,14 @@ def level_histogram(levels, level_min, bin_db, n_bins):
 
 def level_bin(level, level_min, bin_db, n_bins):
     return lib().qmo_level_bin(level, level_min, bin_db, n_bins)
+
+
+def ground_attenuation_bands(plane, source, receiver, g_path, g_impedance, g_floor, state):
+    """A_ground per band over a mean plane (slope, intercept) (physics/src/cnossos/ground.rs)."""
+    out = np.zeros(8)
+    lib().qmo_ground_attenuation_bands(plane[0], plane[1], source[0], source[1], receiver[0], receiver[1], g_path,
+                                       g_impedance, g_floor, state, abi.ptr(out, C.c_double))
+    return out
 
 
 def _pts(points):

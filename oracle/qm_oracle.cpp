@@ -1933,6 +1933,14 @@ static void line_nodes(const LinePiece &g, const double *arcs, size_t n_arcs, st
     }
 }
 
+// A_ground per band over one mean plane (physics/src/cnossos/ground.rs:8-139) for a source at
+// (sx, sz) and a receiver at (rx, rz) with the given ground factors and state.
+void qmo_ground_attenuation_bands(double slope, double intercept, double sx, double sz, double rx, double rz,
+                                  double g_path, double g_impedance, double g_floor, int state, double *out) {
+    const EqGeometry g = geometry_over(MeanPlane{slope, intercept}, sx, sz, rx, rz);
+    ground_attenuation_bands(g, GroundFactors{g_path, g_impedance, g_floor}, state, out);
+}
+
 // ---------------------------------------------------------------------------------------------
 // The state rays and the rubber band on their own (physics/src/cnossos/rubber_band.rs), for the
 // reference's rubber-band tests. Points are (x, z) pairs; state 0 homogeneous, 1 favourable; a
