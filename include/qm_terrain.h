@@ -50,6 +50,35 @@ qm_status qm_terrain_decode(const uint8_t *bytes, size_t n_bytes, qm_terrain_win
 qm_status qm_terrain_fine_decode(const uint8_t *bytes, size_t n_bytes, qm_terrain_window *window,
                                  int16_t *details);
 
+/* The ground at one point, as `Terrain::sample` gives it (tiles/src/terrain.rs:115-127). */
+typedef struct {
+    double height_m;       /* bilinear over the cell's four nodes */
+    double ground_factor;  /* 1 - bilinear imperviousness / 100 */
+    double forest_cover;   /* the nearest node's, in [0, 1] */
+    double canopy_m;       /* the nearest node's */
+} qm_ground_sample;
+
+/* Web Mercator in z12 tile units (x east, y south, both in [0, 4096)) of a latitude and longitude
+ * in degrees, latitude clamped to the Mercator limit, longitude wrapped (tiles/src/geo.rs:28-40). */
+void qm_mercator_from_degrees(double lat_deg, double lon_deg, double *x, double *y);
+
+/* The node window of z12 tile (tile_x, tile_y): floor and ceiling nodes bracketing the tile
+ * (`Window::of_tile`, terrain.rs:66-88), what its `terrain` file holds. */
+qm_status qm_terrain_window_of_tile(uint32_t tile_x, uint32_t tile_y, qm_terrain_window *window);
+
+/* The fractional column (0 at west_node) of Mercator x, across the antimeridian the same meridian
+ * a world away, the column nearest the window (`Window::column_of`, terrain.rs:55-64). */
+double qm_terrain_column_of(const qm_terrain_window *window, double mercator_x);
+
+/* `Terrain::locate` and `sample_at` (terrain.rs:289-387) at n Mercator points (mercator_xy[n][2])
+ * over a decoded window (`qm_terrain_decode`'s arrays): found[k] 1 with out[k] filled, 0 where
+ * the point is outside the window or a node it needs has no data (a missing height or an
+ * imperviousness or forest cover above 100 %). */
+qm_status qm_terrain_sample(const qm_terrain_window *window, const uint16_t *height_codes,
+                            const uint8_t *impervious, const uint8_t *forest, const uint8_t *canopy,
+                            const double *mercator_xy, size_t n, qm_ground_sample *out,
+                            uint8_t *found);
+
 #ifdef __cplusplus
 }
 #endif

@@ -38,6 +38,11 @@ class TerrainWindow(C.Structure):
     _fields_ = [("north_node", C.c_int32), ("west_node", C.c_int32), ("rows", C.c_uint32), ("columns", C.c_uint32)]
 
 
+class GroundSample(C.Structure):
+    _fields_ = [("height_m", C.c_double), ("ground_factor", C.c_double), ("forest_cover", C.c_double),
+                ("canopy_m", C.c_double)]
+
+
 class ObstaclesCounts(C.Structure):
     _fields_ = [(name, C.c_uint32) for name in
                 ("outlines", "vertices", "runs", "occupied_cells", "footprint_squares", "pad_")]

@@ -3006,6 +3006,95 @@ qm_status qm_terrain_decode(const uint8_t *bytes, size_t n_bytes, qm_terrain_win
     return QM_OK;
 }
 
+void qm_mercator_from_degrees(double lat_deg, double lon_deg, double *x, double *y) {
+    const double pi = 3.14159265358979323846, n = 4096.0, max_lat = 85.05112877980659;
+    double lon = std::fmod(lon_deg + 180.0, 360.0);
+    if (lon < 0.0) lon += 360.0;
+    lon -= 180.0;
+    const double phi = std::min(std::max(lat_deg, -max_lat), max_lat) * (pi / 180.0);
+    if (x) *x = (lon + 180.0) / 360.0 * n;
+    if (y) *y = (1.0 - std::asinh(std::tan(phi)) / pi) / 2.0 * n;
+}
+
+qm_status qm_terrain_window_of_tile(uint32_t tile_x, uint32_t tile_y, qm_terrain_window *window) {
+    if (!window) return fail(QM_ERR_ARGUMENT, "qm_terrain_window_of_tile: null window");
+    if (tile_x >= 4096 || tile_y >= 4096) return fail(QM_ERR_ARGUMENT, "qm_terrain_window_of_tile: tile outside z12");
+    const int64_t axis = 4096, longitude_nodes = 360 * 3600;
+    // Longitude edges have denominator 4096: exact integer floor and ceiling.
+    const int64_t west = (int64_t)tile_x * longitude_nodes / axis - longitude_nodes / 2;
+    const int64_t east = (((int64_t)tile_x + 1) * longitude_nodes + axis - 1) / axis - longitude_nodes / 2;
+    const double pi = 3.14159265358979323846;
+    auto edge_latitude_nodes = [&](uint32_t y) {
+        const double mercator = pi * (1.0 - 2.0 * (double)y / 4096.0);
+        return std::atan(std::sinh(mercator)) * (180.0 / pi) * 3600.0;
+    };
+    const int32_t north = (int32_t)std::ceil(edge_latitude_nodes(tile_y));
+    const int32_t south = (int32_t)std::floor(edge_latitude_nodes(tile_y + 1));
+    window->north_node = north;
+    window->west_node = (int32_t)west;
+    window->rows = (uint32_t)(north - south + 1);
+    window->columns = (uint32_t)(east - west + 1);
+    return QM_OK;
+}
+
+double qm_terrain_column_of(const qm_terrain_window *window, double mercator_x) {
+    const double world = 360.0 * 3600.0;
+    const double column = mercator_x * world / 4096.0 - world / 2.0 - (double)window->west_node;
+    double wrapped = std::fmod(column + world / 2.0, world);
+    if (wrapped < 0.0) wrapped += world;
+    return wrapped - world / 2.0;
+}
+
+qm_status qm_terrain_sample(const qm_terrain_window *window, const uint16_t *height_codes, const uint8_t *impervious,
+                            const uint8_t *forest, const uint8_t *canopy, const double *mercator_xy, size_t n,
+                            qm_ground_sample *out, uint8_t *found) {
+    if (!window || (n && (!height_codes || !impervious || !forest || !canopy || !mercator_xy || !out || !found)))
+        return fail(QM_ERR_ARGUMENT, "qm_terrain_sample: null argument");
+    const qm_terrain_window w = *window;
+    if (w.rows < 1 || w.columns < 1) return fail(QM_ERR_ARGUMENT, "qm_terrain_sample: empty window");
+    // Web Mercator y of every node row (terrain.rs:261-267).
+    std::vector<double> rows(w.rows);
+    for (uint32_t r = 0; r < w.rows; ++r)
+        qm_mercator_from_degrees((double)(w.north_node - (int32_t)r) / 3600.0, 0.0, nullptr, &rows[r]);
+    const double spacing = (rows[w.rows - 1] - rows[0]) / (double)std::max<uint32_t>(w.rows - 1, 1);
+    for (size_t k = 0; k < n; ++k) {
+        found[k] = 0;
+        const double px = mercator_xy[2 * k], py = mercator_xy[2 * k + 1];
+        // locate (terrain.rs:289-331)
+        double column_position = qm_terrain_column_of(&w, px);
+        if (column_position > -1e-6) column_position = std::max(column_position, 0.0);
+        const double column = std::floor(column_position), cf = column_position - column;
+        const double guess = std::floor((py - rows[0]) / spacing);
+        int64_t row = std::isfinite(guess) ? (int64_t)std::min(std::max(guess, 0.0), (double)(w.rows - 1)) : 0;
+        while (row > 0 && py < rows[row]) --row;
+        while (row + 1 < (int64_t)w.rows && py >= rows[row + 1]) ++row;
+        if (py < rows[0] - 1e-9 || column < 0.0) continue;
+        const double rf = row + 1 < (int64_t)w.rows ? (py - rows[row]) / (rows[row + 1] - rows[row]) : 0.0;
+        const uint64_t r0 = (uint64_t)row, c0 = column >= 4294967295.0 ? 4294967295ull : (uint64_t)column;
+        const uint64_t r1 = r0 + (rf > 0.0 ? 1 : 0), c1 = c0 + (cf > 0.0 ? 1 : 0);
+        if (r1 >= w.rows || c1 >= w.columns) continue;
+        // sample_at (terrain.rs:339-387)
+        const size_t at[4] = {(size_t)(r0 * w.columns + c0), (size_t)(r0 * w.columns + c1), (size_t)(r1 * w.columns + c0),
+                              (size_t)(r1 * w.columns + c1)};
+        const size_t nearest = at[(rf >= 0.5 ? 2 : 0) + (cf >= 0.5 ? 1 : 0)];
+        bool missing = forest[nearest] > 100;
+        for (size_t c : at) missing = missing || height_codes[c] == QM_TERRAIN_HEIGHT_MISSING || impervious[c] > 100;
+        if (missing) continue;
+        const double weight[4] = {(1.0 - rf) * (1.0 - cf), (1.0 - rf) * cf, rf * (1.0 - cf), rf * cf};
+        double height = 0.0, imp = 0.0;
+        for (int c = 0; c < 4; ++c) {
+            height += weight[c] * (-500.0 + (double)height_codes[at[c]] / 5.0);
+            imp += weight[c] * (double)impervious[at[c]];
+        }
+        out[k].height_m = height;
+        out[k].ground_factor = 1.0 - imp / 100.0;
+        out[k].forest_cover = (double)forest[nearest] / 100.0;
+        out[k].canopy_m = (double)canopy[nearest];
+        found[k] = 1;
+    }
+    return QM_OK;
+}
+
 qm_status qm_terrain_fine_decode(const uint8_t *bytes, size_t n_bytes, qm_terrain_window *window, int16_t *details) {
     constexpr size_t HEADER = 24;
     constexpr uint32_t BLOCK = 128, FINE = 6;

@@ -79,6 +79,15 @@ def lib():
         L.qm_terrain_decode.restype = C.c_int
         L.qm_terrain_fine_decode.argtypes = [_U8, C.c_size_t, C.POINTER(abi.TerrainWindow), C.POINTER(C.c_int16)]
         L.qm_terrain_fine_decode.restype = C.c_int
+        L.qm_mercator_from_degrees.argtypes = [C.c_double, C.c_double, _D, _D]
+        L.qm_mercator_from_degrees.restype = None
+        L.qm_terrain_window_of_tile.argtypes = [C.c_uint32, C.c_uint32, C.POINTER(abi.TerrainWindow)]
+        L.qm_terrain_window_of_tile.restype = C.c_int
+        L.qm_terrain_column_of.argtypes = [C.POINTER(abi.TerrainWindow), C.c_double]
+        L.qm_terrain_column_of.restype = C.c_double
+        L.qm_terrain_sample.argtypes = [C.POINTER(abi.TerrainWindow), C.POINTER(C.c_uint16), _U8, _U8, _U8, _D,
+                                        C.c_size_t, C.POINTER(abi.GroundSample), _U8]
+        L.qm_terrain_sample.restype = C.c_int
         L.qm_weather_place.argtypes = [_U8, C.c_size_t, C.c_double, C.c_double, _D, _D]
         L.qm_weather_place.restype = C.c_int
         L.qm_weather_read_place.argtypes = [C.c_char_p, C.c_double, C.c_double, _D, _D]
@@ -301,6 +310,44 @@ def terrain_fine_decode(data):
     details = np.zeros((w.rows, w.columns), np.int16)
     _check(lib().qm_terrain_fine_decode(p, len(b), C.byref(w), details.ctypes.data_as(C.POINTER(C.c_int16))))
     return dict(north_node=w.north_node, west_node=w.west_node, rows=w.rows, columns=w.columns), details
+
+
+def _window(window):
+    return abi.TerrainWindow(window["north_node"], window["west_node"], window["rows"], window["columns"])
+
+
+def mercator_from_degrees(lat, lon):
+    """Web Mercator in z12 tile units of a latitude and longitude (qm_mercator_from_degrees)."""
+    x, y = C.c_double(), C.c_double()
+    lib().qm_mercator_from_degrees(lat, lon, C.byref(x), C.byref(y))
+    return x.value, y.value
+
+
+def terrain_window_of_tile(tile_x, tile_y):
+    w = abi.TerrainWindow()
+    _check(lib().qm_terrain_window_of_tile(tile_x, tile_y, C.byref(w)))
+    return dict(north_node=w.north_node, west_node=w.west_node, rows=w.rows, columns=w.columns)
+
+
+def terrain_column_of(window, mercator_x):
+    w = _window(window)
+    return lib().qm_terrain_column_of(C.byref(w), mercator_x)
+
+
+def terrain_sample(window, heights, impervious, forest, canopy, mercator_xy):
+    """The ground at Mercator points over a decoded window (qm_terrain_sample): a list of dicts
+    (height_m, ground_factor, forest_cover, canopy_m), None where the reference's sampler refuses."""
+    w = _window(window)
+    h = np.ascontiguousarray(heights, dtype=np.uint16)
+    i, f, c = (np.ascontiguousarray(a, dtype=np.uint8) for a in (impervious, forest, canopy))
+    xy = np.ascontiguousarray(np.asarray(mercator_xy, dtype=np.float64).reshape(-1, 2))
+    out = (abi.GroundSample * max(len(xy), 1))()
+    found = np.zeros(max(len(xy), 1), np.uint8)
+    _check(lib().qm_terrain_sample(C.byref(w), h.ctypes.data_as(C.POINTER(C.c_uint16)), abi.ptr(i, C.c_uint8),
+                                   abi.ptr(f, C.c_uint8), abi.ptr(c, C.c_uint8), abi.ptr(xy, C.c_double), len(xy),
+                                   out, abi.ptr(found, C.c_uint8)))
+    return [dict(height_m=out[k].height_m, ground_factor=out[k].ground_factor, forest_cover=out[k].forest_cover,
+                 canopy_m=out[k].canopy_m) if found[k] else None for k in range(len(xy))]
 
 
 def weather_place(table, lat, lon):

@@ -1,6 +1,8 @@
 """`terrain` tiles (qmterr2): the library's decoder against tiles the oracle writes, pinned to the
 reference's own decode test (tiles/src/terrain.rs:438-473). Host only."""
 
+import math
+
 import numpy as np
 import pytest
 
@@ -92,3 +94,57 @@ def test_a_fine_tile_decodes_to_the_details_it_was_encoded_from():
     assert np.array_equal(native.terrain_fine_decode(ot.encode_fine(6, 0, small))[1], small)
     with pytest.raises(native.QmError, match="a window no tile has"):
         native.terrain_fine_decode(ot.encode_fine(6, 0, small[:1]))
+
+
+def _mercator_to_degrees(x, y):
+    """tiles/src/geo.rs:43-47."""
+    n = 4096.0
+    lat = math.degrees(math.atan(math.sinh(math.pi * (1.0 - 2.0 * y / n))))
+    return lat, x / n * 360.0 - 180.0
+
+
+def test_prague_tile_window_brackets_the_tile():
+    """tiles/src/terrain.rs:392-405."""
+    x, y = native.mercator_from_degrees(50.07553, 14.43781)
+    tile = (int(math.floor(x)), int(math.floor(y)))
+    window = native.terrain_window_of_tile(*tile)
+    assert 204 <= window["rows"] <= 207 and 318 <= window["columns"] <= 320, window
+    north, west = _mercator_to_degrees(tile[0], tile[1])  # the tile's north-west corner
+    assert window["north_node"] >= north * 3600.0 and window["west_node"] <= west * 3600.0
+
+
+def test_columns_wrap_across_the_antimeridian():
+    """tiles/src/terrain.rs:407-422."""
+    west, east = native.terrain_window_of_tile(0, 2241), native.terrain_window_of_tile(4095, 2241)
+    world, just_west = 4096.0, -0.001
+    column = native.terrain_column_of(east, just_west)
+    assert 0.0 <= column < east["columns"], column
+    assert abs(native.terrain_column_of(east, world + just_west) - column) < 1e-6
+    assert 0.0 <= native.terrain_column_of(west, 0.001) < west["columns"]
+    assert abs(native.terrain_column_of(west, 0.001) - native.terrain_column_of(west, world + 0.001)) < 1e-6
+
+
+def test_neighbours_share_their_seam_nodes():
+    """tiles/src/terrain.rs:424-435."""
+    here, east, south = (native.terrain_window_of_tile(2212, 1387), native.terrain_window_of_tile(2213, 1387),
+                         native.terrain_window_of_tile(2212, 1388))
+    assert here["west_node"] + here["columns"] > east["west_node"]
+    assert here["north_node"] - here["rows"] < south["north_node"]
+
+
+def test_samples_interpolate_heights_and_refuse_missing_nodes():
+    """tiles/src/terrain.rs:475-517, through a tile the oracle writes and the library decodes."""
+    code = lambda metres: int((metres + 500.0) * 5.0)
+    heights = np.array([[code(100.0), code(110.0)], [code(120.0), code(130.0)]], np.uint16)
+    imp = np.array([[0, 100], [0, 100]], np.uint8)
+    forest = np.array([[0, 0], [80, 80]], np.uint8)
+    canopy = forest // 4
+    window, h, i, f, c = native.terrain_decode(ot.encode(180_001, 50_000, heights, imp, forest, canopy))
+    at = lambda lat_nodes, lon_nodes: native.mercator_from_degrees(lat_nodes / 3600.0, lon_nodes / 3600.0)
+    points = [at(180_000.5, 50_000.5), at(180_001.0, 50_000.0), at(180_000.5, 50_001.5), at(180_001.5, 50_000.5)]
+    middle, north_west, east, north = native.terrain_sample(window, h, i, f, c, points)
+    assert abs(middle["height_m"] - 115.0) < 1e-4 and abs(middle["ground_factor"] - 0.5) < 1e-5, middle
+    assert abs(north_west["height_m"] - 100.0) < 1e-4 and north_west["forest_cover"] == 0.0
+    assert east is None and north is None
+    h[1, 1] = ot.HEIGHT_MISSING
+    assert native.terrain_sample(window, h, i, f, c, points[:1]) == [None]
