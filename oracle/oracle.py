@@ -374,8 +374,9 @@ def line_in_plane_angle_at(start, end, along_m):
 
 
 def line_nodes(start, end, arcs=()):
-    """A piece's quadrature nodes (physics/src/line.rs:180-355) given obstacle edge arcs
-    [(azimuth lo, azimuth hi, nearest range)]: (along_m, weight_rad, obstacles_on_ray) arrays."""
+    """A piece's quadrature nodes (physics/src/line.rs:180-355) given the arcs a skyline query
+    hands over [(azimuth lo, azimuth hi, nearest range)]: (along_m, weight_rad, obstacles_on_ray)
+    arrays."""
     a = np.ascontiguousarray(np.asarray(arcs, dtype=np.float64).reshape(-1, 3))
     cap = 64 * 9 * 5
     along, weight = np.zeros(cap), np.zeros(cap)

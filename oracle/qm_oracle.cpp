@@ -2009,8 +2009,10 @@ double qmo_line_in_plane_angle_at(const double *start, const double *end, double
     return g.make(start, end) ? g.angle_at(along) : NAN;
 }
 
-// The quadrature nodes of a piece given every obstacle edge's arc (arcs[n][3]: azimuth lo, hi,
-// nearest horizontal range); up to cap written. Returns the count, -1 for a degenerate piece.
+// The quadrature nodes of a piece given the arcs a skyline query hands over (arcs[n][3]: azimuth
+// lo, hi, nearest horizontal range); up to cap written. Returns the count, -1 for a degenerate
+// piece. The mask re-checks each arc's range and span; which edges become arcs (their heights
+// against the source's, popup/src/obstacles/skyline.rs:22-110) is the caller's choice.
 int qmo_line_nodes(const double *start, const double *end, const double *arcs, size_t n_arcs, double *along,
                    double *weight, uint8_t *on_ray, size_t cap) {
     LinePiece g;
