@@ -170,3 +170,89 @@ def tiles_crossed(vertices):
                 continue
             tiles.add(((column // CELLS_PER_SIDE) % TILES_PER_AXIS, y))
     return sorted(tiles)
+
+
+def _wrap_to_pi(angle):
+    """physics/src/line.rs:39-48 (Rust's % on floats is C's fmod)."""
+    a = math.fmod(angle, 2.0 * math.pi)
+    if a > math.pi:
+        return a - 2.0 * math.pi
+    if a <= -math.pi:
+        return a + 2.0 * math.pi
+    return a
+
+
+def _origin_to_segment_distance(a, b):
+    """popup/src/obstacles/skyline.rs:9-20."""
+    ex, ey = b[0] - a[0], b[1] - a[1]
+    length2 = ex * ex + ey * ey
+    t = min(max(-(a[0] * ex + a[1] * ey) / length2, 0.0), 1.0) if length2 > 0.0 else 0.0
+    x, y = a[0] + t * ex, a[1] + t * ey
+    return math.sqrt(x * x + y * y)
+
+
+class Skyline:
+    """The receiver skyline of the line quadrature (popup/src/obstacles/skyline.rs:22-110) over
+    outlines on the global step lattice (y growing south): each edge's supercover cells give the
+    cells' runs and their tallest outline, as a tile's index holds them (tiles/src/obstacles.rs,
+    popup/src/obstacles/tile.rs:93-104)."""
+
+    def __init__(self, outlines, metres_per_step):
+        self.outlines = outlines
+        self.east_m, self.north_m = metres_per_step
+        self.runs = {}
+        for index, outline in enumerate(outlines):
+            vertices = [tuple(v) for v in outline["vertices"]]
+            for edge in range(len(vertices) - 1):
+                for cell in edge_cells(vertices[edge], vertices[edge + 1]):
+                    runs = self.runs.setdefault(cell, [])
+                    if runs and runs[-1][0] == index and runs[-1][1] + runs[-1][2] == edge:
+                        runs[-1][2] += 1
+                    else:
+                        runs.append([index, edge, 1])
+        self.max_height = {cell: max(outlines[r[0]]["height_m"] for r in runs) for cell, runs in self.runs.items()}
+
+    def arcs(self, origin_steps, lo_rad, hi_rad, radius_m, los_floor_m):
+        """Every (lo, hi, nearest) arc an edge near the receiver at `origin_steps` hands over for the
+        wedge [lo_rad, hi_rad], once per cell it is listed in."""
+        ox, oy = origin_steps
+        east_m, north_m = self.east_m, self.north_m
+        cs = float(CELL_STEPS)
+        span = lambda centre, half: range(math.floor((centre - half) / cs), math.floor((centre + half) / cs) + 1)
+        low, high = (math.cos(lo_rad), math.sin(lo_rad)), (math.cos(hi_rad), math.sin(hi_rad))
+        relative = lambda v: ((v[0] - ox) * east_m, (oy - v[1]) * north_m)
+        out = []
+        for row in span(oy, radius_m / north_m):
+            south = (oy - (row + 1) * cs) * north_m
+            north = (oy - row * cs) * north_m
+            dy = max(south, -north, 0.0)
+            for column in span(ox, radius_m / east_m):
+                west = (column * cs - ox) * east_m
+                east = ((column + 1) * cs - ox) * east_m
+                dx = max(west, -east, 0.0)
+                if dx * dx + dy * dy > radius_m * radius_m:
+                    continue
+                corners = [(west, south), (east, south), (west, north), (east, north)]
+                below = all(low[0] * c[1] - low[1] * c[0] < 0.0 for c in corners)
+                above = all(c[0] * high[1] - c[1] * high[0] < 0.0 for c in corners)
+                if below or above:
+                    continue
+                runs = self.runs.get((column, row))
+                if not runs or self.max_height[(column, row)] <= los_floor_m:
+                    continue
+                for index, first_edge, edge_count in runs:
+                    outline = self.outlines[index]
+                    if outline["kind"] == WALL and outline["height_m"] <= los_floor_m:
+                        continue
+                    vertices = outline["vertices"]
+                    a = relative(vertices[first_edge])
+                    azimuth_a = math.atan2(a[1], a[0])
+                    for nxt in range(first_edge + 1, first_edge + edge_count + 1):
+                        b = relative(vertices[nxt])
+                        azimuth_b = math.atan2(b[1], b[0])
+                        nearest = _origin_to_segment_distance(a, b)
+                        if 1e-6 <= nearest <= radius_m:
+                            unwrapped_b = azimuth_a + _wrap_to_pi(azimuth_b - azimuth_a)
+                            out.append((min(azimuth_a, unwrapped_b), max(azimuth_a, unwrapped_b), nearest))
+                        a, azimuth_a = b, azimuth_b
+        return out
