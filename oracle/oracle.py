@@ -67,6 +67,8 @@ def lib():
         L.qmo_level_bin.argtypes = [C.c_double, C.c_double, C.c_double, C.c_uint32]
         L.qmo_level_bin.restype = C.c_uint32
         _B = C.POINTER(C.c_uint8)
+        L.qmo_percentile_table.argtypes = [C.c_int, C.POINTER(C.c_float)]
+        L.qmo_percentile_table.restype = None
         L.qmo_ground_attenuation_bands.argtypes = [C.c_double] * 9 + [C.c_int, _D]
         L.qmo_ground_attenuation_bands.restype = None
         L.qmo_path_difference.argtypes = [C.c_int, C.c_double, _D, _D, _D, _D, C.c_size_t, _D]
@@ -300,6 +302,14 @@ def level_histogram(levels, level_min, bin_db, n_bins):
 
 def level_bin(level, level_min, bin_db, n_bins):
     return lib().qmo_level_bin(level, level_min, bin_db, n_bins)
+
+
+def percentile_table(n_rows=41):
+    """The line-source quantile table by the reference's own seeded simulation
+    (physics/src/percentile_tests.rs:1-102): float32 [n_rows][100]."""
+    out = np.zeros((n_rows, 100), np.float32)
+    lib().qmo_percentile_table(n_rows, abi.ptr(out, C.c_float))
+    return out
 
 
 def ground_attenuation_bands(plane, source, receiver, g_path, g_impedance, g_floor, state):

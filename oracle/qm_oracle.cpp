@@ -1942,6 +1942,75 @@ void qmo_ground_attenuation_bands(double slope, double intercept, double sx, dou
 }
 
 // ---------------------------------------------------------------------------------------------
+// The quantile table of a line of Poisson emitters (Kurze 1971), as the reference generates it
+// (physics/src/percentile_tests.rs:1-102, physics/src/percentile.rs:11-21): one SplitMix64 stream
+// over the rows in order; per sample a Poisson count of emitters uniform on the simulated length,
+// their intensities 1 / (1 + x^2) summed with the mean of those beyond, over the line's mean;
+// each row's samples sorted and read at probabilities (k + 0.5) / 100.
+
+namespace {
+
+struct SplitMix64 {  // percentile_tests.rs:5-21
+    uint64_t state;
+    double uniform() {
+        state += 0x9e3779b97f4a7c15ull;
+        uint64_t z = state;
+        z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
+        z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
+        return (double)((z ^ (z >> 31)) >> 11) / (double)(1ull << 53);
+    }
+};
+
+size_t percentile_poisson(SplitMix64 &random, double mean) {  // percentile_tests.rs:34-47
+    const double pi = 3.14159265358979323846;
+    if (mean > 50.0) {
+        const double a = std::sqrt(-2.0 * std::log(1.0 - random.uniform()));
+        const double normal = a * std::cos(2.0 * pi * random.uniform());
+        return (size_t)std::max(std::round(mean + std::sqrt(mean) * normal), 0.0);
+    }
+    const double limit = std::exp(-mean);
+    size_t count = 0;
+    double product = random.uniform();
+    while (product > limit) {
+        ++count;
+        product *= random.uniform();
+    }
+    return count;
+}
+
+}  // namespace
+
+// Rows [0, n_rows) of the table (row r at lambda = 1e-4 * 10^(r / 8)), each QUANTILES = 100
+// values rounded to float as the table stores them: table[n_rows][100]. Rows are generated in
+// order from the seed, so any row needs the ones before it.
+void qmo_percentile_table(int n_rows, float *table) {
+    const double pi = 3.14159265358979323846;
+    SplitMix64 random{0x5eed1971ull};
+    std::vector<double> samples;
+    for (int row = 0; row < n_rows; ++row) {
+        const double lambda = 1e-4 * std::pow(10.0, (double)row / 8.0);
+        const double half_length = std::max(5.0 / lambda, 200.0);            // percentile_tests.rs:31-33
+        const size_t count = (size_t)std::min(20000.0 * std::max(0.01 / lambda, 1.0), 1000000.0);
+        const double mean_inside = lambda * 2.0 * half_length;
+        const double outside = lambda * 2.0 * (pi / 2.0 - std::atan(half_length));
+        const double mean = lambda * pi;
+        samples.resize(count);
+        for (size_t i = 0; i < count; ++i) {
+            const size_t emitters = percentile_poisson(random, mean_inside);
+            double inside = 0.0;
+            for (size_t e = 0; e < emitters; ++e) {
+                const double x = (2.0 * random.uniform() - 1.0) * half_length;
+                inside += 1.0 / (1.0 + x * x);
+            }
+            samples[i] = (inside + outside) / mean;
+        }
+        std::sort(samples.begin(), samples.end());
+        for (int k = 0; k < 100; ++k)
+            table[row * 100 + k] = (float)samples[(size_t)(((double)k + 0.5) / 100.0 * (double)count)];
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
 // The state rays and the rubber band on their own (physics/src/cnossos/rubber_band.rs), for the
 // reference's rubber-band tests. Points are (x, z) pairs; state 0 homogeneous, 1 favourable; a
 // radius_m <= 0 takes the state ray between source and receiver (`StateRay::between`).
