@@ -69,6 +69,8 @@ def lib():
         _B = C.POINTER(C.c_uint8)
         L.qmo_percentile_table.argtypes = [C.c_int, C.POINTER(C.c_float)]
         L.qmo_percentile_table.restype = None
+        L.qmo_relative_intensities.argtypes = [C.c_double, _D, C.c_size_t, _D]
+        L.qmo_relative_intensities.restype = None
         L.qmo_ground_attenuation_bands.argtypes = [C.c_double] * 9 + [C.c_int, _D]
         L.qmo_ground_attenuation_bands.restype = None
         L.qmo_path_difference.argtypes = [C.c_int, C.c_double, _D, _D, _D, _D, C.c_size_t, _D]
@@ -310,6 +312,15 @@ def percentile_table(n_rows=41):
     out = np.zeros((n_rows, 100), np.float32)
     lib().qmo_percentile_table(n_rows, abi.ptr(out, C.c_float))
     return out
+
+
+def relative_intensity(lam, p):
+    """The intensity, relative to its mean, a line of `lam` emitters per distance stays below with
+    probability p (physics/src/percentile.rs:124-160); p a scalar or an array."""
+    arr = np.ascontiguousarray(np.atleast_1d(np.asarray(p, dtype=np.float64)))
+    out = np.zeros_like(arr)
+    lib().qmo_relative_intensities(float(lam), abi.ptr(arr, C.c_double), len(arr), abi.ptr(out, C.c_double))
+    return out if np.ndim(p) else float(out[0])
 
 
 def ground_attenuation_bands(plane, source, receiver, g_path, g_impedance, g_floor, state):

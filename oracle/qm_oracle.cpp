@@ -2010,6 +2010,83 @@ void qmo_percentile_table(int n_rows, float *table) {
     }
 }
 
+// The sampler over that table (physics/src/percentile.rs:27-160): the intensity, relative to its
+// mean, that a line of `lambda` emitters per distance stays below with probability p.
+
+namespace {
+
+const float *percentile_rows() {  // the 41 x 100 table, from the simulation above, made once
+    static const std::vector<float> table = [] {
+        std::vector<float> t(41 * 100);
+        qmo_percentile_table(41, t.data());
+        return t;
+    }();
+    return table.data();
+}
+
+// The standard normal quantile by Acklam's rational approximation (percentile.rs:27-71).
+double normal_quantile(double p) {
+    static const double A[6] = {-3.969683028665376e1, 2.209460984245205e2, -2.759285104469687e2,
+                                1.38357751867269e2,   -3.066479806614716e1, 2.506628277459239};
+    static const double B[5] = {-5.447609879822406e1, 1.615858368580409e2, -1.556989798598866e2,
+                                6.680131188771972e1, -1.328068155288572e1};
+    static const double C[6] = {-7.784894002430293e-3, -3.223964580411365e-1, -2.400758277161838,
+                                -2.549671010366478,    4.374664141464968,     2.938163982698783};
+    static const double D[4] = {7.784695709041462e-3, 3.224671290700398e-1, 2.445134137142996, 3.754408661907416};
+    auto tail = [&](double q) {
+        return (((((C[0] * q + C[1]) * q + C[2]) * q + C[3]) * q + C[4]) * q + C[5]) /
+               ((((D[0] * q + D[1]) * q + D[2]) * q + D[3]) * q + 1.0);
+    };
+    if (p < 0.02425) return tail(std::sqrt(-2.0 * std::log(p)));
+    if (p > 1.0 - 0.02425) return -tail(std::sqrt(-2.0 * std::log(1.0 - p)));
+    const double q = p - 0.5, r = q * q;
+    return (((((A[0] * r + A[1]) * r + A[2]) * r + A[3]) * r + A[4]) * r + A[5]) * q /
+           (((((B[0] * r + B[1]) * r + B[2]) * r + B[3]) * r + B[4]) * r + 1.0);
+}
+
+double quantile_probability(int k) { return ((double)k + 0.5) / 100.0; }
+
+double relative_intensity(double lambda, double p) {
+    const double pi = 3.14159265358979323846, lambda_min = 1e-4;
+    if (!std::isfinite(lambda)) return 1.0;
+    if (lambda <= 0.0) return 0.0;
+    const double bottom = quantile_probability(0), top = quantile_probability(99);
+    auto passing = [&](double ln_p) {  // percentile.rs:77-80
+        const double s = -ln_p / (2.0 * lambda);
+        return 1.0 / (lambda * pi * (1.0 + s * s));
+    };
+    if (lambda >= 10.0) {  // percentile.rs:83-86: a dense line is normal
+        const double deviation = 1.0 / std::sqrt(2.0 * pi * lambda);
+        return std::max(1.0 + deviation * normal_quantile(std::min(std::max(p, bottom), top)), 0.0);
+    }
+    if (p > top) return relative_intensity(lambda, top) + passing(std::log(p)) - passing(std::log(top));
+    if (lambda < lambda_min) return lambda / lambda_min * relative_intensity(lambda_min, p);
+    // table_position (percentile.rs:89-93)
+    const double position = std::min(std::max(std::log10(lambda / lambda_min) * 8.0, 0.0), 40.0);
+    const int row = (int)std::floor(position);
+    const double fraction = position - std::trunc(position);
+    // quantile_position (percentile.rs:97-104)
+    const double pq = std::max(p, bottom);
+    const int k = std::min((int)std::floor(pq * 100.0 - 0.5), 98);
+    const double t = (std::log(1.0 - pq) - std::log(1.0 - quantile_probability(k))) /
+                     (std::log(1.0 - quantile_probability(k + 1)) - std::log(1.0 - quantile_probability(k)));
+    const float *table = percentile_rows();
+    auto log_quantile = [&](int r) {  // percentile.rs:107-114
+        const double here = std::log(std::max((double)table[r * 100 + k], 1e-30));
+        const double next = std::log(std::max((double)table[r * 100 + k + 1], 1e-30));
+        return here + t * (next - here);
+    };
+    const double low = log_quantile(row), high = log_quantile(std::min(row + 1, 40));
+    return std::exp(low + fraction * (high - low));
+}
+
+}  // namespace
+
+// relative_intensity at n probabilities for one lambda: out[n].
+void qmo_relative_intensities(double lambda, const double *p, size_t n, double *out) {
+    for (size_t i = 0; i < n; ++i) out[i] = relative_intensity(lambda, p[i]);
+}
+
 // ---------------------------------------------------------------------------------------------
 // The state rays and the rubber band on their own (physics/src/cnossos/rubber_band.rs), for the
 // reference's rubber-band tests. Points are (x, z) pairs; state 0 homogeneous, 1 favourable; a
