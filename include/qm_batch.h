@@ -236,6 +236,21 @@ qm_status qm_hm3_predict(qm_ctx *ctx, const uint8_t *cells, const uint8_t *layer
 qm_status qm_hm3_unpredict(const uint8_t *stream, size_t n_bytes, uint32_t layer, int metric,
                            uint8_t *cells);
 
+/* How a line of moving emitters' level varies in time (Kurze 1971; physics/src/percentile.rs):
+ * a line with `lambda` emitters per distance of its closest point stays below
+ * out[k] = its intensity relative to the mean with probability p[k] (0 < p < 1), for n pairs
+ * (lambda[k], p[k]), computed on the device in FP64. Dense lines (lambda >= 10) are normal;
+ * below that the 41 x 100 quantile table is read log-linearly between rows and in log(1 - p)
+ * between quantiles, with the nearest emitter's passing above the last quantile; lambda 0 is
+ * silence, an infinite lambda a steady source (1). The table is the reference's simulation
+ * (physics/src/percentile_tests.rs:1-102) run by this library on its first use (a few seconds). */
+qm_status qm_line_level_quantiles(qm_ctx *ctx, const double *lambda, const double *p, size_t n,
+                                  double *out);
+
+/* That table, 41 rows (lambda = 1e-4 * 10^(row / 8)) of 100 quantiles (probabilities
+ * (k + 0.5) / 100) of the intensity relative to the mean, as floats: table[41 * 100]. Host only. */
+qm_status qm_line_level_table(float *table);
+
 /* The obstacle crossings of n rays from (from_xy) to (to_xy), lattice steps: per ray its count
  * (counts[n]) and, up to `cap` per ray, the crossed edges (the edge's first vertex index),
  * chainages t (f64) and flags (bit 0 building, bit 1 bounds_roof), sorted and deduplicated as

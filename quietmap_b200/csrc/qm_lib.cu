@@ -31,6 +31,7 @@
 #include "qm_aircraft.cuh"
 #include "qm_kernels.cuh"
 #include "qm_mlp.h"
+#include "qm_percentile.cuh"
 #include "qm_surrogate.cuh"
 #include "qm_tiles.cuh"
 
@@ -52,6 +53,7 @@ struct qm_ctx {
     // Scenes and networks made on the context hold it: qm_close releases it once they are freed.
     int children = 0;
     bool closed = false;
+    float *line_table = nullptr;  // the line-level quantile table on the device, on first use
 };
 
 struct DeviceBuffer {
@@ -99,6 +101,7 @@ qm_status fail(qm_status status, const std::string &message) {
 
 void ctx_destroy(qm_ctx *ctx) {
     cudaSetDevice(ctx->device);
+    if (ctx->line_table) cudaFree(ctx->line_table);
     cudaStreamDestroy(ctx->stream);
     delete ctx;
 }
@@ -3157,6 +3160,118 @@ qm_status qm_terrain_fine_decode(const uint8_t *bytes, size_t n_bytes, qm_terrai
             }
         }
     }
+    return QM_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------------------------
+// Line-source levels in time (physics/src/percentile.rs). The quantile table is made here by the
+// reference's own seeded simulation (physics/src/percentile_tests.rs:1-102): one SplitMix64
+// stream over the rows in order, per sample a Poisson count of emitters uniform on the simulated
+// length, their intensities 1 / (1 + x^2) summed with the mean of those beyond, over the line's
+// mean; each row's samples sorted and read at probabilities (k + 0.5) / 100.
+
+namespace {
+
+struct LineLevelRandom {
+    uint64_t state;
+    double uniform() {
+        state += 0x9e3779b97f4a7c15ull;
+        uint64_t z = state;
+        z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
+        z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
+        return (double)((z ^ (z >> 31)) >> 11) / (double)(1ull << 53);
+    }
+    size_t poisson(double mean) {  // a normal approximation above a mean of 50
+        const double pi = 3.14159265358979323846;
+        if (mean > 50.0) {
+            const double radius = std::sqrt(-2.0 * std::log(1.0 - uniform()));
+            const double normal = radius * std::cos(2.0 * pi * uniform());
+            return (size_t)std::max(std::round(mean + std::sqrt(mean) * normal), 0.0);
+        }
+        const double limit = std::exp(-mean);
+        size_t count = 0;
+        double product = uniform();
+        while (product > limit) {
+            ++count;
+            product *= uniform();
+        }
+        return count;
+    }
+};
+
+const std::vector<float> &line_level_table() {
+    static const std::vector<float> table = [] {
+        const double pi = 3.14159265358979323846;
+        std::vector<float> t((size_t)LINE_LEVEL_ROWS * LINE_LEVEL_QUANTILES);
+        LineLevelRandom random{0x5eed1971ull};
+        std::vector<double> samples;
+        for (int row = 0; row < LINE_LEVEL_ROWS; ++row) {
+            const double lambda = LINE_LEVEL_LAMBDA_MIN * std::pow(10.0, (double)row / LINE_LEVEL_STEPS_PER_DECADE);
+            // At least 200 distances each side and ten emitters on average; 20,000 samples, up to
+            // a million for sparse lines whose upper quantiles rest on rare passes.
+            const double half_length = std::max(5.0 / lambda, 200.0);
+            const size_t count = (size_t)std::min(20000.0 * std::max(0.01 / lambda, 1.0), 1000000.0);
+            const double mean_inside = lambda * 2.0 * half_length;
+            const double outside = lambda * 2.0 * (pi / 2.0 - std::atan(half_length));
+            const double mean = lambda * pi;
+            samples.resize(count);
+            for (size_t i = 0; i < count; ++i) {
+                const size_t emitters = random.poisson(mean_inside);
+                double inside = 0.0;
+                for (size_t e = 0; e < emitters; ++e) {
+                    const double x = (2.0 * random.uniform() - 1.0) * half_length;
+                    inside += 1.0 / (1.0 + x * x);
+                }
+                samples[i] = (inside + outside) / mean;
+            }
+            std::sort(samples.begin(), samples.end());
+            for (int k = 0; k < LINE_LEVEL_QUANTILES; ++k)
+                t[(size_t)row * LINE_LEVEL_QUANTILES + k] =
+                    (float)samples[(size_t)(((double)k + 0.5) / LINE_LEVEL_QUANTILES * (double)count)];
+        }
+        return t;
+    }();
+    return table;
+}
+
+}  // namespace
+
+extern "C" {
+
+qm_status qm_line_level_table(float *table) {
+    if (!table) return fail(QM_ERR_ARGUMENT, "qm_line_level_table: null table");
+    const std::vector<float> &t = line_level_table();
+    std::memcpy(table, t.data(), t.size() * sizeof(float));
+    return QM_OK;
+}
+
+qm_status qm_line_level_quantiles(qm_ctx *ctx, const double *lambda, const double *p, size_t n, double *out) {
+    if (!ctx) return fail(QM_ERR_ARGUMENT, "qm_line_level_quantiles: null ctx");
+    if (n == 0) return QM_OK;
+    if (!lambda || !p || !out) return fail(QM_ERR_ARGUMENT, "qm_line_level_quantiles: null lambda, p or out");
+    const std::vector<float> &table = line_level_table();
+    std::lock_guard<std::mutex> guard(ctx->lock);
+    QM_CUDA(cudaSetDevice(ctx->device));
+    cudaStream_t stream = ctx->stream;
+    if (!ctx->line_table) {
+        QM_CUDA(cudaMalloc(&ctx->line_table, table.size() * sizeof(float)));
+        QM_CUDA(cudaMemcpyAsync(ctx->line_table, table.data(), table.size() * sizeof(float), cudaMemcpyHostToDevice,
+                                stream));
+    }
+    Scratch d_lambda, d_p, d_out;
+    QM_CUDA(cudaMalloc(&d_lambda.p, n * sizeof(double)));
+    QM_CUDA(cudaMalloc(&d_p.p, n * sizeof(double)));
+    QM_CUDA(cudaMalloc(&d_out.p, n * sizeof(double)));
+    QM_CUDA(cudaMemcpyAsync(d_lambda.p, lambda, n * sizeof(double), cudaMemcpyHostToDevice, stream));
+    QM_CUDA(cudaMemcpyAsync(d_p.p, p, n * sizeof(double), cudaMemcpyHostToDevice, stream));
+    const unsigned blocks = (unsigned)std::min<size_t>((n + 255) / 256, (size_t)ctx->sm_count * 8);
+    line_level_kernel<<<blocks, 256, 0, stream>>>(ctx->line_table, static_cast<const double *>(d_lambda.p),
+                                                  static_cast<const double *>(d_p.p), n, static_cast<double *>(d_out.p));
+    QM_CUDA(cudaGetLastError());
+    QM_CUDA(cudaMemcpyAsync(out, d_out.p, n * sizeof(double), cudaMemcpyDeviceToHost, stream));
+    QM_CUDA(cudaStreamSynchronize(stream));
     return QM_OK;
 }
 

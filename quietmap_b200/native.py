@@ -62,6 +62,10 @@ def lib():
         L.qm_quantize_cells.restype = C.c_int
         L.qm_hm3_predict.argtypes = [C.c_void_p, _U8, _U8, C.c_size_t, C.c_int, _U8]
         L.qm_hm3_predict.restype = C.c_int
+        L.qm_line_level_table.argtypes = [C.POINTER(C.c_float)]
+        L.qm_line_level_table.restype = C.c_int
+        L.qm_line_level_quantiles.argtypes = [C.c_void_p, _D, _D, C.c_size_t, _D]
+        L.qm_line_level_quantiles.restype = C.c_int
         L.qm_hm3_unpredict.argtypes = [_U8, C.c_size_t, C.c_uint32, C.c_int, _U8]
         L.qm_hm3_unpredict.restype = C.c_int
         L.qm_obstacles_check.argtypes = [_U8, C.c_size_t, C.POINTER(abi.ObstaclesCounts)]
@@ -213,6 +217,16 @@ class Context:
                                     abi.ptr(out, C.c_uint8)), self.handle)
         return out
 
+    def line_level_quantiles(self, lam, p):
+        """The intensity, relative to its mean, a line of `lam` emitters per distance stays below
+        with probability p, on the device (qm_line_level_quantiles); arrays broadcast together."""
+        lam_b, p_b = np.broadcast_arrays(np.asarray(lam, dtype=np.float64), np.asarray(p, dtype=np.float64))
+        lam_c, p_c = np.ascontiguousarray(lam_b.ravel()), np.ascontiguousarray(p_b.ravel())
+        out = np.zeros(lam_c.size)
+        _check(lib().qm_line_level_quantiles(self.handle, abi.ptr(lam_c, C.c_double), abi.ptr(p_c, C.c_double),
+                                             lam_c.size, abi.ptr(out, C.c_double)), self.handle)
+        return out.reshape(lam_b.shape)
+
     def level_histogram(self, levels_db, level_min_db=-30.0, bin_db=0.1, n_bins=1800):
         levels = np.ascontiguousarray(levels_db, dtype=np.float32).ravel()
         counts = np.zeros(n_bins, np.uint32)
@@ -224,6 +238,13 @@ class Context:
 def _tile_bytes(data):
     b = np.frombuffer(bytes(data), dtype=np.uint8)
     return b, abi.ptr(b, C.c_uint8) if len(b) else None
+
+
+def line_level_table():
+    """The library's line-level quantile table (qm_line_level_table): float32 [41][100]."""
+    out = np.zeros((41, 100), np.float32)
+    _check(lib().qm_line_level_table(abi.ptr(out, C.c_float)))
+    return out
 
 
 def hm3_unpredict(stream, layer, metric):

@@ -91,3 +91,8 @@ def test_independent_sparse_lines_add_up_to_a_denser_one():
             sampled = sums[int((1.0 - exceeded) * len(sums))]
             one = oracle.relative_intensity(lam * lines, 1.0 - exceeded)
             assert abs(10.0 * np.log10(sampled / one)) < 0.3, (lines, lam, exceeded)
+
+
+def test_the_library_builds_the_same_table(table):
+    from quietmap_b200 import native
+    np.testing.assert_array_equal(native.line_level_table(), table)
