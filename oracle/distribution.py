@@ -1,0 +1,194 @@
+"""How levels add over time (popup/src/distribution.rs), restated in Python — TEST INFRASTRUCTURE
+ONLY.
+
+A distribution of the summed level over a period on a grid of bin_db decibels from -30 dB over
+180 dB: per bin its share of the time and that share times its moments' mean intensity, so that
+adding an independent sound loses no energy to the grid; silence apart. A line's values are its
+intensities relative to its mean at fixed probabilities with the share of the time each stands
+for (Kurze's quantiles, `oracle.relative_intensity`), an event's mean over its duty, or a
+Poisson stream of passes. Only tests import this module.
+"""
+
+import bisect
+import math
+
+from oracle import oracle
+
+LEVEL_MIN_DB = -30.0   # distribution.rs:11
+SPAN_DB = 180.0        # distribution.rs:12
+LN_10 = 2.302585092994046
+
+
+def energy(level_db):
+    """physics/src/bands.rs:34-36."""
+    return math.exp(level_db * (LN_10 / 10.0))
+
+
+def _round_half_away(x):
+    f = math.floor(x)
+    return f + 1.0 if x - f >= 0.5 else f
+
+
+def node_probabilities():
+    """distribution.rs:17-32: every percent to 0.99, then evenly in log(1 - p) to 1 - 1e-8, each
+    with the share of the time it stands for."""
+    nodes = [((k + 0.5) / 100.0, 0.01) for k in range(99)]
+    at = lambda t: 1.0 - 10.0 ** (-t)
+    for k in range(24):
+        a, b = 2.0 + k * 0.25, 2.25 + k * 0.25
+        nodes.append((at((a + b) / 2.0), at(b) - at(a)))
+    nodes.append((1.0 - 0.5e-8, 1e-8))
+    return nodes
+
+
+class LineValues:
+    """Intensities with their shares of the time, ascending, and the running sums of the shares
+    and of the shares times the intensities (distribution.rs:236-262)."""
+
+    def __init__(self, pairs):
+        self.pairs = sorted(((float(v), float(s)) for v, s in pairs), key=lambda p: p[0])
+        self.values = [v for v, _ in self.pairs]
+        self.sums = [(0.0, 0.0)]
+        for value, share in self.pairs:
+            shares, weighted = self.sums[-1]
+            self.sums.append((shares + share, weighted + share * value))
+
+
+def line_values(lam, duty=None):
+    """distribution.rs:264-281: Kurze's quantiles at `lam` at the nodes, or an event's mean over
+    its duty while it sounds and silence otherwise."""
+    if duty is not None:
+        return LineValues([(0.0, 1.0 - duty), (1.0 / duty, duty)])
+    nodes = node_probabilities()
+    values = oracle.relative_intensity(lam, [p for p, _ in nodes])
+    return LineValues(list(zip(values, [s for _, s in nodes])))
+
+
+def pass_values(mean):
+    """distribution.rs:283-298: passes of one level, a Poisson number `mean` in progress on
+    average, each at the stream's mean over `mean`; the numbers up to the one a moment in 1e12
+    exceeds, which takes what is left of the time and of the mean."""
+    share = math.exp(-mean)
+    pairs = [(0.0, share)]
+    time_left, mean_left = -math.expm1(-mean), 1.0
+    count = 0.0
+    while True:
+        count += 1.0
+        share *= mean / count
+        if time_left - share <= 1e-12:
+            pairs.append((mean_left / time_left, time_left))
+            return LineValues(pairs)
+        time_left -= share
+        mean_left -= share * count / mean
+        pairs.append((count / mean, share))
+
+
+class Distribution:
+    """distribution.rs:44-221."""
+
+    def __init__(self, bin_db):
+        self.silent = 0.0
+        self.bin_db = bin_db
+        self.bins = [[0.0, 0.0] for _ in range(int(_round_half_away(SPAN_DB / bin_db)))]
+
+    def bin_count(self):
+        return len(self.bins)
+
+    def bin(self, level_db):
+        """The bin of a level; one under the grid is held in its lowest bin (distribution.rs:69-73)."""
+        x = (level_db - LEVEL_MIN_DB) / self.bin_db
+        index = 0 if math.isnan(x) else max(_round_half_away(x), 0.0)
+        return int(min(index, len(self.bins) - 1))
+
+    def intensities(self):
+        """Each bin holding time: its moments' mean intensity and its share."""
+        return [(weighted / share, share) for share, weighted in self.bins if share > 0.0]
+
+    def runs(self, intensity, line, scale, visit):
+        """The bins a moment at `intensity` moves to with each of the line's values times `scale`
+        added (`None`: silence), each visited once in increasing order with the shares of the
+        values that take it there and their shares times their values (distribution.rs:91-145)."""
+        pairs, sums, values = line.pairs, line.sums, line.values
+
+        def run(a, b):
+            return (sums[b][0] - sums[a][0], scale * (sums[b][1] - sums[a][1]))
+
+        start = 0
+        if intensity <= 0.0:
+            start = bisect.bisect_right(values, 0.0)
+            if start > 0:
+                visit(None, run(0, start))
+        if start == len(pairs):
+            return
+        last = len(self.bins) - 1
+        step = energy(self.bin_db)
+        b = self.bin(10.0 * math.log10(intensity + scale * pairs[start][0]))
+        ceiling = energy(LEVEL_MIN_DB + (b + 0.5) * self.bin_db)
+        while True:
+            if b == last:
+                to = len(pairs)
+            else:
+                to = bisect.bisect_left(values, (ceiling - intensity) / scale, start + 1)
+            visit(b, run(start, to))
+            start = to
+            if start >= len(pairs):
+                break
+            value = pairs[start][0]
+            while True:
+                b += 1
+                ceiling *= step
+                if b == last or intensity + scale * value < ceiling:
+                    break
+
+    def exceeded_db(self, exceeded):
+        """The level exceeded `exceeded` of the time (distribution.rs:152-162)."""
+        above = 0.0
+        for share, weighted in reversed(self.bins):
+            above += share
+            if share > 0.0 and above > exceeded * (1.0 - 1e-12):
+                return 10.0 * math.log10(weighted / share)
+        return -math.inf
+
+    def with_line(self, line, scale=1.0):
+        """This distribution with an independent line (values times `scale`) added at every moment
+        (distribution.rs:176-196)."""
+        out = Distribution(self.bin_db)
+
+        def add(intensity, share):
+            def visit(b, sums):
+                shares, weighted = sums
+                if b is None:
+                    out.silent += share * shares
+                else:
+                    out.bins[b][0] += share * shares
+                    out.bins[b][1] += share * (intensity * shares + weighted)
+            self.runs(intensity, line, scale, visit)
+
+        if self.silent > 0.0:
+            add(0.0, self.silent)
+        for intensity, share in self.intensities():
+            add(intensity, share)
+        return out
+
+    def with_distribution(self, other):
+        """This with an independent `other` added: its levels as a line's values, its silence a
+        value of nothing (distribution.rs:198-206)."""
+        values = [(i, s) for i, s in other.intensities()] + [(0.0, other.silent)]
+        return self.with_line(LineValues([(i, s) for i, s in values if s > 0.0]))
+
+    def over(self, intensity):
+        """With a steady intensity added at every moment."""
+        return self.with_line(LineValues([(intensity, 1.0)]))
+
+    def add_scaled(self, other, weight):
+        self.silent += other.silent * weight
+        for into, source in zip(self.bins, other.bins):
+            into[0] += source[0] * weight
+            into[1] += source[1] * weight
+
+    @staticmethod
+    def of_levels(levels, bin_db=0.5):
+        """A distribution of given levels (dB, -inf silent) with their shares of the time."""
+        silence = Distribution(bin_db)
+        silence.silent = 1.0
+        return silence.with_line(LineValues([(10.0 ** (level / 10.0), share) for level, share in levels]))
