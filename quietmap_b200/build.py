@@ -11,7 +11,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libqm_b200.so")
-SOURCES = ["qm_lib.cu", "qm_zwicker.cu", "qm_mlp.cu"]
+SOURCES = ["qm_lib.cu", "qm_zwicker.cu", "qm_mlp.cu", "qm_formats.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-O2",
          "--expt-relaxed-constexpr", "-rdc=false"]
@@ -36,7 +36,7 @@ def build(force=False, verbose=False):
         return LIB
     objs = []
     for src in SOURCES:
-        obj = os.path.join(CSRC, "_" + src.replace(".cu", ".o"))
+        obj = os.path.join(CSRC, "_" + os.path.splitext(src)[0] + ".o")
         cmd = [nvcc(), *ARCH, *FLAGS, "-c", os.path.join(CSRC, src), "-o", obj]
         if verbose:
             cmd.insert(1, "-Xptxas=-v")
