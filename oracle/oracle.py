@@ -73,6 +73,12 @@ def lib():
         L.qmo_relative_intensities.restype = None
         L.qmo_ground_attenuation_bands.argtypes = [C.c_double] * 9 + [C.c_int, _D]
         L.qmo_ground_attenuation_bands.restype = None
+        for name in ("qmo_crossings_d", "qmo_crossings_every"):
+            f = getattr(L, name)
+            f.argtypes = [C.c_void_p, _D, _D, _D, _U64, _U32, C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.c_size_t]
+            f.restype = C.c_size_t
+        L.qmo_profile_d.argtypes = [C.c_void_p, _D, _D, _D, _D, _D, C.c_size_t, _D]
+        L.qmo_profile_d.restype = C.c_size_t
         L.qmo_path_difference.argtypes = [C.c_int, C.c_double, _D, _D, _D, _D, C.c_size_t, _D]
         L.qmo_path_difference.restype = C.c_double
         L.qmo_diffraction_path.argtypes = [C.c_int, C.c_double, _D, _D, _D, C.c_size_t, _D,
@@ -213,6 +219,41 @@ class OracleScene:
         n = min(n, cap)
         return dict(t=t[:n].copy(), footprint=fp[:n].copy(), edge=edge[:n].copy(),
                     bounds_roof=br[:n].astype(bool), building=bd[:n].astype(bool))
+
+    def _crossings_f64(self, fn, frm, to, cap=4096):
+        frm = np.ascontiguousarray(frm, dtype=np.float64)
+        to = np.ascontiguousarray(to, dtype=np.float64)
+        t = np.zeros(cap)
+        fp = np.zeros(cap, np.uint64)
+        edge = np.zeros(cap, np.uint32)
+        br = np.zeros(cap, np.int32)
+        bd = np.zeros(cap, np.int32)
+        n = fn(self.handle, abi.ptr(frm, C.c_double), abi.ptr(to, C.c_double), abi.ptr(t, C.c_double),
+               abi.ptr(fp, C.c_uint64), abi.ptr(edge, C.c_uint32), abi.ptr(br, C.c_int32), abi.ptr(bd, C.c_int32),
+               cap)
+        n = min(n, cap)
+        return dict(t=t[:n].copy(), footprint=fp[:n].copy(), edge=edge[:n].copy(),
+                    bounds_roof=br[:n].astype(bool), building=bd[:n].astype(bool))
+
+    def crossings_f64(self, frm, to):
+        """The walk's crossing list for ends anywhere (f64 steps)."""
+        return self._crossings_f64(lib().qmo_crossings_d, frm, to)
+
+    def crossings_every(self, frm, to):
+        """Every edge against the ray with the walk's deduplication: the list the walk must give."""
+        return self._crossings_f64(lib().qmo_crossings_every, frm, to)
+
+    def profile_f64(self, frm, to, cap=65536):
+        """The ground profile under a ray with ends anywhere: (horizontal metres, t, altitude, G), as
+        `profile` gives it."""
+        frm = np.ascontiguousarray(frm, dtype=np.float64)
+        to = np.ascontiguousarray(to, dtype=np.float64)
+        t, z, g = np.zeros(cap), np.zeros(cap), np.zeros(cap)
+        h = np.zeros(1)
+        n = lib().qmo_profile_d(self.handle, abi.ptr(frm, C.c_double), abi.ptr(to, C.c_double), abi.ptr(t, C.c_double),
+                                abi.ptr(z, C.c_double), abi.ptr(g, C.c_double), cap, abi.ptr(h, C.c_double))
+        n = min(n, cap)
+        return float(h[0]), t[:n].copy(), z[:n].copy(), g[:n].copy()
 
     def enclosing(self, xy):
         xy = np.ascontiguousarray(np.asarray(xy).reshape(-1, 2), dtype=np.int64)

@@ -1001,11 +1001,11 @@ bool edge_bounds_roof(const Scene &s, const double start[2], const double delta[
 }
 
 // popup/src/obstacles/crossings.rs:163-226, over the scene's one uniform grid.
-void scene_crossings(const Scene &s, const int64_t from[2], const int64_t to[2], std::vector<Crossing> &out,
+void scene_crossings(const Scene &s, const double from[2], const double to[2], std::vector<Crossing> &out,
                      uint64_t *edges_tested = nullptr) {
     out.clear();
-    double start[2] = {(double)from[0], (double)from[1]};
-    double end[2] = {(double)to[0], (double)to[1]};
+    double start[2] = {from[0], from[1]};
+    double end[2] = {to[0], to[1]};
     double delta[2] = {end[0] - start[0], end[1] - start[1]};
     double cell_steps = (double)s.cell_steps;
     int64_t cell[2] = {(int64_t)std::floor(start[0] / cell_steps), (int64_t)std::floor(start[1] / cell_steps)};
@@ -1084,16 +1084,17 @@ void scene_crossings(const Scene &s, const int64_t from[2], const int64_t to[2],
     sort_and_deduplicate(out);
 }
 
-// The terrain at a lattice point (steps): bilinear between the four DEM nodes around it, as a
-// terrain sample is read at a ray's ends (popup/src/scene.rs:182-200).
-void terrain_at_point(const Scene &s, int64_t x, int64_t y, double &z, double &g) {
+// The terrain at a position (steps): bilinear between the four DEM nodes around it, clamped to
+// the DEM, as a terrain sample is read at a ray's ends (popup/src/scene.rs:182-200). A lattice
+// point's differences are exact in f64, so it reads as its integer form did.
+void terrain_at(const Scene &s, double x, double y, double &z, double &g) {
     if (s.dem_nx == 0) {
         z = s.flat_z;
         g = s.flat_g;
         return;
     }
-    double fx = (double)(x - s.dem_ox) / (double)s.dem_spacing;
-    double fy = (double)(y - s.dem_oy) / (double)s.dem_spacing;
+    double fx = (x - (double)s.dem_ox) / (double)s.dem_spacing;
+    double fy = (y - (double)s.dem_oy) / (double)s.dem_spacing;
     fx = std::min(std::max(fx, 0.0), (double)(s.dem_nx - 1));
     fy = std::min(std::max(fy, 0.0), (double)(s.dem_ny - 1));
     int64_t i0 = std::min<int64_t>((int64_t)std::floor(fx), s.dem_nx - 2);
@@ -1109,19 +1110,23 @@ void terrain_at_point(const Scene &s, int64_t x, int64_t y, double &z, double &g
     g = bil(s.dem_g);
 }
 
+void terrain_at_point(const Scene &s, int64_t x, int64_t y, double &z, double &g) {
+    terrain_at(s, (double)x, (double)y, z, g);
+}
+
 // The ground under a ray (popup/src/scene.rs:242-296 and walk :330-420, on one metric lattice):
 // both ends, and a vertex wherever the ray crosses a row or a column line of the DEM strictly
 // between them, in order; at a tie the row vertex comes first, then the column's at the same t.
-void fill_profile(const Scene &s, const int64_t from[2], const int64_t to[2], Profile &profile) {
-    double ox = (double)(from[0] - to[0]) * s.step_m, oy = (double)(from[1] - to[1]) * s.step_m;
+void fill_profile(const Scene &s, const double from[2], const double to[2], Profile &profile) {
+    double ox = (from[0] - to[0]) * s.step_m, oy = (from[1] - to[1]) * s.step_m;
     double length_m = std::hypot(ox, oy);
     profile.clear(std::max(length_m, 1.0));
     double z, g;
-    terrain_at_point(s, from[0], from[1], z, g);
+    terrain_at(s, from[0], from[1], z, g);
     profile.push(0.0, z, g);
     if (s.dem_nx != 0) {
-        double sx = (double)from[0], sy = (double)from[1];
-        double dx = (double)(to[0] - from[0]), dy = (double)(to[1] - from[1]);
+        double sx = from[0], sy = from[1];
+        double dx = to[0] - from[0], dy = to[1] - from[1];
         double sp = (double)s.dem_spacing;
         // Lattice line indices relative to the DEM origin.
         double cx = (sx - s.dem_ox) / sp, cy = (sy - s.dem_oy) / sp;
@@ -1161,7 +1166,7 @@ void fill_profile(const Scene &s, const int64_t from[2], const int64_t to[2], Pr
             }
         }
     }
-    terrain_at_point(s, to[0], to[1], z, g);
+    terrain_at(s, to[0], to[1], z, g);
     profile.push(1.0, z, g);
 }
 
@@ -1234,6 +1239,18 @@ struct Worker {
     std::vector<Crossing> crossings;
     RayScratch ray;
 };
+
+// The walks from and to lattice points (exact in f64, so these read as the f64 forms do).
+void scene_crossings(const Scene &s, const int64_t from[2], const int64_t to[2], std::vector<Crossing> &out,
+                     uint64_t *edges_tested = nullptr) {
+    const double f[2] = {(double)from[0], (double)from[1]}, t[2] = {(double)to[0], (double)to[1]};
+    scene_crossings(s, f, t, out, edges_tested);
+}
+
+void fill_profile(const Scene &s, const int64_t from[2], const int64_t to[2], Profile &profile) {
+    const double f[2] = {(double)from[0], (double)from[1]}, t[2] = {(double)to[0], (double)to[1]};
+    fill_profile(s, f, t, profile);
+}
 
 // One point source at one receiver: `source_rays` for a point and `add_ray`
 // (popup/src/evaluate.rs:119-152, 171-214, 300-330), `whole_energy` (paint/src/exact.rs:186-205).
@@ -1609,6 +1626,59 @@ size_t qmo_crossings(void *scene, const int64_t from[2], const int64_t to[2], do
     return out.size();
 }
 
+// The same for ends anywhere (f64 steps), as the reference's walk takes them off the lattice
+// (popup/src/obstacles/mod.rs:61-73).
+size_t qmo_crossings_d(void *scene, const double from[2], const double to[2], double *t, uint64_t *footprint,
+                       uint32_t *edge, int32_t *bounds_roof, int32_t *building, size_t cap) {
+    const Scene &s = *static_cast<Scene *>(scene);
+    std::vector<Crossing> out;
+    scene_crossings(s, from, to, out);
+    for (size_t i = 0; i < out.size() && i < cap; ++i) {
+        t[i] = out[i].t;
+        footprint[i] = out[i].footprint_id;
+        edge[i] = out[i].edge;
+        bounds_roof[i] = out[i].bounds_roof;
+        building[i] = out[i].building;
+    }
+    return out.size();
+}
+
+// Every edge of every outline against the ray, with the walk's deduplication: the list the walk
+// must give (the reference's own check of its walk, popup/src/obstacles/tests/mod.rs:198-229).
+size_t qmo_crossings_every(void *scene, const double from[2], const double to[2], double *t, uint64_t *footprint,
+                           uint32_t *edge, int32_t *bounds_roof, int32_t *building, size_t cap) {
+    const Scene &s = *static_cast<Scene *>(scene);
+    const double start[2] = {from[0], from[1]}, delta[2] = {to[0] - from[0], to[1] - from[1]};
+    std::vector<Crossing> out;
+    for (size_t o = 0; o < s.outlines.size(); ++o) {
+        const qm_outline &record = s.outlines[o];
+        for (uint32_t k = 0; k + 1 < record.vertex_count; ++k) {
+            const size_t e = record.first_vertex + k;
+            const double a[2] = {(double)s.vertices[2 * e], (double)s.vertices[2 * e + 1]};
+            const double b[2] = {(double)s.vertices[2 * e + 2], (double)s.vertices[2 * e + 3]};
+            double tt;
+            if (!segment_intersection_t(start, delta, a, b, tt)) continue;
+            Crossing cr;
+            cr.t = tt;
+            cr.height_m = record.height_m;
+            cr.building = record.building != 0;
+            cr.bounds_roof = cr.building && edge_bounds_roof(s, start, delta, e, record.first_vertex, record.vertex_count);
+            cr.footprint_id = record.footprint_id;
+            cr.edge = (uint32_t)e;
+            out.push_back(cr);
+        }
+    }
+    sort_and_deduplicate(out);
+    for (size_t i = 0; i < out.size() && i < cap; ++i) {
+        t[i] = out[i].t;
+        footprint[i] = out[i].footprint_id;
+        edge[i] = out[i].edge;
+        bounds_roof[i] = out[i].bounds_roof;
+        building[i] = out[i].building;
+    }
+    return out.size();
+}
+
 // The building enclosing each of n lattice points (0 none).
 void qmo_enclosing_buildings(void *scene, const int64_t *xy, size_t n, uint64_t *out, int threads) {
     const Scene &s = *static_cast<Scene *>(scene);
@@ -1618,6 +1688,21 @@ void qmo_enclosing_buildings(void *scene, const int64_t *xy, size_t n, uint64_t 
 // The ground profile under a ray (altitude and G at t): returns the count, capped writes.
 size_t qmo_profile(void *scene, const int64_t from[2], const int64_t to[2], double *t, double *z, double *g,
                    size_t cap, double *horizontal_m) {
+    const Scene &s = *static_cast<Scene *>(scene);
+    Profile p;
+    fill_profile(s, from, to, p);
+    *horizontal_m = p.horizontal_m;
+    for (size_t i = 0; i < p.t.size() && i < cap; ++i) {
+        t[i] = p.t[i];
+        z[i] = p.ground_m[i];
+        g[i] = p.ground_factor[i];
+    }
+    return p.t.size();
+}
+
+// The ground profile under a ray with ends anywhere (f64 steps).
+size_t qmo_profile_d(void *scene, const double from[2], const double to[2], double *t, double *z, double *g,
+                     size_t cap, double *horizontal_m) {
     const Scene &s = *static_cast<Scene *>(scene);
     Profile p;
     fill_profile(s, from, to, p);
