@@ -142,3 +142,20 @@ def test_the_library_restores_cells_from_a_stream():
             native.hm3_unpredict(data, layer, metric)
     with pytest.raises(native.QmError, match="unknown HM3 layer"):
         native.hm3_unpredict(stream, 7, 0)
+
+
+def test_every_byte_and_row_boundary_round_trips():
+    """paint/src/hm3_tests.rs:22-39 without its Brotli stage: the stream's residuals come back to
+    the cells; another layer or a cut stream is refused."""
+    from quietmap_b200 import native
+    at = np.arange(512 * 512)
+    cells = ((at // 512 * 19 + at % 512 * 31) % 256).astype(np.uint8).reshape(512, 512)
+    stream = oracle.hm3_predict(cells, 6, 0)
+    np.testing.assert_array_equal(native.hm3_unpredict(stream, 6, 0), cells)
+    np.testing.assert_array_equal(oracle.hm3_unpredict(stream[6:]), cells)
+    with pytest.raises(native.QmError):
+        native.hm3_unpredict(stream, 0, 0)
+    with pytest.raises(native.QmError):
+        native.hm3_unpredict(stream[:len(stream) // 2], 6, 0)
+    with pytest.raises(native.QmError):
+        native.hm3_unpredict(np.concatenate([stream, [0]]).astype(np.uint8), 6, 0)
