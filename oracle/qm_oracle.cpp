@@ -2235,6 +2235,89 @@ int qmo_line_geometry(const double *start, const double *end, double *out) {
     return 0;
 }
 
+// One straight line piece of a source at one receiver: `source_rays` for a line and `add_ray`
+// (popup/src/evaluate.rs:215-265, 118-152). The piece runs from a to b (steps, anywhere); its
+// ends stand on the terrain there plus the source's height; its quadrature nodes
+// (`line_nodes`, over the skyline arcs given) each send a ray from their point along the piece,
+// over the obstacles only where the mask says they can stand, weighted by the node's angle times
+// the line's divergence. `src.energy` is the power per metre of the piece.
+static int evaluate_line_piece(const Scene &s, const Receiver &r, const double a[2], const double b[2],
+                               const qm_source &src, const double *arcs, size_t n_arcs, Worker &w, PairResult &out) {
+    for (int period = 0; period < PERIODS; ++period) {
+        for (int b2 = 0; b2 < BANDS; ++b2) out.bands[period][b2] = 0.0;
+        for (int st = 0; st < 2; ++st) out.states[st][period] = 0.0;
+    }
+    double za, zb, ga, gb;
+    terrain_at(s, a[0], a[1], za, ga);
+    terrain_at(s, b[0], b[1], zb, gb);
+    const double start[3] = {(a[0] - (double)r.x) * s.step_m, (a[1] - (double)r.y) * s.step_m,
+                             za + src.height_m - r.altitude_m};
+    const double end[3] = {(b[0] - (double)r.x) * s.step_m, (b[1] - (double)r.y) * s.step_m,
+                           zb + src.height_m - r.altitude_m};
+    LinePiece g;
+    if (!g.make(start, end)) return 0;
+    std::vector<LineNode> nodes;
+    line_nodes(g, arcs, n_arcs, nodes);
+    const double divergence = g.divergence();
+    const double to[2] = {(double)r.x, (double)r.y};
+    for (const LineNode &node : nodes) {
+        const double fraction = node.along / g.length;
+        const double point[2] = {a[0] + fraction * (b[0] - a[0]), a[1] + fraction * (b[1] - a[1])};
+        fill_profile(s, point, to, w.profile);
+        w.crossings.clear();
+        if (node.on_ray) {
+            scene_crossings(s, point, to, w.crossings);
+            if (r.own_footprint != 0) {
+                size_t kept = 0;
+                for (size_t i = 0; i < w.crossings.size(); ++i)
+                    if (w.crossings[i].footprint_id != r.own_footprint) w.crossings[kept++] = w.crossings[i];
+                w.crossings.resize(kept);
+            }
+        }
+        const double azimuth = std::atan2(((double)r.y - point[1]) * s.step_m, ((double)r.x - point[0]) * s.step_m);
+        double p[PERIODS];
+        for (int period = 0; period < PERIODS; ++period) p[period] = favourable_at(s.favourable[period], azimuth);
+        RayEnds ends;
+        ends.source_height_m = src.height_m;
+        ends.has_source_ground = false;
+        ends.source_ground_m = 0.0;
+        ends.receiver_altitude_m = r.altitude_m;
+        ends.has_source_ground_factor = src.ground_factor >= 0.0f;
+        ends.source_ground_factor = src.ground_factor;
+        ends.platform_half_width_m = src.platform_half_width_m;
+        ends.own_footprint = src.footprint_id;
+        Transfer transfer;
+        StateBoundary boundaries[2];
+        ray_terms(w.profile, w.crossings, ends, p, s.alpha, w.ray, transfer, boundaries, true);
+        const double weight = node.weight * divergence;
+        for (int period = 0; period < PERIODS; ++period)
+            for (int band = 0; band < BANDS; ++band) {
+                const double power = weight * (double)src.energy[period][band];
+                out.bands[period][band] += power * transfer.periods[period][band];
+                out.states[0][period] += power * transfer.states[0][band];
+                out.states[1][period] += power * transfer.states[1][band];
+            }
+    }
+    return (int)nodes.size();
+}
+
+// A line piece's received energy at a receiver (a lattice point at receiver_altitude_m, with its
+// own footprint): bands[3][8], states[2][3]; returns the number of quadrature nodes.
+int qmo_line_piece(void *scene, const int64_t receiver[2], double receiver_altitude_m, uint64_t own_footprint,
+                   const double a[2], const double b[2], const qm_source *source, const double *arcs, size_t n_arcs,
+                   double *bands, double *states) {
+    const Scene &s = *static_cast<Scene *>(scene);
+    const Receiver r{receiver[0], receiver[1], receiver_altitude_m, own_footprint};
+    Worker w;
+    PairResult out;
+    const int n = evaluate_line_piece(s, r, a, b, *source, arcs, n_arcs, w, out);
+    for (int period = 0; period < PERIODS; ++period) {
+        for (int band = 0; band < BANDS; ++band) bands[period * BANDS + band] = out.bands[period][band];
+        for (int st = 0; st < 2; ++st) states[st * PERIODS + period] = out.states[st][period];
+    }
+    return n;
+}
+
 double qmo_line_in_plane_angle_at(const double *start, const double *end, double along) {
     LinePiece g;
     return g.make(start, end) ? g.angle_at(along) : NAN;
