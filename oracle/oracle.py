@@ -80,8 +80,11 @@ def lib():
         L.qmo_profile_d.argtypes = [C.c_void_p, _D, _D, _D, _D, _D, C.c_size_t, _D]
         L.qmo_profile_d.restype = C.c_size_t
         L.qmo_line_piece.argtypes = [C.c_void_p, C.POINTER(C.c_int64), C.c_double, C.c_uint64, _D, _D, C.c_void_p,
-                                     _D, C.c_size_t, _D, _D]
+                                     C.c_int, _D, C.c_size_t, _D, _D]
         L.qmo_line_piece.restype = C.c_int
+        L.qmo_skyline_arcs.argtypes = [C.c_void_p, C.POINTER(C.c_int64), C.c_double, C.c_double, C.c_double,
+                                       C.c_double, _D, C.c_size_t]
+        L.qmo_skyline_arcs.restype = C.c_size_t
         L.qmo_path_difference.argtypes = [C.c_int, C.c_double, _D, _D, _D, _D, C.c_size_t, _D]
         L.qmo_path_difference.restype = C.c_double
         L.qmo_diffraction_path.argtypes = [C.c_int, C.c_double, _D, _D, _D, C.c_size_t, _D,
@@ -258,21 +261,32 @@ class OracleScene:
         n = min(n, cap)
         return float(h[0]), t[:n].copy(), z[:n].copy(), g[:n].copy()
 
-    def line_piece(self, receiver_xy, receiver_altitude_m, a, b, source, arcs=(), own_footprint=0):
+    def line_piece(self, receiver_xy, receiver_altitude_m, a, b, source, arcs=None, own_footprint=0):
         """A line piece's received energy at a lattice receiver (physics/src/line.rs quadrature,
         popup/src/evaluate.rs:215-265): (bands [3][8], states [2][3], quadrature nodes). `a`, `b`
         are the piece's ends in steps (anywhere); `source` a SOURCE_DTYPE record whose energy is
-        the power per metre."""
+        the power per metre. The quadrature sees the scene's skyline from the receiver, or with
+        `arcs` ([n][3] azimuth lo, hi, nearest) those arcs whatever the wedge."""
         rxy = np.ascontiguousarray(receiver_xy, dtype=np.int64)
         pa, pb = np.ascontiguousarray(a, dtype=np.float64), np.ascontiguousarray(b, dtype=np.float64)
         src = np.ascontiguousarray(np.asarray(source, dtype=abi.SOURCE_DTYPE).reshape(1))
-        arc = np.ascontiguousarray(np.asarray(arcs, dtype=np.float64).reshape(-1, 3))
+        arc = np.ascontiguousarray(np.asarray(() if arcs is None else arcs, dtype=np.float64).reshape(-1, 3))
         bands, states = np.zeros(24), np.zeros(6)
         n = lib().qmo_line_piece(self.handle, abi.ptr(rxy, C.c_int64), float(receiver_altitude_m), int(own_footprint),
                                  abi.ptr(pa, C.c_double), abi.ptr(pb, C.c_double), src.ctypes.data,
-                                 abi.ptr(arc, C.c_double) if len(arc) else None, len(arc),
+                                 int(arcs is None), abi.ptr(arc, C.c_double) if len(arc) else None, len(arc),
                                  abi.ptr(bands, C.c_double), abi.ptr(states, C.c_double))
         return bands.reshape(3, 8), states.reshape(2, 3), n
+
+    def skyline_arcs(self, receiver_xy, lo_rad, hi_rad, radius_m, floor_m, cap=4096):
+        """The (lo, hi, nearest) arcs the scene's skyline hands a lattice receiver for the wedge
+        [lo_rad, hi_rad] (popup/src/obstacles/skyline.rs:39-110), in the order it visits them."""
+        rxy = np.ascontiguousarray(receiver_xy, dtype=np.int64)
+        out = np.zeros((cap, 3))
+        n = lib().qmo_skyline_arcs(self.handle, abi.ptr(rxy, C.c_int64), float(lo_rad), float(hi_rad),
+                                   float(radius_m), float(floor_m), abi.ptr(out, C.c_double), cap)
+        assert n <= cap, n
+        return out[:n].copy()
 
     def enclosing(self, xy):
         xy = np.ascontiguousarray(np.asarray(xy).reshape(-1, 2), dtype=np.int64)

@@ -15,7 +15,9 @@
 #include <cstdint>
 #include <cstring>
 #include <limits>
+#include <functional>
 #include <thread>
+#include <unordered_map>
 #include <vector>
 
 #include "../include/qm_batch.h"
@@ -1946,9 +1948,160 @@ static void line_mark(const LinePiece &g, const double arc[3], double radius, do
     }
 }
 
+}  // extern "C" (the skyline below holds member templates)
+
+// A skyline query (popup/src/obstacles/skyline.rs:22-38): every arc (azimuth lo, hi, nearest
+// range) of an edge near the receiver that may meet the wedge [lo, hi] within the radius.
+using SkylineQuery =
+    std::function<void(double lo, double hi, double radius, const std::function<void(const double *arc)> &visit)>;
+
+// The receiver skyline over a scene (popup/src/obstacles/skyline.rs:22-110) in the reference's
+// frame: steps with y growing south, so scene point (x, y) (y north) is (x, -y); cells of 256
+// steps, each edge listed in the cells its supercover walk passes through
+// (tiles/src/obstacles/cells.rs:13-47), consecutive edges of an outline in one run, and a cell's
+// height the tallest of its outlines (popup/src/obstacles/tile.rs:93-104).
+struct SceneSkyline {
+    struct Run {
+        uint32_t outline, first_edge, count;
+    };
+    std::unordered_map<uint64_t, std::vector<Run>> runs;
+    std::unordered_map<uint64_t, double> tallest;
+    static uint64_t key(int64_t column, int64_t row) {
+        return ((uint64_t)(uint32_t)(int32_t)column << 32) | (uint64_t)(uint32_t)(int32_t)row;
+    }
+
+    // The cells start -> end passes through, 4-connected in walking order; a tie steps the row
+    // and the walk never leaves the box of its end cells (cells.rs:13-47).
+    template <class Visit>
+    static void edge_cells(int64_t sx, int64_t sy, int64_t ex, int64_t ey, Visit visit) {
+        const int64_t cs = 256;
+        auto div = [](int64_t a, int64_t b) { return a >= 0 ? a / b : -((-a + b - 1) / b); };
+        int64_t cell[2] = {div(sx, cs), div(sy, cs)};
+        const int64_t last[2] = {div(ex, cs), div(ey, cs)};
+        const double delta[2] = {(double)(ex - sx), (double)(ey - sy)};
+        const int64_t step[2] = {delta[0] >= 0.0 ? 1 : -1, delta[1] >= 0.0 ? 1 : -1};
+        const int64_t start[2] = {sx, sy};
+        double t_delta[2], t_max[2];
+        for (int axis = 0; axis < 2; ++axis) {
+            t_delta[axis] = delta[axis] != 0.0 ? std::fabs((double)cs / delta[axis]) : INF;
+            if (delta[axis] == 0.0) {
+                t_max[axis] = INF;
+            } else {
+                const int64_t boundary = (cell[axis] + (delta[axis] >= 0.0 ? 1 : 0)) * cs;
+                t_max[axis] = std::fabs((double)(boundary - start[axis]) / delta[axis]);
+            }
+        }
+        for (;;) {
+            visit(cell[0], cell[1]);
+            if (cell[0] == last[0] && cell[1] == last[1]) return;
+            int axis;
+            if (cell[0] == last[0])
+                axis = 1;
+            else if (cell[1] == last[1] || t_max[0] < t_max[1])
+                axis = 0;
+            else
+                axis = 1;
+            t_max[axis] += t_delta[axis];
+            cell[axis] += step[axis];
+        }
+    }
+
+    explicit SceneSkyline(const Scene &s) {
+        for (uint32_t o = 0; o < s.outlines.size(); ++o) {
+            const qm_outline &rec = s.outlines[o];
+            for (uint32_t k = 0; k + 1 < rec.vertex_count; ++k) {
+                const size_t e = rec.first_vertex + k;
+                edge_cells(s.vertices[2 * e], -(int64_t)s.vertices[2 * e + 1], s.vertices[2 * e + 2],
+                           -(int64_t)s.vertices[2 * e + 3], [&](int64_t c, int64_t r) {
+                               std::vector<Run> &list = runs[key(c, r)];
+                               if (!list.empty() && list.back().outline == o &&
+                                   list.back().first_edge + list.back().count == k)
+                                   ++list.back().count;
+                               else
+                                   list.push_back(Run{o, k, 1});
+                               double &top = tallest.try_emplace(key(c, r), -INF).first->second;
+                               top = std::max(top, (double)rec.height_m);
+                           });
+            }
+        }
+    }
+
+    // The arcs for the receiver at scene steps (rx, ry), wedge [lo, hi], radius and sight-line
+    // floor: cells beyond the radius or wholly outside the wedge are skipped, so are cells whose
+    // tallest outline and walls whose height stay at or under the floor (skyline.rs:39-110).
+    void query(const Scene &s, int64_t rx, int64_t ry, double lo, double hi, double radius_m, double floor_m,
+               const std::function<void(const double *)> &visit) const {
+        const double m = s.step_m, cs = 256.0;
+        const double ox = (double)rx, oy = -(double)ry;
+        const double low[2] = {std::cos(lo), std::sin(lo)}, high[2] = {std::cos(hi), std::sin(hi)};
+        auto relative = [&](size_t v, double out[2]) {
+            out[0] = ((double)s.vertices[2 * v] - ox) * m;
+            out[1] = (oy + (double)s.vertices[2 * v + 1]) * m;
+        };
+        const int64_t row0 = (int64_t)std::floor((oy - radius_m / m) / cs);
+        const int64_t row1 = (int64_t)std::floor((oy + radius_m / m) / cs);
+        const int64_t col0 = (int64_t)std::floor((ox - radius_m / m) / cs);
+        const int64_t col1 = (int64_t)std::floor((ox + radius_m / m) / cs);
+        for (int64_t row = row0; row <= row1; ++row) {
+            const double south = (oy - (double)(row + 1) * cs) * m, north = (oy - (double)row * cs) * m;
+            const double dy = std::max(std::max(south, -north), 0.0);
+            for (int64_t column = col0; column <= col1; ++column) {
+                const double west = ((double)column * cs - ox) * m, east = ((double)(column + 1) * cs - ox) * m;
+                const double dx = std::max(std::max(west, -east), 0.0);
+                if (dx * dx + dy * dy > radius_m * radius_m) continue;
+                const double corners[4][2] = {{west, south}, {east, south}, {west, north}, {east, north}};
+                bool below = true, above = true;
+                for (const auto &c : corners) {
+                    below = below && low[0] * c[1] - low[1] * c[0] < 0.0;
+                    above = above && c[0] * high[1] - c[1] * high[0] < 0.0;
+                }
+                if (below || above) continue;
+                const auto found = runs.find(key(column, row));
+                if (found == runs.end() || tallest.at(key(column, row)) <= floor_m) continue;
+                for (const Run &run : found->second) {
+                    const qm_outline &rec = s.outlines[run.outline];
+                    if (rec.building == 0 && (double)rec.height_m <= floor_m) continue;
+                    const size_t first = rec.first_vertex + run.first_edge;
+                    double a[2], b[2];
+                    relative(first, a);
+                    double azimuth_a = std::atan2(a[1], a[0]);
+                    for (size_t next = first + 1; next <= first + run.count; ++next) {
+                        relative(next, b);
+                        const double azimuth_b = std::atan2(b[1], b[0]);
+                        // The edge's nearest point to the receiver (skyline.rs:9-20).
+                        const double ex = b[0] - a[0], ey = b[1] - a[1], length2 = ex * ex + ey * ey;
+                        const double t =
+                            length2 > 0.0 ? std::min(std::max(-(a[0] * ex + a[1] * ey) / length2, 0.0), 1.0) : 0.0;
+                        const double px = a[0] + t * ex, py = a[1] + t * ey;
+                        const double nearest = std::sqrt(px * px + py * py);
+                        if (nearest >= 1e-6 && nearest <= radius_m) {
+                            const double unwrapped_b = azimuth_a + line_wrap_to_pi(azimuth_b - azimuth_a);
+                            const double arc[3] = {std::min(azimuth_a, unwrapped_b), std::max(azimuth_a, unwrapped_b),
+                                                   nearest};
+                            visit(arc);
+                        }
+                        a[0] = b[0];
+                        a[1] = b[1];
+                        azimuth_a = azimuth_b;
+                    }
+                }
+            }
+        }
+    }
+};
+
+// A query handing over a fixed list of arcs whatever the wedge (the mask re-checks each).
+static SkylineQuery listed_arcs(const double *arcs, size_t n_arcs) {
+    return [arcs, n_arcs](double, double, double, const std::function<void(const double *)> &visit) {
+        for (size_t k = 0; k < n_arcs; ++k) visit(arcs + 3 * k);
+    };
+}
+
+extern "C" {
+
 // push_wide_bucket_nodes (line.rs:208-315): geometry-placed nodes of a wide bucket with something
 // in front of it; nothing otherwise.
-static void line_wide_nodes(const LinePiece &g, double angle_lo, double angle_hi, const double *arcs, size_t n_arcs,
+static void line_wide_nodes(const LinePiece &g, double angle_lo, double angle_hi, const SkylineQuery &skyline,
                             std::vector<LineNode> &nodes) {
     const double along_lo = g.along_at_angle(angle_lo), along_hi = g.along_at_angle(angle_hi);
     const double azimuth_a = g.azimuth_at(along_lo);
@@ -1966,7 +2119,8 @@ static void line_wide_nodes(const LinePiece &g, double angle_lo, double angle_hi
     const double radius = std::min(std::min(range_lo, range_hi), centre_range) + chord;
     const double width = span / LINE_MASK_BINS;
     bool blocked[LINE_MASK_BINS] = {};
-    for (size_t k = 0; k < n_arcs; ++k) line_mark(g, arcs + 3 * k, radius, span_lo, span_hi, width, blocked);
+    skyline(span_lo, span_hi, radius,
+            [&](const double *arc) { line_mark(g, arc, radius, span_lo, span_hi, width, blocked); });
     bool any = false;
     for (bool v : blocked) any = any || v;
     if (!any) return;
@@ -2004,7 +2158,7 @@ static void line_wide_nodes(const LinePiece &g, double angle_lo, double angle_hi
 
 // line_quadrature_nodes (line.rs:180-206): one bucket under 3 degrees, else five of equal dphi,
 // each its centre node unless it is wide and something stands in front of it.
-static void line_nodes(const LinePiece &g, const double *arcs, size_t n_arcs, std::vector<LineNode> &nodes) {
+static void line_nodes(const LinePiece &g, const SkylineQuery &skyline, std::vector<LineNode> &nodes) {
     nodes.clear();
     const double span = g.span();
     const int buckets = span < LINE_ONE_BUCKET_SPAN ? 1 : LINE_BUCKETS;
@@ -2012,7 +2166,7 @@ static void line_nodes(const LinePiece &g, const double *arcs, size_t n_arcs, st
     for (int bucket = 0; bucket < buckets; ++bucket) {
         const double angle_lo = g.angle0 + bucket * bucket_angle, angle_hi = angle_lo + bucket_angle;
         const size_t before = nodes.size();
-        line_wide_nodes(g, angle_lo, angle_hi, arcs, n_arcs, nodes);
+        line_wide_nodes(g, angle_lo, angle_hi, skyline, nodes);
         if (nodes.size() == before)
             nodes.push_back(LineNode{g.along_at_angle(angle_lo + 0.5 * bucket_angle), angle_hi - angle_lo, true});
     }
@@ -2238,11 +2392,11 @@ int qmo_line_geometry(const double *start, const double *end, double *out) {
 // One straight line piece of a source at one receiver: `source_rays` for a line and `add_ray`
 // (popup/src/evaluate.rs:215-265, 118-152). The piece runs from a to b (steps, anywhere); its
 // ends stand on the terrain there plus the source's height; its quadrature nodes
-// (`line_nodes`, over the skyline arcs given) each send a ray from their point along the piece,
+// (`line_nodes`, over the skyline query given) each send a ray from their point along the piece,
 // over the obstacles only where the mask says they can stand, weighted by the node's angle times
 // the line's divergence. `src.energy` is the power per metre of the piece.
 static int evaluate_line_piece(const Scene &s, const Receiver &r, const double a[2], const double b[2],
-                               const qm_source &src, const double *arcs, size_t n_arcs, Worker &w, PairResult &out) {
+                               const qm_source &src, const SkylineQuery &skyline, Worker &w, PairResult &out) {
     for (int period = 0; period < PERIODS; ++period) {
         for (int b2 = 0; b2 < BANDS; ++b2) out.bands[period][b2] = 0.0;
         for (int st = 0; st < 2; ++st) out.states[st][period] = 0.0;
@@ -2257,7 +2411,7 @@ static int evaluate_line_piece(const Scene &s, const Receiver &r, const double a
     LinePiece g;
     if (!g.make(start, end)) return 0;
     std::vector<LineNode> nodes;
-    line_nodes(g, arcs, n_arcs, nodes);
+    line_nodes(g, skyline, nodes);
     const double divergence = g.divergence();
     const double to[2] = {(double)r.x, (double)r.y};
     for (const LineNode &node : nodes) {
@@ -2302,19 +2456,49 @@ static int evaluate_line_piece(const Scene &s, const Receiver &r, const double a
 }
 
 // A line piece's received energy at a receiver (a lattice point at receiver_altitude_m, with its
-// own footprint): bands[3][8], states[2][3]; returns the number of quadrature nodes.
+// own footprint): bands[3][8], states[2][3]; returns the number of quadrature nodes. With
+// scene_skyline the nodes see the scene's own skyline from the receiver, its floor the source's
+// height and never under the ground (popup/src/evaluate.rs:225-242); otherwise the arcs listed.
 int qmo_line_piece(void *scene, const int64_t receiver[2], double receiver_altitude_m, uint64_t own_footprint,
-                   const double a[2], const double b[2], const qm_source *source, const double *arcs, size_t n_arcs,
-                   double *bands, double *states) {
+                   const double a[2], const double b[2], const qm_source *source, int scene_skyline,
+                   const double *arcs, size_t n_arcs, double *bands, double *states) {
     const Scene &s = *static_cast<Scene *>(scene);
     const Receiver r{receiver[0], receiver[1], receiver_altitude_m, own_footprint};
     Worker w;
     PairResult out;
-    const int n = evaluate_line_piece(s, r, a, b, *source, arcs, n_arcs, w, out);
+    int n;
+    if (scene_skyline) {
+        const SceneSkyline sky(s);
+        const double floor_m = std::max((double)source->height_m, 0.0);
+        const SkylineQuery query = [&](double lo, double hi, double radius,
+                                       const std::function<void(const double *)> &visit) {
+            sky.query(s, r.x, r.y, lo, hi, radius, floor_m, visit);
+        };
+        n = evaluate_line_piece(s, r, a, b, *source, query, w, out);
+    } else {
+        n = evaluate_line_piece(s, r, a, b, *source, listed_arcs(arcs, n_arcs), w, out);
+    }
     for (int period = 0; period < PERIODS; ++period) {
         for (int band = 0; band < BANDS; ++band) bands[period * BANDS + band] = out.bands[period][band];
         for (int st = 0; st < 2; ++st) states[st * PERIODS + period] = out.states[st][period];
     }
+    return n;
+}
+
+// The skyline arcs (azimuth lo, hi, nearest range; metres east and north of the receiver) that a
+// receiver at scene steps `receiver` gets for the wedge [lo, hi] within radius_m above floor_m,
+// once per cell an edge is listed in (popup/src/obstacles/skyline.rs:39-110). Writes at most
+// `cap` arcs; returns how many there are.
+size_t qmo_skyline_arcs(void *scene, const int64_t receiver[2], double lo, double hi, double radius_m, double floor_m,
+                        double *out, size_t cap) {
+    const Scene &s = *static_cast<Scene *>(scene);
+    const SceneSkyline sky(s);
+    size_t n = 0;
+    sky.query(s, receiver[0], receiver[1], lo, hi, radius_m, floor_m, [&](const double *arc) {
+        if (n < cap)
+            for (int k = 0; k < 3; ++k) out[3 * n + k] = arc[k];
+        ++n;
+    });
     return n;
 }
 
@@ -2332,7 +2516,7 @@ int qmo_line_nodes(const double *start, const double *end, const double *arcs, s
     LinePiece g;
     if (!g.make(start, end)) return -1;
     std::vector<LineNode> nodes;
-    line_nodes(g, arcs, n_arcs, nodes);
+    line_nodes(g, listed_arcs(arcs, n_arcs), nodes);
     for (size_t k = 0; k < nodes.size() && k < cap; ++k) {
         along[k] = nodes[k].along;
         weight[k] = nodes[k].weight;

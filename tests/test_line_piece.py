@@ -60,3 +60,32 @@ def test_five_buckets_match_a_401_point_sum(flat_g):
         sources = np.concatenate([_source(stock, (x, 0.0), length / count) for x in xs])
         point_db = _point_sum_db(stock, receiver, sources, flat_g)
         assert abs(line_db - point_db) < 0.15, (flat_g, distance, line_db, point_db)
+
+
+def test_the_scene_skyline_stands_for_the_arcs_it_hands_over():
+    """Each wide bucket asks the scene's skyline for its own wedge and radius
+    (popup/src/evaluate.rs:225-242); handing the quadrature every arc of the two half planes
+    within a kilometre (beyond every bucket's radius) instead gives the same piece to the bit,
+    as the mask re-checks each arc's wedge and range. Something in front of the near piece
+    changes its nodes."""
+    import math
+
+    stock = Stock()
+    stock.building(1, 10.0, [square(-40.0, 12.0, 5.0)])
+    stock.building(2, 3.0, [square(30.0, 8.0, 3.0)])
+    stock.wall(3, 2.0, [(-10.0, 6.0), (10.0, 6.0)])
+    stock.wall(4, 0.04, [(50.0, 4.0), (70.0, 4.0)])          # under the source's height: pruned
+    ora = oracle.OracleScene(stock.scene(flat_ground_factor=0.5))
+    src = _source(stock, (-125.0, 0.0), 1.0)[0]
+    receiver = stock.steps((0.0, 20.0))
+    a, b = stock.steps((-125.0, 0.0)).astype(np.float64), stock.steps((125.0, 0.0)).astype(np.float64)
+    floor = max(float(src["height_m"]), 0.0)
+    everything = np.concatenate([ora.skyline_arcs(receiver, lo, hi, 1000.0, floor)
+                                 for lo, hi in ((0.0, math.pi), (-math.pi, 0.0))])
+    assert len(everything) > 0
+    scene_bands, scene_states, n_scene = ora.line_piece(receiver, 4.0, a, b, src)
+    listed_bands, listed_states, n_listed = ora.line_piece(receiver, 4.0, a, b, src, arcs=everything)
+    assert n_scene == n_listed
+    assert np.array_equal(scene_bands, listed_bands) and np.array_equal(scene_states, listed_states)
+    open_bands, _, n_open = ora.line_piece(receiver, 4.0, a, b, src, arcs=())
+    assert n_open != n_scene or not np.array_equal(open_bands, scene_bands)

@@ -99,3 +99,53 @@ def test_a_wall_half_a_metre_away_is_kept_and_one_through_the_receiver_is_not():
     found = distinct(stock.arcs(EAST, 50.0, 0.0))
     assert len(found) == 1, found
     assert abs(found[0][2] - 0.5) < 0.2
+
+
+def _scene_and_restated(seed):
+    """A random stock scene of buildings and walls, and the same outlines for the restated
+    skyline: steps with y negated (the reference's lattice grows south), heights as the scene
+    holds them (float32)."""
+    import numpy as np
+
+    from helpers import Stock as SceneStock
+
+    rng = np.random.default_rng(seed)
+    stock = SceneStock()
+    for fp in range(1, 41):
+        cx, cy = rng.uniform(-150.0, 150.0, 2)
+        if rng.random() < 0.7:
+            half = rng.uniform(2.0, 15.0)
+            stock.building(fp, float(rng.uniform(1.0, 25.0)), [[(cx - half, cy - half), (cx + half, cy - half),
+                                                                (cx + half, cy + half), (cx - half, cy + half)]])
+        else:
+            points = [(cx, cy)] + [tuple(rng.uniform(-150.0, 150.0, 2)) for _ in range(int(rng.integers(1, 4)))]
+            stock.wall(fp, float(rng.uniform(0.5, 6.0)), points)
+    outlines = []
+    for verts, (first, count, fp, height, building) in zip(stock.verts, stock.records):
+        outlines.append(dict(footprint_id=fp, kind=ob.EXTERIOR if building else ob.WALL,
+                             height_m=float(np.float32(height)), vertices=[(int(x), -int(y)) for x, y in verts]))
+    return stock, ob.Skyline(outlines, (stock.step_m, stock.step_m))
+
+
+def test_the_oracle_scene_skyline_is_the_restated_one():
+    """The C++ skyline over a scene hands over the same arcs, in the same order and to the bit,
+    as the restatement pinned above, across receivers, wedges (some wrapping past pi), radii and
+    sight-line floors that prune walls and whole cells."""
+    import numpy as np
+
+    from oracle import oracle
+
+    stock, restated = _scene_and_restated(11)
+    ora = oracle.OracleScene(stock.scene())
+    rng = np.random.default_rng(5)
+    total = 0
+    for _ in range(60):
+        r = stock.steps(rng.uniform(-120.0, 120.0, 2))
+        lo = rng.uniform(-math.pi, math.pi)
+        hi = lo + rng.uniform(0.01, 3.0)
+        radius, floor = rng.uniform(5.0, 250.0), float(rng.choice([0.0, 0.05, 3.0, 12.0]))
+        got = ora.skyline_arcs(r, lo, hi, radius, floor)
+        want = np.array(restated.arcs((int(r[0]), -int(r[1])), lo, hi, radius, floor)).reshape(-1, 3)
+        assert np.array_equal(got, want), (r, lo, hi, radius, floor, len(got), len(want))
+        total += len(got)
+    assert total > 500
