@@ -85,6 +85,9 @@ def lib():
         L.qmo_skyline_arcs.argtypes = [C.c_void_p, C.POINTER(C.c_int64), C.c_double, C.c_double, C.c_double,
                                        C.c_double, _D, C.c_size_t]
         L.qmo_skyline_arcs.restype = C.c_size_t
+        L.qmo_scene_line_nodes.argtypes = [C.c_void_p, C.POINTER(C.c_int64), C.c_double, _D, _D, _D, _D,
+                                           C.POINTER(C.c_uint8), C.c_size_t]
+        L.qmo_scene_line_nodes.restype = C.c_int
         L.qmo_path_difference.argtypes = [C.c_int, C.c_double, _D, _D, _D, _D, C.c_size_t, _D]
         L.qmo_path_difference.restype = C.c_double
         L.qmo_diffraction_path.argtypes = [C.c_int, C.c_double, _D, _D, _D, C.c_size_t, _D,
@@ -287,6 +290,22 @@ class OracleScene:
                                    float(radius_m), float(floor_m), abi.ptr(out, C.c_double), cap)
         assert n <= cap, n
         return out[:n].copy()
+
+    def line_nodes(self, receiver_xy, start, end, floor_m):
+        """A piece's quadrature nodes (start, end: metres relative to the receiver) with the wide
+        buckets querying this scene's skyline from the lattice receiver above floor_m:
+        (along_m, weight_rad, obstacles_on_ray) arrays, None for a degenerate piece."""
+        rxy = np.ascontiguousarray(receiver_xy, dtype=np.int64)
+        cap = 64 * 9 * 5
+        along, weight = np.zeros(cap), np.zeros(cap)
+        on_ray = np.zeros(cap, np.uint8)
+        n = lib().qmo_scene_line_nodes(self.handle, abi.ptr(rxy, C.c_int64), float(floor_m),
+                                       abi.ptr(_xyz(start), C.c_double), abi.ptr(_xyz(end), C.c_double),
+                                       abi.ptr(along, C.c_double), abi.ptr(weight, C.c_double),
+                                       abi.ptr(on_ray, C.c_uint8), cap)
+        if n < 0:
+            return None
+        return along[:n], weight[:n], on_ray[:n].astype(bool)
 
     def enclosing(self, xy):
         xy = np.ascontiguousarray(np.asarray(xy).reshape(-1, 2), dtype=np.int64)

@@ -1939,6 +1939,7 @@ static void line_mark(const LinePiece &g, const double arc[3], double radius, do
         double along;
         if (!g.along_at_azimuth(0.5 * (piece_lo + piece_hi), along)) continue;
         if (g.range_at(along) - arc[2] <= 1.0) continue;
+        // A first bin past the end (an overlap rounded onto the span's far edge) marks nothing.
         const size_t first = (size_t)std::max(std::floor((piece_lo - lo) / width), 0.0);
         const double up = std::ceil((piece_hi - lo) / width);
         size_t last = up > 0.0 ? (size_t)up : 0;
@@ -2500,6 +2501,29 @@ size_t qmo_skyline_arcs(void *scene, const int64_t receiver[2], double lo, doubl
         ++n;
     });
     return n;
+}
+
+// The quadrature nodes of a piece (start, end: metres relative to the receiver) with each wide
+// bucket querying the scene's skyline from the receiver at scene steps `receiver` above floor_m,
+// as the line evaluation does (popup/src/evaluate.rs:225-242); up to cap written. Returns the
+// count, -1 for a degenerate piece.
+int qmo_scene_line_nodes(void *scene, const int64_t receiver[2], double floor_m, const double *start,
+                         const double *end, double *along, double *weight, uint8_t *on_ray, size_t cap) {
+    const Scene &s = *static_cast<Scene *>(scene);
+    LinePiece g;
+    if (!g.make(start, end)) return -1;
+    const SceneSkyline sky(s);
+    const SkylineQuery query = [&](double lo, double hi, double radius, const std::function<void(const double *)> &visit) {
+        sky.query(s, receiver[0], receiver[1], lo, hi, radius, floor_m, visit);
+    };
+    std::vector<LineNode> nodes;
+    line_nodes(g, query, nodes);
+    for (size_t k = 0; k < nodes.size() && k < cap; ++k) {
+        along[k] = nodes[k].along;
+        weight[k] = nodes[k].weight;
+        on_ray[k] = nodes[k].on_ray ? 1 : 0;
+    }
+    return (int)nodes.size();
 }
 
 double qmo_line_in_plane_angle_at(const double *start, const double *end, double along) {

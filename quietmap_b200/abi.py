@@ -142,6 +142,25 @@ FLIGHT_SEGMENT_DTYPE = np.dtype(
      ("departure", "<u4"), ("flight", "<u4"), ("pad_", "<u4")], align=True)
 
 
+LINE_NODE_DTYPE = np.dtype([("along_m", "<f8"), ("weight_rad", "<f8"), ("obstacles_on_ray", "<u4"),
+                            ("reserved", "<u4")], align=True)
+LINE_MAX_NODES = 705
+
+
+class LinePieceInfo(C.Structure):
+    _fields_ = [("length_m", C.c_double), ("subtended_angle_rad", C.c_double), ("divergence_factor", C.c_double),
+                ("start_angle_rad", C.c_double)]
+
+
+class SkylineReceiver(C.Structure):
+    _fields_ = [("skyline", C.c_void_p), ("x", C.c_int64), ("y", C.c_int64), ("floor_m", C.c_double)]
+
+
+# A skyline query's visit and the query itself (qm_skyline_visit_fn, qm_skyline_query_fn).
+SKYLINE_VISIT_FN = C.CFUNCTYPE(None, C.c_double, C.c_double, C.c_double, C.c_void_p)
+SKYLINE_QUERY_FN = C.CFUNCTYPE(None, C.c_double, C.c_double, C.c_double, SKYLINE_VISIT_FN, C.c_void_p, C.c_void_p)
+
+
 class FlightGridDesc(C.Structure):
     _fields_ = [
         ("origin_m", C.c_double * 2),
@@ -175,6 +194,7 @@ assert AIRCRAFT_TYPE_DTYPE.itemsize == 4 * (200 + 200 + 2 + 28 + 2)
 assert FLIGHT_SEGMENT_DTYPE.itemsize == 48
 assert OUTLINE_DTYPE.itemsize == C.sizeof(Outline)
 assert SOURCE_DTYPE.itemsize == C.sizeof(Source)
+assert LINE_NODE_DTYPE.itemsize == 24
 
 
 def ptr(array, ctype):

@@ -11,7 +11,8 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libqm_b200.so")
-SOURCES = ["qm_lib.cu", "qm_zwicker.cu", "qm_mlp.cu", "qm_formats.cpp"]
+SOURCES = ["qm_lib.cu", "qm_zwicker.cu", "qm_mlp.cu", "qm_formats.cpp", "qm_line.cu"]
+OBJ_DIR = os.path.join(HERE, "_build")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-O2",
          "--expt-relaxed-constexpr", "-rdc=false"]
@@ -31,23 +32,37 @@ def newest_input():
     return max(os.path.getmtime(p) for p in paths)
 
 
+def newest_header():
+    """The newest shared input: headers under csrc/ and include/, and this script."""
+    inc = os.path.join(os.path.dirname(HERE), "include")
+    paths = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".h", ".cuh"))]
+    paths += [os.path.join(inc, f) for f in os.listdir(inc)]
+    paths.append(__file__)
+    return max(os.path.getmtime(p) for p in paths)
+
+
 def build(force=False, verbose=False):
+    """Compiles each source whose object is older than it or than any header, then links."""
     if not force and os.path.exists(LIB) and os.path.getmtime(LIB) >= newest_input():
         return LIB
+    os.makedirs(OBJ_DIR, exist_ok=True)
+    headers = newest_header()
     objs = []
     for src in SOURCES:
-        obj = os.path.join(CSRC, "_" + os.path.splitext(src)[0] + ".o")
-        cmd = [nvcc(), *ARCH, *FLAGS, "-c", os.path.join(CSRC, src), "-o", obj]
-        if verbose:
-            cmd.insert(1, "-Xptxas=-v")
-            print(" ".join(cmd), flush=True)
-        subprocess.run(cmd, check=True)
+        path = os.path.join(CSRC, src)
+        obj = os.path.join(OBJ_DIR, os.path.splitext(src)[0] + ".o")
+        stale = (force or not os.path.exists(obj) or os.path.getmtime(obj) < max(os.path.getmtime(path), headers))
+        if stale:
+            cmd = [nvcc(), *ARCH, *FLAGS, "-c", path, "-o", obj + ".tmp"]
+            if verbose:
+                cmd.insert(1, "-Xptxas=-v")
+                print(" ".join(cmd), flush=True)
+            subprocess.run(cmd, check=True)
+            os.replace(obj + ".tmp", obj)
         objs.append(obj)
     cmd = [nvcc(), *ARCH, "-shared", "-o", LIB + ".tmp", *objs, "-lcudart"]
     subprocess.run(cmd, check=True)
     os.replace(LIB + ".tmp", LIB)
-    for o in objs:
-        os.remove(o)
     return LIB
 
 

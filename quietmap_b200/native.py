@@ -134,6 +134,19 @@ def lib():
         L.qm_batch_plan_run.restype = C.c_int
         L.qm_batch_plan_read.argtypes = [C.c_void_p, _F, _F, _F]
         L.qm_batch_plan_read.restype = C.c_int
+        L.qm_line_quadrature_nodes.argtypes = [_D, _D, C.c_void_p, C.c_void_p, C.c_void_p, C.c_size_t,
+                                               C.POINTER(C.c_size_t), C.POINTER(abi.LinePieceInfo)]
+        L.qm_line_quadrature_nodes.restype = C.c_int
+        L.qm_skyline_build.argtypes = [C.POINTER(C.c_int32), C.c_size_t, C.c_void_p, C.c_size_t, C.c_double,
+                                       C.POINTER(C.c_void_p)]
+        L.qm_skyline_build.restype = C.c_int
+        L.qm_skyline_counts.argtypes = [C.c_void_p, C.POINTER(C.c_size_t), C.POINTER(C.c_size_t)]
+        L.qm_skyline_counts.restype = C.c_int
+        L.qm_skyline_arcs.argtypes = [C.c_void_p, C.c_int64, C.c_int64, C.c_double, C.c_double, C.c_double,
+                                      C.c_double, _D, C.c_size_t, C.POINTER(C.c_size_t)]
+        L.qm_skyline_arcs.restype = C.c_int
+        L.qm_skyline_free.argtypes = [C.c_void_p]
+        L.qm_skyline_free.restype = None
         if L.qm_abi_version() != abi.ABI_VERSION:
             raise QmError(abi.QM_ERR_UNSUPPORTED, "library ABI version mismatch")
         _lib = L
@@ -305,6 +318,81 @@ def obstacles_cell_runs(data, column, row, cap=64):
     count = C.c_uint32()
     _check(lib().qm_obstacles_cell_runs(p, len(b), column, row, abi.ptr(runs, C.c_uint32), cap, C.byref(count)))
     return [tuple(int(v) for v in r) for r in runs[:min(count.value, cap)]]
+
+
+class Skyline:
+    """The receiver skyline over a scene's outlines (qm_skyline_build): the index the line
+    quadrature's wide buckets query, built on the host."""
+
+    def __init__(self, vertices, outlines, step_m):
+        v = np.ascontiguousarray(np.asarray(vertices).reshape(-1, 2), dtype=np.int32)
+        o = np.ascontiguousarray(outlines, dtype=abi.OUTLINE_DTYPE)
+        handle = C.c_void_p()
+        _check(lib().qm_skyline_build(abi.ptr(v, C.c_int32), len(v), o.ctypes.data if len(o) else None, len(o),
+                                      float(step_m), C.byref(handle)))
+        self.handle = handle
+
+    @classmethod
+    def of_scene(cls, scene):
+        return cls(scene.vertices, scene.outlines, scene.step_m)
+
+    def close(self):
+        if self.handle:
+            lib().qm_skyline_free(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def counts(self):
+        cells, runs = C.c_size_t(), C.c_size_t()
+        _check(lib().qm_skyline_counts(self.handle, C.byref(cells), C.byref(runs)))
+        return cells.value, runs.value
+
+    def arcs(self, receiver_xy, lo_rad, hi_rad, radius_m, floor_m, cap=4096):
+        """[n][3] (lo, hi, nearest) for the receiver at scene steps `receiver_xy`."""
+        out = np.zeros((cap, 3))
+        n = C.c_size_t()
+        _check(lib().qm_skyline_arcs(self.handle, int(receiver_xy[0]), int(receiver_xy[1]), float(lo_rad),
+                                     float(hi_rad), float(radius_m), float(floor_m), abi.ptr(out, C.c_double), cap,
+                                     C.byref(n)))
+        return out[:n.value].copy()
+
+
+def line_quadrature_nodes(start, end, arcs=None, skyline=None, receiver_xy=None, floor_m=0.0,
+                          cap=abi.LINE_MAX_NODES):
+    """A piece's quadrature nodes (qm_line_quadrature_nodes) and its figures: start and end in
+    metres relative to the receiver (x east, y north, z up). The wide buckets see `arcs`
+    ([n][3] lo, hi, nearest, handed over whatever the wedge), or the `skyline` index from the
+    receiver at scene steps `receiver_xy` above `floor_m`, or nothing."""
+    s = np.ascontiguousarray(start, dtype=np.float64)
+    e = np.ascontiguousarray(end, dtype=np.float64)
+    nodes = np.zeros(cap, dtype=abi.LINE_NODE_DTYPE)
+    n = C.c_size_t()
+    info = abi.LinePieceInfo()
+    query, user = None, None
+    keep = []
+    if skyline is not None:
+        view = abi.SkylineReceiver(skyline.handle, int(receiver_xy[0]), int(receiver_xy[1]), float(floor_m))
+        keep.append(view)
+        query, user = C.cast(lib().qm_skyline_query, C.c_void_p), C.cast(C.pointer(view), C.c_void_p)
+    elif arcs is not None:
+        listed = np.asarray(arcs, dtype=np.float64).reshape(-1, 3)
+
+        def hand_over(lo, hi, radius, visit, ctx, _user):
+            for a in listed:
+                visit(a[0], a[1], a[2], ctx)
+
+        fn = abi.SKYLINE_QUERY_FN(hand_over)
+        keep.append(fn)
+        query = C.cast(fn, C.c_void_p)
+    _check(lib().qm_line_quadrature_nodes(abi.ptr(s, C.c_double), abi.ptr(e, C.c_double), query, user,
+                                          nodes.ctypes.data, cap, C.byref(n), C.byref(info)))
+    figures = {k: getattr(info, k) for k, _ in abi.LinePieceInfo._fields_}
+    return nodes[:n.value].copy(), figures
 
 
 def terrain_decode(data):

@@ -1,12 +1,47 @@
-"""The line-piece quadrature of the oracle (physics/src/line.rs), pinned to the reference's own
-tests (physics/src/line_tests.rs): free-field exactness against a numeric point sum, the
-normalisation, the in-plane angle, the perpendicular floor, and the bucket and wide-bucket nodes."""
+"""The line-piece quadrature (physics/src/line.rs), pinned to the reference's own tests
+(physics/src/line_tests.rs): free-field exactness against a numeric point sum, the
+normalisation, the in-plane angle, the perpendicular floor, and the bucket and wide-bucket nodes.
+Every test runs twice: on the oracle's restatement and on the library's shared host/device
+quadrature through its C ABI (qm_line_quadrature_nodes, run on the host; no GPU)."""
 
 import math
+import types
 
 import numpy as np
+import pytest
 
 from oracle import oracle
+from quietmap_b200 import native
+
+
+def _library_nodes(start, end, arcs=()):
+    nodes, _ = native.line_quadrature_nodes(start, end, arcs=arcs)
+    if len(nodes) == 0:
+        return None
+    return nodes["along_m"], nodes["weight_rad"], nodes["obstacles_on_ray"].astype(bool)
+
+
+def _library_geometry(start, end):
+    nodes, figures = native.line_quadrature_nodes(start, end)
+    if len(nodes) == 0:
+        return None
+    return dict(length_m=figures["length_m"], subtended_rad=figures["subtended_angle_rad"],
+                divergence_factor=figures["divergence_factor"])
+
+
+IMPLEMENTATIONS = {
+    "oracle": types.SimpleNamespace(line_nodes=oracle.line_nodes, line_geometry=oracle.line_geometry),
+    "library": types.SimpleNamespace(line_nodes=_library_nodes, line_geometry=_library_geometry),
+}
+IMPL = IMPLEMENTATIONS["oracle"]
+
+
+@pytest.fixture(autouse=True, params=sorted(IMPLEMENTATIONS))
+def implementation(request):
+    global IMPL
+    IMPL = IMPLEMENTATIONS[request.param]
+    yield request.param
+    IMPL = IMPLEMENTATIONS["oracle"]
 
 DIVERGENCE = 12.589254117941673  # 10^1.1
 BUCKETS = 5
@@ -24,8 +59,8 @@ def relative(point, receiver):
 def free_field_energy(start, end, receiver):
     """sum(dphi) / (10^1.1 d_perp) per unit L_W' (line_tests.rs:20-27)."""
     s, e = relative(start, receiver), relative(end, receiver)
-    _, weight, _ = oracle.line_nodes(s, e)
-    return weight.sum() * oracle.line_geometry(s, e)["divergence_factor"]
+    _, weight, _ = IMPL.line_nodes(s, e)
+    return weight.sum() * IMPL.line_geometry(s, e)["divergence_factor"]
 
 
 def point_sum_energy(start, end, receiver, steps=400_000):
@@ -68,17 +103,17 @@ def test_the_in_plane_angle_replaces_the_horizontal_one_beside_a_short_elevated_
 
 
 def test_a_receiver_on_the_line_reads_it_half_a_metre_away():
-    g = oracle.line_geometry([-125.0, 0.0, 0.0], [125.0, 0.0, 0.0])
+    g = IMPL.line_geometry([-125.0, 0.0, 0.0], [125.0, 0.0, 0.0])
     assert g["divergence_factor"] == 1.0 / (DIVERGENCE * 0.5)
-    assert oracle.line_geometry([1.0, 2.0, 3.0], [1.0, 2.0, 3.0]) is None
+    assert IMPL.line_geometry([1.0, 2.0, 3.0], [1.0, 2.0, 3.0]) is None
 
 
 def test_nodes_are_uniform_in_the_in_plane_angle():
     s, e = [-125.0, 20.0, -3.95], [125.0, 20.0, -3.95]
-    along, _, _ = oracle.line_nodes(s, e)
+    along, _, _ = IMPL.line_nodes(s, e)
     assert len(along) == BUCKETS
     angles = [oracle.line_in_plane_angle_at(s, e, a) for a in along]
-    step = oracle.line_geometry(s, e)["subtended_rad"] / BUCKETS
+    step = IMPL.line_geometry(s, e)["subtended_rad"] / BUCKETS
     for a, b in zip(angles[:-1], angles[1:]):
         assert abs(b - a - step) < 1e-12
     assert abs(along[2] - 125.0) < 1e-9, "the middle node faces the receiver"
@@ -86,9 +121,9 @@ def test_nodes_are_uniform_in_the_in_plane_angle():
 
 def test_a_piece_seen_under_a_small_angle_takes_one_node():
     s, e = [-10.0, 1000.0, -3.95], [10.0, 1000.0, -3.95]
-    g = oracle.line_geometry(s, e)
+    g = IMPL.line_geometry(s, e)
     assert g["subtended_rad"] < ONE_BUCKET_SPAN
-    along, weight, _ = oracle.line_nodes(s, e)
+    along, weight, _ = IMPL.line_nodes(s, e)
     assert len(along) == 1
     assert abs(weight[0] - g["subtended_rad"]) < 1e-15
     assert abs(along[0] - 10.0) < 1e-9
@@ -96,10 +131,10 @@ def test_a_piece_seen_under_a_small_angle_takes_one_node():
 
 def test_a_wall_in_front_of_a_wide_bucket_places_blocked_and_clear_nodes():
     s, e = [-125.0, 20.0, 0.0], [125.0, 20.0, 0.0]
-    g = oracle.line_geometry(s, e)
+    g = IMPL.line_geometry(s, e)
     for nearest in (10.0, 0.5):
         wall = (math.radians(80.0), math.radians(100.0), nearest)
-        along, weight, on_ray = oracle.line_nodes(s, e, [wall])
+        along, weight, on_ray = IMPL.line_nodes(s, e, [wall])
         assert len(along) > BUCKETS
         assert abs(weight.sum() - g["subtended_rad"]) < 1e-12
         azimuth = np.degrees(np.arctan2(np.full_like(along, 20.0), s[0] + along))

@@ -62,12 +62,14 @@ def test_five_buckets_match_a_401_point_sum(flat_g):
         assert abs(line_db - point_db) < 0.15, (flat_g, distance, line_db, point_db)
 
 
-def test_the_scene_skyline_stands_for_the_arcs_it_hands_over():
+def test_the_scene_skyline_hands_this_piece_the_arcs_that_matter():
     """Each wide bucket asks the scene's skyline for its own wedge and radius
-    (popup/src/evaluate.rs:225-242); handing the quadrature every arc of the two half planes
-    within a kilometre (beyond every bucket's radius) instead gives the same piece to the bit,
-    as the mask re-checks each arc's wedge and range. Something in front of the near piece
-    changes its nodes."""
+    (popup/src/evaluate.rs:225-242). On this scene, every outline above the floor and near the
+    piece, that hands the mask the arcs that matter, so the piece is the same to the bit as with
+    every arc of the two half planes within a kilometre handed over (the mask re-checks each
+    arc's wedge and range). In general the two can differ, as the reference's can: a cell the
+    bucket's wedge, radius or floor prunes may hold the only listing of an edge that reaches the
+    bucket. Something in front of the near piece changes its nodes."""
     import math
 
     stock = Stock()
