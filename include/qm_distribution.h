@@ -1,0 +1,61 @@
+/* How levels add over time: distributions of the summed level over a period on a decibel grid,
+ * and the values of the lines added to them (popup/src/distribution.rs).
+ *
+ * The arithmetic is one __host__ __device__ source (quietmap_b200/csrc/qm_distribution.cuh) for
+ * the per-pixel distributions on the device; these entry points run it on the calling host
+ * thread, as the reference's click detail (popup) does for one point, and for checking it
+ * without a GPU. They need no device and allocate no device memory. A distribution is
+ * bins[n][2] (share of the time, share x the moments' mean intensity) on a grid of bin_db from
+ * -30 dB over 180 dB, plus its share in silence. */
+#ifndef QM_DISTRIBUTION_H
+#define QM_DISTRIBUTION_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#include "qm_batch.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* The finest grid: 0.1 dB, 1800 bins. */
+#define QM_DISTRIBUTION_MAX_BINS 1800
+/* A line's values at the reference's node probabilities (popup/src/distribution.rs:17-32). */
+#define QM_DISTRIBUTION_LINE_NODES 124
+
+/* The bins of a grid of bin_db (180 dB over the step, rounded; distribution.rs:55-62);
+ * QM_ERR_ARGUMENT for a step that is not positive and finite or gives more than
+ * QM_DISTRIBUTION_MAX_BINS. */
+qm_status qm_distribution_bins(double bin_db, size_t *n_bins);
+
+/* Distribution::with_line (distribution.rs:86-145, 176-196): `out` is `in` with a line of
+ * `n_values` (intensity, share) pairs, in any order, times `scale` added at every moment; each
+ * sum lands in the bin of its level with its intensity kept exact. Intensities must be at
+ * least 0 and shares at least 0, scale above 0. out_bins may not alias bins. */
+qm_status qm_distribution_with_line(double bin_db, const double *bins, double silent, const double *values,
+                                    size_t n_values, double scale, double *out_bins, double *out_silent);
+
+/* Distribution::exceeded_db (distribution.rs:152-162): the level exceeded `exceeded` of the
+ * time, -inf where silence is. */
+qm_status qm_distribution_exceeded_db(double bin_db, const double *bins, double exceeded, double *level_db);
+
+/* line_values (distribution.rs:264-281): a line's intensities relative to its mean with their
+ * shares, Kurze's quantiles at `lambda` emitters per distance of its closest point at the node
+ * probabilities (QM_DISTRIBUTION_LINE_NODES pairs, by the library's line-level sampler), or
+ * with `duty` in (0, 1] an event's mean over its duty while it sounds and silence otherwise
+ * (2 pairs). Pass NaN as duty for a line. values[n][2]. */
+qm_status qm_distribution_line_values(double lambda, double duty, double *values, size_t cap, size_t *n_values);
+
+/* pass_values (distribution.rs:283-298): the relative intensities of a stream of passes of one
+ * level of which `mean` are in progress on average, with their shares. `mean` lies in (0, 700]:
+ * above about 745 the silence's share underflows to 0 and the reference's loop does not end.
+ * values[n][2]; more than `cap`: the first `cap` are written, *n_values holds the count and the
+ * call returns QM_ERR_CAPACITY. */
+qm_status qm_distribution_pass_values(double mean, double *values, size_t cap, size_t *n_values);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* QM_DISTRIBUTION_H */

@@ -145,6 +145,8 @@ FLIGHT_SEGMENT_DTYPE = np.dtype(
 LINE_NODE_DTYPE = np.dtype([("along_m", "<f8"), ("weight_rad", "<f8"), ("obstacles_on_ray", "<u4"),
                             ("reserved", "<u4")], align=True)
 LINE_MAX_NODES = 705
+DISTRIBUTION_MAX_BINS = 1800
+DISTRIBUTION_LINE_NODES = 124
 
 
 class LinePieceInfo(C.Structure):

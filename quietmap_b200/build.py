@@ -11,7 +11,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libqm_b200.so")
-SOURCES = ["qm_lib.cu", "qm_zwicker.cu", "qm_mlp.cu", "qm_formats.cpp", "qm_line.cu"]
+SOURCES = ["qm_lib.cu", "qm_zwicker.cu", "qm_mlp.cu", "qm_formats.cpp", "qm_line.cu", "qm_distribution.cu"]
 OBJ_DIR = os.path.join(HERE, "_build")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-O2",

@@ -1,0 +1,170 @@
+// Distributions of the summed level over time on the host side of the library: the C entry
+// points that run the shared __host__ __device__ arithmetic (qm_distribution.cuh) on the calling
+// thread, and the values of the lines added to them.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <string>
+#include <utility>
+#include <vector>
+
+#include "../../include/qm_distribution.h"
+#include "qm_distribution.cuh"
+#include "qm_host.h"
+#include "qm_percentile.cuh"
+
+static_assert(QM_DISTRIBUTION_LINE_NODES == qm::dist::NODES, "the header's node count is the grid's");
+
+namespace {
+
+qm_status grid(const char *who, double bin_db, int &n_bins) {
+    if (!(bin_db > 0.0) || !std::isfinite(bin_db))
+        return qm::set_error(QM_ERR_ARGUMENT, std::string(who) + ": bin_db must be positive and finite");
+    const double count = std::round(qm::dist::SPAN_DB / bin_db);
+    if (!(count >= 1.0) || count > QM_DISTRIBUTION_MAX_BINS)
+        return qm::set_error(QM_ERR_ARGUMENT, std::string(who) + ": bin_db gives " + std::to_string(count) +
+                                                  " bins, at most " + std::to_string(QM_DISTRIBUTION_MAX_BINS));
+    n_bins = (int)count;
+    return QM_OK;
+}
+
+// Values in increasing order of intensity, equal ones in their given order, with their running
+// sums (distribution.rs:243-256).
+struct OwnedValues {
+    std::vector<double> pairs, sums;
+    qm::dist::Values view() const { return qm::dist::Values{pairs.data(), sums.data(), (int)(pairs.size() / 2)}; }
+};
+
+OwnedValues sorted_values(const double *values, size_t n) {
+    std::vector<std::pair<double, double>> list(n);
+    // An intensity of -0 is one of 0: the sort sees them as equal.
+    for (size_t k = 0; k < n; ++k) list[k] = {values[2 * k] + 0.0, values[2 * k + 1]};
+    std::stable_sort(list.begin(), list.end(), [](const auto &a, const auto &b) { return a.first < b.first; });
+    OwnedValues out;
+    out.pairs.resize(2 * n);
+    out.sums.resize(2 * (n + 1));
+    out.sums[0] = out.sums[1] = 0.0;
+    for (size_t k = 0; k < n; ++k) {
+        out.pairs[2 * k] = list[k].first;
+        out.pairs[2 * k + 1] = list[k].second;
+        out.sums[2 * (k + 1)] = out.sums[2 * k] + list[k].second;
+        out.sums[2 * (k + 1) + 1] = out.sums[2 * k + 1] + list[k].second * list[k].first;
+    }
+    return out;
+}
+
+}  // namespace
+
+extern "C" {
+
+qm_status qm_distribution_bins(double bin_db, size_t *n_bins) {
+    if (n_bins == nullptr) return qm::set_error(QM_ERR_ARGUMENT, "qm_distribution_bins: null n_bins");
+    int n = 0;
+    const qm_status status = grid("qm_distribution_bins", bin_db, n);
+    if (status != QM_OK) return status;
+    *n_bins = (size_t)n;
+    return QM_OK;
+}
+
+qm_status qm_distribution_with_line(double bin_db, const double *bins, double silent, const double *values,
+                                    size_t n_values, double scale, double *out_bins, double *out_silent) {
+    int n_bins = 0;
+    const qm_status status = grid("qm_distribution_with_line", bin_db, n_bins);
+    if (status != QM_OK) return status;
+    if (bins == nullptr || out_bins == nullptr || out_silent == nullptr || (n_values > 0 && values == nullptr))
+        return qm::set_error(QM_ERR_ARGUMENT, "qm_distribution_with_line: null bins, values or output");
+    if (bins == out_bins) return qm::set_error(QM_ERR_ARGUMENT, "qm_distribution_with_line: out_bins aliases bins");
+    if (!(scale > 0.0) || !std::isfinite(scale))
+        return qm::set_error(QM_ERR_ARGUMENT, "qm_distribution_with_line: scale must be above 0 and finite");
+    if (n_values > (size_t)INT32_MAX / 2)
+        return qm::set_error(QM_ERR_ARGUMENT, "qm_distribution_with_line: too many values");
+    for (size_t k = 0; k < n_values; ++k)
+        if (!(values[2 * k] >= 0.0) || !(values[2 * k + 1] >= 0.0))
+            return qm::set_error(QM_ERR_ARGUMENT, "qm_distribution_with_line: value " + std::to_string(k) +
+                                                      " has a negative or NaN intensity or share");
+    const OwnedValues line = sorted_values(values, n_values);
+    qm::dist::with_line(bin_db, n_bins, bins, silent, line.view(), scale, out_bins, out_silent);
+    return QM_OK;
+}
+
+qm_status qm_distribution_exceeded_db(double bin_db, const double *bins, double exceeded, double *level_db) {
+    int n_bins = 0;
+    const qm_status status = grid("qm_distribution_exceeded_db", bin_db, n_bins);
+    if (status != QM_OK) return status;
+    if (bins == nullptr || level_db == nullptr)
+        return qm::set_error(QM_ERR_ARGUMENT, "qm_distribution_exceeded_db: null bins or level_db");
+    *level_db = qm::dist::exceeded_db(bins, n_bins, exceeded);
+    return QM_OK;
+}
+
+qm_status qm_distribution_line_values(double lambda, double duty, double *values, size_t cap, size_t *n_values) {
+    if (n_values == nullptr || (cap > 0 && values == nullptr))
+        return qm::set_error(QM_ERR_ARGUMENT, "qm_distribution_line_values: null values or n_values");
+    if (!std::isnan(duty)) {
+        if (!(duty > 0.0 && duty <= 1.0))
+            return qm::set_error(QM_ERR_ARGUMENT, "qm_distribution_line_values: duty must lie in (0, 1]");
+        *n_values = 2;
+        if (cap < 2)
+            return qm::set_error(QM_ERR_CAPACITY, "qm_distribution_line_values: 2 values, room for " + std::to_string(cap));
+        values[0] = 0.0;
+        values[1] = 1.0 - duty;
+        values[2] = 1.0 / duty;
+        values[3] = duty;
+        return QM_OK;
+    }
+    if (std::isnan(lambda)) return qm::set_error(QM_ERR_ARGUMENT, "qm_distribution_line_values: lambda is NaN");
+    *n_values = qm::dist::NODES;
+    if (cap < (size_t)qm::dist::NODES)
+        return qm::set_error(QM_ERR_CAPACITY, "qm_distribution_line_values: " + std::to_string(qm::dist::NODES) +
+                                                  " values, room for " + std::to_string(cap));
+    const float *table = qm::line_level_table_shared().data();
+    for (int k = 0; k < qm::dist::NODES; ++k) {
+        double p, share;
+        qm::dist::node(k, p, share);
+        values[2 * k] = qm::line_relative_intensity(table, lambda, p);
+        values[2 * k + 1] = share;
+    }
+    return QM_OK;
+}
+
+qm_status qm_distribution_pass_values(double mean, double *values, size_t cap, size_t *n_values) {
+    if (n_values == nullptr || (cap > 0 && values == nullptr))
+        return qm::set_error(QM_ERR_ARGUMENT, "qm_distribution_pass_values: null values or n_values");
+    // Above about 745 the silence's share exp(-mean) underflows to 0, every share after it stays
+    // 0 and the time left never falls under 1e-12: the stream is then steady to any decibel grid.
+    if (!(mean > 0.0) || !(mean <= 700.0))
+        return qm::set_error(QM_ERR_ARGUMENT, "qm_distribution_pass_values: mean must lie in (0, 700]");
+    size_t n = 0;
+    auto push = [&](double value, double share) {
+        if (n < cap) {
+            values[2 * n] = value;
+            values[2 * n + 1] = share;
+        }
+        ++n;
+    };
+    // Poisson numbers of passes in progress, each at the stream's mean over `mean`, up to the
+    // number a moment in 1e12 exceeds, which takes what is left of the time and of the mean;
+    // the time left after the silence is -expm1(-mean), exact for tiny means.
+    double share = std::exp(-mean);
+    push(0.0, share);
+    double time_left = -std::expm1(-mean), mean_left = 1.0, count = 0.0;
+    for (;;) {
+        count += 1.0;
+        share *= mean / count;
+        if (time_left - share <= 1e-12) {
+            push(mean_left / time_left, time_left);
+            break;
+        }
+        time_left -= share;
+        mean_left -= share * count / mean;
+        push(count / mean, share);
+    }
+    *n_values = n;
+    if (n > cap)
+        return qm::set_error(QM_ERR_CAPACITY,
+                             "qm_distribution_pass_values: " + std::to_string(n) + " values, room for " + std::to_string(cap));
+    return QM_OK;
+}
+
+}  // extern "C"

@@ -2663,6 +2663,10 @@ const std::vector<float> &line_level_table() {
 
 }  // namespace
 
+namespace qm {
+const std::vector<float> &line_level_table_shared() { return line_level_table(); }
+}  // namespace qm
+
 extern "C" {
 
 qm_status qm_line_level_table(float *table) {

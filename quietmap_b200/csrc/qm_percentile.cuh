@@ -86,8 +86,10 @@ __host__ __device__ inline double line_relative_intensity(const float *table, do
     return value;
 }
 
-__global__ void __launch_bounds__(256) line_level_kernel(const float *table, const double *lambda, const double *p,
-                                                         size_t n, double *out) {
+// Internal linkage: every translation unit that includes this header for the sampler gets its
+// own copy of the kernel, and only qm_lib.cu launches it.
+static __global__ void __launch_bounds__(256) line_level_kernel(const float *table, const double *lambda, const double *p,
+                                                                size_t n, double *out) {
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
         out[i] = line_relative_intensity(table, lambda[i], p[i]);
 }

@@ -5,6 +5,7 @@ raises. The library is built in-tree by quietmap_b200/build.py (or `__graft_entr
 """
 
 import ctypes as C
+import math
 import os
 
 import numpy as np
@@ -147,6 +148,16 @@ def lib():
         L.qm_skyline_arcs.restype = C.c_int
         L.qm_skyline_free.argtypes = [C.c_void_p]
         L.qm_skyline_free.restype = None
+        L.qm_distribution_bins.argtypes = [C.c_double, C.POINTER(C.c_size_t)]
+        L.qm_distribution_bins.restype = C.c_int
+        L.qm_distribution_with_line.argtypes = [C.c_double, _D, C.c_double, _D, C.c_size_t, C.c_double, _D, _D]
+        L.qm_distribution_with_line.restype = C.c_int
+        L.qm_distribution_exceeded_db.argtypes = [C.c_double, _D, C.c_double, _D]
+        L.qm_distribution_exceeded_db.restype = C.c_int
+        L.qm_distribution_line_values.argtypes = [C.c_double, C.c_double, _D, C.c_size_t, C.POINTER(C.c_size_t)]
+        L.qm_distribution_line_values.restype = C.c_int
+        L.qm_distribution_pass_values.argtypes = [C.c_double, _D, C.c_size_t, C.POINTER(C.c_size_t)]
+        L.qm_distribution_pass_values.restype = C.c_int
         if L.qm_abi_version() != abi.ABI_VERSION:
             raise QmError(abi.QM_ERR_UNSUPPORTED, "library ABI version mismatch")
         _lib = L
@@ -393,6 +404,52 @@ def line_quadrature_nodes(start, end, arcs=None, skyline=None, receiver_xy=None,
                                           nodes.ctypes.data, cap, C.byref(n), C.byref(info)))
     figures = {k: getattr(info, k) for k, _ in abi.LinePieceInfo._fields_}
     return nodes[:n.value].copy(), figures
+
+
+def distribution_bins(bin_db):
+    """The bins of a level-distribution grid of bin_db (qm_distribution_bins)."""
+    n = C.c_size_t()
+    _check(lib().qm_distribution_bins(float(bin_db), C.byref(n)))
+    return n.value
+
+
+def distribution_with_line(bin_db, bins, silent, values, scale=1.0):
+    """A distribution (bins [n][2] of share and share x mean intensity, and its silence) with a
+    line of (intensity, share) values times `scale` added (qm_distribution_with_line):
+    (bins, silent)."""
+    b = np.ascontiguousarray(np.asarray(bins, dtype=np.float64).reshape(-1, 2))
+    v = np.ascontiguousarray(np.asarray(values, dtype=np.float64).reshape(-1, 2))
+    out = np.zeros_like(b)
+    out_silent = C.c_double()
+    _check(lib().qm_distribution_with_line(float(bin_db), abi.ptr(b, C.c_double), float(silent),
+                                           abi.ptr(v, C.c_double) if len(v) else None, len(v), float(scale),
+                                           abi.ptr(out, C.c_double), C.byref(out_silent)))
+    return out, out_silent.value
+
+
+def distribution_exceeded_db(bin_db, bins, exceeded):
+    b = np.ascontiguousarray(np.asarray(bins, dtype=np.float64).reshape(-1, 2))
+    level = C.c_double()
+    _check(lib().qm_distribution_exceeded_db(float(bin_db), abi.ptr(b, C.c_double), float(exceeded), C.byref(level)))
+    return level.value
+
+
+def distribution_line_values(lam, duty=None, cap=124):
+    """A line's (relative intensity, share) values (qm_distribution_line_values): Kurze's quantiles
+    at `lam` at the node probabilities, or an event's over its `duty`."""
+    out = np.zeros((cap, 2))
+    n = C.c_size_t()
+    _check(lib().qm_distribution_line_values(float(lam), math.nan if duty is None else float(duty),
+                                             abi.ptr(out, C.c_double), cap, C.byref(n)))
+    return out[:n.value].copy()
+
+
+def distribution_pass_values(mean, cap=4096):
+    """A stream of passes' (relative intensity, share) values (qm_distribution_pass_values)."""
+    out = np.zeros((cap, 2))
+    n = C.c_size_t()
+    _check(lib().qm_distribution_pass_values(float(mean), abi.ptr(out, C.c_double), cap, C.byref(n)))
+    return out[:n.value].copy()
 
 
 def terrain_decode(data):
