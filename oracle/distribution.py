@@ -192,3 +192,130 @@ class Distribution:
         silence = Distribution(bin_db)
         silence.silent = 1.0
         return silence.with_line(LineValues([(10.0 ** (level / 10.0), share) for level, share in levels]))
+
+
+# ---------------------------------------------------------------------------------------------
+# Layers of lines over a period (popup/src/percentiles.rs:88-282, percentiles/lines.rs:8-248),
+# without hourly profiles: every line at its period's mean flow, one group of hours.
+
+WEATHER_STATES = 10                      # percentiles/weather.rs:131
+HOLDS_MEAN_LAMBDA = 10.0                 # lines.rs:240
+PASSES_HOLD_MEAN = 2.0 * math.pi * HOLDS_MEAN_LAMBDA   # lines.rs:243
+HELD_EXCEEDED = 1e-3                     # lines.rs:247
+HELD_SHARE = 1e-2                        # lines.rs:248
+MIN_POSITIVE = 2.2250738585072014e-308   # the least normal f64
+
+
+class Line:
+    """One source whose level varies in time, per period (lines.rs:8-24): its mean energy, its
+    means in the weather states, Kurze's lambda, an event's duty or a stream's passes in
+    progress (None: not that kind)."""
+
+    def __init__(self, energy, means, lam, duty=None, passing=None):
+        self.energy = list(energy)
+        self.means = [list(m) for m in means]
+        self.lam = list(lam)
+        self.duty = None if duty is None else list(duty)
+        self.passing = None if passing is None else list(passing)
+
+    def shape(self, period, factor=1.0):
+        """(values, exceeded) where the line moves the level in `period`, None where it holds
+        its mean or is silent (lines.rs:172-195): a stream's passes unless that many hold the
+        mean, an event's duty while it sounds, a sparse line's Kurze values with the intensity
+        it exceeds a thousandth of the time."""
+        if self.passing is not None:
+            mean = self.passing[period]
+            return (pass_values(mean), None) if MIN_POSITIVE <= mean < PASSES_HOLD_MEAN else None
+        lam = self.lam[period] * factor
+        if self.duty is not None:
+            duty = self.duty[period]
+            return (line_values(0.0, duty=duty), None) if duty > 0.0 else None
+        if lam >= HOLDS_MEAN_LAMBDA:
+            return None
+        return line_values(lam), oracle.relative_intensity(lam, 1.0 - HELD_EXCEEDED)
+
+
+def moment(lines, shapes, state_means, factors, steady, period):
+    """The energy that holds steady and the lines that move the level (percentiles.rs:236-282):
+    (floor, holding [(index, mean)], moving [(index, values, mean)]), the events and streams
+    first, then the sparse lines whose level exceeded a thousandth of the time reaches a
+    hundredth of the steady energy."""
+    floor, holding, moving, held = steady, [], [], []
+    for index, (line, shape) in enumerate(zip(lines, shapes)):
+        mean = state_means[index] * factors[index]
+        if line.energy[period] <= 0.0 or mean <= 0.0:
+            continue
+        if shape is not None and shape[1] is None:
+            moving.append((index, shape[0], mean))
+        elif shape is not None:
+            held.append((index, shape[0], mean, shape[1]))
+        elif line.duty is not None:
+            continue
+        else:
+            floor += mean
+            holding.append((index, mean))
+    steady_energy = floor
+    for _, _, mean, _ in held:
+        steady_energy += mean
+    for index, values, mean, exceeded in held:
+        if mean * exceeded < HELD_SHARE * steady_energy:
+            floor += mean
+            holding.append((index, mean))
+        else:
+            moving.append((index, values, mean))
+    return floor, holding, moving
+
+
+def layer_states(lines, steady, period, bin_db):
+    """A layer's distribution in each weather state of `period` with its floor where no line
+    moves (percentiles.rs:172-211): its steady energy and holding lines first, then each moving
+    line added."""
+    factors = [1.0] * len(lines)
+    shapes = [line.shape(period, 1.0) for line in lines]
+    states = []
+    for state in range(WEATHER_STATES):
+        if state > 0 and all(line.means[period][state] == line.means[period][state - 1] for line in lines):
+            states.append(states[-1])
+            continue
+        state_means = [line.means[period][state] for line in lines]
+        floor, _, moving = moment(lines, shapes, state_means, factors, steady, period)
+        total = Distribution(bin_db)
+        total.silent = 1.0
+        total = total.over(floor)
+        for _, values, mean in moving:
+            total = total.with_line(values, mean)
+        states.append((total, floor if not moving else None))
+    return states
+
+
+def layered_distributions(layers, bin_db):
+    """Per period each layer's distribution and the place's (percentiles.rs:88-160) for layers of
+    (lines, steady per period) that follow no hourly profile: each weather state a tenth of the
+    time; in each, the steady layers' floors summed, then the moving layers' distributions added
+    as independent sounds."""
+    each = [[None] * 3 for _ in layers]
+    whole = []
+    for p in range(3):
+        per_layer = [layer_states(lines, steady[p], p, bin_db) for lines, steady in layers]
+        for k, states in enumerate(per_layer):
+            mixture = Distribution(bin_db)
+            for part, _ in states:
+                mixture.add_scaled(part, 1.0 / WEATHER_STATES)
+            each[k][p] = mixture
+        mixed = Distribution(bin_db)
+        weight = 1.0 / WEATHER_STATES
+        for state in range(WEATHER_STATES):
+            parts = [states[state] for states in per_layer]
+            floor = 0.0
+            for _, f in parts:
+                if f is not None:
+                    floor += f
+            total = Distribution(bin_db)
+            total.silent = 1.0
+            total = total.over(floor)
+            for part, f in parts:
+                if f is None:
+                    total = total.with_distribution(part)
+            mixed.add_scaled(total, weight)
+        whole.append(mixed)
+    return each, whole
