@@ -54,6 +54,33 @@ qm_status qm_distribution_line_values(double lambda, double duty, double *values
  * call returns QM_ERR_CAPACITY. */
 qm_status qm_distribution_pass_values(double mean, double *values, size_t cap, size_t *n_values);
 
+/* One line over one period (popup/src/percentiles/lines.rs:8-24, that period's fields): the
+ * layer it sounds in, its mean energy, its means in the weather states, Kurze's lambda (infinite
+ * for a steady source), an event's duty (NaN: not an event) and a stream's passes in progress
+ * (NaN: not a stream). Every line runs at its period's mean flow: hourly profiles are the
+ * caller's (hours of a profiled road are separate calls). */
+#define QM_WEATHER_STATES 10
+typedef struct {
+    uint32_t layer;
+    uint32_t reserved;
+    double energy;
+    double means[QM_WEATHER_STATES];
+    double lambda;
+    double duty;
+    double passing;
+} qm_period_line;
+
+/* layered_distributions for one period and one group of hours (popup/src/percentiles.rs:88-160
+ * with layer_states and moment, :172-282): each layer's distribution of the summed level over the
+ * period and the place's, each weather state a tenth of the time; in a state each layer is its
+ * steady energy and its lines that hold their mean, with its moving lines added (events, passes,
+ * sparse lines not held), and the place is the steady layers' floors with the moving layers'
+ * distributions added. Lines keep their order within a layer. layer_bins[n_layers][n_bins][2],
+ * layer_silent[n_layers], place_bins[n_bins][2]. */
+qm_status qm_distribution_layers(double bin_db, const qm_period_line *lines, size_t n_lines, const double *steady,
+                                 size_t n_layers, double *layer_bins, double *layer_silent, double *place_bins,
+                                 double *place_silent);
+
 #ifdef __cplusplus
 }
 #endif

@@ -254,9 +254,8 @@ def moment(lines, shapes, state_means, factors, steady, period):
         else:
             floor += mean
             holding.append((index, mean))
-    steady_energy = floor
-    for _, _, mean, _ in held:
-        steady_energy += mean
+    # The held lines' means summed on their own, then added to the floor (percentiles.rs:270-272).
+    steady_energy = floor + sum(mean for _, _, mean, _ in held)
     for index, values, mean, exceeded in held:
         if mean * exceeded < HELD_SHARE * steady_energy:
             floor += mean

@@ -147,6 +147,10 @@ LINE_NODE_DTYPE = np.dtype([("along_m", "<f8"), ("weight_rad", "<f8"), ("obstacl
 LINE_MAX_NODES = 705
 DISTRIBUTION_MAX_BINS = 1800
 DISTRIBUTION_LINE_NODES = 124
+WEATHER_STATES = 10
+PERIOD_LINE_DTYPE = np.dtype([("layer", "<u4"), ("reserved", "<u4"), ("energy", "<f8"),
+                              ("means", "<f8", (WEATHER_STATES,)), ("lambda", "<f8"), ("duty", "<f8"),
+                              ("passing", "<f8")], align=True)
 
 
 class LinePieceInfo(C.Structure):
@@ -197,6 +201,7 @@ assert FLIGHT_SEGMENT_DTYPE.itemsize == 48
 assert OUTLINE_DTYPE.itemsize == C.sizeof(Outline)
 assert SOURCE_DTYPE.itemsize == C.sizeof(Source)
 assert LINE_NODE_DTYPE.itemsize == 24
+assert PERIOD_LINE_DTYPE.itemsize == 120
 
 
 def ptr(array, ctype):

@@ -15,6 +15,7 @@
 #include "qm_percentile.cuh"
 
 static_assert(QM_DISTRIBUTION_LINE_NODES == qm::dist::NODES, "the header's node count is the grid's");
+static_assert(QM_WEATHER_STATES == qm::dist::WEATHER_STATES, "the header's weather states are the mixture's");
 
 namespace {
 
@@ -50,6 +51,38 @@ OwnedValues sorted_values(const double *values, size_t n) {
         out.pairs[2 * k + 1] = list[k].second;
         out.sums[2 * (k + 1)] = out.sums[2 * k] + list[k].second;
         out.sums[2 * (k + 1) + 1] = out.sums[2 * k + 1] + list[k].second * list[k].first;
+    }
+    return out;
+}
+
+// pass_values (distribution.rs:283-298) for a mean in (0, 700], in the order they arise.
+std::vector<double> pass_pairs(double mean) {
+    std::vector<double> out;
+    double share = std::exp(-mean);
+    out.insert(out.end(), {0.0, share});
+    double time_left = -std::expm1(-mean), mean_left = 1.0, count = 0.0;
+    for (;;) {
+        count += 1.0;
+        share *= mean / count;
+        if (time_left - share <= 1e-12) {
+            out.insert(out.end(), {mean_left / time_left, time_left});
+            return out;
+        }
+        time_left -= share;
+        mean_left -= share * count / mean;
+        out.insert(out.end(), {count / mean, share});
+    }
+}
+
+// Kurze's values at lambda at the node probabilities, by the library's sampler.
+std::vector<double> kurze_pairs(double lambda) {
+    const float *table = qm::line_level_table_shared().data();
+    std::vector<double> out(2 * qm::dist::NODES);
+    for (int k = 0; k < qm::dist::NODES; ++k) {
+        double p, share;
+        qm::dist::node(k, p, share);
+        out[2 * k] = qm::line_relative_intensity(table, lambda, p);
+        out[2 * k + 1] = share;
     }
     return out;
 }
@@ -124,6 +157,103 @@ qm_status qm_distribution_line_values(double lambda, double duty, double *values
         qm::dist::node(k, p, share);
         values[2 * k] = qm::line_relative_intensity(table, lambda, p);
         values[2 * k + 1] = share;
+    }
+    return QM_OK;
+}
+
+qm_status qm_distribution_layers(double bin_db, const qm_period_line *lines, size_t n_lines, const double *steady,
+                                 size_t n_layers, double *layer_bins, double *layer_silent, double *place_bins,
+                                 double *place_silent) {
+    int n_bins = 0;
+    const qm_status status = grid("qm_distribution_layers", bin_db, n_bins);
+    if (status != QM_OK) return status;
+    if ((n_lines > 0 && lines == nullptr) || (n_layers > 0 && (steady == nullptr || layer_bins == nullptr ||
+                                                               layer_silent == nullptr)) ||
+        place_bins == nullptr || place_silent == nullptr)
+        return qm::set_error(QM_ERR_ARGUMENT, "qm_distribution_layers: null lines, steady or output");
+    if (n_lines > (size_t)INT32_MAX) return qm::set_error(QM_ERR_ARGUMENT, "qm_distribution_layers: too many lines");
+    for (size_t l = 0; l < n_layers; ++l)
+        if (!(steady[l] >= 0.0) || !std::isfinite(steady[l]))
+            return qm::set_error(QM_ERR_ARGUMENT, "qm_distribution_layers: steady energy of layer " + std::to_string(l) +
+                                                      " is negative or not finite");
+    // Each line's shape in the period (lines.rs:172-195), its values in the order LineValues
+    // keeps them.
+    std::vector<OwnedValues> owned(n_lines);
+    std::vector<std::vector<qm::dist::PeriodLine>> layers(n_layers);
+    const double min_positive = 2.2250738585072014e-308;
+    for (size_t k = 0; k < n_lines; ++k) {
+        const qm_period_line &line = lines[k];
+        const std::string which = "qm_distribution_layers: line " + std::to_string(k);
+        if (line.layer >= n_layers) return qm::set_error(QM_ERR_ARGUMENT, which + " names layer " + std::to_string(line.layer));
+        if (std::isnan(line.energy) || std::isnan(line.lambda))
+            return qm::set_error(QM_ERR_ARGUMENT, which + " has a NaN energy or lambda");
+        for (int st = 0; st < QM_WEATHER_STATES; ++st)
+            if (!(line.means[st] >= 0.0) || !std::isfinite(line.means[st]))
+                return qm::set_error(QM_ERR_ARGUMENT, which + " has a negative or non-finite mean");
+        qm::dist::PeriodLine entry{line.energy, line.means, qm::dist::SHAPE_HOLDS, qm::dist::Values{nullptr, nullptr, 0},
+                                   0.0};
+        std::vector<double> pairs;
+        if (!std::isnan(line.passing)) {
+            if (line.passing >= min_positive && line.passing < qm::dist::PASSES_HOLD_MEAN) {
+                entry.kind = qm::dist::SHAPE_MOVES;
+                pairs = pass_pairs(line.passing);
+            }
+        } else if (!std::isnan(line.duty)) {
+            if (line.duty > 1.0) return qm::set_error(QM_ERR_ARGUMENT, which + " has a duty above 1");
+            if (line.duty > 0.0) {
+                entry.kind = qm::dist::SHAPE_MOVES;
+                pairs = {0.0, 1.0 - line.duty, 1.0 / line.duty, line.duty};
+            } else {
+                entry.kind = qm::dist::SHAPE_SILENT;
+            }
+        } else if (!(line.lambda * 1.0 >= qm::dist::HOLDS_MEAN_LAMBDA)) {
+            entry.kind = qm::dist::SHAPE_SPARSE;
+            pairs = kurze_pairs(line.lambda);
+            entry.exceeded = qm::line_relative_intensity(qm::line_level_table_shared().data(), line.lambda,
+                                                         1.0 - qm::dist::HELD_EXCEEDED);
+        }
+        if (!pairs.empty()) {
+            owned[k] = sorted_values(pairs.data(), pairs.size() / 2);
+            entry.values = owned[k].view();
+        }
+        layers[line.layer].push_back(entry);
+    }
+    const size_t bins2 = 2 * (size_t)n_bins;
+    std::vector<double> a(bins2), b(bins2), c(bins2), d(bins2), states_silent(n_layers);
+    std::vector<double> state_bins(n_layers * bins2), floors(n_layers), pairs(2 * ((size_t)n_bins + 1)),
+        sums(2 * ((size_t)n_bins + 2));
+    std::vector<char> holds(n_layers);
+    for (size_t b2 = 0; b2 < n_layers * bins2; ++b2) layer_bins[b2] = 0.0;
+    for (size_t l = 0; l < n_layers; ++l) layer_silent[l] = 0.0;
+    for (size_t b2 = 0; b2 < bins2; ++b2) place_bins[b2] = 0.0;
+    *place_silent = 0.0;
+    const double weight = 1.0 / (double)qm::dist::WEATHER_STATES;
+    for (int state = 0; state < qm::dist::WEATHER_STATES; ++state) {
+        for (size_t l = 0; l < n_layers; ++l) {
+            double *out = nullptr, silent = 0.0;
+            holds[l] = qm::dist::layer_state(bin_db, n_bins, layers[l].data(), (int)layers[l].size(), state, steady[l],
+                                             a.data(), b.data(), &out, &silent, &floors[l]);
+            std::copy(out, out + bins2, state_bins.begin() + l * bins2);
+            states_silent[l] = silent;
+            qm::dist::add_scaled(layer_bins + l * bins2, layer_silent + l, out, silent, n_bins, weight);
+        }
+        // The place: the floors of the layers that hold, then each moving layer added.
+        double floor = 0.0;
+        for (size_t l = 0; l < n_layers; ++l)
+            if (holds[l]) floor += floors[l];
+        std::fill(c.begin(), c.end(), 0.0);
+        double silent;
+        qm::dist::over(bin_db, n_bins, c.data(), 1.0, floor, d.data(), &silent);
+        double *current = d.data(), *spare = c.data();
+        for (size_t l = 0; l < n_layers; ++l) {
+            if (holds[l]) continue;
+            double next_silent;
+            qm::dist::with_distribution(bin_db, n_bins, current, silent, state_bins.data() + l * bins2, states_silent[l],
+                                        pairs.data(), sums.data(), spare, &next_silent);
+            std::swap(current, spare);
+            silent = next_silent;
+        }
+        qm::dist::add_scaled(place_bins, place_silent, current, silent, n_bins, weight);
     }
     return QM_OK;
 }

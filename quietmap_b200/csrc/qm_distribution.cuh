@@ -176,5 +176,148 @@ __host__ __device__ inline void node(int k, double &p, double &share) {
     }
 }
 
+// A single steady intensity as a line's values: one pair (intensity, all the time) and its sums.
+struct Steady {
+    double pairs[2], sums[4];
+    __host__ __device__ explicit Steady(double intensity) {
+        pairs[0] = intensity;
+        pairs[1] = 1.0;
+        sums[0] = sums[1] = 0.0;
+        sums[2] = 0.0 + 1.0;
+        sums[3] = 0.0 + 1.0 * intensity;
+    }
+    __host__ __device__ Values view() const { return Values{pairs, sums, 1}; }
+};
+
+// out = in with a steady intensity added at every moment (distribution.rs:208-211).
+__host__ __device__ inline void over(double bin_db, int n_bins, const double *in_bins, double in_silent,
+                                     double intensity, double *out_bins, double *out_silent) {
+    const Steady steady(intensity);
+    with_line(bin_db, n_bins, in_bins, in_silent, steady.view(), 1.0, out_bins, out_silent);
+}
+
+// out = in with an independent distribution `other` added at every moment: its bins' mean
+// intensities and its silence as a line's values, ascending, equal ones in bin order with the
+// silence first (distribution.rs:198-206). scratch_pairs holds 2 (n_bins + 1) doubles and
+// scratch_sums 2 (n_bins + 2).
+__host__ __device__ inline void with_distribution(double bin_db, int n_bins, const double *in_bins, double in_silent,
+                                                  const double *other_bins, double other_silent,
+                                                  double *scratch_pairs, double *scratch_sums, double *out_bins,
+                                                  double *out_silent) {
+    int n = 0;
+    // The silence is 0, under every bin's mean intensity, and comes first in a stable sort.
+    if (other_silent > 0.0) {
+        scratch_pairs[0] = 0.0;
+        scratch_pairs[1] = other_silent;
+        n = 1;
+    }
+    for (int b = 0; b < n_bins; ++b) {
+        const double share = other_bins[2 * b];
+        if (!(share > 0.0)) continue;
+        const double intensity = other_bins[2 * b + 1] / share;
+        // Insertion into the ascending run so far (stable: after every equal value); bins' means
+        // rise with the bin, so this is mostly an append.
+        int at = n;
+        while (at > 0 && scratch_pairs[2 * (at - 1)] > intensity) {
+            scratch_pairs[2 * at] = scratch_pairs[2 * (at - 1)];
+            scratch_pairs[2 * at + 1] = scratch_pairs[2 * (at - 1) + 1];
+            --at;
+        }
+        scratch_pairs[2 * at] = intensity;
+        scratch_pairs[2 * at + 1] = share;
+        ++n;
+    }
+    scratch_sums[0] = scratch_sums[1] = 0.0;
+    for (int k = 0; k < n; ++k) {
+        scratch_sums[2 * (k + 1)] = scratch_sums[2 * k] + scratch_pairs[2 * k + 1];
+        scratch_sums[2 * (k + 1) + 1] = scratch_sums[2 * k + 1] + scratch_pairs[2 * k + 1] * scratch_pairs[2 * k];
+    }
+    with_line(bin_db, n_bins, in_bins, in_silent, Values{scratch_pairs, scratch_sums, n}, 1.0, out_bins, out_silent);
+}
+
+// Lines over a period (popup/src/percentiles.rs:172-282, percentiles/lines.rs:172-195), every
+// line at its period's mean flow.
+constexpr int WEATHER_STATES = 10;                                 // percentiles/weather.rs:131
+constexpr double HOLDS_MEAN_LAMBDA = 10.0;                         // lines.rs:240
+constexpr double PASSES_HOLD_MEAN = 2.0 * 3.14159265358979323846 * HOLDS_MEAN_LAMBDA;  // lines.rs:243
+constexpr double HELD_EXCEEDED = 1e-3;                             // lines.rs:247
+constexpr double HELD_SHARE = 1e-2;                                // lines.rs:248
+
+// How a line sounds in a period: holding its mean, silent (an event off then), moving the level
+// (an event while it sounds, a stream of passes), or a sparse line that moves the level unless
+// its intensity exceeded a thousandth of the time stays under a hundredth of the steady energy.
+enum ShapeKind : int { SHAPE_HOLDS = 0, SHAPE_SILENT = 1, SHAPE_MOVES = 2, SHAPE_SPARSE = 3 };
+
+struct PeriodLine {
+    double energy;         // the period's mean energy: a line at or under 0 is silent
+    const double *means;   // [WEATHER_STATES]
+    int kind;              // ShapeKind
+    Values values;         // SHAPE_MOVES, SHAPE_SPARSE: intensities relative to the mean
+    double exceeded;       // SHAPE_SPARSE: the relative intensity exceeded a thousandth of the time
+};
+
+// The moment of a layer's lines in a weather state (percentiles.rs:236-282): the steady energy
+// with the lines that hold their mean, and the steady energy the sparse lines are held against.
+__host__ __device__ inline double moment_floor(const PeriodLine *lines, int n, int state, double steady,
+                                               double &steady_energy) {
+    double floor = steady, held = 0.0;
+    for (int k = 0; k < n; ++k) {
+        const double mean = lines[k].means[state] * 1.0;
+        if (lines[k].energy <= 0.0 || mean <= 0.0) continue;
+        if (lines[k].kind == SHAPE_HOLDS) floor += mean;
+        if (lines[k].kind == SHAPE_SPARSE) held += mean;
+    }
+    steady_energy = floor + held;
+    for (int k = 0; k < n; ++k) {
+        const double mean = lines[k].means[state] * 1.0;
+        if (lines[k].energy <= 0.0 || mean <= 0.0 || lines[k].kind != SHAPE_SPARSE) continue;
+        if (mean * lines[k].exceeded < HELD_SHARE * steady_energy) floor += mean;
+    }
+    return floor;
+}
+
+// The lines that move the level in that moment, in the reference's order: the events and
+// streams, then the sparse lines not held; visit(k, mean).
+#pragma nv_exec_check_disable
+template <class Visit>
+__host__ __device__ void moving_lines(const PeriodLine *lines, int n, int state, double steady_energy, Visit &visit) {
+    for (int pass = 0; pass < 2; ++pass)
+        for (int k = 0; k < n; ++k) {
+            const double mean = lines[k].means[state] * 1.0;
+            if (lines[k].energy <= 0.0 || mean <= 0.0) continue;
+            if (pass == 0 && lines[k].kind == SHAPE_MOVES) visit(k, mean);
+            if (pass == 1 && lines[k].kind == SHAPE_SPARSE && !(mean * lines[k].exceeded < HELD_SHARE * steady_energy))
+                visit(k, mean);
+        }
+}
+
+// A layer's distribution in one weather state (percentiles.rs:172-211): its floor, then each
+// moving line added. Returns true where no line moves (the layer holds its floor, written to
+// *floor). a and b are [n_bins][2] work buffers; the result is in *out (a or b).
+__host__ __device__ inline bool layer_state(double bin_db, int n_bins, const PeriodLine *lines, int n, int state,
+                                            double steady, double *a, double *b, double **out, double *out_silent,
+                                            double *floor) {
+    double steady_energy;
+    *floor = moment_floor(lines, n, state, steady, steady_energy);
+    for (int k = 0; k < 2 * n_bins; ++k) a[k] = 0.0;
+    double silent;
+    over(bin_db, n_bins, a, 1.0, *floor, b, &silent);
+    double *current = b, *spare = a;
+    bool moved = false;
+    auto add = [&](int k, double mean) {
+        double next_silent;
+        with_line(bin_db, n_bins, current, silent, lines[k].values, mean, spare, &next_silent);
+        double *t = current;
+        current = spare;
+        spare = t;
+        silent = next_silent;
+        moved = true;
+    };
+    moving_lines(lines, n, state, steady_energy, add);
+    *out = current;
+    *out_silent = silent;
+    return !moved;
+}
+
 }  // namespace dist
 }  // namespace qm

@@ -158,6 +158,8 @@ def lib():
         L.qm_distribution_line_values.restype = C.c_int
         L.qm_distribution_pass_values.argtypes = [C.c_double, _D, C.c_size_t, C.POINTER(C.c_size_t)]
         L.qm_distribution_pass_values.restype = C.c_int
+        L.qm_distribution_layers.argtypes = [C.c_double, C.c_void_p, C.c_size_t, _D, C.c_size_t, _D, _D, _D, _D]
+        L.qm_distribution_layers.restype = C.c_int
         if L.qm_abi_version() != abi.ABI_VERSION:
             raise QmError(abi.QM_ERR_UNSUPPORTED, "library ABI version mismatch")
         _lib = L
@@ -450,6 +452,24 @@ def distribution_pass_values(mean, cap=4096):
     n = C.c_size_t()
     _check(lib().qm_distribution_pass_values(float(mean), abi.ptr(out, C.c_double), cap, C.byref(n)))
     return out[:n.value].copy()
+
+
+def distribution_layers(bin_db, lines, steady):
+    """One period's layers (qm_distribution_layers): `lines` a PERIOD_LINE_DTYPE array, `steady`
+    each layer's steady energy. Returns (layer bins [n_layers][n_bins][2], layer silence,
+    place bins [n_bins][2], place silence)."""
+    rows = np.ascontiguousarray(lines, dtype=abi.PERIOD_LINE_DTYPE)
+    st = np.ascontiguousarray(steady, dtype=np.float64)
+    n_bins = distribution_bins(bin_db)
+    layer_bins = np.zeros((len(st), n_bins, 2))
+    layer_silent = np.zeros(len(st))
+    place_bins = np.zeros((n_bins, 2))
+    place_silent = C.c_double()
+    _check(lib().qm_distribution_layers(float(bin_db), rows.ctypes.data if len(rows) else None, len(rows),
+                                        abi.ptr(st, C.c_double) if len(st) else None, len(st),
+                                        abi.ptr(layer_bins, C.c_double), abi.ptr(layer_silent, C.c_double),
+                                        abi.ptr(place_bins, C.c_double), C.byref(place_silent)))
+    return layer_bins, layer_silent, place_bins, place_silent.value
 
 
 def terrain_decode(data):

@@ -128,3 +128,106 @@ def test_errors():
     start[100] = (0.5, 0.5 * dist.energy(-30.0 + 100 * 0.5))
     out, silent = native.distribution_with_line(0.5, start, 0.5, np.zeros((0, 2)))
     assert np.array_equal(out, np.zeros((360, 2))) and silent == 0.0
+
+
+def _period_rows(layers, period):
+    """The library's rows for one period of the oracle's layers."""
+    rows = []
+    for index, (lines, _) in enumerate(layers):
+        for line in lines:
+            row = np.zeros((), dtype=abi.PERIOD_LINE_DTYPE)
+            row["layer"] = index
+            row["energy"] = line.energy[period]
+            row["means"] = line.means[period]
+            row["lambda"] = line.lam[period]
+            row["duty"] = math.nan if line.duty is None else line.duty[period]
+            row["passing"] = math.nan if line.passing is None else line.passing[period]
+            rows.append(row)
+    return np.array(rows, dtype=abi.PERIOD_LINE_DTYPE)
+
+
+def _place(seed, sparse):
+    """Layers of a random place: steady energy, roads whose means differ by weather state (dense,
+    and with `sparse` also sparse Kurze lines), bells over a duty, flights in classes."""
+    rng = np.random.default_rng(seed)
+    states = dist.WEATHER_STATES
+    e = dist.energy
+
+    def road(level, lam):
+        base = e(level)
+        means = [[base * (1.0 + 0.3 * rng.random()) for _ in range(states)] for _ in range(3)]
+        return dist.Line([base] * 3, means, lam)
+
+    lams = [[20.0, 12.0, 10.0], [1e3, 50.0, 10.5]] + ([[0.03, 0.01, 0.002], [2.0, 1.0, 0.4], [8.0, 3.0, 0.9]]
+                                                       if sparse else [])
+    roads = ([road(rng.uniform(30.0, 65.0), lam) for lam in lams], [e(rng.uniform(20.0, 40.0))] * 3)
+    bells = dist.Line([e(50.0)] * 3, [[e(50.0)] * states] * 3, [math.inf] * 3, duty=[0.05, 0.0, 0.01])
+    events = ([bells], [0.0] * 3)
+    classes = []
+    for passing, level in ((0.02, 45.0), (0.4, 40.0), (80.0, 35.0), (1e-320, 50.0)):
+        energy = [e(level), e(level - 3.0), 0.0]
+        classes.append(dist.Line(energy, [[x] * states for x in energy], [math.inf] * 3,
+                                 passing=[passing, passing * 0.5, 0.0]))
+    planes = (classes, [0.0] * 3)
+    quiet = ([], [e(25.0)] * 3)
+    return [roads, events, planes, quiet]
+
+
+@pytest.mark.parametrize("bin_db", [0.5, 2.0])
+def test_layers_match_the_oracle_to_the_bit(bin_db):
+    """A place of dense roads, bells, flights and a steady layer: every layer's distribution and
+    the place's, each period, equal the oracle's to the bit."""
+    layers = _place(3, sparse=False)
+    each, whole = dist.layered_distributions(layers, bin_db)
+    for p in range(3):
+        got_each, got_silent, got_whole, got_whole_silent = native.distribution_layers(
+            bin_db, _period_rows(layers, p), [steady[p] for _, steady in layers])
+        for k in range(len(layers)):
+            assert np.array_equal(got_each[k], _bins(each[k][p])) and got_silent[k] == each[k][p].silent, (p, k)
+        assert np.array_equal(got_whole, _bins(whole[p])) and got_whole_silent == whole[p].silent, p
+
+
+def test_layers_with_sparse_lines_match_the_oracle():
+    """With sparse Kurze lines, whose values come from the library's sampler (within 1e-12 of the
+    oracle's), every layer's and the place's mean intensity and exceeded levels stay within the
+    sampler's agreement."""
+    layers = _place(5, sparse=True)
+    each, whole = dist.layered_distributions(layers, 0.5)
+    for p in range(3):
+        got_each, got_silent, got_whole, got_whole_silent = native.distribution_layers(
+            0.5, _period_rows(layers, p), [steady[p] for _, steady in layers])
+        pairs = [(got_each[k], got_silent[k], each[k][p]) for k in range(len(layers))]
+        pairs.append((got_whole, got_whole_silent, whole[p]))
+        for got, silent, want in pairs:
+            mean = float(got[:, 1].sum())
+            want_mean = sum(i * s for i, s in want.intensities())
+            assert abs(mean - want_mean) <= 1e-9 * want_mean and abs(silent - want.silent) <= 1e-12
+            for exceeded in (0.05, 0.1, 0.5, 0.9):
+                level, want_level = native.distribution_exceeded_db(0.5, got, exceeded), want.exceeded_db(exceeded)
+                assert level == want_level or abs(level - want_level) < 1e-6, (p, exceeded, level, want_level)
+
+
+def test_layers_errors():
+    rows = np.zeros(1, dtype=abi.PERIOD_LINE_DTYPE)
+    rows[0]["energy"], rows[0]["means"], rows[0]["lambda"] = 1.0, 1.0, math.inf
+    rows[0]["duty"], rows[0]["passing"] = math.nan, math.nan
+    bad = rows.copy()
+    bad[0]["layer"] = 2
+    for case, steady, words in ((bad, [0.0, 0.0], "names layer 2"), (rows, [-1.0], "steady energy of layer 0")):
+        with pytest.raises(native.QmError) as err:
+            native.distribution_layers(0.5, case, steady)
+        assert err.value.status == abi.QM_ERR_ARGUMENT and words in str(err.value)
+    for field, value in (("lambda", math.nan), ("duty", 1.5)):
+        bad = rows.copy()
+        bad[0][field] = value
+        with pytest.raises(native.QmError) as err:
+            native.distribution_layers(0.5, bad, [0.0])
+        assert err.value.status == abi.QM_ERR_ARGUMENT and "line 0" in str(err.value)
+    bad = rows.copy()
+    bad[0]["means"][3] = -1.0
+    with pytest.raises(native.QmError):
+        native.distribution_layers(0.5, bad, [0.0])
+    # A steady line alone holds its mean in every state: one bin, all the time.
+    layer_bins, silent, place, place_silent = native.distribution_layers(0.5, rows, [0.0])
+    assert silent[0] == 0.0 and np.count_nonzero(layer_bins[0][:, 0]) == 1
+    assert abs(native.distribution_exceeded_db(0.5, place, 0.99)) < 1e-9 and place_silent == 0.0
