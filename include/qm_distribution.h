@@ -57,8 +57,7 @@ qm_status qm_distribution_pass_values(double mean, double *values, size_t cap, s
 /* One line over one period (popup/src/percentiles/lines.rs:8-24, that period's fields): the
  * layer it sounds in, its mean energy, its means in the weather states, Kurze's lambda (infinite
  * for a steady source), an event's duty (NaN: not an event) and a stream's passes in progress
- * (NaN: not a stream). Every line runs at its period's mean flow: hourly profiles are the
- * caller's (hours of a profiled road are separate calls). */
+ * (NaN: not a stream). */
 #define QM_WEATHER_STATES 10
 typedef struct {
     uint32_t layer;
@@ -75,11 +74,24 @@ typedef struct {
  * period and the place's, each weather state a tenth of the time; in a state each layer is its
  * steady energy and its lines that hold their mean, with its moving lines added (events, passes,
  * sparse lines not held), and the place is the steady layers' floors with the moving layers'
- * distributions added. Lines keep their order within a layer. layer_bins[n_layers][n_bins][2],
- * layer_silent[n_layers], place_bins[n_bins][2]. */
+ * distributions added. Lines keep their order within a layer; every line runs at its period's
+ * mean flow. layer_bins[n_layers][n_bins][2], layer_silent[n_layers], place_bins[n_bins][2]. */
 qm_status qm_distribution_layers(double bin_db, const qm_period_line *lines, size_t n_lines, const double *steady,
                                  size_t n_layers, double *layer_bins, double *layer_silent, double *place_bins,
                                  double *place_silent);
+
+/* The same over a period's groups of hours (popup/src/percentiles.rs:88-160 with hour_groups,
+ * percentiles/traffic.rs:251-279): a period of `hours` hours whose groups hold group_hours[g]
+ * hours each; profiled[k] marks a line that follows an hourly profile and factors[g][n_lines]
+ * its flow in group g against the period's mean (the mean of its profile's hour factors there,
+ * which scales its lambda and its means). A layer none of whose lines is profiled is computed
+ * once at its mean flow; the others per group, each group weighing its hours' share. The hourly
+ * profiles themselves are the caller's (the reference's measured shares). */
+qm_status qm_distribution_layers_grouped(double bin_db, const qm_period_line *lines, size_t n_lines,
+                                         const double *steady, size_t n_layers, uint32_t hours,
+                                         const uint32_t *group_hours, size_t n_groups, const double *factors,
+                                         const uint8_t *profiled, double *layer_bins, double *layer_silent,
+                                         double *place_bins, double *place_silent);
 
 #ifdef __cplusplus
 }

@@ -265,12 +265,13 @@ def moment(lines, shapes, state_means, factors, steady, period):
     return floor, holding, moving
 
 
-def layer_states(lines, steady, period, bin_db):
+def layer_states(lines, steady, period, bin_db, factors=None):
     """A layer's distribution in each weather state of `period` with its floor where no line
     moves (percentiles.rs:172-211): its steady energy and holding lines first, then each moving
-    line added."""
-    factors = [1.0] * len(lines)
-    shapes = [line.shape(period, 1.0) for line in lines]
+    line added. `factors`: each line's flow in the hours against the period's mean (1 without a
+    profile)."""
+    factors = [1.0] * len(lines) if factors is None else list(factors)
+    shapes = [line.shape(period, factor) for line, factor in zip(lines, factors)]
     states = []
     for state in range(WEATHER_STATES):
         if state > 0 and all(line.means[period][state] == line.means[period][state - 1] for line in lines):
@@ -287,34 +288,55 @@ def layer_states(lines, steady, period, bin_db):
     return states
 
 
-def layered_distributions(layers, bin_db):
+def layered_distributions(layers, bin_db, groups=None):
     """Per period each layer's distribution and the place's (percentiles.rs:88-160) for layers of
-    (lines, steady per period) that follow no hourly profile: each weather state a tenth of the
-    time; in each, the steady layers' floors summed, then the moving layers' distributions added
-    as independent sounds."""
+    (lines, steady per period): for every group of hours and weather state, each layer's
+    distribution, and the place's with the steady layers' floors summed and the moving layers'
+    distributions added as independent sounds; the groups and states averaged by their shares of
+    the time. `groups` (None: no line follows a profile) gives per period (hours, [(hours in the
+    group, per layer its lines' flow factors in the group or None where no line of the layer
+    follows a profile)]); a layer with no profiled line is computed once at its mean flow."""
     each = [[None] * 3 for _ in layers]
     whole = []
     for p in range(3):
-        per_layer = [layer_states(lines, steady[p], p, bin_db) for lines, steady in layers]
-        for k, states in enumerate(per_layer):
+        hours, parts_of = (1, [(1, [None] * len(layers))]) if groups is None else groups[p]
+        alike = [layer_states(lines, steady[p], p, bin_db) if parts_of[0][1][k] is None else None
+                 for k, (lines, steady) in enumerate(layers)]
+        parts = []
+        for slots, factors in parts_of:
+            own = [None if alike[k] is not None else layer_states(lines, steady[p], p, bin_db, factors[k])
+                   for k, (lines, steady) in enumerate(layers)]
+            wholes = []
+            for state in range(WEATHER_STATES):
+                states = [(own[k] if own[k] is not None else alike[k])[state] for k in range(len(layers))]
+                floor = 0.0
+                for _, f in states:
+                    if f is not None:
+                        floor += f
+                total = Distribution(bin_db)
+                total.silent = 1.0
+                total = total.over(floor)
+                for part, f in states:
+                    if f is None:
+                        total = total.with_distribution(part)
+                wholes.append(total)
+            parts.append((slots / (hours * WEATHER_STATES), own, wholes))
+        mixtures = []
+        for k in range(len(layers)):
             mixture = Distribution(bin_db)
-            for part, _ in states:
-                mixture.add_scaled(part, 1.0 / WEATHER_STATES)
-            each[k][p] = mixture
+            if alike[k] is not None:
+                for part, _ in alike[k]:
+                    mixture.add_scaled(part, 1.0 / WEATHER_STATES)
+            mixtures.append(mixture)
         mixed = Distribution(bin_db)
-        weight = 1.0 / WEATHER_STATES
-        for state in range(WEATHER_STATES):
-            parts = [states[state] for states in per_layer]
-            floor = 0.0
-            for _, f in parts:
-                if f is not None:
-                    floor += f
-            total = Distribution(bin_db)
-            total.silent = 1.0
-            total = total.over(floor)
-            for part, f in parts:
-                if f is None:
-                    total = total.with_distribution(part)
-            mixed.add_scaled(total, weight)
+        for weight, own, wholes in parts:
+            for k in range(len(layers)):
+                if own[k] is not None:
+                    for part, _ in own[k]:
+                        mixtures[k].add_scaled(part, weight)
+            for part in wholes:
+                mixed.add_scaled(part, weight)
+        for k in range(len(layers)):
+            each[k][p] = mixtures[k]
         whole.append(mixed)
     return each, whole

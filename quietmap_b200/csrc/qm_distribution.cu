@@ -161,101 +161,161 @@ qm_status qm_distribution_line_values(double lambda, double duty, double *values
     return QM_OK;
 }
 
-qm_status qm_distribution_layers(double bin_db, const qm_period_line *lines, size_t n_lines, const double *steady,
-                                 size_t n_layers, double *layer_bins, double *layer_silent, double *place_bins,
-                                 double *place_silent) {
+qm_status qm_distribution_layers_grouped(double bin_db, const qm_period_line *lines, size_t n_lines,
+                                         const double *steady, size_t n_layers, uint32_t hours,
+                                         const uint32_t *group_hours, size_t n_groups, const double *factors,
+                                         const uint8_t *profiled, double *layer_bins, double *layer_silent,
+                                         double *place_bins, double *place_silent) {
+    const char *who = "qm_distribution_layers";
     int n_bins = 0;
-    const qm_status status = grid("qm_distribution_layers", bin_db, n_bins);
+    const qm_status status = grid(who, bin_db, n_bins);
     if (status != QM_OK) return status;
     if ((n_lines > 0 && lines == nullptr) || (n_layers > 0 && (steady == nullptr || layer_bins == nullptr ||
                                                                layer_silent == nullptr)) ||
         place_bins == nullptr || place_silent == nullptr)
-        return qm::set_error(QM_ERR_ARGUMENT, "qm_distribution_layers: null lines, steady or output");
-    if (n_lines > (size_t)INT32_MAX) return qm::set_error(QM_ERR_ARGUMENT, "qm_distribution_layers: too many lines");
+        return qm::set_error(QM_ERR_ARGUMENT, std::string(who) + ": null lines, steady or output");
+    if (n_lines > (size_t)INT32_MAX) return qm::set_error(QM_ERR_ARGUMENT, std::string(who) + ": too many lines");
+    if (n_groups == 0 || group_hours == nullptr || (n_lines > 0 && (factors == nullptr || profiled == nullptr)))
+        return qm::set_error(QM_ERR_ARGUMENT, std::string(who) + ": no groups of hours, or null factors");
+    uint64_t grouped = 0;
+    for (size_t g = 0; g < n_groups; ++g) grouped += group_hours[g];
+    if (hours == 0 || grouped > hours)
+        return qm::set_error(QM_ERR_ARGUMENT, std::string(who) + ": the groups hold " + std::to_string(grouped) +
+                                                  " hours of a period of " + std::to_string(hours));
     for (size_t l = 0; l < n_layers; ++l)
         if (!(steady[l] >= 0.0) || !std::isfinite(steady[l]))
-            return qm::set_error(QM_ERR_ARGUMENT, "qm_distribution_layers: steady energy of layer " + std::to_string(l) +
+            return qm::set_error(QM_ERR_ARGUMENT, std::string(who) + ": steady energy of layer " + std::to_string(l) +
                                                       " is negative or not finite");
-    // Each line's shape in the period (lines.rs:172-195), its values in the order LineValues
-    // keeps them.
-    std::vector<OwnedValues> owned(n_lines);
-    std::vector<std::vector<qm::dist::PeriodLine>> layers(n_layers);
-    const double min_positive = 2.2250738585072014e-308;
+    std::vector<char> alike(n_layers, 1);
     for (size_t k = 0; k < n_lines; ++k) {
         const qm_period_line &line = lines[k];
-        const std::string which = "qm_distribution_layers: line " + std::to_string(k);
+        const std::string which = std::string(who) + ": line " + std::to_string(k);
         if (line.layer >= n_layers) return qm::set_error(QM_ERR_ARGUMENT, which + " names layer " + std::to_string(line.layer));
         if (std::isnan(line.energy) || std::isnan(line.lambda))
             return qm::set_error(QM_ERR_ARGUMENT, which + " has a NaN energy or lambda");
+        if (!std::isnan(line.duty) && line.duty > 1.0)
+            return qm::set_error(QM_ERR_ARGUMENT, which + " has a duty above 1");
         for (int st = 0; st < QM_WEATHER_STATES; ++st)
             if (!(line.means[st] >= 0.0) || !std::isfinite(line.means[st]))
                 return qm::set_error(QM_ERR_ARGUMENT, which + " has a negative or non-finite mean");
-        qm::dist::PeriodLine entry{line.energy, line.means, qm::dist::SHAPE_HOLDS, qm::dist::Values{nullptr, nullptr, 0},
-                                   0.0};
-        std::vector<double> pairs;
-        if (!std::isnan(line.passing)) {
-            if (line.passing >= min_positive && line.passing < qm::dist::PASSES_HOLD_MEAN) {
-                entry.kind = qm::dist::SHAPE_MOVES;
-                pairs = pass_pairs(line.passing);
-            }
-        } else if (!std::isnan(line.duty)) {
-            if (line.duty > 1.0) return qm::set_error(QM_ERR_ARGUMENT, which + " has a duty above 1");
-            if (line.duty > 0.0) {
-                entry.kind = qm::dist::SHAPE_MOVES;
-                pairs = {0.0, 1.0 - line.duty, 1.0 / line.duty, line.duty};
-            } else {
-                entry.kind = qm::dist::SHAPE_SILENT;
-            }
-        } else if (!(line.lambda * 1.0 >= qm::dist::HOLDS_MEAN_LAMBDA)) {
-            entry.kind = qm::dist::SHAPE_SPARSE;
-            pairs = kurze_pairs(line.lambda);
-            entry.exceeded = qm::line_relative_intensity(qm::line_level_table_shared().data(), line.lambda,
-                                                         1.0 - qm::dist::HELD_EXCEEDED);
-        }
-        if (!pairs.empty()) {
-            owned[k] = sorted_values(pairs.data(), pairs.size() / 2);
-            entry.values = owned[k].view();
-        }
-        layers[line.layer].push_back(entry);
+        for (size_t g = 0; g < n_groups; ++g)
+            if (profiled[k] && (!(factors[g * n_lines + k] >= 0.0) || !std::isfinite(factors[g * n_lines + k])))
+                return qm::set_error(QM_ERR_ARGUMENT, which + " has a negative or non-finite flow factor");
+        if (profiled[k]) alike[line.layer] = 0;
     }
+    const double min_positive = 2.2250738585072014e-308;
+    const float *table = qm::line_level_table_shared().data();
+    // A layer's lines with their shapes at the flow factors of group g (lines.rs:172-195); g < 0:
+    // every line at its period's mean flow. `owned` keeps the values the entries point at.
+    auto shape_layer = [&](size_t layer, long g, std::vector<OwnedValues> &owned, std::vector<qm::dist::PeriodLine> &out) {
+        out.clear();
+        owned.clear();
+        owned.reserve(n_lines);
+        for (size_t k = 0; k < n_lines; ++k) {
+            const qm_period_line &line = lines[k];
+            if (line.layer != layer) continue;
+            const double factor = (g >= 0 && profiled[k]) ? factors[(size_t)g * n_lines + k] : 1.0;
+            qm::dist::PeriodLine entry{line.energy, line.means, factor, qm::dist::SHAPE_HOLDS,
+                                       qm::dist::Values{nullptr, nullptr, 0}, 0.0};
+            std::vector<double> pairs;
+            const double lambda = line.lambda * factor;
+            if (!std::isnan(line.passing)) {
+                if (line.passing >= min_positive && line.passing < qm::dist::PASSES_HOLD_MEAN) {
+                    entry.kind = qm::dist::SHAPE_MOVES;
+                    pairs = pass_pairs(line.passing);
+                }
+            } else if (!std::isnan(line.duty)) {
+                if (line.duty > 0.0) {
+                    entry.kind = qm::dist::SHAPE_MOVES;
+                    pairs = {0.0, 1.0 - line.duty, 1.0 / line.duty, line.duty};
+                } else {
+                    entry.kind = qm::dist::SHAPE_SILENT;
+                }
+            } else if (!(lambda >= qm::dist::HOLDS_MEAN_LAMBDA)) {
+                entry.kind = qm::dist::SHAPE_SPARSE;
+                pairs = kurze_pairs(lambda);
+                entry.exceeded = qm::line_relative_intensity(table, lambda, 1.0 - qm::dist::HELD_EXCEEDED);
+            }
+            if (!pairs.empty()) {
+                owned.push_back(sorted_values(pairs.data(), pairs.size() / 2));
+                entry.values = owned.back().view();
+            }
+            out.push_back(entry);
+        }
+    };
     const size_t bins2 = 2 * (size_t)n_bins;
-    std::vector<double> a(bins2), b(bins2), c(bins2), d(bins2), states_silent(n_layers);
-    std::vector<double> state_bins(n_layers * bins2), floors(n_layers), pairs(2 * ((size_t)n_bins + 1)),
+    const int S = qm::dist::WEATHER_STATES;
+    // Per layer and state: its distribution, silence, floor and whether it holds.
+    std::vector<double> state_bins(n_layers * S * bins2), state_silent(n_layers * S), floors(n_layers * S);
+    std::vector<char> holds(n_layers * S);
+    std::vector<double> a(bins2), b(bins2), c(bins2), d(bins2), pairs(2 * ((size_t)n_bins + 1)),
         sums(2 * ((size_t)n_bins + 2));
-    std::vector<char> holds(n_layers);
+    std::vector<OwnedValues> owned;
+    std::vector<qm::dist::PeriodLine> entries;
+    auto layer_states = [&](size_t l, long g) {
+        shape_layer(l, g, owned, entries);
+        for (int state = 0; state < S; ++state) {
+            double *out = nullptr, silent = 0.0;
+            const size_t at = l * S + state;
+            holds[at] = qm::dist::layer_state(bin_db, n_bins, entries.data(), (int)entries.size(), state, steady[l],
+                                              a.data(), b.data(), &out, &silent, &floors[at]);
+            std::copy(out, out + bins2, state_bins.begin() + at * bins2);
+            state_silent[at] = silent;
+        }
+    };
     for (size_t b2 = 0; b2 < n_layers * bins2; ++b2) layer_bins[b2] = 0.0;
     for (size_t l = 0; l < n_layers; ++l) layer_silent[l] = 0.0;
     for (size_t b2 = 0; b2 < bins2; ++b2) place_bins[b2] = 0.0;
     *place_silent = 0.0;
-    const double weight = 1.0 / (double)qm::dist::WEATHER_STATES;
-    for (int state = 0; state < qm::dist::WEATHER_STATES; ++state) {
+    // The layers no profiled line moves, once at their mean flow, a tenth of the time a state.
+    for (size_t l = 0; l < n_layers; ++l) {
+        if (!alike[l]) continue;
+        layer_states(l, -1);
+        for (int state = 0; state < S; ++state)
+            qm::dist::add_scaled(layer_bins + l * bins2, layer_silent + l, state_bins.data() + (l * S + state) * bins2,
+                                 state_silent[l * S + state], n_bins, 1.0 / (double)S);
+    }
+    for (size_t g = 0; g < n_groups; ++g) {
+        const double weight = (double)group_hours[g] / (double)((uint64_t)hours * S);
         for (size_t l = 0; l < n_layers; ++l) {
-            double *out = nullptr, silent = 0.0;
-            holds[l] = qm::dist::layer_state(bin_db, n_bins, layers[l].data(), (int)layers[l].size(), state, steady[l],
-                                             a.data(), b.data(), &out, &silent, &floors[l]);
-            std::copy(out, out + bins2, state_bins.begin() + l * bins2);
-            states_silent[l] = silent;
-            qm::dist::add_scaled(layer_bins + l * bins2, layer_silent + l, out, silent, n_bins, weight);
+            if (alike[l]) continue;
+            layer_states(l, (long)g);
+            for (int state = 0; state < S; ++state)
+                qm::dist::add_scaled(layer_bins + l * bins2, layer_silent + l,
+                                     state_bins.data() + (l * S + state) * bins2, state_silent[l * S + state], n_bins,
+                                     weight);
         }
-        // The place: the floors of the layers that hold, then each moving layer added.
-        double floor = 0.0;
-        for (size_t l = 0; l < n_layers; ++l)
-            if (holds[l]) floor += floors[l];
-        std::fill(c.begin(), c.end(), 0.0);
-        double silent;
-        qm::dist::over(bin_db, n_bins, c.data(), 1.0, floor, d.data(), &silent);
-        double *current = d.data(), *spare = c.data();
-        for (size_t l = 0; l < n_layers; ++l) {
-            if (holds[l]) continue;
-            double next_silent;
-            qm::dist::with_distribution(bin_db, n_bins, current, silent, state_bins.data() + l * bins2, states_silent[l],
-                                        pairs.data(), sums.data(), spare, &next_silent);
-            std::swap(current, spare);
-            silent = next_silent;
+        // The place in each state: the floors of the layers that hold, then each moving layer.
+        for (int state = 0; state < S; ++state) {
+            double floor = 0.0;
+            for (size_t l = 0; l < n_layers; ++l)
+                if (holds[l * S + state]) floor += floors[l * S + state];
+            std::fill(c.begin(), c.end(), 0.0);
+            double silent;
+            qm::dist::over(bin_db, n_bins, c.data(), 1.0, floor, d.data(), &silent);
+            double *current = d.data(), *spare = c.data();
+            for (size_t l = 0; l < n_layers; ++l) {
+                if (holds[l * S + state]) continue;
+                double next_silent;
+                qm::dist::with_distribution(bin_db, n_bins, current, silent, state_bins.data() + (l * S + state) * bins2,
+                                            state_silent[l * S + state], pairs.data(), sums.data(), spare, &next_silent);
+                std::swap(current, spare);
+                silent = next_silent;
+            }
+            qm::dist::add_scaled(place_bins, place_silent, current, silent, n_bins, weight);
         }
-        qm::dist::add_scaled(place_bins, place_silent, current, silent, n_bins, weight);
     }
     return QM_OK;
+}
+
+qm_status qm_distribution_layers(double bin_db, const qm_period_line *lines, size_t n_lines, const double *steady,
+                                 size_t n_layers, double *layer_bins, double *layer_silent, double *place_bins,
+                                 double *place_silent) {
+    const uint32_t one = 1;
+    const std::vector<uint8_t> unprofiled(n_lines, 0);
+    const std::vector<double> unit(n_lines, 1.0);
+    return qm_distribution_layers_grouped(bin_db, lines, n_lines, steady, n_layers, 1, &one, 1, unit.data(),
+                                          unprofiled.data(), layer_bins, layer_silent, place_bins, place_silent);
 }
 
 qm_status qm_distribution_pass_values(double mean, double *values, size_t cap, size_t *n_values) {

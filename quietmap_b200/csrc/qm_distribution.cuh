@@ -251,6 +251,7 @@ enum ShapeKind : int { SHAPE_HOLDS = 0, SHAPE_SILENT = 1, SHAPE_MOVES = 2, SHAPE
 struct PeriodLine {
     double energy;         // the period's mean energy: a line at or under 0 is silent
     const double *means;   // [WEATHER_STATES]
+    double factor;         // its flow in the hours against the period's mean (1 without a profile)
     int kind;              // ShapeKind
     Values values;         // SHAPE_MOVES, SHAPE_SPARSE: intensities relative to the mean
     double exceeded;       // SHAPE_SPARSE: the relative intensity exceeded a thousandth of the time
@@ -262,14 +263,14 @@ __host__ __device__ inline double moment_floor(const PeriodLine *lines, int n, i
                                                double &steady_energy) {
     double floor = steady, held = 0.0;
     for (int k = 0; k < n; ++k) {
-        const double mean = lines[k].means[state] * 1.0;
+        const double mean = lines[k].means[state] * lines[k].factor;
         if (lines[k].energy <= 0.0 || mean <= 0.0) continue;
         if (lines[k].kind == SHAPE_HOLDS) floor += mean;
         if (lines[k].kind == SHAPE_SPARSE) held += mean;
     }
     steady_energy = floor + held;
     for (int k = 0; k < n; ++k) {
-        const double mean = lines[k].means[state] * 1.0;
+        const double mean = lines[k].means[state] * lines[k].factor;
         if (lines[k].energy <= 0.0 || mean <= 0.0 || lines[k].kind != SHAPE_SPARSE) continue;
         if (mean * lines[k].exceeded < HELD_SHARE * steady_energy) floor += mean;
     }
@@ -283,7 +284,7 @@ template <class Visit>
 __host__ __device__ void moving_lines(const PeriodLine *lines, int n, int state, double steady_energy, Visit &visit) {
     for (int pass = 0; pass < 2; ++pass)
         for (int k = 0; k < n; ++k) {
-            const double mean = lines[k].means[state] * 1.0;
+            const double mean = lines[k].means[state] * lines[k].factor;
             if (lines[k].energy <= 0.0 || mean <= 0.0) continue;
             if (pass == 0 && lines[k].kind == SHAPE_MOVES) visit(k, mean);
             if (pass == 1 && lines[k].kind == SHAPE_SPARSE && !(mean * lines[k].exceeded < HELD_SHARE * steady_energy))

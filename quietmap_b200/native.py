@@ -160,6 +160,9 @@ def lib():
         L.qm_distribution_pass_values.restype = C.c_int
         L.qm_distribution_layers.argtypes = [C.c_double, C.c_void_p, C.c_size_t, _D, C.c_size_t, _D, _D, _D, _D]
         L.qm_distribution_layers.restype = C.c_int
+        L.qm_distribution_layers_grouped.argtypes = [C.c_double, C.c_void_p, C.c_size_t, _D, C.c_size_t, C.c_uint32,
+                                                     _U32, C.c_size_t, _D, _U8, _D, _D, _D, _D]
+        L.qm_distribution_layers_grouped.restype = C.c_int
         if L.qm_abi_version() != abi.ABI_VERSION:
             raise QmError(abi.QM_ERR_UNSUPPORTED, "library ABI version mismatch")
         _lib = L
@@ -469,6 +472,27 @@ def distribution_layers(bin_db, lines, steady):
                                         abi.ptr(st, C.c_double) if len(st) else None, len(st),
                                         abi.ptr(layer_bins, C.c_double), abi.ptr(layer_silent, C.c_double),
                                         abi.ptr(place_bins, C.c_double), C.byref(place_silent)))
+    return layer_bins, layer_silent, place_bins, place_silent.value
+
+
+def distribution_layers_grouped(bin_db, lines, steady, hours, group_hours, factors, profiled):
+    """One period's layers over groups of hours (qm_distribution_layers_grouped): `factors`
+    [n_groups][n_lines] each profiled line's flow in each group against the period's mean."""
+    rows = np.ascontiguousarray(lines, dtype=abi.PERIOD_LINE_DTYPE)
+    st = np.ascontiguousarray(steady, dtype=np.float64)
+    gh = np.ascontiguousarray(group_hours, dtype=np.uint32)
+    fa = np.ascontiguousarray(np.asarray(factors, dtype=np.float64).reshape(len(gh), len(rows)))
+    pr = np.ascontiguousarray(profiled, dtype=np.uint8)
+    n_bins = distribution_bins(bin_db)
+    layer_bins = np.zeros((len(st), n_bins, 2))
+    layer_silent = np.zeros(len(st))
+    place_bins = np.zeros((n_bins, 2))
+    place_silent = C.c_double()
+    _check(lib().qm_distribution_layers_grouped(
+        float(bin_db), rows.ctypes.data if len(rows) else None, len(rows), abi.ptr(st, C.c_double) if len(st) else None,
+        len(st), int(hours), abi.ptr(gh, C.c_uint32), len(gh), abi.ptr(fa, C.c_double) if fa.size else None,
+        abi.ptr(pr, C.c_uint8) if len(pr) else None, abi.ptr(layer_bins, C.c_double), abi.ptr(layer_silent, C.c_double),
+        abi.ptr(place_bins, C.c_double), C.byref(place_silent)))
     return layer_bins, layer_silent, place_bins, place_silent.value
 
 

@@ -231,3 +231,43 @@ def test_layers_errors():
     layer_bins, silent, place, place_silent = native.distribution_layers(0.5, rows, [0.0])
     assert silent[0] == 0.0 and np.count_nonzero(layer_bins[0][:, 0]) == 1
     assert abs(native.distribution_exceeded_db(0.5, place, 0.99)) < 1e-9 and place_silent == 0.0
+
+
+@pytest.mark.parametrize("bin_db", [0.5, 2.0])
+def test_profiled_roads_over_groups_of_hours_match_the_oracle(bin_db):
+    """Roads that follow an hourly profile, over groups of a period's hours with their own flow
+    factors (the map's four, one and three groups of 16, 4 and 8 hours), beside layers that follow
+    none: every layer's and the place's distribution equal the oracle's to the bit. The dense
+    roads' lambda drops under 10 in quiet groups, so their shape changes from group to group."""
+    rng = np.random.default_rng(8)
+    layers = _place(11, sparse=False)
+    roads_index = 0
+    road_lines = layers[roads_index][0]
+    profiled_roads = [True, False]
+    hours_of = [16, 4, 8]
+    groups_of = [[4, 4, 4, 4], [4], [3, 3, 2]]
+    groups = []
+    factors_of = []
+    for p in range(3):
+        per_group = []
+        factor_rows = []
+        for slots in groups_of[p]:
+            road_factors = [float(rng.uniform(0.2, 2.0)) if prof else 1.0 for prof in profiled_roads]
+            per_layer = [road_factors if k == roads_index else None for k in range(len(layers))]
+            per_group.append((slots, per_layer))
+            factor_rows.append(road_factors + [1.0] * (sum(len(lines) for lines, _ in layers) - len(road_lines)))
+        groups.append((hours_of[p], per_group))
+        factors_of.append(factor_rows)
+    each, whole = dist.layered_distributions(layers, bin_db, groups)
+    profiled = profiled_roads + [False] * (sum(len(lines) for lines, _ in layers) - len(road_lines))
+    for p in range(3):
+        got_each, got_silent, got_whole, got_whole_silent = native.distribution_layers_grouped(
+            bin_db, _period_rows(layers, p), [steady[p] for _, steady in layers], hours_of[p], groups_of[p],
+            factors_of[p], profiled)
+        for k in range(len(layers)):
+            assert np.array_equal(got_each[k], _bins(each[k][p])) and got_silent[k] == each[k][p].silent, (p, k)
+        assert np.array_equal(got_whole, _bins(whole[p])) and got_whole_silent == whole[p].silent, p
+    with pytest.raises(native.QmError) as err:
+        native.distribution_layers_grouped(bin_db, _period_rows(layers, 0), [s[0] for _, s in layers], 15,
+                                           groups_of[0], factors_of[0], profiled)
+    assert err.value.status == abi.QM_ERR_ARGUMENT and "16 hours" in str(err.value)
