@@ -80,6 +80,12 @@ qm_status qm_distribution_layers(double bin_db, const qm_period_line *lines, siz
                                  size_t n_layers, double *layer_bins, double *layer_silent, double *place_bins,
                                  double *place_silent);
 
+/* merge_close_states for one period's lines, in place (popup/src/percentiles/weather.rs:132-176):
+ * each run of consecutive weather states in which every line's mean is finite and within `spread`
+ * (largest over smallest; the map uses 1.2) gives each line its mean over the run in all of the
+ * run's states. The energy stays; equal states then cost one state. */
+qm_status qm_distribution_merge_states(qm_period_line *lines, size_t n_lines, double spread);
+
 /* The same over a period's groups of hours (popup/src/percentiles.rs:88-160 with hour_groups,
  * percentiles/traffic.rs:251-279): a period of `hours` hours whose groups hold group_hours[g]
  * hours each; profiled[k] marks a line that follows an hourly profile and factors[g][n_lines]

@@ -340,3 +340,34 @@ def layered_distributions(layers, bin_db, groups=None):
             each[k][p] = mixtures[k]
         whole.append(mixed)
     return each, whole
+
+
+def merge_close_states(layers, spread):
+    """The weather states merged where their difference cannot show (percentiles/weather.rs:
+    132-176): per period, each run of consecutive states in which every line's mean is finite and
+    within `spread` (largest over smallest) gives each line its mean over the run in all of the
+    run's states. Changes the lines' means in place."""
+    def within(means):
+        low, high = math.inf, 0.0
+        for mean in means:
+            if not math.isfinite(mean):
+                return False
+            low, high = min(low, mean), max(high, mean)
+        return high <= spread * low
+
+    lines = [line for layer_lines, _ in layers for line in layer_lines]
+    for period in range(3):
+        start = 0
+        while start < WEATHER_STATES:
+            end = start + 1
+            while end < WEATHER_STATES and all(within(line.means[period][start:end + 1]) for line in lines):
+                end += 1
+            if end - start > 1:
+                for line in lines:
+                    run = line.means[period][start:end]
+                    if any(mean != run[0] for mean in run):
+                        total = 0.0
+                        for mean in run:
+                            total += mean
+                        line.means[period][start:end] = [total / len(run)] * len(run)
+            start = end

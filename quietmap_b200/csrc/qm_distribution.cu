@@ -318,6 +318,17 @@ qm_status qm_distribution_layers(double bin_db, const qm_period_line *lines, siz
                                           unprofiled.data(), layer_bins, layer_silent, place_bins, place_silent);
 }
 
+qm_status qm_distribution_merge_states(qm_period_line *lines, size_t n_lines, double spread) {
+    if (n_lines > 0 && lines == nullptr) return qm::set_error(QM_ERR_ARGUMENT, "qm_distribution_merge_states: null lines");
+    if (std::isnan(spread)) return qm::set_error(QM_ERR_ARGUMENT, "qm_distribution_merge_states: spread is NaN");
+    if (n_lines > (size_t)INT32_MAX) return qm::set_error(QM_ERR_ARGUMENT, "qm_distribution_merge_states: too many lines");
+    std::vector<double> means(n_lines * QM_WEATHER_STATES);
+    for (size_t k = 0; k < n_lines; ++k) std::copy(lines[k].means, lines[k].means + QM_WEATHER_STATES, &means[k * QM_WEATHER_STATES]);
+    qm::dist::merge_close_states(means.data(), (int)n_lines, spread);
+    for (size_t k = 0; k < n_lines; ++k) std::copy(&means[k * QM_WEATHER_STATES], &means[k * QM_WEATHER_STATES] + QM_WEATHER_STATES, lines[k].means);
+    return QM_OK;
+}
+
 qm_status qm_distribution_pass_values(double mean, double *values, size_t cap, size_t *n_values) {
     if (n_values == nullptr || (cap > 0 && values == nullptr))
         return qm::set_error(QM_ERR_ARGUMENT, "qm_distribution_pass_values: null values or n_values");

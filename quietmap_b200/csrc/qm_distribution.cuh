@@ -320,5 +320,43 @@ __host__ __device__ inline bool layer_state(double bin_db, int n_bins, const Per
     return !moved;
 }
 
+// The weather states merged where their difference cannot show (popup/src/percentiles/
+// weather.rs:132-176) for one period's lines, means[n][WEATHER_STATES] in place: each run of
+// consecutive states in which every line's mean is finite and within `spread` (largest over
+// smallest) gives each line its mean over the run in all of the run's states.
+__host__ __device__ inline void merge_close_states(double *means, int n, double spread) {
+    auto within = [&](int start, int end) {  // states start..=end, every line
+        for (int k = 0; k < n; ++k) {
+            double low = INFINITY, high = 0.0;
+            for (int st = start; st <= end; ++st) {
+                const double mean = means[k * WEATHER_STATES + st];
+                if (!isfinite(mean)) return false;
+                low = fmin(low, mean);
+                high = fmax(high, mean);
+            }
+            if (!(high <= spread * low)) return false;
+        }
+        return true;
+    };
+    int start = 0;
+    while (start < WEATHER_STATES) {
+        int end = start + 1;
+        while (end < WEATHER_STATES && within(start, end)) ++end;
+        if (end - start > 1) {
+            for (int k = 0; k < n; ++k) {
+                double *run = means + k * WEATHER_STATES + start;
+                bool differ = false;
+                for (int st = 0; st < end - start; ++st) differ = differ || run[st] != run[0];
+                if (!differ) continue;
+                double total = 0.0;
+                for (int st = 0; st < end - start; ++st) total += run[st];
+                const double mean = total / (double)(end - start);
+                for (int st = 0; st < end - start; ++st) run[st] = mean;
+            }
+        }
+        start = end;
+    }
+}
+
 }  // namespace dist
 }  // namespace qm

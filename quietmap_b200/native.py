@@ -160,6 +160,8 @@ def lib():
         L.qm_distribution_pass_values.restype = C.c_int
         L.qm_distribution_layers.argtypes = [C.c_double, C.c_void_p, C.c_size_t, _D, C.c_size_t, _D, _D, _D, _D]
         L.qm_distribution_layers.restype = C.c_int
+        L.qm_distribution_merge_states.argtypes = [C.c_void_p, C.c_size_t, C.c_double]
+        L.qm_distribution_merge_states.restype = C.c_int
         L.qm_distribution_layers_grouped.argtypes = [C.c_double, C.c_void_p, C.c_size_t, _D, C.c_size_t, C.c_uint32,
                                                      _U32, C.c_size_t, _D, _U8, _D, _D, _D, _D]
         L.qm_distribution_layers_grouped.restype = C.c_int
@@ -473,6 +475,14 @@ def distribution_layers(bin_db, lines, steady):
                                         abi.ptr(layer_bins, C.c_double), abi.ptr(layer_silent, C.c_double),
                                         abi.ptr(place_bins, C.c_double), C.byref(place_silent)))
     return layer_bins, layer_silent, place_bins, place_silent.value
+
+
+def distribution_merge_states(lines, spread):
+    """A copy of one period's PERIOD_LINE_DTYPE lines with close weather states merged
+    (qm_distribution_merge_states)."""
+    rows = np.array(lines, dtype=abi.PERIOD_LINE_DTYPE, copy=True, order="C")
+    _check(lib().qm_distribution_merge_states(rows.ctypes.data if len(rows) else None, len(rows), float(spread)))
+    return rows
 
 
 def distribution_layers_grouped(bin_db, lines, steady, hours, group_hours, factors, profiled):

@@ -108,3 +108,56 @@ def test_layers_keep_their_energy_in_every_weather_state():
         assert abs(mean(whole[p]) - sum(expected)) <= 1e-9 * sum(expected), p
         assert abs(sum(s for _, s in whole[p].intensities()) + whole[p].silent - 1.0) < 1e-12
     assert moved > 50 and held > 50
+
+
+def _line_of(means):
+    states = dist.WEATHER_STATES
+    return dist.Line([sum(means) / states] * 3, [list(means) for _ in range(3)], [1e6] * 3)
+
+
+def test_close_weather_states_merge_and_keep_their_energy():
+    """What the reference's test states (popup/src/percentiles_tests.rs:464-504): a line apart by
+    more than the spread splits the states where it jumps; the other's first three states take
+    their mean, the rest keep theirs; every line keeps its energy; means falling by more than the
+    spread from state to state merge nowhere."""
+    near = _line_of([1.10, 1.05, 1.0, 1.0, 1.0, 1.0, 1.0, 1.0, 1.0, 1.0])
+    far = _line_of([4.0, 4.0, 4.0, 1.0, 1.0, 1.0, 1.0, 1.0, 1.0, 1.0])
+    before_near, before_far = list(near.means[0]), list(far.means[0])
+    layers = [([near], [0.0] * 3), ([far], [0.0] * 3)]
+    dist.merge_close_states(layers, 1.2)
+    assert far.means[0] == before_far
+    assert near.means[0][0] == near.means[0][2]
+    assert abs(near.means[0][0] - (1.10 + 1.05 + 1.0) / 3.0) < 1e-12
+    assert near.means[0][3:] == before_near[3:]
+    for line in (near, far):
+        assert abs(sum(line.means[0]) / dist.WEATHER_STATES - line.energy[0]) < 1e-12
+    apart = _line_of([2.0, 1.5, 1.0, 0.7, 0.5, 0.35, 0.25, 0.18, 0.12, 0.09])
+    before = [list(m) for m in apart.means]
+    dist.merge_close_states([([apart], [0.0] * 3)], 1.2)
+    assert apart.means == before
+
+
+def test_the_library_merges_states_as_the_oracle_does():
+    import numpy as np
+
+    from quietmap_b200 import abi, native
+
+    rng = np.random.default_rng(12)
+    for trial in range(200):
+        n = int(rng.integers(1, 6))
+        lines = []
+        for _ in range(n):
+            base = 10.0 ** rng.uniform(-2.0, 6.0)
+            steps = rng.choice([1.0, 1.0, 1.05, 1.15, 1.3, 3.0], size=dist.WEATHER_STATES)
+            means = list(base * np.cumprod(steps) / steps[0])
+            if trial % 17 == 0:
+                means[int(rng.integers(0, dist.WEATHER_STATES))] = math.inf
+            lines.append(_line_of(means))
+        rows = np.zeros(n, dtype=abi.PERIOD_LINE_DTYPE)
+        for k, line in enumerate(lines):
+            rows[k]["means"] = line.means[0]
+        spread = float(rng.choice([1.05, 1.2, 2.0]))
+        merged = native.distribution_merge_states(rows, spread)
+        dist.merge_close_states([(lines, [0.0] * 3)], spread)
+        for k, line in enumerate(lines):
+            assert np.array_equal(merged[k]["means"], np.array(line.means[0])), (trial, k)
