@@ -86,6 +86,21 @@ qm_status qm_distribution_layers(double bin_db, const qm_period_line *lines, siz
  * run's states. The energy stays; equal states then cost one state. */
 qm_status qm_distribution_merge_states(qm_period_line *lines, size_t n_lines, double spread);
 
+/* Loudness from the distributions (popup/src/loudness.rs:74-130, 236-269). A period's curve is
+ * the loudness (sone) of its received spectrum set to each whole A-weighted decibel from -30 to
+ * 160 dB: curve[191], linear between; `qm_loudness_curve_shape` gives the spectrum at an
+ * A-weighted 0 dB (thirds[28] energies from 25 Hz to 12.5 kHz; -inf where a band is silent;
+ * *has_shape 0 and no shape for a spectrum without A-weighted energy, whose curve is 0), and
+ * `qm_zwicker` of that shape plus each whole decibel fills the curve. */
+#define QM_LOUDNESS_CURVE_POINTS 191
+qm_status qm_loudness_curve_shape(const double *thirds, double *shape_db, int *has_shape);
+
+/* Each period's mean loudness over its distribution (bins[3][n_bins][2]) on its curve
+ * (curves[3][191]) and Nden: the periods' means with the evening's 5 dB and the night's 10 dB
+ * added to their levels, weighed by their 12, 4 and 8 hours over 24. */
+qm_status qm_distribution_loudness(double bin_db, const double *bins, const double *curves, double *mean_sone,
+                                   double *nden_sone);
+
 /* The same over a period's groups of hours (popup/src/percentiles.rs:88-160 with hour_groups,
  * percentiles/traffic.rs:251-279): a period of `hours` hours whose groups hold group_hours[g]
  * hours each; profiled[k] marks a line that follows an hourly profile and factors[g][n_lines]

@@ -371,3 +371,62 @@ def merge_close_states(layers, spread):
                             total += mean
                         line.means[period][start:end] = [total / len(run)] * len(run)
             start = end
+
+
+# ---------------------------------------------------------------------------------------------
+# Loudness from the distributions (popup/src/loudness.rs:68-130, 236-269).
+
+CURVE_LOW_DB, CURVE_HIGH_DB = -30.0, 160.0          # loudness.rs:68-69
+PERIOD_HOURS = (12.0, 4.0, 8.0)                     # physics/src/bands.rs:16
+PERIOD_PENALTY_DB = (0.0, 5.0, 10.0)                # physics/src/bands.rs:18
+# Third-octave A-weighting, 25 Hz to 12.5 kHz (IEC 61672-1; physics/src/loudness.rs:14-17).
+A_WEIGHTING_THIRDS_DB = (-44.7, -39.4, -34.6, -30.2, -26.2, -22.5, -19.1, -16.1, -13.4, -10.9, -8.6, -6.6,
+                         -4.8, -3.2, -1.9, -0.8, 0.0, 0.6, 1.0, 1.2, 1.3, 1.2, 1.0, 0.5, -0.1, -1.1, -2.5, -4.3)
+
+
+class Curve:
+    """One period's loudness by A-weighted level (loudness.rs:74-130): the received spectrum (28
+    third-octave energies) set to each whole decibel from -30 to 160 dB, Zwicker's loudness there,
+    linear between."""
+
+    def __init__(self, thirds):
+        a_weighted = 0.0
+        for value, weight in zip(thirds, A_WEIGHTING_THIRDS_DB):
+            a_weighted += value * energy(weight)
+        self.shape_db = None
+        if a_weighted > 0.0:
+            self.shape_db = [10.0 * math.log10(v / a_weighted) if v > 0.0 else -math.inf for v in thirds]
+        steps = int(CURVE_HIGH_DB - CURVE_LOW_DB)
+        if self.shape_db is None:
+            self.table = [0.0] * (steps + 1)
+        else:
+            self.table = list(oracle.zwicker_many([[db + (CURVE_LOW_DB + step) for db in self.shape_db]
+                                                   for step in range(steps + 1)]))
+
+    def at(self, level_db):
+        last = int(CURVE_HIGH_DB - CURVE_LOW_DB)
+        position = min(max(level_db - CURVE_LOW_DB, 0.0), float(last))
+        below = min(int(math.floor(position)), last - 1)
+        low, high = self.table[below], self.table[below + 1]
+        return low + (high - low) * (position - below)
+
+
+def loudness(distributions, curves):
+    """Each period's mean loudness and Nden (loudness.rs:236-269): per period the levels' shares
+    times the curve there (the evening's 5 dB and the night's 10 dB added for Nden), the periods
+    over their hours."""
+    def mean(penalty):
+        out = []
+        for p in range(3):
+            total = 0.0
+            for intensity, share in distributions[p].intensities():
+                total += share * curves[p].at(10.0 * math.log10(intensity) + penalty(p))
+            out.append(total)
+        return out
+
+    mean_sone = mean(lambda p: 0.0)
+    penalised = mean(lambda p: PERIOD_PENALTY_DB[p])
+    day = 0.0
+    for p in range(3):
+        day += PERIOD_HOURS[p] * penalised[p]
+    return mean_sone, day / 24.0

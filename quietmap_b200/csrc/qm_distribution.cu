@@ -16,6 +16,7 @@
 
 static_assert(QM_DISTRIBUTION_LINE_NODES == qm::dist::NODES, "the header's node count is the grid's");
 static_assert(QM_WEATHER_STATES == qm::dist::WEATHER_STATES, "the header's weather states are the mixture's");
+static_assert(QM_LOUDNESS_CURVE_POINTS == qm::dist::CURVE_STEPS + 1, "the header's curve is the table's");
 
 namespace {
 
@@ -326,6 +327,45 @@ qm_status qm_distribution_merge_states(qm_period_line *lines, size_t n_lines, do
     for (size_t k = 0; k < n_lines; ++k) std::copy(lines[k].means, lines[k].means + QM_WEATHER_STATES, &means[k * QM_WEATHER_STATES]);
     qm::dist::merge_close_states(means.data(), (int)n_lines, spread);
     for (size_t k = 0; k < n_lines; ++k) std::copy(&means[k * QM_WEATHER_STATES], &means[k * QM_WEATHER_STATES] + QM_WEATHER_STATES, lines[k].means);
+    return QM_OK;
+}
+
+qm_status qm_loudness_curve_shape(const double *thirds, double *shape_db, int *has_shape) {
+    if (thirds == nullptr || shape_db == nullptr || has_shape == nullptr)
+        return qm::set_error(QM_ERR_ARGUMENT, "qm_loudness_curve_shape: null argument");
+    // Third-octave A-weighting, 25 Hz to 12.5 kHz (IEC 61672-1; physics/src/loudness.rs:14-17).
+    static const double a_weighting_db[28] = {-44.7, -39.4, -34.6, -30.2, -26.2, -22.5, -19.1, -16.1, -13.4, -10.9,
+                                              -8.6,  -6.6,  -4.8,  -3.2,  -1.9,  -0.8,  0.0,   0.6,   1.0,   1.2,
+                                              1.3,   1.2,   1.0,   0.5,   -0.1,  -1.1,  -2.5,  -4.3};
+    double a_weighted = 0.0;
+    for (int k = 0; k < 28; ++k) {
+        if (!(thirds[k] >= 0.0) || !std::isfinite(thirds[k]))
+            return qm::set_error(QM_ERR_ARGUMENT, "qm_loudness_curve_shape: band " + std::to_string(k) +
+                                                      " is negative or not finite");
+        a_weighted += thirds[k] * qm::dist::energy(a_weighting_db[k]);
+    }
+    *has_shape = a_weighted > 0.0 ? 1 : 0;
+    for (int k = 0; k < 28; ++k)
+        shape_db[k] = (*has_shape && thirds[k] > 0.0) ? 10.0 * std::log10(thirds[k] / a_weighted) : -INFINITY;
+    return QM_OK;
+}
+
+qm_status qm_distribution_loudness(double bin_db, const double *bins, const double *curves, double *mean_sone,
+                                   double *nden_sone) {
+    int n_bins = 0;
+    const qm_status status = grid("qm_distribution_loudness", bin_db, n_bins);
+    if (status != QM_OK) return status;
+    if (bins == nullptr || curves == nullptr || mean_sone == nullptr || nden_sone == nullptr)
+        return qm::set_error(QM_ERR_ARGUMENT, "qm_distribution_loudness: null argument");
+    double day = 0.0;
+    for (int p = 0; p < 3; ++p) {
+        const double *period_bins = bins + (size_t)p * 2 * n_bins;
+        const double *curve = curves + (size_t)p * QM_LOUDNESS_CURVE_POINTS;
+        mean_sone[p] = qm::dist::mean_loudness(period_bins, n_bins, curve, 0.0);
+        day += qm::dist::PERIOD_HOURS[p] *
+               qm::dist::mean_loudness(period_bins, n_bins, curve, qm::dist::PERIOD_PENALTY_DB[p]);
+    }
+    *nden_sone = day / 24.0;
     return QM_OK;
 }
 

@@ -358,5 +358,33 @@ __host__ __device__ inline void merge_close_states(double *means, int n, double 
     }
 }
 
+// Loudness from the distributions (popup/src/loudness.rs:68-130, 236-269): a period's curve is
+// Zwicker's loudness of its received spectrum set to each whole A-weighted decibel from -30 to
+// 160 (191 values), linear between; its mean loudness the levels' shares times the curve there.
+constexpr double CURVE_LOW_DB = -30.0, CURVE_HIGH_DB = 160.0;  // loudness.rs:68-69
+constexpr int CURVE_STEPS = 190;
+constexpr double PERIOD_HOURS[3] = {12.0, 4.0, 8.0};            // physics/src/bands.rs:16
+constexpr double PERIOD_PENALTY_DB[3] = {0.0, 5.0, 10.0};       // physics/src/bands.rs:18
+
+__host__ __device__ inline double curve_at(const double *table, double level_db) {
+    const double position = fmin(fmax(level_db - CURVE_LOW_DB, 0.0), (double)CURVE_STEPS);
+    const double down = floor(position);
+    const int below = down < (double)(CURVE_STEPS - 1) ? (int)down : CURVE_STEPS - 1;
+    const double low = table[below], high = table[below + 1];
+    return low + (high - low) * (position - (double)below);
+}
+
+// The mean loudness over a distribution with `penalty_db` added to its levels (silence is 0).
+__host__ __device__ inline double mean_loudness(const double *bins, int n_bins, const double *table,
+                                                double penalty_db) {
+    double total = 0.0;
+    for (int b = 0; b < n_bins; ++b) {
+        const double share = bins[2 * b];
+        if (!(share > 0.0)) continue;
+        total += share * curve_at(table, 10.0 * log10(bins[2 * b + 1] / share) + penalty_db);
+    }
+    return total;
+}
+
 }  // namespace dist
 }  // namespace qm

@@ -160,6 +160,10 @@ def lib():
         L.qm_distribution_pass_values.restype = C.c_int
         L.qm_distribution_layers.argtypes = [C.c_double, C.c_void_p, C.c_size_t, _D, C.c_size_t, _D, _D, _D, _D]
         L.qm_distribution_layers.restype = C.c_int
+        L.qm_loudness_curve_shape.argtypes = [_D, _D, C.POINTER(C.c_int)]
+        L.qm_loudness_curve_shape.restype = C.c_int
+        L.qm_distribution_loudness.argtypes = [C.c_double, _D, _D, _D, _D]
+        L.qm_distribution_loudness.restype = C.c_int
         L.qm_distribution_merge_states.argtypes = [C.c_void_p, C.c_size_t, C.c_double]
         L.qm_distribution_merge_states.restype = C.c_int
         L.qm_distribution_layers_grouped.argtypes = [C.c_double, C.c_void_p, C.c_size_t, _D, C.c_size_t, C.c_uint32,
@@ -475,6 +479,27 @@ def distribution_layers(bin_db, lines, steady):
                                         abi.ptr(layer_bins, C.c_double), abi.ptr(layer_silent, C.c_double),
                                         abi.ptr(place_bins, C.c_double), C.byref(place_silent)))
     return layer_bins, layer_silent, place_bins, place_silent.value
+
+
+def loudness_curve_shape(thirds):
+    """A spectrum (28 third-octave energies) at an A-weighted 0 dB, or None without energy."""
+    t = np.ascontiguousarray(thirds, dtype=np.float64)
+    out = np.zeros(28)
+    has = C.c_int()
+    _check(lib().qm_loudness_curve_shape(abi.ptr(t, C.c_double), abi.ptr(out, C.c_double), C.byref(has)))
+    return out if has.value else None
+
+
+def distribution_loudness(bin_db, bins, curves):
+    """Each period's mean loudness and Nden (qm_distribution_loudness): bins [3][n_bins][2],
+    curves [3][191] sone at each whole decibel from -30 dB."""
+    b = np.ascontiguousarray(bins, dtype=np.float64)
+    c = np.ascontiguousarray(curves, dtype=np.float64)
+    mean = np.zeros(3)
+    nden = C.c_double()
+    _check(lib().qm_distribution_loudness(float(bin_db), abi.ptr(b, C.c_double), abi.ptr(c, C.c_double),
+                                          abi.ptr(mean, C.c_double), C.byref(nden)))
+    return mean, nden.value
 
 
 def distribution_merge_states(lines, spread):

@@ -271,3 +271,59 @@ def test_profiled_roads_over_groups_of_hours_match_the_oracle(bin_db):
         native.distribution_layers_grouped(bin_db, _period_rows(layers, 0), [s[0] for _, s in layers], 15,
                                            groups_of[0], factors_of[0], profiled)
     assert err.value.status == abi.QM_ERR_ARGUMENT and "16 hours" in str(err.value)
+
+
+def _road_thirds():
+    """A broadband spectrum peaking near 1 kHz, 2 dB down a band either side (energies)."""
+    return [dist.energy(60.0 - 2.0 * abs(k - 16)) for k in range(28)]
+
+
+def _of_levels(levels, bin_db=0.5):
+    return dist.Distribution.of_levels(levels, bin_db)
+
+
+def test_loudness_matches_the_oracle_and_counts_how_long_a_sound_lasts():
+    """Mean loudness and Nden from the distributions equal the oracle's to the bit on the same
+    curves; and as the reference's test states (popup/src/loudness.rs:396-424): a sound heard half
+    of each period reads half its steady loudness; a pass loud a hundredth of the time adds a
+    hundredth of its loudness; a sound in the day alone reads half its day in Nden, one at night
+    alone a third of its loudness 10 dB up."""
+    curve = dist.Curve(_road_thirds())
+    shape = native.loudness_curve_shape(_road_thirds())
+    assert np.array_equal(shape, np.array(curve.shape_db))
+    assert native.loudness_curve_shape([0.0] * 28) is None
+    curves = np.array([curve.table] * 3)
+
+    def both(distributions):
+        bins = np.array([_bins(d) for d in distributions])
+        got_mean, got_nden = native.distribution_loudness(0.5, bins, curves)
+        want_mean, want_nden = dist.loudness(distributions, [curve] * 3)
+        assert np.array_equal(got_mean, np.array(want_mean)) and got_nden == want_nden
+        return got_mean, got_nden
+
+    silent = _of_levels([(-math.inf, 1.0)])
+    steady, _ = both([_of_levels([(60.0, 1.0)])] * 3)
+    half, _ = both([_of_levels([(60.0, 0.5), (-math.inf, 0.5)])] * 3)
+    assert abs(half[0] / steady[0] - 0.5) < 1e-9
+    rare, _ = both([_of_levels([(40.0, 0.99), (80.0, 0.01)])] * 3)
+    expected = 0.99 * curve.at(40.0) + 0.01 * curve.at(80.0)
+    assert abs(rare[0] - expected) < 1e-9 * expected
+    day_mean, day_nden = both([_of_levels([(60.0, 1.0)]), silent, silent])
+    assert abs(day_nden - day_mean[0] / 2.0) < 1e-9
+    _, night_nden = both([silent, silent, _of_levels([(60.0, 1.0)])])
+    assert abs(night_nden - curve.at(70.0) / 3.0) < 1e-9
+    nothing, nothing_nden = both([silent] * 3)
+    assert np.array_equal(nothing, np.zeros(3)) and nothing_nden == 0.0
+    # A road-like sound's loudness about doubles per 10 dB (loudness.rs:351-391).
+    assert 1.8 < curve.at(70.0) / curve.at(60.0) < 2.3 and 10.0 < curve.at(65.0) < 30.0
+
+
+def test_loudness_of_a_place_matches_the_oracle():
+    """The place of the layer tests, its three periods' distributions read on three curves."""
+    layers = _place(7, sparse=False)
+    _, whole = dist.layered_distributions(layers, 0.5)
+    curves = [dist.Curve([dist.energy(55.0 + p * 3.0 - 1.5 * abs(k - 14 - p)) for k in range(28)]) for p in range(3)]
+    bins = np.array([_bins(whole[p]) for p in range(3)])
+    got_mean, got_nden = native.distribution_loudness(0.5, bins, np.array([c.table for c in curves]))
+    want_mean, want_nden = dist.loudness(whole, curves)
+    assert np.array_equal(got_mean, np.array(want_mean)) and got_nden == want_nden and got_nden > 0.0
