@@ -101,6 +101,21 @@ qm_status qm_loudness_curve_shape(const double *thirds, double *shape_db, int *h
 qm_status qm_distribution_loudness(double bin_db, const double *bins, const double *curves, double *mean_sone,
                                    double *nden_sone);
 
+/* One pixel of the reference's packed loudness input (paint/src/sone.rs:32-51, 217-234; read by
+ * its card, paint-gpu/kernels/loudness.cuh), read for one period: per layer (n_layers of them,
+ * six in the reference) its steady energy per period, its line count and its lines of
+ * QM_PACKED_LINE_FLOATS floats (energy per period, means per period and weather state, lambda
+ * per period, hourly profile or -1, duty per period or NaN, passes in progress per period or
+ * NaN); then each layer's curves and the place's, per period 28 third-octave levels at an
+ * A-weighted 0 dB (NaN: no shape). Writes the period's lines (their layers set; at most `cap`,
+ * *n_lines the count, QM_ERR_CAPACITY beyond), each line's profile (-1: none) into profiles,
+ * steady[n_layers], shapes[n_layers + 1][28] and has_shape[n_layers + 1]. Rejects a pixel
+ * whose counts run past `n_floats` or leave floats over. */
+#define QM_PACKED_LINE_FLOATS 43
+qm_status qm_pixel_read(const float *packed, size_t n_floats, uint32_t n_layers, uint32_t period,
+                        qm_period_line *lines, int32_t *profiles, size_t cap, size_t *n_lines, double *steady,
+                        double *shapes, uint8_t *has_shape);
+
 /* The same over a period's groups of hours (popup/src/percentiles.rs:88-160 with hour_groups,
  * percentiles/traffic.rs:251-279): a period of `hours` hours whose groups hold group_hours[g]
  * hours each; profiled[k] marks a line that follows an hourly profile and factors[g][n_lines]

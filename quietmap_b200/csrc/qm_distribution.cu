@@ -369,6 +369,64 @@ qm_status qm_distribution_loudness(double bin_db, const double *bins, const doub
     return QM_OK;
 }
 
+qm_status qm_pixel_read(const float *packed, size_t n_floats, uint32_t n_layers, uint32_t period,
+                        qm_period_line *lines, int32_t *profiles, size_t cap, size_t *n_lines, double *steady,
+                        double *shapes, uint8_t *has_shape) {
+    if ((n_floats > 0 && packed == nullptr) || n_lines == nullptr || steady == nullptr || shapes == nullptr ||
+        has_shape == nullptr || (cap > 0 && (lines == nullptr || profiles == nullptr)))
+        return qm::set_error(QM_ERR_ARGUMENT, "qm_pixel_read: null argument");
+    if (period >= 3) return qm::set_error(QM_ERR_ARGUMENT, "qm_pixel_read: period must be 0, 1 or 2");
+    const int P = 3, S = QM_WEATHER_STATES;
+    size_t at = 0, count = 0;
+    auto need = [&](size_t floats, const std::string &what) {
+        if (at > n_floats || n_floats - at < floats)
+            return qm::set_error(QM_ERR_ARGUMENT, "qm_pixel_read: " + what + " runs past the pixel's " +
+                                                      std::to_string(n_floats) + " floats");
+        return QM_OK;
+    };
+    for (uint32_t l = 0; l < n_layers; ++l) {
+        const std::string layer = "layer " + std::to_string(l);
+        if (need(P + 1, layer) != QM_OK) return QM_ERR_ARGUMENT;
+        steady[l] = (double)packed[at + period];
+        const float lines_f = packed[at + P];
+        at += P + 1;
+        if (!(lines_f >= 0.0f) || lines_f != std::floor(lines_f) || lines_f > (float)INT32_MAX)
+            return qm::set_error(QM_ERR_ARGUMENT, "qm_pixel_read: " + layer + " has no whole line count");
+        const size_t n = (size_t)lines_f;
+        if (need(n * QM_PACKED_LINE_FLOATS, layer + "'s lines") != QM_OK) return QM_ERR_ARGUMENT;
+        for (size_t k = 0; k < n; ++k, at += QM_PACKED_LINE_FLOATS) {
+            const float *f = packed + at;
+            if (count < cap) {
+                qm_period_line &line = lines[count];
+                line.layer = l;
+                line.reserved = 0;
+                line.energy = (double)f[period];
+                for (int st = 0; st < S; ++st) line.means[st] = (double)f[P + period * S + st];
+                line.lambda = (double)f[P + P * S + period];
+                profiles[count] = f[2 * P + P * S] < 0.0f ? -1 : (int32_t)f[2 * P + P * S];
+                line.duty = (double)f[2 * P + P * S + 1 + period];
+                line.passing = (double)f[3 * P + P * S + 1 + period];
+            }
+            ++count;
+        }
+    }
+    for (uint32_t c = 0; c <= n_layers; ++c) {
+        if (need((size_t)P * 28, "curve " + std::to_string(c)) != QM_OK) return QM_ERR_ARGUMENT;
+        const float *shape = packed + at + (size_t)period * 28;
+        has_shape[c] = std::isnan(shape[0]) ? 0 : 1;
+        for (int k = 0; k < 28; ++k) shapes[(size_t)c * 28 + k] = has_shape[c] ? (double)shape[k] : -INFINITY;
+        at += (size_t)P * 28;
+    }
+    if (at != n_floats)
+        return qm::set_error(QM_ERR_ARGUMENT, "qm_pixel_read: " + std::to_string(n_floats - at) +
+                                                  " floats left over after the curves");
+    *n_lines = count;
+    if (count > cap)
+        return qm::set_error(QM_ERR_CAPACITY, "qm_pixel_read: " + std::to_string(count) + " lines, room for " +
+                                                  std::to_string(cap));
+    return QM_OK;
+}
+
 qm_status qm_distribution_pass_values(double mean, double *values, size_t cap, size_t *n_values) {
     if (n_values == nullptr || (cap > 0 && values == nullptr))
         return qm::set_error(QM_ERR_ARGUMENT, "qm_distribution_pass_values: null values or n_values");

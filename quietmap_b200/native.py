@@ -160,6 +160,9 @@ def lib():
         L.qm_distribution_pass_values.restype = C.c_int
         L.qm_distribution_layers.argtypes = [C.c_double, C.c_void_p, C.c_size_t, _D, C.c_size_t, _D, _D, _D, _D]
         L.qm_distribution_layers.restype = C.c_int
+        L.qm_pixel_read.argtypes = [C.POINTER(C.c_float), C.c_size_t, C.c_uint32, C.c_uint32, C.c_void_p,
+                                    C.POINTER(C.c_int32), C.c_size_t, C.POINTER(C.c_size_t), _D, _D, _U8]
+        L.qm_pixel_read.restype = C.c_int
         L.qm_loudness_curve_shape.argtypes = [_D, _D, C.POINTER(C.c_int)]
         L.qm_loudness_curve_shape.restype = C.c_int
         L.qm_distribution_loudness.argtypes = [C.c_double, _D, _D, _D, _D]
@@ -500,6 +503,22 @@ def distribution_loudness(bin_db, bins, curves):
     _check(lib().qm_distribution_loudness(float(bin_db), abi.ptr(b, C.c_double), abi.ptr(c, C.c_double),
                                           abi.ptr(mean, C.c_double), C.byref(nden)))
     return mean, nden.value
+
+
+def pixel_read(packed, n_layers, period, cap=4096):
+    """One period of a packed pixel (qm_pixel_read): (lines PERIOD_LINE_DTYPE, profiles, steady
+    [n_layers], shapes [n_layers + 1][28], has_shape [n_layers + 1])."""
+    f = np.ascontiguousarray(packed, dtype=np.float32)
+    lines = np.zeros(cap, dtype=abi.PERIOD_LINE_DTYPE)
+    profiles = np.zeros(cap, np.int32)
+    n = C.c_size_t()
+    steady = np.zeros(n_layers)
+    shapes = np.zeros((n_layers + 1, 28))
+    has = np.zeros(n_layers + 1, np.uint8)
+    _check(lib().qm_pixel_read(abi.ptr(f, C.c_float) if len(f) else None, len(f), int(n_layers), int(period),
+                               lines.ctypes.data, abi.ptr(profiles, C.c_int32), cap, C.byref(n),
+                               abi.ptr(steady, C.c_double), abi.ptr(shapes, C.c_double), abi.ptr(has, C.c_uint8)))
+    return lines[:n.value].copy(), profiles[:n.value].copy(), steady, shapes, has.astype(bool)
 
 
 def distribution_merge_states(lines, spread):

@@ -1,0 +1,109 @@
+"""The reference's packed per-pixel loudness input (paint/src/sone.rs:32-51, 217-234) read by the
+library (qm_pixel_read): a pixel packed here by the format's rule (per layer its steady energy,
+line count and 43-float lines; then each layer's curves and the place's, 28 floats per period)
+reads back line by line for every period as float32 values, profiles and missing duties or
+passes included; curves without a shape are marked; malformed pixels are refused."""
+
+import math
+
+import numpy as np
+import pytest
+
+from quietmap_b200 import abi, native
+
+LAYERS = 6
+STATES = abi.WEATHER_STATES
+
+
+def _pack(layers, curves):
+    """layers: [(steady[3], [line dicts])]; curves: [n_layers + 1][3] shapes (28 dB) or None."""
+    out = []
+    for steady, lines in layers:
+        out += list(steady) + [float(len(lines))]
+        for line in lines:
+            out += list(line["energy"])
+            for period in range(3):
+                out += list(line["means"][period])
+            out += list(line["lambda"])
+            out.append(-1.0 if line["profile"] is None else float(line["profile"]))
+            for key in ("duty", "passing"):
+                out += [math.nan] * 3 if line[key] is None else list(line[key])
+    for per_period in curves:
+        for shape in per_period:
+            out += [math.nan] * 28 if shape is None else list(shape)
+    return np.array(out, dtype=np.float32)
+
+
+def _pixel(rng):
+    layers = []
+    for layer in range(LAYERS):
+        lines = []
+        for _ in range(int(rng.integers(0, 5)) if layer != 4 else 0):
+            kind = rng.integers(0, 4)
+            lines.append(dict(
+                energy=list(10.0 ** rng.uniform(2.0, 7.0, 3)),
+                means=[list(10.0 ** rng.uniform(2.0, 7.0, STATES)) for _ in range(3)],
+                **{"lambda": list(10.0 ** rng.uniform(-3.0, 3.0, 3))},
+                profile=None if kind == 0 else int(rng.integers(0, 12)),
+                duty=list(rng.uniform(0.0, 0.3, 3)) if kind == 1 else None,
+                passing=list(rng.uniform(0.0, 5.0, 3)) if kind == 2 else None))
+        layers.append((list(10.0 ** rng.uniform(0.0, 6.0, 3)), lines))
+    curves = [[None if rng.random() < 0.2 else list(rng.uniform(-60.0, 5.0, 28)) for _ in range(3)]
+              for _ in range(LAYERS + 1)]
+    return layers, curves
+
+
+def test_a_packed_pixel_reads_back_for_every_period():
+    rng = np.random.default_rng(21)
+    for _ in range(20):
+        layers, curves = _pixel(rng)
+        packed = _pack(layers, curves)
+        f32 = lambda v: float(np.float32(v))
+        for period in range(3):
+            lines, profiles, steady, shapes, has_shape = native.pixel_read(packed, LAYERS, period)
+            expected = [(layer, line) for layer, (_, ls) in enumerate(layers) for line in ls]
+            assert len(lines) == len(expected)
+            for row, profile, (layer, line) in zip(lines, profiles, expected):
+                assert row["layer"] == layer and row["energy"] == f32(line["energy"][period])
+                assert np.array_equal(row["means"], np.float32(line["means"][period]).astype(np.float64))
+                assert row["lambda"] == f32(line["lambda"][period])
+                assert profile == (-1 if line["profile"] is None else line["profile"])
+                for key in ("duty", "passing"):
+                    if line[key] is None:
+                        assert math.isnan(row[key])
+                    else:
+                        assert row[key] == f32(line[key][period])
+            assert np.array_equal(steady, [f32(st[period]) for st, _ in layers])
+            for c in range(LAYERS + 1):
+                shape = curves[c][period]
+                assert has_shape[c] == (shape is not None)
+                if shape is not None:
+                    assert np.array_equal(shapes[c], np.float32(shape).astype(np.float64))
+            # The lines read go straight into a period's layers.
+            native.distribution_layers(2.0, lines, steady)
+
+
+def test_malformed_pixels_are_refused():
+    rng = np.random.default_rng(2)
+    layers, curves = _pixel(rng)
+    packed = _pack(layers, curves)
+    for cut, words in ((packed[:-1], "curve 6"), (np.concatenate([packed, [0.0]]), "left over")):
+        with pytest.raises(native.QmError) as err:
+            native.pixel_read(cut, LAYERS, 0)
+        assert err.value.status == abi.QM_ERR_ARGUMENT and words in str(err.value)
+    bad = packed.copy()
+    bad[3] = 2.5
+    with pytest.raises(native.QmError) as err:
+        native.pixel_read(bad, LAYERS, 0)
+    assert "no whole line count" in str(err.value)
+    bad[3] = 1e6
+    with pytest.raises(native.QmError) as err:
+        native.pixel_read(bad, LAYERS, 0)
+    assert "runs past" in str(err.value)
+    total = sum(len(ls) for _, ls in layers)
+    if total > 1:
+        with pytest.raises(native.QmError) as err:
+            native.pixel_read(packed, LAYERS, 0, cap=1)
+        assert err.value.status == abi.QM_ERR_CAPACITY
+    with pytest.raises(native.QmError):
+        native.pixel_read(packed, LAYERS, 3)
