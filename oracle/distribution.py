@@ -430,3 +430,85 @@ def loudness(distributions, curves):
     for p in range(3):
         day += PERIOD_HOURS[p] * penalised[p]
     return mean_sone, day / 24.0
+
+
+# ---------------------------------------------------------------------------------------------
+# A line's means in the weather states from its pieces' energies in the two meteorological states
+# (popup/src/percentiles/weather.rs:1-127).
+
+SHARE_BINS = 10                          # weather.rs:6
+EPSILON = 2.220446049250313e-16          # f64::EPSILON
+
+
+def favourable_share(mean, homogeneous, favourable):
+    """The share of the time in the favourable state, from the mean being the mix of the two
+    (weather.rs:77-84)."""
+    if abs(favourable - homogeneous) <= EPSILON * abs(favourable):
+        return 0.0
+    return min(max((mean - homogeneous) / (favourable - homogeneous), 0.0), 1.0)
+
+
+class Weather:
+    """A contributor's energy per period in each state (homogeneous, favourable) and mixed, binned
+    by its pieces' favourable share, pieces louder in calm air in bins of their own
+    (weather.rs:7-75)."""
+
+    def __init__(self):
+        self.bins = [[[0.0] * 3 for _ in range(3)] for _ in range(2 * SHARE_BINS)]
+        self.active = 0
+
+    @staticmethod
+    def binned(energy, states):
+        homogeneous, favourable = states if (states[0] > 0.0 or states[1] > 0.0) else (energy, energy)
+        share = favourable_share(energy, homogeneous, favourable)
+        calm_louder = 1 if favourable < homogeneous else 0
+        position = share * SHARE_BINS
+        bin_ = calm_louder * SHARE_BINS + min(int(position) if position == position else 0, SHARE_BINS - 1)
+        return bin_, (homogeneous, favourable, energy)
+
+    def add_binned(self, period, bin_, values):
+        self.active |= 1 << bin_
+        for state, value in enumerate(values):
+            self.bins[bin_][state][period] += value
+
+    def add(self, energy, states):
+        """A piece of `energy` per period, the mix of its states[0] (homogeneous) and states[1]
+        (favourable) per period."""
+        for period in range(3):
+            bin_, values = Weather.binned(energy[period], (states[0][period], states[1][period]))
+            self.add_binned(period, bin_, values)
+
+
+def weather_means(weather, energy):
+    """Per period the mean of `energy` in each weather state (weather.rs:85-127): each bin's calm
+    energy in every state, its excess downwind in the states wholly under its share and in part
+    in the state its share falls in."""
+    if weather.active == 0:
+        return [[energy[p]] * WEATHER_STATES for p in range(3)]
+    out = []
+    for period in range(3):
+        whole, part = [0.0] * (WEATHER_STATES + 1), [0.0] * (WEATHER_STATES + 1)
+        calm, silent = 0.0, True
+        for bin_ in range(2 * SHARE_BINS):
+            if not (weather.active >> bin_) & 1:
+                continue
+            homogeneous = weather.bins[bin_][0][period]
+            favourable = weather.bins[bin_][1][period]
+            mix = weather.bins[bin_][2][period]
+            silent = silent and homogeneous + favourable <= 0.0
+            share = favourable_share(mix, homogeneous, favourable)
+            position = share * WEATHER_STATES
+            state = min(int(position) if position == position else 0, WEATHER_STATES)
+            whole[state] += favourable - homogeneous
+            part[state] += (position - state) * (favourable - homogeneous)
+            calm += homogeneous
+        if silent:
+            out.append([energy[period]] * WEATHER_STATES)
+            continue
+        means = [0.0] * WEATHER_STATES
+        above = 0.0
+        for state in reversed(range(WEATHER_STATES)):
+            above += whole[state + 1]
+            means[state] = calm + above + part[state]
+        out.append(means)
+    return out

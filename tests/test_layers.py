@@ -161,3 +161,63 @@ def test_the_library_merges_states_as_the_oracle_does():
         dist.merge_close_states([(lines, [0.0] * 3)], spread)
         for k, line in enumerate(lines):
             assert np.array_equal(merged[k]["means"], np.array(line.means[0])), (trial, k)
+
+
+def _steady_site(pieces, total=None):
+    """A steady source made of pieces (energy, calm, favourable), the same every period: its line
+    with means in the weather states."""
+    weather = dist.Weather()
+    energy = 0.0
+    for mean, calm, favourable in pieces:
+        weather.add([mean] * 3, [[calm] * 3, [favourable] * 3])
+        energy += mean
+    energy = energy if total is None else total
+    return dist.Line([energy] * 3, dist.weather_means(weather, [energy] * 3), [math.inf] * 3)
+
+
+def test_pieces_on_either_side_keep_their_own_weather():
+    """percentiles_tests.rs:253-282: one piece always favourable (10 over calm 1), the other
+    never: the level holds at their sum."""
+    site = _steady_site([(10.0, 1.0, 10.0), (1.0, 1.0, 10.0)], total=11.0)
+    day = dist.layered_distributions([([site], [0.0] * 3)], BIN_DB)[1]
+    for p in range(3):
+        for exceeded in (0.05, 0.5, 0.9):
+            assert abs(day[p].exceeded_db(exceeded) - 10.0 * math.log10(11.0)) <= BIN_DB / 2.0
+
+
+def test_pieces_louder_in_opposite_states_keep_their_mean():
+    """percentiles_tests.rs:283-306: one piece louder downwind, one in calm air, in one share bin:
+    the states average to the mean."""
+    pieces, total = [], 0.0
+    for calm, downwind, share in ((1.0, 10.0, 0.41), (10.0, 1.0, 0.49)):
+        mean = calm + share * (downwind - calm)
+        pieces.append((mean, calm, downwind))
+        total += mean
+    line = _steady_site(pieces)
+    assert abs(sum(line.means[0]) / dist.WEATHER_STATES - total) < 1e-9
+
+
+def test_a_source_alone_keeps_its_weather():
+    """percentiles_tests.rs:307-338: favourable (50 dB) half the time and calm (40 dB) the other
+    half, the source is at each for half the period."""
+    calm, favourable = e(40.0), e(50.0)
+    site = _steady_site([(0.5 * (calm + favourable), calm, favourable)])
+    day = dist.layered_distributions([([site], [0.0] * 3)], BIN_DB)[1][0]
+    levels = [(10.0 * math.log10(i), s) for i, s in day.intensities()]
+    at = lambda db: sum(s for level, s in levels if abs(level - db) < 1e-9)
+    assert abs(at(40.0) - 0.5) < 1e-9 and abs(at(50.0) - 0.5) < 1e-9, levels
+
+
+def test_the_weather_moves_the_levels_smoothly():
+    """percentiles_tests.rs:339-370: favourable 24.9 % and 25.1 % of the time (10 over calm 1)
+    give nearly the same spread."""
+    def spread(share):
+        mean = share * 10.0 + (1.0 - share) * 1.0
+        site = _steady_site([(mean, 1.0, 10.0)])
+        return dist.layered_distributions([([site], [0.0] * 3)], BIN_DB)[1][0]
+
+    below, above = spread(0.249), spread(0.251)
+    mean = lambda d: sum(i * s for i, s in d.intensities())
+    assert abs(mean(above) / mean(below) - 1.0) < 0.01
+    for exceeded in (0.1, 0.5, 0.9):
+        assert abs(above.exceeded_db(exceeded) - below.exceeded_db(exceeded)) < 0.2
