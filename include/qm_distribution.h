@@ -116,6 +116,14 @@ qm_status qm_pixel_read(const float *packed, size_t n_floats, uint32_t n_layers,
                         qm_period_line *lines, int32_t *profiles, size_t cap, size_t *n_lines, double *steady,
                         double *shapes, uint8_t *has_shape);
 
+/* A line's means in the weather states (popup/src/percentiles/weather.rs:1-127, `Weather::add`
+ * over its pieces then `weather_means`): piece k's energy per period piece_energy[k][3], the mix
+ * of its homogeneous and favourable energies piece_states[k][2][3] (both 0: it holds its mean in
+ * either); `energy[3]` the line's energy, kept in every state where no piece has any. Writes
+ * means[3][QM_WEATHER_STATES], ready for qm_period_line.means. */
+qm_status qm_distribution_state_means(const double *piece_energy, const double *piece_states, size_t n_pieces,
+                                      const double *energy, double *means);
+
 /* The same over a period's groups of hours (popup/src/percentiles.rs:88-160 with hour_groups,
  * percentiles/traffic.rs:251-279): a period of `hours` hours whose groups hold group_hours[g]
  * hours each; profiled[k] marks a line that follows an hourly profile and factors[g][n_lines]

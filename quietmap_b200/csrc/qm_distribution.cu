@@ -427,6 +427,26 @@ qm_status qm_pixel_read(const float *packed, size_t n_floats, uint32_t n_layers,
     return QM_OK;
 }
 
+qm_status qm_distribution_state_means(const double *piece_energy, const double *piece_states, size_t n_pieces,
+                                      const double *energy, double *means) {
+    if ((n_pieces > 0 && (piece_energy == nullptr || piece_states == nullptr)) || energy == nullptr || means == nullptr)
+        return qm::set_error(QM_ERR_ARGUMENT, "qm_distribution_state_means: null argument");
+    for (size_t k = 0; k < n_pieces; ++k)
+        for (int v = 0; v < 9; ++v) {
+            const double x = v < 3 ? piece_energy[3 * k + v] : piece_states[6 * k + (v - 3)];
+            if (!(x >= 0.0) || !std::isfinite(x))
+                return qm::set_error(QM_ERR_ARGUMENT, "qm_distribution_state_means: piece " + std::to_string(k) +
+                                                          " has a negative or non-finite energy");
+        }
+    qm::dist::WeatherBins weather;
+    weather.clear();
+    for (size_t k = 0; k < n_pieces; ++k)
+        for (int p = 0; p < 3; ++p)
+            weather.add(p, piece_energy[3 * k + p], piece_states[6 * k + p], piece_states[6 * k + 3 + p]);
+    for (int p = 0; p < 3; ++p) weather.means(p, energy[p], means + (size_t)p * QM_WEATHER_STATES);
+    return QM_OK;
+}
+
 qm_status qm_distribution_pass_values(double mean, double *values, size_t cap, size_t *n_values) {
     if (n_values == nullptr || (cap > 0 && values == nullptr))
         return qm::set_error(QM_ERR_ARGUMENT, "qm_distribution_pass_values: null values or n_values");

@@ -386,5 +386,78 @@ __host__ __device__ inline double mean_loudness(const double *bins, int n_bins, 
     return total;
 }
 
+// A line's means in the weather states from its pieces' energies in the two meteorological
+// states (popup/src/percentiles/weather.rs:1-127). Pieces are binned by their favourable share,
+// pieces louder in calm air in bins of their own; each bin's calm energy counts in every state,
+// its excess downwind in the states wholly under its share and in part in the state its share
+// falls in.
+constexpr int SHARE_BINS = 10;                           // weather.rs:6
+constexpr double F64_EPSILON = 2.220446049250313e-16;
+
+__host__ __device__ inline double favourable_share(double mean, double homogeneous, double favourable) {
+    if (fabs(favourable - homogeneous) <= F64_EPSILON * fabs(favourable)) return 0.0;
+    return fmin(fmax((mean - homogeneous) / (favourable - homogeneous), 0.0), 1.0);
+}
+
+// A whole non-negative position's integer part, NaN as 0, held to `most`.
+__host__ __device__ inline int truncated(double position, int most) {
+    if (!(position > 0.0)) return 0;
+    return position >= (double)most ? most : (int)position;
+}
+
+struct WeatherBins {
+    double bins[2 * SHARE_BINS][3][3];  // [bin][homogeneous, favourable, mixed][period]
+    uint32_t active;
+
+    __host__ __device__ void clear() {
+        for (int b = 0; b < 2 * SHARE_BINS; ++b)
+            for (int st = 0; st < 3; ++st)
+                for (int p = 0; p < 3; ++p) bins[b][st][p] = 0.0;
+        active = 0;
+    }
+    // A piece of `energy` in one period, the mix of its homogeneous and favourable energies (a
+    // piece without states holds its mean in either).
+    __host__ __device__ void add(int period, double energy, double homogeneous, double favourable) {
+        if (!(homogeneous > 0.0 || favourable > 0.0)) homogeneous = favourable = energy;
+        const double share = favourable_share(energy, homogeneous, favourable);
+        const int bin = (favourable < homogeneous ? SHARE_BINS : 0) + truncated(share * SHARE_BINS, SHARE_BINS - 1);
+        active |= 1u << bin;
+        bins[bin][0][period] += homogeneous;
+        bins[bin][1][period] += favourable;
+        bins[bin][2][period] += energy;
+    }
+    // The period's mean of `energy` in each weather state.
+    __host__ __device__ void means(int period, double energy, double out[WEATHER_STATES]) const {
+        if (active == 0) {
+            for (int st = 0; st < WEATHER_STATES; ++st) out[st] = energy;
+            return;
+        }
+        double whole[WEATHER_STATES + 1], part[WEATHER_STATES + 1];
+        for (int st = 0; st <= WEATHER_STATES; ++st) whole[st] = part[st] = 0.0;
+        double calm = 0.0;
+        bool silent = true;
+        for (int b = 0; b < 2 * SHARE_BINS; ++b) {
+            if (!((active >> b) & 1u)) continue;
+            const double homogeneous = bins[b][0][period], favourable = bins[b][1][period];
+            silent = silent && homogeneous + favourable <= 0.0;
+            const double share = favourable_share(bins[b][2][period], homogeneous, favourable);
+            const double position = share * WEATHER_STATES;
+            const int state = truncated(position, WEATHER_STATES);
+            whole[state] += favourable - homogeneous;
+            part[state] += (position - (double)state) * (favourable - homogeneous);
+            calm += homogeneous;
+        }
+        if (silent) {
+            for (int st = 0; st < WEATHER_STATES; ++st) out[st] = energy;
+            return;
+        }
+        double above = 0.0;
+        for (int st = WEATHER_STATES - 1; st >= 0; --st) {
+            above += whole[st + 1];
+            out[st] = calm + above + part[st];
+        }
+    }
+};
+
 }  // namespace dist
 }  // namespace qm

@@ -160,6 +160,8 @@ def lib():
         L.qm_distribution_pass_values.restype = C.c_int
         L.qm_distribution_layers.argtypes = [C.c_double, C.c_void_p, C.c_size_t, _D, C.c_size_t, _D, _D, _D, _D]
         L.qm_distribution_layers.restype = C.c_int
+        L.qm_distribution_state_means.argtypes = [_D, _D, C.c_size_t, _D, _D]
+        L.qm_distribution_state_means.restype = C.c_int
         L.qm_pixel_read.argtypes = [C.POINTER(C.c_float), C.c_size_t, C.c_uint32, C.c_uint32, C.c_void_p,
                                     C.POINTER(C.c_int32), C.c_size_t, C.POINTER(C.c_size_t), _D, _D, _U8]
         L.qm_pixel_read.restype = C.c_int
@@ -519,6 +521,19 @@ def pixel_read(packed, n_layers, period, cap=4096):
                                lines.ctypes.data, abi.ptr(profiles, C.c_int32), cap, C.byref(n),
                                abi.ptr(steady, C.c_double), abi.ptr(shapes, C.c_double), abi.ptr(has, C.c_uint8)))
     return lines[:n.value].copy(), profiles[:n.value].copy(), steady, shapes, has.astype(bool)
+
+
+def distribution_state_means(piece_energy, piece_states, energy):
+    """A line's means [3][10] in the weather states from its pieces (qm_distribution_state_means):
+    piece_energy [n][3], piece_states [n][2][3] (homogeneous, favourable), energy [3]."""
+    pe = np.ascontiguousarray(np.asarray(piece_energy, dtype=np.float64).reshape(-1, 3))
+    ps = np.ascontiguousarray(np.asarray(piece_states, dtype=np.float64).reshape(-1, 2, 3))
+    en = np.ascontiguousarray(energy, dtype=np.float64)
+    out = np.zeros((3, abi.WEATHER_STATES))
+    _check(lib().qm_distribution_state_means(abi.ptr(pe, C.c_double) if len(pe) else None,
+                                             abi.ptr(ps, C.c_double) if len(ps) else None, len(pe),
+                                             abi.ptr(en, C.c_double), abi.ptr(out, C.c_double)))
+    return out
 
 
 def distribution_merge_states(lines, spread):

@@ -327,3 +327,37 @@ def test_loudness_of_a_place_matches_the_oracle():
     got_mean, got_nden = native.distribution_loudness(0.5, bins, np.array([c.table for c in curves]))
     want_mean, want_nden = dist.loudness(whole, curves)
     assert np.array_equal(got_mean, np.array(want_mean)) and got_nden == want_nden and got_nden > 0.0
+
+
+def test_weather_state_means_match_the_oracle_to_the_bit():
+    """Random pieces, some louder downwind, some in calm air, some without states, some silent in
+    a period: a line's means in the weather states equal the oracle's to the bit, and their
+    average is the line's energy where its pieces make it up."""
+    rng = np.random.default_rng(31)
+    for trial in range(300):
+        n = int(rng.integers(0, 8))
+        weather = dist.Weather()
+        piece_energy, piece_states = [], []
+        for _ in range(n):
+            calm = 10.0 ** rng.uniform(0.0, 6.0, 3)
+            favourable = calm * 10.0 ** rng.uniform(-1.0, 1.5, 3)
+            share = rng.uniform(0.0, 1.0, 3)
+            mean = calm + share * (favourable - calm)
+            if rng.random() < 0.15:
+                calm, favourable = np.zeros(3), np.zeros(3)
+            if rng.random() < 0.1:
+                mean[int(rng.integers(0, 3))] = 0.0
+            weather.add(list(mean), [list(calm), list(favourable)])
+            piece_energy.append(mean)
+            piece_states.append([calm, favourable])
+        energy = np.sum(piece_energy, axis=0) if n else 10.0 ** rng.uniform(0.0, 3.0, 3)
+        want = dist.weather_means(weather, list(energy))
+        got = native.distribution_state_means(np.array(piece_energy).reshape(-1, 3),
+                                              np.array(piece_states).reshape(-1, 2, 3), energy)
+        assert np.array_equal(got, np.array(want)), trial
+    # Pieces louder in opposite states keep their mean (percentiles_tests.rs:283-306).
+    pieces = [(1.0, 10.0, 0.41), (10.0, 1.0, 0.49)]
+    means = [calm + share * (down - calm) for calm, down, share in pieces]
+    got = native.distribution_state_means([[m] * 3 for m in means],
+                                          [[[calm] * 3, [down] * 3] for calm, down, _ in pieces], [sum(means)] * 3)
+    assert abs(got[0].mean() - sum(means)) < 1e-9
