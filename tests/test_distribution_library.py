@@ -361,3 +361,52 @@ def test_weather_state_means_match_the_oracle_to_the_bit():
     got = native.distribution_state_means([[m] * 3 for m in means],
                                           [[[calm] * 3, [down] * 3] for calm, down, _ in pieces], [sum(means)] * 3)
     assert abs(got[0].mean() - sum(means)) < 1e-9
+
+
+def test_a_pixel_from_its_pieces_to_nden_matches_the_oracle():
+    """The chain a pixel's loudness takes, every step through the library and checked against the
+    oracle: each line's means in the weather states from its pieces' calm and favourable
+    energies, merged where close (the map's spread 1.2), the period's layers on the map's 2 dB grid
+    (roads, bells, flights, steady energy), and each period's loudness on its curve and Nden."""
+    rng = np.random.default_rng(41)
+    states = dist.WEATHER_STATES
+    layers_oracle = []
+    for layer in range(3):
+        lines = []
+        for k in range(3):
+            weather = dist.Weather()
+            total = np.zeros(3)
+            piece_energy, piece_states = [], []
+            for _ in range(int(rng.integers(1, 4))):
+                calm = 10.0 ** rng.uniform(2.0, 5.0, 3)
+                favourable = calm * 10.0 ** rng.uniform(0.0, 1.0, 3)
+                mean = calm + rng.uniform(0.0, 1.0, 3) * (favourable - calm)
+                weather.add(list(mean), [list(calm), list(favourable)])
+                piece_energy.append(mean)
+                piece_states.append([calm, favourable])
+                total += mean
+            means = dist.weather_means(weather, list(total))
+            assert np.array_equal(native.distribution_state_means(piece_energy, piece_states, total), means)
+            if layer == 1 and k == 0:
+                lines.append(dist.Line(list(total), means, [math.inf] * 3, duty=[0.05, 0.02, 0.0]))
+            elif layer == 2:
+                lines.append(dist.Line(list(total), means, [math.inf] * 3, passing=[0.05 * (k + 1), 0.1, 0.0]))
+            else:
+                lines.append(dist.Line(list(total), means, [40.0, 20.0, 12.0]))
+        layers_oracle.append((lines, list(10.0 ** rng.uniform(1.0, 3.0, 3))))
+    dist.merge_close_states(layers_oracle, 1.2)
+    curves = [dist.Curve([dist.energy(58.0 - 1.8 * abs(k - 15 - p)) for k in range(28)]) for p in range(3)]
+    each, whole = dist.layered_distributions(layers_oracle, 2.0)
+    want_mean, want_nden = dist.loudness(whole, curves)
+
+    bins = []
+    for p in range(3):
+        rows = _period_rows(layers_oracle, p)
+        rows = native.distribution_merge_states(rows, 1.2)    # already merged: a fixed point
+        assert np.array_equal(rows["means"], _period_rows(layers_oracle, p)["means"])
+        layer_bins, layer_silent, place, place_silent = native.distribution_layers(
+            2.0, rows, [steady[p] for _, steady in layers_oracle])
+        assert np.array_equal(place, _bins(whole[p])) and place_silent == whole[p].silent
+        bins.append(place)
+    got_mean, got_nden = native.distribution_loudness(2.0, np.array(bins), np.array([c.table for c in curves]))
+    assert np.array_equal(got_mean, np.array(want_mean)) and got_nden == want_nden and got_nden > 0.0
