@@ -124,6 +124,16 @@ qm_status qm_pixel_read(const float *packed, size_t n_floats, uint32_t n_layers,
 qm_status qm_distribution_state_means(const double *piece_energy, const double *piece_states, size_t n_pieces,
                                       const double *energy, double *means);
 
+/* hour_factor and hour_groups (popup/src/percentiles/traffic.rs:31-39, 251-279) over the caller's
+ * hourly shares[n_profiles][24] (by hour of the day; the reference's are measured road profiles):
+ * a period's 12, 4 or 8 hours (from 7, 19 and 23 h) each apart when `runs` is 0, else sorted by
+ * their flow summed over the profiles (ties by hour) and cut into `runs` runs (the map: 4, 1, 3).
+ * Writes group_of_slot[hours], group_hours[n_groups] and factors[n_groups][n_profiles], each
+ * profile's mean hour factor over the group (its flow there against the period's mean), for
+ * qm_distribution_layers_grouped; at most 12 groups. */
+qm_status qm_hour_groups(const double *shares, size_t n_profiles, uint32_t period, uint32_t runs,
+                         uint32_t *group_of_slot, uint32_t *group_hours, double *factors, size_t *n_groups);
+
 /* The same over a period's groups of hours (popup/src/percentiles.rs:88-160 with hour_groups,
  * percentiles/traffic.rs:251-279): a period of `hours` hours whose groups hold group_hours[g]
  * hours each; profiled[k] marks a line that follows an hourly profile and factors[g][n_lines]

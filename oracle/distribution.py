@@ -512,3 +512,45 @@ def weather_means(weather, energy):
             means[state] = calm + above + part[state]
         out.append(means)
     return out
+
+
+# ---------------------------------------------------------------------------------------------
+# Hours of a period grouped by their flow (popup/src/percentiles/traffic.rs:31-39, 251-279), over
+# a caller's hourly shares per profile (shares[profile][24], by hour of the day).
+
+PERIOD_FIRST_HOUR = (7, 19, 23)                     # traffic.rs:31
+
+
+def hour_factor(shares, profile, period, slot):
+    """A road's flow in the slot-th hour of the period against its mean over the period."""
+    hours = int(PERIOD_HOURS[period])
+    share = lambda s: shares[profile][(PERIOD_FIRST_HOUR[period] + s) % 24]
+    total = 0.0
+    for s in range(hours):
+        total += share(s)
+    return share(slot) / (total / hours)
+
+
+def hour_groups(shares, period, runs):
+    """(groups of slots, hours): every hour apart without `runs`, else the hours sorted by their
+    flow summed over the profiles (ties by hour) cut into `runs` runs, each in hour order."""
+    hours = int(PERIOD_HOURS[period])
+    if runs is None:
+        return [[slot] for slot in range(hours)], hours
+
+    def flow(slot):
+        total = 0.0
+        for profile in range(len(shares)):
+            total += hour_factor(shares, profile, period, slot)
+        return total
+
+    slots = sorted(range(hours), key=lambda slot: (flow(slot), slot))
+    return [sorted(slots[run * hours // runs:(run + 1) * hours // runs]) for run in range(runs)], hours
+
+
+def group_factor(shares, profile, period, slots):
+    """A profiled line's flow over a group of hours: the mean of its hours' factors."""
+    total = 0.0
+    for slot in slots:
+        total += hour_factor(shares, profile, period, slot)
+    return total / len(slots)

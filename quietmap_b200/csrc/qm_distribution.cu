@@ -447,6 +447,59 @@ qm_status qm_distribution_state_means(const double *piece_energy, const double *
     return QM_OK;
 }
 
+qm_status qm_hour_groups(const double *shares, size_t n_profiles, uint32_t period, uint32_t runs,
+                         uint32_t *group_of_slot, uint32_t *group_hours, double *factors, size_t *n_groups) {
+    if ((n_profiles > 0 && shares == nullptr) || group_of_slot == nullptr || group_hours == nullptr ||
+        (n_profiles > 0 && factors == nullptr) || n_groups == nullptr)
+        return qm::set_error(QM_ERR_ARGUMENT, "qm_hour_groups: null argument");
+    if (period >= 3) return qm::set_error(QM_ERR_ARGUMENT, "qm_hour_groups: period must be 0, 1 or 2");
+    static const int first_hour[3] = {7, 19, 23};  // traffic.rs:31
+    const int hours = (int)qm::dist::PERIOD_HOURS[period];
+    if (runs > (uint32_t)hours)
+        return qm::set_error(QM_ERR_ARGUMENT, "qm_hour_groups: more runs than the period's " + std::to_string(hours) + " hours");
+    for (size_t k = 0; k < 24 * n_profiles; ++k)
+        if (!(shares[k] > 0.0) || !std::isfinite(shares[k]))
+            return qm::set_error(QM_ERR_ARGUMENT, "qm_hour_groups: share " + std::to_string(k) + " is not positive and finite");
+    auto share = [&](size_t profile, int slot) { return shares[profile * 24 + (first_hour[period] + slot) % 24]; };
+    std::vector<double> mean(n_profiles);
+    for (size_t profile = 0; profile < n_profiles; ++profile) {
+        double total = 0.0;
+        for (int slot = 0; slot < hours; ++slot) total += share(profile, slot);
+        mean[profile] = total / (double)hours;
+    }
+    auto factor = [&](size_t profile, int slot) { return share(profile, slot) / mean[profile]; };
+    std::vector<std::vector<int>> groups;
+    if (runs == 0) {
+        for (int slot = 0; slot < hours; ++slot) groups.push_back({slot});
+    } else {
+        std::vector<double> flow(hours);
+        for (int slot = 0; slot < hours; ++slot) {
+            double total = 0.0;
+            for (size_t profile = 0; profile < n_profiles; ++profile) total += factor(profile, slot);
+            flow[slot] = total;
+        }
+        std::vector<int> slots(hours);
+        for (int slot = 0; slot < hours; ++slot) slots[slot] = slot;
+        std::sort(slots.begin(), slots.end(), [&](int a, int b) { return flow[a] < flow[b] || (flow[a] == flow[b] && a < b); });
+        for (uint32_t run = 0; run < runs; ++run) {
+            std::vector<int> group(slots.begin() + run * hours / runs, slots.begin() + (run + 1) * hours / runs);
+            std::sort(group.begin(), group.end());
+            groups.push_back(group);
+        }
+    }
+    for (size_t g = 0; g < groups.size(); ++g) {
+        group_hours[g] = (uint32_t)groups[g].size();
+        for (int slot : groups[g]) group_of_slot[slot] = (uint32_t)g;
+        for (size_t profile = 0; profile < n_profiles; ++profile) {
+            double total = 0.0;
+            for (int slot : groups[g]) total += factor(profile, slot);
+            factors[g * n_profiles + profile] = total / (double)groups[g].size();
+        }
+    }
+    *n_groups = groups.size();
+    return QM_OK;
+}
+
 qm_status qm_distribution_pass_values(double mean, double *values, size_t cap, size_t *n_values) {
     if (n_values == nullptr || (cap > 0 && values == nullptr))
         return qm::set_error(QM_ERR_ARGUMENT, "qm_distribution_pass_values: null values or n_values");

@@ -160,6 +160,8 @@ def lib():
         L.qm_distribution_pass_values.restype = C.c_int
         L.qm_distribution_layers.argtypes = [C.c_double, C.c_void_p, C.c_size_t, _D, C.c_size_t, _D, _D, _D, _D]
         L.qm_distribution_layers.restype = C.c_int
+        L.qm_hour_groups.argtypes = [_D, C.c_size_t, C.c_uint32, C.c_uint32, _U32, _U32, _D, C.POINTER(C.c_size_t)]
+        L.qm_hour_groups.restype = C.c_int
         L.qm_distribution_state_means.argtypes = [_D, _D, C.c_size_t, _D, _D]
         L.qm_distribution_state_means.restype = C.c_int
         L.qm_pixel_read.argtypes = [C.POINTER(C.c_float), C.c_size_t, C.c_uint32, C.c_uint32, C.c_void_p,
@@ -534,6 +536,21 @@ def distribution_state_means(piece_energy, piece_states, energy):
                                              abi.ptr(ps, C.c_double) if len(ps) else None, len(pe),
                                              abi.ptr(en, C.c_double), abi.ptr(out, C.c_double)))
     return out
+
+
+def hour_groups(shares, period, runs=0):
+    """A period's groups of hours over hourly shares [n_profiles][24] (qm_hour_groups):
+    (group_of_slot, group_hours, factors [n_groups][n_profiles])."""
+    sh = np.ascontiguousarray(shares, dtype=np.float64).reshape(-1, 24)
+    group_of_slot = np.zeros(12, np.uint32)
+    group_hours = np.zeros(12, np.uint32)
+    factors = np.zeros((12, max(len(sh), 1)))
+    n = C.c_size_t()
+    _check(lib().qm_hour_groups(abi.ptr(sh, C.c_double) if len(sh) else None, len(sh), int(period), int(runs),
+                                abi.ptr(group_of_slot, C.c_uint32), abi.ptr(group_hours, C.c_uint32),
+                                abi.ptr(factors, C.c_double), C.byref(n)))
+    hours = int(group_hours[:n.value].sum())
+    return group_of_slot[:hours].copy(), group_hours[:n.value].copy(), factors[:n.value, :len(sh)].copy()
 
 
 def distribution_merge_states(lines, spread):

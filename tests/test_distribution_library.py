@@ -410,3 +410,49 @@ def test_a_pixel_from_its_pieces_to_nden_matches_the_oracle():
         bins.append(place)
     got_mean, got_nden = native.distribution_loudness(2.0, np.array(bins), np.array([c.table for c in curves]))
     assert np.array_equal(got_mean, np.array(want_mean)) and got_nden == want_nden and got_nden > 0.0
+
+
+def test_hour_groups_match_the_oracle_and_feed_the_grouped_layers():
+    """Over random hourly shares of three profiles: each period's hours, apart or in the map's
+    four, one and three groups, and each profile's flow factor per group equal the oracle's to the
+    bit; the groups cover the period's hours and a profile's factors average to 1 over them. A
+    profiled road over those groups then gives the oracle's distributions to the bit."""
+    rng = np.random.default_rng(17)
+    shares = rng.uniform(0.3, 9.0, (3, 24))
+    for period in range(3):
+        hours = int(dist.PERIOD_HOURS[period])
+        for runs in (0, 1, 2, [4, 1, 3][period], hours):
+            slot_group, group_hours, factors = native.hour_groups(shares, period, runs)
+            groups, want_hours = dist.hour_groups(shares.tolist(), period, runs or None)
+            assert want_hours == hours and len(group_hours) == len(groups) and group_hours.sum() == hours
+            for g, slots in enumerate(groups):
+                assert group_hours[g] == len(slots) and all(slot_group[s] == g for s in slots)
+                for profile in range(3):
+                    assert factors[g, profile] == dist.group_factor(shares.tolist(), profile, period, slots)
+            for profile in range(3):
+                assert abs((factors[:, profile] * group_hours).sum() / hours - 1.0) < 1e-12
+    with pytest.raises(native.QmError):
+        native.hour_groups(shares, 1, 5)
+    bad = shares.copy()
+    bad[1, 3] = 0.0
+    with pytest.raises(native.QmError):
+        native.hour_groups(bad, 0, 4)
+
+    # A profiled road (profile 1) beside a steady layer, over the map's groups.
+    states = dist.WEATHER_STATES
+    road = dist.Line([dist.energy(60.0)] * 3, [[dist.energy(60.0) * (1.0 + 0.05 * s) for s in range(states)]] * 3,
+                     [30.0, 15.0, 11.0])
+    layers = [([road], [0.0] * 3), ([], [dist.energy(45.0)] * 3)]
+    oracle_groups = []
+    for period in range(3):
+        groups, hours = dist.hour_groups(shares.tolist(), period, [4, 1, 3][period])
+        oracle_groups.append((hours, [(len(slots), [[dist.group_factor(shares.tolist(), 1, period, slots)], None])
+                                      for slots in groups]))
+    each, whole = dist.layered_distributions(layers, 2.0, oracle_groups)
+    for period in range(3):
+        _, group_hours, factors = native.hour_groups(shares, period, [4, 1, 3][period])
+        got_each, _, got_whole, got_silent = native.distribution_layers_grouped(
+            2.0, _period_rows(layers, period), [steady[period] for _, steady in layers],
+            int(dist.PERIOD_HOURS[period]), group_hours, factors[:, [1]], [True])
+        assert np.array_equal(got_whole, _bins(whole[period])) and got_silent == whole[period].silent
+        assert np.array_equal(got_each[0], _bins(each[0][period]))
