@@ -134,6 +134,17 @@ qm_status qm_distribution_state_means(const double *piece_energy, const double *
 qm_status qm_hour_groups(const double *shares, size_t n_profiles, uint32_t period, uint32_t runs,
                          uint32_t *group_of_slot, uint32_t *group_hours, double *factors, size_t *n_groups);
 
+/* A packed pixel's distributions for all three periods (layered_distributions on its placed
+ * layers, popup/src/percentiles.rs:88-160): the pixel read as qm_pixel_read reads it; where any
+ * line follows an hourly profile, each period's hours grouped as qm_hour_groups groups them over
+ * shares[n_profiles][24] with runs[3] runs (NULL: every hour apart), each profiled line at its
+ * profile's factor in each group; else one group at the mean flow. Writes
+ * layer_bins[n_layers][3][n_bins][2], layer_silent[n_layers][3], place_bins[3][n_bins][2] and
+ * place_silent[3]. A line naming a profile past n_profiles is refused. */
+qm_status qm_pixel_distributions(const float *packed, size_t n_floats, uint32_t n_layers, double bin_db,
+                                 const double *shares, size_t n_profiles, const uint32_t *runs, double *layer_bins,
+                                 double *layer_silent, double *place_bins, double *place_silent);
+
 /* The same over a period's groups of hours (popup/src/percentiles.rs:88-160 with hour_groups,
  * percentiles/traffic.rs:251-279): a period of `hours` hours whose groups hold group_hours[g]
  * hours each; profiled[k] marks a line that follows an hourly profile and factors[g][n_lines]

@@ -500,6 +500,76 @@ qm_status qm_hour_groups(const double *shares, size_t n_profiles, uint32_t perio
     return QM_OK;
 }
 
+qm_status qm_pixel_distributions(const float *packed, size_t n_floats, uint32_t n_layers, double bin_db,
+                                 const double *shares, size_t n_profiles, const uint32_t *runs, double *layer_bins,
+                                 double *layer_silent, double *place_bins, double *place_silent) {
+    int n_bins = 0;
+    const qm_status status = grid("qm_pixel_distributions", bin_db, n_bins);
+    if (status != QM_OK) return status;
+    if ((n_layers > 0 && (layer_bins == nullptr || layer_silent == nullptr)) || place_bins == nullptr ||
+        place_silent == nullptr)
+        return qm::set_error(QM_ERR_ARGUMENT, "qm_pixel_distributions: null output");
+    const size_t bins2 = 2 * (size_t)n_bins;
+    std::vector<double> steady(n_layers), shapes(((size_t)n_layers + 1) * 28), each(n_layers * bins2),
+        each_silent(n_layers);
+    std::vector<uint8_t> has_shape(n_layers + 1);
+    for (uint32_t period = 0; period < 3; ++period) {
+        // The period's lines: counted first, then read.
+        size_t n_lines = 0;
+        qm_status read = qm_pixel_read(packed, n_floats, n_layers, period, nullptr, nullptr, 0, &n_lines,
+                                       steady.data(), shapes.data(), has_shape.data());
+        if (read != QM_OK && read != QM_ERR_CAPACITY) return read;
+        std::vector<qm_period_line> lines(n_lines);
+        std::vector<int32_t> profiles(n_lines);
+        read = qm_pixel_read(packed, n_floats, n_layers, period, lines.data(), profiles.data(), n_lines, &n_lines,
+                             steady.data(), shapes.data(), has_shape.data());
+        if (read != QM_OK) return read;
+        std::vector<uint8_t> profiled(n_lines, 0);
+        bool any = false;
+        for (size_t k = 0; k < n_lines; ++k) {
+            if (profiles[k] < 0) continue;
+            if ((size_t)profiles[k] >= n_profiles)
+                return qm::set_error(QM_ERR_ARGUMENT, "qm_pixel_distributions: line " + std::to_string(k) +
+                                                          " follows profile " + std::to_string(profiles[k]) + " of " +
+                                                          std::to_string(n_profiles));
+            profiled[k] = 1;
+            any = true;
+        }
+        // The period's groups of hours (traffic.rs:251-279): one at the mean flow unless a line
+        // follows a profile.
+        uint32_t hours = 1;
+        std::vector<uint32_t> group_hours(1, 1);
+        std::vector<double> factors(n_lines, 1.0);
+        if (any) {
+            hours = (uint32_t)qm::dist::PERIOD_HOURS[period];
+            std::vector<uint32_t> slot_group(12);
+            std::vector<double> profile_factors(12 * n_profiles);
+            group_hours.assign(12, 0);
+            size_t n_groups = 0;
+            const qm_status grouped = qm_hour_groups(shares, n_profiles, period, runs ? runs[period] : 0,
+                                                     slot_group.data(), group_hours.data(), profile_factors.data(),
+                                                     &n_groups);
+            if (grouped != QM_OK) return grouped;
+            group_hours.resize(n_groups);
+            factors.assign(n_groups * n_lines, 1.0);
+            for (size_t g = 0; g < n_groups; ++g)
+                for (size_t k = 0; k < n_lines; ++k)
+                    if (profiled[k]) factors[g * n_lines + k] = profile_factors[g * n_profiles + (size_t)profiles[k]];
+        }
+        double silent = 0.0;
+        const qm_status layered = qm_distribution_layers_grouped(
+            bin_db, lines.data(), n_lines, steady.data(), n_layers, hours, group_hours.data(), group_hours.size(),
+            factors.data(), profiled.data(), each.data(), each_silent.data(), place_bins + period * bins2, &silent);
+        if (layered != QM_OK) return layered;
+        place_silent[period] = silent;
+        for (uint32_t l = 0; l < n_layers; ++l) {
+            std::copy(each.begin() + l * bins2, each.begin() + (l + 1) * bins2, layer_bins + ((size_t)l * 3 + period) * bins2);
+            layer_silent[(size_t)l * 3 + period] = each_silent[l];
+        }
+    }
+    return QM_OK;
+}
+
 qm_status qm_distribution_pass_values(double mean, double *values, size_t cap, size_t *n_values) {
     if (n_values == nullptr || (cap > 0 && values == nullptr))
         return qm::set_error(QM_ERR_ARGUMENT, "qm_distribution_pass_values: null values or n_values");

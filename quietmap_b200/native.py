@@ -160,6 +160,9 @@ def lib():
         L.qm_distribution_pass_values.restype = C.c_int
         L.qm_distribution_layers.argtypes = [C.c_double, C.c_void_p, C.c_size_t, _D, C.c_size_t, _D, _D, _D, _D]
         L.qm_distribution_layers.restype = C.c_int
+        L.qm_pixel_distributions.argtypes = [C.POINTER(C.c_float), C.c_size_t, C.c_uint32, C.c_double, _D, C.c_size_t,
+                                             _U32, _D, _D, _D, _D]
+        L.qm_pixel_distributions.restype = C.c_int
         L.qm_hour_groups.argtypes = [_D, C.c_size_t, C.c_uint32, C.c_uint32, _U32, _U32, _D, C.POINTER(C.c_size_t)]
         L.qm_hour_groups.restype = C.c_int
         L.qm_distribution_state_means.argtypes = [_D, _D, C.c_size_t, _D, _D]
@@ -551,6 +554,25 @@ def hour_groups(shares, period, runs=0):
                                 abi.ptr(factors, C.c_double), C.byref(n)))
     hours = int(group_hours[:n.value].sum())
     return group_of_slot[:hours].copy(), group_hours[:n.value].copy(), factors[:n.value, :len(sh)].copy()
+
+
+def pixel_distributions(packed, n_layers, bin_db, shares=None, runs=None):
+    """A packed pixel's distributions (qm_pixel_distributions): (layer bins [n_layers][3][n][2],
+    layer silence [n_layers][3], place bins [3][n][2], place silence [3])."""
+    f = np.ascontiguousarray(packed, dtype=np.float32)
+    sh = np.ascontiguousarray(np.zeros((0, 24)) if shares is None else shares, dtype=np.float64).reshape(-1, 24)
+    ru = None if runs is None else np.ascontiguousarray(runs, dtype=np.uint32)
+    n_bins = distribution_bins(bin_db)
+    layer_bins = np.zeros((n_layers, 3, n_bins, 2))
+    layer_silent = np.zeros((n_layers, 3))
+    place_bins = np.zeros((3, n_bins, 2))
+    place_silent = np.zeros(3)
+    _check(lib().qm_pixel_distributions(abi.ptr(f, C.c_float) if len(f) else None, len(f), int(n_layers),
+                                        float(bin_db), abi.ptr(sh, C.c_double) if len(sh) else None, len(sh),
+                                        None if ru is None else abi.ptr(ru, C.c_uint32),
+                                        abi.ptr(layer_bins, C.c_double), abi.ptr(layer_silent, C.c_double),
+                                        abi.ptr(place_bins, C.c_double), abi.ptr(place_silent, C.c_double)))
+    return layer_bins, layer_silent, place_bins, place_silent
 
 
 def distribution_merge_states(lines, spread):

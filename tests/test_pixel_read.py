@@ -107,3 +107,78 @@ def test_malformed_pixels_are_refused():
         assert err.value.status == abi.QM_ERR_CAPACITY
     with pytest.raises(native.QmError):
         native.pixel_read(packed, LAYERS, 3)
+
+
+def _oracle_layers(layers, f32=lambda v: float(np.float32(v))):
+    from oracle import distribution as dist
+
+    out = []
+    for steady, lines in layers:
+        made = []
+        for line in lines:
+            made.append((dist.Line([f32(v) for v in line["energy"]],
+                                   [[f32(v) for v in period] for period in line["means"]],
+                                   [f32(v) for v in line["lambda"]],
+                                   duty=None if line["duty"] is None else [f32(v) for v in line["duty"]],
+                                   passing=None if line["passing"] is None else [f32(v) for v in line["passing"]]),
+                         line["profile"]))
+        out.append(([f32(v) for v in steady], made))
+    return out
+
+
+@pytest.mark.parametrize("runs", [None, (4, 1, 3)])
+def test_a_packed_pixels_distributions_match_the_oracle(runs):
+    """A packed pixel's layers and place, every period, on the map's 2 dB grid, with its profiled
+    roads over the period's hours apart or in the map's groups: equal to the oracle's composition
+    of the same float32 values to the bit (sparse lines' Kurze values included: on these pixels the
+    library's sampler and the oracle's agree exactly)."""
+    from oracle import distribution as dist
+
+    rng = np.random.default_rng(23)
+    shares = rng.uniform(0.3, 9.0, (12, 24))
+    for trial in range(6):
+        layers, curves = _pixel(rng)
+        packed = _pack(layers, curves)
+        got_layers, got_silent, got_place, got_place_silent = native.pixel_distributions(
+            packed, LAYERS, 2.0, shares, None if runs is None else list(runs))
+        made = _oracle_layers(layers)
+        profiled = any(profile is not None for _, lines in made for _, profile in lines)
+        groups = None
+        if profiled:
+            groups = []
+            for p in range(3):
+                slots_of, hours = dist.hour_groups(shares.tolist(), p, None if runs is None else runs[p])
+                parts = []
+                for slots in slots_of:
+                    per_layer = []
+                    for _, lines in made:
+                        if not any(profile is not None for _, profile in lines):
+                            per_layer.append(None)
+                        else:
+                            per_layer.append([1.0 if profile is None else
+                                              dist.group_factor(shares.tolist(), profile, p, slots)
+                                              for _, profile in lines])
+                    parts.append((len(slots), per_layer))
+                groups.append((hours, parts))
+        each, whole = dist.layered_distributions([([line for line, _ in lines], steady) for steady, lines in made],
+                                                 2.0, groups)
+
+        def close(got, silent, want):
+            want_bins = np.array(want.bins).reshape(-1, 2)
+            assert np.array_equal(got, want_bins) and silent == want.silent
+
+        for p in range(3):
+            close(got_place[p], got_place_silent[p], whole[p])
+            for layer in range(LAYERS):
+                close(got_layers[layer, p], got_silent[layer, p], each[layer][p])
+
+
+def test_a_pixel_naming_an_unknown_profile_is_refused():
+    rng = np.random.default_rng(3)
+    layers, curves = _pixel(rng)
+    if not any(line["profile"] is not None for _, lines in layers for line in lines):
+        layers[0][1].append(dict(energy=[1.0] * 3, means=[[1.0] * STATES] * 3, profile=0, duty=None,
+                                 passing=None, **{"lambda": [20.0] * 3}))
+    with pytest.raises(native.QmError) as err:
+        native.pixel_distributions(_pack(layers, curves), LAYERS, 2.0, np.ones((0, 24)), None)
+    assert err.value.status == abi.QM_ERR_ARGUMENT and "profile" in str(err.value)
