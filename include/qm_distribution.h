@@ -147,7 +147,7 @@ qm_status qm_pixel_distributions(const float *packed, size_t n_floats, uint32_t 
 
 /* The same over a period's groups of hours (popup/src/percentiles.rs:88-160 with hour_groups,
  * percentiles/traffic.rs:251-279): a period of `hours` hours whose groups hold group_hours[g]
- * hours each; profiled[k] marks a line that follows an hourly profile and factors[g][n_lines]
+ * hours each, together every hour of the period; profiled[k] marks a line that follows an hourly profile and factors[g][n_lines]
  * its flow in group g against the period's mean (the mean of its profile's hour factors there,
  * which scales its lambda and its means). A layer none of whose lines is profiled is computed
  * once at its mean flow; the others per group, each group weighing its hours' share. The hourly

@@ -180,7 +180,7 @@ qm_status qm_distribution_layers_grouped(double bin_db, const qm_period_line *li
         return qm::set_error(QM_ERR_ARGUMENT, std::string(who) + ": no groups of hours, or null factors");
     uint64_t grouped = 0;
     for (size_t g = 0; g < n_groups; ++g) grouped += group_hours[g];
-    if (hours == 0 || grouped > hours)
+    if (hours == 0 || grouped != hours)
         return qm::set_error(QM_ERR_ARGUMENT, std::string(who) + ": the groups hold " + std::to_string(grouped) +
                                                   " hours of a period of " + std::to_string(hours));
     for (size_t l = 0; l < n_layers; ++l)
