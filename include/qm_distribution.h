@@ -145,6 +145,14 @@ qm_status qm_pixel_distributions(const float *packed, size_t n_floats, uint32_t 
                                  const double *shares, size_t n_profiles, const uint32_t *runs, double *layer_bins,
                                  double *layer_silent, double *place_bins, double *place_silent);
 
+/* A packed pixel's Nden per layer and for the place (popup/src/loudness.rs:179-205
+ * `layers_loudness`, as paint/src/sone.rs:197-215 gathers them): qm_pixel_distributions, then each
+ * layer's distributions on its own curves and the place's on the place's
+ * (curves[n_layers + 1][3][191], each the loudness of that curve's shape at each whole decibel
+ * from -30 dB; a curve without a shape is all 0 and reads 0). ndens[n_layers + 1]. */
+qm_status qm_pixel_ndens(const float *packed, size_t n_floats, uint32_t n_layers, double bin_db, const double *shares,
+                         size_t n_profiles, const uint32_t *runs, const double *curves, double *ndens);
+
 /* The same over a period's groups of hours (popup/src/percentiles.rs:88-160 with hour_groups,
  * percentiles/traffic.rs:251-279): a period of `hours` hours whose groups hold group_hours[g]
  * hours each, together every hour of the period; profiled[k] marks a line that follows an hourly profile and factors[g][n_lines]

@@ -590,6 +590,28 @@ qm_status qm_pixel_distributions(const float *packed, size_t n_floats, uint32_t 
     return QM_OK;
 }
 
+qm_status qm_pixel_ndens(const float *packed, size_t n_floats, uint32_t n_layers, double bin_db, const double *shares,
+                         size_t n_profiles, const uint32_t *runs, const double *curves, double *ndens) {
+    if (curves == nullptr || ndens == nullptr) return qm::set_error(QM_ERR_ARGUMENT, "qm_pixel_ndens: null curves or ndens");
+    int n_bins = 0;
+    const qm_status status = grid("qm_pixel_ndens", bin_db, n_bins);
+    if (status != QM_OK) return status;
+    const size_t bins2 = 2 * (size_t)n_bins, curve = 3 * (size_t)QM_LOUDNESS_CURVE_POINTS;
+    std::vector<double> layer_bins(n_layers * 3 * bins2), layer_silent(n_layers * 3), place_bins(3 * bins2),
+        place_silent(3);
+    const qm_status made = qm_pixel_distributions(packed, n_floats, n_layers, bin_db, shares, n_profiles, runs,
+                                                  layer_bins.data(), layer_silent.data(), place_bins.data(),
+                                                  place_silent.data());
+    if (made != QM_OK) return made;
+    double mean[3];
+    for (uint32_t l = 0; l <= n_layers; ++l) {
+        const double *bins = l < n_layers ? layer_bins.data() + (size_t)l * 3 * bins2 : place_bins.data();
+        const qm_status read = qm_distribution_loudness(bin_db, bins, curves + l * curve, mean, ndens + l);
+        if (read != QM_OK) return read;
+    }
+    return QM_OK;
+}
+
 qm_status qm_distribution_pass_values(double mean, double *values, size_t cap, size_t *n_values) {
     if (n_values == nullptr || (cap > 0 && values == nullptr))
         return qm::set_error(QM_ERR_ARGUMENT, "qm_distribution_pass_values: null values or n_values");

@@ -160,6 +160,9 @@ def lib():
         L.qm_distribution_pass_values.restype = C.c_int
         L.qm_distribution_layers.argtypes = [C.c_double, C.c_void_p, C.c_size_t, _D, C.c_size_t, _D, _D, _D, _D]
         L.qm_distribution_layers.restype = C.c_int
+        L.qm_pixel_ndens.argtypes = [C.POINTER(C.c_float), C.c_size_t, C.c_uint32, C.c_double, _D, C.c_size_t, _U32,
+                                     _D, _D]
+        L.qm_pixel_ndens.restype = C.c_int
         L.qm_pixel_distributions.argtypes = [C.POINTER(C.c_float), C.c_size_t, C.c_uint32, C.c_double, _D, C.c_size_t,
                                              _U32, _D, _D, _D, _D]
         L.qm_pixel_distributions.restype = C.c_int
@@ -573,6 +576,21 @@ def pixel_distributions(packed, n_layers, bin_db, shares=None, runs=None):
                                         abi.ptr(layer_bins, C.c_double), abi.ptr(layer_silent, C.c_double),
                                         abi.ptr(place_bins, C.c_double), abi.ptr(place_silent, C.c_double)))
     return layer_bins, layer_silent, place_bins, place_silent
+
+
+def pixel_ndens(packed, n_layers, bin_db, curves, shares=None, runs=None):
+    """A packed pixel's Nden per layer and for the place (qm_pixel_ndens): curves
+    [n_layers + 1][3][191]."""
+    f = np.ascontiguousarray(packed, dtype=np.float32)
+    sh = np.ascontiguousarray(np.zeros((0, 24)) if shares is None else shares, dtype=np.float64).reshape(-1, 24)
+    ru = None if runs is None else np.ascontiguousarray(runs, dtype=np.uint32)
+    cu = np.ascontiguousarray(curves, dtype=np.float64)
+    out = np.zeros(n_layers + 1)
+    _check(lib().qm_pixel_ndens(abi.ptr(f, C.c_float) if len(f) else None, len(f), int(n_layers), float(bin_db),
+                                abi.ptr(sh, C.c_double) if len(sh) else None, len(sh),
+                                None if ru is None else abi.ptr(ru, C.c_uint32), abi.ptr(cu, C.c_double),
+                                abi.ptr(out, C.c_double)))
+    return out
 
 
 def distribution_merge_states(lines, spread):

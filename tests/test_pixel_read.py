@@ -182,3 +182,46 @@ def test_a_pixel_naming_an_unknown_profile_is_refused():
     with pytest.raises(native.QmError) as err:
         native.pixel_distributions(_pack(layers, curves), LAYERS, 2.0, np.ones((0, 24)), None)
     assert err.value.status == abi.QM_ERR_ARGUMENT and "profile" in str(err.value)
+
+
+def test_a_packed_pixels_ndens_match_the_oracle():
+    """Nden per layer and for the place: each layer's distributions on its own curves, the place's
+    on the place's (curves from the packed shapes, the loudness at each whole decibel by the
+    oracle's Zwicker), equal to the oracle's loudness of its composition to the bit; a layer
+    without a shape reads 0."""
+    from oracle import distribution as dist
+    from oracle import oracle
+
+    rng = np.random.default_rng(29)
+    shares = rng.uniform(0.3, 9.0, (12, 24))
+    layers, curves = _pixel(rng)
+    curves[2] = [None, None, None]
+    packed = _pack(layers, curves)
+    tables = np.zeros((LAYERS + 1, 3, 191))
+    oracle_curves = []
+    for c in range(LAYERS + 1):
+        per_period = []
+        for p in range(3):
+            curve = dist.Curve.__new__(dist.Curve)
+            shape = curves[c][p]
+            if shape is None:
+                curve.table = [0.0] * 191
+            else:
+                shape32 = np.float32(shape).astype(np.float64)
+                curve.table = list(oracle.zwicker_many([shape32 + (-30.0 + step) for step in range(191)]))
+            tables[c, p] = curve.table
+            per_period.append(curve)
+        oracle_curves.append(per_period)
+    got = native.pixel_ndens(packed, LAYERS, 2.0, tables, shares, [4, 1, 3])
+    layer_bins, layer_silent, place_bins, place_silent = native.pixel_distributions(packed, LAYERS, 2.0, shares,
+                                                                                    [4, 1, 3])
+    for c in range(LAYERS + 1):
+        bins = place_bins if c == LAYERS else layer_bins[c]
+        distributions = []
+        for p in range(3):
+            d = dist.Distribution(2.0)
+            d.bins = [list(row) for row in bins[p]]
+            distributions.append(d)
+        _, want = dist.loudness(distributions, oracle_curves[c])
+        assert got[c] == want, c
+    assert got[2] == 0.0 and got[LAYERS] > 0.0
