@@ -389,9 +389,12 @@ qm_status qm_distribution_loudness(double bin_db, const double *bins, const doub
     return QM_OK;
 }
 
-qm_status qm_pixel_read(const float *packed, size_t n_floats, uint32_t n_layers, uint32_t period,
-                        qm_period_line *lines, int32_t *profiles, size_t cap, size_t *n_lines, double *steady,
-                        double *shapes, uint8_t *has_shape) {
+namespace {
+
+// qm_pixel_read without its capacity error: the lines past `cap` are counted, not written.
+qm_status read_pixel(const float *packed, size_t n_floats, uint32_t n_layers, uint32_t period, qm_period_line *lines,
+                     int32_t *profiles, size_t cap, size_t *n_lines, double *steady, double *shapes,
+                     uint8_t *has_shape) {
     if ((n_floats > 0 && packed == nullptr) || n_lines == nullptr || steady == nullptr || shapes == nullptr ||
         has_shape == nullptr || (cap > 0 && (lines == nullptr || profiles == nullptr)))
         return qm::set_error(QM_ERR_ARGUMENT, "qm_pixel_read: null argument");
@@ -441,8 +444,19 @@ qm_status qm_pixel_read(const float *packed, size_t n_floats, uint32_t n_layers,
         return qm::set_error(QM_ERR_ARGUMENT, "qm_pixel_read: " + std::to_string(n_floats - at) +
                                                   " floats left over after the curves");
     *n_lines = count;
-    if (count > cap)
-        return qm::set_error(QM_ERR_CAPACITY, "qm_pixel_read: " + std::to_string(count) + " lines, room for " +
+    return QM_OK;
+}
+
+}  // namespace
+
+qm_status qm_pixel_read(const float *packed, size_t n_floats, uint32_t n_layers, uint32_t period,
+                        qm_period_line *lines, int32_t *profiles, size_t cap, size_t *n_lines, double *steady,
+                        double *shapes, uint8_t *has_shape) {
+    const qm_status status =
+        read_pixel(packed, n_floats, n_layers, period, lines, profiles, cap, n_lines, steady, shapes, has_shape);
+    if (status != QM_OK) return status;
+    if (*n_lines > cap)
+        return qm::set_error(QM_ERR_CAPACITY, "qm_pixel_read: " + std::to_string(*n_lines) + " lines, room for " +
                                                   std::to_string(cap));
     return QM_OK;
 }
@@ -536,9 +550,9 @@ qm_status qm_pixel_distributions(const float *packed, size_t n_floats, uint32_t 
     for (uint32_t period = 0; period < 3; ++period) {
         // The period's lines: counted first, then read.
         size_t n_lines = 0;
-        qm_status read = qm_pixel_read(packed, n_floats, n_layers, period, nullptr, nullptr, 0, &n_lines,
-                                       steady.data(), shapes.data(), has_shape.data());
-        if (read != QM_OK && read != QM_ERR_CAPACITY) return read;
+        qm_status read = read_pixel(packed, n_floats, n_layers, period, nullptr, nullptr, 0, &n_lines, steady.data(),
+                                    shapes.data(), has_shape.data());
+        if (read != QM_OK) return read;
         std::vector<qm_period_line> lines(n_lines);
         std::vector<int32_t> profiles(n_lines);
         read = qm_pixel_read(packed, n_floats, n_layers, period, lines.data(), profiles.data(), n_lines, &n_lines,
