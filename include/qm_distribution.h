@@ -153,6 +153,11 @@ qm_status qm_pixel_distributions(const float *packed, size_t n_floats, uint32_t 
 qm_status qm_pixel_ndens(const float *packed, size_t n_floats, uint32_t n_layers, double bin_db, const double *shares,
                          size_t n_profiles, const uint32_t *runs, const double *curves, double *ndens);
 
+/* Percentiles::of (popup/src/percentiles.rs:284-296): the levels exceeded 5, 10, 50 and 90 % of
+ * each period's time (dB, -inf where silence is), from bins[3][n_bins][2]; levels[4][3] (L5,
+ * L10, L50, L90 by period). */
+qm_status qm_distribution_percentiles(double bin_db, const double *bins, double *levels);
+
 /* The same over a period's groups of hours (popup/src/percentiles.rs:88-160 with hour_groups,
  * percentiles/traffic.rs:251-279): a period of `hours` hours whose groups hold group_hours[g]
  * hours each, together every hour of the period; profiled[k] marks a line that follows an hourly profile and factors[g][n_lines]

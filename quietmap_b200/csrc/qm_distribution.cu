@@ -626,6 +626,19 @@ qm_status qm_pixel_ndens(const float *packed, size_t n_floats, uint32_t n_layers
     return QM_OK;
 }
 
+qm_status qm_distribution_percentiles(double bin_db, const double *bins, double *levels) {
+    int n_bins = 0;
+    const qm_status status = grid("qm_distribution_percentiles", bin_db, n_bins);
+    if (status != QM_OK) return status;
+    if (bins == nullptr || levels == nullptr)
+        return qm::set_error(QM_ERR_ARGUMENT, "qm_distribution_percentiles: null bins or levels");
+    static const double exceeded[4] = {0.05, 0.1, 0.5, 0.9};
+    for (int k = 0; k < 4; ++k)
+        for (int p = 0; p < 3; ++p)
+            levels[k * 3 + p] = qm::dist::exceeded_db(bins + (size_t)p * 2 * n_bins, n_bins, exceeded[k]);
+    return QM_OK;
+}
+
 qm_status qm_distribution_pass_values(double mean, double *values, size_t cap, size_t *n_values) {
     if (n_values == nullptr || (cap > 0 && values == nullptr))
         return qm::set_error(QM_ERR_ARGUMENT, "qm_distribution_pass_values: null values or n_values");

@@ -160,6 +160,8 @@ def lib():
         L.qm_distribution_pass_values.restype = C.c_int
         L.qm_distribution_layers.argtypes = [C.c_double, C.c_void_p, C.c_size_t, _D, C.c_size_t, _D, _D, _D, _D]
         L.qm_distribution_layers.restype = C.c_int
+        L.qm_distribution_percentiles.argtypes = [C.c_double, _D, _D]
+        L.qm_distribution_percentiles.restype = C.c_int
         L.qm_pixel_ndens.argtypes = [C.POINTER(C.c_float), C.c_size_t, C.c_uint32, C.c_double, _D, C.c_size_t, _U32,
                                      _D, _D]
         L.qm_pixel_ndens.restype = C.c_int
@@ -590,6 +592,14 @@ def pixel_ndens(packed, n_layers, bin_db, curves, shares=None, runs=None):
                                 abi.ptr(sh, C.c_double) if len(sh) else None, len(sh),
                                 None if ru is None else abi.ptr(ru, C.c_uint32), abi.ptr(cu, C.c_double),
                                 abi.ptr(out, C.c_double)))
+    return out
+
+
+def distribution_percentiles(bin_db, bins):
+    """L5, L10, L50 and L90 per period (qm_distribution_percentiles): [4][3] dB from bins [3][n][2]."""
+    b = np.ascontiguousarray(bins, dtype=np.float64)
+    out = np.zeros((4, 3))
+    _check(lib().qm_distribution_percentiles(float(bin_db), abi.ptr(b, C.c_double), abi.ptr(out, C.c_double)))
     return out
 
 

@@ -456,3 +456,18 @@ def test_hour_groups_match_the_oracle_and_feed_the_grouped_layers():
             int(dist.PERIOD_HOURS[period]), group_hours, factors[:, [1]], [True])
         assert np.array_equal(got_whole, _bins(whole[period])) and got_silent == whole[period].silent
         assert np.array_equal(got_each[0], _bins(each[0][period]))
+
+
+def test_percentiles_of_a_place():
+    """Percentiles::of (popup/src/percentiles.rs:284-296): the place's levels exceeded 5, 10, 50
+    and 90 % of each period, equal to the oracle's; a silent period reads -inf."""
+    layers = _place(9, sparse=False)
+    _, whole = dist.layered_distributions(layers, 0.5)
+    bins = np.array([_bins(whole[p]) for p in range(3)])
+    got = native.distribution_percentiles(0.5, bins)
+    for k, exceeded in enumerate((0.05, 0.1, 0.5, 0.9)):
+        for p in range(3):
+            assert got[k, p] == whole[p].exceeded_db(exceeded)
+    assert np.all(np.diff(got[:, 0]) <= 0.0), "L5 >= L10 >= L50 >= L90"
+    silent = np.zeros((3, 360, 2))
+    assert np.all(np.isneginf(native.distribution_percentiles(0.5, silent)))
