@@ -135,6 +135,7 @@ def _place_buildings(rng, n, side_m, make, min_gap_m, margin_m):
 
 def _rings_to_arrays(polygons, heights, step_m, first_id=1):
     verts, records = [], []
+    total = 0  # vertices so far: the next ring's first vertex
     for k, (poly, height) in enumerate(zip(polygons, heights)):
         pts = np.round(poly / step_m).astype(np.int64)
         # Counter-clockwise, distinct consecutive vertices, closed by repeating the first.
@@ -150,8 +151,9 @@ def _rings_to_arrays(polygons, heights, step_m, first_id=1):
         if _signed_area2(pts.astype(np.float64)) < 0:
             pts = pts[::-1]
         ring = np.vstack([pts, pts[:1]])
-        records.append((sum(len(v) for v in verts), len(ring), first_id + k, float(height), 1))
+        records.append((total, len(ring), first_id + k, float(height), 1))
         verts.append(ring)
+        total += len(ring)
     vertices = np.vstack(verts).astype(np.int32) if verts else np.zeros((0, 2), np.int32)
     return vertices, _outlines(records)
 
