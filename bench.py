@@ -109,19 +109,7 @@ def workload(name, rank, slices, sources):
     n_src = min(sources, n_all) if sources else n_all
     slices = max(1, slices)
     per = (n_src + slices - 1) // slices
-    tile_w, tile_h = 16, 8
-    rng = np.random.default_rng(1000 + rank)
-    steps = []
-    for t in range(8):
-        tx = int(rng.integers(0, full.nx // tile_w))
-        ty = int(rng.integers(0, full.ny // tile_h))
-        for s in range(slices):
-            b, e = s * per, min((s + 1) * per, n_src)
-            if b >= e:
-                continue
-            steps.append([scenes.Grid(origin=(full.origin[0] + tx * tile_w * full.spacing,
-                                              full.origin[1] + ty * tile_h * full.spacing),
-                                      spacing=full.spacing, nx=tile_w, ny=tile_h, source_begin=b, source_end=e)])
+    steps = [[g] for g in scenes.terrain_tile_steps(full, n_src, seed=1000 + rank, slices=slices)]
     desc = dict(workload=f"terrain square 16 km^2 (2048^2 grid at 1.953 m, fBm DEM, 30,000 buildings, "
                          f"{n_all} point sources from 20,000 road/rail segments, p=0.5): a step is one seeded "
                          f"16x8 receiver tile x one 1/{slices} slice ({per} sources) of the source list",

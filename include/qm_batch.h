@@ -270,9 +270,11 @@ qm_status qm_list_crossings(qm_scene *scene, const int32_t *from_xy, const int32
  * partial sums must fit the array (rejected with QM_ERR_CAPACITY otherwise); paths over the
  * per-path capacities are not re-run (QM_ERR_CAPACITY: use qm_paint_grid). cell_bands, cell_dba
  * and cell_lden are required host outputs; stats->kernel_ms is -1 (not timed). The first call on a
- * device looks up the array's device address with that device current, so make the first call
- * before any stream capture. Every call reuses the one array: calls that overlap on the GPU (from
- * two contexts on one device) race. */
+ * device looks up the array's device address and loads the kernels this entry point launches, with
+ * that device current, so make the first call before any stream capture; the no-allocation promise
+ * holds from the first call's launches on. Receivers are set up on the device by the host set-up's
+ * rules (ground altitude in double, the lowest containing footprint id). Every call reuses the one
+ * array: calls that overlap on the GPU (from two contexts on one device) race. */
 #define QM_STATIC_SCRATCH_BYTES (64u << 20)
 #define QM_STATIC_MAX_CELLS 65536
 #define QM_STATIC_MAX_BINS 4096

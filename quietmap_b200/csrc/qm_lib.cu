@@ -485,9 +485,10 @@ void grid_receivers(const qm_scene *s, const qm_grid_desc *g, std::vector<float>
         int64_t x = g->origin[0] + (int64_t)(c % g->nx) * g->spacing, y = g->origin[1] + (int64_t)(c / g->nx) * g->spacing;
         alt[c] = (float)(terrain_altitude(s, x, y) + g->height_m);
     }
-    // The building a receiver stands in: the lowest footprint id among the rings containing it.
+    // The building a receiver stands in: the lowest footprint id among the rings containing it (a
+    // ring without a footprint id, 0, names no building).
     for (const qm_outline &o : s->outlines) {
-        if (!o.building || o.vertex_count < 4) continue;
+        if (!o.building || o.vertex_count < 4 || o.footprint_id == 0) continue;
         int64_t x0 = INT64_MAX, x1 = INT64_MIN, y0 = INT64_MAX, y1 = INT64_MIN;
         for (uint32_t k = 0; k < o.vertex_count; ++k) {
             int64_t vx = s->vertices[2 * (o.first_vertex + k)], vy = s->vertices[2 * (o.first_vertex + k) + 1];
@@ -1091,13 +1092,30 @@ qm_status static_scratch(int device, unsigned char **out) {
     return QM_OK;
 }
 
+// The ground's altitude at a lattice point in double, by the host's `terrain_altitude` rule and
+// operation for operation (each product and sum rounded on its own, no contraction), so that a
+// receiver set up on the device stands exactly where qm_paint_grid's host set-up puts it.
+__device__ double static_terrain_altitude(const SceneDev &S, long long x, long long y) {
+    if (S.dem_nx == 0) return (double)S.flat_z;
+    double fx = (double)(x - S.dem_ox) / (double)S.dem_sp, fy = (double)(y - S.dem_oy) / (double)S.dem_sp;
+    fx = fmin(fmax(fx, 0.0), (double)(S.dem_nx - 1));
+    fy = fmin(fmax(fy, 0.0), (double)(S.dem_ny - 1));
+    long long i0 = min((long long)floor(fx), (long long)S.dem_nx - 2);
+    long long j0 = min((long long)floor(fy), (long long)S.dem_ny - 2);
+    double ax = __dsub_rn(fx, (double)i0), ay = __dsub_rn(fy, (double)j0);
+    auto node = [&](long long i, long long j) { return (double)S.dem[j * S.dem_nx + i].x; };
+    double lo = __dadd_rn(node(i0, j0), __dmul_rn(ax, __dsub_rn(node(i0 + 1, j0), node(i0, j0))));
+    double hi = __dadd_rn(node(i0, j0 + 1), __dmul_rn(ax, __dsub_rn(node(i0 + 1, j0 + 1), node(i0, j0 + 1))));
+    return __dadd_rn(lo, __dmul_rn(ay, __dsub_rn(hi, lo)));
+}
+
 // Receiver altitude (ground + height) of every grid cell, and UINT_MAX as "no building yet".
 __global__ void static_receivers_kernel(SceneDev S, int ox, int oy, int spacing, int nx, int ny, float height,
                                         float *alt, uint32_t *own) {
     int cell = blockIdx.x * blockDim.x + threadIdx.x;
     if (cell >= nx * ny) return;
-    float2 zg = terrain_point(S, ox + (cell % nx) * spacing, oy + (cell / nx) * spacing);
-    alt[cell] = zg.x + height;
+    double z = static_terrain_altitude(S, ox + (long long)(cell % nx) * spacing, oy + (long long)(cell / nx) * spacing);
+    alt[cell] = (float)__dadd_rn(z, (double)height);
     own[cell] = 0xFFFFFFFFu;
 }
 
@@ -1109,7 +1127,8 @@ __global__ void static_own_kernel(SceneDev S, uint32_t n_outlines, int ox, int o
     uint32_t o = blockIdx.x * blockDim.x + threadIdx.x;
     if (o >= n_outlines) return;
     OutlineDev ol = S.outlines[o];
-    if (!ol.building || ol.count < 4) return;
+    // A ring without a footprint id (dense id 0) names no building, as in the host set-up.
+    if (!ol.building || ol.count < 4 || ol.fp == 0) return;
     long long x0 = LLONG_MAX, x1 = LLONG_MIN, y0 = LLONG_MAX, y1 = LLONG_MIN;
     for (uint32_t k = 0; k < ol.count; ++k) {
         int2 v = S.vertices[ol.first + k];
@@ -1142,6 +1161,32 @@ __global__ void static_own_finish_kernel(uint32_t *own, int cells) {
 
 size_t align256(size_t v) { return (v + 255) & ~size_t(255); }
 
+// Loads every kernel the static painter launches, once per device, with that device current. Under
+// CUDA's lazy module loading a kernel's first launch would otherwise load its code then, which can
+// allocate device memory inside the caller's first paint; loading them here, in the first call's
+// set-up beside the array's address, keeps every later launch free of it.
+bool g_static_loaded[64] = {false};
+qm_status static_load_kernels(int device) {
+    std::lock_guard<std::mutex> guard(g_static_lock);
+    if (g_static_loaded[device]) return QM_OK;
+    cudaFuncAttributes attr;
+    const void *kernels[] = {
+        reinterpret_cast<const void *>(&static_receivers_kernel),
+        reinterpret_cast<const void *>(&static_own_kernel),
+        reinterpret_cast<const void *>(&static_own_finish_kernel),
+        reinterpret_cast<const void *>(&paint_grid_kernel<CapsTerrain>),
+        reinterpret_cast<const void *>(&paint_grid_kernel<CapsFlat>),
+        reinterpret_cast<const void *>(&reduce_cells_kernel),
+    };
+    for (const void *k : kernels) {
+        cudaError_t e = cudaFuncGetAttributes(&attr, k);
+        if (e != cudaSuccess)
+            return fail(QM_ERR_CUDA, std::string("cuda: loading the static painter's kernels: ") + cudaGetErrorString(e));
+    }
+    g_static_loaded[device] = true;
+    return QM_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -1172,6 +1217,8 @@ qm_status qm_paint_grid_static(qm_scene *scene, const qm_grid_desc *grid, float 
     QM_CUDA(cudaSetDevice(ctx->device));
     unsigned char *base = nullptr;
     qm_status st = static_scratch(ctx->device, &base);
+    if (st != QM_OK) return st;
+    st = static_load_kernels(ctx->device);
     if (st != QM_OK) return st;
     cudaStream_t stream = ctx->stream;
     const int cells = g.nx * g.ny;

@@ -297,6 +297,27 @@ def terrain_square(seed=2, scale=1.0, n_segments=20000, n_buildings=30000, side_
     return scene, grid
 
 
+def terrain_tile_steps(full, n_sources, seed=1000, tiles=8, slices=8, tile=(16, 8)):
+    """Seeded receiver tiles of the terrain square's grid, each painted against the source list in
+    `slices` consecutive slices: a list of Grids, tile after tile, slice after slice. Painting the
+    whole square is ~10^13 paths; these tiles are the sample a timing step paints."""
+    tile_w, tile_h = tile
+    per = (n_sources + slices - 1) // slices
+    rng = np.random.default_rng(seed)
+    steps = []
+    for _ in range(tiles):
+        tx = int(rng.integers(0, full.nx // tile_w))
+        ty = int(rng.integers(0, full.ny // tile_h))
+        for s in range(slices):
+            b, e = s * per, min((s + 1) * per, n_sources)
+            if b >= e:
+                continue
+            steps.append(Grid(origin=(full.origin[0] + tx * tile_w * full.spacing,
+                                      full.origin[1] + ty * tile_h * full.spacing),
+                              spacing=full.spacing, nx=tile_w, ny=tile_h, source_begin=b, source_end=e))
+    return steps
+
+
 # ---------------------------------------------------------------------------------------------
 # Aircraft: Doc 29 flights over a receiver grid.
 

@@ -2,7 +2,7 @@
 
 Bars: crossing lists bit-exact (edge ids, chainage t, flags); histogram counts bit-exact given the
 device's own cell levels; cell band levels, dBA and Lden within 0.05 dB of the oracle; Zwicker
-within 0.5 %; per-pair energies within 0.05 dB at the 99th percentile.
+within 0.5 %; per-pair energies within 0.05 dB at the maximum.
 """
 
 import numpy as np
@@ -163,13 +163,14 @@ def _check_pairs(ctx, scene, rng):
     assert np.array_equal(np.isfinite(got), np.isfinite(ref))
     heard = np.isfinite(ref)
     err = np.abs(got[heard] - ref[heard])
-    assert np.percentile(err, 99) < TOL_DB, np.percentile(err, [50, 99, 100])
+    print("pair sums |error| p50, p99, max (dB):", np.percentile(err, [50, 99, 100]))
+    assert err.max() < TOL_DB, np.percentile(err, [50, 99, 100])
     assert np.median(err) < 0.005
     got_p, ref_p = _levels_db(points.astype(np.float64)), _levels_db(ref_points)
     assert np.array_equal(np.isfinite(got_p), np.isfinite(ref_p))
     heard = np.isfinite(ref_p)
     pe = np.abs(got_p[heard] - ref_p[heard])
-    assert np.percentile(pe, 99) < TOL_DB
+    assert pe.max() < TOL_DB, np.percentile(pe, [50, 99, 100])
 
 
 def test_pairs_match_the_oracle_on_the_road_square(ctx, road):

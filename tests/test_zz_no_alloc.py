@@ -79,3 +79,31 @@ def test_static_scratch_painter_rejects_grids_beyond_its_limit():
     assert b"65536" in native.lib().qm_last_error(ctx.handle)
     dev.close()
     ctx.close()
+
+
+def test_static_scratch_painter_sets_up_receivers_as_the_host_does_on_terrain():
+    """On a DEM with grid receivers inside buildings: the device set-up's altitudes and own
+    footprints must be those of qm_paint_grid's host set-up, or the levels would differ (a receiver
+    inside a building hears through its own walls only when it knows them as its own)."""
+    f = _bind()
+    scene, _ = scenes.terrain_square(scale=0.125)
+    # A 32 x 32 grid at 1 m around the first building's first vertex.
+    v = scene.vertices[scene.outlines[0]["first_vertex"]]
+    spacing = int(round(1.0 / scene.step_m))
+    grid = scenes.Grid(origin=(int(v[0]) - 16 * spacing, int(v[1]) - 16 * spacing), spacing=spacing, nx=32, ny=32)
+    ora = oracle.OracleScene(scene)
+    inside = ora.enclosing(grid.receiver_xy())
+    assert np.count_nonzero(inside) > 0
+    ctx = native.Context(0)
+    dev = ctx.scene(scene)
+    ref_bands, ref_dba, ref_lden, _, ref_stats = dev.paint_grid(grid)
+    assert ref_stats["failed_paths"] == 0
+    for _ in range(2):
+        status, bands, dba, lden, hist, stats = _paint_static(f, dev, grid)
+        assert status == abi.QM_OK, native.lib().qm_last_error(ctx.handle)
+        np.testing.assert_allclose(dba, ref_dba, atol=TOL_DB)
+        np.testing.assert_allclose(lden, ref_lden, atol=TOL_DB)
+        ok = np.isfinite(ref_bands)
+        np.testing.assert_allclose(bands[ok], ref_bands[ok], atol=TOL_DB)
+    dev.close()
+    ctx.close()
