@@ -376,6 +376,8 @@ qm_status qm_scene_upload(qm_ctx *ctx, const qm_scene_desc *d, qm_scene **out) {
         cell_ref[i] = make_uint2(en.edge, en.outline);
     }
     for (size_t c = 1; c < cell_start.size(); ++c) cell_start[c] += cell_start[c - 1];
+    std::vector<uint2> cell_range((size_t)cells_x * cells_y);
+    for (size_t c = 0; c < cell_range.size(); ++c) cell_range[c] = make_uint2(cell_start[c], cell_start[c + 1]);
     s->n_edges_listed = entries.size();
     std::vector<OutlineDev> outl(d->n_outlines);
     for (uint32_t o = 0; o < d->n_outlines; ++o) {
@@ -427,7 +429,7 @@ qm_status qm_scene_upload(qm_ctx *ctx, const qm_scene_desc *d, qm_scene **out) {
     dv.cells_x = cells_x;
     dv.cells_y = cells_y;
     qm_status st;
-    if ((st = upload(s, cell_start.data(), cell_start.size(), &dv.cell_start)) != QM_OK ||
+    if ((st = upload(s, cell_range.data(), cell_range.size(), &dv.cell_range)) != QM_OK ||
         (st = upload(s, cell_seg.data(), cell_seg.size(), &dv.cell_seg)) != QM_OK ||
         (st = upload(s, cell_ref.data(), cell_ref.size(), &dv.cell_ref)) != QM_OK ||
         (st = upload(s, reinterpret_cast<const int2 *>(d->vertices), (size_t)d->n_vertices, &dv.vertices)) != QM_OK ||

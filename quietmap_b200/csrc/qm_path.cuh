@@ -37,7 +37,7 @@ static_assert(sizeof(SourceDev) == 128, "SourceDev layout");
 struct SceneDev {
     float step_m;
     int cell_steps, cells_x, cells_y;
-    const uint32_t *cell_start;  // [cells + 1]
+    const uint2 *cell_range;     // [cells]: each cell's first entry and one past its last
     const int4 *cell_seg;        // per entry: the edge's ends (ax, ay, bx, by)
     const uint2 *cell_ref;       // per entry: (edge start vertex, outline)
     const int2 *vertices;
@@ -64,16 +64,19 @@ __device__ __forceinline__ long long floor_div64(long long a, long long b) {
 // ---------------------------------------------------------------------------------------------
 // Crossings
 
-// One crossing: chainage, crossed edge (its first vertex) and the outline index with flags
-// (bit 30 building, bit 31 bounds_roof); footprint and height are read from the outline.
+// One crossing: chainage, crossed edge (its first vertex), the outline index with flags (bit 30
+// building, bit 31 bounds_roof), and the outline's height and dense footprint, copied from the
+// outline when the crossing is listed so that the path's later steps read no outline records.
 struct XRec {
     double t;
     uint32_t edge;
     uint32_t info;
+    float height;
+    uint32_t fp;
 };
 constexpr uint32_t X_OUTLINE = 0x3fffffffu, X_BUILDING = 0x40000000u, X_BOUNDS = 0x80000000u;
 
-__device__ __forceinline__ uint32_t xrec_fp(const SceneDev &S, const XRec &r) { return S.outlines[r.info & X_OUTLINE].fp; }
+__device__ __forceinline__ uint32_t xrec_fp(const SceneDev &, const XRec &r) { return r.fp; }
 
 __device__ __forceinline__ int sgn64(long long v) { return (v > 0) - (v < 0); }
 
@@ -121,62 +124,74 @@ __device__ int list_crossings(const SceneDev &S, int sx, int sy, int rx, int ry,
     const long long adx = dx >= 0 ? dx : -dx, ady = dy >= 0 ? dy : -dy;
     const int minx = min(sx, rx), maxx = max(sx, rx), miny = min(sy, ry), maxy = max(sy, ry);
     int guard = abs(lx - cx) + abs(ly - cy) + 2;
+    // The walk is software-pipelined: the next cell is found and its entry range requested before
+    // the current cell's entries are tested, so the range's load overlaps the tests.
+    auto range_of = [&](int x, int y) {
+        return (x >= 0 && y >= 0 && x < S.cells_x && y < S.cells_y) ? __ldg(S.cell_range + y * S.cells_x + x)
+                                                                    : make_uint2(0u, 0u);
+    };
+    uint2 range = range_of(cx, cy);
     for (; guard > 0; --guard) {
-        if (cx >= 0 && cy >= 0 && cx < S.cells_x && cy < S.cells_y) {
-            int c = cy * S.cells_x + cx;
-            uint32_t b = __ldg(S.cell_start + c), e = __ldg(S.cell_start + c + 1);
-            for (uint32_t k = b; k < e; ++k) {
-                int4 seg = __ldg(S.cell_seg + k);
-                if (max(seg.x, seg.z) < minx || min(seg.x, seg.z) > maxx || max(seg.y, seg.w) < miny ||
-                    min(seg.y, seg.w) > maxy)
-                    continue;
-                ++edges_tested;
-                const int ex = seg.z - seg.x, ey = seg.w - seg.y;
-                long long den = mulw(idx, ey) - mulw(idy, ex);
-                if (den == 0) continue;
-                const int wx = seg.x - sx, wy = seg.y - sy;
-                long long tn = mulw(wx, ey) - mulw(wy, ex);
-                long long un = mulw(wx, idy) - mulw(wy, idx);
-                long long d = den;
-                if (d < 0) {
-                    d = -d;
-                    tn = -tn;
-                    un = -un;
-                }
-                if (!(tn > 0 && tn < d && un >= 0 && un <= d)) continue;
-                if (n >= MAXC) {
-                    status |= FAILED_CAPACITY;
-                    return n;
-                }
-                uint2 ref = __ldg(S.cell_ref + k);
-                OutlineDev o = S.outlines[ref.y];
-                bool building = o.building != 0;
-                // The segment's side of the edge's ends is -un and den - un: when the segment passes
-                // through neither end the hit bounds the roof (edge_bounds_roof's first case), so
-                // the ring is walked only for hits through a vertex.
-                bool bounds = building && ((un != 0 && un != d) || edge_bounds_roof(S, sx, sy, dx, dy, ref.x, o.first, o.count));
-                xs[n++] = XRec{(double)tn / (double)d, ref.x, ref.y | (building ? X_BUILDING : 0u) | (bounds ? X_BOUNDS : 0u)};
+        const bool last = cx == lx && cy == ly;
+        int ncx = cx, ncy = cy;
+        if (!last) {
+            int axis;
+            if (cx == lx)
+                axis = 1;
+            else if (cy == ly)
+                axis = 0;
+            else {
+                int ax_ = (int)(bx - sx), ay_ = (int)(by - sy);
+                if (ax_ < 0) ax_ = -ax_;
+                if (ay_ < 0) ay_ = -ay_;
+                axis = (mulw(ax_, (int)ady) < mulw(ay_, (int)adx)) ? 0 : 1;  // a tie steps the row
+            }
+            if (axis == 0) {
+                ncx += stx;
+                bx += (long long)stx * C;
+            } else {
+                ncy += sty;
+                by += (long long)sty * C;
             }
         }
-        if (cx == lx && cy == ly) break;
-        int axis;
-        if (cx == lx)
-            axis = 1;
-        else if (cy == ly)
-            axis = 0;
-        else {
-            int ax_ = (int)(bx - sx), ay_ = (int)(by - sy);
-            if (ax_ < 0) ax_ = -ax_;
-            if (ay_ < 0) ay_ = -ay_;
-            axis = (mulw(ax_, (int)ady) < mulw(ay_, (int)adx)) ? 0 : 1;  // a tie steps the row
+        const uint2 next_range = last ? make_uint2(0u, 0u) : range_of(ncx, ncy);
+        for (uint32_t k = range.x; k < range.y; ++k) {
+            int4 seg = __ldg(S.cell_seg + k);
+            if (max(seg.x, seg.z) < minx || min(seg.x, seg.z) > maxx || max(seg.y, seg.w) < miny ||
+                min(seg.y, seg.w) > maxy)
+                continue;
+            ++edges_tested;
+            const int ex = seg.z - seg.x, ey = seg.w - seg.y;
+            long long den = mulw(idx, ey) - mulw(idy, ex);
+            if (den == 0) continue;
+            const int wx = seg.x - sx, wy = seg.y - sy;
+            long long tn = mulw(wx, ey) - mulw(wy, ex);
+            long long un = mulw(wx, idy) - mulw(wy, idx);
+            long long d = den;
+            if (d < 0) {
+                d = -d;
+                tn = -tn;
+                un = -un;
+            }
+            if (!(tn > 0 && tn < d && un >= 0 && un <= d)) continue;
+            if (n >= MAXC) {
+                status |= FAILED_CAPACITY;
+                return n;
+            }
+            uint2 ref = __ldg(S.cell_ref + k);
+            OutlineDev o = S.outlines[ref.y];
+            bool building = o.building != 0;
+            // The segment's side of the edge's ends is -un and den - un: when the segment passes
+            // through neither end the hit bounds the roof (edge_bounds_roof's first case), so
+            // the ring is walked only for hits through a vertex.
+            bool bounds = building && ((un != 0 && un != d) || edge_bounds_roof(S, sx, sy, dx, dy, ref.x, o.first, o.count));
+            xs[n++] = XRec{(double)tn / (double)d, ref.x, ref.y | (building ? X_BUILDING : 0u) | (bounds ? X_BOUNDS : 0u),
+                           o.height, o.fp};
         }
-        if (axis == 0) {
-            cx += stx;
-            bx += (long long)stx * C;
-        } else {
-            cy += sty;
-            by += (long long)sty * C;
-        }
+        if (last) break;
+        cx = ncx;
+        cy = ncy;
+        range = next_range;
     }
     // Sort by (t, footprint, edge): the walk's cells come in order, so the list is nearly sorted; an
     // edge listed in several cells appears once per visited cell, its copies side by side after.
@@ -259,36 +274,36 @@ __device__ inline float2 terrain_point(const SceneDev &S, int x, int y) {
     return make_float2(lz + fy * (hz - lz), lg + fy * (hg - lg));
 }
 
-__device__ __forceinline__ float2 dem_node(const SceneDev &S, long long i, long long j) {
+__device__ __forceinline__ float2 dem_node(const SceneDev &S, int i, int j) {
     i = i < 0 ? 0 : (i >= S.dem_nx ? S.dem_nx - 1 : i);
     j = j < 0 ? 0 : (j >= S.dem_ny ? S.dem_ny - 1 : j);
-    return __ldg(S.dem + j * S.dem_nx + i);
+    return __ldg(S.dem + (size_t)j * S.dem_nx + i);
 }
 
 struct TV {
     float x, z, g;
 };
 
-// floor(n / d) for d > 0 from a float estimate corrected exactly (no 64-bit division).
-__device__ __forceinline__ long long floor_div_pos(long long n, long long d) {
-    long long q = (long long)floorf((float)n / (float)d);
-    while (q * d > n) --q;
-    while ((q + 1) * d <= n) ++q;
-    return q;
-}
-
 // The ground profile under a ray (popup/src/scene.rs:242-296 on one metric lattice): the source end,
 // a vertex wherever the ray crosses a DEM row or column line strictly inside, the receiver end.
 // Orders of crossing are decided exactly on integers (a tie takes the row line first); each line
-// vertex's node pair and fraction follow incrementally from exact rationals, without divisions.
+// vertex's node pair and fraction follow incrementally from exact rationals. Every step is additions
+// only: the order test compares running products (steps to the next row line x |dx| against steps
+// to the next column line x |dy|), and a vertex's node index and remainder advance by a fixed
+// quotient and remainder taken once, carrying one when the remainder passes its denominator.
 struct TerrainWalk {
-    long long adx, ady, sp;
+    long long adx, ady;
     long long a_col, a_row;          // steps along x (y) from the source to the next column (row) line
-    long long next_col, next_row;    // line indices ahead
-    long long col_i, col_rem, col_den, col_inc;  // column vertex: node row j0 and remainder (in den units)
-    long long row_i, row_rem, row_den, row_inc;  // row vertex: node column i0 and remainder
+    long long p_col, p_row;          // a_col * ady and a_row * adx: the order of the next two lines
+    long long step_pc, step_pr;      // sp * ady and sp * adx: their increments per line
+    long long sp;
+    long long col_rem, col_den, col_qrem;  // column vertex: remainder of its node row (in den units)
+    long long row_rem, row_den, row_qrem;  // row vertex: remainder of its node column
+    int col_i, row_i;                // node row (column) index of the next column (row) vertex
+    int col_q, row_q;                // whole nodes the index advances per line
+    int next_col, next_row;          // line indices ahead
     int col_step, row_step;
-    float length, inv_adx, inv_ady;
+    float length, inv_adx, inv_ady, inv_col_den, inv_row_den;
     bool dem;
     int stage;  // 0 start, 1 inner, 2 end, 3 done
     float2 start_zg, end_zg;
@@ -309,31 +324,47 @@ struct TerrainWalk {
         bool on_col = fc * sp == rx, on_row = fr * sp == ry;
         col_step = dx > 0 ? 1 : -1;
         row_step = dy > 0 ? 1 : -1;
-        next_col = dx > 0 ? fc + 1 : (on_col ? fc - 1 : fc);
-        next_row = dy > 0 ? fr + 1 : (on_row ? fr - 1 : fr);
-        a_col = dx != 0 ? (next_col * sp - rx) * col_step : -1;
-        a_row = dy != 0 ? (next_row * sp - ry) * row_step : -1;
+        long long nc = dx > 0 ? fc + 1 : (on_col ? fc - 1 : fc);
+        long long nr = dy > 0 ? fr + 1 : (on_row ? fr - 1 : fr);
+        next_col = (int)nc;
+        next_row = (int)nr;
+        a_col = dx != 0 ? (nc * sp - rx) * col_step : -1;
+        a_row = dy != 0 ? (nr * sp - ry) * row_step : -1;
+        p_col = a_col * ady;
+        p_row = a_row * adx;
+        step_pc = sp * ady;
+        step_pr = sp * adx;
         inv_adx = adx ? 1.0f / (float)adx : 0.0f;
         inv_ady = ady ? 1.0f / (float)ady : 0.0f;
         if (dy != 0) {
             // x of the row line's vertex relative to the DEM origin, in units of sp: num / den.
-            long long num = (rx * dy + (next_row * sp - ry) * dx) * row_step;
+            long long num = (rx * dy + (nr * sp - ry) * dx) * row_step;
             row_den = ady * sp;
-            row_inc = sp * dx;  // per row step (both signs folded in)
-            row_i = floor_div64(num, row_den);
-            row_rem = num - row_i * row_den;
+            long long inc = sp * dx;  // per row step (both signs folded in)
+            long long i = floor_div64(num, row_den);
+            row_i = (int)i;
+            row_rem = num - i * row_den;
+            long long q = floor_div64(inc, row_den);
+            row_q = (int)q;
+            row_qrem = inc - q * row_den;
+            inv_row_den = 1.0f / (float)row_den;
         }
         if (dx != 0) {
-            long long num = (ry * dx + (next_col * sp - rx) * dy) * col_step;
+            long long num = (ry * dx + (nc * sp - rx) * dy) * col_step;
             col_den = adx * sp;
-            col_inc = sp * dy;
-            col_i = floor_div64(num, col_den);
-            col_rem = num - col_i * col_den;
+            long long inc = sp * dy;
+            long long i = floor_div64(num, col_den);
+            col_i = (int)i;
+            col_rem = num - i * col_den;
+            long long q = floor_div64(inc, col_den);
+            col_q = (int)q;
+            col_qrem = inc - q * col_den;
+            inv_col_den = 1.0f / (float)col_den;
         }
     }
 
     // The next vertex; false when the walk is done.
-    __device__ bool next(const SceneDev &S, TV &v) {
+    __device__ __forceinline__ bool next(const SceneDev &S, TV &v) {
         if (stage == 0) {
             stage = dem ? 1 : 2;
             v = TV{0.0f, start_zg.x, start_zg.y};
@@ -343,29 +374,35 @@ struct TerrainWalk {
             bool col_ok = adx != 0 && a_col < adx;
             bool row_ok = ady != 0 && a_row < ady;
             if (col_ok || row_ok) {
-                bool take_row = !col_ok || (row_ok && a_row * adx <= a_col * ady);
+                bool take_row = !col_ok || (row_ok && p_row <= p_col);
                 if (take_row) {
                     float t = (float)a_row * inv_ady;
-                    float f = (float)row_rem / (float)row_den;
+                    float f = (float)row_rem * inv_row_den;
                     float2 a = dem_node(S, row_i, next_row), b = dem_node(S, row_i + 1, next_row);
                     v = TV{t * length, a.x + f * (b.x - a.x), a.y + f * (b.y - a.y)};
                     next_row += row_step;
                     a_row += sp;
-                    long long r = row_rem + row_inc;
-                    long long q = floor_div_pos(r, row_den);
-                    row_i += q;
-                    row_rem = r - q * row_den;
+                    p_row += step_pr;
+                    row_i += row_q;
+                    row_rem += row_qrem;
+                    if (row_rem >= row_den) {
+                        row_rem -= row_den;
+                        ++row_i;
+                    }
                 } else {
                     float t = (float)a_col * inv_adx;
-                    float f = (float)col_rem / (float)col_den;
+                    float f = (float)col_rem * inv_col_den;
                     float2 a = dem_node(S, next_col, col_i), b = dem_node(S, next_col, col_i + 1);
                     v = TV{t * length, a.x + f * (b.x - a.x), a.y + f * (b.y - a.y)};
                     next_col += col_step;
                     a_col += sp;
-                    long long r = col_rem + col_inc;
-                    long long q = floor_div_pos(r, col_den);
-                    col_i += q;
-                    col_rem = r - q * col_den;
+                    p_col += step_pc;
+                    col_i += col_q;
+                    col_rem += col_qrem;
+                    if (col_rem >= col_den) {
+                        col_rem -= col_den;
+                        ++col_i;
+                    }
                 }
                 return true;
             }
@@ -705,15 +742,18 @@ __device__ void evaluate_path(const SceneDev &S, const SourceDev &src, int rx, i
         bool open = false;
         PlanePoint best{0.f, 0.f};
         long long at = 0;
+        // The next crossing's place along the ray, kept in a register (infinite past the last).
+        float xc = nx > 0 ? (float)w.xs[0].t * L : INFINITY;
         while (walk.next(S, v)) {
             if (v.x < platform) v.z = fminf(v.z, source_ground);
             // Crossings whose interpolation interval ends here (first vertex with x > crossing x).
-            while (ci < nx && have_prev && (float)w.xs[ci].t * L < v.x) {
-                float xc = (float)w.xs[ci].t * L;
-                float f = v.x > prev.x ? fminf(fmaxf((xc - prev.x) / (v.x - prev.x), 0.f), 1.f) : 0.f;
-                w.tops[ci] = PlanePoint{prev.z + f * (v.z - prev.z), prev.g + f * (v.g - prev.g)};
-                ++ci;
-            }
+            if (have_prev)
+                while (xc < v.x) {
+                    float f = v.x > prev.x ? fminf(fmaxf((xc - prev.x) / (v.x - prev.x), 0.f), 1.f) : 0.f;
+                    w.tops[ci] = PlanePoint{prev.z + f * (v.z - prev.z), prev.g + f * (v.g - prev.g)};
+                    ++ci;
+                    xc = ci < nx ? (float)w.xs[ci].t * L : INFINITY;
+                }
             // crests_of (ray.rs:360-385)
             if (walk.dem) {
                 bool middle = v.x > 300.0f && v.x < L - 300.0f;
@@ -747,8 +787,7 @@ __device__ void evaluate_path(const SceneDev &S, const SourceDev &src, int rx, i
     {
         uint32_t own = src.fp;
         for (int i = 0; i < nx; ++i) {
-            const OutlineDev &o = S.outlines[w.xs[i].info & X_OUTLINE];
-            uint32_t fp = o.fp;
+            const uint32_t fp = w.xs[i].fp;
             bool bounds = (w.xs[i].info & X_BOUNDS) != 0;
             if (own != 0) {
                 // containing_footprints (ray.rs:201-226): the own footprint and every footprint with an
@@ -764,7 +803,7 @@ __device__ void evaluate_path(const SceneDev &S, const SourceDev &src, int rx, i
             }
             float x = (float)w.xs[i].t * L;
             float zt = w.tops[i].x, g = w.tops[i].z;
-            float top = zt + o.height;
+            float top = zt + w.xs[i].height;
             if (bounds) w.hits[nb++] = BuildingHit{fp, x, top, zt, g};
             w.tops[nt++] = PlanePoint{x, top};
         }
@@ -835,28 +874,31 @@ __device__ void evaluate_path(const SceneDev &S, const SourceDev &src, int rx, i
         vprev = tv;
         int ri = 0;
         float covered_to = 0.0f;
-        TV pend[4];
-        int npend = 0, ipend = 0;
+        // The roof being emitted (its four vertices: ground, top, top, ground) and the next roof's
+        // start, kept in registers.
+        Roof roof;
+        int roof_stage = 4;
+        float next_roof_x0 = nr > 0 ? w.roofs[0].x0 : INFINITY;
         bool have_tv = walk.next(S, tv);
         if (have_tv && tv.x < platform) tv.z = fminf(tv.z, source_ground);
         // The next vertex of the vertical profile.
         auto next_vertex = [&](TV &out_v) -> bool {
             for (;;) {
-                if (ipend < npend) {
-                    out_v = pend[ipend++];
+                if (roof_stage < 4) {
+                    const bool first_end = roof_stage < 2, ground = roof_stage == 0 || roof_stage == 3;
+                    out_v = TV{first_end ? roof.x0 : roof.x1,
+                               roof_stage == 0 ? roof.zt0 : roof_stage == 1 ? roof.top0 : roof_stage == 2 ? roof.top1 : roof.zt1,
+                               ground ? (first_end ? roof.g0 : roof.g1) : 0.0f};
+                    ++roof_stage;
                     return true;
                 }
                 if (!have_tv) return false;
-                if (ri < nr && w.roofs[ri].x0 < tv.x) {
-                    const Roof &r = w.roofs[ri];
-                    pend[0] = TV{r.x0, r.zt0, r.g0};
-                    pend[1] = TV{r.x0, r.top0, 0.0f};
-                    pend[2] = TV{r.x1, r.top1, 0.0f};
-                    pend[3] = TV{r.x1, r.zt1, r.g1};
-                    npend = 4;
-                    ipend = 0;
-                    covered_to = r.x1;
+                if (next_roof_x0 < tv.x) {
+                    roof = w.roofs[ri];
+                    roof_stage = 0;
+                    covered_to = roof.x1;
                     ++ri;
+                    next_roof_x0 = ri < nr ? w.roofs[ri].x0 : INFINITY;
                     continue;
                 }
                 TV t = tv;
@@ -888,21 +930,33 @@ __device__ void evaluate_path(const SceneDev &S, const SourceDev &src, int rx, i
             seg_x = vprev.x;
             seg_z = vprev.z;
         };
+        // The next crest and the next top strictly inside (0, L), kept in registers.
         int ik = 0, it = 0;
-        for (;;) {
-            // Next candidate strictly inside (0, L), terrain first at equal x.
-            while (ik < nk && !(w.crests[ik].x > 0.0f && w.crests[ik].x < L)) ++ik;
-            while (it < nt && !(w.tops[it].x > 0.0f && w.tops[it].x < L)) ++it;
-            PlanePoint c;
-            if (ik < nk && it < nt) {
-                if (w.tops[it].x < w.crests[ik].x)
-                    c = w.tops[it++];
-                else
-                    c = w.crests[ik++];
-            } else if (ik < nk) {
+        auto next_crest = [&](PlanePoint &c) -> bool {
+            while (ik < nk) {
                 c = w.crests[ik++];
-            } else if (it < nt) {
+                if (c.x > 0.0f && c.x < L) return true;
+            }
+            return false;
+        };
+        auto next_top = [&](PlanePoint &c) -> bool {
+            while (it < nt) {
                 c = w.tops[it++];
+                if (c.x > 0.0f && c.x < L) return true;
+            }
+            return false;
+        };
+        PlanePoint crest_c, top_c;
+        bool have_crest = next_crest(crest_c), have_top = next_top(top_c);
+        for (;;) {
+            // Next candidate, terrain first at equal x.
+            PlanePoint c;
+            if (have_crest && (!have_top || !(top_c.x < crest_c.x))) {
+                c = crest_c;
+                have_crest = next_crest(crest_c);
+            } else if (have_top) {
+                c = top_c;
+                have_top = next_top(top_c);
             } else {
                 break;
             }
