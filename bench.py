@@ -29,7 +29,6 @@ tiles with no exchange) and rank 0 prints the JSON line with the max time over r
 import argparse
 import json
 import os
-import re
 import subprocess
 import sys
 import threading
@@ -71,6 +70,10 @@ def parse():
     ap.add_argument("--sources", type=int, default=0,
                     help="paint only the first N sources (a small case for profiling; 0: all)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-surrogate", action="store_true",
+                    help="terrain: leave out the surrogate leg (its training launches many kernels)")
+    ap.add_argument("--oracle-cells", type=int, default=32,
+                    help="terrain: cells of the timed steps checked against the FP64 oracle")
     return ap.parse_args()
 
 
@@ -171,57 +174,78 @@ def measured_peaks():
         return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "source": "fallback"}
 
 
-def profile_figure(name, key):
-    """A figure (`key = value`) from a committed ncu summary under profiles/, or None."""
-    try:
-        with open(os.path.join(ROOT, "profiles", name)) as f:
-            for line in f:
-                m = re.match(rf"\s*[-*]?\s*`?{re.escape(key)}`?\s*=\s*([0-9.eE+-]+)", line)
-                if m:
-                    return float(m.group(1))
-    except OSError:
-        pass
-    return None
+# DRAM bytes per path of the painting kernel, from one ncu capture of this build's kernel on a
+# small case of the workload (dram__bytes_read.sum + dram__bytes_write.sum over its paths), scaled
+# by paths to a full launch; the capture's command and figures are in
+# profiles/paint_grid_kernel_terrain.md. None where no capture of the current kernel exists.
+DRAM_BYTES_PER_PATH = {"terrain": None, "road": None}
 
 
-def cpu_sample(scene, g0, seconds):
-    """Grows a sample (receivers of the first tile x a prefix of the sources) until the oracle
-    takes about `seconds` on all host threads; returns (receivers, sources)."""
+def stratified_sources(grid, m, seed):
+    """`m` source indices spread evenly over the grid's source range from a seeded offset: every
+    part of the slice is sampled, near and far sources alike."""
+    n = grid.source_end - grid.source_begin
+    u = np.random.default_rng(seed).uniform()
+    return grid.source_begin + np.minimum(((np.arange(m) + u) * (n / m)).astype(np.int64), n - 1)
+
+
+def cpu_sample(scene, g, seconds, seed=17):
+    """The oracle's bounded sample of a timed step: the step's receivers (its whole tile) against a
+    stratified, seeded subsample of the step's source slice, grown until the oracle takes about
+    `seconds` on all host threads. Returns (oracle scene, grid, sources sampled, threads)."""
+    from dataclasses import replace
     from oracle import oracle
-    from quietmap_b200 import scenes
-    ora = oracle.OracleScene(scene)
     threads = oracle.threads()
-    k = max(1, min(threads, 16))
-    n = 500
+    n_slice = g.source_end - g.source_begin
+
+    def sub(m):
+        idx = stratified_sources(g, m, seed)
+        return oracle.OracleScene(replace(scene, sources=scene.sources[idx])), replace(g, source_begin=0,
+                                                                                     source_end=len(idx)), idx
+    m = 64
     while True:
-        grid = scenes.Grid(origin=g0.origin, spacing=g0.spacing, nx=k, ny=1, source_begin=0,
-                           source_end=min(n, len(scene.sources)))
+        ora, grid, _ = sub(m)
         t0 = time.perf_counter()
         ora.paint_grid(grid, nthreads=threads)
         dt = time.perf_counter() - t0
-        if dt > seconds / 3 or n >= len(scene.sources):
+        if dt > seconds / 4 or m >= n_slice:
             break
-        n = min(int(n * max(2.0, seconds / 3 / max(dt, 1e-3))), len(scene.sources))
-    n = min(len(scene.sources), max(1, int(n * seconds / max(dt, 1e-3))))
-    return ora, k, n, threads
+        m = min(int(m * max(2.0, seconds / 4 / max(dt, 1e-3))), n_slice)
+    m = min(n_slice, max(1, int(m * seconds / max(dt, 1e-3))))
+    ora, grid, idx = sub(m)
+    return ora, grid, idx, threads
 
 
-def cpu_run(ora, g0, k, n, threads):
-    from quietmap_b200 import scenes
-    grid = scenes.Grid(origin=g0.origin, spacing=g0.spacing, nx=k, ny=1, source_begin=0, source_end=n)
+def cpu_run(ora, grid, threads):
     t0 = time.perf_counter()
     ora.paint_grid(grid, nthreads=threads)
     return time.perf_counter() - t0
 
 
-def cpu_baseline(scene, steps, seconds=12.0):
-    """The FP64 oracle on all host threads: paths/s on a bounded sample of the workload."""
-    g0 = steps[0][0]
-    ora, k, n, threads = cpu_sample(scene, g0, seconds)
-    dt = cpu_run(ora, g0, k, n, threads)
-    return dict(value=k * n / dt, unit="paths/s", cores=threads, kind="port",
-                sample=f"{k} receivers of the first tile x the first {n} point sources ({k * n} paths, "
-                       f"{dt:.1f} s)")
+def cpu_work(ora, scene, grid, idx, n_pairs=256, seed=19):
+    """The oracle's work per path on a seeded subset of the sample's pairs: crossings, profile
+    vertices and diffraction candidates (qmo_path_counts)."""
+    rng = np.random.default_rng(seed)
+    cells = rng.integers(0, grid.cells, n_pairs)
+    srcs = rng.integers(0, len(idx), n_pairs)
+    rxy = grid.receiver_xy()[cells]
+    sxy = np.stack([scene.sources["x"][idx[srcs]], scene.sources["y"][idx[srcs]]], axis=1)
+    counts = ora.path_counts(sxy, rxy)
+    return {"crossings": float(counts[:, 0].mean()), "vertices": float(counts[:, 1].mean()),
+            "candidates": float(counts[:, 2].mean()), "pairs_counted": n_pairs}
+
+
+def cpu_description(grid, g, idx, dt):
+    return (f"the first timed step's {grid.cells} receivers x {len(idx)} of its {g.source_end - g.source_begin} "
+            f"sources (stratified, seeded) = {grid.cells * len(idx)} paths, {dt:.1f} s")
+
+
+def cpu_baseline(scene, g, seconds=12.0):
+    """The FP64 oracle on all host threads: paths/s on a bounded sample of a timed step."""
+    ora, grid, idx, threads = cpu_sample(scene, g, seconds)
+    dt = cpu_run(ora, grid, threads)
+    return dict(value=grid.cells * len(idx) / dt, unit="paths/s", cores=threads, kind="port",
+                sample=cpu_description(grid, g, idx, dt), per_path=cpu_work(ora, scene, grid, idx))
 
 
 def algorithmic_bytes(scene, grid, n_src):
@@ -264,20 +288,23 @@ def main():
     flush = torch.empty(64 << 20, dtype=torch.float32, device="cuda")  # 256 MB > 126 MB L2
 
     work = dict(paths=0, edge_tests=0, vertices=0, candidates=0, crossings=0, failed_paths=0)
-    timing = dict(kernel_ms=0.0, paint_ms=0.0, wall_s=0.0, launches=0, paint_launches=0, alg_bytes=0)
+    timing = dict(kernel_ms=0.0, paint_ms=0.0, wall_s=0.0, launches=0, paint_launches=0, alg_bytes=0, paths_timed=0)
+    timed_dba = {}  # step index -> the exact painter's cell dBA (the surrogate leg compares with it)
 
     def step(i):
         for g in steps[i % len(steps)]:
             flush.zero_()
             torch.cuda.synchronize()
             t0 = time.perf_counter()
-            _, _, _, _, st = dev.paint_grid(g)
+            _, dba, _, _, st = dev.paint_grid(g)
+            timed_dba[i] = dba
             timing["wall_s"] += time.perf_counter() - t0
             timing["kernel_ms"] += st["kernel_ms"]
             timing["paint_ms"] += st["paint_ms"]
             timing["launches"] += 2 + (2 if st["failed_paths"] else 0)
             timing["paint_launches"] += 1
             timing["alg_bytes"] += algorithmic_bytes(scene, g, g.source_end - g.source_begin)
+            timing["paths_timed"] += st["paths"]
             for k in work:
                 work[k] += st[k]
 
@@ -311,7 +338,7 @@ def main():
         achieved = ops / paint_s / 1e12 if paint_s > 0 else None
         sfu_peak = SM_COUNT * MUFU_LANES * NOMINAL_SM_MHZ * 1e6
         caps = "terrain" if args.workload == "terrain" else "road"
-        traffic_per_path = profile_figure(f"paint_grid_kernel_{caps}.md", "dram_bytes_per_path")
+        traffic_per_path = DRAM_BYTES_PER_PATH.get(caps)
         hbm_peak = peaks.get("hbm_gbs")
         alg_gbs = timing["alg_bytes"] / paint_s / 1e9 if paint_s > 0 else None
         line = {
@@ -364,12 +391,106 @@ def main():
             "failed_paths_rerun": work["failed_paths"],
         }
         if not args.no_cpu_baseline and world == 1:
-            line["cpu_baseline"] = cpu_baseline(scene, steps)
+            line["cpu_baseline"] = cpu_baseline(scene, steps[args.warmup % len(steps)][0])
+    if args.workload == "terrain" and not args.no_surrogate and world == 1:
+        sur = surrogate_leg(args, ctx, dev, scene, steps, timed_dba, timing, flush, rank)
+        if rank == 0:
+            line["surrogate"] = sur
+    if rank == 0:
         print(json.dumps(line), flush=True)
     dev.close()
     ctx.close()
     if world > 1:
         torch.distributed.destroy_process_group()
+
+
+def oracle_cells(scene, jobs, threads):
+    """The FP64 oracle's dBA of each (grid, cell) job, one host thread a cell (the oracle's calls
+    release the GIL), all threads busy."""
+    from concurrent.futures import ThreadPoolExecutor
+    from oracle import oracle
+    ora = oracle.OracleScene(scene)
+
+    def one(job):
+        g, c = job
+        e, _, _ = ora.paint_grid(g, c, c + 1, nthreads=1)
+        return 10.0 * np.log10(e[0].sum())
+    with ThreadPoolExecutor(max_workers=threads) as pool:
+        return np.array(list(pool.map(one, jobs)))
+
+
+def surrogate_leg(args, ctx, dev, scene, steps, exact_dba, timing, flush, rank):
+    """The learned surrogate on the same timed steps as the exact painter. The network is trained
+    first (untimed): exact paths of 12 coarse receiver grids x 25,000-source slices (80 M rows, two
+    per path), paths shorter than 200 m left to the exact path. Its painting is timed on the same
+    steps (L2 flushed before each); its speed-up is against the exact painter's time on those
+    steps. Seeded cells of the timed steps are checked against the FP64 oracle, for the surrogate
+    and for the exact painter alike."""
+    import torch
+    from oracle import oracle
+    from quietmap_b200 import native, scenes
+    ns = len(scene.sources)
+    spacing = steps[0][0].spacing
+    cells = steps[0][0].cells
+    grids = [scenes.Grid(origin=(spacing // 2 + 131 * k, spacing // 2 + 257 * k), spacing=spacing * 128, nx=16, ny=16,
+                         source_begin=(k * 331_001) % (ns - 25_000), source_end=(k * 331_001) % (ns - 25_000) + 25_000)
+             for k in range(12)]
+    net = native.Surrogate(ctx, seed=1)
+    exact_within_m = 200.0
+    t0 = time.perf_counter()
+    hist, n_train = net.train(dev, grids, epochs=6, batch=16384, learning_rate=2e-3, seed=3, max_samples=80_000_000,
+                              exact_within_m=exact_within_m)
+    train_s = time.perf_counter() - t0
+    for i in range(args.warmup):
+        dev.paint_grid_surrogate(steps[i % len(steps)][0], net)
+    s_ms = 0.0
+    paths = taken = 0
+    sur_dba = {}
+    torch.cuda.synchronize()
+    with ClockSampler(0) as clocks:
+        for i in range(args.steps):
+            g = steps[(args.warmup + i) % len(steps)][0]
+            flush.zero_()
+            torch.cuda.synchronize()
+            _, dba, _, _, st = dev.paint_grid_surrogate(g, net)
+            s_ms += st["kernel_ms"]
+            paths += st["paths"]
+            taken += st["surrogate_paths"]
+            sur_dba[args.warmup + i] = dba
+    net.close()
+    # Against the exact painter on every timed cell.
+    vs_exact = np.concatenate([np.abs(sur_dba[k] - exact_dba[k]) for k in sur_dba])
+    # Against the FP64 oracle on seeded cells of the timed steps.
+    rng = np.random.default_rng(23)
+    keys = sorted(sur_dba)
+    jobs, picks = [], []
+    for j in range(args.oracle_cells):
+        k = keys[j % len(keys)]
+        c = int(rng.integers(0, cells))
+        jobs.append((steps[k % len(steps)][0], c))
+        picks.append((k, c))
+    t0 = time.perf_counter()
+    ref = oracle_cells(scene, jobs, oracle.threads())
+    oracle_s = time.perf_counter() - t0
+    sur_err = np.abs(np.array([sur_dba[k][c] for k, c in picks]) - ref)
+    exa_err = np.abs(np.array([exact_dba[k][c] for k, c in picks]) - ref)
+    exact_paths_per_s = timing["paths_timed"] / (timing["kernel_ms"] / 1e3)
+    value = paths / (s_ms / 1e3)
+
+    def stats(e):
+        return {"p50": float(np.percentile(e, 50)), "p99": float(np.percentile(e, 99)), "max": float(e.max())}
+    return {
+        "value": value, "unit": "paths/s", "exact_value": exact_paths_per_s, "speedup_vs_exact": value / exact_paths_per_s,
+        "ms_per_step": s_ms / args.steps, "surrogate_share": taken / max(paths, 1),
+        "dtype": "bf16 network (fp32 accumulate, tcgen05), f32 path code",
+        "cell_dba_error_vs_oracle_db": dict(stats(sur_err), cells=len(sur_err)),
+        "exact_cell_dba_error_vs_oracle_db": dict(stats(exa_err), cells=len(exa_err)),
+        "cell_dba_error_vs_exact_db": dict(stats(vs_exact), cells=int(vs_exact.size)),
+        "oracle_seconds": oracle_s,
+        "training": {"samples": int(n_train), "epochs": 6, "seconds": train_s, "loss": [float(v) for v in hist],
+                     "exact_within_m": exact_within_m},
+        "clocks": clocks.summary(),
+    }
 
 
 # Doc 29 operation model per (cell, segment) pair in reach: about 150 FP32 operations and 10 SFU
@@ -665,26 +786,30 @@ def tile_batch(args, rank, world, local):
 
 
 def reference_arm(args, rank, world):
-    """The reference's CPU path (its FP64 restatement) on all host threads, rank 0 only."""
+    """The reference's CPU path (its FP64 restatement) on all host threads, rank 0 only, on the
+    same workload and the same sample rule as the GPU arm's CPU baseline: the receivers of the GPU
+    arm's first timed step against a stratified, seeded subsample of that step's source slice."""
     if rank != 0:
         if world > 1:
             import torch.distributed as tdist
             tdist.destroy_process_group()
         return
-    workload_name = "terrain" if args.workload == "flights" else args.workload
+    workload_name = "terrain" if args.workload not in ("terrain", "road") else args.workload
     scene, steps, desc = workload(workload_name, 0, args.slices, args.sources)
-    g0 = steps[0][0]
+    g = steps[args.warmup % len(steps)][0]
     # Warm-up: the sample is sized here (untimed), then each timed step runs it once.
-    ora, k, n, threads = cpu_sample(scene, g0, seconds=8.0)
-    samples = [k * n / cpu_run(ora, g0, k, n, threads) for _ in range(max(args.steps, 1))]
-    value = float(np.median(samples))
+    ora, grid, idx, threads = cpu_sample(scene, g, seconds=8.0)
+    times = [cpu_run(ora, grid, threads) for _ in range(max(args.steps, 1))]
+    dt = float(np.median(times))
+    value = grid.cells * len(idx) / dt
     line = {
         "metric": METRIC, "value": value, "unit": "paths/s", "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": k * n / value * 1e3, "higher_is_better": True, "scaling": "weak",
+        "warmup": args.warmup, "ms_per_step": dt * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generator of the workload's geometry)",
         "config": dict(desc, parallelism="host threads"), "impl": "reference",
         "cpu_baseline": dict(value=value, unit="paths/s", cores=threads, kind="port",
-                             sample=f"{k} receivers of the first tile x the first {n} point sources per step"),
+                             sample=cpu_description(grid, g, idx, dt) + " per step"),
+        "per_path": cpu_work(ora, scene, grid, idx),
         "e2e": {"value": value, "unit": "paths/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)

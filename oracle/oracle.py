@@ -58,6 +58,8 @@ def lib():
         L.qmo_profile.restype = C.c_size_t
         L.qmo_evaluate_pairs.argtypes = [C.c_void_p, _I64, _D, _U64, _U32, C.c_size_t, _U32, _U32, _D,
                                          C.c_size_t, _D, _D, _D, C.c_size_t, C.c_int]
+        L.qmo_path_counts.argtypes = [C.c_void_p, _I64, _I64, _D]
+        L.qmo_path_counts.restype = None
         L.qmo_paint_grid.argtypes = [C.c_void_p, C.POINTER(abi.GridDesc), C.c_uint32, C.c_uint32, _D, _D,
                                      C.c_int, _U64]
         L.qmo_zwicker.argtypes = [_D]
@@ -343,6 +345,18 @@ class OracleScene:
                                  abi.ptr(sums, C.c_double), abi.ptr(bands, C.c_double), abi.ptr(points, C.c_double),
                                  n_points, nthreads or threads())
         return sums, bands, points
+
+    def path_counts(self, frm, to):
+        """Work counts of each pair's path [n][7]: crossings, profile vertices, diffraction
+        candidates, and per state (homogeneous, favourable) the blocking candidates and hull
+        points (receiver 4 m above its ground, source 0.05 m above its own)."""
+        frm = np.ascontiguousarray(np.asarray(frm).reshape(-1, 2), dtype=np.int64)
+        to = np.ascontiguousarray(np.asarray(to).reshape(-1, 2), dtype=np.int64)
+        out = np.zeros((len(frm), 7))
+        f = lib().qmo_path_counts
+        for k in range(len(frm)):
+            f(self.handle, abi.ptr(frm[k], C.c_int64), abi.ptr(to[k], C.c_int64), abi.ptr(out[k], C.c_double))
+        return out
 
     def paint_grid(self, grid, cell_begin=0, cell_end=0, nthreads=None):
         """Per cell (of [cell_begin, cell_end), all when empty) the day band energies [n][8],

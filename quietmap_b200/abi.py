@@ -1,7 +1,7 @@
 """ctypes mirror of include/qm_batch.h: the structs and constants of the C ABI.
 
-The Rust painter binds the same structs through its FFI; this module is the
-Python binding used by the host mirror of `paint::exact::Batch`, the tests and the benchmark.
+A Rust painter binds the same structs through its own FFI declarations; this module is the Python
+binding used by the host mirror of `paint::exact::Batch`, the tests and the benchmark.
 """
 
 import ctypes as C

@@ -9,6 +9,7 @@
 #include <cstdint>
 
 #include "../../include/qm_aircraft.h"
+#include "qm_stage.cuh"
 
 namespace qm {
 
@@ -53,41 +54,6 @@ constexpr int AC_THREADS = 256;
 __constant__ float LOG10_NPD_FT[10] = {2.3010299956639813f, 2.6020599913279625f, 2.7993405494535817f, 3.0f,
                                     3.3010299956639813f, 3.6020599913279625f, 3.7993405494535817f, 4.0f,
                                     4.2041199826559246f, 4.3979400086720376f};
-
-__device__ __forceinline__ void mbar_init(uint64_t *bar, unsigned count) {
-    unsigned a = (unsigned)__cvta_generic_to_shared(bar);
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(a), "r"(count));
-}
-
-__device__ __forceinline__ void bulk_load(void *dst, const void *src, unsigned bytes, uint64_t *bar) {
-    unsigned d = (unsigned)__cvta_generic_to_shared(dst), b = (unsigned)__cvta_generic_to_shared(bar);
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(b), "r"(bytes) : "memory");
-    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(d),
-                 "l"(src), "r"(bytes), "r"(b)
-                 : "memory");
-}
-
-__device__ __forceinline__ uint64_t global_ns() {
-    uint64_t t;
-    asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
-    return t;
-}
-
-// Waits for the barrier's phase for at most about a second; false when it gave up.
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, unsigned phase) {
-    unsigned b = (unsigned)__cvta_generic_to_shared(bar);
-    const uint64_t start = global_ns();
-    for (;;) {
-        unsigned done;
-        asm volatile(
-            "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2; selp.u32 %0, 1, 0, p; }"
-            : "=r"(done)
-            : "r"(b), "r"(phase)
-            : "memory");
-        if (done) return true;
-        if (global_ns() - start > 1000000000ull) return false;
-    }
-}
 
 // What a segment contributes at every receiver, worked out once per tile by one thread a segment:
 // its start, direction and lengths, the lower power row and the lerp weight, and the speed

@@ -103,11 +103,16 @@ __device__ __forceinline__ int2 tile_slot(int tile_w, int tile_h) {
 #endif
 
 // Thread = one receiver of a tile; CTA = (receiver tile, source chunk). Each thread walks its chunk
-// of sources and keeps its cell's band energies in compensated registers; one store per cell.
+// of sources and keeps its cell's band energies in compensated registers; one store per cell. The
+// warp lists the crossings of its 32 rays to each source together (warp_list_crossings: the
+// obstacle entries staged in shared memory by bulk copies); each lane then follows its own path.
 template <class Caps>
 __global__ void __launch_bounds__(128, QM_PAINT_MIN_BLOCKS) paint_grid_kernel(SceneDev S, GridArgs A) {
     __shared__ unsigned long long s_counts[6];
+    __shared__ CrossStage s_stage[4];
     if (threadIdx.x < 6) s_counts[threadIdx.x] = 0;
+    CrossStage &stage = s_stage[threadIdx.x >> 5];
+    stage_init(stage);
     __syncthreads();
     const int tiles_x = (A.nx + A.tile_w - 1) / A.tile_w;
     const int tile = blockIdx.x;
@@ -124,35 +129,47 @@ __global__ void __launch_bounds__(128, QM_PAINT_MIN_BLOCKS) paint_grid_kernel(Sc
     for (int b = 0; b < QM_BANDS; ++b) bands[b] = KSum{0.f, 0.f};
     uint32_t failed = 0;
     unsigned long long paths = 0, crossings = 0, tested = 0, failed_paths = 0, vertices = 0, candidates = 0;
-    if (active) {
-        const int rx = A.origin_x + ix * A.spacing, ry = A.origin_y + iy * A.spacing;
-        const float alt = A.rcv_alt[cell];
-        const uint32_t own = A.rcv_own[cell];
-        PathWork<Caps::C, Caps::K, Caps::H> work;
-        const uint32_t s0 = A.source_begin + chunk * A.chunk;
-        const uint32_t s1 = min(s0 + A.chunk, A.source_end);
-        for (uint32_t s = s0; s < s1; ++s) {
-            const SourceDev &src = S.sources[s];
-            PathResult r;
-            evaluate_path<Caps::C, Caps::K, Caps::H>(S, src, rx, ry, alt, own, A.want_fav, work, r);
-            ++paths;
-            crossings += r.crossings;
-            tested += r.edges_tested;
-            vertices += r.vertices;
-            candidates += r.candidates;
-            if (r.status) {
-                failed |= r.status;
-                ++failed_paths;
-                unsigned int slot = atomicAdd(A.retry_count, 1u);
-                if (slot < A.retry_cap) A.retry[slot] = make_uint2((uint32_t)cell, s);
-                continue;
-            }
-            float day[QM_BANDS], le;
-            path_energies(S, r, src, A.lden_w, day, le);
-#pragma unroll
-            for (int b = 0; b < QM_BANDS; ++b) bands[b].add(day[b]);
-            lden.add(le);
+    const int rx = A.origin_x + ix * A.spacing, ry = A.origin_y + iy * A.spacing;
+    const float alt = active ? A.rcv_alt[cell] : 0.0f;
+    const uint32_t own = active ? A.rcv_own[cell] : 0u;
+    PathWork<Caps::C, Caps::K, Caps::H> work;
+    StageState ss{0u, false};
+    const uint32_t s0 = A.source_begin + chunk * A.chunk;
+    const uint32_t s1 = min(s0 + A.chunk, A.source_end);
+    for (uint32_t s = s0; s < s1; ++s) {
+        const SourceDev &src = S.sources[s];
+        PathResult r;
+        r.status = 0;
+        r.edges_tested = 0;
+        const int nx = warp_list_crossings<Caps::C>(S, stage, ss, src.x, src.y, rx, ry, active, own, work.xs, r.status,
+                                                    r.edges_tested);
+        if (!active) continue;
+        if (r.status == 0) {
+            evaluate_listed<Caps::C, Caps::K, Caps::H>(S, src, rx, ry, alt, A.want_fav, work, nx, r);
+        } else {
+            r.crossings = nx;
+            r.vertices = 0;
+            r.candidates = 0;
         }
+        ++paths;
+        crossings += r.crossings;
+        tested += r.edges_tested;
+        vertices += r.vertices;
+        candidates += r.candidates;
+        if (r.status) {
+            failed |= r.status;
+            ++failed_paths;
+            unsigned int slot = atomicAdd(A.retry_count, 1u);
+            if (slot < A.retry_cap) A.retry[slot] = make_uint2((uint32_t)cell, s);
+            continue;
+        }
+        float day[QM_BANDS], le;
+        path_energies(S, r, src, A.lden_w, day, le);
+#pragma unroll
+        for (int b = 0; b < QM_BANDS; ++b) bands[b].add(day[b]);
+        lden.add(le);
+    }
+    if (active) {
         float *out = A.partial + ((size_t)chunk * (A.nx * A.ny) + cell) * GRID_SLOTS;
 #pragma unroll
         for (int b = 0; b < QM_BANDS; ++b) out[b] = bands[b].value();

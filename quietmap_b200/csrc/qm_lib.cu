@@ -378,6 +378,32 @@ qm_status qm_scene_upload(qm_ctx *ctx, const qm_scene_desc *d, qm_scene **out) {
     for (size_t c = 1; c < cell_start.size(); ++c) cell_start[c] += cell_start[c - 1];
     std::vector<uint2> cell_range((size_t)cells_x * cells_y);
     for (size_t c = 0; c < cell_range.size(); ++c) cell_range[c] = make_uint2(cell_start[c], cell_start[c + 1]);
+    // The same entries column by column (cell (cx, cy) at cx * cells_y + cy), each cell's entries
+    // in the row-ordered copy's order.
+    std::vector<uint32_t> col_order(entries.size());
+    for (size_t i = 0; i < col_order.size(); ++i) col_order[i] = (uint32_t)i;
+    auto col_key = [&](uint32_t i) {
+        const uint32_t c = entries[i].cell;
+        return (uint64_t)(c % (uint32_t)cells_x) * (uint64_t)cells_y + c / (uint32_t)cells_x;
+    };
+    std::stable_sort(col_order.begin(), col_order.end(), [&](uint32_t a, uint32_t b) { return col_key(a) < col_key(b); });
+    std::vector<int4> col_seg(entries.size());
+    std::vector<uint2> col_ref(entries.size());
+    std::vector<uint2> col_range((size_t)cells_x * cells_y, make_uint2(0u, 0u));
+    for (size_t k = 0; k < col_order.size(); ++k) {
+        const uint32_t i = col_order[k];
+        col_seg[k] = cell_seg[i];
+        col_ref[k] = cell_ref[i];
+    }
+    {
+        // Each column-ordered cell's range; empty cells start where the next entries do.
+        size_t k = 0;
+        for (uint64_t key = 0; key < (uint64_t)cells_x * cells_y; ++key) {
+            const size_t b = k;
+            while (k < col_order.size() && col_key(col_order[k]) == key) ++k;
+            col_range[key] = make_uint2((uint32_t)b, (uint32_t)k);
+        }
+    }
     s->n_edges_listed = entries.size();
     std::vector<OutlineDev> outl(d->n_outlines);
     for (uint32_t o = 0; o < d->n_outlines; ++o) {
@@ -430,6 +456,9 @@ qm_status qm_scene_upload(qm_ctx *ctx, const qm_scene_desc *d, qm_scene **out) {
     dv.cells_y = cells_y;
     qm_status st;
     if ((st = upload(s, cell_range.data(), cell_range.size(), &dv.cell_range)) != QM_OK ||
+        (st = upload(s, col_range.data(), col_range.size(), &dv.col_range)) != QM_OK ||
+        (st = upload(s, col_seg.data(), col_seg.size(), &dv.col_seg)) != QM_OK ||
+        (st = upload(s, col_ref.data(), col_ref.size(), &dv.col_ref)) != QM_OK ||
         (st = upload(s, cell_seg.data(), cell_seg.size(), &dv.cell_seg)) != QM_OK ||
         (st = upload(s, cell_ref.data(), cell_ref.size(), &dv.cell_ref)) != QM_OK ||
         (st = upload(s, reinterpret_cast<const int2 *>(d->vertices), (size_t)d->n_vertices, &dv.vertices)) != QM_OK ||

@@ -8,7 +8,10 @@
 // popup/src/evaluate.rs:171-214 (a point source's ray and divergence).
 #pragma once
 
+#include <climits>
+
 #include "qm_physics.cuh"
+#include "qm_stage.cuh"
 
 namespace qm {
 
@@ -37,9 +40,14 @@ static_assert(sizeof(SourceDev) == 128, "SourceDev layout");
 struct SceneDev {
     float step_m;
     int cell_steps, cells_x, cells_y;
-    const uint2 *cell_range;     // [cells]: each cell's first entry and one past its last
+    const uint2 *cell_range;     // [cells_y][cells_x]: each cell's first entry and one past its last
     const int4 *cell_seg;        // per entry: the edge's ends (ax, ay, bx, by)
     const uint2 *cell_ref;       // per entry: (edge start vertex, outline)
+    // The same entries column by column ([cells_x][cells_y]), so that a column's cells are one
+    // contiguous run of entries: what a warp sweeping along x stages with one bulk copy.
+    const uint2 *col_range;
+    const int4 *col_seg;
+    const uint2 *col_ref;
     const int2 *vertices;
     const OutlineDev *outlines;
     int dem_nx, dem_ny, dem_ox, dem_oy, dem_sp;
@@ -102,6 +110,57 @@ __device__ __noinline__ bool edge_bounds_roof(const SceneDev &S, long long sx, l
         if (n0 != 0 && n1 != 0) break;
     }
     return n0 * n1 < 0;
+}
+
+// A lane's listed crossings sorted by (t, footprint, edge), deduplicated as the reference does
+// (crossings.rs:34-56) and without the receiver's own walls; returns the count kept.
+__device__ __forceinline__ int finish_crossings(const SceneDev &S, XRec *xs, int n, uint32_t rcv_own) {
+    // The walk's cells come in order, so the list is nearly sorted; an edge listed in several cells
+    // appears once per visited cell, its copies side by side after.
+    for (int i = 1; i < n; ++i) {
+        XRec v = xs[i];
+        int j = i - 1;
+        while (j >= 0) {
+            const XRec &u = xs[j];
+            bool after = u.t > v.t;
+            if (!after && u.t == v.t) {
+                uint32_t fu = xrec_fp(S, u), fv = xrec_fp(S, v);
+                after = fu > fv || (fu == fv && u.edge > v.edge);
+            }
+            if (!after) break;
+            xs[j + 1] = u;
+            --j;
+        }
+        xs[j + 1] = v;
+    }
+    // One crossing per footprint and chainage within 1e-9 (crossings.rs:39-55); copies of one edge
+    // (equal t and edge) are the common case of it.
+    int kept = 0;
+    for (int i = 0; i < n; ++i) {
+        XRec c = xs[i];
+        if (kept > 0 && xs[kept - 1].edge == c.edge && xs[kept - 1].t == c.t) continue;
+        bool merged = false;
+        if (kept > 0 && c.t - xs[kept - 1].t < 1e-9) {
+            uint32_t fc = xrec_fp(S, c);
+            for (int k = kept - 1; k >= 0; --k) {
+                if (!(c.t - xs[k].t < 1e-9)) break;
+                if (xrec_fp(S, xs[k]) == fc) {
+                    xs[k].info |= (c.info & X_BOUNDS);
+                    merged = true;
+                    break;
+                }
+            }
+        }
+        if (!merged) xs[kept++] = c;
+    }
+    // The receiver's own walls (popup/src/evaluate.rs:293-297).
+    if (rcv_own != 0) {
+        int m = 0;
+        for (int i = 0; i < kept; ++i)
+            if (xrec_fp(S, xs[i]) != rcv_own) xs[m++] = xs[i];
+        kept = m;
+    }
+    return kept;
 }
 
 // Every crossing of the segment (sx, sy) -> (rx, ry) with an obstacle edge, sorted by (t, footprint)
@@ -193,52 +252,209 @@ __device__ int list_crossings(const SceneDev &S, int sx, int sy, int rx, int ry,
         cy = ncy;
         range = next_range;
     }
-    // Sort by (t, footprint, edge): the walk's cells come in order, so the list is nearly sorted; an
-    // edge listed in several cells appears once per visited cell, its copies side by side after.
-    for (int i = 1; i < n; ++i) {
-        XRec v = xs[i];
-        int j = i - 1;
-        while (j >= 0) {
-            const XRec &u = xs[j];
-            bool after = u.t > v.t;
-            if (!after && u.t == v.t) {
-                uint32_t fu = xrec_fp(S, u), fv = xrec_fp(S, v);
-                after = fu > fv || (fu == fv && u.edge > v.edge);
-            }
-            if (!after) break;
-            xs[j + 1] = u;
-            --j;
-        }
-        xs[j + 1] = v;
+    return finish_crossings(S, xs, n, rcv_own);
+}
+
+// ---------------------------------------------------------------------------------------------
+// Crossings of a warp's rays, found together
+
+// Entries staged per buffer; each warp has two buffers (2 KB) in shared memory.
+constexpr int STAGE_ENTRIES = 64;
+
+struct __align__(16) CrossStage {
+    int4 seg[2][STAGE_ENTRIES];
+    uint64_t bar[2];
+};
+
+// The staging state a warp carries from one source to the next: the parity each buffer's barrier
+// waits for next, and whether a copy ever failed to land (the warp then stages nothing more).
+struct StageState {
+    unsigned phases;
+    bool dead;
+};
+
+__device__ __forceinline__ void stage_init(CrossStage &st) {
+    if ((threadIdx.x & 31) == 0) {
+        mbar_init(&st.bar[0], 1);
+        mbar_init(&st.bar[1], 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
-    // One crossing per footprint and chainage within 1e-9 (crossings.rs:39-55); copies of one edge
-    // (equal t and edge) are the common case of it.
-    int kept = 0;
-    for (int i = 0; i < n; ++i) {
-        XRec c = xs[i];
-        if (kept > 0 && xs[kept - 1].edge == c.edge && xs[kept - 1].t == c.t) continue;
-        bool merged = false;
-        if (kept > 0 && c.t - xs[kept - 1].t < 1e-9) {
-            uint32_t fc = xrec_fp(S, c);
-            for (int k = kept - 1; k >= 0; --k) {
-                if (!(c.t - xs[k].t < 1e-9)) break;
-                if (xrec_fp(S, xs[k]) == fc) {
-                    xs[k].info |= (c.info & X_BOUNDS);
-                    merged = true;
-                    break;
+    __syncwarp();
+}
+
+__device__ __forceinline__ int warp_min_i(int v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = min(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+__device__ __forceinline__ int warp_max_i(int v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = max(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+
+// The crossings of each lane's segment (sx, sy) -> (rx, ry) (`ray` false: none), listed as
+// list_crossings lists them, by the whole warp at once. Every lane must call it, with warp-uniform
+// staging state. The rays of a warp run from one source to nearby receivers and so meet nearly the
+// same obstacle cells. The warp sweeps the union of their cells a column at a time along the
+// leading lane's main axis: each lane finds the cell rows its own segment touches in the column
+// (with a margin, so the union never misses a cell), the warp takes their span, and the span's
+// entries, contiguous in the column-ordered (or, sweeping along y, the row-ordered) copy of the cell
+// lists, arrive in shared memory by one bulk copy per piece of at most STAGE_ENTRIES, the next piece's
+// copy in flight while the current one is tested. Each lane tests every staged entry against its own
+// segment by the exact integer test. An edge a segment crosses is listed in the cell holding the
+// crossing point, which lies in the span, so each lane finds every crossing it would find alone
+// (some more than once, as the lone walk does for an edge listed in several cells), and
+// finish_crossings then yields the same list.
+template <int MAXC>
+__device__ int warp_list_crossings(const SceneDev &S, CrossStage &st, StageState &ss, int sx, int sy, int rx, int ry,
+                                   bool ray, uint32_t rcv_own, XRec *xs, uint32_t &status, uint32_t &edges_tested) {
+    const unsigned FULL = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    ray = ray && (rx != sx || ry != sy);
+    const unsigned rays = __ballot_sync(FULL, ray);
+    if (rays == 0) return 0;
+    if (ss.dead) {
+        status |= FAILED_TIMEOUT;
+        return 0;
+    }
+    const int leader = __ffs(rays) - 1;
+    const int ldx = __shfl_sync(FULL, rx - sx, leader), ldy = __shfl_sync(FULL, ry - sy, leader);
+    const bool xmajor = abs(ldx) >= abs(ldy);
+    const int su = xmajor ? sx : sy, sv = xmajor ? sy : sx, ru = xmajor ? rx : ry, rv = xmajor ? ry : rx;
+    const int C = S.cell_steps;
+    const int cells_u = xmajor ? S.cells_x : S.cells_y, cells_v = xmajor ? S.cells_y : S.cells_x;
+    const int dir = (xmajor ? ldx : ldy) >= 0 ? 1 : -1;
+    const int u_lo = ray ? min(su, ru) : INT_MAX, u_hi = ray ? max(su, ru) : INT_MIN;
+    int cu = max(floor_div(warp_min_i(u_lo), C), 0), cu_end = min(floor_div(warp_max_i(u_hi), C), cells_u - 1);
+    if (dir < 0) {
+        const int t = cu;
+        cu = cu_end;
+        cu_end = t;
+    }
+    bool columns_left = dir > 0 ? cu <= cu_end : cu >= cu_end;
+    const uint2 *ranges = xmajor ? S.col_range : S.cell_range;
+    const int4 *segs = xmajor ? S.col_seg : S.cell_seg;
+    const uint2 *refs = xmajor ? S.col_ref : S.cell_ref;
+    const double slope = (ray && ru != su) ? (double)(rv - sv) / (double)(ru - su) : 0.0;
+    const double inv_c = 1.0 / (double)C;
+    const int minx = min(sx, rx), maxx = max(sx, rx), miny = min(sy, ry), maxy = max(sy, ry);
+    const int idx = rx - sx, idy = ry - sy;
+    const long long dx = idx, dy = idy;
+    uint32_t cb = 0, ce = 0;  // entries of the current column not yet staged
+    // The next piece of entries in sweep order; warp-uniform.
+    auto next_piece = [&](uint32_t &start, uint32_t &count) -> bool {
+        while (cb == ce) {
+            if (!columns_left) return false;
+            int vlo = INT_MAX, vhi = INT_MIN;
+            if (ray) {
+                const long long x0 = max((long long)cu * C, (long long)u_lo), x1 = min((long long)(cu + 1) * C, (long long)u_hi);
+                if (x0 <= x1) {
+                    double v0, v1;
+                    if (ru == su) {
+                        v0 = min(sv, rv);
+                        v1 = max(sv, rv);
+                    } else {
+                        v0 = (double)sv + (double)(x0 - su) * slope;
+                        v1 = (double)sv + (double)(x1 - su) * slope;
+                        if (v0 > v1) {
+                            const double t = v0;
+                            v0 = v1;
+                            v1 = t;
+                        }
+                    }
+                    vlo = (int)floor((v0 - 1e-3) * inv_c);
+                    vhi = (int)floor((v1 + 1e-3) * inv_c);
                 }
             }
+            const int wlo = max(warp_min_i(vlo), 0), whi = min(warp_max_i(vhi), cells_v - 1);
+            if (wlo <= whi) {
+                cb = __ldg(&ranges[(size_t)cu * cells_v + wlo].x);
+                ce = __ldg(&ranges[(size_t)cu * cells_v + whi].y);
+            }
+            cu += dir;
+            columns_left = dir > 0 ? cu <= cu_end : cu >= cu_end;
         }
-        if (!merged) xs[kept++] = c;
+        start = cb;
+        count = min(ce - cb, (uint32_t)STAGE_ENTRIES);
+        cb += count;
+        return true;
+    };
+    int n = 0;
+    bool full = false;
+    uint32_t g_cur = 0, n_cur = 0;
+    bool have = next_piece(g_cur, n_cur);
+    if (have && lane == 0) bulk_load(st.seg[0], segs + g_cur, n_cur * (unsigned)sizeof(int4), &st.bar[0]);
+    int b = 0;
+    while (have) {
+        uint32_t g_next = 0, n_next = 0;
+        const bool have_next = next_piece(g_next, n_next);
+        if (have_next && lane == 0) {
+            // Buffer b ^ 1 was read in the previous round, before the warp's last __syncwarp.
+            fence_proxy_async_shared();
+            bulk_load(st.seg[b ^ 1], segs + g_next, n_next * (unsigned)sizeof(int4), &st.bar[b ^ 1]);
+        }
+        const bool landed = __all_sync(FULL, mbar_wait(&st.bar[b], (ss.phases >> b) & 1u));
+        ss.phases ^= 1u << b;
+        if (!landed) {
+            // Wait once more, bounded, for the copy still in flight, then stage nothing more.
+            if (have_next) {
+                mbar_wait(&st.bar[b ^ 1], (ss.phases >> (b ^ 1)) & 1u);
+                ss.phases ^= 1u << (b ^ 1);
+            }
+            __syncwarp();
+            ss.dead = true;
+            status |= FAILED_TIMEOUT;
+            return n;
+        }
+        if (ray) {
+            const int4 *piece = st.seg[b];
+            for (uint32_t j = 0; j < n_cur; ++j) {
+                const int4 seg = piece[j];
+                if (max(seg.x, seg.z) < minx || min(seg.x, seg.z) > maxx || max(seg.y, seg.w) < miny ||
+                    min(seg.y, seg.w) > maxy)
+                    continue;
+                ++edges_tested;
+                const int ex = seg.z - seg.x, ey = seg.w - seg.y;
+                long long den = mulw(idx, ey) - mulw(idy, ex);
+                if (den == 0) continue;
+                const int wx = seg.x - sx, wy = seg.y - sy;
+                long long tn = mulw(wx, ey) - mulw(wy, ex);
+                long long un = mulw(wx, idy) - mulw(wy, idx);
+                long long d = den;
+                if (d < 0) {
+                    d = -d;
+                    tn = -tn;
+                    un = -un;
+                }
+                if (!(tn > 0 && tn < d && un >= 0 && un <= d)) continue;
+                const uint2 ref = __ldg(refs + g_cur + j);
+                // An edge listed in several swept cells is met again; a segment meets an edge at most
+                // once, so a repeat of an edge among the lane's last few hits is that crossing again.
+                bool repeat = false;
+                for (int k = n - 1; k >= 0 && k >= n - 4; --k) repeat |= xs[k].edge == ref.x;
+                if (repeat) continue;
+                if (n >= MAXC) {
+                    status |= FAILED_CAPACITY;
+                    full = true;
+                    continue;
+                }
+                const OutlineDev o = S.outlines[ref.y];
+                const bool building = o.building != 0;
+                const bool bounds =
+                    building && ((un != 0 && un != d) || edge_bounds_roof(S, sx, sy, dx, dy, ref.x, o.first, o.count));
+                xs[n++] = XRec{(double)tn / (double)d, ref.x, ref.y | (building ? X_BUILDING : 0u) | (bounds ? X_BOUNDS : 0u),
+                               o.height, o.fp};
+            }
+        }
+        __syncwarp();
+        g_cur = g_next;
+        n_cur = n_next;
+        have = have_next;
+        b ^= 1;
     }
-    // The receiver's own walls (popup/src/evaluate.rs:293-297).
-    if (rcv_own != 0) {
-        int m = 0;
-        for (int i = 0; i < kept; ++i)
-            if (xrec_fp(S, xs[i]) != rcv_own) xs[m++] = xs[i];
-        kept = m;
-    }
-    return kept;
+    if (full) return n;
+    return finish_crossings(S, xs, n, rcv_own);
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -713,19 +929,16 @@ __device__ __forceinline__ float favourable_at(const float row[QM_SECTORS], floa
     return row[lower] + fraction * (row[upper] - row[lower]);
 }
 
-// One point source at one receiver: boundary transfer per state, slant, divergence weight and p.
-// `want_fav` false skips the favourable state (its p is zero everywhere).
+// The rest of a path once its crossings are listed in w.xs[0, nx): terrain, roofs, both states'
+// bands and boundaries, slant, divergence and p. out.status and out.edges_tested hold what the
+// listing set.
 template <int CAP_C, int CAP_K, int CAP_H>
-__device__ void evaluate_path(const SceneDev &S, const SourceDev &src, int rx, int ry, float rcv_alt, uint32_t rcv_own,
-                              bool want_fav, PathWork<CAP_C, CAP_K, CAP_H> &w, PathResult &out) {
-    out.status = 0;
-    out.edges_tested = 0;
+__device__ void evaluate_listed(const SceneDev &S, const SourceDev &src, int rx, int ry, float rcv_alt, bool want_fav,
+                                PathWork<CAP_C, CAP_K, CAP_H> &w, int nx, PathResult &out) {
     const int sx = src.x, sy = src.y;
     const float dxm = (float)(rx - sx) * S.step_m, dym = (float)(ry - sy) * S.step_m;
     const float dist = sqrtf(dxm * dxm + dym * dym);
     const float L = fmaxf(dist, 1.0f);
-    // Crossings.
-    int nx = list_crossings<CAP_C>(S, sx, sy, rx, ry, rcv_own, w.xs, out.status, out.edges_tested);
     out.crossings = nx;
     // Pass 1: terrain heights and G at the crossings, and the crests (physics/src/ray.rs:255-309).
     TerrainWalk walk;
@@ -1010,6 +1223,17 @@ __device__ void evaluate_path(const SceneDev &S, const SourceDev &src, int rx, i
     float azimuth = atan2f(dym, dxm);
 #pragma unroll
     for (int p = 0; p < QM_PERIODS; ++p) out.p[p] = want_fav ? favourable_at(S.fav[p], azimuth) : 0.0f;
+}
+
+// One point source at one receiver: boundary transfer per state, slant, divergence weight and p.
+// `want_fav` false skips the favourable state (its p is zero everywhere).
+template <int CAP_C, int CAP_K, int CAP_H>
+__device__ void evaluate_path(const SceneDev &S, const SourceDev &src, int rx, int ry, float rcv_alt, uint32_t rcv_own,
+                              bool want_fav, PathWork<CAP_C, CAP_K, CAP_H> &w, PathResult &out) {
+    out.status = 0;
+    out.edges_tested = 0;
+    const int nx = list_crossings<CAP_C>(S, src.x, src.y, rx, ry, rcv_own, w.xs, out.status, out.edges_tested);
+    evaluate_listed<CAP_C, CAP_K, CAP_H>(S, src, rx, ry, rcv_alt, want_fav, w, nx, out);
 }
 
 }  // namespace qm

@@ -30,9 +30,10 @@ def test_a_timed_tile_of_the_full_terrain_square_matches_the_oracle_at_the_maxim
     dev = ctx.scene(scene)
     bands, dba, lden, hist, stats = dev.paint_grid(grid)
     assert stats["paths"] == grid.cells * (grid.source_end - grid.source_begin)
-    # Long rays overflow the per-path capacities now and then; those paths are re-run with large
-    # capacities and are part of every cell's sums (about 0.1 % of paths, spread over the tile).
-    assert stats["failed_paths"] > 0, stats
+    # A path whose lists overflow the per-path capacities is re-run with large capacities and is part
+    # of its cell's sums like any other; with crossings deduplicated as they are listed, this tile's
+    # ~5.7 km rays fit (the re-run itself is checked by the over-capacity case in test_gpu_parity).
+    print("full terrain tile: paths re-run over capacity:", stats["failed_paths"])
     row = int(np.random.default_rng(21).integers(0, grid.ny))
     c0, c1 = row * grid.nx, (row + 1) * grid.nx
     e, l, _ = oracle.OracleScene(scene).paint_grid(grid, c0, c1)

@@ -91,6 +91,34 @@ def test_crossing_edge_cases_corners_tangents_and_walls(ctx):
     _assert_crossings_equal(dev, ora, frm, to)
 
 
+def test_the_painters_warp_crossing_walk_lists_what_single_rays_list(ctx, terrain):
+    """The grid painter lists the crossings of a warp's 32 rays together (a sweep over the union of
+    their cells, staged in shared memory); every ray must get exactly the crossings the single-ray
+    walk of qm_list_crossings gives it. Checked by the total over a tile's receivers and 4,000
+    sources in every direction, the receivers standing outside every building (the single-ray entry
+    keeps a receiver's own walls)."""
+    scene, grid = terrain
+    ora = oracle.OracleScene(scene)
+    rng = np.random.default_rng(13)
+    ext = np.array(scene.extent_steps)
+    for _ in range(200):
+        o = rng.integers(0, ext - 16 * grid.spacing)
+        g = scenes.Grid(origin=(int(o[0]), int(o[1])), spacing=grid.spacing, nx=16, ny=8, source_begin=0,
+                        source_end=4000)
+        rxy = g.receiver_xy()
+        if not ora.enclosing(rxy).any():
+            break
+    dev = ctx.scene(scene)
+    _, _, _, _, stats = dev.paint_grid(g)
+    assert stats["failed_paths"] == 0
+    src = np.stack([scene.sources["x"][:4000], scene.sources["y"][:4000]], axis=1)
+    frm = np.repeat(src, len(rxy), axis=0)
+    to = np.tile(rxy, (len(src), 1))
+    counts, _, _, _, status = dev.list_crossings(frm, to)
+    assert not status.any()
+    assert stats["crossings"] == int(counts.sum()), (stats["crossings"], int(counts.sum()))
+
+
 def _levels_db(energy):
     with np.errstate(divide="ignore"):
         return 10.0 * np.log10(energy)
