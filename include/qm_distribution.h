@@ -153,6 +153,22 @@ qm_status qm_pixel_distributions(const float *packed, size_t n_floats, uint32_t 
 qm_status qm_pixel_ndens(const float *packed, size_t n_floats, uint32_t n_layers, double bin_db, const double *shares,
                          size_t n_profiles, const uint32_t *runs, const double *curves, double *ndens);
 
+/* Batch::loudness on the device (paint/src/exact.rs:171-175; the reference's card:
+ * paint-gpu/src/loudness.rs:270-372, kernels/loudness.cuh): `n_pixels` packed pixels laid end to
+ * end in input[n_floats], pixel k starting at offsets[k] and ending where the next starts (the last
+ * at n_floats), each read as qm_pixel_read reads it. Per pixel, what qm_pixel_ndens computes on the
+ * host: its layers' and place's distributions over each period (hours grouped by shares[n_profiles]
+ * [24] and runs[3] as qm_pixel_distributions groups them), then Nden per layer and for the place on
+ * curves made on the device from the pixel's own shapes (Zwicker's loudness of each shape at every
+ * whole decibel a level needs). ndens[n_pixels][n_layers + 1] (a layer without a shape reads 0).
+ * Limits: n_layers at most 8; bin_db at least 1.875 dB (at most 96 bins; the map's grid is 2 dB);
+ * a moving line of at most 256 values. A malformed pixel, a line that breaks the host's checks or
+ * names a profile past n_profiles, or a line over the values limit fails the call with the pixel's
+ * index; its Nden is NaN. kernel_ms (nullable) receives the kernel's device time. */
+qm_status qm_pixel_loudness(qm_ctx *ctx, const float *input, size_t n_floats, const uint64_t *offsets,
+                            size_t n_pixels, uint32_t n_layers, double bin_db, const double *shares,
+                            size_t n_profiles, const uint32_t *runs, float *ndens, double *kernel_ms);
+
 /* Percentiles::of (popup/src/percentiles.rs:284-296): the levels exceeded 5, 10, 50 and 90 % of
  * each period's time (dB, -inf where silence is), from bins[3][n_bins][2]; levels[4][3] (L5,
  * L10, L50, L90 by period). */

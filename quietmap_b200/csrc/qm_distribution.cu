@@ -118,27 +118,7 @@ qm_status qm_distribution_with_line(double bin_db, const double *bins, double si
             return qm::set_error(QM_ERR_ARGUMENT, "qm_distribution_with_line: value " + std::to_string(k) +
                                                       " has a negative or NaN intensity or share");
     const OwnedValues line = sorted_values(values, n_values);
-    // The two phases a warp runs (lanes over moments, then over output bins), here in turn.
-    std::vector<double> intensity(n_bins + 1), share(n_bins + 1);
-    const int n_moments = qm::dist::moment_of(bins, silent, n_bins, intensity.data(), share.data());
-    std::vector<qm::dist::RunRecord> records((size_t)n_moments * (n_bins + 1));
-    std::vector<int> first(n_moments + 1, 0);
-    int at = 0;
-    for (int m = 0; m < n_moments; ++m) {
-        first[m] = at;
-        at += qm::dist::moment_runs(bin_db, n_bins, intensity[m], line.view(), scale, records.data() + at);
-    }
-    first[n_moments] = at;
-    for (int b = -1; b < n_bins; ++b) {
-        double a, w;
-        qm::dist::bin_sums(b, n_moments, intensity.data(), share.data(), records.data(), first.data(), &a, &w);
-        if (b < 0) {
-            *out_silent = a;
-        } else {
-            out_bins[2 * b] = a;
-            out_bins[2 * b + 1] = w;
-        }
-    }
+    qm::dist::with_line(bin_db, n_bins, bins, silent, line.view(), scale, out_bins, out_silent);
     return QM_OK;
 }
 

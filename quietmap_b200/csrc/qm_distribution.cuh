@@ -141,60 +141,6 @@ __host__ __device__ inline void with_line(double bin_db, int n_bins, const doubl
     *out_silent = silent;
 }
 
-// with_line in two phases whose work is independent within each phase, for lanes of a warp: the
-// first lists each input moment's runs (bin, shares, weighted; bin -1 silence), bins ascending;
-// the second gives each output bin (and the silence) its sums over the moments in their order.
-// Every output bin receives the same products in the same order as with_line adds them, so the
-// result is the same to the bit. Moment m is the silence (when in_silent > 0) and then each bin
-// holding time, in order: moment_of lists them, returns their count.
-struct RunRecord {
-    int bin;
-    double shares, weighted;
-};
-
-__host__ __device__ inline int moment_of(const double *in_bins, double in_silent, int n_bins, double *intensity,
-                                         double *share) {
-    int m = 0;
-    if (in_silent > 0.0) {
-        intensity[m] = 0.0;
-        share[m] = in_silent;
-        ++m;
-    }
-    for (int b = 0; b < n_bins; ++b)
-        if (in_bins[2 * b] > 0.0) {
-            intensity[m] = in_bins[2 * b + 1] / in_bins[2 * b];
-            share[m] = in_bins[2 * b];
-            ++m;
-        }
-    return m;
-}
-
-// Phase one for one moment: its runs into `records` (at most n_bins + 1), returns their count.
-__host__ __device__ inline int moment_runs(double bin_db, int n_bins, double intensity, const Values &line, double scale,
-                                           RunRecord *records) {
-    int count = 0;
-    auto visit = [&](int bin, double shares, double weighted) { records[count++] = RunRecord{bin, shares, weighted}; };
-    runs(bin_db, n_bins, intensity, line, scale, visit);
-    return count;
-}
-
-// Phase two for output bin `bin` (-1: the silence): its two sums over the moments in order, each
-// moment's records found from `first[m]` (its records are records[first[m] .. first[m + 1])).
-__host__ __device__ inline void bin_sums(int bin, int n_moments, const double *intensity, const double *share,
-                                         const RunRecord *records, const int *first, double *sum_share,
-                                         double *sum_weighted) {
-    double a = 0.0, w = 0.0;
-    for (int m = 0; m < n_moments; ++m)
-        for (int r = first[m]; r < first[m + 1]; ++r) {
-            if (records[r].bin > bin) break;
-            if (records[r].bin != bin) continue;
-            a += share[m] * records[r].shares;
-            w += share[m] * (intensity[m] * records[r].shares + records[r].weighted);
-        }
-    *sum_share = a;
-    *sum_weighted = w;
-}
-
 // The level exceeded `exceeded` of the time, -inf where silence is (distribution.rs:152-162).
 __host__ __device__ inline double exceeded_db(const double *bins, int n_bins, double exceeded) {
     double above = 0.0;

@@ -33,6 +33,8 @@
 #include "qm_host.h"
 #include "qm_mlp.h"
 #include "qm_percentile.cuh"
+#include "qm_pixel.cuh"
+#include "../../include/qm_distribution.h"
 #include "qm_surrogate.cuh"
 #include "qm_tiles.cuh"
 
@@ -2745,6 +2747,21 @@ namespace qm {
 const std::vector<float> &line_level_table_shared() { return line_level_table(); }
 }  // namespace qm
 
+namespace {
+
+// The line-level table on the context's device, uploaded on first use (the context's lock held,
+// its device current).
+qm_status device_line_table(qm_ctx *ctx) {
+    if (ctx->line_table) return QM_OK;
+    const std::vector<float> &table = line_level_table();
+    QM_CUDA(cudaMalloc(&ctx->line_table, table.size() * sizeof(float)));
+    QM_CUDA(cudaMemcpyAsync(ctx->line_table, table.data(), table.size() * sizeof(float), cudaMemcpyHostToDevice,
+                            ctx->stream));
+    return QM_OK;
+}
+
+}  // namespace
+
 extern "C" {
 
 qm_status qm_line_level_table(float *table) {
@@ -2758,15 +2775,11 @@ qm_status qm_line_level_quantiles(qm_ctx *ctx, const double *lambda, const doubl
     if (!ctx) return fail(QM_ERR_ARGUMENT, "qm_line_level_quantiles: null ctx");
     if (n == 0) return QM_OK;
     if (!lambda || !p || !out) return fail(QM_ERR_ARGUMENT, "qm_line_level_quantiles: null lambda, p or out");
-    const std::vector<float> &table = line_level_table();
     std::lock_guard<std::mutex> guard(ctx->lock);
     QM_CUDA(cudaSetDevice(ctx->device));
     cudaStream_t stream = ctx->stream;
-    if (!ctx->line_table) {
-        QM_CUDA(cudaMalloc(&ctx->line_table, table.size() * sizeof(float)));
-        QM_CUDA(cudaMemcpyAsync(ctx->line_table, table.data(), table.size() * sizeof(float), cudaMemcpyHostToDevice,
-                                stream));
-    }
+    const qm_status table_status = device_line_table(ctx);
+    if (table_status != QM_OK) return table_status;
     Scratch d_lambda, d_p, d_out;
     QM_CUDA(cudaMalloc(&d_lambda.p, n * sizeof(double)));
     QM_CUDA(cudaMalloc(&d_p.p, n * sizeof(double)));
@@ -2779,6 +2792,113 @@ qm_status qm_line_level_quantiles(qm_ctx *ctx, const double *lambda, const doubl
     QM_CUDA(cudaGetLastError());
     QM_CUDA(cudaMemcpyAsync(out, d_out.p, n * sizeof(double), cudaMemcpyDeviceToHost, stream));
     QM_CUDA(cudaStreamSynchronize(stream));
+    return QM_OK;
+}
+
+}  // extern "C"
+
+// =============================================================================================
+// Batch::loudness on the device (qm_distribution.h, qm_pixel.cuh).
+
+extern "C" {
+
+qm_status qm_pixel_loudness(qm_ctx *ctx, const float *input, size_t n_floats, const uint64_t *offsets,
+                            size_t n_pixels, uint32_t n_layers, double bin_db, const double *shares,
+                            size_t n_profiles, const uint32_t *runs, float *ndens, double *kernel_ms) {
+    using namespace qm::pix;
+    if (!ctx) return fail(QM_ERR_ARGUMENT, "qm_pixel_loudness: null ctx");
+    if (n_pixels == 0) return QM_OK;
+    if (!input || !offsets || !ndens) return fail(QM_ERR_ARGUMENT, "qm_pixel_loudness: null input, offsets or ndens");
+    if (n_layers > (uint32_t)MAX_LAYERS)
+        return fail(QM_ERR_ARGUMENT, "qm_pixel_loudness: " + std::to_string(n_layers) + " layers, at most " +
+                                         std::to_string(MAX_LAYERS));
+    if (!(bin_db > 0.0) || !std::isfinite(bin_db))
+        return fail(QM_ERR_ARGUMENT, "qm_pixel_loudness: bin_db must be positive and finite");
+    const double bins_f = std::round(qm::dist::SPAN_DB / bin_db);
+    if (!(bins_f >= 1.0) || bins_f > MAX_BINS)
+        return fail(QM_ERR_ARGUMENT, "qm_pixel_loudness: bin_db gives " + std::to_string(bins_f) + " bins, at most " +
+                                         std::to_string(MAX_BINS) + " on the device");
+    if (n_pixels > 0xFFFFFFFFu) return fail(QM_ERR_ARGUMENT, "qm_pixel_loudness: too many pixels");
+    for (size_t k = 0; k < n_pixels; ++k) {
+        const uint64_t end = k + 1 < n_pixels ? offsets[k + 1] : n_floats;
+        if (offsets[k] > end || end > n_floats)
+            return fail(QM_ERR_ARGUMENT, "qm_pixel_loudness: pixel " + std::to_string(k) +
+                                             " does not lie within the input before the next pixel");
+    }
+    // The periods' groups of hours (the caller's hourly shares, as qm_pixel_distributions groups them).
+    std::vector<double> factors((size_t)3 * MAX_GROUPS * std::max<size_t>(n_profiles, 1), 1.0);
+    std::vector<uint32_t> group_hours(3 * MAX_GROUPS, 0);
+    uint32_t n_groups[3] = {0, 0, 0};
+    if (n_profiles > 0) {
+        if (!shares) return fail(QM_ERR_ARGUMENT, "qm_pixel_loudness: null shares with profiles");
+        for (uint32_t p = 0; p < 3; ++p) {
+            uint32_t slot_group[12];
+            size_t groups = 0;
+            const qm_status st = qm_hour_groups(shares, n_profiles, p, runs ? runs[p] : 0, slot_group,
+                                                group_hours.data() + p * MAX_GROUPS,
+                                                factors.data() + (size_t)p * MAX_GROUPS * n_profiles, &groups);
+            if (st != QM_OK) return st;
+            n_groups[p] = (uint32_t)groups;
+        }
+    }
+    std::lock_guard<std::mutex> guard(ctx->lock);
+    QM_CUDA(cudaSetDevice(ctx->device));
+    cudaStream_t stream = ctx->stream;
+    qm_status st = device_line_table(ctx);
+    if (st != QM_OK) return st;
+    const uint32_t L = n_layers;
+    Scratch d_in, d_off, d_fac, d_groups, d_nden, d_status;
+    QM_CUDA(cudaMalloc(&d_in.p, std::max<size_t>(n_floats, 1) * sizeof(float)));
+    QM_CUDA(cudaMalloc(&d_off.p, n_pixels * sizeof(uint64_t)));
+    QM_CUDA(cudaMalloc(&d_fac.p, factors.size() * sizeof(double)));
+    QM_CUDA(cudaMalloc(&d_groups.p, group_hours.size() * sizeof(uint32_t)));
+    QM_CUDA(cudaMalloc(&d_nden.p, n_pixels * (L + 1) * sizeof(float)));
+    QM_CUDA(cudaMalloc(&d_status.p, n_pixels * sizeof(uint32_t)));
+    if (n_floats) QM_CUDA(cudaMemcpyAsync(d_in.p, input, n_floats * sizeof(float), cudaMemcpyHostToDevice, stream));
+    QM_CUDA(cudaMemcpyAsync(d_off.p, offsets, n_pixels * sizeof(uint64_t), cudaMemcpyHostToDevice, stream));
+    QM_CUDA(cudaMemcpyAsync(d_fac.p, factors.data(), factors.size() * sizeof(double), cudaMemcpyHostToDevice, stream));
+    QM_CUDA(cudaMemcpyAsync(d_groups.p, group_hours.data(), group_hours.size() * sizeof(uint32_t),
+                            cudaMemcpyHostToDevice, stream));
+    Args A{};
+    A.input = static_cast<const float *>(d_in.p);
+    A.offsets = static_cast<const uint64_t *>(d_off.p);
+    A.n_floats = n_floats;
+    A.n_pixels = (uint32_t)n_pixels;
+    A.n_layers = L;
+    A.bin_db = bin_db;
+    A.n_bins = (int)bins_f;
+    A.table = ctx->line_table;
+    A.factors = static_cast<const double *>(d_fac.p);
+    A.group_hours = static_cast<const uint32_t *>(d_groups.p);
+    for (int p = 0; p < 3; ++p) A.n_groups[p] = n_groups[p];
+    A.n_profiles = (uint32_t)n_profiles;
+    A.ndens = static_cast<float *>(d_nden.p);
+    A.status = static_cast<uint32_t *>(d_status.p);
+    const size_t smem = shared_bytes(A.n_bins);
+    QM_CUDA(cudaFuncSetAttribute(pixel_loudness_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    Events ev;
+    QM_CUDA(ev.create());
+    QM_CUDA(cudaEventRecord(ev.e0, stream));
+    pixel_loudness_kernel<<<(unsigned)n_pixels, THREADS, smem, stream>>>(A);
+    QM_CUDA(cudaGetLastError());
+    QM_CUDA(cudaEventRecord(ev.e1, stream));
+    std::vector<uint32_t> status(n_pixels);
+    QM_CUDA(cudaMemcpyAsync(ndens, d_nden.p, n_pixels * (L + 1) * sizeof(float), cudaMemcpyDeviceToHost, stream));
+    QM_CUDA(cudaMemcpyAsync(status.data(), d_status.p, n_pixels * sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
+    QM_CUDA(cudaStreamSynchronize(stream));
+    if (kernel_ms) {
+        float ms = 0.0f;
+        QM_CUDA(cudaEventElapsedTime(&ms, ev.e0, ev.e1));
+        *kernel_ms = ms;
+    }
+    for (size_t k = 0; k < n_pixels; ++k) {
+        if (status[k] == 0) continue;
+        std::string why = (status[k] & BAD_PACKING) ? "its counts run past its floats or leave floats over"
+                          : (status[k] & BAD_PROFILE) ? "a line follows a profile past n_profiles"
+                          : (status[k] & BAD_LINE)    ? "a line or steady energy fails the host's checks"
+                                                      : "a moving line has more than 256 values";
+        return fail(QM_ERR_ARGUMENT, "qm_pixel_loudness: pixel " + std::to_string(k) + ": " + why);
+    }
     return QM_OK;
 }
 

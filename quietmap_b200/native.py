@@ -165,6 +165,9 @@ def lib():
         L.qm_pixel_ndens.argtypes = [C.POINTER(C.c_float), C.c_size_t, C.c_uint32, C.c_double, _D, C.c_size_t, _U32,
                                      _D, _D]
         L.qm_pixel_ndens.restype = C.c_int
+        L.qm_pixel_loudness.argtypes = [C.c_void_p, C.POINTER(C.c_float), C.c_size_t, _U64, C.c_size_t, C.c_uint32,
+                                        C.c_double, _D, C.c_size_t, _U32, _F, _D]
+        L.qm_pixel_loudness.restype = C.c_int
         L.qm_pixel_distributions.argtypes = [C.POINTER(C.c_float), C.c_size_t, C.c_uint32, C.c_double, _D, C.c_size_t,
                                              _U32, _D, _D, _D, _D]
         L.qm_pixel_distributions.restype = C.c_int
@@ -223,6 +226,24 @@ class Context:
         _check(lib().qm_zwicker(self.handle, abi.ptr(thirds, C.c_float), len(thirds), abi.ptr(out, C.c_float)),
                self.handle)
         return out
+
+    def pixel_loudness(self, pixels, n_layers, bin_db=2.0, shares=None, runs=None, stats=False):
+        """Batch::loudness on the device (qm_pixel_loudness): Nden per layer and for the place
+        [n][n_layers + 1] of packed pixels (a list of float32 arrays, laid end to end), and the
+        kernel's device time in ms when `stats`."""
+        sizes = [len(p) for p in pixels]
+        offsets = np.ascontiguousarray(np.concatenate([[0], np.cumsum(sizes)[:-1]]) if sizes else [], dtype=np.uint64)
+        f = np.ascontiguousarray(np.concatenate(pixels) if pixels else np.zeros(0), dtype=np.float32)
+        sh = np.ascontiguousarray(np.zeros((0, 24)) if shares is None else shares, dtype=np.float64).reshape(-1, 24)
+        ru = None if runs is None else np.ascontiguousarray(runs, dtype=np.uint32)
+        out = np.zeros((len(pixels), n_layers + 1), np.float32)
+        ms = C.c_double(0.0)
+        _check(lib().qm_pixel_loudness(self.handle, abi.ptr(f, C.c_float) if len(f) else None, len(f),
+                                       abi.ptr(offsets, C.c_uint64) if len(offsets) else None, len(pixels),
+                                       int(n_layers), float(bin_db), abi.ptr(sh, C.c_double) if len(sh) else None,
+                                       len(sh), None if ru is None else abi.ptr(ru, C.c_uint32),
+                                       abi.ptr(out, C.c_float), C.byref(ms)), self.handle)
+        return (out, ms.value) if stats else out
 
     def flight_grid(self, flights, grid=None, sone=True, stats=False):
         """Doc 29 flights over a receiver grid: (LAE [cells], thirds [cells][28], sone [cells]),
