@@ -178,7 +178,7 @@ def measured_peaks():
 # small case of the workload (dram__bytes_read.sum + dram__bytes_write.sum over its paths), scaled
 # by paths to a full launch; the capture's command and figures are in
 # profiles/paint_grid_kernel_terrain.md. None where no capture of the current kernel exists.
-DRAM_BYTES_PER_PATH = {"terrain": None, "road": None}
+DRAM_BYTES_PER_PATH = {"terrain": 18429.0, "road": None}
 
 
 def stratified_sources(grid, m, seed):
