@@ -4,8 +4,9 @@ Packed pixels (paint/src/sone.rs's format, packed by the format's rule) are read
 read on their curves by the device kernel; the host form of the same path, qm_pixel_ndens (equal to
 the oracle's composition bit for bit, tests/test_pixel_read.py), with curves of the oracle's Zwicker
 in double, is the checker. The device takes its curves from the pixel's shapes with its own FP32
-Zwicker, so Nden agrees within the loudness tolerance of the reference's own check (0.5 %); a layer
-without a shape reads 0 on both.
+Zwicker and adds a line's runs in shared memory in any order, so Nden agrees to 1e-4 relative, far
+inside the 0.5 % of the reference's loudness check (about 5e-7 is seen); a layer without a shape
+reads 0 on both.
 """
 
 import numpy as np
@@ -17,7 +18,7 @@ from test_pixel_read import LAYERS, _pack, _pixel
 
 pytestmark = pytest.mark.gpu
 
-REL = 5e-3
+REL = 1e-4
 
 
 def _host_ndens(packed, curves, shares, runs):
