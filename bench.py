@@ -62,7 +62,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="terrain", choices=["terrain", "road", "flights", "surrogate", "surrogate_terrain", "tiles"])
+    ap.add_argument("--workload", default="terrain", choices=["terrain", "road", "flights", "surrogate", "surrogate_terrain", "tiles", "loudness"])
     ap.add_argument("--tiles", type=int, default=32, help="tiles workload: tiles per batch, drawn from the 4096")
     ap.add_argument("--flights", type=int, default=2000, help="flights workload: flights (a small case for profiling)")
     ap.add_argument("--cells-side", type=int, default=1024, help="flights workload: receivers per side")
@@ -279,6 +279,8 @@ def main():
         return surrogate_terrain(args, rank, world, local)
     if args.workload == "tiles":
         return tile_batch(args, rank, world, local)
+    if args.workload == "loudness":
+        return loudness(args, rank, world, local)
     import torch
     from quietmap_b200 import native
     scene, steps, desc = workload(args.workload, rank, args.slices, args.sources)
@@ -703,6 +705,87 @@ def surrogate_terrain(args, rank, world, local):
             "training": {"samples": int(n_train), "epochs": 6, "seconds": train_s, "loss": [float(v) for v in hist]},
             "clocks": clocks.summary(), "gpu_launches": args.steps * 5,
         }), flush=True)
+    ctx.close()
+
+
+def host_ndens(pixels, shares, runs, threads):
+    """Nden of each packed pixel by the library's host composition (qm_pixel_ndens, equal to the
+    FP64 oracle's composition bit for bit) on curves of the oracle's Zwicker in double, a host
+    thread a pixel."""
+    from concurrent.futures import ThreadPoolExecutor
+    from oracle import oracle
+    from quietmap_b200 import native
+
+    def one(packed):
+        at, n_layers = 0, 6
+        for _ in range(n_layers):
+            at += 4 + int(packed[at + 3]) * 43
+        tables = np.zeros((n_layers + 1, 3, 191))
+        for c in range(n_layers + 1):
+            for p in range(3):
+                shape = packed[at + (c * 3 + p) * 28: at + (c * 3 + p + 1) * 28].astype(np.float64)
+                if not np.isnan(shape[0]):
+                    tables[c, p] = oracle.zwicker_many(shape[None, :] + (-30.0 + np.arange(191))[:, None], nthreads=1)
+        return native.pixel_ndens(packed, n_layers, 2.0, tables, shares, runs)
+    with ThreadPoolExecutor(max_workers=threads) as pool:
+        return np.array(list(pool.map(one, pixels)))
+
+
+def loudness(args, rank, world, local):
+    """Batch::loudness on the device: a step is one call of 8,192 packed pixels (the reference's
+    batch, paint/src/exact.rs:21-22), 6 layers, the map's 2 dB grid, hours grouped 4/1/3 by 12
+    hourly profiles; pixels/s of device time, and end to end through the C ABI with the pixels'
+    upload and the Nden read back."""
+    import torch
+    from oracle import oracle
+    from quietmap_b200 import native, scenes
+    n = 8192
+    pixels, shares, runs = scenes.loudness_pixels(n, seed=11 + rank)
+    n_floats = sum(len(p) for p in pixels)
+    ctx = native.Context(local if world > 1 else 0)
+    torch.cuda.set_device(local if world > 1 else 0)
+    flush = torch.empty(64 << 20, dtype=torch.float32, device="cuda")
+    for _ in range(args.warmup):
+        ctx.pixel_loudness(pixels, 6, 2.0, shares, runs)
+    k_ms, wall = 0.0, 0.0
+    with ClockSampler(local) as clocks:
+        for _ in range(args.steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            got, ms = ctx.pixel_loudness(pixels, 6, 2.0, shares, runs, stats=True)
+            wall += time.perf_counter() - t0
+            k_ms += ms
+    if rank == 0:
+        line = {
+            "metric": "Batch::loudness pixels/s (packed pixels to Nden per layer and place), 1 B200",
+            "value": n * args.steps / (k_ms / 1e3), "unit": "pixels/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": k_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64 distributions, f32 Zwicker", "data": "synthetic (seeded packed pixels)",
+            "config": {"workload": f"{n} packed pixels a call (6 layers, 0-4 lines each: roads at mean flow, profiled "
+                                   "roads, events, streams), 2 dB grid, hours in 4/1/3 groups of 12 profiles",
+                       "floats_per_call": n_floats, "l2": "flushed between steps"},
+            "e2e": {"value": n * args.steps / wall, "unit": "pixels/s", "h2d_bytes_per_step": n_floats * 4 + n * 8,
+                    "d2h_bytes_per_step": n * 7 * 4 + n * 4},
+            "clocks": clocks.summary(), "gpu_launches": args.steps,
+        }
+        if not args.no_cpu_baseline and world == 1:
+            threads = oracle.threads()
+            m = threads
+            t0 = time.perf_counter()
+            host_ndens(pixels[:m], shares, runs, threads)
+            dt = time.perf_counter() - t0
+            m = min(n, max(m, int(m * 12.0 / max(dt, 1e-3))))
+            t0 = time.perf_counter()
+            want = host_ndens(pixels[:m], shares, runs, threads)
+            dt = time.perf_counter() - t0
+            rel = np.abs(got[:m] - want) / np.maximum(np.abs(want), 1e-12)
+            line["cpu_baseline"] = dict(value=m / dt, unit="pixels/s", cores=threads, kind="port",
+                                        sample=f"the first {m} pixels by the host composition equal to the FP64 "
+                                               f"oracle's, curves by the oracle's Zwicker ({dt:.1f} s)")
+            line["parity"] = {"pixels": m, "max_relative_nden_error": float(rel[want != 0].max()),
+                              "zero_where_host_zero": bool(np.all(got[:m][want == 0] == 0))}
+        print(json.dumps(line), flush=True)
     ctx.close()
 
 

@@ -425,3 +425,40 @@ def uneven_tiles(scene, n_tiles=4096, seed=5, side=(32, 512), sources=(10, 50000
                         source_end=b + k, cell_offset=offset))
         offset += nx * ny
     return out
+
+
+# ---------------------------------------------------------------------------------------------
+# Packed pixels for Batch::loudness.
+
+PACKED_LINE_FLOATS = 43
+
+
+def loudness_pixels(n, seed=11, layers=6, profiles=12):
+    """`n` seeded packed pixels in the reference's format (paint/src/sone.rs:32-51, 217-234): per
+    layer its steady energy per period, its line count and its 43-float lines (energy per period,
+    means per period and weather state, lambda per period, hourly profile or -1, duty per period or
+    NaN, passes in progress per period or NaN), then each layer's curves and the place's (28
+    third-octave levels at an A-weighted 0 dB per period, NaN: no shape). Lines mix roads at mean
+    flow, profiled roads, events and streams of passes; energies span 20-70 dB. Returns (pixels as
+    float32 arrays, hourly shares [profiles][24], the map's runs per period)."""
+    rng = np.random.default_rng(seed)
+    shares = rng.uniform(0.3, 9.0, (profiles, 24))
+    out = []
+    for _ in range(n):
+        f = []
+        for layer in range(layers):
+            count = int(rng.integers(0, 5))
+            f += list(10.0 ** rng.uniform(0.0, 6.0, 3)) + [float(count)]
+            for _ in range(count):
+                kind = int(rng.integers(0, 4))
+                f += list(10.0 ** rng.uniform(2.0, 7.0, 3))
+                f += list(10.0 ** rng.uniform(2.0, 7.0, 30))
+                f += list(10.0 ** rng.uniform(-3.0, 3.0, 3))
+                f.append(-1.0 if kind == 0 else float(rng.integers(0, profiles)))
+                f += list(rng.uniform(0.0, 0.3, 3)) if kind == 1 else [np.nan] * 3
+                f += list(rng.uniform(0.0, 5.0, 3)) if kind == 2 else [np.nan] * 3
+        for _ in range(layers + 1):
+            for _ in range(3):
+                f += [np.nan] * 28 if rng.random() < 0.2 else list(rng.uniform(-60.0, 5.0, 28))
+        out.append(np.array(f, dtype=np.float32))
+    return out, shares, [4, 1, 3]

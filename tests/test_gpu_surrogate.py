@@ -189,19 +189,28 @@ def test_terrain_surrogate_trains_and_paints(ctx, terrain):
     net = native.Surrogate(ctx, seed=2)
     grids = [scenes.Grid(origin=(full.origin[0] + 13 * k, full.origin[1] + 29 * k), spacing=full.spacing * 32,
                          nx=16, ny=16) for k in range(2)]
-    hist, n = net.train(dev, grids, epochs=3, batch=8192, learning_rate=2e-3, seed=5, max_samples=3_000_000)
+    # The painter's recipe: paths within 200 m stay exact (the near field carries a cell's energy).
+    hist, n = net.train(dev, grids, epochs=3, batch=8192, learning_rate=2e-3, seed=5, max_samples=3_000_000,
+                        exact_within_m=200.0)
     assert hist[-1] < 0.8 * hist[0], hist
     tile = scenes.Grid(origin=(full.origin[0] + 100 * full.spacing, full.origin[1] + 60 * full.spacing),
                        spacing=full.spacing, nx=16, ny=8)
     _, edba, _, _, est = dev.paint_grid(tile)
     _, sdba, _, _, sst = dev.paint_grid_surrogate(tile, net)
     d = np.abs(sdba - edba)
+    # The north star's bar: the surrogate painter's cells within 0.5 dB at p99 of the FP64 oracle, here
+    # on a seeded row of the tile against every source.
+    row = int(np.random.default_rng(25).integers(0, tile.ny))
+    e, _, _ = oracle.OracleScene(scene).paint_grid(tile, row * tile.nx, (row + 1) * tile.nx)
+    vs_oracle = np.abs(sdba[row * tile.nx:(row + 1) * tile.nx] - 10.0 * np.log10(e.sum(axis=1)))
     print(f"terrain: samples {n}, loss {hist}, surrogate paths {sst['surrogate_paths']} of {sst['paths']}, cell dBA "
-          f"p50 {np.median(d):.3f} p99 {np.percentile(d, 99):.3f} max {d.max():.3f}; exact {est['kernel_ms']:.1f} ms, "
+          f"vs exact p50 {np.median(d):.3f} p99 {np.percentile(d, 99):.3f} max {d.max():.3f}; vs oracle p99 "
+          f"{np.percentile(vs_oracle, 99):.3f} max {vs_oracle.max():.3f}; exact {est['kernel_ms']:.1f} ms, "
           f"surrogate {sst['kernel_ms']:.1f} ms")
     assert sst["paths"] == est["paths"]
     assert sst["surrogate_paths"] > 0.3 * sst["paths"]
-    assert np.percentile(d, 99) < 1.0
+    assert np.percentile(d, 99) < 0.5
+    assert np.percentile(vs_oracle, 99) <= 0.5, vs_oracle
     # a flat network refuses terrain scenes
     flat = native.Surrogate(ctx, seed=3)
     with pytest.raises(native.QmError):
