@@ -757,25 +757,21 @@ struct Band {
         float line = S.z + slope_sr * (c.x - S.x);
         if (STATE == QM_FAV) line += sag_sr.at(c.x - S.x);
         if (c.z > line) {
+            // Blocking: the first opens the band (from the total so far), an equal-x one higher than
+            // the hull's last replaces it, any other extends the hull; one push for all three.
             if (!blocked) {
                 blocked = true;
                 open = total;
                 oox = 0.0f;
                 ooz = z0;
-                push(c.x, c.z, oz, og);
-                return;
-            }
-            if (h[n - 1].x == c.x && n >= 2) {
-                if (c.z > h[n - 1].z) {
-                    const HullEntry &b = h[n - 1];
-                    const HullEntry &a = h[n - 2];
-                    open = join(b.seg, rebase(open, b.ox, b.oz, a.ox, a.oz));
-                    oox = a.ox;
-                    ooz = a.oz;
-                    --n;
-                    push(c.x, c.z, oz, og);
-                }
-                return;
+            } else if (h[n - 1].x == c.x && n >= 2) {
+                if (!(c.z > h[n - 1].z)) return;
+                const HullEntry &b = h[n - 1];
+                const HullEntry &a = h[n - 2];
+                open = join(b.seg, rebase(open, b.ox, b.oz, a.ox, a.oz));
+                oox = a.ox;
+                ooz = a.oz;
+                --n;
             }
             push(c.x, c.z, oz, og);
             return;
