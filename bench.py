@@ -790,29 +790,25 @@ def loudness(args, rank, world, local):
 
 
 def tile_batch(args, rank, world, local):
-    """Uneven tiles: 4096 tiles (sides log-uniform 32-512 receivers at 1.875 m, 10-50,000 point
-    sources each) over the config-1 road square; a step paints a seeded batch of `--tiles` of them
-    as one autotuned, graph-captured persistent launch. Beside it: the same batch with the default
-    launch shape, and one qm_paint_grid call per tile."""
+    """Uneven tiles (config 4): 4096 tiles, sides log-uniform 32-512 receivers at 7.8125 m, each with
+    its own road segments (log-uniform 10-50,000) and buildings (log-uniform 0-20,000) drawn in a
+    region of its own; a step paints a seeded batch of `--tiles` of them as one autotuned,
+    graph-captured persistent launch per thread count. A tile paints every receiver against its
+    first roads up to 2^26 paths (a prefix of independent draws). Beside it: the same batch with
+    the default launch shape, and one qm_paint_grid call per tile."""
     import torch
     from quietmap_b200 import native, scenes
-    world_scene = scenes.tiles_world()
-    all_tiles = scenes.uneven_tiles(world_scene, n_tiles=4096)
+    specs = scenes.uneven_tile_specs(n_tiles=4096)
     rng = np.random.default_rng(7 + rank)
-    pick = sorted(rng.choice(len(all_tiles), args.tiles, replace=False))
-    tiles, offset = [], 0
-    for k in pick:
-        t = dict(all_tiles[k], cell_offset=offset)
-        offset += t["nx"] * t["ny"]
-        tiles.append(t)
-    cells = offset
+    pick = sorted(rng.choice(len(specs), args.tiles, replace=False))
+    world_scene, tiles = scenes.uneven_tile_world([specs[k] for k in pick], max_paths_per_tile=1 << 26)
+    cells = sum(t["nx"] * t["ny"] for t in tiles)
     paths = sum(t["nx"] * t["ny"] * (t["source_end"] - t["source_begin"]) for t in tiles)
     ctx = native.Context(local if world > 1 else 0)
     dev = ctx.scene(world_scene)
-    # Autotuner: two sample tiles per bucket from the tiles not in the batch.
-    rest = [t for i, t in enumerate(all_tiles) if i not in set(pick)]
+    # Autotuner: two sample tiles per size bucket from the batch.
     sample, per = [], {}
-    for t in rest:
+    for t in tiles:
         b = native.tile_bucket(t)
         if per.get(b, 0) < 2:
             sample.append(t)
@@ -853,11 +849,14 @@ def tile_batch(args, rank, world, local):
             "value": paths / per_step_s, "unit": "paths/s", "cells_per_s": cells / per_step_s,
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-            "data": "synthetic (seeded road square and tiles)",
-            "config": {"workload": f"{args.tiles} of 4096 uneven tiles over the 1 km road square (sides log-uniform "
-                                   f"32-512 receivers at 1.875 m, "
-                                   f"10-50,000 point sources each): {cells} cells, {paths} paths per step, one "
-                                   "autotuned persistent launch per thread count, CUDA graph",
+            "data": "synthetic (seeded tiles, each its own roads and buildings)",
+            "config": {"workload": f"{args.tiles} of 4096 uneven tiles (sides log-uniform 32-512 receivers at "
+                                   "7.8125 m; each its own roads, log-uniform 10-50,000 segments at 1 m points, and "
+                                   "buildings, log-uniform 0-20,000 rectangles, in a region of its own; a tile's "
+                                   f"paths capped at 2^26 by a prefix of its roads): {cells} cells, {paths} paths per "
+                                   "step, one autotuned persistent launch per thread count, CUDA graph",
+                       "buildings": sum(t["buildings"] for t in tiles),
+                       "segments_kept": sum(t["kept_segments"] for t in tiles),
                        "l2": "flushed between steps", "tuned": cfg, "autotune_s": tune_s},
             "default_shape_paths_per_s": paths / (default_ms / 1e3),
             "one_call_per_tile": {"paths_per_s_device": paths / (one_ms / 1e3), "paths_per_s_wall": paths / one_wall,

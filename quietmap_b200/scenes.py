@@ -158,11 +158,17 @@ def _rings_to_arrays(polygons, heights, step_m, first_id=1):
     return vertices, _outlines(records)
 
 
-def _segments_to_points(rng, n_segments, side_m, step_m, kind_of, base_of, margin_m=1.0):
+def _segments_to_points(rng, n_segments, side_m, step_m, kind_of, base_of, margin_m=1.0, origin_m=(0.0, 0.0),
+                        max_points=None, kept=None):
     """Straight segments with ends uniform in the square, length clipped to [20, 200] m, split
-    into 1 m point sources at their piece centres (snapped to the lattice)."""
+    into 1 m point sources at their piece centres (snapped to the lattice). The square starts at
+    `origin_m`; past `max_points` points no further segment is added (`kept`, a list, receives
+    the count of segments kept)."""
     xs, ys, hs, energy, layers = [], [], [], [], []
+    total = 0
     for k in range(n_segments):
+        if max_points is not None and total >= max_points:
+            break
         a = rng.uniform(margin_m, side_m - margin_m, 2)
         b = rng.uniform(margin_m, side_m - margin_m, 2)
         d = b - a
@@ -179,7 +185,10 @@ def _segments_to_points(rng, n_segments, side_m, step_m, kind_of, base_of, margi
         shape = ROAD_SHAPE_DB if kind == 0 else RAIL_SHAPE_DB
         levels = base + shape + rng.normal(0.0, 2.0, 8)  # per metre, A-weighted
         f = (np.arange(count) + 0.5) / count
-        pts = a + f[:, None] * d
+        pts = a + f[:, None] * d + np.asarray(origin_m)
+        total += count
+        if kept is not None:
+            kept.append(k)
         xs.append(np.round(pts[:, 0] / step_m))
         ys.append(np.round(pts[:, 1] / step_m))
         piece_m = length / count
@@ -462,3 +471,87 @@ def loudness_pixels(n, seed=11, layers=6, profiles=12):
                 f += [np.nan] * 28 if rng.random() < 0.2 else list(rng.uniform(-60.0, 5.0, 28))
         out.append(np.array(f, dtype=np.float32))
     return out, shares, [4, 1, 3]
+
+
+# ---------------------------------------------------------------------------------------------
+# Uneven tiles, each with its own buildings and roads.
+
+TILE_SPACING_M = 7.8125  # the receivers' spacing of the road square
+
+
+def uneven_tile_specs(n_tiles=4096, seed=5, side=(32, 512), segments=(10, 50000), buildings=(0, 20000)):
+    """Per tile of a batch: receivers nx x ny (each side log-uniform in `side`), its count of road
+    segments (log-uniform in `segments`) and of buildings (log-uniform over 1 .. buildings[1] + 1,
+    less one, so 0 occurs), and its own seed. Cheap: a tile's geometry is drawn only when a batch
+    holding it is built (`uneven_tile_world`)."""
+    rng = np.random.default_rng(seed)
+    lu = lambda lo, hi: float(np.exp(rng.uniform(np.log(lo), np.log(hi))))
+    out = []
+    for _ in range(n_tiles):
+        nx, ny = int(round(lu(*side))), int(round(lu(*side)))
+        n_seg = int(round(lu(*segments)))
+        n_b = int(round(lu(buildings[0] + 1, buildings[1] + 1))) - 1
+        out.append(dict(nx=nx, ny=ny, segments=n_seg, buildings=n_b, seed=int(rng.integers(0, 2**31))))
+    return out
+
+
+def _tile_region_m(spec):
+    """A tile's square region: its receivers with 100 m around them, widened so that its buildings
+    (config-1 rectangles, 8-40 m sides) cover about a quarter of it."""
+    rec = (max(spec["nx"], spec["ny"]) - 1) * TILE_SPACING_M + 200.0
+    return max(rec, float(np.sqrt(spec["buildings"])) * 48.0)
+
+
+def uneven_tile_world(specs, max_paths_per_tile=1 << 28, step_m=1.0 / 32.0, cell_steps=1024):
+    """One scene holding each tile of `specs` in a square region of its own (on a grid of regions
+    the size of the largest, 200 m apart), drawn from the tile's seed as the road square is drawn:
+    its buildings (rotated rectangles, sides 8-40 m, heights 3-30 m, apart by rejection) and its
+    roads (ends uniform in the region, length clipped to 20-200 m, 1 m points at 0.05 m, base
+    level 70-100 dB plus the road tilt and N(0, 2 dB) a band); flat G = 0.5, homogeneous air. A
+    tile's receivers stand at 7.8125 m in the middle of its region and hear only its own sources
+    (a contiguous range). A tile whose cells x points would pass `max_paths_per_tile` keeps its
+    first roads up to that bound (independent draws, so a prefix is a sample of them). Returns
+    (scene, tiles as dicts for BatchPlan, each with `kept_segments`)."""
+    regions = [_tile_region_m(sp) for sp in specs]
+    cellm = max(regions) + 200.0
+    cols = int(np.ceil(np.sqrt(len(specs))))
+    rows = (len(specs) + cols - 1) // cols
+    spacing = int(round(TILE_SPACING_M / step_m))
+
+    def rect(rng):
+        sides = rng.uniform(8.0, 40.0, 2)
+        return _rectangle(rng, np.zeros(2), sides, rng.uniform(0, np.pi)), float(np.hypot(*sides) / 2)
+    verts, outls, srcs, tiles = [], [], [], []
+    n_vert = n_src = cell_offset = 0
+    first_id = 1
+    for k, sp in enumerate(specs):
+        rng = np.random.default_rng(sp["seed"])
+        side = regions[k]
+        ox, oy = 100.0 + (k % cols) * cellm, 100.0 + (k // cols) * cellm
+        polys = _place_buildings(rng, sp["buildings"], side, rect, 1.0, 1.0)
+        heights = rng.uniform(3.0, 30.0, len(polys))
+        v, o = _rings_to_arrays([p + np.array([ox, oy]) for p in polys], heights, step_m, first_id=first_id)
+        first_id += len(polys)
+        o["first_vertex"] += n_vert
+        n_vert += len(v)
+        verts.append(v)
+        outls.append(o)
+        cells = sp["nx"] * sp["ny"]
+        kept = []
+        src = _segments_to_points(rng, sp["segments"], side, step_m, lambda i: 0, lambda kind: rng.uniform(70.0, 100.0),
+                                  origin_m=(ox, oy), max_points=max(1, max_paths_per_tile // cells), kept=kept)
+        srcs.append(src)
+        rx0 = ox + side / 2 - (sp["nx"] - 1) * TILE_SPACING_M / 2
+        ry0 = oy + side / 2 - (sp["ny"] - 1) * TILE_SPACING_M / 2
+        tiles.append(dict(origin=(int(round(rx0 / step_m)), int(round(ry0 / step_m))), spacing=spacing, nx=sp["nx"],
+                          ny=sp["ny"], height_m=4.0, source_begin=n_src, source_end=n_src + len(src),
+                          cell_offset=cell_offset, kept_segments=len(kept), buildings=len(polys)))
+        n_src += len(src)
+        cell_offset += cells
+    extent = int(round((max(cols, rows) * cellm + 200.0) / step_m))
+    vertices = np.concatenate(verts) if verts else np.zeros((0, 2), np.int32)
+    scene = Scene(step_m=step_m, cell_steps=cell_steps, extent_steps=(extent, extent), vertices=vertices,
+                  outlines=np.concatenate(outls), sources=np.concatenate(srcs), favourable=np.zeros((3, 16)),
+                  alpha_db_per_km=alpha_bands(15.0, 70.0), flat_altitude_m=0.0, flat_ground_factor=0.5,
+                  name="uneven_tile_world", info=dict(tiles=len(specs)))
+    return scene, tiles
