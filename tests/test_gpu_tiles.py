@@ -104,3 +104,30 @@ def test_plans_mixing_thread_counts_keep_their_buffers(setup):
     again.run()
     assert np.array_equal(again.read()[1], ref_dba)
     again.close()
+
+
+def test_batch_of_tiles_each_with_its_own_roads_and_buildings():
+    """Config 4's tiles: each its own roads and buildings in a region of its own; the batch paints
+    them as one call per tile does, and a tile's levels come from its own scene only (a tile alone
+    in a world of its own paints the same)."""
+    ctx = native.Context(0)
+    specs = scenes.uneven_tile_specs(n_tiles=64, seed=11, side=(16, 48), segments=(10, 60), buildings=(0, 400))
+    world, tiles = scenes.uneven_tile_world(specs[:6], max_paths_per_tile=1 << 22)
+    assert sum(t["buildings"] for t in tiles) > 0
+    dev = ctx.scene(world)
+    n_cells = tiles[-1]["cell_offset"] + tiles[-1]["nx"] * tiles[-1]["ny"]
+    plan = native.BatchPlan(dev, tiles, n_cells=n_cells)
+    plan.run()
+    bands, dba, _ = plan.read()
+    ref_bands, ref_dba = _per_tile(dev, tiles, n_cells)
+    np.testing.assert_allclose(dba, ref_dba, atol=0.01)
+    np.testing.assert_allclose(bands, ref_bands, atol=0.01)
+    alone, alone_tiles = scenes.uneven_tile_world(specs[2:3], max_paths_per_tile=1 << 22)
+    t = alone_tiles[0]
+    g = scenes.Grid(origin=t["origin"], spacing=t["spacing"], nx=t["nx"], ny=t["ny"], source_begin=t["source_begin"],
+                    source_end=t["source_end"])
+    _, d_alone, _, _, _ = ctx.scene(alone).paint_grid(g, histogram=False)
+    o = tiles[2]["cell_offset"]
+    np.testing.assert_allclose(d_alone, dba[o:o + g.cells], atol=0.01)
+    plan.close()
+    ctx.close()
