@@ -513,7 +513,9 @@ def uneven_tile_world(specs, max_paths_per_tile=1 << 28, step_m=1.0 / 32.0, cell
     first roads up to that bound (independent draws, so a prefix is a sample of them). Returns
     (scene, tiles as dicts for BatchPlan, each with `kept_segments`)."""
     regions = [_tile_region_m(sp) for sp in specs]
-    cellm = max(regions) + 200.0
+    # Regions start on whole lattice steps, so a tile's geometry on the lattice is the same wherever
+    # its region lies.
+    cellm = float(np.ceil((max(regions) + 200.0) / step_m)) * step_m
     cols = int(np.ceil(np.sqrt(len(specs))))
     rows = (len(specs) + cols - 1) // cols
     spacing = int(round(TILE_SPACING_M / step_m))
