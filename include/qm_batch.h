@@ -154,6 +154,21 @@ qm_status qm_scene_upload(qm_ctx *ctx, const qm_scene_desc *desc, qm_scene **out
 /* Frees a scene; batch plans made on it stay usable, and it is released with the last of them. */
 void qm_scene_free(qm_scene *scene);
 
+/* A line piece candidate (a road or rail piece, popup/src/evaluate.rs:171-267 `source_rays` with
+ * physics/src/line.rs): its ends in lattice steps (fractional positions allowed) and its source
+ * properties as a point source has them, `energy` per metre of the piece; source.x and .y are not
+ * read. */
+typedef struct {
+    double a[2], b[2];
+    qm_source source;
+} qm_line_source;
+
+/* Sets a scene's line pieces: candidate k of qm_evaluate_pairs is point source k below the
+ * scene's n_sources and piece k - n_sources from there on. Builds the receivers' skyline index of
+ * the scene's outlines (popup/src/obstacles/skyline.rs, qm_skyline_build) on the device beside
+ * them. Replaces any pieces set before. */
+qm_status qm_scene_line_pieces(qm_scene *scene, const qm_line_source *pieces, size_t n_pieces);
+
 /* Batch::evaluate and Batch::pair_spectra (paint/src/exact.rs:164-170; GPU
  * `Gpu::evaluate_pairs`, paint-gpu/src/device.rs:440). Receivers at `receiver_xy`
  * (metres, snapped to the scene lattice), `receiver_height_m` above their ground,
@@ -163,7 +178,10 @@ void qm_scene_free(qm_scene *scene);
  * Outputs: pair_sums[n_pairs][9] = mixed[3], calm[3], downwind[3] (PairEnergy,
  * exact.rs:128-132); pair_bands (nullable) [n_pairs][3][8] each pair's unweighted bands
  * (pair_spectra); point_bands[n_points][6][3][8] += weighted bands by source layer
- * (add_bands, exact.rs:208-215); pair_status[n_pairs] failure bits. */
+ * (add_bands, exact.rs:208-215); pair_status[n_pairs] failure bits. A candidate at or past the
+ * scene's n_sources is a line piece (qm_scene_line_pieces): its pair sums its quadrature nodes'
+ * rays (each from its point along the piece, by the f64 walks, with the skyline's mask), as
+ * Point::line evaluation does (popup/src/evaluate.rs:171-267, paint-gpu/kernels/line.cuh). */
 qm_status qm_evaluate_pairs(qm_scene *scene,
                             const double *receiver_xy, const float *receiver_height_m,
                             const uint64_t *own_footprint, const uint32_t *point_of_receiver,

@@ -133,6 +133,8 @@ SOURCE_DTYPE = np.dtype(
     [("x", "<i4"), ("y", "<i4"), ("height_m", "<f4"), ("ground_factor", "<f4"),
      ("exclusion_radius_m", "<f4"), ("platform_half_width_m", "<f4"), ("footprint_id", "<u8"),
      ("layer", "<u4"), ("pad_", "<u4"), ("energy", "<f4", (PERIODS, BANDS))], align=True)
+# qm_line_source: a line piece candidate's ends (steps) and its source properties (energy per metre).
+LINE_SOURCE_DTYPE = np.dtype([("a", "<f8", (2,)), ("b", "<f8", (2,)), ("source", SOURCE_DTYPE)], align=True)
 
 AIRCRAFT_TYPE_DTYPE = np.dtype(
     [("sel_db", "<f4", (2, 10, 10)), ("lamax_db", "<f4", (2, 10, 10)), ("v_ref_kt", "<f4"), ("installation", "<u4"),

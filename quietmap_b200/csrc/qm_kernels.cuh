@@ -145,7 +145,8 @@ __global__ void __launch_bounds__(128, QM_PAINT_MIN_BLOCKS) paint_grid_kernel(Sc
                                                     r.edges_tested);
         if (!active) continue;
         if (r.status == 0) {
-            evaluate_listed<Caps::C, Caps::K, Caps::H>(S, src, rx, ry, alt, A.want_fav, work, nx, r);
+            evaluate_listed<Caps::C, Caps::K, Caps::H>(S, src, rx, ry, alt, A.want_fav, work, nx, r, (double)src.x,
+                                                       (double)src.y);
         } else {
             r.crossings = nx;
             r.vertices = 0;
@@ -442,6 +443,7 @@ template <class Caps>
 __global__ void __launch_bounds__(128) evaluate_pairs_kernel(SceneDev S, PairArgs A) {
     size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
     if (i >= A.n_pairs) return;
+    if (A.source_of_pair[i] >= S.n_sources) return;  // a line piece: the line pairs' kernel
     uint32_t r = A.receiver_of_pair[i];
     const SourceDev &src = S.sources[A.source_of_pair[i]];
     int2 xy = A.rcv_xy[r];

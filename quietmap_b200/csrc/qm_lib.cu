@@ -30,7 +30,13 @@
 #include "../../include/qm_weather.h"
 #include "qm_aircraft.cuh"
 #include "qm_kernels.cuh"
+#include "qm_linepairs.cuh"
 #include "qm_host.h"
+#include "../../include/qm_line.h"
+
+namespace qm {
+skyline::Index skyline_view(const qm_skyline *s);
+}
 #include "qm_mlp.h"
 #include "qm_percentile.cuh"
 #include "qm_pixel.cuh"
@@ -94,11 +100,19 @@ struct qm_scene {
     std::vector<uint32_t> source_layer;
     bool any_favourable;
     size_t n_edges_listed;
+    // Line pieces (qm_scene_line_pieces): candidates n_sources .. n_sources + n_pieces - 1, and the
+    // receivers' skyline index on the device; replaced whole when set again.
+    uint32_t n_pieces = 0;
+    std::vector<uint32_t> piece_layer;
+    const qm::PieceDev *pieces = nullptr;
+    qm::skyline::Index sky{};
+    std::vector<DeviceBuffer *> piece_buffers;
     // Batch plans made on the scene hold it: qm_scene_free releases it once they are freed.
     int plans = 0;
     bool freed = false;
     ~qm_scene() {
         for (auto *b : buffers) delete b;
+        for (auto *b : piece_buffers) delete b;
     }
 };
 
@@ -755,6 +769,88 @@ qm_status qm_paint_grid(qm_scene *scene, const qm_grid_desc *grid, float *cell_b
     return QM_OK;
 }
 
+qm_status qm_scene_line_pieces(qm_scene *scene, const qm_line_source *pieces, size_t n_pieces) {
+    if (!scene) return fail(QM_ERR_ARGUMENT, "qm_scene_line_pieces: null scene");
+    if (n_pieces && !pieces) return fail(QM_ERR_ARGUMENT, "qm_scene_line_pieces: null pieces");
+    if ((uint64_t)scene->n_sources + n_pieces > 0xFFFFFFFFull)
+        return fail(QM_ERR_ARGUMENT, "qm_scene_line_pieces: too many candidates");
+    std::vector<PieceDev> dev(n_pieces);
+    std::vector<uint32_t> layers(n_pieces);
+    for (size_t k = 0; k < n_pieces; ++k) {
+        const qm_line_source &p = pieces[k];
+        for (int e = 0; e < 2; ++e)
+            if (!std::isfinite(p.a[e]) || !std::isfinite(p.b[e]) || p.a[e] < 0.0 || p.b[e] < 0.0 ||
+                p.a[e] >= scene->extent[e] || p.b[e] >= scene->extent[e])
+                return fail(QM_ERR_ARGUMENT, "qm_scene_line_pieces: piece " + std::to_string(k) +
+                                                 " has an end outside the scene extent");
+        if (p.source.layer >= QM_LAYERS)
+            return fail(QM_ERR_ARGUMENT, "qm_scene_line_pieces: piece " + std::to_string(k) + " names layer " +
+                                             std::to_string(p.source.layer));
+        PieceDev &d = dev[k];
+        d.ax = p.a[0];
+        d.ay = p.a[1];
+        d.bx = p.b[0];
+        d.by = p.b[1];
+        d.src.x = (int32_t)std::llround(p.a[0]);
+        d.src.y = (int32_t)std::llround(p.a[1]);
+        d.src.height = p.source.height_m;
+        d.src.gf = p.source.ground_factor;
+        d.src.excl = p.source.exclusion_radius_m;
+        d.src.platform = p.source.platform_half_width_m;
+        d.src.fp = dense_fp(scene, p.source.footprint_id);
+        d.src.layer = p.source.layer;
+        for (int q = 0; q < 3; ++q)
+            for (int b = 0; b < 8; ++b) d.src.energy[q * 8 + b] = p.source.energy[q][b];
+        layers[k] = p.source.layer;
+    }
+    // The receivers' skyline index of the scene's outlines, built on the host and copied as is.
+    qm_skyline *sky = nullptr;
+    qm_status st = qm_skyline_build(scene->vertices.data(), scene->vertices.size() / 2, scene->outlines.data(),
+                                    scene->outlines.size(), scene->step_m, &sky);
+    if (st != QM_OK) return fail(st, std::string("qm_scene_line_pieces: ") + qm::last_error());
+    const qm::skyline::Index host = qm::skyline_view(sky);
+    std::lock_guard<std::mutex> guard(scene->ctx->lock);
+    QM_CUDA(cudaSetDevice(scene->ctx->device));
+    for (auto *b : scene->piece_buffers) delete b;
+    scene->piece_buffers.clear();
+    scene->n_pieces = 0;
+    auto put = [&](const void *data, size_t bytes, const void **out) -> qm_status {
+        auto *b = new DeviceBuffer();
+        scene->piece_buffers.push_back(b);
+        b->bytes = std::max<size_t>(bytes, 16);
+        QM_CUDA(cudaMalloc(&b->ptr, b->bytes));
+        if (bytes) QM_CUDA(cudaMemcpy(b->ptr, data, bytes, cudaMemcpyHostToDevice));
+        *out = b->ptr;
+        return QM_OK;
+    };
+    const size_t n_cells = host.n_cells, n_runs = n_cells ? host.run_start[n_cells] : 0;
+    qm::skyline::Index d = host;
+    const void *p_keys, *p_start, *p_tall, *p_runs, *p_outl, *p_pieces;
+    std::vector<uint32_t> start_copy(n_cells + 1, 0u);
+    if (n_cells) std::copy(host.run_start, host.run_start + n_cells + 1, start_copy.begin());
+    if ((st = put(host.keys, n_cells * sizeof(uint64_t), &p_keys)) != QM_OK ||
+        (st = put(start_copy.data(), start_copy.size() * sizeof(uint32_t), &p_start)) != QM_OK ||
+        (st = put(host.tallest, n_cells * sizeof(float), &p_tall)) != QM_OK ||
+        (st = put(host.runs, n_runs * sizeof(qm::skyline::Run), &p_runs)) != QM_OK ||
+        (st = put(scene->outlines.data(), scene->outlines.size() * sizeof(qm_outline), &p_outl)) != QM_OK ||
+        (st = put(dev.data(), dev.size() * sizeof(PieceDev), &p_pieces)) != QM_OK) {
+        qm_skyline_free(sky);
+        return st;
+    }
+    qm_skyline_free(sky);
+    d.keys = static_cast<const uint64_t *>(p_keys);
+    d.run_start = static_cast<const uint32_t *>(p_start);
+    d.tallest = static_cast<const float *>(p_tall);
+    d.runs = static_cast<const qm::skyline::Run *>(p_runs);
+    d.outlines = static_cast<const qm_outline *>(p_outl);
+    d.vertices = reinterpret_cast<const int32_t *>(scene->dev.vertices);
+    scene->sky = d;
+    scene->pieces = static_cast<const PieceDev *>(p_pieces);
+    scene->piece_layer = layers;
+    scene->n_pieces = (uint32_t)n_pieces;
+    return QM_OK;
+}
+
 qm_status qm_evaluate_pairs(qm_scene *scene, const double *receiver_xy, const float *receiver_height_m,
                             const uint64_t *own_footprint, const uint32_t *point_of_receiver, size_t n_receivers,
                             const uint32_t *source_of_pair, const uint32_t *receiver_of_pair, const float *band_weight,
@@ -780,7 +876,7 @@ qm_status qm_evaluate_pairs(qm_scene *scene, const double *receiver_xy, const fl
         rown[r] = dense_fp(scene, own_footprint[r]);
     }
     for (size_t i = 0; i < n_pairs; ++i)
-        if (source_of_pair[i] >= scene->n_sources || receiver_of_pair[i] >= n_receivers)
+        if ((uint64_t)source_of_pair[i] >= (uint64_t)scene->n_sources + scene->n_pieces || receiver_of_pair[i] >= n_receivers)
             return fail(QM_ERR_ARGUMENT,
                         "qm_evaluate_pairs: a candidate outside the square, a receiver outside the receivers");
     if (n_pairs == 0) return QM_OK;
@@ -792,7 +888,8 @@ qm_status qm_evaluate_pairs(qm_scene *scene, const double *receiver_xy, const fl
     std::vector<uint32_t> order(n_pairs), layer(n_pairs);
     for (size_t i = 0; i < n_pairs; ++i) {
         order[i] = (uint32_t)i;
-        layer[i] = scene->source_layer[source_of_pair[i]];
+        const uint32_t c = source_of_pair[i];
+        layer[i] = c < scene->n_sources ? scene->source_layer[c] : scene->piece_layer[c - scene->n_sources];
     }
     std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) {
         return point_of_receiver[receiver_of_pair[a]] < point_of_receiver[receiver_of_pair[b]];
@@ -848,14 +945,48 @@ qm_status qm_evaluate_pairs(qm_scene *scene, const double *receiver_xy, const fl
     else
         evaluate_pairs_kernel<CapsFlat><<<blocks, 128, 0, stream>>>(scene->dev, A);
     QM_CUDA(cudaGetLastError());
+    // Line pieces: one thread a (receiver, piece) pair over the piece's quadrature nodes.
+    std::vector<uint32_t> line_pairs;
+    for (size_t i = 0; i < n_pairs; ++i)
+        if (source_of_pair[i] >= scene->n_sources) line_pairs.push_back((uint32_t)i);
+    Scratch d_lines;
+    LinePairArgs LA{};
+    LA.pieces = scene->pieces;
+    LA.sky = scene->sky;
+    if (!line_pairs.empty()) {
+        QM_CUDA(cudaMalloc(&d_lines.p, line_pairs.size() * sizeof(uint32_t)));
+        QM_CUDA(cudaMemcpyAsync(d_lines.p, line_pairs.data(), line_pairs.size() * sizeof(uint32_t),
+                                cudaMemcpyHostToDevice, stream));
+        LA.line_pairs = static_cast<uint32_t *>(d_lines.p);
+        LA.n_line_pairs = (uint32_t)line_pairs.size();
+        const unsigned line_blocks = (unsigned)((line_pairs.size() + 127) / 128);
+        if (terrain_caps(scene))
+            evaluate_line_pairs_kernel<CapsTerrain><<<line_blocks, 128, 0, stream>>>(scene->dev, A, LA);
+        else
+            evaluate_line_pairs_kernel<CapsFlat><<<line_blocks, 128, 0, stream>>>(scene->dev, A, LA);
+        QM_CUDA(cudaGetLastError());
+    }
     // Pairs over the per-path capacities again with large ones (global scratch work areas).
     std::vector<uint32_t> status_host(n_pairs);
     QM_CUDA(cudaMemcpyAsync(status_host.data(), d_status.p, n_pairs * sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
     QM_CUDA(cudaStreamSynchronize(stream));
-    std::vector<uint32_t> again;
+    std::vector<uint32_t> again, again_lines;
     for (size_t i = 0; i < n_pairs; ++i)
-        if (status_host[i] & QM_FAILED_CAPACITY) again.push_back((uint32_t)i);
-    Scratch d_again, d_works;
+        if (status_host[i] & QM_FAILED_CAPACITY)
+            (source_of_pair[i] < scene->n_sources ? again : again_lines).push_back((uint32_t)i);
+    Scratch d_again, d_works, d_again_lines, d_line_works;
+    if (!again_lines.empty()) {
+        using Large = PathWork<CapsLarge::C, CapsLarge::K, CapsLarge::H>;
+        const uint32_t threads = std::min<uint32_t>(((uint32_t)again_lines.size() + 63) / 64 * 64, 4096);
+        QM_CUDA(cudaMalloc(&d_again_lines.p, again_lines.size() * sizeof(uint32_t)));
+        QM_CUDA(cudaMalloc(&d_line_works.p, (size_t)threads * sizeof(Large)));
+        QM_CUDA(cudaMemcpyAsync(d_again_lines.p, again_lines.data(), again_lines.size() * sizeof(uint32_t),
+                                cudaMemcpyHostToDevice, stream));
+        retry_line_pairs_kernel<<<threads / 64, 64, 0, stream>>>(scene->dev, A, LA, static_cast<uint32_t *>(d_again_lines.p),
+                                                                 (uint32_t)again_lines.size(),
+                                                                 static_cast<Large *>(d_line_works.p));
+        QM_CUDA(cudaGetLastError());
+    }
     if (!again.empty()) {
         using Large = PathWork<CapsLarge::C, CapsLarge::K, CapsLarge::H>;
         const uint32_t threads = std::min<uint32_t>(((uint32_t)again.size() + 63) / 64 * 64, 8192);

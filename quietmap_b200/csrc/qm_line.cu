@@ -210,3 +210,9 @@ void qm_skyline_query(double wedge_lo_rad, double wedge_hi_rad, double radius_m,
 }
 
 }  // extern "C"
+
+namespace qm {
+// The index's host arrays (the library uploads them for the device's line pairs); the run count is
+// run_start[n_cells].
+skyline::Index skyline_view(const qm_skyline *s) { return s->view(); }
+}  // namespace qm

@@ -925,20 +925,28 @@ __device__ __forceinline__ float favourable_at(const float row[QM_SECTORS], floa
     return row[lower] + fraction * (row[upper] - row[lower]);
 }
 
+// A walk's start: the lattice walk from the source's lattice point, the f64 walk
+// (qm_offlattice.cuh) from its fractional position.
+__device__ __forceinline__ void start_walk(TerrainWalk &walk, const SceneDev &S, double, double, int sx, int sy, int rx,
+                                           int ry, float L) {
+    walk.init(S, sx, sy, rx, ry, L);
+}
+
 // The rest of a path once its crossings are listed in w.xs[0, nx): terrain, roofs, both states'
 // bands and boundaries, slant, divergence and p. out.status and out.edges_tested hold what the
-// listing set.
-template <int CAP_C, int CAP_K, int CAP_H>
+// listing set. The ray starts at (sxd, syd) steps: the source's lattice point for a point source,
+// a quadrature node's fractional position with the f64 walk (Walk = TerrainWalkD) for a line.
+template <int CAP_C, int CAP_K, int CAP_H, class Walk = TerrainWalk>
 __device__ void evaluate_listed(const SceneDev &S, const SourceDev &src, int rx, int ry, float rcv_alt, bool want_fav,
-                                PathWork<CAP_C, CAP_K, CAP_H> &w, int nx, PathResult &out) {
+                                PathWork<CAP_C, CAP_K, CAP_H> &w, int nx, PathResult &out, double sxd, double syd) {
     const int sx = src.x, sy = src.y;
-    const float dxm = (float)(rx - sx) * S.step_m, dym = (float)(ry - sy) * S.step_m;
+    const float dxm = (float)((double)rx - sxd) * S.step_m, dym = (float)((double)ry - syd) * S.step_m;
     const float dist = sqrtf(dxm * dxm + dym * dym);
     const float L = fmaxf(dist, 1.0f);
     out.crossings = nx;
     // Pass 1: terrain heights and G at the crossings, and the crests (physics/src/ray.rs:255-309).
-    TerrainWalk walk;
-    walk.init(S, sx, sy, rx, ry, L);
+    Walk walk;
+    start_walk(walk, S, sxd, syd, sx, sy, rx, ry, L);
     const float z0 = walk.start_zg.x, g0 = walk.start_zg.y;
     const float source_ground = z0;
     const float platform = src.platform;
@@ -1075,7 +1083,7 @@ __device__ void evaluate_listed(const SceneDev &S, const SourceDev &src, int rx,
     if (want_fav) fav.init(w.hull[1], Sp, Rp, z0, g0);
     Moments total = moments_zero();
     {
-        walk.init(S, sx, sy, rx, ry, L);
+        start_walk(walk, S, sxd, syd, sx, sy, rx, ry, L);
         // Profile stream state: pending roof vertices, covered_to, current terrain vertex.
         TV vprev, tv;
         walk.next(S, tv);  // x = 0
@@ -1229,7 +1237,7 @@ __device__ void evaluate_path(const SceneDev &S, const SourceDev &src, int rx, i
     out.status = 0;
     out.edges_tested = 0;
     const int nx = list_crossings<CAP_C>(S, src.x, src.y, rx, ry, rcv_own, w.xs, out.status, out.edges_tested);
-    evaluate_listed<CAP_C, CAP_K, CAP_H>(S, src, rx, ry, rcv_alt, want_fav, w, nx, out);
+    evaluate_listed<CAP_C, CAP_K, CAP_H>(S, src, rx, ry, rcv_alt, want_fav, w, nx, out, (double)src.x, (double)src.y);
 }
 
 }  // namespace qm

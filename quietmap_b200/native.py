@@ -52,6 +52,8 @@ def lib():
         L.qm_evaluate_pairs.argtypes = [C.c_void_p, _D, _F, _U64, _U32, C.c_size_t, _U32, _U32, _F, C.c_size_t,
                                         _F, _F, _U32, _F, C.c_size_t]
         L.qm_evaluate_pairs.restype = C.c_int
+        L.qm_scene_line_pieces.argtypes = [C.c_void_p, C.c_void_p, C.c_size_t]
+        L.qm_scene_line_pieces.restype = C.c_int
         L.qm_paint_grid.argtypes = [C.c_void_p, C.POINTER(abi.GridDesc), _F, _F, _F, _U32,
                                     C.POINTER(abi.PaintStats)]
         L.qm_paint_grid.restype = C.c_int
@@ -832,6 +834,13 @@ class DeviceScene:
                                        abi.ptr(status, C.c_uint32), abi.ptr(point_bands, C.c_float), n_points),
                self.ctx.handle)
         return sums, bands, status, point_bands
+
+    def line_pieces(self, pieces):
+        """Sets the scene's line pieces (qm_scene_line_pieces, LINE_SOURCE_DTYPE records): candidate
+        n_sources + k of evaluate_pairs is piece k."""
+        arr = np.ascontiguousarray(pieces, dtype=abi.LINE_SOURCE_DTYPE)
+        _check(lib().qm_scene_line_pieces(self.handle, arr.ctypes.data if len(arr) else None, len(arr)),
+               self.ctx.handle)
 
     def list_crossings(self, frm, to, cap=256):
         frm = np.ascontiguousarray(np.asarray(frm).reshape(-1, 2), dtype=np.int32)
