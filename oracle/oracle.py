@@ -130,6 +130,25 @@ def lib():
                                             C.POINTER(C.c_uint8), C.c_int]
         L.qmo_flight_grid.argtypes = [C.c_void_p, C.c_uint32, C.c_void_p, C.c_size_t, C.POINTER(abi.FlightGridDesc),
                                       C.c_uint32, C.c_uint32, _D, _D, _D, C.c_int]
+        for name in ("qmo_path_difference_loss_db",):
+            getattr(L, name).argtypes = [C.c_double]
+            getattr(L, name).restype = C.c_double
+        for name in ("qmo_edge_loss_db", "qmo_screened_sel_db"):
+            getattr(L, name).argtypes = [C.c_double] * 4
+            getattr(L, name).restype = C.c_double
+        L.qmo_flight_weight.argtypes = [C.c_uint32, C.c_double, C.c_double]
+        L.qmo_flight_weight.restype = C.c_double
+        L.qmo_horizon_loss_db.argtypes = [C.POINTER(C.c_float), C.c_int, _D]
+        L.qmo_horizon_loss_db.restype = C.c_double
+        L.qmo_segment_sel_db.argtypes = [C.c_void_p, C.c_void_p, C.c_double, C.c_double, C.c_double]
+        L.qmo_segment_sel_db.restype = C.c_double
+        L.qmo_box_sums.argtypes = [C.c_void_p, C.c_void_p, C.c_size_t, _D, C.c_void_p]
+        L.qmo_box_sums.restype = C.c_int
+        L.qmo_box_sel.argtypes = [C.c_void_p, C.c_void_p, C.POINTER(C.c_float), _D, _D]
+        L.qmo_box_sel.restype = None
+        L.qmo_flight_sums.argtypes = [C.c_void_p, C.c_void_p, C.POINTER(C.c_float), C.c_void_p, C.c_size_t, _D,
+                                      C.c_size_t, C.c_int]
+        L.qmo_flight_sums.restype = C.c_uint64
         _lib = L
     return _lib
 
@@ -617,3 +636,71 @@ def flight_grid(flights, cell_begin=0, cell_end=0, grid=None, nthreads=None):
                           cell_end, abi.ptr(lae, C.c_double), abi.ptr(thirds, C.c_double), abi.ptr(sone, C.c_double),
                           nthreads or threads())
     return lae, thirds, sone
+
+
+# ---------------------------------------------------------------------------------------------
+# Aircraft boxes (physics/src/doc29/{box_sums,boxes,screening}.rs, popup/src/aircraft/{boxes,horizons}.rs,
+# paint/src/flight_boxes.rs)
+
+def path_difference_loss_db(delta_m):
+    return lib().qmo_path_difference_loss_db(delta_m)
+
+
+def edge_loss_db(edge_range_m, edge_height_m, source_range_m, source_height_m):
+    return lib().qmo_edge_loss_db(edge_range_m, edge_height_m, source_range_m, source_height_m)
+
+
+def screened_sel_db(free_db, lateral_db, terrain_db, building_db):
+    return lib().qmo_screened_sel_db(free_db, lateral_db, terrain_db, building_db)
+
+
+def flight_weight(kind, distance_m, coarse_m):
+    return lib().qmo_flight_weight(kind, distance_m, coarse_m)
+
+
+def horizon_loss_db(floats, sectors, point_m):
+    f = np.ascontiguousarray(floats, dtype=np.float32)
+    p = _d(point_m)
+    return lib().qmo_horizon_loss_db(abi.ptr(f, C.c_float), sectors, abi.ptr(p, C.c_double))
+
+
+def segment_sel_db(aircraft_type, segment, receiver_m):
+    t = np.ascontiguousarray(np.atleast_1d(aircraft_type), dtype=abi.AIRCRAFT_TYPE_DTYPE)
+    g = np.ascontiguousarray(np.atleast_1d(segment), dtype=abi.FLIGHT_SEGMENT_DTYPE)
+    rx, ry, rz = (float(v) for v in receiver_m)
+    return lib().qmo_segment_sel_db(t.ctypes.data, g.ctypes.data, rx, ry, rz)
+
+
+def box_sums(types, pieces, period_weights):
+    """The box of `pieces` (FLIGHT_SEGMENT_DTYPE, each of types[piece.type]) weighted per period by
+    period_weights [n][3], as the builder closes it; None for a box without energy."""
+    t = np.ascontiguousarray(types, dtype=abi.AIRCRAFT_TYPE_DTYPE)
+    g = np.ascontiguousarray(np.atleast_1d(pieces), dtype=abi.FLIGHT_SEGMENT_DTYPE)
+    w = _d(np.asarray(period_weights, dtype=np.float64).reshape(len(g), 3))
+    out = np.zeros(1, dtype=abi.FLIGHT_BOX_DTYPE)
+    if not lib().qmo_box_sums(t.ctypes.data, g.ctypes.data, len(g), abi.ptr(w, C.c_double), out.ctypes.data):
+        return None
+    return out[0]
+
+
+def box_sel(box, point, horizons=None):
+    """(sel_energy [3], installation fractions [3][3]) of one box at one point."""
+    b = np.ascontiguousarray(np.atleast_1d(box), dtype=abi.FLIGHT_BOX_DTYPE)
+    p = np.ascontiguousarray(np.atleast_1d(point), dtype=abi.FLIGHT_POINT_DTYPE)
+    h = None if horizons is None else np.ascontiguousarray(horizons, dtype=np.float32)
+    sel, fractions = np.zeros(3), np.zeros((3, 3))
+    lib().qmo_box_sel(b.ctypes.data, p.ctypes.data, None if h is None else abi.ptr(h, C.c_float),
+                      abi.ptr(sel, C.c_double), abi.ptr(fractions, C.c_double))
+    return sel, fractions
+
+
+def flight_sums(boxes, points, horizons, segments, n_sums, nthreads=None):
+    """sums [n_sums][FLIGHT_SUMS] of every request band and the number of boxes heard."""
+    b = np.ascontiguousarray(boxes, dtype=abi.FLIGHT_BOX_DTYPE)
+    p = np.ascontiguousarray(points, dtype=abi.FLIGHT_POINT_DTYPE)
+    h = None if horizons is None else np.ascontiguousarray(horizons, dtype=np.float32)
+    s = np.ascontiguousarray(segments, dtype=abi.BOX_SEGMENT_DTYPE)
+    sums = np.zeros((n_sums, abi.FLIGHT_SUMS))
+    heard = lib().qmo_flight_sums(b.ctypes.data, p.ctypes.data, None if h is None else abi.ptr(h, C.c_float),
+                                  s.ctypes.data, len(s), abi.ptr(sums, C.c_double), n_sums, nthreads or threads())
+    return sums, heard

@@ -143,6 +143,30 @@ FLIGHT_SEGMENT_DTYPE = np.dtype(
     [("start", "<f4", (3,)), ("end", "<f4", (3,)), ("power", "<f4"), ("speed_mps", "<f4"), ("type", "<u4"),
      ("departure", "<u4"), ("flight", "<u4"), ("pad_", "<u4")], align=True)
 
+# include/qm_flights.h: a square's aircraft boxes, lattice points and their segments of boxes.
+PASS_CLASSES = 48
+FLIGHT_SUMS = PERIODS + 2 * PERIODS * PASS_CLASSES
+TERRAIN_SECTORS, BUILDING_SECTORS, HORIZON_BANDS = 32, 256, 6
+TERRAIN_HORIZON_FLOATS = 1 + TERRAIN_SECTORS * (1 + 2 * HORIZON_BANDS)
+HORIZON_FLOATS = TERRAIN_HORIZON_FLOATS + 1 + BUILDING_SECTORS * (1 + 2 * HORIZON_BANDS)
+FLIGHT_WEIGHT_ONE, FLIGHT_WEIGHT_FAR, FLIGHT_WEIGHT_NEAR = 0, 1, 2
+FLIGHT_BOX_DTYPE = np.dtype(
+    [("east_m", "<f8"), ("north_m", "<f8"), ("centroid_altitude_m", "<f8"), ("ground_m", "<f8"), ("axis_rad", "<f8"),
+     ("gradient", "<f8"), ("gradient_spread", "<f8"), ("piece_length_m", "<f8", (PERIODS,)),
+     ("levels_db", "<f8", (PERIODS, 10)), ("tail_levels_db", "<f8", (PERIODS,)), ("lg_scaled_distance", "<f8", (10,)),
+     ("installation_shares", "<f8", (PERIODS, 2, 3)), ("passing", "<f8", (PERIODS,)), ("helicopter", "<u4"),
+     ("pad_", "<u4")], align=True)
+FLIGHT_POINT_DTYPE = np.dtype(
+    [("x", "<f8"), ("y", "<f8"), ("altitude_m", "<f8"), ("horizons", "<u8"), ("impedance_gain", "<f8")], align=True)
+BOX_SEGMENT_DTYPE = np.dtype(
+    [("within_m", "<f8"), ("coarse_m", "<f8"), ("point", "<u4"), ("sum", "<u4"), ("first", "<u4"), ("count", "<u4"),
+     ("weight", "<u4"), ("pad_", "<u4")], align=True)
+assert FLIGHT_BOX_DTYPE.itemsize == 600 and FLIGHT_POINT_DTYPE.itemsize == 40 and BOX_SEGMENT_DTYPE.itemsize == 40
+
+
+class FlightSumsStats(C.Structure):
+    _fields_ = [("box_reads", C.c_uint64), ("boxes_heard", C.c_uint64), ("kernel_ms", C.c_double)]
+
 
 LINE_NODE_DTYPE = np.dtype([("along_m", "<f8"), ("weight_rad", "<f8"), ("obstacles_on_ray", "<u4"),
                             ("reserved", "<u4")], align=True)
