@@ -62,10 +62,13 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="terrain", choices=["terrain", "road", "flights", "surrogate", "surrogate_terrain", "tiles", "loudness"])
+    ap.add_argument("--workload", default="terrain", choices=["terrain", "road", "flights", "surrogate", "surrogate_terrain", "tiles", "loudness",
+                             "flight_sums"])
     ap.add_argument("--tiles", type=int, default=32, help="tiles workload: tiles per batch, drawn from the 4096")
     ap.add_argument("--flights", type=int, default=2000, help="flights workload: flights (a small case for profiling)")
     ap.add_argument("--cells-side", type=int, default=1024, help="flights workload: receivers per side")
+    ap.add_argument("--lattice-side", type=int, default=64,
+                    help="flight_sums workload: lattice points per side of the square")
     ap.add_argument("--slices", type=int, default=8, help="terrain: source-list slices (a step paints one)")
     ap.add_argument("--sources", type=int, default=0,
                     help="paint only the first N sources (a small case for profiling; 0: all)")
@@ -281,6 +284,8 @@ def main():
         return tile_batch(args, rank, world, local)
     if args.workload == "loudness":
         return loudness(args, rank, world, local)
+    if args.workload == "flight_sums":
+        return flight_sums(args, rank, world, local)
     import torch
     from quietmap_b200 import native
     scene, steps, desc = workload(args.workload, rank, args.slices, args.sources)
@@ -787,6 +792,79 @@ def loudness(args, rank, world, local):
                               "zero_where_host_zero": bool(np.all(got[:m][want == 0] == 0))}
         print(json.dumps(line), flush=True)
     ctx.close()
+
+
+def flight_sums(args, rank, world, local):
+    """Batch::flight_sums on the device: the flight workload's square (2000 flights x 50 segments over
+    1024^2 cells at 100 m) summed into 400 m and 1,600 m boxes, asked at a lattice of points with their
+    horizons (every aircraft tile within 16 km, its fine boxes within 3 km); a step is one call for
+    every point."""
+    import torch
+    from quietmap_b200 import native, scenes
+    world_boxes = scenes.flight_boxes_square(seed=3 + rank, n_flights=args.flights, receivers=args.cells_side)
+    n = args.lattice_side
+    xs = (np.arange(n) + 0.5) * world_boxes.side_m / n
+    xy = np.stack(np.meshgrid(xs, xs), -1).reshape(-1, 2)
+    points, hz, segs, n_sums = scenes.flight_requests(world_boxes, xy, seed=5 + rank)
+    ctx = native.Context(local if world > 1 else 0)
+    torch.cuda.set_device(local if world > 1 else 0)
+    dev = ctx.flight_boxes(world_boxes.boxes)
+    for _ in range(args.warmup):
+        dev.sums(points, hz, segs, n_sums)
+    torch.cuda.synchronize()
+    k_ms, wall, reads, heard = 0.0, 0.0, 0, 0
+    with ClockSampler(local) as clocks:
+        for _ in range(args.steps):
+            t0 = time.perf_counter()
+            got, st = dev.sums(points, hz, segs, n_sums, stats=True)
+            wall += time.perf_counter() - t0
+            k_ms += st["kernel_ms"]
+            reads += st["box_reads"]
+            heard += st["boxes_heard"]
+    if rank == 0:
+        n_pts = len(points)
+        line = {
+            "metric": "Batch::flight_sums points/s (aircraft boxes within 16 km summed with pass classes), 1 B200",
+            "value": n_pts * args.steps / (k_ms / 1e3), "unit": "points/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": k_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded flights, NPD tables and horizons)",
+            "config": {"workload": f"{n}^2 lattice points over the {args.cells_side * 0.1:.1f} km square of "
+                                   f"{args.flights} flights x 50 segments, {len(world_boxes.boxes)} boxes",
+                       "box_reads_per_step": reads // args.steps, "boxes_heard_per_step": heard // args.steps,
+                       "l2": "boxes resident (the square's boxes are decoded once and read by every point)"},
+            "box_reads_per_s": reads / (k_ms / 1e3), "boxes_heard_per_s": heard / (k_ms / 1e3),
+            "e2e": {"value": n_pts * args.steps / wall, "unit": "points/s",
+                    "h2d_bytes_per_step": points.nbytes + hz.nbytes + segs.nbytes,
+                    "d2h_bytes_per_step": n_sums * abi_flight_sums() * 8},
+            "clocks": clocks.summary(), "gpu_launches": args.steps,
+        }
+        if not args.no_cpu_baseline and world == 1:
+            from oracle import oracle
+            threads = oracle.threads()
+            m = 8
+            pick = np.random.default_rng(43).permutation(n_pts)
+            for _ in range(2):
+                mine = np.isin(segs["point"], pick[:m])
+                t0 = time.perf_counter()
+                want, _ = oracle.flight_sums(world_boxes.boxes, points, hz, segs[mine], n_sums, threads)
+                dt = time.perf_counter() - t0
+                if dt > 6.0 or m >= n_pts:
+                    break
+                m = min(n_pts, max(m, int(m * 12.0 / max(dt, 1e-3))))
+            rows = np.concatenate([2 * pick[:m], 2 * pick[:m] + 1])
+            scale = np.maximum(np.abs(want[rows]), 1e-300)
+            rel = np.where(want[rows] != 0.0, np.abs(got[rows] - want[rows]) / scale, np.abs(got[rows]))
+            line["cpu_baseline"] = dict(value=m / dt, unit="points/s", cores=threads, kind="port",
+                                        sample=f"{m} of the lattice's points, every box they hear ({dt:.1f} s)")
+            line["parity"] = {"points": m, "max_relative_error": float(rel.max())}
+        print(json.dumps(line), flush=True)
+    dev.close()
+    ctx.close()
+
+
+def abi_flight_sums():
+    from quietmap_b200 import abi
+    return abi.FLIGHT_SUMS
 
 
 def tile_batch(args, rank, world, local):

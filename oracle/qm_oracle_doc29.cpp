@@ -537,7 +537,9 @@ double flight_weight(uint32_t kind, double distance_m, double coarse_m) {
 void add_pass(double *class_energy, double *class_passing, int period, double e, double passing) {
     if (e <= 0.0 || passing <= 0.0) return;
     double level = 10.0 * std::log10(e / passing);
-    int c = std::min((int)std::max((level - PASS_LOWEST_DB) / PASS_CLASS_DB, 0.0), PASS_CLASSES - 1);
+    // Rust's float-to-integer cast saturates: a level past the top class (an infinite one too) is the top class.
+    double at = std::max((level - PASS_LOWEST_DB) / PASS_CLASS_DB, 0.0);
+    int c = at >= (double)(PASS_CLASSES - 1) ? PASS_CLASSES - 1 : (int)at;
     class_energy[period * PASS_CLASSES + c] += e;
     class_passing[period * PASS_CLASSES + c] += passing;
 }

@@ -29,6 +29,7 @@
 #include "../../include/qm_tiles.h"
 #include "../../include/qm_weather.h"
 #include "qm_aircraft.cuh"
+#include "qm_flights.cuh"
 #include "qm_kernels.cuh"
 #include "qm_linepairs.cuh"
 #include "qm_host.h"
@@ -1662,6 +1663,228 @@ extern "C" qm_status qm_flight_grid(qm_ctx *ctx, const qm_aircraft_type *types, 
         stats->pairs_in_reach = pairs_in_reach;
         stats->kernel_ms = k_ms;
         stats->loudness_ms = sone ? z_ms : 0.0;
+    }
+    return QM_OK;
+}
+
+// ---------------------------------------------------------------------------------------------
+// A square's aircraft boxes at lattice points (include/qm_flights.h).
+
+namespace {
+
+// A device buffer that grows to the largest size asked of it and is kept between calls.
+struct GrowBuffer {
+    void *p = nullptr;
+    size_t bytes = 0;
+    GrowBuffer() = default;
+    GrowBuffer(const GrowBuffer &) = delete;
+    GrowBuffer &operator=(const GrowBuffer &) = delete;
+    ~GrowBuffer() {
+        if (p) cudaFree(p);
+    }
+    cudaError_t reserve(size_t want) {
+        want = std::max<size_t>(want, 16);
+        if (want <= bytes) return cudaSuccess;
+        if (p) cudaFree(p);
+        p = nullptr;
+        bytes = 0;
+        cudaError_t e = cudaMalloc(&p, want);
+        if (e == cudaSuccess) bytes = want;
+        return e;
+    }
+};
+
+bool finite_or_silent(double level) { return !std::isnan(level) && level != INFINITY; }
+
+}  // namespace
+
+struct qm_flight_boxes {
+    qm_ctx *ctx = nullptr;
+    qm::fl::BoxDev *boxes = nullptr;
+    size_t n = 0;
+    qm::fl::NpdLogs logs{};
+    // The per-call buffers of qm_flight_sums, kept between calls.
+    GrowBuffer points, horizons, segments, order, read_start, slices, sums, heard;
+    ~qm_flight_boxes() {
+        if (boxes) cudaFree(boxes);
+    }
+};
+
+extern "C" qm_status qm_flight_boxes_upload(qm_ctx *ctx, const qm_flight_box *boxes, size_t n_boxes,
+                                            qm_flight_boxes **out) {
+    if (!ctx || !out) return fail(QM_ERR_ARGUMENT, "qm_flight_boxes_upload: null ctx or out");
+    *out = nullptr;
+    if (n_boxes && !boxes) return fail(QM_ERR_ARGUMENT, "qm_flight_boxes_upload: boxes is null");
+    if (n_boxes >= (1ull << 32)) return fail(QM_ERR_ARGUMENT, "qm_flight_boxes_upload: more than 2^32 - 1 boxes");
+    for (size_t i = 0; i < n_boxes; ++i) {
+        const qm_flight_box &b = boxes[i];
+        auto bad = [&](const char *what) {
+            return fail(QM_ERR_ARGUMENT, "qm_flight_boxes_upload: box " + std::to_string(i) + " " + what);
+        };
+        if (!std::isfinite(b.east_m) || !std::isfinite(b.north_m) || !std::isfinite(b.centroid_altitude_m) ||
+            !std::isfinite(b.ground_m))
+            return bad("position");
+        if (!std::isfinite(b.axis_rad) || !std::isfinite(b.gradient) || !(b.gradient_spread >= 0.0) ||
+            !std::isfinite(b.gradient_spread))
+            return bad("axis, gradient or spread");
+        if (b.helicopter > 1) return bad("helicopter flag");
+        for (int p = 0; p < QM_PERIODS; ++p) {
+            if (!(b.piece_length_m[p] >= 0.0) || !std::isfinite(b.piece_length_m[p])) return bad("piece length");
+            if (!(b.passing[p] >= 0.0) || !std::isfinite(b.passing[p])) return bad("passing share");
+            if (!finite_or_silent(b.tail_levels_db[p])) return bad("tail level");
+            for (int k = 0; k < QM_NPD_DISTANCES; ++k)
+                if (!finite_or_silent(b.levels_db[p][k])) return bad("level");
+            for (int s = 0; s < 2; ++s)
+                for (int k = 0; k < 3; ++k)
+                    if (!std::isfinite(b.installation_shares[p][s][k])) return bad("installation share");
+        }
+        for (int k = 0; k < QM_NPD_DISTANCES; ++k)
+            if (!std::isfinite(b.lg_scaled_distance[k])) return bad("scaled distance");
+    }
+    std::unique_ptr<qm_flight_boxes> h(new qm_flight_boxes);
+    h->ctx = ctx;
+    h->n = n_boxes;
+    const double feet[QM_NPD_DISTANCES] = {200.0, 400.0, 630.0, 1000.0, 2000.0, 4000.0, 6300.0, 10000.0, 16000.0, 25000.0};
+    for (int k = 0; k < QM_NPD_DISTANCES; ++k) h->logs.lg[k] = std::log10(feet[k]);  // npd.rs:21-23
+    {
+        std::lock_guard<std::mutex> guard(ctx->lock);
+        QM_CUDA(cudaSetDevice(ctx->device));
+        QM_CUDA(cudaMalloc(&h->boxes, std::max<size_t>(n_boxes, 1) * sizeof(qm::fl::BoxDev)));
+        if (n_boxes) {
+            Scratch staged;
+            QM_CUDA(cudaMalloc(&staged.p, n_boxes * sizeof(qm_flight_box)));
+            QM_CUDA(cudaMemcpyAsync(staged.p, boxes, n_boxes * sizeof(qm_flight_box), cudaMemcpyHostToDevice, ctx->stream));
+            qm::fl::derive_boxes_kernel<<<(unsigned)((n_boxes + 127) / 128), 128, 0, ctx->stream>>>(
+                static_cast<const qm_flight_box *>(staged.p), (uint32_t)n_boxes, h->boxes);
+            QM_CUDA(cudaGetLastError());
+            QM_CUDA(cudaStreamSynchronize(ctx->stream));
+        }
+        ++ctx->children;
+    }
+    *out = h.release();
+    return QM_OK;
+}
+
+extern "C" void qm_flight_boxes_free(qm_flight_boxes *boxes) {
+    if (!boxes) return;
+    qm_ctx *ctx = boxes->ctx;
+    cudaSetDevice(ctx->device);
+    delete boxes;
+    ctx_release(ctx);
+}
+
+extern "C" qm_status qm_flight_sums(qm_ctx *ctx, const qm_flight_boxes *boxes, const qm_flight_point *points,
+                                    size_t n_points, const float *horizons, size_t n_horizon_floats,
+                                    const qm_box_segment *segments, size_t n_segments, double *sums, size_t n_sums,
+                                    qm_flight_sums_stats *stats) {
+    using qm::fl::Slice;
+    if (!ctx || !boxes || boxes->ctx != ctx) return fail(QM_ERR_ARGUMENT, "qm_flight_sums: null ctx, or boxes of another context");
+    if (n_sums && !sums) return fail(QM_ERR_ARGUMENT, "qm_flight_sums: sums is null");
+    if (n_segments && (!segments || !points)) return fail(QM_ERR_ARGUMENT, "qm_flight_sums: segments or points is null");
+    if (n_points >= (1ull << 31) || n_sums >= (1ull << 32) || n_segments >= (1ull << 32))
+        return fail(QM_ERR_ARGUMENT, "qm_flight_sums: too many points, sums or segments");
+    for (size_t i = 0; i < n_points; ++i) {
+        const qm_flight_point &p = points[i];
+        if (!std::isfinite(p.x) || !std::isfinite(p.y) || !std::isfinite(p.altitude_m) ||
+            !(p.impedance_gain >= 0.0) || !std::isfinite(p.impedance_gain))
+            return fail(QM_ERR_ARGUMENT, "qm_flight_sums: point " + std::to_string(i) + " position or impedance gain");
+        if (horizons && (p.horizons > n_horizon_floats || n_horizon_floats - p.horizons < QM_HORIZON_FLOATS))
+            return fail(QM_ERR_ARGUMENT, "qm_flight_sums: point " + std::to_string(i) + " horizons outside the horizon floats");
+    }
+    // The segments grouped by sum (a counting sort keeps each group in the caller's order).
+    std::vector<uint32_t> group_start(n_sums + 1, 0);
+    uint64_t total_reads = 0;
+    for (size_t i = 0; i < n_segments; ++i) {
+        const qm_box_segment &s = segments[i];
+        auto bad = [&](const char *what) {
+            return fail(QM_ERR_ARGUMENT, "qm_flight_sums: segment " + std::to_string(i) + " " + what);
+        };
+        if (s.point >= n_points) return bad("point");
+        if (s.sum >= n_sums) return bad("sum");
+        if ((uint64_t)s.first + s.count > boxes->n) return bad("boxes outside the uploaded boxes");
+        if (s.weight > QM_FLIGHT_WEIGHT_NEAR) return bad("weight");
+        if (std::isnan(s.within_m)) return bad("within_m");
+        if (s.weight != QM_FLIGHT_WEIGHT_ONE && !(s.coarse_m > 0.0 && std::isfinite(s.coarse_m))) return bad("coarse_m");
+        if (s.count) ++group_start[s.sum + 1];
+        total_reads += s.count;
+    }
+    for (size_t k = 0; k < n_sums; ++k) group_start[k + 1] += group_start[k];
+    const uint32_t n_ordered = n_sums ? group_start[n_sums] : 0;
+    std::vector<uint32_t> order(std::max<uint32_t>(n_ordered, 1));
+    {
+        std::vector<uint32_t> next(group_start.begin(), group_start.end() - (n_sums ? 1 : 0));
+        for (size_t i = 0; i < n_segments; ++i)
+            if (segments[i].count) order[next[segments[i].sum]++] = (uint32_t)i;
+    }
+    std::vector<uint64_t> read_start(std::max<uint32_t>(n_ordered, 1), 0);
+    std::vector<Slice> slices;
+    uint64_t at = 0;
+    for (size_t k = 0; k < n_sums; ++k) {
+        const uint32_t g0 = group_start[k], g1 = group_start[k + 1];
+        if (g0 == g1) continue;
+        const uint64_t begin = at;
+        int32_t point = (int32_t)segments[order[g0]].point;
+        for (uint32_t j = g0; j < g1; ++j) {
+            read_start[j] = at;
+            at += segments[order[j]].count;
+            if ((int32_t)segments[order[j]].point != point) point = -1;
+        }
+        for (uint64_t r = begin; r < at; r += qm::fl::SLICE_READS)
+            slices.push_back(Slice{r, std::min(at, r + qm::fl::SLICE_READS), g0, g1, (uint32_t)k, point});
+    }
+    if (slices.size() >= (1ull << 31)) return fail(QM_ERR_ARGUMENT, "qm_flight_sums: too many box reads");
+    qm_flight_boxes *h = const_cast<qm_flight_boxes *>(boxes);
+    std::lock_guard<std::mutex> guard(ctx->lock);
+    QM_CUDA(cudaSetDevice(ctx->device));
+    cudaStream_t stream = ctx->stream;
+    const size_t sum_bytes = n_sums * QM_FLIGHT_SUMS * sizeof(double);
+    QM_CUDA(h->sums.reserve(sum_bytes));
+    QM_CUDA(h->heard.reserve(sizeof(unsigned long long)));
+    QM_CUDA(h->points.reserve(n_points * sizeof(qm_flight_point)));
+    QM_CUDA(h->horizons.reserve(horizons ? n_horizon_floats * sizeof(float) : 0));
+    QM_CUDA(h->segments.reserve(n_segments * sizeof(qm_box_segment)));
+    QM_CUDA(h->order.reserve(order.size() * sizeof(uint32_t)));
+    QM_CUDA(h->read_start.reserve(read_start.size() * sizeof(uint64_t)));
+    QM_CUDA(h->slices.reserve(slices.size() * sizeof(Slice)));
+    if (sum_bytes) QM_CUDA(cudaMemsetAsync(h->sums.p, 0, sum_bytes, stream));
+    QM_CUDA(cudaMemsetAsync(h->heard.p, 0, sizeof(unsigned long long), stream));
+    Events ev;
+    QM_CUDA(ev.create());
+    if (!slices.empty()) {
+        QM_CUDA(cudaMemcpyAsync(h->points.p, points, n_points * sizeof(qm_flight_point), cudaMemcpyHostToDevice, stream));
+        if (horizons && n_horizon_floats)
+            QM_CUDA(cudaMemcpyAsync(h->horizons.p, horizons, n_horizon_floats * sizeof(float), cudaMemcpyHostToDevice, stream));
+        QM_CUDA(cudaMemcpyAsync(h->segments.p, segments, n_segments * sizeof(qm_box_segment), cudaMemcpyHostToDevice, stream));
+        QM_CUDA(cudaMemcpyAsync(h->order.p, order.data(), order.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, stream));
+        QM_CUDA(cudaMemcpyAsync(h->read_start.p, read_start.data(), read_start.size() * sizeof(uint64_t),
+                                cudaMemcpyHostToDevice, stream));
+        QM_CUDA(cudaMemcpyAsync(h->slices.p, slices.data(), slices.size() * sizeof(Slice), cudaMemcpyHostToDevice, stream));
+        qm::fl::SumsArgs A{};
+        A.boxes = h->boxes;
+        A.points = static_cast<const qm_flight_point *>(h->points.p);
+        A.horizons = horizons ? static_cast<const float *>(h->horizons.p) : nullptr;
+        A.segments = static_cast<const qm_box_segment *>(h->segments.p);
+        A.order = static_cast<const uint32_t *>(h->order.p);
+        A.read_start = static_cast<const uint64_t *>(h->read_start.p);
+        A.slices = static_cast<const Slice *>(h->slices.p);
+        A.sums = static_cast<double *>(h->sums.p);
+        A.heard = static_cast<unsigned long long *>(h->heard.p);
+        A.logs = h->logs;
+        QM_CUDA(cudaEventRecord(ev.e0, stream));
+        qm::fl::flight_sums_kernel<<<(unsigned)slices.size(), qm::fl::THREADS, 0, stream>>>(A);
+        QM_CUDA(cudaGetLastError());
+        QM_CUDA(cudaEventRecord(ev.e1, stream));
+    }
+    unsigned long long heard = 0;
+    QM_CUDA(cudaMemcpyAsync(&heard, h->heard.p, sizeof(heard), cudaMemcpyDeviceToHost, stream));
+    if (sum_bytes) QM_CUDA(cudaMemcpyAsync(sums, h->sums.p, sum_bytes, cudaMemcpyDeviceToHost, stream));
+    QM_CUDA(cudaStreamSynchronize(stream));
+    if (stats) {
+        float ms = 0.f;
+        if (!slices.empty()) QM_CUDA(cudaEventElapsedTime(&ms, ev.e0, ev.e1));
+        stats->box_reads = total_reads;
+        stats->boxes_heard = heard;
+        stats->kernel_ms = ms;
     }
     return QM_OK;
 }

@@ -170,6 +170,13 @@ def lib():
         L.qm_pixel_loudness.argtypes = [C.c_void_p, C.POINTER(C.c_float), C.c_size_t, _U64, C.c_size_t, C.c_uint32,
                                         C.c_double, _D, C.c_size_t, _U32, _F, _D]
         L.qm_pixel_loudness.restype = C.c_int
+        L.qm_flight_boxes_upload.argtypes = [C.c_void_p, C.c_void_p, C.c_size_t, C.POINTER(C.c_void_p)]
+        L.qm_flight_boxes_upload.restype = C.c_int
+        L.qm_flight_boxes_free.argtypes = [C.c_void_p]
+        L.qm_flight_boxes_free.restype = None
+        L.qm_flight_sums.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_size_t, _F, C.c_size_t, C.c_void_p,
+                                     C.c_size_t, _D, C.c_size_t, C.POINTER(abi.FlightSumsStats)]
+        L.qm_flight_sums.restype = C.c_int
         L.qm_pixel_distributions.argtypes = [C.POINTER(C.c_float), C.c_size_t, C.c_uint32, C.c_double, _D, C.c_size_t,
                                              _U32, _D, _D, _D, _D]
         L.qm_pixel_distributions.restype = C.c_int
@@ -199,6 +206,46 @@ def _check(status, ctx=None):
     if status != abi.QM_OK:
         message = lib().qm_last_error(ctx).decode(errors="replace")
         raise QmError(status, message)
+
+
+class DeviceFlightBoxes:
+    """A square's aircraft boxes decoded once on the device (qm_flight_boxes_upload); `sums` runs
+    Batch::flight_sums over them (qm_flight_sums)."""
+
+    def __init__(self, ctx, boxes):
+        self.ctx = ctx
+        b = np.ascontiguousarray(boxes, dtype=abi.FLIGHT_BOX_DTYPE)
+        self.n = len(b)
+        self.handle = C.c_void_p()
+        _check(lib().qm_flight_boxes_upload(ctx.handle, b.ctypes.data if len(b) else None, len(b),
+                                            C.byref(self.handle)), ctx.handle)
+
+    def sums(self, points, horizons, segments, n_sums, stats=False):
+        """sums [n_sums][FLIGHT_SUMS] of every request band, and a dict of work and device time
+        when `stats`."""
+        p = np.ascontiguousarray(points, dtype=abi.FLIGHT_POINT_DTYPE)
+        h = None if horizons is None else np.ascontiguousarray(horizons, dtype=np.float32)
+        s = np.ascontiguousarray(segments, dtype=abi.BOX_SEGMENT_DTYPE)
+        out = np.zeros((n_sums, abi.FLIGHT_SUMS))
+        st = abi.FlightSumsStats()
+        _check(lib().qm_flight_sums(self.ctx.handle, self.handle, p.ctypes.data if len(p) else None, len(p),
+                                    None if h is None else abi.ptr(h, C.c_float), 0 if h is None else len(h),
+                                    s.ctypes.data if len(s) else None, len(s), abi.ptr(out, C.c_double), n_sums,
+                                    C.byref(st)), self.ctx.handle)
+        if stats:
+            return out, dict(box_reads=st.box_reads, boxes_heard=st.boxes_heard, kernel_ms=st.kernel_ms)
+        return out
+
+    def close(self):
+        if self.handle:
+            lib().qm_flight_boxes_free(self.handle)
+            self.handle = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 class Context:
@@ -265,6 +312,10 @@ class Context:
             return lae, thirds, out_sone, dict(pairs=st.pairs, pairs_in_reach=st.pairs_in_reach,
                                                kernel_ms=st.kernel_ms, loudness_ms=st.loudness_ms)
         return lae, thirds, out_sone
+
+    def flight_boxes(self, boxes):
+        """A square's aircraft boxes on the device (qm_flight_boxes_upload)."""
+        return DeviceFlightBoxes(self, boxes)
 
     def quantize_cells(self, lden_energy, sone=None, assessed=None):
         """Map cells of pixels (qm_quantize_cells): (lden_cells [n][7], nden_cells [n][7] or None)

@@ -405,6 +405,236 @@ def flights_square(seed=3, n_flights=2000, segments_per_flight=50, n_types=10, r
 
 
 # ---------------------------------------------------------------------------------------------
+# Aircraft boxes: the flights of a square summed into boxes, and lattice points asking for them.
+
+TAIL_ANCHOR_M = 16000.0
+FINE_BOXES_WITHIN_M = 3000.0
+
+
+def _row_energies(types):
+    """Per type, operation and power row: SEL at the ten NPD distances, d_lambda there and the SEL
+    at the tail anchor (the NPD curve beyond 25,000 ft falls by spherical spreading and the
+    absorption fitted to its last three distances)."""
+    d = NPD_DISTANCES_FT * 0.3048
+    last = d[-1]
+    sel = types["sel_db"].astype(np.float64)                      # [t][2][10][10]
+    sml = sel - types["lamax_db"].astype(np.float64)
+    v = types["v_ref_kt"].astype(np.float64) * 1852.0 / 3600.0
+    d0 = (2.0 / np.pi * v)[:, None, None, None]
+    scaled = d0 * 10.0 ** (sml / 10.0)
+    y = sel[..., -3:] + 20.0 * np.log10(d[-3:] / last)
+    x = d[-3:] - d[-3:].mean()
+    slope = (x * (y - y.mean(axis=-1, keepdims=True))).sum(-1) / (x * x).sum()
+    alpha = np.maximum(-slope, 0.0)
+    tail = sel[..., -1] - 20.0 * np.log10(TAIL_ANCHOR_M / last) - alpha * (TAIL_ANCHOR_M - last)
+    return sel, scaled, tail
+
+
+def _cell_boxes(pieces, cell_m, slab_m, n_flights):
+    """BoxSums of the pieces by their cells (physics/src/doc29/box_sums.rs:82-199 in numpy)."""
+    mid = 0.5 * (pieces["start"] + pieces["end"])
+    ix = np.floor(mid[:, 0] / cell_m).astype(np.int64)
+    iy = np.floor(mid[:, 1] / cell_m).astype(np.int64)
+    iz = np.floor(mid[:, 2] / slab_m).astype(np.int64)
+    key = (ix + (1 << 20)) * (1 << 40) + (iy + (1 << 20)) * (1 << 20) + iz
+    keys, inv = np.unique(key, return_inverse=True)
+    nb = len(keys)
+    add = lambda w: np.bincount(inv, weights=w, minlength=nb)
+    pw = pieces["period_weights"]                                   # [n][3]
+    E = pieces["energy"]                                            # [n][10]
+    energy = np.stack([np.stack([add(pw[:, p] * E[:, k]) for k in range(10)], 1) for p in range(3)], 1)
+    tail = np.stack([add(pw[:, p] * pieces["tail"]) for p in range(3)], 1)
+    total = pw.sum(1)
+    over = np.stack([add(total * E[:, k] / np.maximum(pieces["scaled"][:, k], 1.0)) for k in range(10)], 1)
+    w = total * E[:, 3]
+    delta = pieces["end"] - pieces["start"]
+    length = np.hypot(delta[:, 0], delta[:, 1])
+    weight = add(w)
+    midpoint = np.stack([add(w * mid[:, a]) for a in range(3)], 1)
+    period_weight = np.stack([add(pw[:, p] * E[:, 3]) for p in range(3)], 1)
+    period_length = np.stack([add(pw[:, p] * E[:, 3] * length) for p in range(3)], 1)
+    safe = np.maximum(length, 1e-300)
+    c, s_, g = delta[:, 0] / safe, delta[:, 1] / safe, delta[:, 2] / safe
+    on = length > 0.0
+    dd = np.stack([add(np.where(on, w * (c * c - s_ * s_), 0.0)), add(np.where(on, w * 2.0 * s_ * c, 0.0))], 1)
+    gd = np.stack([add(np.where(on, w * g * c, 0.0)), add(np.where(on, w * g * s_, 0.0))], 1)
+    sq = w * g * g
+    sg = np.stack([add(np.where(on, sq * c * c, 0.0)), add(np.where(on, sq * s_ * s_, 0.0)),
+                   add(np.where(on, sq * s_ * c, 0.0))], 1)
+    inst = np.zeros((nb, 3, 2, 3))
+    for slot in range(3):
+        mine = pieces["installation"] == slot
+        for p in range(3):
+            inst[:, p, 0, slot] = add(np.where(mine, pw[:, p] * E[:, 3], 0.0))
+            inst[:, p, 1, slot] = add(np.where(mine, pw[:, p] * pieces["tail"], 0.0))
+    out = np.zeros(nb, dtype=abi.FLIGHT_BOX_DTYPE)
+    with np.errstate(divide="ignore"):
+        out["levels_db"] = np.where(energy > 0.0, 10.0 * np.log10(np.maximum(energy, 1e-300)), -np.inf)
+        out["tail_levels_db"] = np.where(tail > 0.0, 10.0 * np.log10(np.maximum(tail, 1e-300)), -np.inf)
+    out["lg_scaled_distance"] = np.log10(energy.sum(1) / over)
+    axis = np.mod(0.5 * np.arctan2(dd[:, 1], dd[:, 0]), np.pi)
+    sa, ca = np.sin(axis), np.cos(axis)
+    gradient = (gd[:, 0] * ca + gd[:, 1] * sa) / weight
+    mean_square = (sg[:, 0] * ca * ca + sg[:, 1] * sa * sa + 2.0 * sg[:, 2] * sa * ca) / weight
+    out["east_m"], out["north_m"], out["centroid_altitude_m"] = (midpoint / weight[:, None]).T
+    out["axis_rad"], out["gradient"] = axis, gradient
+    out["gradient_spread"] = np.sqrt(np.maximum(mean_square - gradient * gradient, 0.0))
+    out["piece_length_m"] = np.where(period_weight > 0.0, period_length / np.maximum(period_weight, 1e-300), 0.0)
+    tot = inst.sum(-1, keepdims=True)
+    out["installation_shares"] = np.where(tot > 0.0, inst / np.maximum(tot, 1e-300), np.array([0.0, 0.0, 1.0]))
+    # popup/src/aircraft/boxes.rs:225-266 box_passing: flights a day in the box over the period's seconds,
+    # times the cell's mean chord along the box's axis over the pieces' mean speed.
+    flight_key = inv.astype(np.int64) * n_flights + pieces["flight"]
+    _, first = np.unique(flight_key, return_index=True)
+    per_day = np.stack([np.bincount(inv[first], weights=pw[first, p], minlength=nb) for p in range(3)], 1)
+    up = slab_m
+    shadow = np.abs(ca) * cell_m * up + np.abs(sa) * cell_m * up
+    spread = out["gradient_spread"]
+    chord = 0.5 * sum(cell_m * cell_m * up / (shadow + np.abs(gradient + side * spread) * cell_m * cell_m)
+                      for side in (-1.0, 1.0))
+    seconds_per_metre = add(1.0 / pieces["speed_mps"]) / np.bincount(inv, minlength=nb)
+    hours = np.array([12.0, 4.0, 8.0])
+    out["passing"] = per_day / (hours * 3600.0) * (chord * seconds_per_metre)[:, None]
+    return out
+
+
+@dataclass
+class FlightBoxScene:
+    boxes: np.ndarray        # FLIGHT_BOX_DTYPE, grouped by aircraft tile and file (fine, far)
+    tile_ranges: np.ndarray  # [tiles][2 files] (first, count) into boxes
+    tile_m: float
+    tiles_side: int
+    side_m: float
+    info: dict = field(default_factory=dict)
+
+
+def flight_boxes_square(seed=3, n_flights=2000, segments_per_flight=50, receivers=1024, spacing_m=100.0,
+                        tile_m=6400.0, fine_m=400.0, fine_slab_m=150.0, far_m=1600.0, far_slab_m=600.0,
+                        helicopter_share=0.03):
+    """The aircraft boxes of the flight workload's square (`flights_square`: its flights and NPD
+    tables): each segment cut into pieces of at most half a cell, each piece's energies at the NPD
+    distances and tail anchor, every piece summed into its fine cell (fine_m, fine_slab_m) and its far
+    cell (far_m, far_slab_m) as the builder sums a box, flights flown by day, evening or night
+    (70/15/15 %), the boxes grouped by aircraft tile (tile_m) and file. A share of the boxes is
+    marked as helicopters'."""
+    f = flights_square(seed=seed, n_flights=n_flights, segments_per_flight=segments_per_flight, receivers=receivers,
+                       spacing_m=spacing_m)
+    rng = np.random.default_rng(seed + 101)
+    segs = f.segments
+    sel, scaled, tail = _row_energies(f.types)
+    t, op = segs["type"].astype(np.int64), segs["departure"].astype(np.int64)
+    power = segs["power"].astype(np.float64)
+    row = np.minimum(np.floor(power).astype(np.int64), 8)
+    w = (power - row)[:, None]
+    lerp = lambda a: a[t, op, row] + w * (a[t, op, row + 1] - a[t, op, row])
+    v_ref = f.types["v_ref_kt"].astype(np.float64)[t]
+    speed_kt = segs["speed_mps"].astype(np.float64) * 3600.0 / 1852.0
+    dv = np.where(speed_kt > 10.0, 10.0 * np.log10(v_ref / np.maximum(speed_kt, 1e-9)), 0.0)
+    seg_sel = lerp(sel) + dv[:, None]
+    seg_scaled = lerp(scaled)
+    seg_tail = (lerp(tail[..., None])[:, 0]) + dv
+    period_of_flight = rng.choice(3, size=n_flights, p=[0.7, 0.15, 0.15])
+    start, end = segs["start"].astype(np.float64), segs["end"].astype(np.float64)
+    hlen = np.hypot(*(end - start)[:, :2].T)
+    out = []
+    for cell, slab in ((fine_m, fine_slab_m), (far_m, far_slab_m)):
+        n_sub = np.maximum(1, np.ceil(hlen / (0.5 * cell))).astype(np.int64)
+        owner = np.repeat(np.arange(len(segs)), n_sub)
+        k = np.arange(len(owner)) - np.repeat(np.cumsum(n_sub) - n_sub, n_sub)
+        a0, a1 = (k / n_sub[owner])[:, None], ((k + 1) / n_sub[owner])[:, None]
+        d = end[owner] - start[owner]
+        pieces = dict(start=start[owner] + a0 * d, end=start[owner] + a1 * d, energy=10.0 ** (seg_sel[owner] / 10.0),
+                      tail=10.0 ** (seg_tail[owner] / 10.0), scaled=seg_scaled[owner],
+                      installation=f.types["installation"].astype(np.int64)[t[owner]],
+                      flight=segs["flight"].astype(np.int64)[owner], speed_mps=segs["speed_mps"].astype(np.float64)[owner])
+        pw = np.zeros((len(owner), 3))
+        pw[np.arange(len(owner)), period_of_flight[pieces["flight"]]] = 1.0
+        pieces["period_weights"] = pw
+        out.append(_cell_boxes(pieces, cell, slab, n_flights))
+    side = receivers * spacing_m
+    tiles_side = int(np.ceil(side / tile_m))
+    groups, ranges = [], np.zeros((tiles_side * tiles_side, 2, 2), np.int64)
+    for file, boxes in enumerate(out):
+        tx = np.clip(np.floor(boxes["east_m"] / tile_m).astype(np.int64), 0, tiles_side - 1)
+        ty = np.clip(np.floor(boxes["north_m"] / tile_m).astype(np.int64), 0, tiles_side - 1)
+        boxes["helicopter"] = rng.random(len(boxes)) < helicopter_share
+        groups.append((ty * tiles_side + tx, file, boxes))
+    ordered, at = [], 0
+    for tile in range(tiles_side * tiles_side):
+        for tiles, file, boxes in groups:
+            mine = boxes[tiles == tile]
+            ranges[tile, file] = (at, len(mine))
+            ordered.append(mine)
+            at += len(mine)
+    all_boxes = np.concatenate(ordered)
+    return FlightBoxScene(boxes=all_boxes, tile_ranges=ranges, tile_m=tile_m, tiles_side=tiles_side, side_m=side,
+                          info=dict(seed=seed, flights=n_flights, fine_boxes=len(out[0]), far_boxes=len(out[1])))
+
+
+def synthetic_horizons(n, seed=5):
+    """`n` points' horizons as the card keeps them (popup/src/aircraft/horizons.rs:50-64): gentle
+    terrain (tangents -0.03..0.06 in 32 sectors x 6 bands of 30 m - 8 km, a fifth of the bands empty)
+    and an urban building horizon (256 sectors x 6 bands of 16-512 m, tangents 0..0.6, half empty)."""
+    rng = np.random.default_rng(seed)
+    bands = abi.HORIZON_BANDS
+
+    def one(sectors, limits, lo, hi, empty):
+        edges = np.empty((n, sectors, bands, 2), np.float32)
+        inner = np.concatenate([[limits[0] * 0.25], limits[:-1]])
+        edges[..., 0] = rng.uniform(inner, limits, (n, sectors, bands))
+        edges[..., 1] = rng.uniform(lo, hi, (n, sectors, bands))
+        blank = rng.random((n, sectors, bands)) < empty
+        edges[..., 0][blank] = np.nan
+        tang = np.where(blank, -np.inf, edges[..., 1])
+        steepest = tang.max(-1)
+        out = np.empty((n, 1 + sectors * (1 + 2 * bands)), np.float32)
+        out[:, 0] = steepest.max(-1)
+        per = out[:, 1:].reshape(n, sectors, 1 + 2 * bands)
+        per[:, :, 0] = steepest
+        per[:, :, 1:] = edges.reshape(n, sectors, 2 * bands)
+        return out
+
+    terrain = one(abi.TERRAIN_SECTORS, np.array([500.0, 1000.0, 2000.0, 3500.0, 5500.0, 8000.0]), -0.03, 0.06, 0.2)
+    buildings = one(abi.BUILDING_SECTORS, np.array([16.0, 32.0, 64.0, 128.0, 256.0, 512.0]), 0.0, 0.6, 0.5)
+    return np.concatenate([terrain, buildings], 1).reshape(-1)
+
+
+def flight_requests(world, points_xy, altitude_m=4.0, weights=(abi.FLIGHT_WEIGHT_ONE, None), within_m=16000.0,
+                    coarse_m=0.0, impedance_gain=1.0, horizons=True, seed=5):
+    """Lattice points asking for the square's boxes (paint/src/flights.rs:84-107 tiles_heard and
+    paint-gpu/src/aircraft.rs:245-290): per point and band with a weight, a segment per aircraft tile
+    within `within_m` of it, its fine boxes within 3 km and its far boxes beyond. Returns (points,
+    horizons or None, segments, n_sums): sums 2 k + band for point k."""
+    pts = np.asarray(points_xy, dtype=np.float64).reshape(-1, 2)
+    n = len(pts)
+    points = np.zeros(n, dtype=abi.FLIGHT_POINT_DTYPE)
+    points["x"], points["y"] = pts[:, 0], pts[:, 1]
+    points["altitude_m"] = altitude_m
+    points["impedance_gain"] = impedance_gain
+    points["horizons"] = np.arange(n, dtype=np.uint64) * abi.HORIZON_FLOATS
+    hz = synthetic_horizons(n, seed) if horizons else None
+    side, tm = world.tiles_side, world.tile_m
+    tx, ty = np.meshgrid(np.arange(side), np.arange(side))
+    lo_x, lo_y = (tx.ravel() * tm), (ty.ravel() * tm)
+    segs = []
+    for k in range(n):
+        gx = np.maximum(np.maximum(lo_x - pts[k, 0], 0.0), pts[k, 0] - (lo_x + tm))
+        gy = np.maximum(np.maximum(lo_y - pts[k, 1], 0.0), pts[k, 1] - (lo_y + tm))
+        gap = np.hypot(gx, gy)
+        for tile in np.nonzero(gap <= within_m)[0]:
+            file = 0 if gap[tile] <= FINE_BOXES_WITHIN_M and world.tile_ranges[tile, 0, 1] else 1
+            first, count = world.tile_ranges[tile, file]
+            if count == 0:
+                continue
+            for band, weight in enumerate(weights):
+                if weight is None:
+                    continue
+                segs.append((within_m, coarse_m, k, 2 * k + band, first, count, weight, 0))
+    segments = np.array(segs, dtype=abi.BOX_SEGMENT_DTYPE) if segs else np.zeros(0, dtype=abi.BOX_SEGMENT_DTYPE)
+    return points, hz, segments, 2 * n
+
+
+# ---------------------------------------------------------------------------------------------
 # Batches of uneven tiles.
 
 def tiles_world():

@@ -66,6 +66,34 @@ int main(void) {
                        abi.SceneDesc.alpha_db_per_km.offset, abi.GridDesc.n_bins.offset]
 
 
+def test_flight_records_match_the_header():
+    src = r'''
+#include <stdio.h>
+#include <stddef.h>
+#include "qm_flights.h"
+int main(void) {
+  printf("%zu %zu %zu %zu\n", sizeof(qm_flight_box), sizeof(qm_flight_point), sizeof(qm_box_segment),
+         sizeof(qm_flight_sums_stats));
+  printf("%zu %zu %zu %zu %zu\n", offsetof(qm_flight_box, levels_db), offsetof(qm_flight_box, installation_shares),
+         offsetof(qm_flight_box, helicopter), offsetof(qm_flight_point, impedance_gain), offsetof(qm_box_segment, weight));
+  printf("%d %d %d\n", QM_FLIGHT_SUMS, QM_TERRAIN_HORIZON_FLOATS, QM_HORIZON_FLOATS);
+  return 0;
+}
+'''
+    import tempfile
+    with tempfile.TemporaryDirectory() as d:
+        path = os.path.join(d, "flights.c")
+        open(path, "w").write(src)
+        exe = os.path.join(d, "flights")
+        subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), path, "-o", exe], check=True)
+        out = list(map(int, subprocess.run([exe], check=True, capture_output=True, text=True).stdout.split()))
+    assert out[:4] == [abi.FLIGHT_BOX_DTYPE.itemsize, abi.FLIGHT_POINT_DTYPE.itemsize, abi.BOX_SEGMENT_DTYPE.itemsize,
+                       C.sizeof(abi.FlightSumsStats)]
+    assert out[4:9] == [abi.FLIGHT_BOX_DTYPE.fields[k][1] for k in ("levels_db", "installation_shares", "helicopter")] + [
+        abi.FLIGHT_POINT_DTYPE.fields["impedance_gain"][1], abi.BOX_SEGMENT_DTYPE.fields["weight"][1]]
+    assert out[9:] == [abi.FLIGHT_SUMS, abi.TERRAIN_HORIZON_FLOATS, abi.HORIZON_FLOATS]
+
+
 def test_open_without_a_device_fails_loudly():
     import torch
     if torch.cuda.is_available():
