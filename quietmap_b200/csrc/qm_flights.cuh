@@ -57,6 +57,8 @@ static_assert(sizeof(BoxDev) == 624, "BoxDev layout");
 // log10 of the NPD distances in feet, taken on the host by the cores' log10 (npd.rs:115-150).
 struct NpdLogs {
     double lg[ND];
+    double lg_share_span;   // log10 of the installation shares' far slant over their near one
+    double tail_anchor_db;  // 20 log10 of the tail anchor over 25,000 ft
 };
 
 // One copy each of the FP64 functions the equation calls at many sites: inlined at every site,
@@ -94,13 +96,15 @@ __device__ __forceinline__ double npd_linear(const Position &p, const double *cu
 }
 
 // boxes.rs:137-149 box_level_db
-__device__ double box_level_db(const double *levels, double tail_db, const Position &p) {
+// `spherical`: 20 log10 of the slant over 25,000 ft, taken once a piece.
+__device__ __forceinline__ double box_level_db(const NpdLogs &L, const double *levels, double tail_db,
+                                               const Position &p, double spherical) {
     const double last = levels[ND - 1];
     if (p.slant < NPD_LAST_DISTANCE_M) return npd_linear(p, levels);
     if (isinf(last) && last < 0.0) return -CUDART_INF;
-    const double anchor = 20.0 * f_log10(TAIL_ANCHOR_M / NPD_LAST_DISTANCE_M);
-    const double absorption = fmax((last - anchor - tail_db) / (TAIL_ANCHOR_M - NPD_LAST_DISTANCE_M), 0.0);
-    return last - 20.0 * f_log10(p.slant / NPD_LAST_DISTANCE_M) - absorption * (p.slant - NPD_LAST_DISTANCE_M);
+    const double absorption =
+        fmax((last - L.tail_anchor_db - tail_db) / (TAIL_ANCHOR_M - NPD_LAST_DISTANCE_M), 0.0);
+    return last - spherical - absorption * (p.slant - NPD_LAST_DISTANCE_M);
 }
 
 // corrections.rs:33-42
@@ -133,14 +137,6 @@ __device__ __forceinline__ double installation_gain(int installation, double hei
     return (den > 0.0 && num > 0.0) ? f_pow(num, b) / den : 1.0;
 }
 
-// screening.rs:19-44
-__device__ __forceinline__ double edge_loss_db(double er, double eh, double sr, double sh) {
-    if (!(er < sr && eh * sr > sh * er)) return 0.0;
-    const double delta = f_hypot(er, eh) + f_hypot(sr - er, sh - eh) - f_hypot(sr, sh);
-    const double raw = 10.0 * f_log10(3.0 + PATH_DIFFERENCE_SLOPE_PER_M * fmax(delta, 0.0));
-    return fmin(fmax(raw - GRAZING_LOSS_DB, 0.0), SCREENING_CAP_DB);
-}
-
 // popup/src/aircraft/horizons.rs:84-112 SectorEdges::loss_db over the card floats at `at`.
 __device__ __noinline__ double horizon_loss_db(const float *at, int sectors, double x, double y, double z) {
     const double range = f_hypot(x, y);
@@ -150,14 +146,24 @@ __device__ __noinline__ double horizon_loss_db(const float *at, int sectors, dou
     const int sector = min((int)(angle / TAU_D * (double)sectors), sectors - 1);
     const float *e = at + 1 + sector * (1 + 2 * QM_HORIZON_BANDS);
     if (z >= (double)e[0] * range) return 0.0;
-    double loss = 0.0;
+    // The largest loss of the blocking edges is the loss of their largest path difference (the loss
+    // grows with it): one logarithm a lookup, and the direct path taken once.
+    const double direct = f_hypot(range, z);
+    double worst = 0.0;
+    bool blocked = false;
 #pragma unroll 1
     for (int band = 0; band < QM_HORIZON_BANDS; ++band) {
         const double r = e[1 + 2 * band], t = e[2 + 2 * band];
         if (isnan(r)) continue;
-        loss = fmax(loss, edge_loss_db(r, t * r, range, z));
+        const double eh = t * r;
+        if (!(r < range && eh * range > z * r)) continue;  // screening.rs:35-38
+        const double delta = f_hypot(r, eh) + f_hypot(range - r, z - eh) - direct;
+        worst = blocked ? fmax(worst, delta) : delta;
+        blocked = true;
     }
-    return loss;
+    if (!blocked) return 0.0;
+    const double raw = 10.0 * f_log10(3.0 + PATH_DIFFERENCE_SLOPE_PER_M * fmax(worst, 0.0));
+    return fmin(fmax(raw - GRAZING_LOSS_DB, 0.0), SCREENING_CAP_DB);
 }
 
 // boxes.rs:198-280 average_piece_sel: one average piece's SEL energy per period at the point, the
@@ -204,7 +210,8 @@ __device__ void average_piece_sel(const NpdLogs &L, const BoxDev &b, const doubl
     const double stretch = f_hypot(gradient, 1.0);
     const double lateral_db = lateral_attenuation_db(lambda_height, lateral);
     const double corrections[3] = {installation_gain(0, height, slant), installation_gain(1, height, slant), 1.0};
-    const double fraction = fmin(fmax(f_log10(slant / SHARE_NEAR_M) / f_log10(SHARE_FAR_M / SHARE_NEAR_M), 0.0), 1.0);
+    const double fraction = fmin(fmax(f_log10(slant / SHARE_NEAR_M) / L.lg_share_span, 0.0), 1.0);
+    const double spherical = pos.slant < NPD_LAST_DISTANCE_M ? 0.0 : 20.0 * f_log10(pos.slant / NPD_LAST_DISTANCE_M);
     double terrain = 0.0, building = 0.0;
     if (screened && horizons) {
         terrain = horizon_loss_db(horizons, QM_TERRAIN_SECTORS, on_line[0], on_line[1], on_line[2]);
@@ -228,7 +235,7 @@ __device__ void average_piece_sel(const NpdLogs &L, const BoxDev &b, const doubl
             parts += share * corrections[k];
         }
         const double installation = parts > 0.0 ? parts : 1.0;
-        sel[p] = energy_of(box_level_db(b.levels[p], b.tail[p], pos)) * finite * installation * gain;
+        sel[p] = energy_of(box_level_db(L, b.levels[p], b.tail[p], pos, spherical)) * finite * installation * gain;
     }
 }
 

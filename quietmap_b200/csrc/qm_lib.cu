@@ -1746,6 +1746,9 @@ extern "C" qm_status qm_flight_boxes_upload(qm_ctx *ctx, const qm_flight_box *bo
     h->n = n_boxes;
     const double feet[QM_NPD_DISTANCES] = {200.0, 400.0, 630.0, 1000.0, 2000.0, 4000.0, 6300.0, 10000.0, 16000.0, 25000.0};
     for (int k = 0; k < QM_NPD_DISTANCES; ++k) h->logs.lg[k] = std::log10(feet[k]);  // npd.rs:21-23
+    // box_sums.rs:14 and boxes.rs:137-149, as the cores take them
+    h->logs.lg_share_span = std::log10(qm::fl::SHARE_FAR_M / qm::fl::SHARE_NEAR_M);
+    h->logs.tail_anchor_db = 20.0 * std::log10(qm::fl::TAIL_ANCHOR_M / qm::fl::NPD_LAST_DISTANCE_M);
     {
         std::lock_guard<std::mutex> guard(ctx->lock);
         QM_CUDA(cudaSetDevice(ctx->device));
