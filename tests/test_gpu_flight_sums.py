@@ -4,8 +4,10 @@ boxes, box_sel_at_receiver through the point's horizons).
 
 The boxes are the flight workload's flights summed into fine and far cells; the points stand on the
 square with synthetic terrain and building horizons. Every request band's energy per period and its
-pass classes' energies and passing shares agree within 1e-9 relative, and each pass lands in the
-oracle's class."""
+pass classes' energies and passing shares agree within 1e-8 relative, and each pass lands in the
+oracle's class. The bound is the reference's own rounding: its finite-segment fraction subtracts two
+arctangent terms near pi/2 for a far piece, so one unit in the last place of either arctangent
+(the device's or the C library's) moves a far box's energy by up to a few 1e-9."""
 
 import numpy as np
 import pytest
@@ -15,7 +17,7 @@ from quietmap_b200 import abi, native, scenes
 
 pytestmark = pytest.mark.gpu
 
-RTOL = 1e-9
+RTOL = 1e-8
 
 
 @pytest.fixture(scope="module")
