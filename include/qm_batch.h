@@ -205,6 +205,13 @@ qm_status qm_paint_grid(qm_scene *scene, const qm_grid_desc *grid,
  * (physics/src/loudness.rs:148; GPU `loud_zwicker`, paint-gpu/kernels/loudness.cuh:85). */
 qm_status qm_zwicker(qm_ctx *ctx, const float *thirds_db, size_t n, float *sone);
 
+/* The bounded wait's own check. Every wait on a bulk copy's mbarrier gives up after about a second
+ * and becomes QM_ERR_TIMEOUT (or a failed path's QM_FAILED_TIMEOUT) instead of a hang; here one
+ * kernel waits `limit_ms` (at most 2,000) on an mbarrier that nothing completes. QM_OK when the wait
+ * gave up no sooner than its limit and the kernel returned; waited_ms (nullable) is the device time
+ * it waited. The context stays usable. */
+qm_status qm_check_bounded_wait(qm_ctx *ctx, double limit_ms, double *waited_ms);
+
 /* Level histogram of n levels (dB): counts[n_bins] of round((L - level_min)/bin), clamped
  * into the grid (popup/src/distribution.rs:69-72). Counts are exact. */
 qm_status qm_level_histogram(qm_ctx *ctx, const float *levels_db, size_t n,

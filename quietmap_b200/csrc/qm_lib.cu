@@ -1668,6 +1668,50 @@ extern "C" qm_status qm_flight_grid(qm_ctx *ctx, const qm_aircraft_type *types, 
 }
 
 // ---------------------------------------------------------------------------------------------
+// The bounded wait's own check (include/qm_batch.h).
+
+namespace qm {
+
+// One thread waits on a barrier that nothing completes, so the wait gives up after `limit_ns`; the
+// kernel records that it did and how long it waited, and returns. No copy is in flight, so
+// returning is safe.
+__global__ void bounded_wait_check_kernel(uint64_t limit_ns, unsigned *gave_up, unsigned long long *waited_ns) {
+    __shared__ uint64_t bar;
+    if (threadIdx.x != 0) return;
+    mbar_init(&bar, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    const uint64_t t0 = global_ns();
+    const bool landed = mbar_wait(&bar, 0, limit_ns);
+    *waited_ns = global_ns() - t0;
+    *gave_up = landed ? 0u : 1u;
+}
+
+}  // namespace qm
+
+extern "C" qm_status qm_check_bounded_wait(qm_ctx *ctx, double limit_ms, double *waited_ms) {
+    if (!ctx) return fail(QM_ERR_ARGUMENT, "qm_check_bounded_wait: null ctx");
+    if (!(limit_ms > 0.0 && limit_ms <= 2000.0)) return fail(QM_ERR_ARGUMENT, "qm_check_bounded_wait: limit_ms in (0, 2000]");
+    std::lock_guard<std::mutex> guard(ctx->lock);
+    QM_CUDA(cudaSetDevice(ctx->device));
+    Scratch d_flag, d_ns;
+    QM_CUDA(cudaMalloc(&d_flag.p, sizeof(unsigned)));
+    QM_CUDA(cudaMalloc(&d_ns.p, sizeof(unsigned long long)));
+    QM_CUDA(cudaMemsetAsync(d_flag.p, 0, sizeof(unsigned), ctx->stream));
+    qm::bounded_wait_check_kernel<<<1, 32, 0, ctx->stream>>>((uint64_t)(limit_ms * 1e6), static_cast<unsigned *>(d_flag.p),
+                                                             static_cast<unsigned long long *>(d_ns.p));
+    QM_CUDA(cudaGetLastError());
+    unsigned gave_up = 0;
+    unsigned long long ns = 0;
+    QM_CUDA(cudaMemcpyAsync(&gave_up, d_flag.p, sizeof(gave_up), cudaMemcpyDeviceToHost, ctx->stream));
+    QM_CUDA(cudaMemcpyAsync(&ns, d_ns.p, sizeof(ns), cudaMemcpyDeviceToHost, ctx->stream));
+    QM_CUDA(cudaStreamSynchronize(ctx->stream));
+    if (waited_ms) *waited_ms = (double)ns / 1e6;
+    if (!gave_up) return fail(QM_ERR_CUDA, "qm_check_bounded_wait: a barrier that nothing completes was seen complete");
+    if ((double)ns < limit_ms * 1e6) return fail(QM_ERR_CUDA, "qm_check_bounded_wait: the wait gave up before its limit");
+    return QM_OK;
+}
+
+// ---------------------------------------------------------------------------------------------
 // A square's aircraft boxes at lattice points (include/qm_flights.h).
 
 namespace {

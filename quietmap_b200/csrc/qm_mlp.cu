@@ -2,6 +2,7 @@
 // (mma.sync m16n8k16), fused five-layer inference with the activations chained through
 // registers, training products for the backward pass, and Adam on FP32 master weights.
 #include "qm_mlp.h"
+#include "qm_stage.cuh"
 
 #include <algorithm>
 #include <cmath>
@@ -361,26 +362,8 @@ __device__ __forceinline__ void um_bulk(void *dst, const void *src, unsigned byt
                  "l"(src), "r"(bytes), "r"(smem_u32(bar))
                  : "memory");
 }
-__device__ __forceinline__ uint64_t um_ns() {
-    uint64_t t;
-    asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
-    return t;
-}
-// Waits for the barrier's phase for at most about a second; false when it gave up.
-__device__ __forceinline__ bool um_wait(uint64_t *bar, unsigned phase) {
-    const uint32_t b = smem_u32(bar);
-    const uint64_t start = um_ns();
-    for (;;) {
-        unsigned done;
-        asm volatile(
-            "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2; selp.u32 %0, 1, 0, p; }"
-            : "=r"(done)
-            : "r"(b), "r"(phase)
-            : "memory");
-        if (done) return true;
-        if (um_ns() - start > 1000000000ull) return false;
-    }
-}
+// Waits for the barrier's phase for at most about a second (qm_stage.cuh); false when it gave up.
+__device__ __forceinline__ bool um_wait(uint64_t *bar, unsigned phase) { return mbar_wait(bar, phase); }
 
 // Packs the BF16 matrices into the tcgen05 operand layout (output layer padded to 16 rows).
 __global__ void pack_umma_kernel(const __nv_bfloat16 *w16, __nv_bfloat16 *packed) {

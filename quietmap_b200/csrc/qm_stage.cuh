@@ -26,8 +26,9 @@ __device__ __forceinline__ uint64_t global_ns() {
     return t;
 }
 
-// Waits for the barrier's phase for at most about a second; false when it gave up.
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, unsigned phase) {
+// Waits for the barrier's phase for at most `limit_ns` (about a second by default); false when it
+// gave up.
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, unsigned phase, uint64_t limit_ns = 1000000000ull) {
     unsigned b = (unsigned)__cvta_generic_to_shared(bar);
     const uint64_t start = global_ns();
     for (;;) {
@@ -38,7 +39,7 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, unsigned phase) {
             : "r"(b), "r"(phase)
             : "memory");
         if (done) return true;
-        if (global_ns() - start > 1000000000ull) return false;
+        if (global_ns() - start > limit_ns) return false;
     }
 }
 

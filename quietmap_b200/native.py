@@ -58,6 +58,8 @@ def lib():
                                     C.POINTER(abi.PaintStats)]
         L.qm_paint_grid.restype = C.c_int
         L.qm_zwicker.argtypes = [C.c_void_p, _F, C.c_size_t, _F]
+        L.qm_check_bounded_wait.argtypes = [C.c_void_p, C.c_double, _D]
+        L.qm_check_bounded_wait.restype = C.c_int
         L.qm_zwicker.restype = C.c_int
         L.qm_level_histogram.argtypes = [C.c_void_p, _F, C.c_size_t, C.c_double, C.c_double, C.c_uint32, _U32]
         L.qm_level_histogram.restype = C.c_int
@@ -312,6 +314,13 @@ class Context:
             return lae, thirds, out_sone, dict(pairs=st.pairs, pairs_in_reach=st.pairs_in_reach,
                                                kernel_ms=st.kernel_ms, loudness_ms=st.loudness_ms)
         return lae, thirds, out_sone
+
+    def check_bounded_wait(self, limit_ms=1000.0):
+        """The bounded wait's own check (qm_check_bounded_wait): the device time (ms) a wait on an
+        mbarrier that nothing completes took to give up."""
+        ms = C.c_double(0.0)
+        _check(lib().qm_check_bounded_wait(self.handle, float(limit_ms), C.byref(ms)), self.handle)
+        return ms.value
 
     def flight_boxes(self, boxes):
         """A square's aircraft boxes on the device (qm_flight_boxes_upload)."""
