@@ -22,6 +22,8 @@
 #include <unordered_map>
 #include <vector>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "../../include/qm_batch.h"
 #include "../../include/qm_surrogate.h"
 #include "../../include/qm_terrain.h"
@@ -174,6 +176,15 @@ struct Scratch {
 };
 
 // Timing events destroyed when the holder leaves scope (not copyable, for the same reason).
+// A named NVTX range over an entry point's host and device work (a profiler's timeline shows each
+// call; without a tool attached a range costs a test of a null pointer).
+struct NvtxRange {
+    explicit NvtxRange(const char *name) { nvtxRangePushA(name); }
+    ~NvtxRange() { nvtxRangePop(); }
+    NvtxRange(const NvtxRange &) = delete;
+    NvtxRange &operator=(const NvtxRange &) = delete;
+};
+
 struct Events {
     Events() = default;
     Events(const Events &) = delete;
@@ -307,6 +318,7 @@ void qm_close(qm_ctx *ctx) {
 }
 
 qm_status qm_scene_upload(qm_ctx *ctx, const qm_scene_desc *d, qm_scene **out) {
+    NvtxRange nvtx_range("qm_scene_upload");
     if (!ctx || !d || !out) return fail(QM_ERR_ARGUMENT, "qm_scene_upload: null ctx, desc or out");
     *out = nullptr;
     if (!(d->step_m > 0.0) || !std::isfinite(d->step_m)) return fail(QM_ERR_ARGUMENT, "qm_scene_upload: step_m");
@@ -626,6 +638,7 @@ extern "C" {
 
 qm_status qm_paint_grid(qm_scene *scene, const qm_grid_desc *grid, float *cell_bands, float *cell_dba,
                         float *cell_lden, uint32_t *histogram, qm_paint_stats *stats) {
+    NvtxRange nvtx_range("qm_paint_grid");
     if (!scene || !grid) return fail(QM_ERR_ARGUMENT, "qm_paint_grid: null scene or grid");
     const qm_grid_desc &g = *grid;
     if (g.nx <= 0 || g.ny <= 0 || g.spacing <= 0 || (int64_t)g.nx * g.ny > (int64_t(1) << 30))
@@ -771,6 +784,7 @@ qm_status qm_paint_grid(qm_scene *scene, const qm_grid_desc *grid, float *cell_b
 }
 
 qm_status qm_scene_line_pieces(qm_scene *scene, const qm_line_source *pieces, size_t n_pieces) {
+    NvtxRange nvtx_range("qm_scene_line_pieces");
     if (!scene) return fail(QM_ERR_ARGUMENT, "qm_scene_line_pieces: null scene");
     if (n_pieces && !pieces) return fail(QM_ERR_ARGUMENT, "qm_scene_line_pieces: null pieces");
     if ((uint64_t)scene->n_sources + n_pieces > 0xFFFFFFFFull)
@@ -857,6 +871,7 @@ qm_status qm_evaluate_pairs(qm_scene *scene, const double *receiver_xy, const fl
                             const uint32_t *source_of_pair, const uint32_t *receiver_of_pair, const float *band_weight,
                             size_t n_pairs, float *pair_sums, float *pair_bands, uint32_t *pair_status,
                             float *point_bands, size_t n_points) {
+    NvtxRange nvtx_range("qm_evaluate_pairs");
     if (!scene) return fail(QM_ERR_ARGUMENT, "qm_evaluate_pairs: null scene");
     if (n_pairs && (!source_of_pair || !receiver_of_pair || !pair_sums || !pair_status))
         return fail(QM_ERR_ARGUMENT, "qm_evaluate_pairs: a source and receiver per pair, sums and status outputs");
@@ -1012,6 +1027,7 @@ qm_status qm_evaluate_pairs(qm_scene *scene, const double *receiver_xy, const fl
 }
 
 qm_status qm_zwicker(qm_ctx *ctx, const float *thirds_db, size_t n, float *sone) {
+    NvtxRange nvtx_range("qm_zwicker");
     if (!ctx) return fail(QM_ERR_ARGUMENT, "qm_zwicker: null ctx");
     if (n && (!thirds_db || !sone)) return fail(QM_ERR_ARGUMENT, "qm_zwicker: null thirds_db or sone");
     if (n == 0) return QM_OK;
@@ -1057,6 +1073,7 @@ qm_status qm_level_histogram(qm_ctx *ctx, const float *levels_db, size_t n, doub
 
 qm_status qm_quantize_cells(qm_ctx *ctx, const double *lden_energy, const double *sone, const uint8_t *assessed,
                             size_t n, uint8_t *lden_cells, uint8_t *nden_cells) {
+    NvtxRange nvtx_range("qm_quantize_cells");
     if (!ctx) return fail(QM_ERR_ARGUMENT, "qm_quantize_cells: null ctx");
     if ((sone == nullptr) != (nden_cells == nullptr))
         return fail(QM_ERR_ARGUMENT, "qm_quantize_cells: sone and nden_cells are given together or not at all");
@@ -1143,6 +1160,7 @@ qm_status qm_hm3_unpredict(const uint8_t *stream, size_t n_bytes, uint32_t layer
 
 qm_status qm_hm3_predict(qm_ctx *ctx, const uint8_t *cells, const uint8_t *layers, size_t n_tiles, int metric,
                          uint8_t *streams) {
+    NvtxRange nvtx_range("qm_hm3_predict");
     if (!ctx) return fail(QM_ERR_ARGUMENT, "qm_hm3_predict: null ctx");
     if (metric != 0 && metric != 1) return fail(QM_ERR_ARGUMENT, "qm_hm3_predict: metric is 0 (loudness) or 1 (Lden)");
     if (n_tiles == 0) return QM_OK;
@@ -1358,6 +1376,7 @@ extern "C" {
 
 qm_status qm_paint_grid_static(qm_scene *scene, const qm_grid_desc *grid, float *cell_bands, float *cell_dba,
                                float *cell_lden, uint32_t *histogram, qm_paint_stats *stats) {
+    NvtxRange nvtx_range("qm_paint_grid_static");
     if (!scene || !grid) return fail(QM_ERR_ARGUMENT, "qm_paint_grid_static: null scene or grid");
     const qm_grid_desc &g = *grid;
     if (g.nx <= 0 || g.ny <= 0 || g.spacing <= 0)
@@ -1531,6 +1550,7 @@ extern "C" qm_status qm_flight_grid(qm_ctx *ctx, const qm_aircraft_type *types, 
                                     const qm_flight_segment *segments, size_t n_segments,
                                     const qm_flight_grid_desc *grid, float *lae_db, float *thirds_db, float *sone,
                                     qm_flight_stats *stats) {
+    NvtxRange nvtx_range("qm_flight_grid");
     if (!ctx || !grid) return fail(QM_ERR_ARGUMENT, "qm_flight_grid: null ctx or grid");
     if (n_types == 0 || n_types > 48 || !types) return fail(QM_ERR_ARGUMENT, "qm_flight_grid: 1 to 48 aircraft types");
     if (n_segments && !segments) return fail(QM_ERR_ARGUMENT, "qm_flight_grid: segments is null");
@@ -1756,6 +1776,7 @@ struct qm_flight_boxes {
 
 extern "C" qm_status qm_flight_boxes_upload(qm_ctx *ctx, const qm_flight_box *boxes, size_t n_boxes,
                                             qm_flight_boxes **out) {
+    NvtxRange nvtx_range("qm_flight_boxes_upload");
     if (!ctx || !out) return fail(QM_ERR_ARGUMENT, "qm_flight_boxes_upload: null ctx or out");
     *out = nullptr;
     if (n_boxes && !boxes) return fail(QM_ERR_ARGUMENT, "qm_flight_boxes_upload: boxes is null");
@@ -1824,6 +1845,7 @@ extern "C" qm_status qm_flight_sums(qm_ctx *ctx, const qm_flight_boxes *boxes, c
                                     size_t n_points, const float *horizons, size_t n_horizon_floats,
                                     const qm_box_segment *segments, size_t n_segments, double *sums, size_t n_sums,
                                     qm_flight_sums_stats *stats) {
+    NvtxRange nvtx_range("qm_flight_sums");
     using qm::fl::Slice;
     if (!ctx || !boxes || boxes->ctx != ctx) return fail(QM_ERR_ARGUMENT, "qm_flight_sums: null ctx, or boxes of another context");
     if (n_sums && !sums) return fail(QM_ERR_ARGUMENT, "qm_flight_sums: sums is null");
@@ -2179,6 +2201,7 @@ qm_status qm_surrogate_params(const qm_surrogate *net, float *params) {
 
 qm_status qm_surrogate_samples(qm_scene *scene, const qm_grid_desc *grid, float *features, float *labels,
                                uint8_t *eligible) {
+    NvtxRange nvtx_range("qm_surrogate_samples");
     if (!scene || !grid || !features || !labels || !eligible)
         return fail(QM_ERR_ARGUMENT, "qm_surrogate_samples: null scene, grid or output");
     qm_status st = check_grid(scene, *grid, "qm_surrogate_samples");
@@ -2198,6 +2221,7 @@ qm_status qm_surrogate_samples(qm_scene *scene, const qm_grid_desc *grid, float 
 }
 
 qm_status qm_surrogate_forward(qm_surrogate *net, const float *features, size_t n, float *outputs) {
+    NvtxRange nvtx_range("qm_surrogate_forward");
     if (!net || (n && (!features || !outputs))) return fail(QM_ERR_ARGUMENT, "qm_surrogate_forward: null net, features or outputs");
     if (n == 0) return QM_OK;
     std::lock_guard<std::mutex> guard(net->ctx->lock);
@@ -2254,6 +2278,7 @@ qm_status qm_surrogate_gradients(qm_surrogate *net, const float *features, const
 
 qm_status qm_surrogate_train(qm_surrogate *net, qm_scene *scene, const qm_grid_desc *grids, size_t n_grids,
                              const qm_train_config *config, double *loss_history, uint64_t *n_samples) {
+    NvtxRange nvtx_range("qm_surrogate_train");
     if (!net || !scene || !grids || !config || n_grids == 0)
         return fail(QM_ERR_ARGUMENT, "qm_surrogate_train: null net, scene, grids or config");
     if (scene->ctx != net->ctx) return fail(QM_ERR_ARGUMENT, "qm_surrogate_train: net and scene on different contexts");
@@ -2457,6 +2482,7 @@ qm_status qm_surrogate_train(qm_surrogate *net, qm_scene *scene, const qm_grid_d
 qm_status qm_paint_grid_surrogate(qm_scene *scene, const qm_grid_desc *grid, qm_surrogate *net, float *cell_bands,
                                   float *cell_dba, float *cell_lden, uint32_t *histogram, qm_paint_stats *stats,
                                   uint64_t *surrogate_paths) {
+    NvtxRange nvtx_range("qm_paint_grid_surrogate");
     if (!scene || !grid || !net) return fail(QM_ERR_ARGUMENT, "qm_paint_grid_surrogate: null scene, grid or net");
     if (scene->ctx != net->ctx) return fail(QM_ERR_ARGUMENT, "qm_paint_grid_surrogate: net and scene on different contexts");
     const bool terrain = scene->dem_nx != 0;
@@ -2746,6 +2772,7 @@ void qm_batch_plan_free(qm_batch_plan *plan) {
 
 qm_status qm_batch_plan_create(qm_scene *scene, const qm_tile_desc *tiles, size_t n_tiles, uint64_t n_cells,
                                const qm_tune_table *table, uint32_t flags, qm_batch_plan **out) {
+    NvtxRange nvtx_range("qm_batch_plan_create");
     if (!scene || !out || (n_tiles && !tiles)) return fail(QM_ERR_ARGUMENT, "qm_batch_plan_create: null scene, tiles or out");
     if (n_tiles == 0 || n_tiles > (1u << 20)) return fail(QM_ERR_ARGUMENT, "qm_batch_plan_create: 1 to 2^20 tiles");
     if (n_cells == 0 || n_cells > (1ull << 31)) return fail(QM_ERR_ARGUMENT, "qm_batch_plan_create: n_cells in [1, 2^31]");
@@ -2909,6 +2936,7 @@ qm_status qm_batch_plan_create(qm_scene *scene, const qm_tile_desc *tiles, size_
 }
 
 qm_status qm_batch_plan_run(qm_batch_plan *P, qm_paint_stats *stats) {
+    NvtxRange nvtx_range("qm_batch_plan_run");
     if (!P) return fail(QM_ERR_ARGUMENT, "qm_batch_plan_run: null plan");
     qm_scene *scene = P->scene;
     qm_ctx *ctx = scene->ctx;
@@ -3021,6 +3049,7 @@ qm_status qm_batch_plan_read(qm_batch_plan *P, float *cell_bands, float *cell_db
 
 qm_status qm_batch_autotune(qm_scene *scene, const qm_tile_desc *sample, size_t n_sample, qm_tune_table *table,
                             float *timings) {
+    NvtxRange nvtx_range("qm_batch_autotune");
     if (!scene || !table || (n_sample && !sample)) return fail(QM_ERR_ARGUMENT, "qm_batch_autotune: null scene, sample or table");
     qm_tune_default(table);
     if (timings)
@@ -3173,6 +3202,7 @@ qm_status qm_line_level_table(float *table) {
 }
 
 qm_status qm_line_level_quantiles(qm_ctx *ctx, const double *lambda, const double *p, size_t n, double *out) {
+    NvtxRange nvtx_range("qm_line_level_quantiles");
     if (!ctx) return fail(QM_ERR_ARGUMENT, "qm_line_level_quantiles: null ctx");
     if (n == 0) return QM_OK;
     if (!lambda || !p || !out) return fail(QM_ERR_ARGUMENT, "qm_line_level_quantiles: null lambda, p or out");
@@ -3206,6 +3236,7 @@ extern "C" {
 qm_status qm_pixel_loudness(qm_ctx *ctx, const float *input, size_t n_floats, const uint64_t *offsets,
                             size_t n_pixels, uint32_t n_layers, double bin_db, const double *shares,
                             size_t n_profiles, const uint32_t *runs, float *ndens, double *kernel_ms) {
+    NvtxRange nvtx_range("qm_pixel_loudness");
     using namespace qm::pix;
     if (!ctx) return fail(QM_ERR_ARGUMENT, "qm_pixel_loudness: null ctx");
     if (n_pixels == 0) return QM_OK;
