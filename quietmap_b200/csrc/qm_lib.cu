@@ -86,6 +86,28 @@ struct DeviceBuffer {
     }
 };
 
+// A device buffer that grows to the largest size asked of it and is kept between calls.
+struct GrowBuffer {
+    void *p = nullptr;
+    size_t bytes = 0;
+    GrowBuffer() = default;
+    GrowBuffer(const GrowBuffer &) = delete;
+    GrowBuffer &operator=(const GrowBuffer &) = delete;
+    ~GrowBuffer() {
+        if (p) cudaFree(p);
+    }
+    cudaError_t reserve(size_t want) {
+        want = std::max<size_t>(want, 16);
+        if (want <= bytes) return cudaSuccess;
+        if (p) cudaFree(p);
+        p = nullptr;
+        bytes = 0;
+        cudaError_t e = cudaMalloc(&p, want);
+        if (e == cudaSuccess) bytes = want;
+        return e;
+    }
+};
+
 struct qm_scene {
     qm_ctx *ctx;
     SceneDev dev;
@@ -110,6 +132,11 @@ struct qm_scene {
     const qm::PieceDev *pieces = nullptr;
     qm::skyline::Index sky{};
     std::vector<DeviceBuffer *> piece_buffers;
+    // qm_paint_grid's device buffers, kept between calls and grown as a call needs (the call holds
+    // the context's lock throughout, so calls on the scene never share them at once).
+    struct GridScratch {
+        GrowBuffer alt, own, partial, failed, counters, dba, retry, rcount, bands, dbaout, lden, hist;
+    } grid_scratch;
     // Batch plans made on the scene hold it: qm_scene_free releases it once they are freed.
     int plans = 0;
     bool freed = false;
@@ -690,16 +717,19 @@ qm_status qm_paint_grid(qm_scene *scene, const qm_grid_desc *grid, float *cell_b
     // The re-run list holds up to 1 path in 16 (at least 1 M, at most 2^27): over-capacity paths are
     // rare, but tiles in dense quarters with kilometre-long rays reach a few per cent.
     A.retry_cap = (uint32_t)std::min<int64_t>(std::max<int64_t>((int64_t)cells * n_src / 16, 1 << 20), 1 << 27);
-    Scratch d_alt, d_own, d_partial, d_failed, d_counters, d_dba, d_hist, d_bands, d_dbaout, d_lden, d_retry, d_rcount;
+    qm_scene::GridScratch &G = scene->grid_scratch;
+    GrowBuffer &d_alt = G.alt, &d_own = G.own, &d_partial = G.partial, &d_failed = G.failed, &d_counters = G.counters,
+               &d_dba = G.dba, &d_hist = G.hist, &d_bands = G.bands, &d_dbaout = G.dbaout, &d_lden = G.lden,
+               &d_retry = G.retry, &d_rcount = G.rcount;
     size_t partial_bytes = (size_t)slices * cells * GRID_SLOTS * sizeof(float);
-    QM_CUDA(cudaMalloc(&d_alt.p, cells * sizeof(float)));
-    QM_CUDA(cudaMalloc(&d_own.p, cells * sizeof(uint32_t)));
-    QM_CUDA(cudaMalloc(&d_partial.p, partial_bytes));
-    QM_CUDA(cudaMalloc(&d_failed.p, cells * sizeof(uint32_t)));
-    QM_CUDA(cudaMalloc(&d_counters.p, 6 * sizeof(unsigned long long)));
-    QM_CUDA(cudaMalloc(&d_dba.p, cells * sizeof(float)));
-    QM_CUDA(cudaMalloc(&d_retry.p, (size_t)A.retry_cap * sizeof(uint2)));
-    QM_CUDA(cudaMalloc(&d_rcount.p, sizeof(unsigned int)));
+    QM_CUDA(d_alt.reserve(cells * sizeof(float)));
+    QM_CUDA(d_own.reserve(cells * sizeof(uint32_t)));
+    QM_CUDA(d_partial.reserve(partial_bytes));
+    QM_CUDA(d_failed.reserve(cells * sizeof(uint32_t)));
+    QM_CUDA(d_counters.reserve(6 * sizeof(unsigned long long)));
+    QM_CUDA(d_dba.reserve(cells * sizeof(float)));
+    QM_CUDA(d_retry.reserve((size_t)A.retry_cap * sizeof(uint2)));
+    QM_CUDA(d_rcount.reserve(sizeof(unsigned int)));
     QM_CUDA(cudaMemcpyAsync(d_alt.p, alt.data(), cells * sizeof(float), cudaMemcpyHostToDevice, stream));
     QM_CUDA(cudaMemcpyAsync(d_own.p, own.data(), cells * sizeof(uint32_t), cudaMemcpyHostToDevice, stream));
     QM_CUDA(cudaMemsetAsync(d_partial.p, 0, partial_bytes, stream));
@@ -744,17 +774,18 @@ qm_status qm_paint_grid(qm_scene *scene, const qm_grid_desc *grid, float *cell_b
     R.bin_db = g.bin_db;
     R.n_bins = histogram ? g.n_bins : 0;
     R.dba_scratch = static_cast<float *>(d_dba.p);
-    if (cell_bands) QM_CUDA(cudaMalloc(&d_bands.p, (size_t)cells * 8 * sizeof(float)));
-    if (cell_dba) QM_CUDA(cudaMalloc(&d_dbaout.p, (size_t)cells * sizeof(float)));
-    if (cell_lden) QM_CUDA(cudaMalloc(&d_lden.p, (size_t)cells * sizeof(float)));
+    if (cell_bands) QM_CUDA(d_bands.reserve((size_t)cells * 8 * sizeof(float)));
+    if (cell_dba) QM_CUDA(d_dbaout.reserve((size_t)cells * sizeof(float)));
+    if (cell_lden) QM_CUDA(d_lden.reserve((size_t)cells * sizeof(float)));
     if (histogram) {
-        QM_CUDA(cudaMalloc(&d_hist.p, g.n_bins * sizeof(uint32_t)));
+        QM_CUDA(d_hist.reserve(g.n_bins * sizeof(uint32_t)));
         QM_CUDA(cudaMemsetAsync(d_hist.p, 0, g.n_bins * sizeof(uint32_t), stream));
     }
-    R.cell_bands = static_cast<float *>(d_bands.p);
-    R.cell_dba = static_cast<float *>(d_dbaout.p);
-    R.cell_lden = static_cast<float *>(d_lden.p);
-    R.histogram = static_cast<uint32_t *>(d_hist.p);
+    // Outputs the caller did not ask for stay null (the kept buffers may hold an earlier call's).
+    R.cell_bands = cell_bands ? static_cast<float *>(d_bands.p) : nullptr;
+    R.cell_dba = cell_dba ? static_cast<float *>(d_dbaout.p) : nullptr;
+    R.cell_lden = cell_lden ? static_cast<float *>(d_lden.p) : nullptr;
+    R.histogram = histogram ? static_cast<uint32_t *>(d_hist.p) : nullptr;
     size_t smem = histogram ? g.n_bins * sizeof(uint32_t) : 0;
     if (smem > 48 * 1024) QM_CUDA(cudaFuncSetAttribute(reduce_cells_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     reduce_cells_kernel<<<(cells + 255) / 256, 256, smem, stream>>>(R);
@@ -1736,27 +1767,6 @@ extern "C" qm_status qm_check_bounded_wait(qm_ctx *ctx, double limit_ms, double 
 
 namespace {
 
-// A device buffer that grows to the largest size asked of it and is kept between calls.
-struct GrowBuffer {
-    void *p = nullptr;
-    size_t bytes = 0;
-    GrowBuffer() = default;
-    GrowBuffer(const GrowBuffer &) = delete;
-    GrowBuffer &operator=(const GrowBuffer &) = delete;
-    ~GrowBuffer() {
-        if (p) cudaFree(p);
-    }
-    cudaError_t reserve(size_t want) {
-        want = std::max<size_t>(want, 16);
-        if (want <= bytes) return cudaSuccess;
-        if (p) cudaFree(p);
-        p = nullptr;
-        bytes = 0;
-        cudaError_t e = cudaMalloc(&p, want);
-        if (e == cudaSuccess) bytes = want;
-        return e;
-    }
-};
 
 bool finite_or_silent(double level) { return !std::isnan(level) && level != INFINITY; }
 
