@@ -593,120 +593,133 @@ __global__ void __launch_bounds__(UM_THREADS, 1) mlp_umma_kernel(UmmaArgs A) {
 }
 
 // ---------------------------------------------------------------------------------------------
-// Training product: C[M][N] (op) A(m, k) * B(k, n), BF16 operands, FP32 accumulation.
-// A is stored [M][K] (A_MK) or [K][M]; B is stored [N][K] (B_NK) or [K][N]. Tiles of 128 x 128
-// x 32 per CTA of 8 warps (warp tile 64 x 32); split-K over blockIdx.z.
+// Training product: C[M][N] (op) A(m, k) * B(k, n), BF16 operands, FP32 accumulation, on the
+// fifth-generation tensor cores. A is stored [M][K] (A_MK) or [K][M]; B is stored [N][K] (B_NK) or
+// [K][N]. A CTA computes a 128 x 128 tile of C over its share of K (split-K over blockIdx.z): the
+// threads stage each 64-wide K chunk of both operands into shared memory in the canonical K-major
+// layout (transposing an operand stored [K][...] on the way), one thread issues the chunk's
+// `tcgen05.mma` (M 128, N 128, K 16) into 128 tensor-memory columns and commits them to the
+// chunk's mbarrier, and the next chunk is staged into the other buffer meanwhile. The epilogue reads
+// the accumulators with `tcgen05.ld` and applies the layer's bias, GELU or GELU gradient.
 
 enum { EPI_STORE = 0, EPI_ATOMIC = 1, EPI_BIAS_GELU = 2, EPI_BIAS = 3, EPI_GELU_GRAD = 4 };
 
 struct GemmArgs {
     const __nv_bfloat16 *a, *b;
-    int M, N, K;
-    int lda, ldb;      // row strides of the stored matrices
-    int k_per_split;   // multiple of 32
+    int M, N, K;       // each a multiple of 8
+    int lda, ldb;      // row strides of the stored matrices (multiples of 8)
+    int k_per_split;   // multiple of GT_KC
     float *c;          // [M][N] FP32 (EPI_STORE, EPI_ATOMIC, EPI_BIAS: output; EPI_BIAS_GELU: Z)
     const float *bias; // [N]
     __nv_bfloat16 *h;  // [M][N] BF16 (EPI_BIAS_GELU: GELU(Z); EPI_GELU_GRAD: dZ of the layer below)
     const float *z;    // [M][N] (EPI_GELU_GRAD: the layer below's pre-activation)
+    unsigned *error;   // set when a bounded wait gave up
 };
 
-constexpr int GT_M = 128, GT_N = 128, GT_K = 32, GT_STRIDE = GT_K + 8;
+constexpr int GT_M = 128, GT_N = 128, GT_KC = 64;
+constexpr int GT_TILE_BYTES = 128 * GT_KC * 2;      // one operand's chunk: 16 KB
+constexpr int GT_SBO = GT_KC / 8 * 128;             // bytes between 8-row groups of a chunk
+constexpr size_t GT_SMEM = 4 * GT_TILE_BYTES + 64;  // two buffers of A and B, three barriers, TMEM address
+constexpr int GT_TMEM_COLS = 128;
+
+// One operand's chunk [kb, kb + GT_KC) of rows [r0, r0 + 128) into `dst` (canonical K-major, no
+// swizzle: element (row, k) at (row / 8) * GT_SBO + (k / 8) * 128 + (row % 8) * 16 + (k % 8) * 2);
+// rows at or past `rows` and columns at or past `k_end` read zero.
+template <bool ROW_K>
+__device__ __forceinline__ void stage_operand(unsigned char *dst, const __nv_bfloat16 *src, int ld, int r0, int rows,
+                                              int kb, int k_end, int tid) {
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        const int v = tid + 256 * i;  // 1024 groups of 8 elements
+        if (ROW_K) {
+            // Stored [row][k]: a group is 8 consecutive k of one row.
+            const int row = v >> 3, k8 = v & 7, k = kb + 8 * k8;
+            const bool ok = r0 + row < rows && k < k_end;
+            const uint4 val = ok ? *reinterpret_cast<const uint4 *>(src + (size_t)(r0 + row) * ld + k) : make_uint4(0, 0, 0, 0);
+            *reinterpret_cast<uint4 *>(dst + (row >> 3) * GT_SBO + k8 * 128 + (row & 7) * 16) = val;
+        } else {
+            // Stored [k][row]: a group is 8 consecutive rows at one k, scattered to their rows.
+            const int rg = v >> 6, kl = v & 63, k = kb + kl, row = 8 * rg;
+            const bool ok = r0 + row < rows && k < k_end;
+            const uint4 val = ok ? *reinterpret_cast<const uint4 *>(src + (size_t)k * ld + r0 + row) : make_uint4(0, 0, 0, 0);
+            const __nv_bfloat16 *e = reinterpret_cast<const __nv_bfloat16 *>(&val);
+            unsigned char *base = dst + rg * GT_SBO + (kl >> 3) * 128 + (kl & 7) * 2;
+#pragma unroll
+            for (int q = 0; q < 8; ++q) *reinterpret_cast<__nv_bfloat16 *>(base + q * 16) = e[q];
+        }
+    }
+}
 
 template <bool A_MK, bool B_NK, int EPI>
 __global__ void __launch_bounds__(256) gemm_kernel(GemmArgs G) {
-    __shared__ __align__(16) __nv_bfloat16 As[GT_M * GT_STRIDE];
-    __shared__ __align__(16) __nv_bfloat16 Bs[GT_N * GT_STRIDE];
+    extern __shared__ __align__(1024) unsigned char gt_smem[];
+    uint64_t *bars = reinterpret_cast<uint64_t *>(gt_smem + 4 * GT_TILE_BYTES);
+    uint32_t *sTmem = reinterpret_cast<uint32_t *>(bars + 2);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int wm = warp >> 2, wn = warp & 3;  // 2 x 4 warps
     const int m0 = blockIdx.y * GT_M, n0 = blockIdx.x * GT_N;
     const int k_begin = blockIdx.z * G.k_per_split;
     const int k_end = min(G.K, k_begin + G.k_per_split);
-    float acc[4][4][4];
-#pragma unroll
-    for (int a = 0; a < 4; ++a)
-#pragma unroll
-        for (int b = 0; b < 4; ++b)
-#pragma unroll
-            for (int c = 0; c < 4; ++c) acc[a][b][c] = 0.0f;
-    const __nv_bfloat16 zero = __float2bfloat16(0.0f);
-    for (int kb = k_begin; kb < k_end; kb += GT_K) {
-        // Stage the tiles as [row][k] in shared memory.
-        uint4 ra[2], rb[2];
-#pragma unroll
-        for (int i = 0; i < 2; ++i) {
-            int v = tid + 256 * i;
-            if (A_MK) {
-                int r = v >> 2, k = kb + (v & 3) * 8;
-                bool ok = m0 + r < G.M && k < k_end;
-                ra[i] = ok ? *reinterpret_cast<const uint4 *>(G.a + (size_t)(m0 + r) * G.lda + k) : make_uint4(0, 0, 0, 0);
-            } else {
-                int k = kb + (v >> 4), m = m0 + (v & 15) * 8;
-                bool ok = m < G.M && k < k_end;
-                ra[i] = ok ? *reinterpret_cast<const uint4 *>(G.a + (size_t)k * G.lda + m) : make_uint4(0, 0, 0, 0);
-            }
-            if (B_NK) {
-                int r = v >> 2, k = kb + (v & 3) * 8;
-                bool ok = n0 + r < G.N && k < k_end;
-                rb[i] = ok ? *reinterpret_cast<const uint4 *>(G.b + (size_t)(n0 + r) * G.ldb + k) : make_uint4(0, 0, 0, 0);
-            } else {
-                int k = kb + (v >> 4), n = n0 + (v & 15) * 8;
-                bool ok = n < G.N && k < k_end;
-                rb[i] = ok ? *reinterpret_cast<const uint4 *>(G.b + (size_t)k * G.ldb + n) : make_uint4(0, 0, 0, 0);
-            }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(sTmem)),
+                     "r"(GT_TMEM_COLS)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    if (tid == 0) {
+        um_mbar_init(&bars[0], 1);
+        um_mbar_init(&bars[1], 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    tc_before_sync();
+    __syncthreads();
+    tc_after_sync();
+    const uint32_t tmem = *sTmem;
+    unsigned phases = 0u;  // bit b: the parity buffer b's barrier completes next
+    bool ok = true;
+    int chunk = 0;
+    for (int kb = k_begin; kb < k_end && ok; kb += GT_KC, ++chunk) {
+        const int b = chunk & 1;
+        if (chunk >= 2) {
+            // The MMAs that read this buffer two chunks ago must be done before it is refilled.
+            ok = __syncthreads_and(um_wait(&bars[b], (phases >> b) & 1u));
+            phases ^= 1u << b;
+            if (!ok) break;
         }
+        unsigned char *sA = gt_smem + b * GT_TILE_BYTES, *sB = gt_smem + (2 + b) * GT_TILE_BYTES;
+        stage_operand<A_MK>(sA, G.a, G.lda, m0, G.M, kb, k_end, tid);
+        stage_operand<B_NK>(sB, G.b, G.ldb, n0, G.N, kb, k_end, tid);
+        async_proxy_fence();
         __syncthreads();
-#pragma unroll
-        for (int i = 0; i < 2; ++i) {
-            int v = tid + 256 * i;
-            if (A_MK) {
-                *reinterpret_cast<uint4 *>(As + (v >> 2) * GT_STRIDE + (v & 3) * 8) = ra[i];
-            } else {
-                const __nv_bfloat16 *e = reinterpret_cast<const __nv_bfloat16 *>(&ra[i]);
-                int k = v >> 4, m = (v & 15) * 8;
-#pragma unroll
-                for (int q = 0; q < 8; ++q) As[(m + q) * GT_STRIDE + k] = e[q];
-            }
-            if (B_NK) {
-                *reinterpret_cast<uint4 *>(Bs + (v >> 2) * GT_STRIDE + (v & 3) * 8) = rb[i];
-            } else {
-                const __nv_bfloat16 *e = reinterpret_cast<const __nv_bfloat16 *>(&rb[i]);
-                int k = v >> 4, n = (v & 15) * 8;
-#pragma unroll
-                for (int q = 0; q < 8; ++q) Bs[(n + q) * GT_STRIDE + k] = e[q];
-            }
-        }
-        (void)zero;
-        __syncthreads();
-        const int j = lane >> 3, i = lane & 7;
-#pragma unroll
-        for (int kk = 0; kk < GT_K; kk += 16) {
-            uint32_t af[4][4], bf[4][2];
-#pragma unroll
-            for (int mt = 0; mt < 4; ++mt)
-                ldsm_x4(af[mt][0], af[mt][1], af[mt][2], af[mt][3],
-                        As + (wm * 64 + mt * 16 + i + 8 * (j & 1)) * GT_STRIDE + kk + 8 * (j >> 1));
-#pragma unroll
-            for (int p = 0; p < 2; ++p)
-                ldsm_x4(bf[2 * p][0], bf[2 * p][1], bf[2 * p + 1][0], bf[2 * p + 1][1],
-                        Bs + (wn * 32 + 16 * p + i + 8 * (j >> 1)) * GT_STRIDE + kk + 8 * (j & 1));
-#pragma unroll
-            for (int mt = 0; mt < 4; ++mt)
-#pragma unroll
-                for (int nt = 0; nt < 4; ++nt) mma_bf16(acc[mt][nt], af[mt], bf[nt][0], bf[nt][1]);
+        if (tid == 0) {
+            tc_after_sync();
+            const uint32_t a0 = smem_u32(sA), b0 = smem_u32(sB);
+            for (int s = 0; s < GT_KC / 16; ++s)
+                umma_bf16(tmem, umma_desc(a0 + 256 * s, 128, GT_SBO), umma_desc(b0 + 256 * s, 128, GT_SBO),
+                          umma_idesc(GT_M, GT_N), (chunk > 0 || s > 0) ? 1u : 0u);
+            umma_commit(&bars[b]);
         }
     }
-    const int g = lane >> 2, t = lane & 3;
+    // The last commit tracks every MMA this thread issued before it.
+    if (ok && chunk > 0) {
+        const int b = (chunk - 1) & 1;
+        ok = __syncthreads_and(um_wait(&bars[b], (phases >> b) & 1u));
+    }
+    tc_after_sync();
+    if (ok && chunk > 0) {
+        const int lq = warp & 3, ch = warp >> 2;  // TMEM lane quarter and column half
+        const int m = m0 + 32 * lq + lane;
+        const uint32_t t_row = tmem + ((uint32_t)(32 * lq) << 16);
+        for (int c = 0; c < 4; ++c) {
+            const int col = 64 * ch + 16 * c;
+            float v[16];
+            tmem_ld16(t_row + col, v);
+            if (m >= G.M) continue;
 #pragma unroll
-    for (int mt = 0; mt < 4; ++mt)
-#pragma unroll
-        for (int nt = 0; nt < 4; ++nt)
-#pragma unroll
-            for (int h = 0; h < 2; ++h) {
-                int m = m0 + wm * 64 + mt * 16 + g + 8 * h;
-                int n = n0 + wn * 32 + nt * 8 + 2 * t;
-                if (m >= G.M || n >= G.N) continue;
-                float v0 = acc[mt][nt][2 * h], v1 = acc[mt][nt][2 * h + 1];
-                size_t idx = (size_t)m * G.N + n;
+            for (int j = 0; j < 16; j += 2) {
+                const int n = n0 + col + j;
+                if (n >= G.N) break;
+                float v0 = v[j], v1 = v[j + 1];
+                const size_t idx = (size_t)m * G.N + n;
                 if (EPI == EPI_STORE) {
                     *reinterpret_cast<float2 *>(G.c + idx) = make_float2(v0, v1);
                 } else if (EPI == EPI_ATOMIC) {
@@ -719,21 +732,33 @@ __global__ void __launch_bounds__(256) gemm_kernel(GemmArgs G) {
                     if (EPI == EPI_BIAS_GELU)
                         *reinterpret_cast<uint32_t *>(G.h + idx) = pack_bf16(gelu(v0), gelu(v1));
                 } else {  // EPI_GELU_GRAD
-                    float2 z = *reinterpret_cast<const float2 *>(G.z + idx);
+                    const float2 z = *reinterpret_cast<const float2 *>(G.z + idx);
                     *reinterpret_cast<uint32_t *>(G.h + idx) = pack_bf16(v0 * gelu_grad(z.x), v1 * gelu_grad(z.y));
                 }
             }
+        }
+    }
+    if (!ok && tid == 0 && G.error) atomicOr(G.error, 1u);
+    tc_before_sync();
+    __syncthreads();
+    tc_after_sync();
+    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(GT_TMEM_COLS) : "memory");
 }
 
 template <bool A_MK, bool B_NK, int EPI>
 cudaError_t gemm(const GemmArgs &g, int splits, cudaStream_t stream) {
+    if (g.M % 8 || g.N % 8 || g.K % 8 || g.lda % 8 || g.ldb % 8) return cudaErrorInvalidValue;
+    // Set on every call: the attribute belongs to the current device.
+    cudaError_t e = cudaFuncSetAttribute(gemm_kernel<A_MK, B_NK, EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)GT_SMEM);
+    if (e != cudaSuccess) return e;
     GemmArgs a = g;
-    int k_tiles = (g.K + GT_K - 1) / GT_K;
-    splits = std::max(1, std::min(splits, k_tiles));
-    a.k_per_split = ((k_tiles + splits - 1) / splits) * GT_K;
+    int k_chunks = (g.K + GT_KC - 1) / GT_KC;
+    splits = std::max(1, std::min(splits, k_chunks));
+    a.k_per_split = ((k_chunks + splits - 1) / splits) * GT_KC;
     splits = (g.K + a.k_per_split - 1) / a.k_per_split;
     dim3 grid((g.N + GT_N - 1) / GT_N, (g.M + GT_M - 1) / GT_M, splits);
-    gemm_kernel<A_MK, B_NK, EPI><<<grid, 256, 0, stream>>>(a);
+    gemm_kernel<A_MK, B_NK, EPI><<<grid, 256, GT_SMEM, stream>>>(a);
     return cudaGetLastError();
 }
 
@@ -1040,6 +1065,7 @@ cudaError_t mlp_gradients(const MlpDev &net, MlpWork *w, const __nv_bfloat16 *x,
         g.K = mlp_dim(l);
         g.c = w->z[l];
         g.bias = net.master + mlp_b_offset(l);
+        g.error = net.error;
         if (l < MLP_LAYERS - 1) {
             g.h = w->h[l];
             e = gemm<true, true, EPI_BIAS_GELU>(g, 1, stream);
@@ -1067,6 +1093,7 @@ cudaError_t mlp_gradients(const MlpDev &net, MlpWork *w, const __nv_bfloat16 *x,
         g.N = in_w;
         g.K = M;
         g.c = grads + mlp_w_offset(l);
+        g.error = net.error;
         int splits = std::max(1, std::min(128, M / 256));
         if ((e = gemm<false, false, EPI_ATOMIC>(g, splits, stream)) != cudaSuccess) return e;
         dim3 bg((out_w + 31) / 32, (unsigned)std::max<size_t>(1, std::min<size_t>(256, n / 64)));
@@ -1083,6 +1110,7 @@ cudaError_t mlp_gradients(const MlpDev &net, MlpWork *w, const __nv_bfloat16 *x,
             d.K = out_w;
             d.z = w->z[l - 1];
             d.h = w->dz[flip];
+            d.error = net.error;
             if ((e = gemm<true, false, EPI_GELU_GRAD>(d, 1, stream)) != cudaSuccess) return e;
             dz = w->dz[flip];
             flip ^= 1;
