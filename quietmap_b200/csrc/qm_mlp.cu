@@ -619,30 +619,50 @@ struct GemmArgs {
 constexpr int GT_M = 128, GT_N = 128, GT_KC = 64;
 constexpr int GT_TILE_BYTES = 128 * GT_KC * 2;      // one operand's chunk: 16 KB
 constexpr int GT_SBO = GT_KC / 8 * 128;             // bytes between 8-row groups of a chunk
-constexpr size_t GT_SMEM = 4 * GT_TILE_BYTES + 64;  // two buffers of A and B, three barriers, TMEM address
+constexpr int GT_TILE_STRIDE = 128 + 1;              // floats a row of the epilogue's accumulator tile
+constexpr size_t GT_EPI_BYTES = 128 * GT_TILE_STRIDE * 4;
+// Two buffers of A and B (reused by the epilogue's accumulator tile), then two barriers and the
+// tensor-memory address.
+constexpr size_t GT_DATA_BYTES = GT_EPI_BYTES > 4 * GT_TILE_BYTES ? GT_EPI_BYTES : 4 * GT_TILE_BYTES;
+constexpr size_t GT_SMEM = (GT_DATA_BYTES + 15) / 16 * 16 + 64;
 constexpr int GT_TMEM_COLS = 128;
 
-// One operand's chunk [kb, kb + GT_KC) of rows [r0, r0 + 128) into `dst` (canonical K-major, no
-// swizzle: element (row, k) at (row / 8) * GT_SBO + (k / 8) * 128 + (row % 8) * 16 + (k % 8) * 2);
-// rows at or past `rows` and columns at or past `k_end` read zero.
+// One operand's chunk [kb, kb + GT_KC) of rows [r0, r0 + 128): each thread loads 4 groups of 8
+// elements into registers (rows at or past `rows` and columns at or past `k_end` read zero), then
+// stores them in the canonical K-major layout without swizzle: element (row, k) at
+// (row / 8) * GT_SBO + (k / 8) * 128 + (row % 8) * 16 + (k % 8) * 2.
 template <bool ROW_K>
-__device__ __forceinline__ void stage_operand(unsigned char *dst, const __nv_bfloat16 *src, int ld, int r0, int rows,
-                                              int kb, int k_end, int tid) {
+__device__ __forceinline__ void load_operand(uint4 (&r)[4], const __nv_bfloat16 *src, int ld, int r0, int rows, int kb,
+                                             int k_end, int tid) {
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
         const int v = tid + 256 * i;  // 1024 groups of 8 elements
         if (ROW_K) {
             // Stored [row][k]: a group is 8 consecutive k of one row.
-            const int row = v >> 3, k8 = v & 7, k = kb + 8 * k8;
+            const int row = v >> 3, k = kb + 8 * (v & 7);
             const bool ok = r0 + row < rows && k < k_end;
-            const uint4 val = ok ? *reinterpret_cast<const uint4 *>(src + (size_t)(r0 + row) * ld + k) : make_uint4(0, 0, 0, 0);
-            *reinterpret_cast<uint4 *>(dst + (row >> 3) * GT_SBO + k8 * 128 + (row & 7) * 16) = val;
+            r[i] = ok ? *reinterpret_cast<const uint4 *>(src + (size_t)(r0 + row) * ld + k) : make_uint4(0, 0, 0, 0);
         } else {
-            // Stored [k][row]: a group is 8 consecutive rows at one k, scattered to their rows.
-            const int rg = v >> 6, kl = v & 63, k = kb + kl, row = 8 * rg;
+            // Stored [k][row]: a group is 8 consecutive rows at one k.
+            const int row = 8 * (v >> 6), k = kb + (v & 63);
             const bool ok = r0 + row < rows && k < k_end;
-            const uint4 val = ok ? *reinterpret_cast<const uint4 *>(src + (size_t)k * ld + r0 + row) : make_uint4(0, 0, 0, 0);
-            const __nv_bfloat16 *e = reinterpret_cast<const __nv_bfloat16 *>(&val);
+            r[i] = ok ? *reinterpret_cast<const uint4 *>(src + (size_t)k * ld + r0 + row) : make_uint4(0, 0, 0, 0);
+        }
+    }
+}
+
+template <bool ROW_K>
+__device__ __forceinline__ void store_operand(unsigned char *dst, const uint4 (&r)[4], int tid) {
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        const int v = tid + 256 * i;
+        if (ROW_K) {
+            const int row = v >> 3, k8 = v & 7;
+            *reinterpret_cast<uint4 *>(dst + (row >> 3) * GT_SBO + k8 * 128 + (row & 7) * 16) = r[i];
+        } else {
+            // The group's 8 rows scattered to their places at column k.
+            const int rg = v >> 6, kl = v & 63;
+            const __nv_bfloat16 *e = reinterpret_cast<const __nv_bfloat16 *>(&r[i]);
             unsigned char *base = dst + rg * GT_SBO + (kl >> 3) * 128 + (kl & 7) * 2;
 #pragma unroll
             for (int q = 0; q < 8; ++q) *reinterpret_cast<__nv_bfloat16 *>(base + q * 16) = e[q];
@@ -653,7 +673,7 @@ __device__ __forceinline__ void stage_operand(unsigned char *dst, const __nv_bfl
 template <bool A_MK, bool B_NK, int EPI>
 __global__ void __launch_bounds__(256) gemm_kernel(GemmArgs G) {
     extern __shared__ __align__(1024) unsigned char gt_smem[];
-    uint64_t *bars = reinterpret_cast<uint64_t *>(gt_smem + 4 * GT_TILE_BYTES);
+    uint64_t *bars = reinterpret_cast<uint64_t *>(gt_smem + (GT_DATA_BYTES + 15) / 16 * 16);
     uint32_t *sTmem = reinterpret_cast<uint32_t *>(bars + 2);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int m0 = blockIdx.y * GT_M, n0 = blockIdx.x * GT_N;
@@ -677,6 +697,13 @@ __global__ void __launch_bounds__(256) gemm_kernel(GemmArgs G) {
     unsigned phases = 0u;  // bit b: the parity buffer b's barrier completes next
     bool ok = true;
     int chunk = 0;
+    // Each chunk's operands are loaded into registers one chunk ahead, while the tensor cores work
+    // on the chunk before.
+    uint4 ra[4], rb[4];
+    if (k_begin < k_end) {
+        load_operand<A_MK>(ra, G.a, G.lda, m0, G.M, k_begin, k_end, tid);
+        load_operand<B_NK>(rb, G.b, G.ldb, n0, G.N, k_begin, k_end, tid);
+    }
     for (int kb = k_begin; kb < k_end && ok; kb += GT_KC, ++chunk) {
         const int b = chunk & 1;
         if (chunk >= 2) {
@@ -686,10 +713,14 @@ __global__ void __launch_bounds__(256) gemm_kernel(GemmArgs G) {
             if (!ok) break;
         }
         unsigned char *sA = gt_smem + b * GT_TILE_BYTES, *sB = gt_smem + (2 + b) * GT_TILE_BYTES;
-        stage_operand<A_MK>(sA, G.a, G.lda, m0, G.M, kb, k_end, tid);
-        stage_operand<B_NK>(sB, G.b, G.ldb, n0, G.N, kb, k_end, tid);
+        store_operand<A_MK>(sA, ra, tid);
+        store_operand<B_NK>(sB, rb, tid);
         async_proxy_fence();
         __syncthreads();
+        if (kb + GT_KC < k_end) {
+            load_operand<A_MK>(ra, G.a, G.lda, m0, G.M, kb + GT_KC, k_end, tid);
+            load_operand<B_NK>(rb, G.b, G.ldb, n0, G.N, kb + GT_KC, k_end, tid);
+        }
         if (tid == 0) {
             tc_after_sync();
             const uint32_t a0 = smem_u32(sA), b0 = smem_u32(sB);
@@ -706,35 +737,41 @@ __global__ void __launch_bounds__(256) gemm_kernel(GemmArgs G) {
     }
     tc_after_sync();
     if (ok && chunk > 0) {
-        const int lq = warp & 3, ch = warp >> 2;  // TMEM lane quarter and column half
-        const int m = m0 + 32 * lq + lane;
+        // The accumulators through shared memory (the operand buffers are free now): each lane holds
+        // a row of tensor memory, and rows written straight to global memory would scatter.
+        float *tile = reinterpret_cast<float *>(gt_smem);  // [128][GT_TILE_STRIDE]
+        const int lq = warp & 3, ch = warp >> 2;           // TMEM lane quarter and column half
+        const int row = 32 * lq + lane;
         const uint32_t t_row = tmem + ((uint32_t)(32 * lq) << 16);
         for (int c = 0; c < 4; ++c) {
             const int col = 64 * ch + 16 * c;
             float v[16];
             tmem_ld16(t_row + col, v);
-            if (m >= G.M) continue;
 #pragma unroll
-            for (int j = 0; j < 16; j += 2) {
-                const int n = n0 + col + j;
-                if (n >= G.N) break;
-                float v0 = v[j], v1 = v[j + 1];
-                const size_t idx = (size_t)m * G.N + n;
-                if (EPI == EPI_STORE) {
-                    *reinterpret_cast<float2 *>(G.c + idx) = make_float2(v0, v1);
-                } else if (EPI == EPI_ATOMIC) {
-                    atomicAdd(G.c + idx, v0);
-                    atomicAdd(G.c + idx + 1, v1);
-                } else if (EPI == EPI_BIAS || EPI == EPI_BIAS_GELU) {
-                    v0 += G.bias[n];
-                    v1 += G.bias[n + 1];
-                    *reinterpret_cast<float2 *>(G.c + idx) = make_float2(v0, v1);
-                    if (EPI == EPI_BIAS_GELU)
-                        *reinterpret_cast<uint32_t *>(G.h + idx) = pack_bf16(gelu(v0), gelu(v1));
-                } else {  // EPI_GELU_GRAD
-                    const float2 z = *reinterpret_cast<const float2 *>(G.z + idx);
-                    *reinterpret_cast<uint32_t *>(G.h + idx) = pack_bf16(v0 * gelu_grad(z.x), v1 * gelu_grad(z.y));
-                }
+            for (int j = 0; j < 16; ++j) tile[row * GT_TILE_STRIDE + col + j] = v[j];
+        }
+        __syncthreads();
+        // Then by pairs of columns along rows, a warp writing 64 consecutive columns of one row.
+        for (int p = tid; p < 128 * 64; p += 256) {
+            const int r = p >> 6, cp = 2 * (p & 63);
+            const int m = m0 + r, n = n0 + cp;
+            if (m >= G.M || n >= G.N) continue;
+            float v0 = tile[r * GT_TILE_STRIDE + cp], v1 = tile[r * GT_TILE_STRIDE + cp + 1];
+            const size_t idx = (size_t)m * G.N + n;
+            if (EPI == EPI_STORE) {
+                *reinterpret_cast<float2 *>(G.c + idx) = make_float2(v0, v1);
+            } else if (EPI == EPI_ATOMIC) {
+                atomicAdd(G.c + idx, v0);
+                atomicAdd(G.c + idx + 1, v1);
+            } else if (EPI == EPI_BIAS || EPI == EPI_BIAS_GELU) {
+                v0 += G.bias[n];
+                v1 += G.bias[n + 1];
+                *reinterpret_cast<float2 *>(G.c + idx) = make_float2(v0, v1);
+                if (EPI == EPI_BIAS_GELU)
+                    *reinterpret_cast<uint32_t *>(G.h + idx) = pack_bf16(gelu(v0), gelu(v1));
+            } else {  // EPI_GELU_GRAD
+                const float2 z = *reinterpret_cast<const float2 *>(G.z + idx);
+                *reinterpret_cast<uint32_t *>(G.h + idx) = pack_bf16(v0 * gelu_grad(z.x), v1 * gelu_grad(z.y));
             }
         }
     }
