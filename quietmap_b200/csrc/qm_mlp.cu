@@ -293,7 +293,11 @@ __global__ void __launch_bounds__(FT_THREADS, 1) mlp_fused_kernel(FusedArgs A) {
 // 16-byte core matrices, adjacent along K 128 bytes apart (LBO), 8-row groups K/8 * 128 bytes
 // apart (SBO). Every wait on an mbarrier is bounded by %globaltimer.
 
-constexpr int UM_THREADS = 256;
+constexpr int UM_THREADS = 512;
+// Warps share a lane quarter of tensor memory (a warp reads only its quarter's 32 rows): UM_GROUPS
+// warps a quarter, each taking UM_GROUP_COLS of a hidden layer's 256 columns in the epilogue.
+constexpr int UM_GROUPS = UM_THREADS / 128;
+constexpr int UM_GROUP_COLS = 256 / UM_GROUPS;
 constexpr int UM_A_BYTES = 128 * 256 * 2;   // layer input, 128 rows x 256
 constexpr int UM_B_BYTES = 256 * 256 * 2;   // one layer's weights
 constexpr int UM_X_BYTES = 128 * MLP_IN * 2; // feature rows as they arrive (row-major)
@@ -432,7 +436,7 @@ __global__ void __launch_bounds__(UM_THREADS, 1) mlp_umma_kernel(UmmaArgs A) {
         um_bulk(sB, A.wpack, (unsigned)(um_n(0) * um_k(0) * 2), &bars[0]);
         um_bulk(sX, A.x + blockIdx.x * 128 * MLP_IN, x_bytes(blockIdx.x), &bars[1]);
     }
-    const int lq = warp & 3, ch = warp >> 2;  // TMEM lane quarter and column half of this warp
+    const int lq = warp & 3, ch = warp >> 2;  // TMEM lane quarter and column group of this warp
     const int row = 32 * lq + lane;            // this thread's row of the tile
     for (size_t tile = blockIdx.x; tile < n_tiles && ok; tile += gridDim.x) {
         const bool has_next = tile + gridDim.x < n_tiles;
@@ -478,10 +482,10 @@ __global__ void __launch_bounds__(UM_THREADS, 1) mlp_umma_kernel(UmmaArgs A) {
             }
             const uint32_t t_row = tmem + ((uint32_t)(32 * lq) << 16);
             if (l < MLP_LAYERS - 1) {
-                // Hidden epilogue: this warp's 128 columns of its 32 rows -> GELU -> BF16 A layout (K = 256).
+                // Hidden epilogue: this warp's UM_GROUP_COLS columns of its 32 rows -> GELU -> BF16 A layout (K = 256).
                 const float *bias = sBias + l * 256;
-                for (int c = 0; c < 8; ++c) {
-                    const int col = 128 * ch + 16 * c;
+                for (int c = 0; c < UM_GROUP_COLS / 16; ++c) {
+                    const int col = UM_GROUP_COLS * ch + 16 * c;
                     float v[16];
                     tmem_ld16(t_row + col, v);
                     uint32_t pk[8];
