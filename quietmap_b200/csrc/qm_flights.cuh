@@ -137,10 +137,17 @@ __device__ __forceinline__ double installation_gain(int installation, double hei
     return (den > 0.0 && num > 0.0) ? f_pow(num, b) / den : 1.0;
 }
 
-// popup/src/aircraft/horizons.rs:84-112 SectorEdges::loss_db over the card floats at `at`.
-__device__ __noinline__ double horizon_loss_db(const float *at, int sectors, double x, double y, double z) {
-    const double range = f_hypot(x, y);
-    if (range <= 1.0 || z >= (double)at[0] * range) return 0.0;
+// popup/src/aircraft/horizons.rs:84-112 SectorEdges::loss_db over the card floats at `at`, in two
+// parts. The first: no loss for a point within a metre or at or above the steepest tangent of all
+// (`range` its horizontal distance).
+__device__ __forceinline__ bool horizon_may_screen(const float *at, double x, double y, double z, double &range) {
+    range = f_hypot(x, y);
+    return !(range <= 1.0 || z >= (double)at[0] * range);
+}
+
+// The second: the point's sector, its steepest tangent, and the largest loss of its blocking edges.
+__device__ __noinline__ double horizon_sector_loss_db(const float *at, int sectors, double x, double y, double z,
+                                                      double range) {
     double angle = fmod(atan2(y, x), TAU_D);
     if (angle < 0.0) angle += TAU_D;
     const int sector = min((int)(angle / TAU_D * (double)sectors), sectors - 1);
@@ -166,10 +173,12 @@ __device__ __noinline__ double horizon_loss_db(const float *at, int sectors, dou
     return fmin(fmax(raw - GRAZING_LOSS_DB, 0.0), SCREENING_CAP_DB);
 }
 
-// boxes.rs:198-280 average_piece_sel: one average piece's SEL energy per period at the point, the
-// centroid `c` relative to it, at `gradient`; `screened`: the box is low enough for its horizons.
+// boxes.rs:198-280 average_piece_sel: one average piece's SEL energy per period at the point before
+// screening, the centroid `c` relative to it, at `gradient`; with its lateral attenuation and the two
+// points its horizons are asked at (the closest point of the line for terrain, of the piece for
+// buildings).
 __device__ void average_piece_sel(const NpdLogs &L, const BoxDev &b, const double c[3], double gradient,
-                                  const float *horizons, bool screened, double sel[3]) {
+                                  double sel[3], double &lateral_out, double on_line_out[3], double on_segment_out[3]) {
     const double half = 0.5 * fmax(b.average_length, 1.0);
     const double step[3] = {b.cos_axis * half, b.sin_axis * half, gradient * half};
     double s[3], d[3];
@@ -212,14 +221,13 @@ __device__ void average_piece_sel(const NpdLogs &L, const BoxDev &b, const doubl
     const double corrections[3] = {installation_gain(0, height, slant), installation_gain(1, height, slant), 1.0};
     const double fraction = fmin(fmax(f_log10(slant / SHARE_NEAR_M) / L.lg_share_span, 0.0), 1.0);
     const double spherical = pos.slant < NPD_LAST_DISTANCE_M ? 0.0 : 20.0 * f_log10(pos.slant / NPD_LAST_DISTANCE_M);
-    double terrain = 0.0, building = 0.0;
-    if (screened && horizons) {
-        terrain = horizon_loss_db(horizons, QM_TERRAIN_SECTORS, on_line[0], on_line[1], on_line[2]);
-        building = horizon_loss_db(horizons + QM_TERRAIN_HORIZON_FLOATS, QM_BUILDING_SECTORS, on_segment[0],
-                                   on_segment[1], on_segment[2]);
+    // The screening's gain is applied by the caller once the horizons are read (it multiplies last).
+    lateral_out = lateral_db;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        on_line_out[k] = on_line[k];
+        on_segment_out[k] = on_segment[k];
     }
-    // screening.rs:48-55 screened_sel_db(0, ...) less the lateral attenuation
-    const double gain = energy_of((0.0 - fmax(fmax(terrain, building) - lateral_db, 0.0)) - lateral_db);
 #pragma unroll 1
     for (int p = 0; p < 3; ++p) {
         if (b.silent & (1u << p)) {
@@ -235,7 +243,7 @@ __device__ void average_piece_sel(const NpdLogs &L, const BoxDev &b, const doubl
             parts += share * corrections[k];
         }
         const double installation = parts > 0.0 ? parts : 1.0;
-        sel[p] = energy_of(box_level_db(L, b.levels[p], b.tail[p], pos, spherical)) * finite * installation * gain;
+        sel[p] = energy_of(box_level_db(L, b.levels[p], b.tail[p], pos, spherical)) * finite * installation;
     }
 }
 
@@ -347,22 +355,39 @@ __device__ __forceinline__ PointView point_of(const SumsArgs &A, const Slice &sl
     return v;
 }
 
+// A warp's working space for up to 32 boxes' average pieces (two a box at most).
+struct WarpWork {
+    double sel[64][3];      // each piece's SEL energy per period before screening
+    double lateral[64];     // its lateral attenuation (dB)
+    double loss[64][2];     // its terrain and building losses (dB)
+    // A round's horizon lookups that passed their first test: per lane of the round its piece, its
+    // point's horizons and the two points with their ranges; the queue holds 2 x lane + horizon.
+    double point[32][2][4];
+    const float *horizons[32];
+    int piece[32];
+    int look[64];
+};
+
 // The first `n` (at most 32) boxes of a warp's queue: their average pieces (one a box, two for a
-// box whose gradients spread) spread over the lanes, one piece a lane, then each box's pieces
-// joined by its own lane into period energies and pass classes (popup/src/aircraft/boxes.rs:187-223
-// box_at, popup/src/aircraft.rs:86-95 add_pass).
+// box whose gradients spread) spread over the lanes, one piece a lane; the horizon lookups that
+// pass their first test queued and read on full warps; then each box's pieces joined by its own lane
+// with their screening gains into period energies and pass classes (popup/src/aircraft/boxes.rs:
+// 187-223 box_at, popup/src/aircraft.rs:86-95 add_pass).
 __device__ void evaluate_queue(const SumsArgs &A, const Slice &sl, const float *staged, const Heard *queue,
-                               double (*sel)[3], int n, int lane, double energy[3], double *class_energy,
+                               WarpWork &w, int n, int lane, double energy[3], double *class_energy,
                                double *class_passing) {
     bool two = false;
     if (lane < n) two = A.boxes[queue[lane].box].spread > 0.0;
     const unsigned twos = __ballot_sync(0xffffffffu, two);
     const int total = n + __popc(twos);
+    const unsigned below = (1u << lane) - 1u;
     for (int k0 = 0; k0 < total; k0 += 32) {
         const int k = k0 + lane;
+        bool t_look = false, b_look = false;
         if (k < total) {
             const int slot = k < n ? k : (int)__fns(twos, 0, k - n + 1);
             const int which = k < n ? 0 : 1;
+            const int piece = 2 * slot + which;
             const Heard h = queue[slot];
             const BoxDev &b = A.boxes[h.box];
             const PointView v = point_of(A, sl, staged, h.at);
@@ -370,17 +395,58 @@ __device__ void evaluate_queue(const SumsArgs &A, const Slice &sl, const float *
             const bool screened = c[2] - (b.ground - v.pt.altitude_m) < SCREENING_CEILING_M;
             const double spread = b.spread;
             const double gradient = spread > 0.0 ? (which ? b.gradient + spread : b.gradient - spread) : b.gradient;
-            average_piece_sel(A.logs, b, c, gradient, v.horizons, screened, sel[2 * slot + which]);
+            double on_line[3], on_segment[3];
+            average_piece_sel(A.logs, b, c, gradient, w.sel[piece], w.lateral[piece], on_line, on_segment);
+            w.loss[piece][0] = w.loss[piece][1] = 0.0;
+            if (screened && v.horizons) {
+                double r;
+                w.piece[lane] = piece;
+                w.horizons[lane] = v.horizons;
+                if (horizon_may_screen(v.horizons, on_line[0], on_line[1], on_line[2], r)) {
+                    t_look = true;
+                    w.point[lane][0][0] = on_line[0];
+                    w.point[lane][0][1] = on_line[1];
+                    w.point[lane][0][2] = on_line[2];
+                    w.point[lane][0][3] = r;
+                }
+                if (horizon_may_screen(v.horizons + QM_TERRAIN_HORIZON_FLOATS, on_segment[0], on_segment[1],
+                                       on_segment[2], r)) {
+                    b_look = true;
+                    w.point[lane][1][0] = on_segment[0];
+                    w.point[lane][1][1] = on_segment[1];
+                    w.point[lane][1][2] = on_segment[2];
+                    w.point[lane][1][3] = r;
+                }
+            }
         }
+        const unsigned mt = __ballot_sync(0xffffffffu, t_look), mb = __ballot_sync(0xffffffffu, b_look);
+        if (t_look) w.look[__popc(mt & below)] = 2 * lane;
+        if (b_look) w.look[__popc(mt) + __popc(mb & below)] = 2 * lane + 1;
+        const int n_look = __popc(mt) + __popc(mb);
+        __syncwarp();
+        for (int j = lane; j < n_look; j += 32) {
+            const int src = w.look[j] >> 1, hz = w.look[j] & 1;
+            const double *q = w.point[src][hz];
+            const float *at = w.horizons[src] + (hz ? QM_TERRAIN_HORIZON_FLOATS : 0);
+            w.loss[w.piece[src]][hz] =
+                horizon_sector_loss_db(at, hz ? QM_BUILDING_SECTORS : QM_TERRAIN_SECTORS, q[0], q[1], q[2], q[3]);
+        }
+        __syncwarp();
     }
-    __syncwarp();
     if (lane < n) {
         const Heard h = queue[lane];
         const BoxDev &b = A.boxes[h.box];
         const double impedance = b.helicopter ? 1.0 : A.points[A.segments[A.order[h.at]].point].impedance_gain;
+        // screening.rs:48-55 screened_sel_db(0, ...) less the lateral attenuation, a piece's gain
+        auto gain_of = [&](int piece) {
+            const double lat = w.lateral[piece];
+            return energy_of((0.0 - fmax(fmax(w.loss[piece][0], w.loss[piece][1]) - lat, 0.0)) - lat);
+        };
+        const double g0 = gain_of(2 * lane), g1 = two ? gain_of(2 * lane + 1) : 0.0;
 #pragma unroll 1
         for (int p = 0; p < 3; ++p) {
-            const double s = two ? 0.5 * (sel[2 * lane][p] + sel[2 * lane + 1][p]) : sel[2 * lane][p];
+            const double lo = w.sel[2 * lane][p] * g0;
+            const double s = two ? 0.5 * (lo + w.sel[2 * lane + 1][p] * g1) : lo;
             const double hours = p == 0 ? 12.0 : p == 1 ? 4.0 : 8.0;  // physics/src/bands.rs:16
             const double e = h.share * (s * impedance / (hours * 3600.0));
             const double passing = h.share * b.passing[p];
@@ -403,7 +469,7 @@ __global__ void __launch_bounds__(THREADS) flight_sums_kernel(SumsArgs A) {
     __shared__ double s_class_energy[3 * CLASSES], s_class_passing[3 * CLASSES];
     __shared__ double s_energy[3][THREADS];
     __shared__ Heard s_queue[WARPS][64];
-    __shared__ double s_sel[WARPS][64][3];
+    __shared__ WarpWork s_work[WARPS];
     __shared__ unsigned s_heard;
     const Slice sl = A.slices[blockIdx.x];
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -449,7 +515,7 @@ __global__ void __launch_bounds__(THREADS) flight_sums_kernel(SumsArgs A) {
         heard += hit ? 1u : 0u;
         __syncwarp();
         if (queued >= 32) {
-            evaluate_queue(A, sl, staged, queue, s_sel[warp], 32, lane, energy, s_class_energy, s_class_passing);
+            evaluate_queue(A, sl, staged, queue, s_work[warp], 32, lane, energy, s_class_energy, s_class_passing);
             const bool move = lane < queued - 32;
             Heard keep;
             if (move) keep = queue[32 + lane];
@@ -460,7 +526,7 @@ __global__ void __launch_bounds__(THREADS) flight_sums_kernel(SumsArgs A) {
         }
     }
     if (queued > 0)
-        evaluate_queue(A, sl, staged, queue, s_sel[warp], queued, lane, energy, s_class_energy, s_class_passing);
+        evaluate_queue(A, sl, staged, queue, s_work[warp], queued, lane, energy, s_class_energy, s_class_passing);
 #pragma unroll
     for (int p = 0; p < 3; ++p) s_energy[p][tid] = energy[p];
     if (heard) atomicAdd(&s_heard, heard);
