@@ -108,6 +108,28 @@ struct GrowBuffer {
     }
 };
 
+// A pinned host buffer that grows to the largest size asked of it and is kept between calls.
+struct PinnedBuffer {
+    void *p = nullptr;
+    size_t bytes = 0;
+    PinnedBuffer() = default;
+    PinnedBuffer(const PinnedBuffer &) = delete;
+    PinnedBuffer &operator=(const PinnedBuffer &) = delete;
+    ~PinnedBuffer() {
+        if (p) cudaFreeHost(p);
+    }
+    cudaError_t reserve(size_t want) {
+        want = std::max<size_t>(want, 16);
+        if (want <= bytes) return cudaSuccess;
+        if (p) cudaFreeHost(p);
+        p = nullptr;
+        bytes = 0;
+        cudaError_t e = cudaHostAlloc(&p, want, cudaHostAllocDefault);
+        if (e == cudaSuccess) bytes = want;
+        return e;
+    }
+};
+
 struct qm_scene {
     qm_ctx *ctx;
     SceneDev dev;
@@ -1777,10 +1799,14 @@ struct qm_flight_boxes {
     qm::fl::BoxDev *boxes = nullptr;
     size_t n = 0;
     qm::fl::NpdLogs logs{};
-    // The per-call buffers of qm_flight_sums, kept between calls.
+    // The per-call buffers of qm_flight_sums, kept between calls: on the device, and pinned on the
+    // host for the horizons going up and the sums coming down while batches compute.
     GrowBuffer points, horizons, segments, order, read_start, slices, sums, heard;
+    PinnedBuffer pinned_horizons, pinned_sums;
+    cudaStream_t copies = nullptr;  // the copies' stream, beside the context's
     ~qm_flight_boxes() {
         if (boxes) cudaFree(boxes);
+        if (copies) cudaStreamDestroy(copies);
     }
 };
 
@@ -1927,17 +1953,54 @@ extern "C" qm_status qm_flight_sums(qm_ctx *ctx, const qm_flight_boxes *boxes, c
     QM_CUDA(h->slices.reserve(slices.size() * sizeof(Slice)));
     if (sum_bytes) QM_CUDA(cudaMemsetAsync(h->sums.p, 0, sum_bytes, stream));
     QM_CUDA(cudaMemsetAsync(h->heard.p, 0, sizeof(unsigned long long), stream));
-    Events ev;
-    QM_CUDA(ev.create());
-    if (!slices.empty()) {
+    unsigned long long heard = 0;
+    double kernel_ms = 0.0;
+    if (slices.empty()) {
+        if (sum_bytes) QM_CUDA(cudaMemcpyAsync(sums, h->sums.p, sum_bytes, cudaMemcpyDeviceToHost, stream));
+        QM_CUDA(cudaStreamSynchronize(stream));
+    } else {
         QM_CUDA(cudaMemcpyAsync(h->points.p, points, n_points * sizeof(qm_flight_point), cudaMemcpyHostToDevice, stream));
-        if (horizons && n_horizon_floats)
-            QM_CUDA(cudaMemcpyAsync(h->horizons.p, horizons, n_horizon_floats * sizeof(float), cudaMemcpyHostToDevice, stream));
         QM_CUDA(cudaMemcpyAsync(h->segments.p, segments, n_segments * sizeof(qm_box_segment), cudaMemcpyHostToDevice, stream));
         QM_CUDA(cudaMemcpyAsync(h->order.p, order.data(), order.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, stream));
         QM_CUDA(cudaMemcpyAsync(h->read_start.p, read_start.data(), read_start.size() * sizeof(uint64_t),
                                 cudaMemcpyHostToDevice, stream));
         QM_CUDA(cudaMemcpyAsync(h->slices.p, slices.data(), slices.size() * sizeof(Slice), cudaMemcpyHostToDevice, stream));
+        if (!h->copies) QM_CUDA(cudaStreamCreateWithFlags(&h->copies, cudaStreamNonBlocking));
+        QM_CUDA(h->pinned_sums.reserve(sum_bytes));
+        if (horizons) QM_CUDA(h->pinned_horizons.reserve(n_horizon_floats * sizeof(float)));
+        // Batches of whole request bands, each with the prefix of the horizons its points read: a
+        // batch's horizons go up (through pinned memory, on the copies' stream) while the batch before
+        // it computes, and its sums come down while the batches after it compute.
+        // A batch of at least five full waves of CTAs (four an SM), so that the launches' partly
+        // filled last waves stay a small part of the time; small calls are one batch.
+        const size_t wave = (size_t)ctx->sm_count * 4;
+        const size_t n_batches = std::max<size_t>(1, std::min<size_t>(8, slices.size() / (5 * wave)));
+        std::vector<size_t> cut(1, 0);  // slice boundaries
+        for (size_t k = 1; k < n_batches; ++k) {
+            size_t at = std::max(cut.back() + 1, slices.size() * k / n_batches);
+            while (at < slices.size() && slices[at].sum == slices[at - 1].sum) ++at;
+            if (at < slices.size()) cut.push_back(at);
+        }
+        cut.push_back(slices.size());
+        const size_t batches = cut.size() - 1;
+        struct BatchEvents {
+            cudaEvent_t up = nullptr, start = nullptr, end = nullptr, down = nullptr;
+        };
+        std::vector<BatchEvents> bev(batches);
+        struct EventsGuard {
+            std::vector<BatchEvents> &v;
+            ~EventsGuard() {
+                for (auto &e : v)
+                    for (cudaEvent_t x : {e.up, e.start, e.end, e.down})
+                        if (x) cudaEventDestroy(x);
+            }
+        } guard_events{bev};
+        for (auto &e : bev) {
+            QM_CUDA(cudaEventCreateWithFlags(&e.up, cudaEventDisableTiming));
+            QM_CUDA(cudaEventCreate(&e.start));
+            QM_CUDA(cudaEventCreate(&e.end));
+            QM_CUDA(cudaEventCreateWithFlags(&e.down, cudaEventDisableTiming));
+        }
         qm::fl::SumsArgs A{};
         A.boxes = h->boxes;
         A.points = static_cast<const qm_flight_point *>(h->points.p);
@@ -1945,25 +2008,63 @@ extern "C" qm_status qm_flight_sums(qm_ctx *ctx, const qm_flight_boxes *boxes, c
         A.segments = static_cast<const qm_box_segment *>(h->segments.p);
         A.order = static_cast<const uint32_t *>(h->order.p);
         A.read_start = static_cast<const uint64_t *>(h->read_start.p);
-        A.slices = static_cast<const Slice *>(h->slices.p);
         A.sums = static_cast<double *>(h->sums.p);
         A.heard = static_cast<unsigned long long *>(h->heard.p);
         A.logs = h->logs;
-        QM_CUDA(cudaEventRecord(ev.e0, stream));
-        qm::fl::flight_sums_kernel<<<(unsigned)slices.size(), qm::fl::THREADS, 0, stream>>>(A);
-        QM_CUDA(cudaGetLastError());
-        QM_CUDA(cudaEventRecord(ev.e1, stream));
+        // The sums' memset precedes every batch's read-back.
+        cudaEvent_t zeroed = nullptr;
+        QM_CUDA(cudaEventCreateWithFlags(&zeroed, cudaEventDisableTiming));
+        std::unique_ptr<CUevent_st, cudaError_t (*)(cudaEvent_t)> zeroed_guard(zeroed, cudaEventDestroy);
+        QM_CUDA(cudaEventRecord(zeroed, stream));
+        QM_CUDA(cudaStreamWaitEvent(h->copies, zeroed, 0));
+        unsigned char *pin_hz = static_cast<unsigned char *>(h->pinned_horizons.p);
+        double *pin_sums = static_cast<double *>(h->pinned_sums.p);
+        size_t have = 0;  // horizon floats already sent
+        for (size_t bi = 0; bi < batches; ++bi) {
+            const Slice &first = slices[cut[bi]], &last = slices[cut[bi + 1] - 1];
+            if (horizons) {
+                size_t need = have;
+                for (uint32_t j = first.seg_begin; j < last.seg_end; ++j)
+                    need = std::max<size_t>(need, points[segments[order[j]].point].horizons + QM_HORIZON_FLOATS);
+                if (need > have) {
+                    const size_t off = have * sizeof(float), bytes = (need - have) * sizeof(float);
+                    std::memcpy(pin_hz + off, reinterpret_cast<const unsigned char *>(horizons) + off, bytes);
+                    QM_CUDA(cudaMemcpyAsync(static_cast<unsigned char *>(h->horizons.p) + off, pin_hz + off, bytes,
+                                            cudaMemcpyHostToDevice, h->copies));
+                    have = need;
+                }
+            }
+            QM_CUDA(cudaEventRecord(bev[bi].up, h->copies));
+            QM_CUDA(cudaStreamWaitEvent(stream, bev[bi].up, 0));
+            A.slices = static_cast<const Slice *>(h->slices.p) + cut[bi];
+            QM_CUDA(cudaEventRecord(bev[bi].start, stream));
+            qm::fl::flight_sums_kernel<<<(unsigned)(cut[bi + 1] - cut[bi]), qm::fl::THREADS, 0, stream>>>(A);
+            QM_CUDA(cudaGetLastError());
+            QM_CUDA(cudaEventRecord(bev[bi].end, stream));
+            // The batch's bands: the sums from its first slice's to its last slice's.
+            QM_CUDA(cudaStreamWaitEvent(h->copies, bev[bi].end, 0));
+            const size_t k0 = first.sum, k1 = (size_t)last.sum + 1;
+            QM_CUDA(cudaMemcpyAsync(pin_sums + k0 * QM_FLIGHT_SUMS, static_cast<double *>(h->sums.p) + k0 * QM_FLIGHT_SUMS,
+                                    (k1 - k0) * QM_FLIGHT_SUMS * sizeof(double), cudaMemcpyDeviceToHost, h->copies));
+            QM_CUDA(cudaEventRecord(bev[bi].down, h->copies));
+        }
+        // Bands no segment names stay zero; each batch's bands are copied out as they arrive.
+        if (sum_bytes) std::memset(sums, 0, sum_bytes);
+        for (size_t bi = 0; bi < batches; ++bi) {
+            QM_CUDA(cudaEventSynchronize(bev[bi].down));
+            const size_t k0 = slices[cut[bi]].sum, k1 = (size_t)slices[cut[bi + 1] - 1].sum + 1;
+            std::memcpy(sums + k0 * QM_FLIGHT_SUMS, pin_sums + k0 * QM_FLIGHT_SUMS, (k1 - k0) * QM_FLIGHT_SUMS * sizeof(double));
+            float ms = 0.f;
+            QM_CUDA(cudaEventElapsedTime(&ms, bev[bi].start, bev[bi].end));
+            kernel_ms += ms;
+        }
+        QM_CUDA(cudaMemcpyAsync(&heard, h->heard.p, sizeof(heard), cudaMemcpyDeviceToHost, stream));
+        QM_CUDA(cudaStreamSynchronize(stream));
     }
-    unsigned long long heard = 0;
-    QM_CUDA(cudaMemcpyAsync(&heard, h->heard.p, sizeof(heard), cudaMemcpyDeviceToHost, stream));
-    if (sum_bytes) QM_CUDA(cudaMemcpyAsync(sums, h->sums.p, sum_bytes, cudaMemcpyDeviceToHost, stream));
-    QM_CUDA(cudaStreamSynchronize(stream));
     if (stats) {
-        float ms = 0.f;
-        if (!slices.empty()) QM_CUDA(cudaEventElapsedTime(&ms, ev.e0, ev.e1));
         stats->box_reads = total_reads;
         stats->boxes_heard = heard;
-        stats->kernel_ms = ms;
+        stats->kernel_ms = kernel_ms;
     }
     return QM_OK;
 }
