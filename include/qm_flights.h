@@ -113,6 +113,17 @@ qm_status qm_flight_sums(qm_ctx *ctx, const qm_flight_boxes *boxes, const qm_fli
                          const qm_box_segment *segments, size_t n_segments, double *sums,
                          size_t n_sums, qm_flight_sums_stats *stats);
 
+/* The points' horizons for aircraft screening, built on the device from a scene's terrain and
+ * buildings (popup/src/aircraft/horizons.rs:145-198 Horizons::build, which the reference runs on the
+ * host for every request): per point its position in the scene's lattice steps (x, y; fractional
+ * allowed), its altitude (m) and the footprint it stands in (0 none, its walls are no horizon),
+ * QM_HORIZON_FLOATS floats into `horizons` (n_points x QM_HORIZON_FLOATS) as qm_flight_sums reads
+ * them. Terrain: 32 sectors x 48 samples from 30 m to 8 km growing geometrically, a sample outside
+ * the scene's DEM is no terrain; buildings: 256 sectors, a 512 m ray each, the crossings within
+ * 1 cm left out. QM_ERR_CAPACITY when a ray crosses more than 256 edges. */
+qm_status qm_scene_flight_horizons(qm_scene *scene, const double *xy_steps, const double *altitude_m,
+                                   const uint64_t *own_footprint, size_t n_points, float *horizons);
+
 #ifdef __cplusplus
 }
 #endif

@@ -136,6 +136,8 @@ def lib():
         for name in ("qmo_edge_loss_db", "qmo_screened_sel_db"):
             getattr(L, name).argtypes = [C.c_double] * 4
             getattr(L, name).restype = C.c_double
+        L.qmo_flight_horizons.argtypes = [C.c_void_p, _D, _D, _U64, C.c_size_t, C.POINTER(C.c_float), C.c_int]
+        L.qmo_flight_horizons.restype = None
         L.qmo_flight_weight.argtypes = [C.c_uint32, C.c_double, C.c_double]
         L.qmo_flight_weight.restype = C.c_double
         L.qmo_horizon_loss_db.argtypes = [C.POINTER(C.c_float), C.c_int, _D]
@@ -268,6 +270,17 @@ class OracleScene:
     def crossings_f64(self, frm, to):
         """The walk's crossing list for ends anywhere (f64 steps)."""
         return self._crossings_f64(lib().qmo_crossings_d, frm, to)
+
+    def flight_horizons(self, xy_steps, altitude_m, own_footprint, nthreads=None):
+        """Each point's horizons for aircraft screening (Horizons::build), [n][HORIZON_FLOATS]
+        float32 as the card keeps them."""
+        xy = np.ascontiguousarray(np.asarray(xy_steps, dtype=np.float64).reshape(-1, 2))
+        alt = np.ascontiguousarray(np.asarray(altitude_m, dtype=np.float64).reshape(-1))
+        own = np.ascontiguousarray(np.asarray(own_footprint, dtype=np.uint64).reshape(-1))
+        out = np.zeros((len(xy), abi.HORIZON_FLOATS), np.float32)
+        lib().qmo_flight_horizons(self.handle, abi.ptr(xy, C.c_double), abi.ptr(alt, C.c_double),
+                                  abi.ptr(own, C.c_uint64), len(xy), abi.ptr(out, C.c_float), nthreads or threads())
+        return out
 
     def crossings_every(self, frm, to):
         """Every edge against the ray with the walk's deduplication: the list the walk must give."""

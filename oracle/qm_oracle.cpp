@@ -2729,4 +2729,101 @@ void qmo_surrogate_samples(void *scene, const qm_grid_desc *grid, uint32_t cell_
     });
 }
 
+
+// A receiver's horizons for aircraft screening (popup/src/aircraft/horizons.rs:145-198
+// Horizons::build) on this scene, laid out as write_f32 lays them out (horizons.rs:50-64, 196-201):
+// per point (x, y in steps, fractional allowed), its altitude (m) and the footprint it stands in (0
+// none). Terrain: 32 sectors x 48 samples from 30 m to 8 km growing geometrically, a sample outside
+// the DEM is no terrain (a flat scene's ground is everywhere); buildings: 256 sectors, a 512 m ray
+// each, every building crossing but the point's own footprint's walls and those within 1 cm.
+void qmo_flight_horizons(void *scene, const double *xy, const double *altitude_m, const uint64_t *own,
+                         size_t n, float *out, int threads) {
+    const Scene &s = *static_cast<Scene *>(scene);
+    constexpr int BANDS = 6, TSECT = 32, BSECT = 256, SAMPLES = 48;
+    const double terrain_limits[BANDS] = {500.0, 1000.0, 2000.0, 3500.0, 5500.0, 8000.0};
+    const double building_limits[BANDS] = {16.0, 32.0, 64.0, 128.0, 256.0, 512.0};
+    const double tau = 6.283185307179586;
+    const double growth = std::pow(8000.0 / 30.0, 1.0 / (double)(SAMPLES - 1));
+    const size_t floats = 1 + TSECT * (1 + 2 * BANDS) + 1 + BSECT * (1 + 2 * BANDS);
+    struct Edge {
+        bool set = false;
+        double range = 0.0, tangent = 0.0;
+    };
+    auto band_of = [&](double range, const double *limits) {
+        for (int k = 0; k < BANDS; ++k)
+            if (range <= limits[k] + 0.5) return k;
+        return BANDS - 1;
+    };
+    // SectorEdges::write_f32 of one horizon.
+    auto write = [&](float *at, int sectors, const std::vector<Edge> &edges, const std::vector<double> &steepest,
+                     double all) {
+        at[0] = (float)all;
+        for (int k = 0; k < sectors; ++k) {
+            float *e = at + 1 + k * (1 + 2 * BANDS);
+            e[0] = (float)steepest[k];
+            for (int b = 0; b < BANDS; ++b) {
+                const Edge &edge = edges[k * BANDS + b];
+                e[1 + 2 * b] = edge.set ? (float)edge.range : NAN;
+                e[2 + 2 * b] = edge.set ? (float)edge.tangent : NAN;
+            }
+        }
+    };
+    const bool dem = s.dem_nx != 0;
+    const double dem_x1 = dem ? (double)(s.dem_ox + (int64_t)(s.dem_nx - 1) * s.dem_spacing) : 0.0;
+    const double dem_y1 = dem ? (double)(s.dem_oy + (int64_t)(s.dem_ny - 1) * s.dem_spacing) : 0.0;
+    parallel_for(n, threads, [&](size_t i, int) {
+        const double px = xy[2 * i], py = xy[2 * i + 1], alt = altitude_m[i];
+        float *o = out + i * floats;
+        // Terrain (horizons.rs:154-173)
+        std::vector<Edge> te(TSECT * BANDS);
+        std::vector<double> ts(TSECT, -INFINITY);
+        double tall = -INFINITY;
+        for (int k = 0; k < TSECT; ++k) {
+            const double angle = ((double)k + 0.5) * tau / (double)TSECT;
+            const double dx = std::cos(angle), dy = std::sin(angle);
+            double range = 30.0;
+            for (int j = 0; j < SAMPLES; ++j) {
+                const double qx = px + dx * range / s.step_m, qy = py + dy * range / s.step_m;
+                const bool inside = !dem || (qx >= (double)s.dem_ox && qx <= dem_x1 && qy >= (double)s.dem_oy && qy <= dem_y1);
+                if (inside) {
+                    double z, g;
+                    terrain_at(s, qx, qy, z, g);
+                    const double tangent = (z - alt) / range;
+                    Edge &slot = te[k * BANDS + band_of(range, terrain_limits)];
+                    if (!slot.set || tangent > slot.tangent) slot = Edge{true, range, tangent};
+                    ts[k] = std::max(ts[k], tangent);
+                    tall = std::max(tall, tangent);
+                }
+                range *= growth;
+            }
+        }
+        write(o, TSECT, te, ts, tall);
+        // Buildings (horizons.rs:174-196)
+        std::vector<Edge> be(BSECT * BANDS);
+        std::vector<double> bs(BSECT, -INFINITY);
+        double ball = -INFINITY;
+        std::vector<Crossing> crossings;
+        const double reach = 512.0;
+        for (int k = 0; k < BSECT; ++k) {
+            const double angle = ((double)k + 0.5) * tau / (double)BSECT;
+            const double dx = std::cos(angle), dy = std::sin(angle);
+            const double from[2] = {px, py}, to[2] = {px + dx * reach / s.step_m, py + dy * reach / s.step_m};
+            scene_crossings(s, from, to, crossings);
+            for (const Crossing &c : crossings) {
+                if (!c.building || c.footprint_id == own[i]) continue;
+                const double range = c.t * reach;
+                if (range <= 0.01) continue;
+                double z, g;
+                terrain_at(s, px + dx * range / s.step_m, py + dy * range / s.step_m, z, g);
+                const double tangent = (z + c.height_m - alt) / range;
+                Edge &slot = be[k * BANDS + band_of(range, building_limits)];
+                if (!slot.set || tangent > slot.tangent) slot = Edge{true, range, tangent};
+                bs[k] = std::max(bs[k], tangent);
+                ball = std::max(ball, tangent);
+            }
+        }
+        write(o + 1 + TSECT * (1 + 2 * BANDS), BSECT, be, bs, ball);
+    });
+}
+
 }  // extern "C"

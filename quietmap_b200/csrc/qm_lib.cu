@@ -32,6 +32,7 @@
 #include "../../include/qm_weather.h"
 #include "qm_aircraft.cuh"
 #include "qm_flights.cuh"
+#include "qm_horizons.cuh"
 #include "qm_kernels.cuh"
 #include "qm_linepairs.cuh"
 #include "qm_host.h"
@@ -1737,6 +1738,59 @@ extern "C" qm_status qm_flight_grid(qm_ctx *ctx, const qm_aircraft_type *types, 
         stats->kernel_ms = k_ms;
         stats->loudness_ms = sone ? z_ms : 0.0;
     }
+    return QM_OK;
+}
+
+// ---------------------------------------------------------------------------------------------
+// The points' horizons for aircraft screening (include/qm_flights.h).
+
+extern "C" qm_status qm_scene_flight_horizons(qm_scene *scene, const double *xy_steps, const double *altitude_m,
+                                              const uint64_t *own_footprint, size_t n_points, float *horizons) {
+    NvtxRange nvtx_range("qm_scene_flight_horizons");
+    if (!scene) return fail(QM_ERR_ARGUMENT, "qm_scene_flight_horizons: null scene");
+    if (n_points == 0) return QM_OK;
+    if (!xy_steps || !altitude_m || !own_footprint || !horizons)
+        return fail(QM_ERR_ARGUMENT, "qm_scene_flight_horizons: null points, altitudes, footprints or horizons");
+    if (n_points >= (1ull << 31)) return fail(QM_ERR_ARGUMENT, "qm_scene_flight_horizons: too many points");
+    std::vector<uint32_t> own(n_points);
+    for (size_t i = 0; i < n_points; ++i) {
+        if (!std::isfinite(xy_steps[2 * i]) || !std::isfinite(xy_steps[2 * i + 1]) || !std::isfinite(altitude_m[i]))
+            return fail(QM_ERR_ARGUMENT, "qm_scene_flight_horizons: point " + std::to_string(i) + " position or altitude");
+        own[i] = dense_fp(scene, own_footprint[i]);
+    }
+    qm_ctx *ctx = scene->ctx;
+    std::lock_guard<std::mutex> guard(ctx->lock);
+    QM_CUDA(cudaSetDevice(ctx->device));
+    cudaStream_t stream = ctx->stream;
+    const size_t out_bytes = n_points * QM_HORIZON_FLOATS * sizeof(float);
+    Scratch d_xy, d_alt, d_own, d_out, d_failed;
+    QM_CUDA(cudaMalloc(&d_xy.p, n_points * 2 * sizeof(double)));
+    QM_CUDA(cudaMalloc(&d_alt.p, n_points * sizeof(double)));
+    QM_CUDA(cudaMalloc(&d_own.p, n_points * sizeof(uint32_t)));
+    QM_CUDA(cudaMalloc(&d_out.p, out_bytes));
+    QM_CUDA(cudaMalloc(&d_failed.p, n_points * sizeof(unsigned)));
+    QM_CUDA(cudaMemcpyAsync(d_xy.p, xy_steps, n_points * 2 * sizeof(double), cudaMemcpyHostToDevice, stream));
+    QM_CUDA(cudaMemcpyAsync(d_alt.p, altitude_m, n_points * sizeof(double), cudaMemcpyHostToDevice, stream));
+    QM_CUDA(cudaMemcpyAsync(d_own.p, own.data(), n_points * sizeof(uint32_t), cudaMemcpyHostToDevice, stream));
+    QM_CUDA(cudaMemsetAsync(d_failed.p, 0, n_points * sizeof(unsigned), stream));
+    qm::hz::Args H{};
+    H.xy = static_cast<const double *>(d_xy.p);
+    H.altitude_m = static_cast<const double *>(d_alt.p);
+    H.own = static_cast<const uint32_t *>(d_own.p);
+    H.n = (uint32_t)n_points;
+    H.growth = std::pow(8000.0 / 30.0, 1.0 / (double)(qm::hz::SAMPLES - 1));  // horizons.rs:155-156
+    H.out = static_cast<float *>(d_out.p);
+    H.failed = static_cast<unsigned *>(d_failed.p);
+    qm::hz::flight_horizons_kernel<<<(unsigned)n_points, qm::hz::THREADS, 0, stream>>>(scene->dev, H);
+    QM_CUDA(cudaGetLastError());
+    std::vector<unsigned> failed(n_points);
+    QM_CUDA(cudaMemcpyAsync(horizons, d_out.p, out_bytes, cudaMemcpyDeviceToHost, stream));
+    QM_CUDA(cudaMemcpyAsync(failed.data(), d_failed.p, n_points * sizeof(unsigned), cudaMemcpyDeviceToHost, stream));
+    QM_CUDA(cudaStreamSynchronize(stream));
+    for (size_t i = 0; i < n_points; ++i)
+        if (failed[i])
+            return fail(QM_ERR_CAPACITY, "qm_scene_flight_horizons: a ray from point " + std::to_string(i) +
+                                             " crosses more than 256 edges");
     return QM_OK;
 }
 

@@ -135,16 +135,17 @@ __device__ __noinline__ bool edge_bounds_roof_d(const SceneDev &S, double sx, do
     return n0 * n1 < 0.0;
 }
 
-// Every crossing of the segment from the fractional point (sx, sy) to the lattice point (rx, ry)
+// Every crossing of the segment from the fractional point (sx, sy) to the point (rx, ry) (a lattice
+// point for a path, fractional for a horizon's ray)
 // with an obstacle edge (crossings.rs:163-226 in f64): the cells the segment passes in order, and
 // in each cell the edges whose box meets the segment's piece in the cell (padded by 1e-9 of the
 // segment's size), each tested by segment_intersection_t (crossings.rs:13-28); then sorted and
 // deduplicated as list_crossings does, without the receiver's own walls.
 template <int MAXC>
-__device__ int list_crossings_d(const SceneDev &S, double sx, double sy, int rx, int ry, uint32_t rcv_own, XRec *xs,
-                                uint32_t &status, uint32_t &edges_tested) {
+__device__ int list_crossings_d(const SceneDev &S, double sx, double sy, double rx, double ry, uint32_t rcv_own,
+                                XRec *xs, uint32_t &status, uint32_t &edges_tested) {
     int n = 0;
-    const double ex_ = (double)rx, ey_ = (double)ry;
+    const double ex_ = rx, ey_ = ry;
     const double d0 = __dsub_rn(ex_, sx), d1 = __dsub_rn(ey_, sy);
     const double cs = (double)S.cell_steps;
     long long cell[2] = {(long long)floor(__ddiv_rn(sx, cs)), (long long)floor(__ddiv_rn(sy, cs))};
