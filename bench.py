@@ -63,7 +63,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="terrain", choices=["terrain", "road", "flights", "surrogate", "surrogate_terrain", "tiles", "loudness",
-                             "flight_sums"])
+                             "flight_sums", "horizons"])
     ap.add_argument("--tiles", type=int, default=32, help="tiles workload: tiles per batch, drawn from the 4096")
     ap.add_argument("--flights", type=int, default=2000, help="flights workload: flights (a small case for profiling)")
     ap.add_argument("--cells-side", type=int, default=1024, help="flights workload: receivers per side")
@@ -286,6 +286,8 @@ def main():
         return loudness(args, rank, world, local)
     if args.workload == "flight_sums":
         return flight_sums(args, rank, world, local)
+    if args.workload == "horizons":
+        return horizons(args, rank, world, local)
     import torch
     from quietmap_b200 import native
     scene, steps, desc = workload(args.workload, rank, args.slices, args.sources)
@@ -860,6 +862,79 @@ def flight_sums(args, rank, world, local):
         print(json.dumps(line), flush=True)
     dev.close()
     ctx.close()
+
+
+def horizons(args, rank, world, local):
+    """The points' horizons for aircraft screening on the device (Horizons::build, which the
+    reference runs on the cores for every flight request): the terrain square (16 km^2, fBm DEM,
+    30,000 buildings), a step builds a 64^2 lattice of points' horizons (32 terrain sectors x 48
+    samples, 256 building rays of 512 m each)."""
+    import torch
+    from quietmap_b200 import native, scenes
+    scene, _ = scenes.terrain_square()
+    ext = np.array(scene.extent_steps, dtype=np.float64)
+    n = args.lattice_side
+    xs = (np.arange(n) + 0.5) / n
+    xy = np.stack(np.meshgrid(xs * ext[0], xs * ext[1]), -1).reshape(-1, 2)
+    ctx = native.Context(local if world > 1 else 0)
+    torch.cuda.set_device(local if world > 1 else 0)
+    dev = ctx.scene(scene)
+    alt = np.full(len(xy), 4.0) + scenes_ground(scene, xy)
+    own = np.zeros(len(xy), np.uint64)
+    for _ in range(args.warmup):
+        dev.flight_horizons(xy, alt, own)
+    k_ms, wall = 0.0, 0.0
+    with ClockSampler(local) as clocks:
+        for _ in range(args.steps):
+            t0 = time.perf_counter()
+            got, ms = dev.flight_horizons(xy, alt, own, stats=True)
+            wall += time.perf_counter() - t0
+            k_ms += ms
+    if rank == 0:
+        pts = len(xy)
+        line = {
+            "metric": "receiver horizons/s for aircraft screening (Horizons::build), 1 B200", "value": pts * args.steps / (k_ms / 1e3),
+            "unit": "points/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": k_ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic (seeded terrain square)",
+            "config": {"workload": f"{n}^2 lattice points over the terrain square (16 km^2, 30,000 buildings): "
+                                   "32 terrain sectors x 48 samples and 256 building rays of 512 m a point"},
+            "e2e": {"value": pts * args.steps / wall, "unit": "points/s", "h2d_bytes_per_step": pts * 28,
+                    "d2h_bytes_per_step": int(got.nbytes)},
+            "clocks": clocks.summary(), "gpu_launches": args.steps,
+        }
+        if not args.no_cpu_baseline and world == 1:
+            from oracle import oracle
+            ora = oracle.OracleScene(scene)
+            threads = oracle.threads()
+            m = len(xy)  # the whole lattice: a fraction of a second on 16 threads
+            t0 = time.perf_counter()
+            want = ora.flight_horizons(xy[:m], alt[:m], own[:m], threads)
+            dt = time.perf_counter() - t0
+            same = bool(np.array_equal(np.nan_to_num(got[:m], nan=7.0, neginf=-7.0),
+                                       np.nan_to_num(want, nan=7.0, neginf=-7.0)))
+            line["cpu_baseline"] = dict(value=m / dt, unit="points/s", cores=threads, kind="port",
+                                        sample=f"the lattice's {m} points ({dt:.2f} s)")
+            line["parity"] = {"points": m, "bit_identical": same}
+        print(json.dumps(line), flush=True)
+    dev.close()
+    ctx.close()
+
+
+def scenes_ground(scene, xy):
+    """The ground (m) under lattice positions of a scene: its DEM bilinear, or its flat ground."""
+    if scene.dem_altitude is None:
+        return np.full(len(xy), scene.flat_altitude_m if hasattr(scene, "flat_altitude_m") else 0.0)
+    z = np.asarray(scene.dem_altitude, dtype=np.float64)
+    sp, ox, oy = scene.dem_spacing, scene.dem_origin[0], scene.dem_origin[1]
+    fx = np.clip((xy[:, 0] - ox) / sp, 0, z.shape[1] - 1)
+    fy = np.clip((xy[:, 1] - oy) / sp, 0, z.shape[0] - 1)
+    i0 = np.minimum(np.floor(fx).astype(int), z.shape[1] - 2)
+    j0 = np.minimum(np.floor(fy).astype(int), z.shape[0] - 2)
+    ax, ay = fx - i0, fy - j0
+    lo = z[j0, i0] + ax * (z[j0, i0 + 1] - z[j0, i0])
+    hi = z[j0 + 1, i0] + ax * (z[j0 + 1, i0 + 1] - z[j0 + 1, i0])
+    return lo + ay * (hi - lo)
 
 
 def abi_flight_sums():

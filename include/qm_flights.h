@@ -120,9 +120,11 @@ qm_status qm_flight_sums(qm_ctx *ctx, const qm_flight_boxes *boxes, const qm_fli
  * QM_HORIZON_FLOATS floats into `horizons` (n_points x QM_HORIZON_FLOATS) as qm_flight_sums reads
  * them. Terrain: 32 sectors x 48 samples from 30 m to 8 km growing geometrically, a sample outside
  * the scene's DEM is no terrain; buildings: 256 sectors, a 512 m ray each, the crossings within
- * 1 cm left out. QM_ERR_CAPACITY when a ray crosses more than 256 edges. */
+ * 1 cm left out. QM_ERR_CAPACITY when a ray crosses more than 256 edges. kernel_ms (nullable): the
+ * kernel's device time. */
 qm_status qm_scene_flight_horizons(qm_scene *scene, const double *xy_steps, const double *altitude_m,
-                                   const uint64_t *own_footprint, size_t n_points, float *horizons);
+                                   const uint64_t *own_footprint, size_t n_points, float *horizons,
+                                   double *kernel_ms);
 
 #ifdef __cplusplus
 }

@@ -1745,8 +1745,10 @@ extern "C" qm_status qm_flight_grid(qm_ctx *ctx, const qm_aircraft_type *types, 
 // The points' horizons for aircraft screening (include/qm_flights.h).
 
 extern "C" qm_status qm_scene_flight_horizons(qm_scene *scene, const double *xy_steps, const double *altitude_m,
-                                              const uint64_t *own_footprint, size_t n_points, float *horizons) {
+                                              const uint64_t *own_footprint, size_t n_points, float *horizons,
+                                              double *kernel_ms) {
     NvtxRange nvtx_range("qm_scene_flight_horizons");
+    if (kernel_ms) *kernel_ms = 0.0;
     if (!scene) return fail(QM_ERR_ARGUMENT, "qm_scene_flight_horizons: null scene");
     if (n_points == 0) return QM_OK;
     if (!xy_steps || !altitude_m || !own_footprint || !horizons)
@@ -1781,12 +1783,21 @@ extern "C" qm_status qm_scene_flight_horizons(qm_scene *scene, const double *xy_
     H.growth = std::pow(8000.0 / 30.0, 1.0 / (double)(qm::hz::SAMPLES - 1));  // horizons.rs:155-156
     H.out = static_cast<float *>(d_out.p);
     H.failed = static_cast<unsigned *>(d_failed.p);
+    Events ev;
+    QM_CUDA(ev.create());
+    QM_CUDA(cudaEventRecord(ev.e0, stream));
     qm::hz::flight_horizons_kernel<<<(unsigned)n_points, qm::hz::THREADS, 0, stream>>>(scene->dev, H);
     QM_CUDA(cudaGetLastError());
+    QM_CUDA(cudaEventRecord(ev.e1, stream));
     std::vector<unsigned> failed(n_points);
     QM_CUDA(cudaMemcpyAsync(horizons, d_out.p, out_bytes, cudaMemcpyDeviceToHost, stream));
     QM_CUDA(cudaMemcpyAsync(failed.data(), d_failed.p, n_points * sizeof(unsigned), cudaMemcpyDeviceToHost, stream));
     QM_CUDA(cudaStreamSynchronize(stream));
+    if (kernel_ms) {
+        float ms = 0.f;
+        QM_CUDA(cudaEventElapsedTime(&ms, ev.e0, ev.e1));
+        *kernel_ms = ms;
+    }
     for (size_t i = 0; i < n_points; ++i)
         if (failed[i])
             return fail(QM_ERR_CAPACITY, "qm_scene_flight_horizons: a ray from point " + std::to_string(i) +

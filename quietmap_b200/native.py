@@ -172,7 +172,7 @@ def lib():
         L.qm_pixel_loudness.argtypes = [C.c_void_p, C.POINTER(C.c_float), C.c_size_t, _U64, C.c_size_t, C.c_uint32,
                                         C.c_double, _D, C.c_size_t, _U32, _F, _D]
         L.qm_pixel_loudness.restype = C.c_int
-        L.qm_scene_flight_horizons.argtypes = [C.c_void_p, _D, _D, _U64, C.c_size_t, _F]
+        L.qm_scene_flight_horizons.argtypes = [C.c_void_p, _D, _D, _U64, C.c_size_t, _F, _D]
         L.qm_scene_flight_horizons.restype = C.c_int
         L.qm_flight_boxes_upload.argtypes = [C.c_void_p, C.c_void_p, C.c_size_t, C.POINTER(C.c_void_p)]
         L.qm_flight_boxes_upload.restype = C.c_int
@@ -839,17 +839,19 @@ class DeviceScene:
                                              vertices=stats.vertices, candidates=stats.candidates,
                                              kernel_ms=stats.kernel_ms, paint_ms=stats.paint_ms)
 
-    def flight_horizons(self, xy_steps, altitude_m, own_footprint):
+    def flight_horizons(self, xy_steps, altitude_m, own_footprint, stats=False):
         """Each point's horizons for aircraft screening built on the device (qm_scene_flight_horizons):
-        [n][HORIZON_FLOATS] float32, as qm_flight_sums reads them."""
+        [n][HORIZON_FLOATS] float32, as qm_flight_sums reads them, and the kernel's device time (ms)
+        when `stats`."""
         xy = np.ascontiguousarray(np.asarray(xy_steps, dtype=np.float64).reshape(-1, 2))
         alt = np.ascontiguousarray(np.asarray(altitude_m, dtype=np.float64).reshape(-1))
         own = np.ascontiguousarray(np.asarray(own_footprint, dtype=np.uint64).reshape(-1))
         out = np.zeros((len(xy), abi.HORIZON_FLOATS), np.float32)
+        ms = C.c_double(0.0)
         _check(lib().qm_scene_flight_horizons(self.handle, abi.ptr(xy, C.c_double), abi.ptr(alt, C.c_double),
-                                              abi.ptr(own, C.c_uint64), len(xy), abi.ptr(out, C.c_float)),
-               self.ctx.handle)
-        return out
+                                              abi.ptr(own, C.c_uint64), len(xy), abi.ptr(out, C.c_float),
+                                              C.byref(ms)), self.ctx.handle)
+        return (out, ms.value) if stats else out
 
     def surrogate_samples(self, grid):
         """Every path of `grid`: (raw features [rows][32], exact A_boundary labels [rows][8] dB,
