@@ -126,6 +126,15 @@ qm_status qm_scene_flight_horizons(qm_scene *scene, const double *xy_steps, cons
                                    const uint64_t *own_footprint, size_t n_points, float *horizons,
                                    double *kernel_ms);
 
+/* qm_flight_sums with the points' horizons built on the device from the scene (as
+ * qm_scene_flight_horizons builds them) and read there, nothing of them crossing to the host. The
+ * points' positions are in the square's metres, the scene's lattice steps being step_m metres from
+ * the same origin; their `horizons` fields are ignored; own_footprint (nullable) names the footprint
+ * each stands in. The boxes must belong to the scene's context. */
+qm_status qm_flight_sums_on_scene(qm_scene *scene, const qm_flight_boxes *boxes, const qm_flight_point *points,
+                                  const uint64_t *own_footprint, size_t n_points, const qm_box_segment *segments,
+                                  size_t n_segments, double *sums, size_t n_sums, qm_flight_sums_stats *stats);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1942,11 +1942,21 @@ extern "C" void qm_flight_boxes_free(qm_flight_boxes *boxes) {
     ctx_release(ctx);
 }
 
-extern "C" qm_status qm_flight_sums(qm_ctx *ctx, const qm_flight_boxes *boxes, const qm_flight_point *points,
-                                    size_t n_points, const float *horizons, size_t n_horizon_floats,
-                                    const qm_box_segment *segments, size_t n_segments, double *sums, size_t n_sums,
-                                    qm_flight_sums_stats *stats) {
-    NvtxRange nvtx_range("qm_flight_sums");
+// qm_flight_sums, and with a scene qm_flight_sums_on_scene: the points' horizons then come from the
+// horizons kernel into the handle's device buffer (each point's at its own row) and go nowhere else.
+static qm_status flight_sums_impl(qm_ctx *ctx, const qm_flight_boxes *boxes, qm_scene *scene,
+                                  const uint64_t *own_footprint, const qm_flight_point *points_in, size_t n_points,
+                                  const float *horizons, size_t n_horizon_floats, const qm_box_segment *segments,
+                                  size_t n_segments, double *sums, size_t n_sums, qm_flight_sums_stats *stats) {
+    // On a scene every point reads its own row of the horizons built on the device.
+    std::vector<qm_flight_point> own_rows;
+    const qm_flight_point *points = points_in;
+    if (scene && points_in) {
+        own_rows.assign(points_in, points_in + n_points);
+        for (size_t i = 0; i < n_points; ++i) own_rows[i].horizons = (uint64_t)i * QM_HORIZON_FLOATS;
+        points = own_rows.data();
+        n_horizon_floats = n_points * QM_HORIZON_FLOATS;
+    }
     using qm::fl::Slice;
     if (!ctx || !boxes || boxes->ctx != ctx) return fail(QM_ERR_ARGUMENT, "qm_flight_sums: null ctx, or boxes of another context");
     if (n_sums && !sums) return fail(QM_ERR_ARGUMENT, "qm_flight_sums: sums is null");
@@ -1958,7 +1968,7 @@ extern "C" qm_status qm_flight_sums(qm_ctx *ctx, const qm_flight_boxes *boxes, c
         if (!std::isfinite(p.x) || !std::isfinite(p.y) || !std::isfinite(p.altitude_m) ||
             !(p.impedance_gain >= 0.0) || !std::isfinite(p.impedance_gain))
             return fail(QM_ERR_ARGUMENT, "qm_flight_sums: point " + std::to_string(i) + " position or impedance gain");
-        if (horizons && (p.horizons > n_horizon_floats || n_horizon_floats - p.horizons < QM_HORIZON_FLOATS))
+        if ((horizons || scene) && (p.horizons > n_horizon_floats || n_horizon_floats - p.horizons < QM_HORIZON_FLOATS))
             return fail(QM_ERR_ARGUMENT, "qm_flight_sums: point " + std::to_string(i) + " horizons outside the horizon floats");
     }
     // The segments grouped by sum (a counting sort keeps each group in the caller's order).
@@ -2007,11 +2017,51 @@ extern "C" qm_status qm_flight_sums(qm_ctx *ctx, const qm_flight_boxes *boxes, c
     std::lock_guard<std::mutex> guard(ctx->lock);
     QM_CUDA(cudaSetDevice(ctx->device));
     cudaStream_t stream = ctx->stream;
+    GrowBuffer d_failed;
+    if (scene && n_points) {
+        // The horizons on the device (qm_scene_flight_horizons' kernel), positions in the scene's steps.
+        std::vector<double> xy(2 * n_points), alt(n_points);
+        std::vector<uint32_t> own(n_points);
+        for (size_t i = 0; i < n_points; ++i) {
+            xy[2 * i] = points[i].x / scene->step_m;
+            xy[2 * i + 1] = points[i].y / scene->step_m;
+            alt[i] = points[i].altitude_m;
+            own[i] = own_footprint ? dense_fp(scene, own_footprint[i]) : 0u;
+        }
+        GrowBuffer d_xy, d_alt, d_own;
+        QM_CUDA(d_xy.reserve(xy.size() * sizeof(double)));
+        QM_CUDA(d_alt.reserve(alt.size() * sizeof(double)));
+        QM_CUDA(d_own.reserve(own.size() * sizeof(uint32_t)));
+        QM_CUDA(d_failed.reserve(n_points * sizeof(unsigned)));
+        QM_CUDA(h->horizons.reserve(n_horizon_floats * sizeof(float)));
+        QM_CUDA(cudaMemcpyAsync(d_xy.p, xy.data(), xy.size() * sizeof(double), cudaMemcpyHostToDevice, stream));
+        QM_CUDA(cudaMemcpyAsync(d_alt.p, alt.data(), alt.size() * sizeof(double), cudaMemcpyHostToDevice, stream));
+        QM_CUDA(cudaMemcpyAsync(d_own.p, own.data(), own.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, stream));
+        QM_CUDA(cudaMemsetAsync(d_failed.p, 0, n_points * sizeof(unsigned), stream));
+        qm::hz::Args H{};
+        H.xy = static_cast<const double *>(d_xy.p);
+        H.altitude_m = static_cast<const double *>(d_alt.p);
+        H.own = static_cast<const uint32_t *>(d_own.p);
+        H.n = (uint32_t)n_points;
+        H.growth = std::pow(8000.0 / 30.0, 1.0 / (double)(qm::hz::SAMPLES - 1));  // horizons.rs:155-156
+        H.out = static_cast<float *>(h->horizons.p);
+        H.failed = static_cast<unsigned *>(d_failed.p);
+        qm::hz::flight_horizons_kernel<<<(unsigned)n_points, qm::hz::THREADS, 0, stream>>>(scene->dev, H);
+        QM_CUDA(cudaGetLastError());
+        std::vector<unsigned> failed(n_points);
+        QM_CUDA(cudaMemcpyAsync(failed.data(), d_failed.p, n_points * sizeof(unsigned), cudaMemcpyDeviceToHost, stream));
+        QM_CUDA(cudaStreamSynchronize(stream));
+        for (size_t i = 0; i < n_points; ++i)
+            if (failed[i])
+                return fail(QM_ERR_CAPACITY, "qm_flight_sums_on_scene: a horizon ray from point " + std::to_string(i) +
+                                                 " crosses more than 256 edges");
+    }
+    const bool resident = scene != nullptr;  // the horizons are on the device already
     const size_t sum_bytes = n_sums * QM_FLIGHT_SUMS * sizeof(double);
     QM_CUDA(h->sums.reserve(sum_bytes));
     QM_CUDA(h->heard.reserve(sizeof(unsigned long long)));
     QM_CUDA(h->points.reserve(n_points * sizeof(qm_flight_point)));
-    QM_CUDA(h->horizons.reserve(horizons ? n_horizon_floats * sizeof(float) : 0));
+    if (!resident) QM_CUDA(h->horizons.reserve(horizons ? n_horizon_floats * sizeof(float) : 0));
     QM_CUDA(h->segments.reserve(n_segments * sizeof(qm_box_segment)));
     QM_CUDA(h->order.reserve(order.size() * sizeof(uint32_t)));
     QM_CUDA(h->read_start.reserve(read_start.size() * sizeof(uint64_t)));
@@ -2032,7 +2082,7 @@ extern "C" qm_status qm_flight_sums(qm_ctx *ctx, const qm_flight_boxes *boxes, c
         QM_CUDA(cudaMemcpyAsync(h->slices.p, slices.data(), slices.size() * sizeof(Slice), cudaMemcpyHostToDevice, stream));
         if (!h->copies) QM_CUDA(cudaStreamCreateWithFlags(&h->copies, cudaStreamNonBlocking));
         QM_CUDA(h->pinned_sums.reserve(sum_bytes));
-        if (horizons) QM_CUDA(h->pinned_horizons.reserve(n_horizon_floats * sizeof(float)));
+        if (horizons && !resident) QM_CUDA(h->pinned_horizons.reserve(n_horizon_floats * sizeof(float)));
         // Batches of whole request bands, each with the prefix of the horizons its points read: a
         // batch's horizons go up (through pinned memory, on the copies' stream) while the batch before
         // it computes, and its sums come down while the batches after it compute.
@@ -2069,7 +2119,7 @@ extern "C" qm_status qm_flight_sums(qm_ctx *ctx, const qm_flight_boxes *boxes, c
         qm::fl::SumsArgs A{};
         A.boxes = h->boxes;
         A.points = static_cast<const qm_flight_point *>(h->points.p);
-        A.horizons = horizons ? static_cast<const float *>(h->horizons.p) : nullptr;
+        A.horizons = (horizons || resident) ? static_cast<const float *>(h->horizons.p) : nullptr;
         A.segments = static_cast<const qm_box_segment *>(h->segments.p);
         A.order = static_cast<const uint32_t *>(h->order.p);
         A.read_start = static_cast<const uint64_t *>(h->read_start.p);
@@ -2087,7 +2137,7 @@ extern "C" qm_status qm_flight_sums(qm_ctx *ctx, const qm_flight_boxes *boxes, c
         size_t have = 0;  // horizon floats already sent
         for (size_t bi = 0; bi < batches; ++bi) {
             const Slice &first = slices[cut[bi]], &last = slices[cut[bi + 1] - 1];
-            if (horizons) {
+            if (horizons && !resident) {
                 size_t need = have;
                 for (uint32_t j = first.seg_begin; j < last.seg_end; ++j)
                     need = std::max<size_t>(need, points[segments[order[j]].point].horizons + QM_HORIZON_FLOATS);
@@ -2132,6 +2182,28 @@ extern "C" qm_status qm_flight_sums(qm_ctx *ctx, const qm_flight_boxes *boxes, c
         stats->kernel_ms = kernel_ms;
     }
     return QM_OK;
+}
+
+extern "C" qm_status qm_flight_sums(qm_ctx *ctx, const qm_flight_boxes *boxes, const qm_flight_point *points,
+                                    size_t n_points, const float *horizons, size_t n_horizon_floats,
+                                    const qm_box_segment *segments, size_t n_segments, double *sums, size_t n_sums,
+                                    qm_flight_sums_stats *stats) {
+    NvtxRange nvtx_range("qm_flight_sums");
+    return flight_sums_impl(ctx, boxes, nullptr, nullptr, points, n_points, horizons, n_horizon_floats, segments,
+                            n_segments, sums, n_sums, stats);
+}
+
+extern "C" qm_status qm_flight_sums_on_scene(qm_scene *scene, const qm_flight_boxes *boxes,
+                                             const qm_flight_point *points, const uint64_t *own_footprint,
+                                             size_t n_points, const qm_box_segment *segments, size_t n_segments,
+                                             double *sums, size_t n_sums, qm_flight_sums_stats *stats) {
+    NvtxRange nvtx_range("qm_flight_sums_on_scene");
+    if (!scene) return fail(QM_ERR_ARGUMENT, "qm_flight_sums_on_scene: null scene");
+    for (size_t i = 0; points && i < n_points; ++i)
+        if (!std::isfinite(points[i].x) || !std::isfinite(points[i].y))
+            return fail(QM_ERR_ARGUMENT, "qm_flight_sums_on_scene: point " + std::to_string(i) + " position");
+    return flight_sums_impl(scene->ctx, boxes, scene, own_footprint, points, n_points, nullptr, 0, segments, n_segments,
+                            sums, n_sums, stats);
 }
 
 // ---------------------------------------------------------------------------------------------

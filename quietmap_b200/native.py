@@ -173,6 +173,9 @@ def lib():
                                         C.c_double, _D, C.c_size_t, _U32, _F, _D]
         L.qm_pixel_loudness.restype = C.c_int
         L.qm_scene_flight_horizons.argtypes = [C.c_void_p, _D, _D, _U64, C.c_size_t, _F, _D]
+        L.qm_flight_sums_on_scene.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, _U64, C.c_size_t, C.c_void_p,
+                                              C.c_size_t, _D, C.c_size_t, C.POINTER(abi.FlightSumsStats)]
+        L.qm_flight_sums_on_scene.restype = C.c_int
         L.qm_scene_flight_horizons.restype = C.c_int
         L.qm_flight_boxes_upload.argtypes = [C.c_void_p, C.c_void_p, C.c_size_t, C.POINTER(C.c_void_p)]
         L.qm_flight_boxes_upload.restype = C.c_int
@@ -236,6 +239,22 @@ class DeviceFlightBoxes:
                                     None if h is None else abi.ptr(h, C.c_float), 0 if h is None else len(h),
                                     s.ctypes.data if len(s) else None, len(s), abi.ptr(out, C.c_double), n_sums,
                                     C.byref(st)), self.ctx.handle)
+        if stats:
+            return out, dict(box_reads=st.box_reads, boxes_heard=st.boxes_heard, kernel_ms=st.kernel_ms)
+        return out
+
+    def sums_on_scene(self, device_scene, points, own_footprint, segments, n_sums, stats=False):
+        """`sums` with the points' horizons built and read on the device from `device_scene`
+        (qm_flight_sums_on_scene); the points' positions in the square's metres."""
+        p = np.ascontiguousarray(points, dtype=abi.FLIGHT_POINT_DTYPE)
+        own = None if own_footprint is None else np.ascontiguousarray(own_footprint, dtype=np.uint64)
+        s = np.ascontiguousarray(segments, dtype=abi.BOX_SEGMENT_DTYPE)
+        out = np.zeros((n_sums, abi.FLIGHT_SUMS))
+        st = abi.FlightSumsStats()
+        _check(lib().qm_flight_sums_on_scene(device_scene.handle, self.handle, p.ctypes.data if len(p) else None,
+                                             None if own is None else abi.ptr(own, C.c_uint64), len(p),
+                                             s.ctypes.data if len(s) else None, len(s), abi.ptr(out, C.c_double),
+                                             n_sums, C.byref(st)), self.ctx.handle)
         if stats:
             return out, dict(box_reads=st.box_reads, boxes_heard=st.boxes_heard, kernel_ms=st.kernel_ms)
         return out

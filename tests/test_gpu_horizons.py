@@ -81,3 +81,37 @@ def test_bad_points_are_refused():
         dev.flight_horizons([[10.0, 10.0], [np.nan, 3.0]], [4.0, 4.0], [0, 0])
     dev.close()
     ctx.close()
+
+
+def test_flight_sums_on_the_scene_read_the_scenes_horizons():
+    """qm_flight_sums_on_scene builds the horizons on the device and sums through them: the sums of
+    qm_flight_sums given qm_scene_flight_horizons' floats from the host (the lattice step is a power
+    of two, so the points' metres divide back to the same steps), up to the order in which the
+    kernel's FP64 atomic additions land (1e-12 relative), and within the horizons' own 1e-5
+    rounding of the oracle's sums through the oracle's horizons."""
+    scene = scenes.terrain_square(scale=0.125)[0]
+    ora = oracle.OracleScene(scene)
+    rng = np.random.default_rng(79)
+    xy, alt, own = _points(scene, ora, rng, 12)
+    world = scenes.flight_boxes_square(seed=17, n_flights=80, receivers=64)
+    points, _, segs, n_sums = scenes.flight_requests(world, xy * scene.step_m, horizons=False)
+    points["altitude_m"] = alt
+    ctx = native.Context(0)
+    dev = ctx.scene(scene)
+    boxes = ctx.flight_boxes(world.boxes)
+    got, st = boxes.sums_on_scene(dev, points, own, segs, n_sums, stats=True)
+    assert np.frexp(scene.step_m)[0] == 0.5  # a power of two
+    rows = points.copy()
+    rows["horizons"] = np.arange(len(rows), dtype=np.uint64) * abi.HORIZON_FLOATS
+    same = boxes.sums(rows, dev.flight_horizons(xy, alt, own).reshape(-1), segs, n_sums)
+    assert np.array_equal(got != 0.0, same != 0.0)
+    assert (np.abs(got - same) <= 1e-12 * np.abs(same)).all()
+    hz = ora.flight_horizons(xy, alt, own)
+    want, heard = oracle.flight_sums(world.boxes, rows, hz.reshape(-1), segs, n_sums)
+    assert st["boxes_heard"] == heard > 0
+    rel = np.abs(got - want) / np.maximum(np.abs(want), 1e-300)
+    rel[want == 0] = np.abs(got[want == 0])
+    assert rel.max() < 1e-6, float(rel.max())
+    boxes.close()
+    dev.close()
+    ctx.close()
