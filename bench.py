@@ -903,6 +903,7 @@ def horizons(args, rank, world, local):
                     "d2h_bytes_per_step": int(got.nbytes)},
             "clocks": clocks.summary(), "gpu_launches": args.steps,
         }
+        line["flight_sums_on_scene"] = flight_sums_on_scene(args, rank, ctx, dev, scene, xy, alt, own)
         if not args.no_cpu_baseline and world == 1:
             from oracle import oracle
             ora = oracle.OracleScene(scene)
@@ -919,6 +920,41 @@ def horizons(args, rank, world, local):
         print(json.dumps(line), flush=True)
     dev.close()
     ctx.close()
+
+
+def flight_sums_on_scene(args, rank, ctx, dev, scene, xy, alt, own):
+    """Batch::flight_sums for the lattice's points end to end, their horizons built on the device
+    and read there (qm_flight_sums_on_scene), against the same sums through two calls: the horizons
+    down to the host (qm_scene_flight_horizons) and up again with the requests (qm_flight_sums).
+    The boxes are the flight workload's (2000 flights over the 102.4 km square); the points hear
+    every aircraft tile within 16 km of the terrain square's corner of it."""
+    from quietmap_b200 import scenes
+    world_boxes = scenes.flight_boxes_square(seed=3 + rank, n_flights=args.flights, receivers=args.cells_side)
+    points, _, segs, n_sums = scenes.flight_requests(world_boxes, xy * scene.step_m, horizons=False, seed=5 + rank)
+    points["altitude_m"] = alt
+    boxes = ctx.flight_boxes(world_boxes.boxes)
+    for _ in range(args.warmup):
+        boxes.sums_on_scene(dev, points, own, segs, n_sums)
+    one = two = 0.0
+    worst = 0.0
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        a = boxes.sums_on_scene(dev, points, own, segs, n_sums)
+        one += time.perf_counter() - t0
+        t0 = time.perf_counter()
+        hz = dev.flight_horizons(xy, alt, own)
+        b = boxes.sums(points, hz.reshape(-1), segs, n_sums)
+        two += time.perf_counter() - t0
+        rel = np.where(b != 0.0, np.abs(a - b) / np.maximum(np.abs(b), 1e-300), np.abs(a))
+        worst = max(worst, float(rel.max()))
+    boxes.close()
+    pts = len(points)
+    return {"value": pts * args.steps / one, "unit": "points/s", "two_calls_value": pts * args.steps / two,
+            "speedup_vs_two_calls": two / one, "box_reads_per_step": int(segs["count"].sum()),
+            "horizon_bytes_kept_on_device_per_step": 2 * int(hz.nbytes),
+            "h2d_bytes_per_step": int(points.nbytes + segs.nbytes + pts * 28),
+            "d2h_bytes_per_step": int(n_sums * abi_flight_sums() * 8),
+            "max_relative_difference_vs_two_calls": worst}
 
 
 def scenes_ground(scene, xy):
