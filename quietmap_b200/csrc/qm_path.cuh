@@ -524,7 +524,7 @@ struct TerrainWalk {
     int stage;  // 0 start, 1 inner, 2 end, 3 done
     float2 start_zg, end_zg;
 
-    __device__ void init(const SceneDev &S, int x0, int y0, int x1, int y1, float length_m) {
+    __device__ __forceinline__ void init(const SceneDev &S, int x0, int y0, int x1, int y1, float length_m) {
         long long dx = (long long)x1 - x0, dy = (long long)y1 - y0;
         adx = dx >= 0 ? dx : -dx;
         ady = dy >= 0 ? dy : -dy;
@@ -646,9 +646,10 @@ struct BuildingHit {
     float x, top, zt, g;
 };
 
+// 32 bytes: the next segment's origin is the profile at the entry's own x (the source end's at x = 0).
 struct HullEntry {
     float x, z;    // the point of the band
-    float ox, oz;  // the profile at x: its origin for the next segment
+    float oz;      // the profile's height at x: the next segment's origin is (x, oz)
     float og;      // G at x
     Moments seg;   // profile from the previous entry's origin to x, about that origin
 };
@@ -697,7 +698,7 @@ struct Band {
     Moments open;
     bool failed;
 
-    __device__ void init(HullEntry *storage, PlanePoint s, PlanePoint r, float z0, float g0) {
+    __device__ __forceinline__ void init(HullEntry *storage, PlanePoint s, PlanePoint r, float z0, float g0) {
         S = s;
         R = r;
         float dx = r.x - s.x, dz = r.z - s.z;
@@ -706,7 +707,7 @@ struct Band {
         slope_sr = dz / dx;
         if (STATE == QM_FAV) sag_sr = make_sag(radius, s, r);
         h = storage;
-        h[0] = HullEntry{s.x, s.z, 0.0f, z0, g0, moments_zero()};
+        h[0] = HullEntry{s.x, s.z, z0, g0, moments_zero()};
         n = 1;
         blocked = false;
         have_best = false;
@@ -722,7 +723,7 @@ struct Band {
         open = join(open, rebase(seg, sx0, sz0, oox, ooz));
     }
 
-    __device__ void push(float px, float pz, float oz, float og) {
+    __device__ __forceinline__ void push(float px, float pz, float oz, float og) {
         Moments seg = open;
         while (n >= 2) {
             const HullEntry &a = h[n - 2];
@@ -735,7 +736,7 @@ struct Band {
                 under = b.z <= ray_altitude<STATE>(radius, PlanePoint{a.x, a.z}, PlanePoint{px, pz}, b.x);
             }
             if (under) {
-                seg = join(b.seg, rebase(seg, b.ox, b.oz, a.ox, a.oz));
+                seg = join(b.seg, rebase(seg, b.x, b.oz, a.x, a.oz));
                 --n;
             } else {
                 break;
@@ -745,14 +746,14 @@ struct Band {
             failed = true;
             return;
         }
-        h[n++] = HullEntry{px, pz, px, oz, og, seg};
+        h[n++] = HullEntry{px, pz, oz, og, seg};
         open = moments_zero();
         oox = px;
         ooz = oz;
     }
 
     // A candidate at x with the profile moments [0, x] about (0, z0) and the profile at x.
-    __device__ void candidate(PlanePoint c, const Moments &total, float z0, float oz, float og) {
+    __device__ __forceinline__ void candidate(PlanePoint c, const Moments &total, float z0, float oz, float og) {
         if (failed) return;
         float line = S.z + slope_sr * (c.x - S.x);
         if (STATE == QM_FAV) line += sag_sr.at(c.x - S.x);
@@ -768,8 +769,8 @@ struct Band {
                 if (!(c.z > h[n - 1].z)) return;
                 const HullEntry &b = h[n - 1];
                 const HullEntry &a = h[n - 2];
-                open = join(b.seg, rebase(open, b.ox, b.oz, a.ox, a.oz));
-                oox = a.ox;
+                open = join(b.seg, rebase(open, b.x, b.oz, a.x, a.oz));
+                oox = a.x;
                 ooz = a.oz;
                 --n;
             }
@@ -818,7 +819,7 @@ __device__ __noinline__ void state_boundary(Band<STATE, CAP_H> &band, const EqGe
         src_m = band.h[1].seg;
         first_og = band.h[1].og;
         rcv_m = band.h[band.n - 1].seg;
-        last_ox = band.h[band.n - 2].ox;
+        last_ox = band.h[band.n - 2].x;
         last_oz = band.h[band.n - 2].oz;
         last_og = band.h[band.n - 2].og;
     } else if (band.have_best) {
@@ -1205,13 +1206,19 @@ __device__ void evaluate_listed(const SceneDev &S, const SourceDev &src, int rx,
     float source_gf = src.gf >= 0.0f ? src.gf : g0;
     float near_source = ground_factor_near_source(direct, path_ground, source_gf);
     float att[QM_BANDS];
-    state_boundary<QM_HOM, CAP_H>(hom, direct, path_ground, near_source, source_gf, z0, g0, L, att);
-    if (hom.failed) out.status |= FAILED_CAPACITY;
+    // Each band goes to state_boundary as a copy: the band itself never has its address taken, so its
+    // fields can stay in registers through the candidate loop.
+    {
+        Band<QM_HOM, CAP_H> done = hom;
+        state_boundary<QM_HOM, CAP_H>(done, direct, path_ground, near_source, source_gf, z0, g0, L, att);
+        if (done.failed) out.status |= FAILED_CAPACITY;
+    }
 #pragma unroll
     for (int b = 0; b < QM_BANDS; ++b) out.boundary[0][b] = __expf(-att[b] * LN10_OVER_10);
     if (want_fav) {
-        state_boundary<QM_FAV, CAP_H>(fav, direct, path_ground, near_source, source_gf, z0, g0, L, att);
-        if (fav.failed) out.status |= FAILED_CAPACITY;
+        Band<QM_FAV, CAP_H> done = fav;
+        state_boundary<QM_FAV, CAP_H>(done, direct, path_ground, near_source, source_gf, z0, g0, L, att);
+        if (done.failed) out.status |= FAILED_CAPACITY;
 #pragma unroll
         for (int b = 0; b < QM_BANDS; ++b) out.boundary[1][b] = __expf(-att[b] * LN10_OVER_10);
     } else {
