@@ -177,11 +177,11 @@ def measured_peaks():
         return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "source": "fallback"}
 
 
-# DRAM bytes per path of the painting kernel, from one ncu capture of this build's kernel on a
-# small case of the workload (dram__bytes_read.sum + dram__bytes_write.sum over its paths), scaled
-# by paths to a full launch; the capture's command and figures are in
-# profiles/paint_grid_kernel_terrain.md. None where no capture of the current kernel exists.
-DRAM_BYTES_PER_PATH = {"terrain": 18429.0, "road": None}
+# DRAM bytes per path of the painting kernel, from one ncu capture of the current kernel on a small
+# case of the workload (one 16 x 8 tile x the first 20,000 sources, 2.56 M paths:
+# dram__bytes_read.sum 19.88 GB + dram__bytes_write.sum 27.09 GB), scaled by paths to a full
+# launch. None where no capture of the current kernel exists.
+DRAM_BYTES_PER_PATH = {"terrain": 18347.0, "road": None}
 
 
 def stratified_sources(grid, m, seed):
