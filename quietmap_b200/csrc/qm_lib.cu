@@ -1960,7 +1960,8 @@ static qm_status flight_sums_impl(qm_ctx *ctx, const qm_flight_boxes *boxes, qm_
     using qm::fl::Slice;
     if (!ctx || !boxes || boxes->ctx != ctx) return fail(QM_ERR_ARGUMENT, "qm_flight_sums: null ctx, or boxes of another context");
     if (n_sums && !sums) return fail(QM_ERR_ARGUMENT, "qm_flight_sums: sums is null");
-    if (n_segments && (!segments || !points)) return fail(QM_ERR_ARGUMENT, "qm_flight_sums: segments or points is null");
+    if ((n_segments && !segments) || (n_points && !points))
+        return fail(QM_ERR_ARGUMENT, "qm_flight_sums: segments or points is null");
     if (n_points >= (1ull << 31) || n_sums >= (1ull << 32) || n_segments >= (1ull << 32))
         return fail(QM_ERR_ARGUMENT, "qm_flight_sums: too many points, sums or segments");
     for (size_t i = 0; i < n_points; ++i) {
