@@ -766,6 +766,12 @@ qm_status qm_paint_grid(qm_scene *scene, const qm_grid_desc *grid, float *cell_b
     A.counters = static_cast<unsigned long long *>(d_counters.p);
     A.retry = static_cast<uint2 *>(d_retry.p);
     A.retry_count = static_cast<unsigned int *>(d_rcount.p);
+    // The terrain painter's three resident CTAs need 28 KB of shared memory (8.3 KB each plus the
+    // 1 KB the device reserves); a 32 KB carveout (14 % of 228 KB) leaves the rest of the SM's
+    // 256 KB to L1, which caches the threads' local work areas. Left to itself the driver takes
+    // 64 KB.
+    if (terrain_caps(scene))
+        QM_CUDA(cudaFuncSetAttribute(paint_grid_kernel<CapsTerrain>, cudaFuncAttributePreferredSharedMemoryCarveout, 14));
     Events ev;
     QM_CUDA(ev.create());
     QM_CUDA(cudaEventRecord(ev.e0, stream));
