@@ -772,6 +772,8 @@ qm_status qm_paint_grid(qm_scene *scene, const qm_grid_desc *grid, float *cell_b
     // 64 KB.
     if (terrain_caps(scene))
         QM_CUDA(cudaFuncSetAttribute(paint_grid_kernel<CapsTerrain>, cudaFuncAttributePreferredSharedMemoryCarveout, 14));
+    else
+        QM_CUDA(cudaFuncSetAttribute(paint_grid_kernel<CapsFlat>, cudaFuncAttributePreferredSharedMemoryCarveout, 14));
     Events ev;
     QM_CUDA(ev.create());
     QM_CUDA(cudaEventRecord(ev.e0, stream));
