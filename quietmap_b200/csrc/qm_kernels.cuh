@@ -141,9 +141,17 @@ __global__ void __launch_bounds__(128, QM_PAINT_MIN_BLOCKS) paint_grid_kernel(Sc
         PathResult r;
         r.status = 0;
         r.edges_tested = 0;
-        const int nx = warp_list_crossings<Caps::C>(S, stage, ss, src.x, src.y, rx, ry, active, own, work.xs, r.status,
-                                                    r.edges_tested);
-        if (!active) continue;
+        // Flat scenes' short rays cross few cells: each lane walks its own (the warp's shared sweep
+        // pays off on the long terrain rays).
+        int nx;
+        if constexpr (Caps::C == CapsFlat::C) {
+            if (!active) continue;
+            nx = list_crossings<Caps::C>(S, src.x, src.y, rx, ry, own, work.xs, r.status, r.edges_tested);
+        } else {
+            nx = warp_list_crossings<Caps::C>(S, stage, ss, src.x, src.y, rx, ry, active, own, work.xs, r.status,
+                                              r.edges_tested);
+            if (!active) continue;
+        }
         if (r.status == 0) {
             evaluate_listed<Caps::C, Caps::K, Caps::H>(S, src, rx, ry, alt, A.want_fav, work, nx, r, (double)src.x,
                                                        (double)src.y);
