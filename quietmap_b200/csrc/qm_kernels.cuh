@@ -103,9 +103,10 @@ __device__ __forceinline__ int2 tile_slot(int tile_w, int tile_h) {
 #endif
 
 // Thread = one receiver of a tile; CTA = (receiver tile, source chunk). Each thread walks its chunk
-// of sources and keeps its cell's band energies in compensated registers; one store per cell. The
-// warp lists the crossings of its 32 rays to each source together (warp_list_crossings: the
-// obstacle entries staged in shared memory by bulk copies); each lane then follows its own path.
+// of sources and keeps its cell's band energies in compensated registers; one store per cell. On
+// terrain the warp lists the crossings of its 32 rays to each source together (warp_list_crossings:
+// the obstacle entries staged in shared memory by bulk copies); on flat scenes each lane lists its
+// own ray's. Each lane then follows its own path.
 template <class Caps>
 __global__ void __launch_bounds__(128, QM_PAINT_MIN_BLOCKS) paint_grid_kernel(SceneDev S, GridArgs A) {
     __shared__ unsigned long long s_counts[6];
